@@ -1,0 +1,376 @@
+#!/usr/bin/env python
+"""Batched virtual-screen benchmark: ligands/s of the Monte-Carlo + BFGS docking
+search on B200, Vina scoring, FP32, search_mode fast (exhaustiveness 128,
+max_step 20), synthetic 3,000-atom receptor with a 22.5 A box at 0.375 A
+(61^3 points per map) and random-tree ligands (12..48 heavy atoms, 0..10
+torsions).  A step is one batch of ligands searched by the batched persistent
+form; `value` times the search kernels on device-resident inputs, `e2e` the
+whole C-ABI path from PDBQT text to written poses with host buffers.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "uni-dock_b200"))
+
+METRIC = "ligands/s on 1 B200, batched vs plain form, at ≤1e-4 rel energy err vs ref"
+EXHAUSTIVENESS = 128
+MAX_STEP = 20
+N_LIGANDS = 4096
+BOX = 22.5
+SPACING = 0.375
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=1024, help="ligands per step (per GPU)")
+    ap.add_argument("--plain-sample", type=int, default=32, help="ligands timed in the plain form")
+    ap.add_argument("--cpu-sample", type=int, default=16, help="ligands timed on the reference CPU path")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--chains-per-block", type=int, default=0)
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ workload
+def make_workload(seed=20261203):
+    from unidock_tools import synth
+    rec = synth.make_receptor(3000, seed=1)
+    ligs = synth.ligand_set(N_LIGANDS, seed=seed, heavy=(12, 48), torsions=(0, 10))
+    return rec, [l.to_pdbqt() for l in ligs]
+
+
+def _ligand_texts(n, start=0, seed=20261203):
+    from unidock_tools import synth
+    rng_ligs = []
+    for k in range(start, start + n):
+        # same per-ligand seeds as synth.ligand_set (sizes drawn from its stream)
+        rng_ligs.append(k)
+    return rng_ligs
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    def __init__(self):
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self, gpu_index=0):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9 or f[0] != str(gpu_index):
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def flush_l2(torch, buf):
+    buf.add_(1.0)  # 256 MB write: larger than the 126 MB L2
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args, rank, world):
+    import torch
+    from unidock_tools import engine, synth
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    rec = synth.make_receptor(3000, seed=1)
+    center = np.zeros(3, np.float32)
+    size = np.full(3, BOX, np.float32)
+    maps = engine.Maps(rec.xyz, rec.xs, center, size, SPACING)
+
+    steps_total = args.warmup + args.steps
+    B = args.batch
+    n_batches = max(1, N_LIGANDS // (B * world))
+    # ligand texts of this rank's batches (weak scaling: every rank searches B ligands per step)
+    from unidock_tools.synth import ligand_set
+    all_ligs = ligand_set(min(N_LIGANDS, B * world * min(steps_total, n_batches)), seed=20261203,
+                          heavy=(12, 48), torsions=(0, 10))
+    texts = [l.to_pdbqt() for l in all_ligs]
+
+    def batch_texts(step):
+        b = step % n_batches
+        lo = (b * world + rank) * B
+        return texts[lo:lo + B]
+
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    P = dict(exhaustiveness=EXHAUSTIVENESS, max_step=MAX_STEP, num_modes=9, min_rmsd=1.0, seed=42, form=1,
+             chains_per_block=args.chains_per_block)
+
+    # ---- device-resident form: topology uploaded before the timed region
+    batches = []
+    for s in range(steps_total):
+        ligs = [engine.Ligand(t) for t in batch_texts(s)]
+        batches.append((ligs, engine.Batch(maps, ligs)))
+    torch.cuda.synchronize()
+    for s in range(args.warmup):
+        flush_l2(torch, flush)
+        batches[s][1].search_launch(**P)
+        torch.cuda.synchronize()
+        batches[s][1].search_collect()
+    clocks = Clocks()
+    clocks.start()
+    times = []
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    for s in range(args.warmup, steps_total):
+        flush_l2(torch, flush)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        batches[s][1].search_launch(**P)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    if world > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop(dev)
+    t_total = sum(times) / 1e3
+    if world > 1:
+        tt = torch.tensor([t_total], device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_total = float(tt.item())
+    # work accounting of the timed steps (algorithmic bytes and flops per evaluation)
+    evals_total, bytes_total, flops_total = 0, 0.0, 0.0
+    for s in range(args.warmup, steps_total):
+        ligs, b = batches[s]
+        b.search_collect()
+        _, e, ev = b.chains()
+        ev = ev.reshape(len(ligs), EXHAUSTIVENESS).sum(axis=1)
+        for L, n_ev in zip(ligs, ev):
+            ex = L.export()
+            n_grid = int(np.sum(ex["xs"] < 36))
+            bytes_total += n_ev * (32.0 * n_grid + 16.0 * L.n_pairs)
+            flops_total += n_ev * (90.0 * n_grid + 22.0 * L.n_pairs + 50.0 * L.n_nodes)
+        evals_total += int(ev.sum())
+    ligands_timed = B * args.steps * world
+    value = ligands_timed / t_total
+
+    # ---- end-to-end through the C ABI with host buffers (parse -> upload -> search -> results -> text)
+    e2e_times = []
+    h2d = d2h = 0
+    for s in range(args.warmup, steps_total):
+        tx = batch_texts(s)
+        flush_l2(torch, flush)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ligs = [engine.Ligand(t) for t in tx]
+        bb = engine.Batch(maps, ligs)
+        bb.search(**P)
+        outs = [bb.write(i) for i in range(len(ligs))]
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_times.append(e0.elapsed_time(e1))
+        if s == args.warmup:
+            n_atoms = sum(L.n_atoms for L in ligs)
+            n_nodes = sum(L.n_nodes for L in ligs)
+            n_pairs = sum(L.n_pairs for L in ligs)
+            h2d = 16 * n_atoms + 48 * n_nodes + 4 * n_pairs + 48 * len(ligs) + 4 * len(ligs)
+            stride = 7 + bb.max_torsions
+            n_modes = sum(len(bb.modes(i)) for i in range(len(ligs)))
+            d2h = len(ligs) * EXHAUSTIVENESS * (4 * stride + 16) + 8 * n_modes
+            h2d += 4 * n_modes + 4 * stride * n_modes  # rescoring upload
+        del bb, ligs
+    e2e_t = sum(e2e_times) / 1e3
+    if world > 1:
+        tt = torch.tensor([e2e_t], device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        e2e_t = float(tt.item())
+    e2e_value = ligands_timed / e2e_t
+
+    # ---- plain form: one launch per ligand with fixed tiling, same search parameters
+    plain = None
+    if rank == 0 and args.plain_sample > 0:
+        ligs, b = batches[args.warmup]
+        sub = ligs[:args.plain_sample]
+        bp = engine.Batch(maps, sub)
+        bp.search_launch(**dict(P, form=0))
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        bp.search_launch(**dict(P, form=0))
+        e1.record()
+        torch.cuda.synchronize()
+        bp.search_collect()
+        plain = len(sub) / (e0.elapsed_time(e1) / 1e3)
+
+    result = None
+    if rank == 0:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+        hbm_peak = peaks.get("hbm_gbs", 6650.0)
+        fp32_peak = engine.fp32_peak_tflops()
+        ms_launch = t_total * 1e3 / args.steps
+        achieved_gbs = bytes_total / t_total / 1e9
+        achieved_tf = flops_total / t_total / 1e12
+        result = {
+            "metric": METRIC, "value": round(value, 3), "unit": "ligands/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_total * 1e3 / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded receptor, random-tree ligands)",
+            "config": {"workload": "batched virtual screen, Vina, search_mode fast (exhaustiveness 128, "
+                                   "max_step 20), 4096 ligands U{12..48} heavy / U{0..10} torsions, "
+                                   "3000-atom receptor, 22.5 A box at 0.375 A (61^3)",
+                       "ligands_per_step": B * world, "exhaustiveness": EXHAUSTIVENESS, "max_step": MAX_STEP,
+                       "form": "batched persistent", "l2": "flushed between timed steps (256 MB write)",
+                       "parallelism": f"ligand shards x{world}" if world > 1 else "1 GPU"},
+            "plain_form_ligands_per_s": None if plain is None else round(plain, 3),
+            "batched_over_plain": None if plain is None else round(value / plain, 2),
+            "evals_per_s": round(evals_total / t_total, 1),
+            "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 2), "peak": hbm_peak, "unit": "GB/s",
+                         "frac": round(achieved_gbs / hbm_peak, 4), "traffic": None,
+                         "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)",
+                         "kernel": "ud::dev::search_kernel",
+                         "fp32": {"achieved": round(achieved_tf, 3), "peak": round(fp32_peak, 2),
+                                  "unit": "TFLOP/s", "frac": round(achieved_tf / fp32_peak, 4),
+                                  "peak_source": "measured FMA probe (ud_device_fp32_peak)"},
+                         "ms_per_launch": round(ms_launch, 3)},
+            "e2e": {"value": round(e2e_value, 3), "unit": "ligands/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "clocks": clk,
+            "gpu_launches": args.steps * 1,
+        }
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return result
+
+
+# ------------------------------------------------------------------ reference CPU path
+def reference_cpu(sample, step_index, threads=None, seed=7):
+    """Reference CPU Vina search (oracle/_ref, the reference's own sources) on
+    `sample` ligands at the same exhaustiveness / max_step; returns ligands/s."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import ref
+    from unidock_tools import synth
+    if not ref.available():
+        raise RuntimeError("oracle/_ref/libudref.so missing (build it with make -C oracle)")
+    threads = threads or os.cpu_count()
+    rec = synth.make_receptor(3000, seed=1)
+    maps = ref.RefMaps(rec.xyz, rec.xs, np.zeros(3, np.float32), np.full(3, BOX, np.float32), SPACING)
+    ligs = synth.ligand_set(sample * (step_index + 1), seed=20261203, heavy=(12, 48), torsions=(0, 10))
+    ligs = ligs[sample * step_index:]
+    t_total = 0.0
+    with tempfile.TemporaryDirectory() as d:
+        for k, L in enumerate(ligs):
+            p = Path(d) / f"l{k}.pdbqt"
+            p.write_text(L.to_pdbqt())
+            R = ref.RefLigand(p)
+            heur = R.n_atoms + 10 * (6 + R.n_torsions)
+            gsteps = min(70 * 3 * (50 + heur) // 2, MAX_STEP)
+            t0 = time.perf_counter()
+            R.mc(maps, seed, EXHAUSTIVENESS, gsteps, None, threads)
+            t_total += time.perf_counter() - t0
+    return len(ligs) / t_total, threads
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    sample = max(1, args.cpu_sample)
+    for s in range(args.warmup):
+        reference_cpu(1, s)
+    vals = []
+    for s in range(args.steps):
+        v, thr = reference_cpu(sample, args.warmup + s)
+        vals.append(v)
+    value = len(vals) * sample / sum(sample / v for v in vals)
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "ligands/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * sample / value, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded receptor, random-tree ligands)",
+        "config": {"workload": "batched virtual screen, Vina, search_mode fast (exhaustiveness 128, max_step 20), "
+                               "4096 ligands U{12..48} heavy / U{0..10} torsions, 3000-atom receptor, 22.5 A box",
+                   "sample_ligands_per_step": sample},
+        "cpu_baseline": {"value": round(value, 4), "unit": "ligands/s", "cores": thr, "kind": "reference",
+                         "sample": f"{sample} ligands per step x {args.steps} steps, 128 chains x 20 MC steps each, "
+                                   "reference CPU Vina search (unidock/src/lib compiled by oracle/Makefile)"},
+        "e2e": {"value": round(value, 4), "unit": "ligands/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus == 1 else 1)))
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+    else:
+        res = run_ours(args, rank, world)
+        if res is not None and world == 1 and not args.no_cpu_baseline:
+            try:
+                v, thr = reference_cpu(args.cpu_sample, 0)
+                res["cpu_baseline"] = {"value": round(v, 4), "unit": "ligands/s", "cores": thr, "kind": "reference",
+                                       "sample": f"{args.cpu_sample} ligands, 128 chains x 20 MC steps, reference "
+                                                 "CPU Vina search on all host threads"}
+            except Exception as ex:  # the baseline never blocks the GPU line
+                res["cpu_baseline"] = {"value": None, "unit": "ligands/s", "cores": os.cpu_count(),
+                                       "kind": "reference", "sample": f"unavailable: {ex}"}
+    if res is not None:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,173 @@
+/*
+ * unidock_b200 -- C ABI of the B200 docking engine.
+ *
+ * The reference (dptech-corp/Uni-Dock) has no C ABI: its batched search sits
+ * behind internal C++ calls.  Each entry point below names the reference
+ * interface it replaces.  All arguments are plain pointers and sizes; device
+ * memory is owned by the library behind opaque handles; host arrays are owned
+ * by the caller.  Every function returns UD_OK (0) or an error code and never
+ * throws or exits; ud_last_error() describes the last failure of the calling
+ * thread.  A `stream` argument is a cudaStream_t (NULL = default stream).
+ */
+#ifndef UNIDOCK_B200_H
+#define UNIDOCK_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UD_OK 0
+#define UD_ERR_ARG 1      /* invalid argument */
+#define UD_ERR_PARSE 2    /* malformed PDBQT input */
+#define UD_ERR_CUDA 3     /* CUDA runtime failure (message has the CUDA error) */
+#define UD_ERR_CAPACITY 4 /* ligand exceeds a capacity limit (atoms, torsions) */
+#define UD_ERR_STATE 5    /* call out of order (e.g. results before a search) */
+
+#define UD_SF_VINA 0
+#define UD_SF_AD4 1
+#define UD_SF_VINARDO 2
+
+typedef struct ud_maps_s* ud_maps;
+typedef struct ud_ligand_s* ud_ligand;
+typedef struct ud_batch_s* ud_batch;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int ud_version(void);
+/* Message of the last failed call on this thread ("" if none). */
+const char* ud_last_error(void);
+
+/* ---------------------------------------------------------------- receptor
+ * Parse a rigid receptor PDBQT and assign X-Score types from its bonds.
+ * Replaces parse_receptor_pdbqt (unidock/src/lib/parse_pdbqt.cpp:1214) +
+ * model::assign_types (unidock/src/lib/model.cpp:408).  With xyz/xs NULL only
+ * *n_atoms is set.  Untyped atoms (hydrogens) get xs = 36. */
+int ud_receptor_parse(const char* pdbqt, size_t len, float* xyz, int* xs, int capacity,
+                      int* n_atoms);
+
+/* ---------------------------------------------------------------- grid maps
+ * Build grid maps on the GPU for the listed XS types (all 24 Vina map types
+ * when types == NULL) over the box center +- size/2 at `spacing`.
+ * Replaces Vina::compute_vina_maps (unidock/src/lib/vina.cpp:491-567) and
+ * cache::populate_no_bias (unidock/src/lib/cache.cpp:471-549).  `sf` is
+ * UD_SF_VINA or UD_SF_VINARDO; weights follow the reference's order
+ * (Vina: gauss1, gauss2, repulsion, hydrophobic, hbond, glue, rot) with the
+ * rotatable weight in raw form (e.g. 0.05846); NULL = defaults. */
+int ud_maps_create(int sf, const float* weights, int n_weights, const float* rec_xyz,
+                   const int* rec_xs, int n_rec, const float center[3], const float size[3],
+                   float spacing, const int* types, int n_types, void* stream, ud_maps* out);
+/* dims[3] sample points, init[3] box corner, factor[3] samples per Angstrom. */
+int ud_maps_info(ud_maps maps, int dims[3], float init[3], float factor[3], int* n_maps);
+/* Copy the map of XS type `xs` to host memory (dims[0]*dims[1]*dims[2] floats,
+ * x fastest).  Replaces igrid::get_grids (unidock/src/lib/igrid.h:39). */
+int ud_maps_read(ud_maps maps, int xs, float* out, size_t n);
+int ud_maps_destroy(ud_maps maps);
+
+/* ---------------------------------------------------------------- ligands
+ * Parse a Vina PDBQT ligand into a torsion-tree model (host memory).
+ * Replaces parse_ligand_pdbqt_from_file_no_failure
+ * (unidock/src/lib/parse_pdbqt.cpp:1089-1122) + model::initialize
+ * (unidock/src/lib/model.cpp:613-619). */
+int ud_ligand_parse(const char* pdbqt, size_t len, ud_ligand* out);
+/* counts[0] atoms, [1] heavy atoms, [2] torsions, [3] rigid nodes,
+ * [4] intramolecular pairs, [5] TORSDOF, [6] glue pairs, [7] BFGS steps. */
+int ud_ligand_counts(ud_ligand lig, int counts[8]);
+/* Flat export of the model; any pointer may be NULL.  node_rel holds 6 floats
+ * per node (origin relative to parent, unit axis), input frame. */
+int ud_ligand_export(ud_ligand lig, float* lab_xyz, float* local_xyz, int* xs, int* ad, int* el,
+                     float* charge, int* atom_node, int* node_parent, int* node_begin,
+                     int* node_end, float* node_rel, int* pair_a, int* pair_b);
+/* Pose of the input coordinates: [x y z qw qx qy qz t0 .. t(T-1)]. */
+int ud_ligand_initial_pose(ud_ligand lig, float* pose);
+/* Lab coordinates (3 per atom) of a pose (host forward kinematics,
+ * model::set, unidock/src/lib/model.cpp:848-851). */
+int ud_ligand_coords(ud_ligand lig, const float* pose, float* xyz);
+/* Conformation-independent inputs (num_tors, num_rotors, heavy atoms,
+ * hydrophobic atoms, h-bond atoms, ligands, length). */
+int ud_ligand_conf_indep(ud_ligand lig, float out[7]);
+int ud_ligand_destroy(ud_ligand lig);
+
+/* ---------------------------------------------------------------- batches
+ * Upload the topology of n ligands to device memory for scoring and search
+ * against `maps`.  Replaces the per-batch marshalling of do_docking_base
+ * (unidock/src/cuda/monte_carlo.cu:2397-2900) and precalculate_parallel
+ * (unidock/src/cuda/precalculate.cu:169-326): type-pair tables of the
+ * scoring function are shared by all ligands. */
+int ud_batch_create(ud_maps maps, const ud_ligand* ligs, int n, void* stream, ud_batch* out);
+int ud_batch_destroy(ud_batch batch);
+
+/* Energy and pose gradient at fixed poses, host buffers.  pose_ligand[i]
+ * selects the ligand of pose i; poses has pose_stride floats per pose in the
+ * layout of ud_ligand_initial_pose; g_out receives 6 + T floats per pose in
+ * the reference's change layout (d/dposition, torque, d/dtorsions) with
+ * stride g_stride.  v_intra / v_inter are the curl caps of the intramolecular
+ * and grid terms (1000 = scoring, 10 = search).  Replaces model::eval_deriv
+ * (unidock/src/lib/model.cpp:935-962). */
+int ud_score_grad(ud_batch batch, const int* pose_ligand, const float* poses, int n_poses,
+                  int pose_stride, float v_intra, float v_inter, float* e_out, float* g_out,
+                  int g_stride, void* stream);
+/* Same with device pointers; asynchronous on `stream`. */
+int ud_score_grad_device(ud_batch batch, const int* pose_ligand, const float* poses, int n_poses,
+                         int pose_stride, float v_intra, float v_inter, float* e_out,
+                         float* g_out, int g_stride, void* stream);
+/* Scoring-path energies: out[2*i] grid (cache::eval, cache.cpp:84-120),
+ * out[2*i+1] intramolecular pairs from the nearest-bin table (model::evali,
+ * model.cpp:927-933), both with curl cap v. */
+int ud_score(ud_batch batch, const int* pose_ligand, const float* poses, int n_poses,
+             int pose_stride, float v, float* out, void* stream);
+
+/* ---------------------------------------------------------------- search */
+typedef struct {
+    int exhaustiveness;     /* MC chains per ligand (--exhaustiveness) */
+    int max_step;           /* cap on MC steps per chain, 0 = heuristic only (--max_step) */
+    int num_modes;          /* poses kept per ligand (--num_modes) */
+    float min_rmsd;         /* clustering radius (--min_rmsd) */
+    float energy_range;     /* output energy window (--energy_range) */
+    unsigned long long seed;/* --seed */
+    int form;               /* 0 = plain (one launch per ligand), 1 = batched persistent */
+    int chains_per_block;   /* warps (chains) per CTA, 0 = autotuned/default */
+    int bfgs_cap;           /* 0 = per-ligand (25 + atoms)/3 BFGS steps; >0 caps it */
+    int use_graph;          /* batched form: replay the per-batch sequence as a CUDA graph */
+} ud_search_params;
+
+/* Run the Monte-Carlo + BFGS search of every ligand of the batch.
+ * Replaces Vina::global_search_gpu (unidock/src/lib/vina.h:154-354) and
+ * monte_carlo_template::do_docking (unidock/src/cuda/monte_carlo.cu:2975-3010).
+ * Synchronous: returns after the results are on the host. */
+int ud_search(ud_batch batch, const ud_search_params* params, void* stream);
+/* ud_search split in two: the asynchronous device part (kernels enqueued on
+ * `stream`, inputs already resident) and the host part (device-to-host copy,
+ * clustering, rescoring).  ud_search == ud_search_launch + ud_search_collect. */
+int ud_search_launch(ud_batch batch, const ud_search_params* params, void* stream);
+int ud_search_collect(ud_batch batch, void* stream);
+/* Raw per-chain results of the last search: best pose (pose_stride floats
+ * per chain, chain-major per ligand), best energy and evaluations spent. */
+int ud_search_chains(ud_batch batch, float* poses, int pose_stride, float* e, int* evals);
+/* Number of modes kept for ligand `lig` after clustering and rescoring. */
+int ud_result_count(ud_batch batch, int lig, int* n_modes);
+/* Mode k of ligand `lig`: pose (7+T floats) and
+ * energies[8] = {affinity, rmsd_lb, rmsd_ub, inter+intra, inter, intra,
+ * conf_independent, unbound} as written in "REMARK VINA RESULT"
+ * (unidock/src/lib/vina.cpp:725-748). */
+int ud_result_mode(ud_batch batch, int lig, int k, float* pose, float energies[8]);
+/* Output text of ligand `lig` (format 0 = PDBQT MODEL blocks, 1 = SDF),
+ * written into buf (cap bytes, NUL-terminated); *len = full length.
+ * Replaces Vina::get_poses_gpu / get_sdf_poses_gpu (vina.cpp:872-996). */
+int ud_result_write(ud_batch batch, int lig, int format, char* buf, size_t cap, size_t* len);
+/* Local optimisation (BFGS at curl cap v, max_steps iterations or the
+ * per-ligand (25 + atoms)/3 when 0) from the given poses, updated in place.
+ * Replaces quasi_newton::operator() (unidock/src/lib/quasi_newton.cpp:42-53),
+ * the --local_only path of Vina::optimize (unidock/src/lib/vina.cpp:1385-1428). */
+int ud_optimize(ud_batch batch, const int* pose_ligand, float* poses, int n_poses, int pose_stride,
+                int max_steps, float v, float* e_out, int* evals_out, void* stream);
+/* Measured FP32 FMA throughput of the current device in TFLOP/s (roofline
+ * denominator of the search kernels).  No counterpart in the reference. */
+int ud_device_fp32_peak(float* tflops);
+/* Evaluations and device time of the last search. */
+int ud_search_stats(ud_batch batch, long long* evals, float* kernel_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UNIDOCK_B200_H */

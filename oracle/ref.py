@@ -1,0 +1,180 @@
+"""Test-only ctypes wrapper of oracle/_ref/libudref.so: the reference's own CPU
+sources (unidock/src/lib) built by oracle/Makefile.  Only tests, the bench's CPU
+baseline leg and the smoke check call it."""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB = Path(__file__).resolve().parent / "_ref" / "libudref.so"
+_lib = None
+
+
+def available() -> bool:
+    return LIB.exists()
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(str(LIB))
+        vp, fp, ip = C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_int)
+        L.udref_maps_new.restype = vp
+        L.udref_maps_new.argtypes = [C.c_int, fp, C.c_int, fp, ip, C.c_int, fp, fp, C.c_float, ip, C.c_int]
+        L.udref_maps_free.argtypes = [vp]
+        L.udref_maps_dims.argtypes = [vp, ip, fp, fp, fp]
+        L.udref_maps_get.argtypes = [vp, C.c_int, fp]
+        L.udref_table_fast.argtypes = [vp, C.c_int, C.c_int, C.c_float]
+        L.udref_table_fast.restype = C.c_float
+        L.udref_ligand_new.restype = vp
+        L.udref_ligand_new.argtypes = [C.c_char_p, C.c_int, fp, C.c_int]
+        L.udref_ligand_free.argtypes = [vp]
+        L.udref_ligand_counts.argtypes = [vp, ip]
+        L.udref_ligand_atoms.argtypes = [vp, fp, fp, ip, ip, ip, fp]
+        L.udref_ligand_pairs.argtypes = [vp, ip, ip]
+        L.udref_ligand_tree.argtypes = [vp, ip, ip, ip, fp]
+        L.udref_initial_conf.argtypes = [vp, fp, fp, fp]
+        L.udref_ligand_conf_indep.argtypes = [vp, fp]
+        L.udref_eval_deriv.argtypes = [vp, vp, fp, fp, fp, C.c_float, C.c_float, fp, fp]
+        L.udref_eval_deriv.restype = C.c_float
+        L.udref_score.argtypes = [vp, vp, fp, fp, fp, C.c_float, fp]
+        L.udref_bfgs.argtypes = [vp, vp, fp, fp, fp, C.c_float, C.c_int, ip]
+        L.udref_bfgs.restype = C.c_float
+        L.udref_mc.argtypes = [vp, vp, C.c_uint, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, fp, fp, C.c_int,
+                               C.POINTER(C.c_longlong)]
+        _lib = L
+    return _lib
+
+
+def _f(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _i(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+VINA_W = np.array([-0.035579, -0.005156, 0.840245, -0.035069, -0.587439, 50, 5 * 0.05846 / 0.1 - 1], np.float32)
+VINARDO_W = np.array([-0.045, 0.8, -0.035, -0.600, 50, 5 * 0.05846 / 0.1 - 1], np.float32)
+
+
+def weights_for(sf):
+    return {0: VINA_W, 2: VINARDO_W}[sf]
+
+
+class RefMaps:
+    def __init__(self, rec_xyz, rec_xs, center, size, spacing=0.375, sf=0, types=None):
+        w = weights_for(sf)
+        xyz = np.ascontiguousarray(rec_xyz, np.float32)
+        xs = np.ascontiguousarray(rec_xs, np.int32)
+        c = np.ascontiguousarray(center, np.float32)
+        s = np.ascontiguousarray(size, np.float32)
+        t = np.ascontiguousarray(types if types is not None else np.arange(36), np.int32)
+        self.h = lib().udref_maps_new(sf, _f(w), len(w), _f(xyz), _i(xs), len(xs), _f(c), _f(s), spacing, _i(t), len(t))
+        if not self.h:
+            raise RuntimeError("reference maps failed")
+        self.dims = np.zeros(3, np.int32)
+        self.init = np.zeros(3, np.float32)
+        self.factor = np.zeros(3, np.float32)
+        self.factor_inv = np.zeros(3, np.float32)
+        lib().udref_maps_dims(self.h, _i(self.dims), _f(self.init), _f(self.factor), _f(self.factor_inv))
+
+    def get(self, xs):
+        out = np.zeros(int(self.dims.prod()), np.float32)
+        n = lib().udref_maps_get(self.h, int(xs), _f(out))
+        if n < 0:
+            return None
+        return out.reshape(self.dims[2], self.dims[1], self.dims[0])
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().udref_maps_free(self.h)
+
+
+class RefLigand:
+    def __init__(self, path, sf=0):
+        w = weights_for(sf)
+        self.h = lib().udref_ligand_new(str(path).encode(), sf, _f(w), len(w))
+        if not self.h:
+            raise RuntimeError("reference parse failed")
+        c = np.zeros(5, np.int32)
+        lib().udref_ligand_counts(self.h, _i(c))
+        self.n_atoms, self.n_movable, self.n_torsions, self.n_pairs, self.n_nodes = [int(v) for v in c]
+
+    def atoms(self):
+        n = self.n_atoms
+        lab = np.zeros((n, 3), np.float32)
+        local = np.zeros((n, 3), np.float32)
+        xs = np.zeros(n, np.int32)
+        ad = np.zeros(n, np.int32)
+        el = np.zeros(n, np.int32)
+        q = np.zeros(n, np.float32)
+        lib().udref_ligand_atoms(self.h, _f(lab), _f(local), _i(xs), _i(ad), _i(el), _f(q))
+        return dict(lab=lab, local=local, xs=xs, ad=ad, el=el, charge=q)
+
+    def pairs(self):
+        a = np.zeros(max(self.n_pairs, 1), np.int32)
+        b = np.zeros(max(self.n_pairs, 1), np.int32)
+        lib().udref_ligand_pairs(self.h, _i(a), _i(b))
+        return a[:self.n_pairs], b[:self.n_pairs]
+
+    def tree(self):
+        R = self.n_nodes
+        par = np.zeros(R + 64, np.int32)
+        beg = np.zeros(R + 64, np.int32)
+        end = np.zeros(R + 64, np.int32)
+        rel = np.zeros((R + 64, 6), np.float32)
+        n = lib().udref_ligand_tree(self.h, _i(par), _i(beg), _i(end), _f(rel))
+        return par[:n], beg[:n], end[:n], rel[:n]
+
+    def conf_indep(self):
+        o = np.zeros(7, np.float32)
+        lib().udref_ligand_conf_indep(self.h, _f(o))
+        return o
+
+    def initial_pose(self):
+        p = np.zeros(3, np.float32)
+        q = np.zeros(4, np.float32)
+        t = np.zeros(max(self.n_torsions, 1), np.float32)
+        lib().udref_initial_conf(self.h, _f(p), _f(q), _f(t))
+        return np.concatenate([p, q, t[:self.n_torsions]])
+
+    def eval_deriv(self, maps, pose, v_intra=1000.0, v_inter=1000.0):
+        pose = np.ascontiguousarray(pose, np.float32)
+        p, q, t = pose[0:3].copy(), pose[3:7].copy(), np.ascontiguousarray(pose[7:].copy() if self.n_torsions else np.zeros(1, np.float32))
+        g = np.zeros(6 + self.n_torsions, np.float32)
+        xyz = np.zeros((self.n_atoms, 3), np.float32)
+        e = lib().udref_eval_deriv(self.h, maps.h, _f(p), _f(q), _f(t), v_intra, v_inter, _f(g), _f(xyz))
+        return float(e), g, xyz
+
+    def score(self, maps, pose, v=1000.0):
+        pose = np.ascontiguousarray(pose, np.float32)
+        p, q, t = pose[0:3].copy(), pose[3:7].copy(), np.ascontiguousarray(pose[7:].copy() if self.n_torsions else np.zeros(1, np.float32))
+        out = np.zeros(4, np.float32)
+        lib().udref_score(self.h, maps.h, _f(p), _f(q), _f(t), v, _f(out))
+        return out
+
+    def bfgs(self, maps, pose, v=10.0, max_steps=None):
+        pose = np.array(pose, np.float32)
+        p, q = pose[0:3].copy(), pose[3:7].copy()
+        t = pose[7:].copy() if self.n_torsions else np.zeros(1, np.float32)
+        steps = (25 + self.n_atoms) // 3 if max_steps is None else max_steps
+        ec = C.c_int()
+        e = lib().udref_bfgs(self.h, maps.h, _f(p), _f(q), _f(t), v, steps, C.byref(ec))
+        return float(e), np.concatenate([p, q, t[:self.n_torsions]]), ec.value
+
+    def mc(self, maps, seed, n_chains, global_steps, local_steps=None, threads=1, hunt_cap=10.0):
+        steps = (25 + self.n_atoms) // 3 if local_steps is None else local_steps
+        stride = 7 + self.n_torsions
+        be = np.zeros(n_chains, np.float32)
+        bp = np.zeros((n_chains, stride), np.float32)
+        ev = C.c_longlong()
+        lib().udref_mc(self.h, maps.h, seed, n_chains, global_steps, steps, threads, hunt_cap, _f(be), _f(bp),
+                       stride, C.byref(ev))
+        return be, bp, ev.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().udref_ligand_free(self.h)

@@ -1,0 +1,2 @@
+#pragma once
+#include "_shim_common.hpp"

@@ -1,0 +1,965 @@
+// C ABI of the engine (include/unidock_b200.h): handle management, host <->
+// device marshalling, batch scheduling and result post-processing.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <thread>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <iomanip>
+#include <memory>
+#include <numeric>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/unidock_b200.h"
+#include "ud_engine.h"
+#include "ud_model.h"
+
+namespace ud {
+// ud_engine.cu
+struct DeviceBatchView {
+    const LigDesc* ligs;
+    const AtomRec* atoms;
+    const NodeRec* nodes;
+    const uint32_t* pairs;
+    int max_atoms, max_torsions;
+};
+struct DeviceMapsView {
+    const float* data;
+    MapsDesc desc;
+};
+struct DeviceTablesView {
+    const float* smooth;
+    const float* fast;
+    int n_bins;
+    float factor;
+    float cutoff2;
+};
+cudaError_t launch_maps(const float* rec_xyzt, int n_rec, const float* fastT, int n_bins, int n_slots,
+                        int n_slots_pad, float factor, float cutoff2, const MapsDesc& d, float* out,
+                        cudaStream_t stream);
+cudaError_t launch_score(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
+                         const int* pose_lig, const float* poses, int pose_stride, int n_poses,
+                         float v_intra, float v_inter, float* e_out, float* g_out, int g_stride,
+                         float* score_out, cudaStream_t stream);
+cudaError_t launch_search(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
+                          const SearchParams& P, const int* order, int n_items, int first_item,
+                          unsigned int* queue, float* poses, int pose_stride, ChainResult* results,
+                          int grid_blocks, cudaStream_t stream);
+int search_blocks_per_sm(const DeviceBatchView& b, int warps);
+cudaError_t launch_optimize(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
+                            const int* pose_lig, float* poses, int pose_stride, int n_poses, int max_steps,
+                            float v, float* e_out, int* evals_out, cudaStream_t stream);
+float measure_fp32_peak_tflops();
+int engine_chain_smem_bytes(int max_atoms, int max_torsions);
+}  // namespace ud
+
+using namespace ud;
+
+namespace {
+
+thread_local std::string g_error;
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess)
+        throw Error(UD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorName(e) + " " + cudaGetErrorString(e));
+}
+
+template <class T> struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count) {
+        if (count <= n && p) return;
+        release();
+        cuda_check(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)), "cudaMalloc");
+        n = count;
+    }
+    void upload(const T* src, size_t count, cudaStream_t s) {
+        alloc(count);
+        if (count) cuda_check(cudaMemcpyAsync(p, src, count * sizeof(T), cudaMemcpyHostToDevice, s), "H2D");
+    }
+};
+
+template <class F> int guarded(F&& f) {
+    try {
+        f();
+        return UD_OK;
+    } catch (const Error& e) {
+        g_error = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return UD_ERR_PARSE;
+    } catch (...) {
+        g_error = "unknown error";
+        return UD_ERR_ARG;
+    }
+}
+
+}  // namespace
+
+struct ud_maps_s {
+    Scoring sf;
+    MapsDesc desc{};
+    std::vector<int> slot_types;     // XS type of each map slot
+    DevBuf<float> maps;              // [slot][z][y][x]
+    DevBuf<float> smooth;            // [tp][bin][2]
+    DevBuf<float> fast;              // [tp][bin]
+    int n_bins = 0;
+    float factor = 32.0f;
+    float cutoff2 = 64.0f;
+};
+
+struct LigandPost {
+    std::vector<PoseResult> modes;
+};
+
+struct ud_ligand_s {
+    Ligand lig;
+};
+
+struct ud_batch_s {
+    ud_maps maps = nullptr;
+    std::vector<const Ligand*> ligs;
+    std::vector<LigDesc> desc;
+    DevBuf<LigDesc> d_desc;
+    DevBuf<AtomRec> d_atoms;
+    DevBuf<NodeRec> d_nodes;
+    DevBuf<uint32_t> d_pairs;
+    int max_atoms = 0, max_tors = 0;
+    // search state
+    DevBuf<int> d_order;
+    DevBuf<unsigned int> d_queue;
+    DevBuf<float> d_poses;
+    DevBuf<ChainResult> d_results;
+    std::vector<float> h_poses;
+    std::vector<ChainResult> h_results;
+    int pose_stride = 0;
+    int exhaustiveness = 0;
+    bool searched = false;
+    bool launched = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    long long evals = 0;
+    float kernel_ms = 0;
+    std::vector<LigandPost> post;
+    ud_search_params params{};
+    // scoring scratch
+    DevBuf<int> d_pose_lig;
+    DevBuf<float> d_pose;
+    DevBuf<float> d_e, d_g, d_score;
+
+    ~ud_batch_s() {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
+    DeviceBatchView view() const {
+        return DeviceBatchView{d_desc.p, d_atoms.p, d_nodes.p, d_pairs.p, max_atoms, max_tors};
+    }
+};
+
+static DeviceMapsView maps_view(const ud_maps_s* m) { return DeviceMapsView{m->maps.p, m->desc}; }
+static DeviceTablesView tables_view(const ud_maps_s* m) {
+    return DeviceTablesView{m->smooth.p, m->fast.p, m->n_bins, m->factor, m->cutoff2};
+}
+
+// ---------------------------------------------------------------- receptor
+
+extern "C" int ud_version(void) { return 100; }
+extern "C" const char* ud_last_error(void) { return g_error.c_str(); }
+
+extern "C" int ud_receptor_parse(const char* pdbqt, size_t len, float* xyz, int* xs, int capacity,
+                                 int* n_atoms) {
+    return guarded([&] {
+        if (!pdbqt || !n_atoms) throw Error(UD_ERR_ARG, "null argument");
+        Receptor R = parse_receptor_pdbqt(std::string(pdbqt, len));
+        *n_atoms = (int)R.xyz.size();
+        if (xyz || xs) {
+            if (capacity < (int)R.xyz.size()) throw Error(UD_ERR_CAPACITY, "receptor capacity too small");
+            for (size_t i = 0; i < R.xyz.size(); ++i) {
+                if (xyz)
+                    for (int k = 0; k < 3; ++k) xyz[3 * i + k] = R.xyz[i][k];
+                if (xs) xs[i] = R.xs[i];
+            }
+        }
+    });
+}
+
+// ---------------------------------------------------------------- maps
+
+static std::vector<int> default_map_types() {
+    // Vina batch mode computes all XS types of the scoring function with CG
+    // folded onto C_H/C_P and glue types skipped (cache.cpp:476-505).
+    std::vector<int> t;
+    for (int i = 0; i < XS_SIZE; ++i) {
+        int g = xs_grid_type(i);
+        if (g >= 0 && std::find(t.begin(), t.end(), g) == t.end()) t.push_back(g);
+    }
+    return t;
+}
+
+extern "C" int ud_maps_create(int sf, const float* weights, int n_weights, const float* rec_xyz,
+                              const int* rec_xs, int n_rec, const float center[3], const float size[3],
+                              float spacing, const int* types, int n_types, void* stream, ud_maps* out) {
+    return guarded([&] {
+        if (!out || !center || !size || (n_rec > 0 && (!rec_xyz || !rec_xs)) || spacing <= 0)
+            throw Error(UD_ERR_ARG, "invalid maps arguments");
+        if (sf != UD_SF_VINA && sf != UD_SF_VINARDO)
+            throw Error(UD_ERR_ARG, "grid maps are built for Vina or Vinardo scoring");
+        for (int i = 0; i < 3; ++i)
+            if (!(size[i] > 0)) throw Error(UD_ERR_ARG, "box size must be positive");
+        cudaStream_t s = (cudaStream_t)stream;
+        auto m = std::make_unique<ud_maps_s>();
+        std::vector<float> w;
+        if (weights && n_weights > 0) {
+            w.assign(weights, weights + n_weights);
+            // rotatable weight given raw: store 5*w/0.1-1 (vina.cpp:392-432)
+            w.back() = (float)(5 * (double)w.back() / 0.1 - 1);
+        }
+        m->sf = Scoring::make(sf, w.empty() ? nullptr : w.data(), (int)w.size());
+        // box (vina.cpp:528-539) and grid frame (grid.cpp:25-38)
+        MapsDesc& d = m->desc;
+        for (int i = 0; i < 3; ++i) {
+            size_t nvox = (size_t)std::ceil((float)size[i] / (float)spacing);
+            float real_span = (float)spacing * nvox;
+            float begin = (float)center[i] - real_span / 2;
+            float end = begin + real_span;
+            d.dims[i] = (int)nvox + 1;
+            d.init[i] = begin;
+            d.corner2[i] = end;
+            float range = end - begin;
+            d.dim_m1[i] = (float)(d.dims[i] - 1);
+            d.factor[i] = d.dim_m1[i] / range;
+            d.factor_inv[i] = 1 / d.factor[i];
+        }
+        d.slope = 1e6f;
+        std::vector<int> req = types && n_types > 0 ? std::vector<int>(types, types + n_types) : default_map_types();
+        for (int t : req) {
+            int g = xs_grid_type(t);
+            if (g < 0) continue;
+            if (std::find(m->slot_types.begin(), m->slot_types.end(), g) == m->slot_types.end())
+                m->slot_types.push_back(g);
+        }
+        if (m->slot_types.size() > 36) throw Error(UD_ERR_ARG, "too many map types");
+        std::fill(d.slot_of_xs, d.slot_of_xs + 36, (int8_t)-1);
+        for (size_t k = 0; k < m->slot_types.size(); ++k) d.slot_of_xs[m->slot_types[k]] = (int8_t)k;
+        d.n_maps = (int)m->slot_types.size();
+        // pair tables of the scoring function
+        PairTable tab;
+        tab.build(m->sf);
+        m->n_bins = tab.n;
+        m->factor = tab.factor;
+        m->cutoff2 = m->sf.cutoff * m->sf.cutoff;
+        m->smooth.upload(tab.smooth.data(), tab.smooth.size(), s);
+        m->fast.upload(tab.fast.data(), tab.fast.size(), s);
+        // receptor-type-major table for the map kernel: [t1][bin][slot]
+        const int nslot = d.n_maps, nslot_pad = std::max(4, (nslot + 3) & ~3);
+        std::vector<float> fastT((size_t)XS_SIZE * tab.n * nslot_pad, 0.0f);
+        for (int t1 = 0; t1 < XS_SIZE; ++t1)
+            for (int k = 0; k < nslot; ++k) {
+                const float* row = &tab.fast[(size_t)tri_index(t1, m->slot_types[k]) * tab.n];
+                for (int b = 0; b < tab.n; ++b) fastT[((size_t)t1 * tab.n + b) * nslot_pad + k] = row[b];
+            }
+        DevBuf<float> d_fastT;
+        d_fastT.upload(fastT.data(), fastT.size(), s);
+        std::vector<float> rec;
+        rec.reserve(4 * (size_t)n_rec);
+        for (int i = 0; i < n_rec; ++i) {
+            if (rec_xs[i] < 0 || rec_xs[i] >= XS_SIZE) continue;  // untyped atoms contribute nothing
+            rec.push_back(rec_xyz[3 * i]);
+            rec.push_back(rec_xyz[3 * i + 1]);
+            rec.push_back(rec_xyz[3 * i + 2]);
+            int t = rec_xs[i];
+            float tf;
+            std::memcpy(&tf, &t, 4);
+            rec.push_back(tf);
+        }
+        DevBuf<float> d_rec;
+        d_rec.upload(rec.data(), rec.size(), s);
+        const size_t plane = (size_t)d.dims[0] * d.dims[1] * d.dims[2];
+        m->maps.alloc(plane * std::max(1, nslot));
+        if (nslot > 0) {
+            cuda_check(launch_maps(d_rec.p, (int)(rec.size() / 4), d_fastT.p, tab.n, nslot, nslot_pad,
+                                   tab.factor, m->cutoff2, d, m->maps.p, s),
+                       "maps kernel");
+        }
+        cuda_check(cudaStreamSynchronize(s), "maps sync");
+        *out = m.release();
+    });
+}
+
+extern "C" int ud_maps_info(ud_maps maps, int dims[3], float init[3], float factor[3], int* n_maps) {
+    return guarded([&] {
+        if (!maps) throw Error(UD_ERR_ARG, "null maps");
+        for (int i = 0; i < 3; ++i) {
+            if (dims) dims[i] = maps->desc.dims[i];
+            if (init) init[i] = maps->desc.init[i];
+            if (factor) factor[i] = maps->desc.factor[i];
+        }
+        if (n_maps) *n_maps = maps->desc.n_maps;
+    });
+}
+
+extern "C" int ud_maps_read(ud_maps maps, int xs, float* out, size_t n) {
+    return guarded([&] {
+        if (!maps || !out || xs < 0 || xs >= XS_SIZE) throw Error(UD_ERR_ARG, "invalid argument");
+        int slot = maps->desc.slot_of_xs[xs];
+        if (slot < 0) throw Error(UD_ERR_ARG, std::string("no map for type ") + xs_name(xs));
+        const size_t plane = (size_t)maps->desc.dims[0] * maps->desc.dims[1] * maps->desc.dims[2];
+        if (n < plane) throw Error(UD_ERR_CAPACITY, "output buffer too small");
+        cuda_check(cudaMemcpy(out, maps->maps.p + plane * slot, plane * sizeof(float), cudaMemcpyDeviceToHost),
+                   "map D2H");
+    });
+}
+
+extern "C" int ud_maps_destroy(ud_maps maps) {
+    delete maps;
+    return UD_OK;
+}
+
+// ---------------------------------------------------------------- ligands
+
+static int ligand_local_steps(const Ligand& L) { return (25 + (int)L.atoms.size()) / 3; }
+
+extern "C" int ud_ligand_parse(const char* pdbqt, size_t len, ud_ligand* out) {
+    return guarded([&] {
+        if (!pdbqt || !out) throw Error(UD_ERR_ARG, "null argument");
+        auto h = std::make_unique<ud_ligand_s>();
+        h->lig = parse_ligand_pdbqt(std::string(pdbqt, len));
+        *out = h.release();
+    });
+}
+
+extern "C" int ud_ligand_counts(ud_ligand lig, int counts[8]) {
+    return guarded([&] {
+        if (!lig || !counts) throw Error(UD_ERR_ARG, "null argument");
+        const Ligand& L = lig->lig;
+        counts[0] = (int)L.atoms.size();
+        counts[1] = L.n_heavy();
+        counts[2] = L.n_torsions();
+        counts[3] = (int)L.nodes.size();
+        counts[4] = (int)L.pairs.size();
+        counts[5] = L.torsdof;
+        counts[6] = (int)L.glue_pairs.size();
+        counts[7] = ligand_local_steps(L);
+    });
+}
+
+extern "C" int ud_ligand_export(ud_ligand lig, float* lab_xyz, float* local_xyz, int* xs, int* ad,
+                                int* el, float* charge, int* atom_node, int* node_parent, int* node_begin,
+                                int* node_end, float* node_rel, int* pair_a, int* pair_b) {
+    return guarded([&] {
+        if (!lig) throw Error(UD_ERR_ARG, "null ligand");
+        const Ligand& L = lig->lig;
+        for (size_t i = 0; i < L.atoms.size(); ++i) {
+            const Atom& a = L.atoms[i];
+            for (int k = 0; k < 3; ++k) {
+                if (lab_xyz) lab_xyz[3 * i + k] = a.lab[k];
+                if (local_xyz) local_xyz[3 * i + k] = a.local[k];
+            }
+            if (xs) xs[i] = a.xs;
+            if (ad) ad[i] = a.ad;
+            if (el) el[i] = a.el;
+            if (charge) charge[i] = a.charge;
+            if (atom_node) atom_node[i] = a.node;
+        }
+        for (size_t n = 0; n < L.nodes.size(); ++n) {
+            const Node& nd = L.nodes[n];
+            if (node_parent) node_parent[n] = nd.parent;
+            if (node_begin) node_begin[n] = nd.begin;
+            if (node_end) node_end[n] = nd.end;
+            if (node_rel)
+                for (int k = 0; k < 3; ++k) {
+                    node_rel[6 * n + k] = nd.rel_origin[k];
+                    node_rel[6 * n + 3 + k] = nd.rel_axis[k];
+                }
+        }
+        for (size_t p = 0; p < L.pairs.size(); ++p) {
+            if (pair_a) pair_a[p] = L.pairs[p].a;
+            if (pair_b) pair_b[p] = L.pairs[p].b;
+        }
+    });
+}
+
+extern "C" int ud_ligand_initial_pose(ud_ligand lig, float* pose) {
+    return guarded([&] {
+        if (!lig || !pose) throw Error(UD_ERR_ARG, "null argument");
+        const Ligand& L = lig->lig;
+        for (int k = 0; k < 3; ++k) pose[k] = L.nodes[0].origin0[k];
+        pose[3] = 1; pose[4] = 0; pose[5] = 0; pose[6] = 0;
+        for (int t = 0; t < L.n_torsions(); ++t) pose[7 + t] = 0;
+    });
+}
+
+extern "C" int ud_ligand_coords(ud_ligand lig, const float* pose, float* xyz) {
+    return guarded([&] {
+        if (!lig || !pose || !xyz) throw Error(UD_ERR_ARG, "null argument");
+        ligand_coords(lig->lig, pose, xyz);
+    });
+}
+
+extern "C" int ud_ligand_conf_indep(ud_ligand lig, float out[7]) {
+    return guarded([&] {
+        if (!lig || !out) throw Error(UD_ERR_ARG, "null argument");
+        auto v = lig->lig.conf_indep_inputs();
+        for (int i = 0; i < 7; ++i) out[i] = v[i];
+    });
+}
+
+extern "C" int ud_ligand_destroy(ud_ligand lig) {
+    delete lig;
+    return UD_OK;
+}
+
+// ---------------------------------------------------------------- batches
+
+extern "C" int ud_batch_create(ud_maps maps, const ud_ligand* ligs, int n, void* stream, ud_batch* out) {
+    return guarded([&] {
+        if (!maps || !out || n < 0 || (n > 0 && !ligs)) throw Error(UD_ERR_ARG, "invalid batch arguments");
+        cudaStream_t s = (cudaStream_t)stream;
+        auto b = std::make_unique<ud_batch_s>();
+        b->maps = maps;
+        std::vector<AtomRec> atoms;
+        std::vector<NodeRec> nodes;
+        std::vector<uint32_t> pairs;
+        for (int i = 0; i < n; ++i) {
+            if (!ligs[i]) throw Error(UD_ERR_ARG, "null ligand in batch");
+            const Ligand& L = ligs[i]->lig;
+            if ((int)L.atoms.size() > kMaxLigAtoms)
+                throw Error(UD_ERR_CAPACITY, "ligand " + std::to_string(i) + " has more than 256 atoms");
+            if (L.n_torsions() > kMaxLigTorsions)
+                throw Error(UD_ERR_CAPACITY, "ligand " + std::to_string(i) + " has more than 48 torsions");
+            b->ligs.push_back(&L);
+            LigDesc d{};
+            d.atom_off = (int)atoms.size();
+            d.n_atoms = (int)L.atoms.size();
+            d.node_off = (int)nodes.size();
+            d.n_nodes = (int)L.nodes.size();
+            d.pair_off = (int)pairs.size();
+            d.n_pairs = (int)L.pairs.size();
+            d.n_heavy = L.n_heavy();
+            d.local_steps = ligand_local_steps(L);
+            std::vector<int> depth(L.nodes.size(), 0);
+            for (size_t k = 1; k < L.nodes.size(); ++k) depth[k] = depth[L.nodes[k].parent] + 1;
+            d.max_depth = *std::max_element(depth.begin(), depth.end());
+            for (size_t k = 0; k < L.nodes.size(); ++k) {
+                const Node& nd = L.nodes[k];
+                NodeRec r{};
+                for (int q = 0; q < 3; ++q) {
+                    r.rel_origin[q] = nd.rel_origin[q];
+                    r.rel_axis[q] = nd.rel_axis[q];
+                    r.origin0[q] = nd.origin0[q];
+                }
+                r.parent = nd.parent < 0 ? 0 : nd.parent;
+                r.depth = depth[k];
+                r.begin_end = nd.begin | (nd.end << 16);
+                nodes.push_back(r);
+            }
+            for (const Atom& a : L.atoms) {
+                AtomRec r;
+                r.x = a.local[0];
+                r.y = a.local[1];
+                r.z = a.local[2];
+                int g = (a.xs < XS_SIZE) ? xs_grid_type(a.xs) : -1;
+                int slot = (g >= 0) ? maps->desc.slot_of_xs[g] : -1;
+                if (g >= 0 && slot < 0)
+                    throw Error(UD_ERR_ARG, std::string("no grid map for ligand atom type ") + xs_name(g));
+                int heavy = (a.el != EL_H) ? 1 : 0;
+                int xsp = (a.xs < XS_SIZE) ? a.xs + 1 : 0;
+                r.packed = a.node | ((slot + 1) << 8) | (heavy << 16) | (xsp << 24);
+                atoms.push_back(r);
+            }
+            for (const Pair& p : L.pairs) pairs.push_back((uint32_t)p.a | ((uint32_t)p.b << 8) | ((uint32_t)p.tp << 16));
+            b->desc.push_back(d);
+            b->max_atoms = std::max(b->max_atoms, d.n_atoms);
+            b->max_tors = std::max(b->max_tors, d.n_nodes - 1);
+        }
+        b->d_desc.upload(b->desc.data(), b->desc.size(), s);
+        b->d_atoms.upload(atoms.data(), atoms.size(), s);
+        b->d_nodes.upload(nodes.data(), nodes.size(), s);
+        b->d_pairs.upload(pairs.data(), pairs.size(), s);
+        cuda_check(cudaStreamSynchronize(s), "batch upload");
+        *out = b.release();
+    });
+}
+
+extern "C" int ud_batch_destroy(ud_batch batch) {
+    delete batch;
+    return UD_OK;
+}
+
+// ---------------------------------------------------------------- scoring
+
+static void check_poses(ud_batch b, const int* pose_ligand, int n_poses, int pose_stride) {
+    if (!b || n_poses < 0 || !pose_ligand) throw Error(UD_ERR_ARG, "invalid pose arguments");
+    if (pose_stride < 7 + b->max_tors) throw Error(UD_ERR_ARG, "pose_stride smaller than 7 + max torsions");
+}
+
+extern "C" int ud_score_grad_device(ud_batch b, const int* pose_ligand, const float* poses, int n_poses,
+                                    int pose_stride, float v_intra, float v_inter, float* e_out, float* g_out,
+                                    int g_stride, void* stream) {
+    return guarded([&] {
+        if (!b || !poses || !e_out || !g_out || g_stride < 6 + b->max_tors)
+            throw Error(UD_ERR_ARG, "invalid score arguments");
+        if (pose_stride < 7 + b->max_tors) throw Error(UD_ERR_ARG, "pose_stride too small");
+        if (n_poses == 0) return;
+        cuda_check(launch_score(b->view(), maps_view(b->maps), tables_view(b->maps), pose_ligand, poses,
+                                pose_stride, n_poses, v_intra, v_inter, e_out, g_out, g_stride, nullptr,
+                                (cudaStream_t)stream),
+                   "score kernel");
+    });
+}
+
+extern "C" int ud_score_grad(ud_batch b, const int* pose_ligand, const float* poses, int n_poses,
+                             int pose_stride, float v_intra, float v_inter, float* e_out, float* g_out,
+                             int g_stride, void* stream) {
+    return guarded([&] {
+        check_poses(b, pose_ligand, n_poses, pose_stride);
+        if (!poses || !e_out || !g_out || g_stride < 6 + b->max_tors) throw Error(UD_ERR_ARG, "invalid buffers");
+        for (int i = 0; i < n_poses; ++i)
+            if (pose_ligand[i] < 0 || pose_ligand[i] >= (int)b->desc.size())
+                throw Error(UD_ERR_ARG, "pose_ligand out of range");
+        if (n_poses == 0) return;
+        cudaStream_t s = (cudaStream_t)stream;
+        b->d_pose_lig.upload(pose_ligand, n_poses, s);
+        b->d_pose.upload(poses, (size_t)n_poses * pose_stride, s);
+        b->d_e.alloc(n_poses);
+        b->d_g.alloc((size_t)n_poses * g_stride);
+        cuda_check(launch_score(b->view(), maps_view(b->maps), tables_view(b->maps), b->d_pose_lig.p, b->d_pose.p,
+                                pose_stride, n_poses, v_intra, v_inter, b->d_e.p, b->d_g.p, g_stride, nullptr, s),
+                   "score kernel");
+        cuda_check(cudaMemcpyAsync(e_out, b->d_e.p, n_poses * sizeof(float), cudaMemcpyDeviceToHost, s), "D2H");
+        cuda_check(cudaMemcpyAsync(g_out, b->d_g.p, (size_t)n_poses * g_stride * sizeof(float),
+                                   cudaMemcpyDeviceToHost, s),
+                   "D2H");
+        cuda_check(cudaStreamSynchronize(s), "score sync");
+    });
+}
+
+static void score_poses_device(ud_batch b, const std::vector<int>& lig, const std::vector<float>& poses,
+                               int stride, float v, std::vector<float>& out, cudaStream_t s) {
+    const int n = (int)lig.size();
+    out.assign(2 * (size_t)n, 0.0f);
+    if (n == 0) return;
+    b->d_pose_lig.upload(lig.data(), n, s);
+    b->d_pose.upload(poses.data(), poses.size(), s);
+    b->d_score.alloc(2 * (size_t)n);
+    cuda_check(launch_score(b->view(), maps_view(b->maps), tables_view(b->maps), b->d_pose_lig.p, b->d_pose.p,
+                            stride, n, v, v, nullptr, nullptr, 0, b->d_score.p, s),
+               "score kernel");
+    cuda_check(cudaMemcpyAsync(out.data(), b->d_score.p, 2 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, s),
+               "D2H");
+    cuda_check(cudaStreamSynchronize(s), "score sync");
+}
+
+extern "C" int ud_score(ud_batch b, const int* pose_ligand, const float* poses, int n_poses, int pose_stride,
+                        float v, float* out, void* stream) {
+    return guarded([&] {
+        check_poses(b, pose_ligand, n_poses, pose_stride);
+        if (!poses || !out) throw Error(UD_ERR_ARG, "null buffer");
+        for (int i = 0; i < n_poses; ++i)
+            if (pose_ligand[i] < 0 || pose_ligand[i] >= (int)b->desc.size())
+                throw Error(UD_ERR_ARG, "pose_ligand out of range");
+        std::vector<int> l(pose_ligand, pose_ligand + n_poses);
+        std::vector<float> p(poses, poses + (size_t)n_poses * pose_stride), o;
+        score_poses_device(b, l, p, pose_stride, v, o, (cudaStream_t)stream);
+        std::copy(o.begin(), o.end(), out);
+    });
+}
+
+// ---------------------------------------------------------------- search
+
+// MC steps per chain (vina.h:187-204): 70*3*(50 + max(atoms + 10*dof))/2,
+// capped by max_step.
+static int global_steps_for(const std::vector<const Ligand*>& ligs, int max_step) {
+    size_t heuristic = 0;
+    for (auto* L : ligs) heuristic = std::max(heuristic, L->atoms.size() + 10 * (size_t)(6 + L->n_torsions()));
+    unsigned gs = (unsigned)(70 * 3 * (50 + heuristic) / 2);
+    if (max_step > 0 && gs > (unsigned)max_step) gs = (unsigned)max_step;
+    return (int)gs;
+}
+
+static float rmsd_ub(const std::vector<float>& a, const std::vector<float>& b) {
+    double acc = 0;
+    size_t n = a.size() / 3;
+    float accf = 0;
+    for (size_t i = 0; i < n; ++i) {
+        float dx = a[3 * i] - b[3 * i], dy = a[3 * i + 1] - b[3 * i + 1], dz = a[3 * i + 2] - b[3 * i + 2];
+        accf += dx * dx + dy * dy + dz * dz;
+    }
+    (void)acc;
+    return n > 0 ? std::sqrt(accf / n) : 0.0f;
+}
+
+// add_to_output_container (unidock/src/lib/coords.cpp:44-68)
+static void add_to_container(std::vector<PoseResult>& out, const PoseResult& t, float min_rmsd, size_t max_size) {
+    if (!out.empty() && t.heavy_xyz.size() != out[0].heavy_xyz.size()) return;
+    const float eps = std::numeric_limits<float>::epsilon();
+    if (t.e < eps && t.e > -eps) return;
+    size_t best_i = out.size();
+    float best_r = std::numeric_limits<float>::max();
+    for (size_t i = 0; i < out.size(); ++i) {
+        float r = rmsd_ub(t.heavy_xyz, out[i].heavy_xyz);
+        if (i == 0 || r < best_r) {
+            best_i = i;
+            best_r = r;
+        }
+    }
+    if (best_i < out.size() && best_r < min_rmsd) {
+        if (t.e < out[best_i].e) out[best_i] = t;
+    } else {
+        if (out.size() < max_size) out.push_back(t);
+        else if (!out.empty() && t.e < out.back().e) out.back() = t;
+    }
+    std::stable_sort(out.begin(), out.end(), [](const PoseResult& x, const PoseResult& y) { return x.e < y.e; });
+}
+
+static std::vector<float> heavy_coords(const Ligand& L, const std::vector<float>& all) {
+    std::vector<float> h;
+    for (size_t i = 0; i < L.atoms.size(); ++i)
+        if (L.atoms[i].el != EL_H)
+            for (int k = 0; k < 3; ++k) h.push_back(all[3 * i + k]);
+    return h;
+}
+
+static float rmsd_lb_asym(const Ligand& L, const std::vector<float>& x, const std::vector<float>& y) {
+    float sum = 0;
+    unsigned cnt = 0;
+    for (size_t i = 0; i < L.atoms.size(); ++i) {
+        if (L.atoms[i].el == EL_H) continue;
+        float r2 = std::numeric_limits<float>::max();
+        for (size_t j = 0; j < L.atoms.size(); ++j) {
+            const Atom& b = L.atoms[j];
+            if (L.atoms[i].el == b.el && !(b.ad == AD_H || b.ad == AD_HD)) {
+                float dx = x[3 * i] - y[3 * j], dy = x[3 * i + 1] - y[3 * j + 1], dz = x[3 * i + 2] - y[3 * j + 2];
+                r2 = std::min(r2, dx * dx + dy * dy + dz * dz);
+            }
+        }
+        sum += r2;
+        ++cnt;
+    }
+    return cnt ? std::sqrt(sum / cnt) : 0.0f;
+}
+
+// Runs body(i) for i in [0, n) on the host's hardware threads (dynamic chunks of one).
+template <class F> static void parallel_for(int n, F&& body) {
+    int nt = (int)std::min<unsigned>(std::max(1u, std::thread::hardware_concurrency()), 64u);
+    nt = std::min(nt, std::max(1, n / 4));
+    if (nt <= 1) {
+        for (int i = 0; i < n; ++i) body(i);
+        return;
+    }
+    std::atomic<int> next{0};
+    std::vector<std::thread> ts;
+    for (int t = 0; t < nt; ++t)
+        ts.emplace_back([&] {
+            for (int i = next.fetch_add(1); i < n; i = next.fetch_add(1)) body(i);
+        });
+    for (auto& t : ts) t.join();
+}
+
+// Clustering and rescoring of the chain results of every ligand
+// (monte_carlo.cu:2939-2942, vina.h:236-343 without explicit-receptor refinement).
+static void post_process(ud_batch b, cudaStream_t s) {
+    const int n_lig = (int)b->ligs.size();
+    const int E = b->exhaustiveness;
+    const ud_search_params& P = b->params;
+    b->post.assign(n_lig, LigandPost{});
+    std::vector<std::vector<PoseResult>> cont(n_lig);
+    parallel_for(n_lig, [&](int l) {
+        const Ligand& L = *b->ligs[l];
+        std::vector<float> xyz(3 * L.atoms.size());
+        std::vector<PoseResult> out;
+        for (int c = 0; c < E; ++c) {
+            const int slot = l * E + c;
+            PoseResult r;
+            const float* p = &b->h_poses[(size_t)slot * b->pose_stride];
+            r.pose.assign(p, p + 7 + L.n_torsions());
+            r.e = b->h_results[slot].e;
+            ligand_coords(L, r.pose.data(), xyz.data());
+            r.heavy_xyz = heavy_coords(L, xyz);
+            add_to_container(out, r, P.min_rmsd, (size_t)std::max(1, P.num_modes));
+        }
+        std::vector<PoseResult> red;
+        for (auto& r : out) add_to_container(red, r, P.min_rmsd, out.size());
+        cont[l] = std::move(red);
+    });
+    // rescoring: grid + intramolecular (fast table) energies at the authentic cap, one launch
+    const int stride = 7 + b->max_tors;
+    std::vector<int> lig;
+    std::vector<float> poses;
+    std::vector<int> first(n_lig + 1, 0);
+    for (int l = 0; l < n_lig; ++l) {
+        first[l] = (int)lig.size();
+        for (auto& r : cont[l]) {
+            lig.push_back(l);
+            size_t off = poses.size();
+            poses.resize(off + stride, 0.0f);
+            std::copy(r.pose.begin(), r.pose.end(), poses.begin() + off);
+        }
+    }
+    first[n_lig] = (int)lig.size();
+    std::vector<float> sc;
+    score_poses_device(b, lig, poses, stride, 1000.0f, sc, s);
+    const Scoring& sf = b->maps->sf;
+    parallel_for(n_lig, [&](int l) {
+        auto& v = cont[l];
+        if (v.empty()) return;
+        const Ligand& L = *b->ligs[l];
+        auto ci = L.conf_indep_inputs();
+        const int f = first[l];
+        const float intramolecular = sc[2 * f + 1];  // best pose by search energy
+        for (size_t i = 0; i < v.size(); ++i) {
+            float grid = sc[2 * (f + i)], intra = sc[2 * (f + i) + 1];
+            float inter = grid;
+            float total = sf.conf_independent(inter + intra - intramolecular, ci[0], (float)L.torsdof);
+            v[i].e = total;
+            v[i].inter = inter;
+            v[i].intra = intra;
+            v[i].total = inter + intra;
+            v[i].conf_indep = total - (inter + intra - intramolecular);
+            v[i].unbound = intramolecular;
+        }
+        std::stable_sort(v.begin(), v.end(), [](const PoseResult& x, const PoseResult& y) { return x.e < y.e; });
+        std::vector<float> best(3 * L.atoms.size()), cur(3 * L.atoms.size());
+        ligand_coords(L, v[0].pose.data(), best.data());
+        for (auto& r : v) {
+            ligand_coords(L, r.pose.data(), cur.data());
+            r.lb = std::max(rmsd_lb_asym(L, cur, best), rmsd_lb_asym(L, best, cur));
+            r.ub = rmsd_ub(heavy_coords(L, cur), heavy_coords(L, best));
+        }
+        b->post[l].modes = v;
+    });
+}
+
+// Launch the search kernels of the batch asynchronously on `s`.
+static void search_launch(ud_batch b, const ud_search_params* params, cudaStream_t s) {
+        if (!b || !params) throw Error(UD_ERR_ARG, "null argument");
+        const ud_search_params& P = *params;
+        if (P.exhaustiveness < 1) throw Error(UD_ERR_ARG, "exhaustiveness must be >= 1");
+        b->params = P;
+        b->searched = false;
+        const int n_lig = (int)b->ligs.size();
+        const int E = P.exhaustiveness;
+        b->exhaustiveness = E;
+        b->pose_stride = 7 + b->max_tors;
+        const size_t n_chain = (size_t)n_lig * E;
+        b->d_poses.alloc(n_chain * b->pose_stride);
+        b->d_results.alloc(n_chain);
+        b->d_queue.alloc(1);
+        // most expensive ligands first (atoms x pairs as the cost proxy)
+        std::vector<int> order(n_lig);
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            long long cx = (long long)b->desc[x].local_steps * (b->desc[x].n_atoms + b->desc[x].n_pairs);
+            long long cy = (long long)b->desc[y].local_steps * (b->desc[y].n_atoms + b->desc[y].n_pairs);
+            return cx > cy;
+        });
+        b->d_order.upload(order.data(), order.size(), s);
+        SearchParams sp{};
+        sp.global_steps = global_steps_for(b->ligs, P.max_step);
+        sp.exhaustiveness = E;
+        sp.seed = P.seed;
+        sp.hunt_cap = 10.0f;
+        sp.authentic_v = 1000.0f;
+        sp.temperature = 1.2f;
+        sp.mutation_amplitude = 2.0f;
+        sp.lanes_per_chain = 32;
+        sp.chains_per_block = P.chains_per_block > 0 ? P.chains_per_block : 4;
+        sp.persistent = P.form == 1 ? 1 : 0;
+        sp.bfgs_cap = P.bfgs_cap;
+        int dev = 0, n_sm = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+        if (!b->ev0) {
+            cuda_check(cudaEventCreate(&b->ev0), "event");
+            cuda_check(cudaEventCreate(&b->ev1), "event");
+        }
+        cudaEventRecord(b->ev0, s);
+        if (sp.persistent) {
+            cuda_check(cudaMemsetAsync(b->d_queue.p, 0, sizeof(unsigned int), s), "queue reset");
+            int per_sm = search_blocks_per_sm(b->view(), sp.chains_per_block);
+            int blocks = per_sm * n_sm;
+            int needed = (int)((n_chain + sp.chains_per_block - 1) / sp.chains_per_block);
+            blocks = std::max(1, std::min(blocks, needed));
+            cuda_check(launch_search(b->view(), maps_view(b->maps), tables_view(b->maps), sp, b->d_order.p,
+                                     (int)n_chain, 0, b->d_queue.p, b->d_poses.p, b->pose_stride, b->d_results.p,
+                                     blocks, s),
+                       "search kernel");
+        } else {
+            for (int k = 0; k < n_lig; ++k) {
+                cuda_check(launch_search(b->view(), maps_view(b->maps), tables_view(b->maps), sp, b->d_order.p, E,
+                                         k * E, b->d_queue.p, b->d_poses.p, b->pose_stride, b->d_results.p, 0, s),
+                           "search kernel");
+            }
+        }
+        cudaEventRecord(b->ev1, s);
+        b->launched = true;
+}
+
+// Copy the chain results of the launched search to the host, cluster and rescore.
+static void search_collect(ud_batch b, cudaStream_t s) {
+        if (!b || !b->launched) throw Error(UD_ERR_STATE, "no search launched");
+        const size_t n_chain = (size_t)b->ligs.size() * b->exhaustiveness;
+        b->h_poses.resize(n_chain * b->pose_stride);
+        b->h_results.resize(n_chain);
+        cuda_check(cudaMemcpyAsync(b->h_poses.data(), b->d_poses.p, b->h_poses.size() * sizeof(float),
+                                   cudaMemcpyDeviceToHost, s),
+                   "D2H poses");
+        cuda_check(cudaMemcpyAsync(b->h_results.data(), b->d_results.p, n_chain * sizeof(ChainResult),
+                                   cudaMemcpyDeviceToHost, s),
+                   "D2H results");
+        cuda_check(cudaStreamSynchronize(s), "search sync");
+        cudaEventElapsedTime(&b->kernel_ms, b->ev0, b->ev1);
+        b->evals = 0;
+        for (auto& r : b->h_results) b->evals += r.evals;
+        post_process(b, s);
+        b->launched = false;
+        b->searched = true;
+}
+
+extern "C" int ud_search(ud_batch b, const ud_search_params* params, void* stream) {
+    return guarded([&] {
+        search_launch(b, params, (cudaStream_t)stream);
+        search_collect(b, (cudaStream_t)stream);
+    });
+}
+
+extern "C" int ud_search_launch(ud_batch b, const ud_search_params* params, void* stream) {
+    return guarded([&] { search_launch(b, params, (cudaStream_t)stream); });
+}
+
+extern "C" int ud_search_collect(ud_batch b, void* stream) {
+    return guarded([&] { search_collect(b, (cudaStream_t)stream); });
+}
+
+extern "C" int ud_search_chains(ud_batch b, float* poses, int pose_stride, float* e, int* evals) {
+    return guarded([&] {
+        if (!b || !b->searched) throw Error(UD_ERR_STATE, "no search results");
+        const size_t n = b->h_results.size();
+        for (size_t i = 0; i < n; ++i) {
+            if (e) e[i] = b->h_results[i].e;
+            if (evals) evals[i] = b->h_results[i].evals;
+            if (poses) {
+                if (pose_stride < b->pose_stride) throw Error(UD_ERR_ARG, "pose_stride too small");
+                std::copy(&b->h_poses[i * b->pose_stride], &b->h_poses[i * b->pose_stride] + b->pose_stride,
+                          poses + i * pose_stride);
+            }
+        }
+    });
+}
+
+extern "C" int ud_result_count(ud_batch b, int lig, int* n_modes) {
+    return guarded([&] {
+        if (!b || !b->searched) throw Error(UD_ERR_STATE, "no search results");
+        if (lig < 0 || lig >= (int)b->post.size() || !n_modes) throw Error(UD_ERR_ARG, "ligand out of range");
+        *n_modes = (int)b->post[lig].modes.size();
+    });
+}
+
+extern "C" int ud_result_mode(ud_batch b, int lig, int k, float* pose, float energies[8]) {
+    return guarded([&] {
+        if (!b || !b->searched) throw Error(UD_ERR_STATE, "no search results");
+        if (lig < 0 || lig >= (int)b->post.size()) throw Error(UD_ERR_ARG, "ligand out of range");
+        const auto& m = b->post[lig].modes;
+        if (k < 0 || k >= (int)m.size()) throw Error(UD_ERR_ARG, "mode out of range");
+        if (pose) std::copy(m[k].pose.begin(), m[k].pose.end(), pose);
+        if (energies) {
+            energies[0] = m[k].e;
+            energies[1] = m[k].lb;
+            energies[2] = m[k].ub;
+            energies[3] = m[k].total;
+            energies[4] = m[k].inter;
+            energies[5] = m[k].intra;
+            energies[6] = m[k].conf_indep;
+            energies[7] = m[k].unbound;
+        }
+    });
+}
+
+extern "C" int ud_result_write(ud_batch b, int lig, int format, char* buf, size_t cap, size_t* len) {
+    return guarded([&] {
+        if (!b || !b->searched) throw Error(UD_ERR_STATE, "no search results");
+        if (lig < 0 || lig >= (int)b->post.size()) throw Error(UD_ERR_ARG, "ligand out of range");
+        const Ligand& L = *b->ligs[lig];
+        const auto& modes = b->post[lig].modes;
+        std::vector<PoseResult> sel;
+        if (!modes.empty()) {
+            const float best = modes[0].e;
+            for (auto& m : modes) {
+                if ((int)sel.size() >= b->params.num_modes) break;
+                if (!(m.e < 0.1f * std::numeric_limits<float>::max()) || m.e > best + b->params.energy_range) break;
+                sel.push_back(m);
+            }
+        }
+        std::string s = format == 1 ? write_sdf_models(L, sel, false) : write_pdbqt_models(L, sel, false);
+        if (len) *len = s.size();
+        if (buf && cap > 0) {
+            size_t n = std::min(cap - 1, s.size());
+            std::memcpy(buf, s.data(), n);
+            buf[n] = 0;
+        }
+    });
+}
+
+extern "C" int ud_search_stats(ud_batch b, long long* evals, float* kernel_ms) {
+    return guarded([&] {
+        if (!b || !b->searched) throw Error(UD_ERR_STATE, "no search results");
+        if (evals) *evals = b->evals;
+        if (kernel_ms) *kernel_ms = b->kernel_ms;
+    });
+}
+
+extern "C" int ud_optimize(ud_batch b, const int* pose_ligand, float* poses, int n_poses, int pose_stride,
+                           int max_steps, float v, float* e_out, int* evals_out, void* stream) {
+    return guarded([&] {
+        check_poses(b, pose_ligand, n_poses, pose_stride);
+        if (!poses || !e_out) throw Error(UD_ERR_ARG, "null buffer");
+        for (int i = 0; i < n_poses; ++i)
+            if (pose_ligand[i] < 0 || pose_ligand[i] >= (int)b->desc.size())
+                throw Error(UD_ERR_ARG, "pose_ligand out of range");
+        if (n_poses == 0) return;
+        cudaStream_t s = (cudaStream_t)stream;
+        b->d_pose_lig.upload(pose_ligand, n_poses, s);
+        b->d_pose.upload(poses, (size_t)n_poses * pose_stride, s);
+        b->d_e.alloc(n_poses);
+        DevBuf<int> d_ev;
+        d_ev.alloc(n_poses);
+        cuda_check(launch_optimize(b->view(), maps_view(b->maps), tables_view(b->maps), b->d_pose_lig.p, b->d_pose.p,
+                                   pose_stride, n_poses, max_steps, v, b->d_e.p, d_ev.p, s),
+                   "optimize kernel");
+        cuda_check(cudaMemcpyAsync(poses, b->d_pose.p, (size_t)n_poses * pose_stride * sizeof(float),
+                                   cudaMemcpyDeviceToHost, s), "D2H");
+        cuda_check(cudaMemcpyAsync(e_out, b->d_e.p, n_poses * sizeof(float), cudaMemcpyDeviceToHost, s), "D2H");
+        std::vector<int> ev(n_poses);
+        cuda_check(cudaMemcpyAsync(ev.data(), d_ev.p, n_poses * sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
+        cuda_check(cudaStreamSynchronize(s), "optimize sync");
+        if (evals_out) std::copy(ev.begin(), ev.end(), evals_out);
+    });
+}
+
+extern "C" int ud_device_fp32_peak(float* tflops) {
+    return guarded([&] {
+        if (!tflops) throw Error(UD_ERR_ARG, "null argument");
+        *tflops = measure_fp32_peak_tflops();
+        if (!(*tflops > 0)) throw Error(UD_ERR_CUDA, "fp32 probe failed");
+    });
+}

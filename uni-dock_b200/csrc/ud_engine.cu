@@ -1,0 +1,1088 @@
+// Docking engine kernels for sm_100a.
+//
+//  * ud_maps_kernel      receptor grid maps (one thread per grid point, all
+//                        requested types at once, receptor atoms of the tile
+//                        staged in shared memory in index order)
+//  * ud_score_kernel     energy + pose gradient at fixed poses (one warp per pose)
+//  * ud_search_kernel    Monte-Carlo + BFGS chains (one warp per chain), plain
+//                        fixed tiling or a persistent queue over (ligand, chain)
+//
+// Chain state (conformations, gradients, inverse Hessian, atom coordinates,
+// forces and node frames) lives in shared memory; ligand topology is read
+// through the read-only cache; grid maps and pair tables stay L2-resident.
+// Per-evaluation arithmetic follows the reference's model::eval_deriv
+// (unidock/src/lib/model.cpp:935-962): forward kinematics (tree.h:89-128),
+// trilinear grid energy/gradient with out-of-box penalty (grid.cpp:40-129),
+// lerped pair tables (precalculate.h:48-65), curl (curl.h:28-43) and the
+// force/torque reverse sweep up the torsion tree (tree.h:75-84,164-192).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <algorithm>
+#include <cstdio>
+
+#include "ud_engine.h"
+
+namespace ud {
+namespace dev {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr float kPi = 3.1415926535897931f;
+constexpr float kEps = 1.1920928955078125e-07f;  // FLT_EPSILON
+constexpr float kMaxFl = 3.402823466e+38f;
+
+// ---------------------------------------------------------------- RNG
+// Philox4x32-10 counter-based generator (Salmon, Moraes, Dror, Shaw,
+// "Parallel random numbers: as easy as 1, 2, 3", SC 2011).
+struct Philox {
+    uint32_t k0, k1;   // key (seed)
+    uint32_t c0, c1, c2, c3;
+    __device__ void init(unsigned long long seed, uint32_t stream, uint32_t sub) {
+        k0 = (uint32_t)seed;
+        k1 = (uint32_t)(seed >> 32);
+        c0 = 0; c1 = 0; c2 = stream; c3 = sub;
+    }
+    __device__ uint4 next() {
+        uint32_t x0 = c0, x1 = c1, x2 = c2, x3 = c3, a = k0, b = k1;
+#pragma unroll
+        for (int r = 0; r < 10; ++r) {
+            uint32_t hi0 = __umulhi(0xD2511F53u, x0), lo0 = 0xD2511F53u * x0;
+            uint32_t hi1 = __umulhi(0xCD9E8D57u, x2), lo1 = 0xCD9E8D57u * x2;
+            uint32_t n0 = hi1 ^ x1 ^ a, n2 = hi0 ^ x3 ^ b;
+            x0 = n0; x1 = lo1; x2 = n2; x3 = lo0;
+            a += 0x9E3779B9u;
+            b += 0xBB67AE85u;
+        }
+        if (++c0 == 0) ++c1;
+        return make_uint4(x0, x1, x2, x3);
+    }
+};
+__device__ __forceinline__ float u01(uint32_t u) { return (u >> 8) * (1.0f / 16777216.0f); }
+
+// ---------------------------------------------------------------- math
+__device__ __forceinline__ float normalized_angle(float x) {
+    // normalize_angle of unidock/src/lib/common.h:252-270
+    for (int it = 0; it < 64; ++it) {
+        if (x > 3 * kPi) {
+            float n = (x - kPi) / (2 * kPi);
+            x -= 2 * kPi * ceilf(n);
+        } else if (x < -3 * kPi) {
+            float n = (-x - kPi) / (2 * kPi);
+            x += 2 * kPi * ceilf(n);
+        } else if (x > kPi) {
+            x -= 2 * kPi;
+            break;
+        } else if (x < -kPi) {
+            x += 2 * kPi;
+            break;
+        } else {
+            break;
+        }
+    }
+    return x;
+}
+
+__device__ __forceinline__ void qmul(const float* a, const float* b, float* o) {
+    float t0 = a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3];
+    float t1 = a[0] * b[1] + a[1] * b[0] + a[2] * b[3] - a[3] * b[2];
+    float t2 = a[0] * b[2] - a[1] * b[3] + a[2] * b[0] + a[3] * b[1];
+    float t3 = a[0] * b[3] + a[1] * b[2] - a[2] * b[1] + a[3] * b[0];
+    o[0] = t0; o[1] = t1; o[2] = t2; o[3] = t3;
+}
+
+__device__ __forceinline__ void qnormalize_approx(float* q) {
+    float s = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+    if (fabsf(s - 1) >= 1e-6f) {
+        float a = sqrtf(s);
+        float inv = 1 / a;
+        q[0] *= inv; q[1] *= inv; q[2] *= inv; q[3] *= inv;
+    }
+}
+
+__device__ __forceinline__ void axis_angle_q(const float* axis, float angle, float* q) {
+    angle = normalized_angle(angle);
+    float s, c;
+    sincosf(angle / 2, &s, &c);
+    q[0] = c; q[1] = s * axis[0]; q[2] = s * axis[1]; q[3] = s * axis[2];
+}
+
+// q <- angle_to_quaternion(rotation) * q, normalised (quaternion.cpp:116-132)
+__device__ __forceinline__ void quaternion_increment(float* q, const float* rot) {
+    float angle = sqrtf(rot[0] * rot[0] + rot[1] * rot[1] + rot[2] * rot[2]);
+    float t[4] = {1, 0, 0, 0};
+    if (angle > kEps) {
+        float ax[3] = {rot[0] / angle, rot[1] / angle, rot[2] / angle};
+        axis_angle_q(ax, angle, t);
+    }
+    float o[4];
+    qmul(t, q, o);
+    qnormalize_approx(o);
+    q[0] = o[0]; q[1] = o[1]; q[2] = o[2]; q[3] = o[3];
+}
+
+// Row-major rotation matrix of quaternion_to_r3 (quaternion.cpp:84-115)
+__device__ __forceinline__ void q_to_r3(const float* q, float* m) {
+    float a = q[0], b = q[1], c = q[2], d = q[3];
+    float aa = a * a, ab = a * b, ac = a * c, ad = a * d, bb = b * b, bc = b * c, bd = b * d,
+          cc = c * c, cd = c * d, dd = d * d;
+    m[0] = aa + bb - cc - dd; m[1] = 2 * (-ad + bc); m[2] = 2 * (ac + bd);
+    m[3] = 2 * (ad + bc); m[4] = aa - bb + cc - dd; m[5] = 2 * (-ab + cd);
+    m[6] = 2 * (-ac + bd); m[7] = 2 * (ab + cd); m[8] = aa - bb - cc + dd;
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+__device__ __forceinline__ int tri_j(int k) {  // column of packed index k (i <= j)
+    int j = (int)((sqrtf(8.0f * k + 1.0f) - 1.0f) * 0.5f);
+    while (j * (j + 1) / 2 > k) --j;
+    while ((j + 1) * (j + 2) / 2 <= k) ++j;
+    return j;
+}
+
+// ---------------------------------------------------------------- batch views
+struct Batch {
+    const LigDesc* ligs;
+    const AtomRec* atoms;
+    const NodeRec* nodes;
+    const uint32_t* pairs;
+};
+
+struct Tables {
+    const float2* smooth;  // [tp][bin] (e, dE/dr / r)
+    const float* fast;     // [tp][bin]
+    int n_bins;
+    float factor;
+    float cutoff2;
+};
+
+struct Maps {
+    const float* data;     // [slot][z][y][x]
+    int nx, ny, nz;
+    float init[3], factor[3], factor_inv[3], dim_m1[3];
+    float slope;
+};
+
+// Shared-memory layout of one chain (floats).
+struct Layout {
+    int cs, gs;            // conformation / gradient sizes of the largest ligand
+    int x, xnew, xorig, tmp, cand, best;
+    int g, gnew, gorig, p, y, mhy;
+    int h;
+    int coords, forces;
+    int frames, accum;
+    int misc;
+    int total;
+};
+
+__host__ __device__ inline int pad4(int v) { return (v + 3) & ~3; }
+
+__host__ inline Layout make_layout(int max_atoms, int max_tors) {
+    Layout L;
+    int cs = 7 + max_tors, gs = 6 + max_tors, R = max_tors + 1;
+    L.cs = cs;
+    L.gs = gs;
+    int o = 0;
+    auto take = [&](int n) { int r = o; o += pad4(n); return r; };
+    L.x = take(cs); L.xnew = take(cs); L.xorig = take(cs); L.tmp = take(cs); L.cand = take(cs);
+    L.best = take(cs);
+    L.g = take(gs); L.gnew = take(gs); L.gorig = take(gs); L.p = take(gs); L.y = take(gs);
+    L.mhy = take(gs);
+    L.h = take(gs * (gs + 1) / 2);
+    L.coords = take(3 * max_atoms);
+    L.forces = take(3 * max_atoms);
+    L.frames = take(20 * R);
+    L.accum = take(6 * R);
+    L.misc = take(32);
+    L.total = o;
+    return L;
+}
+
+// Per-warp chain context.
+struct Chain {
+    float* s;              // shared-memory base of this chain
+    Layout L;
+    LigDesc lig;
+    const AtomRec* atoms;
+    const NodeRec* nodes;
+    const uint32_t* pairs;
+    int lane;
+    int T;                 // torsions
+    int R;                 // nodes
+};
+
+// Forward kinematics: node frames by tree depth, then atom coordinates.
+__device__ void kinematics(const Chain& c, const float* conf) {
+    float* fr = c.s + c.L.frames;
+    if (c.lane == 0) {
+        fr[0] = conf[0]; fr[1] = conf[1]; fr[2] = conf[2];
+        fr[3] = conf[3]; fr[4] = conf[4]; fr[5] = conf[5]; fr[6] = conf[6];
+        q_to_r3(fr + 3, fr + 7);
+    }
+    __syncwarp();
+    for (int d = 1; d <= c.lig.max_depth; ++d) {
+        for (int n = 1 + c.lane; n < c.R; n += 32) {
+            const NodeRec* nr = c.nodes + n;
+            if (__ldg(&nr->depth) != d) continue;
+            const float* pf = fr + 20 * __ldg(&nr->parent);
+            float* f = fr + 20 * n;
+            const float* pm = pf + 7;
+            float ro[3] = {__ldg(&nr->rel_origin[0]), __ldg(&nr->rel_origin[1]), __ldg(&nr->rel_origin[2])};
+            float ra[3] = {__ldg(&nr->rel_axis[0]), __ldg(&nr->rel_axis[1]), __ldg(&nr->rel_axis[2])};
+            float ax[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                f[i] = pf[i] + (pm[3 * i] * ro[0] + pm[3 * i + 1] * ro[1] + pm[3 * i + 2] * ro[2]);
+                ax[i] = pm[3 * i] * ra[0] + pm[3 * i + 1] * ra[1] + pm[3 * i + 2] * ra[2];
+            }
+            float t[4], q[4];
+            axis_angle_q(ax, conf[7 + n - 1], t);
+            qmul(t, pf + 3, q);
+            qnormalize_approx(q);
+            f[3] = q[0]; f[4] = q[1]; f[5] = q[2]; f[6] = q[3];
+            q_to_r3(q, f + 7);
+            f[16] = ax[0]; f[17] = ax[1]; f[18] = ax[2];
+        }
+        __syncwarp();
+    }
+    float* xyz = c.s + c.L.coords;
+    for (int a = c.lane; a < c.lig.n_atoms; a += 32) {
+        AtomRec ar = c.atoms[a];
+        int n = ar.packed & 0xFF;
+        const float* f = fr + 20 * n;
+        const float* m = f + 7;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            xyz[3 * a + i] = f[i] + (m[3 * i] * ar.x + m[3 * i + 1] * ar.y + m[3 * i + 2] * ar.z);
+    }
+    __syncwarp();
+}
+
+// Trilinear map energy, gradient and out-of-box penalty of one atom.
+__device__ __forceinline__ float grid_eval(const Maps& M, int slot, const float* p, float v,
+                                           float& gx, float& gy, float& gz, bool want_deriv) {
+    float s[3], miss[3];
+    int reg[3], a[3];
+    const int dims[3] = {M.nx, M.ny, M.nz};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float si = (p[i] - M.init[i]) * M.factor[i];
+        if (si < 0) {
+            miss[i] = -si; reg[i] = -1; a[i] = 0; si = 0;
+        } else if (si >= M.dim_m1[i]) {
+            miss[i] = si - M.dim_m1[i]; reg[i] = 1; a[i] = dims[i] - 2; si = 1;
+        } else {
+            miss[i] = 0; reg[i] = 0; a[i] = (int)si; si -= a[i];
+        }
+        s[i] = si;
+    }
+    const float penalty = M.slope * (miss[0] * M.factor_inv[0] + miss[1] * M.factor_inv[1] +
+                                     miss[2] * M.factor_inv[2]);
+    const float* g = M.data + (size_t)slot * M.nx * M.ny * M.nz;
+    const size_t sx = 1, sy = M.nx, sz = (size_t)M.nx * M.ny;
+    const size_t base = a[0] + sy * a[1] + sz * a[2];
+    const float f000 = __ldg(g + base), f100 = __ldg(g + base + sx);
+    const float f010 = __ldg(g + base + sy), f110 = __ldg(g + base + sx + sy);
+    const float f001 = __ldg(g + base + sz), f101 = __ldg(g + base + sx + sz);
+    const float f011 = __ldg(g + base + sy + sz), f111 = __ldg(g + base + sx + sy + sz);
+    const float x = s[0], y = s[1], z = s[2];
+    const float mx = 1 - x, my = 1 - y, mz = 1 - z;
+    float f = f000 * mx * my * mz + f100 * x * my * mz + f010 * mx * y * mz + f110 * x * y * mz +
+              f001 * mx * my * z + f101 * x * my * z + f011 * mx * y * z + f111 * x * y * z;
+    if (want_deriv) {
+        float xg = -f000 * my * mz + f100 * my * mz - f010 * y * mz + f110 * y * mz -
+                   f001 * my * z + f101 * my * z - f011 * y * z + f111 * y * z;
+        float yg = -f000 * mx * mz - f100 * x * mz + f010 * mx * mz + f110 * x * mz -
+                   f001 * mx * z - f101 * x * z + f011 * mx * z + f111 * x * z;
+        float zg = -f000 * mx * my - f100 * x * my - f010 * mx * y - f110 * x * y +
+                   f001 * mx * my + f101 * x * my + f011 * mx * y + f111 * x * y;
+        if (f > 0 && v < 0.1f * kMaxFl) {  // curl
+            float tmp = (v < kEps) ? 0 : (v / (v + f));
+            f *= tmp;
+            float t2 = tmp * tmp;
+            xg *= t2; yg *= t2; zg *= t2;
+        }
+        gx = M.factor[0] * (reg[0] == 0 ? xg : 0.0f) + M.slope * reg[0];
+        gy = M.factor[1] * (reg[1] == 0 ? yg : 0.0f) + M.slope * reg[1];
+        gz = M.factor[2] * (reg[2] == 0 ? zg : 0.0f) + M.slope * reg[2];
+    } else {
+        if (f > 0 && v < 0.1f * kMaxFl) {
+            float tmp = (v < kEps) ? 0 : (v / (v + f));
+            f *= tmp;
+        }
+    }
+    return f + penalty;
+}
+
+// Energy and gradient (change layout: position, torque, torsions) of `conf`.
+__device__ float eval_deriv(const Chain& c, const Maps& M, const Tables& Tb, const float* conf,
+                            float* g, float v_intra, float v_inter) {
+    kinematics(c, conf);
+    const float* xyz = c.s + c.L.coords;
+    float* frc = c.s + c.L.forces;
+    float e = 0;
+    for (int a = c.lane; a < c.lig.n_atoms; a += 32) {
+        int packed = __ldg(&c.atoms[a].packed);
+        int slot = ((packed >> 8) & 0xFF) - 1;
+        float gx = 0, gy = 0, gz = 0;
+        if (slot >= 0) e += grid_eval(M, slot, xyz + 3 * a, v_inter, gx, gy, gz, true);
+        frc[3 * a] = gx; frc[3 * a + 1] = gy; frc[3 * a + 2] = gz;
+    }
+    __syncwarp();
+    for (int k = c.lane; k < c.lig.n_pairs; k += 32) {
+        uint32_t pr = __ldg(c.pairs + k);
+        int a = pr & 0xFF, b = (pr >> 8) & 0xFF, tp = pr >> 16;
+        float rx = xyz[3 * b] - xyz[3 * a], ry = xyz[3 * b + 1] - xyz[3 * a + 1],
+              rz = xyz[3 * b + 2] - xyz[3 * a + 2];
+        float r2 = rx * rx + ry * ry + rz * rz;
+        if (r2 < Tb.cutoff2) {
+            float rf = Tb.factor * r2;
+            int i1 = (int)rf;
+            float rem = rf - i1;
+            const float2* row = Tb.smooth + (size_t)tp * Tb.n_bins;
+            float2 p1 = __ldg(row + i1), p2 = __ldg(row + i1 + 1);
+            float ep = p1.x + rem * (p2.x - p1.x);
+            float dor = p1.y + rem * (p2.y - p1.y);
+            float fx = dor * rx, fy = dor * ry, fz = dor * rz;
+            if (ep > 0 && v_intra < 0.1f * kMaxFl) {
+                float tmp = (v_intra < kEps) ? 0 : (v_intra / (v_intra + ep));
+                ep *= tmp;
+                float t2 = tmp * tmp;
+                fx *= t2; fy *= t2; fz *= t2;
+            }
+            e += ep;
+            atomicAdd(frc + 3 * a, -fx); atomicAdd(frc + 3 * a + 1, -fy); atomicAdd(frc + 3 * a + 2, -fz);
+            atomicAdd(frc + 3 * b, fx); atomicAdd(frc + 3 * b + 1, fy); atomicAdd(frc + 3 * b + 2, fz);
+        }
+    }
+    __syncwarp();
+    e = warp_sum(e);
+    // per-node force and torque of the node's own atoms about its origin
+    const float* fr = c.s + c.L.frames;
+    float* acc = c.s + c.L.accum;
+    for (int n = c.lane; n < c.R; n += 32) {
+        int be = __ldg(&c.nodes[n].begin_end);
+        int b0 = be & 0xFFFF, b1 = be >> 16;
+        const float* o = fr + 20 * n;
+        float F0 = 0, F1 = 0, F2 = 0, T0 = 0, T1 = 0, T2 = 0;
+        for (int a = b0; a < b1; ++a) {
+            float f0 = frc[3 * a], f1 = frc[3 * a + 1], f2 = frc[3 * a + 2];
+            float r0 = xyz[3 * a] - o[0], r1 = xyz[3 * a + 1] - o[1], r2 = xyz[3 * a + 2] - o[2];
+            F0 += f0; F1 += f1; F2 += f2;
+            T0 += r1 * f2 - r2 * f1;
+            T1 += r2 * f0 - r0 * f2;
+            T2 += r0 * f1 - r1 * f0;
+        }
+        acc[6 * n] = F0; acc[6 * n + 1] = F1; acc[6 * n + 2] = F2;
+        acc[6 * n + 3] = T0; acc[6 * n + 4] = T1; acc[6 * n + 5] = T2;
+    }
+    __syncwarp();
+    if (c.lane == 0) {
+        for (int n = c.R - 1; n >= 1; --n) {
+            const float* an = acc + 6 * n;
+            const float* on = fr + 20 * n;
+            g[6 + n - 1] = an[3] * on[16] + an[4] * on[17] + an[5] * on[18];
+            int p = __ldg(&c.nodes[n].parent);
+            float* ap = acc + 6 * p;
+            const float* op = fr + 20 * p;
+            float r0 = on[0] - op[0], r1 = on[1] - op[1], r2 = on[2] - op[2];
+            ap[0] += an[0]; ap[1] += an[1]; ap[2] += an[2];
+            ap[3] += (r1 * an[2] - r2 * an[1]) + an[3];
+            ap[4] += (r2 * an[0] - r0 * an[2]) + an[4];
+            ap[5] += (r0 * an[1] - r1 * an[0]) + an[5];
+        }
+        g[0] = acc[0]; g[1] = acc[1]; g[2] = acc[2];
+        g[3] = acc[3]; g[4] = acc[4]; g[5] = acc[5];
+    }
+    __syncwarp();
+    return e;
+}
+
+// Scoring-path energy (no gradient): grid with curl cap v, intramolecular
+// pairs from the nearest-bin `fast` table (model.cpp:867-886, cache.cpp:84-120).
+__device__ void eval_score(const Chain& c, const Maps& M, const Tables& Tb, const float* conf,
+                           float v, float& e_grid, float& e_intra) {
+    kinematics(c, conf);
+    const float* xyz = c.s + c.L.coords;
+    float eg = 0, ei = 0;
+    for (int a = c.lane; a < c.lig.n_atoms; a += 32) {
+        int packed = __ldg(&c.atoms[a].packed);
+        int slot = ((packed >> 8) & 0xFF) - 1;
+        float gx, gy, gz;
+        if (slot >= 0) eg += grid_eval(M, slot, xyz + 3 * a, v, gx, gy, gz, false);
+    }
+    for (int k = c.lane; k < c.lig.n_pairs; k += 32) {
+        uint32_t pr = __ldg(c.pairs + k);
+        int a = pr & 0xFF, b = (pr >> 8) & 0xFF, tp = pr >> 16;
+        float dx = xyz[3 * a] - xyz[3 * b], dy = xyz[3 * a + 1] - xyz[3 * b + 1],
+              dz = xyz[3 * a + 2] - xyz[3 * b + 2];
+        float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 < Tb.cutoff2) {
+            float t = __ldg(Tb.fast + (size_t)tp * Tb.n_bins + (int)(Tb.factor * r2));
+            if (t > 0 && v < 0.1f * kMaxFl) t *= (v < kEps) ? 0 : (v / (v + t));
+            ei += t;
+        }
+    }
+    e_grid = warp_sum(eg);
+    e_intra = warp_sum(ei);
+}
+
+__device__ __forceinline__ float dotw(const Chain& c, const float* a, const float* b, int n) {
+    float s = 0;
+    for (int i = c.lane; i < n; i += 32) s += a[i] * b[i];
+    return warp_sum(s);
+}
+
+__device__ __forceinline__ void copyw(const Chain& c, float* dst, const float* src, int n) {
+    for (int i = c.lane; i < n; i += 32) dst[i] = src[i];
+    __syncwarp();
+}
+
+// x_new = x + alpha * p in conformation space (conf.h:98-104, 146-150).
+__device__ void conf_increment(const Chain& c, const float* x, const float* p, float alpha,
+                               float* out) {
+    if (c.lane < 3) out[c.lane] = x[c.lane] + alpha * p[c.lane];
+    if (c.lane == 3) {
+        float rot[3] = {alpha * p[3], alpha * p[4], alpha * p[5]};
+        float q[4] = {x[3], x[4], x[5], x[6]};
+        quaternion_increment(q, rot);
+        out[3] = q[0]; out[4] = q[1]; out[5] = q[2]; out[6] = q[3];
+    }
+    for (int t = c.lane; t < c.T; t += 32) {
+        float v = x[7 + t] + normalized_angle(alpha * p[6 + t]);
+        out[7 + t] = normalized_angle(v);
+    }
+    __syncwarp();
+}
+
+// Vina BFGS with Armijo backtracking (bfgs.h:27-146); x and g updated in
+// place, returns the final energy.
+__device__ float bfgs(Chain& c, const Maps& M, const Tables& Tb, float* x, int max_steps,
+                      float v, int& evals) {
+    const int n = c.L.gs - (c.L.gs - 6 - c.T);  // 6 + T
+    float* s = c.s;
+    float* g = s + c.L.g;
+    float* gnew = s + c.L.gnew;
+    float* gorig = s + c.L.gorig;
+    float* p = s + c.L.p;
+    float* y = s + c.L.y;
+    float* mhy = s + c.L.mhy;
+    float* H = s + c.L.h;
+    float* xnew = s + c.L.xnew;
+    float* xorig = s + c.L.xorig;
+    const int cs = 7 + c.T;
+    const int nh = n * (n + 1) / 2;
+    for (int k = c.lane; k < nh; k += 32) H[k] = 0;
+    __syncwarp();
+    for (int i = c.lane; i < n; i += 32) H[i + i * (i + 1) / 2] = 1;
+    float f0 = eval_deriv(c, M, Tb, x, g, v, v);
+    ++evals;
+    const float f_orig = f0;
+    copyw(c, gorig, g, n);
+    copyw(c, xorig, x, cs);
+    for (int step = 0; step < max_steps; ++step) {
+        for (int i = c.lane; i < n; i += 32) {
+            float sum = 0;
+            for (int j = 0; j < n; ++j) sum += H[i < j ? i + j * (j + 1) / 2 : j + i * (i + 1) / 2] * g[j];
+            p[i] = -sum;
+        }
+        __syncwarp();
+        // line search
+        const float pg = dotw(c, p, g, n);
+        float alpha = 1.0f, f1 = 0;
+        for (int trial = 0; trial < 10; ++trial) {
+            conf_increment(c, x, p, alpha, xnew);
+            f1 = eval_deriv(c, M, Tb, xnew, gnew, v, v);
+            ++evals;
+            if (f1 - f0 < 0.0001f * alpha * pg) break;
+            alpha *= 0.5f;
+        }
+        for (int i = c.lane; i < n; i += 32) y[i] = gnew[i] - g[i];
+        __syncwarp();
+        f0 = f1;
+        copyw(c, x, xnew, cs);
+        const float gg = dotw(c, g, g, n);
+        if (!(sqrtf(gg) >= 1e-5f)) break;
+        copyw(c, g, gnew, n);
+        if (step == 0) {
+            float yy = dotw(c, y, y, n);
+            if (fabsf(yy) > kEps) {
+                float yp = dotw(c, y, p, n);
+                for (int i = c.lane; i < n; i += 32) H[i + i * (i + 1) / 2] = alpha * yp / yy;
+                __syncwarp();
+            }
+        }
+        // BFGS update of the inverse Hessian
+        const float yp = dotw(c, y, p, n);
+        if (alpha * yp < kEps) continue;
+        for (int i = c.lane; i < n; i += 32) {
+            float sum = 0;
+            for (int j = 0; j < n; ++j) sum += H[i < j ? i + j * (j + 1) / 2 : j + i * (i + 1) / 2] * y[j];
+            mhy[i] = -sum;
+        }
+        __syncwarp();
+        const float yhy = -dotw(c, y, mhy, n);
+        const float r = 1 / (alpha * yp);
+        for (int k = c.lane; k < nh; k += 32) {
+            int j = tri_j(k), i = k - j * (j + 1) / 2;
+            H[k] += alpha * r * (mhy[i] * p[j] + mhy[j] * p[i]) +
+                    alpha * alpha * (r * r * yhy + r) * p[i] * p[j];
+        }
+        __syncwarp();
+    }
+    if (!(f0 <= f_orig)) {
+        f0 = f_orig;
+        copyw(c, x, xorig, cs);
+        copyw(c, g, gorig, n);
+    }
+    return f0;
+}
+
+__device__ void random_inside_sphere(Philox& rng, float* v) {
+    for (int it = 0; it < 64; ++it) {
+        uint4 u = rng.next();
+        float a = 2 * u01(u.x) - 1, b = 2 * u01(u.y) - 1, d = 2 * u01(u.z) - 1;
+        float r2 = a * a + b * b + d * d;
+        if (r2 < 1 && sqrtf(r2) > 10 * kEps) {
+            v[0] = a; v[1] = b; v[2] = d;
+            return;
+        }
+    }
+    v[0] = v[1] = v[2] = 0;
+}
+
+// Initial chain conformation: position uniform in the box, orientation a
+// normalised 4-D Gaussian, torsions uniform (conf.h:105-108,173-176; quaternion.cpp:116-126).
+__device__ void random_conf(Chain& c, Philox& rng, const float* lo, const float* hi, float* x) {
+    if (c.lane == 0) {
+        uint4 u = rng.next();
+        x[0] = lo[0] + (hi[0] - lo[0]) * u01(u.x);
+        x[1] = lo[1] + (hi[1] - lo[1]) * u01(u.y);
+        x[2] = lo[2] + (hi[2] - lo[2]) * u01(u.z);
+        for (int it = 0; it < 16; ++it) {
+            uint4 a = rng.next();
+            float r1 = sqrtf(-2.0f * logf(fmaxf(u01(a.x), 1e-12f))), t1 = 2 * kPi * u01(a.y);
+            float r2 = sqrtf(-2.0f * logf(fmaxf(u01(a.z), 1e-12f))), t2 = 2 * kPi * u01(a.w);
+            float q[4] = {r1 * cosf(t1), r1 * sinf(t1), r2 * cosf(t2), r2 * sinf(t2)};
+            float nrm = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+            if (nrm > kEps) {
+                x[3] = q[0] / nrm; x[4] = q[1] / nrm; x[5] = q[2] / nrm; x[6] = q[3] / nrm;
+                break;
+            }
+            x[3] = 1; x[4] = x[5] = x[6] = 0;
+        }
+        for (int t = 0; t < c.T; t += 4) {
+            uint4 a = rng.next();
+            uint32_t w[4] = {a.x, a.y, a.z, a.w};
+            for (int k = 0; k < 4 && t + k < c.T; ++k) x[7 + t + k] = -kPi + 2 * kPi * u01(w[k]);
+        }
+    }
+    __syncwarp();
+}
+
+// Mutation of one of {position, orientation, one torsion} (mutate.cpp:36-80).
+__device__ void mutate(Chain& c, Philox& rng, float amplitude, float* x) {
+    float* misc = c.s + c.L.misc;
+    if (c.lane == 0) {
+        uint4 u = rng.next();
+        int which = (int)(u.x % (uint32_t)(2 + c.T));
+        float sph[3];
+        random_inside_sphere(rng, sph);
+        misc[0] = __int_as_float(which);
+        misc[1] = sph[0]; misc[2] = sph[1]; misc[3] = sph[2];
+        misc[4] = -kPi + 2 * kPi * u01(u.y);
+    }
+    __syncwarp();
+    const int which = __float_as_int(misc[0]);
+    if (which == 1) {
+        // gyration radius of heavy atoms about the root origin (model.cpp:853-865)
+        const float* xyz = c.s + c.L.coords;
+        const float* o = c.s + c.L.frames;
+        float acc = 0, cnt = 0;
+        for (int a = c.lane; a < c.lig.n_atoms; a += 32) {
+            int packed = __ldg(&c.atoms[a].packed);
+            if ((packed >> 16) & 1) {
+                float dx = xyz[3 * a] - o[0], dy = xyz[3 * a + 1] - o[1], dz = xyz[3 * a + 2] - o[2];
+                acc += dx * dx + dy * dy + dz * dz;
+                cnt += 1;
+            }
+        }
+        acc = warp_sum(acc);
+        cnt = warp_sum(cnt);
+        float gr = cnt > 0 ? sqrtf(acc / cnt) : 0;
+        if (c.lane == 0 && gr > kEps) {
+            float rot[3] = {amplitude / gr * misc[1], amplitude / gr * misc[2], amplitude / gr * misc[3]};
+            float q[4] = {x[3], x[4], x[5], x[6]};
+            quaternion_increment(q, rot);
+            x[3] = q[0]; x[4] = q[1]; x[5] = q[2]; x[6] = q[3];
+        }
+    } else if (c.lane == 0) {
+        if (which == 0) {
+            x[0] += amplitude * misc[1];
+            x[1] += amplitude * misc[2];
+            x[2] += amplitude * misc[3];
+        } else {
+            x[7 + which - 2] = misc[4];
+        }
+    }
+    __syncwarp();
+}
+
+// One Monte-Carlo chain (monte_carlo.cu:237-356 semantics): mutate, local
+// BFGS at the hunt cap, Metropolis at temperature T, refine improving poses
+// at the authentic cap and keep the best.
+__device__ void run_chain(Chain& c, const Maps& M, const Tables& Tb, const SearchParams& P,
+                          const float* box_lo, const float* box_hi, int lig_index, int chain,
+                          float* out_pose, int pose_stride, ChainResult* out_res) {
+    Philox rng;
+    rng.init(P.seed, (uint32_t)lig_index, (uint32_t)chain);
+    float* tmp = c.s + c.L.tmp;
+    float* cand = c.s + c.L.cand;
+    float* best = c.s + c.L.best;
+    const int cs = 7 + c.T;
+    int steps = c.lig.local_steps;
+    if (P.bfgs_cap > 0 && P.bfgs_cap < steps) steps = P.bfgs_cap;
+    random_conf(c, rng, box_lo, box_hi, tmp);
+    copyw(c, best, tmp, cs);
+    float tmp_e = kMaxFl, best_e = kMaxFl;
+    int evals = 0;
+    for (int step = 0; step < P.global_steps; ++step) {
+        copyw(c, cand, tmp, cs);
+        mutate(c, rng, P.mutation_amplitude, cand);
+        float cand_e = bfgs(c, M, Tb, cand, steps, P.hunt_cap, evals);
+        int accept = 0;
+        if (c.lane == 0) {
+            uint4 u = rng.next();
+            accept = (step == 0) || (cand_e < tmp_e) ||
+                     (u01(u.x) < expf((tmp_e - cand_e) / P.temperature));
+        }
+        accept = __shfl_sync(kFull, accept, 0);
+        if (accept) {
+            copyw(c, tmp, cand, cs);
+            tmp_e = cand_e;
+            if (tmp_e < best_e) {
+                tmp_e = bfgs(c, M, Tb, tmp, steps, P.authentic_v, evals);
+                if (tmp_e < best_e) {
+                    copyw(c, best, tmp, cs);
+                    best_e = tmp_e;
+                }
+            }
+        }
+    }
+    for (int i = c.lane; i < cs; i += 32) out_pose[i] = best[i];
+    if (c.lane == 0) {
+        out_res->e = best_e;
+        out_res->evals = evals;
+        out_res->ligand = lig_index;
+        out_res->chain = chain;
+    }
+}
+
+__device__ __forceinline__ void bind_chain(Chain& c, const Batch& B, const Layout& L, int lig,
+                                           float* smem_warp) {
+    c.s = smem_warp;
+    c.L = L;
+    c.lig = B.ligs[lig];
+    c.atoms = B.atoms + c.lig.atom_off;
+    c.nodes = B.nodes + c.lig.node_off;
+    c.pairs = B.pairs + c.lig.pair_off;
+    c.T = c.lig.n_nodes - 1;
+    c.R = c.lig.n_nodes;
+    c.lane = threadIdx.x & 31;
+}
+
+// ---------------------------------------------------------------- kernels
+
+// Search: plain form (grid covers the chains of `first_lig` .. with a fixed
+// tiling) or persistent form (warps pull (ligand, chain) items from a queue).
+__global__ void __launch_bounds__(128) search_kernel(Batch B, Maps M, Tables Tb, SearchParams P,
+                                                     Layout L, const int* order, int n_items,
+                                                     int first_item, unsigned int* queue,
+                                                     float box_lo0, float box_lo1, float box_lo2,
+                                                     float box_hi0, float box_hi1, float box_hi2,
+                                                     float* poses, int pose_stride,
+                                                     ChainResult* results) {
+    extern __shared__ float smem[];
+    const int warp = threadIdx.x >> 5;
+    float* sw = smem + (size_t)warp * L.total;
+    const float lo[3] = {box_lo0, box_lo1, box_lo2}, hi[3] = {box_hi0, box_hi1, box_hi2};
+    const int lane = threadIdx.x & 31;
+    int item;
+    if (!P.persistent) {
+        item = first_item + blockIdx.x * (blockDim.x >> 5) + warp;
+        if (item >= first_item + n_items) return;
+    }
+    for (;;) {
+        if (P.persistent) {
+            unsigned int it = 0;
+            if (lane == 0) it = atomicAdd(queue, 1u);
+            it = __shfl_sync(kFull, it, 0);
+            if ((int)it >= n_items) return;
+            item = (int)it;
+        }
+        const int lig = order[item / P.exhaustiveness];
+        const int chain = item % P.exhaustiveness;
+        const int slot = lig * P.exhaustiveness + chain;
+        Chain c;
+        bind_chain(c, B, L, lig, sw);
+        run_chain(c, M, Tb, P, lo, hi, lig, chain, poses + (size_t)slot * pose_stride, pose_stride,
+                  results + slot);
+        if (!P.persistent) return;
+    }
+}
+
+// Fixed poses: energy (search form, caps v_intra / v_inter) and gradient per pose.
+__global__ void __launch_bounds__(128) score_kernel(Batch B, Maps M, Tables Tb, Layout L,
+                                                    const int* pose_lig, const float* poses,
+                                                    int pose_stride, int n_poses, float v_intra,
+                                                    float v_inter, float* e_out, float* g_out,
+                                                    int g_stride, float* score_out) {
+    extern __shared__ float smem[];
+    const int warp = threadIdx.x >> 5;
+    const int pose = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (pose >= n_poses) return;
+    float* sw = smem + (size_t)warp * L.total;
+    Chain c;
+    bind_chain(c, B, L, pose_lig[pose], sw);
+    float* x = sw + L.x;
+    const int cs = 7 + c.T;
+    for (int i = c.lane; i < cs; i += 32) x[i] = poses[(size_t)pose * pose_stride + i];
+    __syncwarp();
+    if (g_out) {
+        float* g = sw + L.g;
+        float e = eval_deriv(c, M, Tb, x, g, v_intra, v_inter);
+        for (int i = c.lane; i < 6 + c.T; i += 32) g_out[(size_t)pose * g_stride + i] = g[i];
+        if (c.lane == 0) e_out[pose] = e;
+    }
+    if (score_out) {
+        float eg, ei;
+        eval_score(c, M, Tb, x, v_inter, eg, ei);
+        if (c.lane == 0) {
+            score_out[2 * pose] = eg;
+            score_out[2 * pose + 1] = ei;
+        }
+    }
+}
+
+// Local optimisation from given poses (quasi_newton, quasi_newton.cpp:42-53):
+// one warp per pose, BFGS at curl cap v; poses updated in place.
+__global__ void __launch_bounds__(128) optimize_kernel(Batch B, Maps M, Tables Tb, Layout L,
+                                                       const int* pose_lig, float* poses,
+                                                       int pose_stride, int n_poses, int max_steps,
+                                                       float v, float* e_out, int* evals_out) {
+    extern __shared__ float smem[];
+    const int warp = threadIdx.x >> 5;
+    const int pose = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (pose >= n_poses) return;
+    float* sw = smem + (size_t)warp * L.total;
+    Chain c;
+    bind_chain(c, B, L, pose_lig[pose], sw);
+    float* x = sw + L.x;
+    const int cs = 7 + c.T;
+    for (int i = c.lane; i < cs; i += 32) x[i] = poses[(size_t)pose * pose_stride + i];
+    __syncwarp();
+    int evals = 0;
+    const int steps = max_steps > 0 ? max_steps : c.lig.local_steps;
+    float e = bfgs(c, M, Tb, x, steps, v, evals);
+    for (int i = c.lane; i < cs; i += 32) poses[(size_t)pose * pose_stride + i] = x[i];
+    if (c.lane == 0) {
+        e_out[pose] = e;
+        if (evals_out) evals_out[pose] = evals;
+    }
+}
+
+// FP32 issue-rate probe: independent FMA chains, used to report the FP32
+// roofline denominator measured on the running GPU.
+__global__ void fp32_peak_kernel(float* out, int iters) {
+    float a0 = threadIdx.x * 1e-7f, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5,
+          a6 = a0 + 6, a7 = a0 + 7;
+    const float m = 0.9999999f, k = 1e-7f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            a0 = fmaf(a0, m, k); a1 = fmaf(a1, m, k); a2 = fmaf(a2, m, k); a3 = fmaf(a3, m, k);
+            a4 = fmaf(a4, m, k); a5 = fmaf(a5, m, k); a6 = fmaf(a6, m, k); a7 = fmaf(a7, m, k);
+        }
+    }
+    float r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (r == 123.456f) out[0] = r;
+}
+
+// Grid maps.  Block = 8x4x4 grid points; receptor atoms within reach of the
+// tile are compacted into shared memory in ascending index order so every
+// point sums its contributions in the reference's order (cache.cpp:471-549,
+// szv_grid.cpp:26-57); arithmetic uses explicit round-to-nearest intrinsics
+// (no contraction) to reproduce the reference's FP32 sums.
+constexpr int kMapTX = 8, kMapTY = 4, kMapTZ = 4;
+constexpr int kMapThreads = kMapTX * kMapTY * kMapTZ;
+constexpr int kMaxSlots = 36;
+constexpr int kMapStage = 1024;
+
+__global__ void __launch_bounds__(kMapThreads) maps_kernel(
+    const float4* __restrict__ rec, int n_rec, const float* __restrict__ fastT, int n_bins,
+    int n_slots_pad, int n_slots, float factor, float cutoff2, int nx, int ny, int nz,
+    float init0, float init1, float init2, float finv0, float finv1, float finv2,
+    float* __restrict__ out) {
+    __shared__ float4 stage[kMapStage];
+    __shared__ int warp_cnt[kMapThreads / 32];
+    __shared__ int total;
+    const int tx = threadIdx.x % kMapTX, ty = (threadIdx.x / kMapTX) % kMapTY,
+              tz = threadIdx.x / (kMapTX * kMapTY);
+    const int gx0 = blockIdx.x * kMapTX, gy0 = blockIdx.y * kMapTY, gz0 = blockIdx.z * kMapTZ;
+    const int x = gx0 + tx, y = gy0 + ty, z = gz0 + tz;
+    // tile bounding box
+    const float lo[3] = {init0 + finv0 * gx0, init1 + finv1 * gy0, init2 + finv2 * gz0};
+    const float hi[3] = {init0 + finv0 * (gx0 + kMapTX - 1), init1 + finv1 * (gy0 + kMapTY - 1),
+                         init2 + finv2 * (gz0 + kMapTZ - 1)};
+    const float reach2 = cutoff2 * 1.0001f + 1e-3f;
+    const float px = __fadd_rn(init0, __fmul_rn(finv0, (float)x));
+    const float py = __fadd_rn(init1, __fmul_rn(finv1, (float)y));
+    const float pz = __fadd_rn(init2, __fmul_rn(finv2, (float)z));
+    float acc[kMaxSlots];
+#pragma unroll
+    for (int k = 0; k < kMaxSlots; ++k) acc[k] = 0.0f;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int base = 0; base < n_rec; base += kMapThreads) {
+        // order-preserving compaction of the next chunk of candidate atoms
+        const int i = base + threadIdx.x;
+        bool take = false;
+        float4 a = make_float4(0, 0, 0, 0);
+        if (i < n_rec) {
+            a = rec[i];
+            float d2 = 0;
+            float c[3] = {a.x, a.y, a.z};
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                float d = fmaxf(fmaxf(lo[k] - c[k], c[k] - hi[k]), 0.0f);
+                d2 += d * d;
+            }
+            take = d2 <= reach2;
+        }
+        unsigned m = __ballot_sync(kFull, take);
+        if (lane == 0) warp_cnt[wid] = __popc(m);
+        __syncthreads();
+        int off = 0, tot = 0;
+        for (int w = 0; w < kMapThreads / 32; ++w) {
+            if (w < wid) off += warp_cnt[w];
+            tot += warp_cnt[w];
+        }
+        if (take) stage[off + __popc(m & ((1u << lane) - 1))] = a;
+        __syncthreads();
+        if (x < nx && y < ny && z < nz) {
+            for (int k = 0; k < tot; ++k) {
+                float4 r = stage[k];
+                float dx = __fsub_rn(r.x, px), dy = __fsub_rn(r.y, py), dz = __fsub_rn(r.z, pz);
+                float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+                if (r2 <= cutoff2) {
+                    const int t1 = __float_as_int(r.w);
+                    const int bin = (int)__fmul_rn(factor, r2);
+                    const float4* row = reinterpret_cast<const float4*>(
+                        fastT + ((size_t)t1 * n_bins + bin) * n_slots_pad);
+#pragma unroll
+                    for (int q = 0; q < kMaxSlots / 4; ++q) {
+                        if (4 * q < n_slots) {
+                            float4 v = __ldg(row + q);
+                            acc[4 * q] = __fadd_rn(acc[4 * q], v.x);
+                            acc[4 * q + 1] = __fadd_rn(acc[4 * q + 1], v.y);
+                            acc[4 * q + 2] = __fadd_rn(acc[4 * q + 2], v.z);
+                            acc[4 * q + 3] = __fadd_rn(acc[4 * q + 3], v.w);
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        (void)total;
+    }
+    if (x < nx && y < ny && z < nz) {
+        const size_t plane = (size_t)nx * ny * nz;
+        const size_t idx = x + (size_t)nx * (y + (size_t)ny * z);
+#pragma unroll
+        for (int k = 0; k < kMaxSlots; ++k)
+            if (k < n_slots) out[k * plane + idx] = acc[k];
+    }
+}
+
+}  // namespace dev
+
+// ---------------------------------------------------------------- host side
+// Launch helpers called from the C-ABI layer (ud_capi.cpp).
+
+struct DeviceBatchView {
+    const LigDesc* ligs;
+    const AtomRec* atoms;
+    const NodeRec* nodes;
+    const uint32_t* pairs;
+    int max_atoms, max_torsions;
+};
+
+struct DeviceMapsView {
+    const float* data;
+    MapsDesc desc;
+};
+
+struct DeviceTablesView {
+    const float* smooth;   // float2 per bin
+    const float* fast;
+    int n_bins;
+    float factor;
+    float cutoff2;
+};
+
+static dev::Maps to_maps(const DeviceMapsView& m) {
+    dev::Maps M;
+    M.data = m.data;
+    M.nx = m.desc.dims[0];
+    M.ny = m.desc.dims[1];
+    M.nz = m.desc.dims[2];
+    for (int i = 0; i < 3; ++i) {
+        M.init[i] = m.desc.init[i];
+        M.factor[i] = m.desc.factor[i];
+        M.factor_inv[i] = m.desc.factor_inv[i];
+        M.dim_m1[i] = m.desc.dim_m1[i];
+    }
+    M.slope = m.desc.slope;
+    return M;
+}
+
+static dev::Tables to_tables(const DeviceTablesView& t) {
+    dev::Tables T;
+    T.smooth = reinterpret_cast<const float2*>(t.smooth);
+    T.fast = t.fast;
+    T.n_bins = t.n_bins;
+    T.factor = t.factor;
+    T.cutoff2 = t.cutoff2;
+    return T;
+}
+
+static dev::Batch to_batch(const DeviceBatchView& b) {
+    dev::Batch B;
+    B.ligs = b.ligs;
+    B.atoms = b.atoms;
+    B.nodes = b.nodes;
+    B.pairs = b.pairs;
+    return B;
+}
+
+int engine_chain_smem_bytes(int max_atoms, int max_torsions) {
+    return dev::make_layout(max_atoms, max_torsions).total * (int)sizeof(float);
+}
+
+cudaError_t launch_maps(const float* rec_xyzt, int n_rec, const float* fastT, int n_bins,
+                        int n_slots, int n_slots_pad, float factor, float cutoff2,
+                        const MapsDesc& d, float* out, cudaStream_t stream) {
+    dim3 block(dev::kMapThreads);
+    dim3 grid((d.dims[0] + dev::kMapTX - 1) / dev::kMapTX, (d.dims[1] + dev::kMapTY - 1) / dev::kMapTY,
+              (d.dims[2] + dev::kMapTZ - 1) / dev::kMapTZ);
+    dev::maps_kernel<<<grid, block, 0, stream>>>(
+        reinterpret_cast<const float4*>(rec_xyzt), n_rec, fastT, n_bins, n_slots_pad, n_slots, factor,
+        cutoff2, d.dims[0], d.dims[1], d.dims[2], d.init[0], d.init[1], d.init[2], d.factor_inv[0],
+        d.factor_inv[1], d.factor_inv[2], out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_score(const DeviceBatchView& b, const DeviceMapsView& m,
+                         const DeviceTablesView& t, const int* pose_lig, const float* poses,
+                         int pose_stride, int n_poses, float v_intra, float v_inter, float* e_out,
+                         float* g_out, int g_stride, float* score_out, cudaStream_t stream) {
+    dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
+    const int warps = 4;
+    size_t smem = (size_t)warps * L.total * sizeof(float);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(dev::score_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    dim3 grid((n_poses + warps - 1) / warps);
+    dev::score_kernel<<<grid, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t), L,
+                                                          pose_lig, poses, pose_stride, n_poses,
+                                                          v_intra, v_inter, e_out, g_out, g_stride,
+                                                          score_out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_search(const DeviceBatchView& b, const DeviceMapsView& m,
+                          const DeviceTablesView& t, const SearchParams& P, const int* order,
+                          int n_items, int first_item, unsigned int* queue, float* poses,
+                          int pose_stride, ChainResult* results, int grid_blocks,
+                          cudaStream_t stream) {
+    dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
+    const int warps = P.chains_per_block > 0 ? P.chains_per_block : 4;
+    size_t smem = (size_t)warps * L.total * sizeof(float);
+    cudaError_t e = cudaFuncSetAttribute(dev::search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid;
+    if (P.persistent) grid = dim3(grid_blocks);
+    else grid = dim3((n_items + warps - 1) / warps);
+    const float* lo = m.desc.init;
+    const float* hi = m.desc.corner2;
+    dev::search_kernel<<<grid, warps * 32, smem, stream>>>(
+        to_batch(b), to_maps(m), to_tables(t), P, L, order, n_items, first_item, queue, lo[0], lo[1],
+        lo[2], hi[0], hi[1], hi[2], poses, pose_stride, results);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_optimize(const DeviceBatchView& b, const DeviceMapsView& m,
+                            const DeviceTablesView& t, const int* pose_lig, float* poses,
+                            int pose_stride, int n_poses, int max_steps, float v, float* e_out,
+                            int* evals_out, cudaStream_t stream) {
+    dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
+    const int warps = 4;
+    size_t smem = (size_t)warps * L.total * sizeof(float);
+    cudaError_t e = cudaFuncSetAttribute(dev::optimize_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid((n_poses + warps - 1) / warps);
+    dev::optimize_kernel<<<grid, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t),
+                                                             L, pose_lig, poses, pose_stride,
+                                                             n_poses, max_steps, v, e_out,
+                                                             evals_out);
+    return cudaGetLastError();
+}
+
+// Measured FP32 FMA throughput (TFLOP/s) of the current device.
+float measure_fp32_peak_tflops() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    float* out = nullptr;
+    if (cudaMalloc(&out, sizeof(float)) != cudaSuccess) return 0;
+    const int blocks = sms * 8, threads = 256, iters = 4096;
+    dev::fp32_peak_kernel<<<blocks, threads>>>(out, 16);
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float best = 0;
+    for (int rep = 0; rep < 3; ++rep) {
+        cudaEventRecord(a);
+        dev::fp32_peak_kernel<<<blocks, threads>>>(out, iters);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+        best = std::max(best, (float)(flops / (ms * 1e-3) / 1e12));
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    return best;
+}
+
+int search_blocks_per_sm(const DeviceBatchView& b, int warps) {
+    dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
+    size_t smem = (size_t)warps * L.total * sizeof(float);
+    cudaFuncSetAttribute(dev::search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, dev::search_kernel, warps * 32, smem) !=
+        cudaSuccess)
+        return 1;
+    return nb > 0 ? nb : 1;
+}
+
+}  // namespace ud

@@ -1,0 +1,79 @@
+// Device-side data layout of the docking engine and the host entry points
+// into ud_engine.cu.  Plain C++ (no CUDA types) so the C-ABI layer and the
+// host model code can include it.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+namespace ud {
+
+constexpr int kMaxLigAtoms = 256;  // atom indices packed in 8 bits in pair records
+constexpr int kMaxLigTorsions = 48;
+constexpr int kMaxNodes = kMaxLigTorsions + 1;
+constexpr int kTableBins = 2051;   // Vina/Vinardo r^2 bins (factor 32, cutoff 8 A)
+
+// Grid maps of one receptor box: x fastest, one map per requested XS type.
+struct MapsDesc {
+    int dims[3];           // sample points per axis (n_voxels + 1)
+    float init[3];         // box corner (grid::m_init)
+    float factor[3];       // samples per Angstrom (grid::m_factor)
+    float factor_inv[3];
+    float dim_m1[3];       // dims - 1 as float
+    float corner2[3];      // box end
+    float slope;           // out-of-box penalty slope
+    int n_maps;
+    int8_t slot_of_xs[36]; // map slot per XS grid type, -1 when absent
+};
+
+// One ligand's topology as it sits in device memory (offsets into the batch
+// arrays).  Nodes are in DFS pre-order: node k >= 1 owns torsion k - 1.
+struct LigDesc {
+    int atom_off, n_atoms;
+    int node_off, n_nodes;
+    int pair_off, n_pairs;
+    int n_heavy;
+    int max_depth;
+    int local_steps;       // BFGS iteration cap of this ligand
+    int pad[3];
+};
+
+struct NodeRec {            // 48 bytes
+    float rel_origin[3];
+    float rel_axis[3];
+    float origin0[3];      // input-frame origin (root: initial position)
+    int parent;
+    int depth;
+    int begin_end;         // begin | end << 16
+};
+
+// Atom record: local xyz and packed fields (node | (map slot + 1) << 8 |
+// heavy << 16 | (xs + 1) << 24).
+struct AtomRec {
+    float x, y, z;
+    int packed;
+};
+
+struct SearchParams {
+    int global_steps;
+    int exhaustiveness;    // chains per ligand
+    unsigned long long seed;
+    float hunt_cap;        // curl cap during the search (10)
+    float authentic_v;     // curl cap of the refinement (1000)
+    float temperature;     // Metropolis temperature (1.2)
+    float mutation_amplitude;
+    int lanes_per_chain;   // 32 (warp) or 16 / 8 (sub-warp)
+    int chains_per_block;
+    int persistent;        // 0: plain fixed-tiling launch, 1: persistent queue
+    int bfgs_cap;          // 0: per-ligand local_steps; >0: min(local_steps, cap)
+};
+
+// Result record of one chain.
+struct ChainResult {
+    float e;               // best energy (refined, authentic cap)
+    int evals;             // energy+gradient evaluations spent
+    int ligand;
+    int chain;
+};
+
+}  // namespace ud

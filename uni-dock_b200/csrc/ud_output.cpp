@@ -1,0 +1,111 @@
+// Pose output in the reference's formats: PDBQT MODEL blocks with the
+// "REMARK VINA RESULT" header (unidock/src/lib/vina.cpp:725-748, model.cpp:726-846)
+// and SDF records with the "> <Uni-Dock RESULT>" block (vina.cpp:750-770).
+#include <cstdio>
+#include <iomanip>
+#include <sstream>
+#include <stdexcept>
+
+#include "ud_model.h"
+
+namespace ud {
+
+static std::string fixed(float v, int width, int prec) {
+    std::ostringstream o;
+    o.setf(std::ios::fixed, std::ios::floatfield);
+    o.setf(std::ios::showpoint);
+    o << std::setw(width) << std::setprecision(prec) << v;
+    return o.str();
+}
+
+static void put_coord(std::string& line, std::size_t col, float v) {  // 1-based column, 8 wide
+    std::string s = fixed(v, 8, 3);
+    if (s.size() != 8) throw std::runtime_error("coordinate does not fit PDBQT columns");
+    if (line.size() < col - 1 + 8) line.resize(col - 1 + 8, ' ');
+    line.replace(col - 1, 8, s);
+}
+
+static std::string vina_remarks(const PoseResult& p, bool ad4) {
+    std::ostringstream r;
+    r << "REMARK VINA RESULT: " << fixed(p.e, 9, 3) << "  " << fixed(p.lb, 9, 3) << "  " << fixed(p.ub, 9, 3)
+      << '\n';
+    r << "REMARK INTER + INTRA:    " << fixed(p.total, 12, 3) << "\n";
+    r << "REMARK INTER:            " << fixed(p.inter, 12, 3) << "\n";
+    r << "REMARK INTRA:            " << fixed(p.intra, 12, 3) << "\n";
+    if (ad4) r << "REMARK CONF_INDEPENDENT: " << fixed(p.conf_indep, 12, 3) << "\n";
+    r << "REMARK UNBOUND:          " << fixed(p.unbound, 12, 3) << "\n";
+    return r.str();
+}
+
+static std::string sdf_remarks(const PoseResult& p, bool ad4) {
+    std::ostringstream r;
+    r << "> <Uni-Dock RESULT> \nENERGY=" << fixed(p.e, 9, 3) << "  LOWER_BOUND=" << fixed(p.lb, 9, 3)
+      << "  UPPER_BOUND=" << fixed(p.ub, 9, 3) << '\n';
+    r << "INTER + INTRA:    " << fixed(p.total, 12, 3) << "\n";
+    r << "INTER:            " << fixed(p.inter, 12, 3) << "\n";
+    r << "INTRA:            " << fixed(p.intra, 12, 3) << "\n";
+    if (ad4) r << "CONF_INDEPENDENT: " << fixed(p.conf_indep, 12, 3) << "\n";
+    r << "UNBOUND:          " << fixed(p.unbound, 12, 3) << "\n";
+    r << '\n';
+    return r.str();
+}
+
+std::string write_pdbqt_models(const Ligand& lig, const std::vector<PoseResult>& poses, bool ad4) {
+    std::ostringstream out;
+    std::vector<float> xyz(3 * lig.atoms.size());
+    for (std::size_t m = 0; m < poses.size(); ++m) {
+        ligand_coords(lig, poses[m].pose.data(), xyz.data());
+        out << "MODEL " << (m + 1) << '\n';
+        out << vina_remarks(poses[m], ad4);
+        for (const auto& c : lig.context) {
+            if (c.second >= 0) {
+                std::string line = c.first;
+                put_coord(line, 31, xyz[3 * c.second]);
+                put_coord(line, 39, xyz[3 * c.second + 1]);
+                put_coord(line, 47, xyz[3 * c.second + 2]);
+                out << line << '\n';
+            } else {
+                out << c.first << '\n';
+            }
+        }
+        out << "ENDMDL\n";
+    }
+    return out.str();
+}
+
+std::string write_sdf_models(const Ligand& lig, const std::vector<PoseResult>& poses, bool ad4) {
+    // SDF records are written for ligands that came from SDF input; PDBQT
+    // input is written as a minimal V2000 block of its atoms.
+    std::ostringstream out;
+    std::vector<float> xyz(3 * lig.atoms.size());
+    static const char* el_name[] = {"H", "C", "N", "O", "S", "P", "F", "Cl", "Br", "I", "Si", "At", "X", "X"};
+    for (std::size_t m = 0; m < poses.size(); ++m) {
+        ligand_coords(lig, poses[m].pose.data(), xyz.data());
+        out << (lig.name.empty() ? "ligand" : lig.name) << "\n  unidock_b200\n\n";
+        int nb = 0;
+        for (auto& a : lig.atoms) nb += (int)a.bonds.size();
+        nb /= 2;
+        char buf[128];
+        std::snprintf(buf, sizeof buf, "%3d%3d  0  0  0  0  0  0  0  0999 V2000\n", (int)lig.atoms.size(), nb);
+        out << buf;
+        for (std::size_t i = 0; i < lig.atoms.size(); ++i) {
+            int el = lig.atoms[i].el;
+            const char* nm = (el >= 0 && el < 14) ? el_name[el] : "X";
+            std::snprintf(buf, sizeof buf, "%10.4f%10.4f%10.4f %-3s 0  0  0  0  0  0  0  0  0  0  0  0\n",
+                          xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], nm);
+            out << buf;
+        }
+        for (std::size_t i = 0; i < lig.atoms.size(); ++i)
+            for (int j : lig.atoms[i].bonds)
+                if ((int)i < j) {
+                    std::snprintf(buf, sizeof buf, "%3d%3d  1  0\n", (int)i + 1, j + 1);
+                    out << buf;
+                }
+        out << "M  END\n";
+        out << sdf_remarks(poses[m], ad4);
+        out << "$$$$\n";
+    }
+    return out.str();
+}
+
+}  // namespace ud

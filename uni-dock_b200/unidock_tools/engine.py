@@ -1,0 +1,327 @@
+"""ctypes binding of the C ABI in include/unidock_b200.h.
+
+This module is the Python-side mirror of the reference's docking entry points
+(receptor maps, ligand parsing, fixed-pose scoring, batched search).  It loads
+the in-tree ``lib/libunidock_b200.so`` and raises when it is missing: there is
+no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG_ROOT = Path(__file__).resolve().parent.parent      # uni-dock_b200/
+LIB_PATH = PKG_ROOT / "lib" / "libunidock_b200.so"
+
+SF_VINA, SF_AD4, SF_VINARDO = 0, 1, 2
+UD_OK = 0
+
+_lib = None
+
+
+class UdError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"unidock_b200 error {code}: {msg}")
+        self.code = code
+
+
+class SearchParams(C.Structure):
+    _fields_ = [
+        ("exhaustiveness", C.c_int),
+        ("max_step", C.c_int),
+        ("num_modes", C.c_int),
+        ("min_rmsd", C.c_float),
+        ("energy_range", C.c_float),
+        ("seed", C.c_ulonglong),
+        ("form", C.c_int),
+        ("chains_per_block", C.c_int),
+        ("bfgs_cap", C.c_int),
+        ("use_graph", C.c_int),
+    ]
+
+
+def lib():
+    """Load the engine library (once)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise FileNotFoundError(
+            f"{LIB_PATH} is missing: build it with `make -C {PKG_ROOT}` (or __graft_entry__.build())")
+    L = C.CDLL(str(LIB_PATH))
+    vp, ip, fp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_float)
+    sig = {
+        "ud_version": ([], C.c_int),
+        "ud_last_error": ([], C.c_char_p),
+        "ud_receptor_parse": ([C.c_char_p, C.c_size_t, fp, ip, C.c_int, ip], C.c_int),
+        "ud_maps_create": ([C.c_int, fp, C.c_int, fp, ip, C.c_int, fp, fp, C.c_float, ip, C.c_int, vp,
+                            C.POINTER(vp)], C.c_int),
+        "ud_maps_info": ([vp, ip, fp, fp, ip], C.c_int),
+        "ud_maps_read": ([vp, C.c_int, fp, C.c_size_t], C.c_int),
+        "ud_maps_destroy": ([vp], C.c_int),
+        "ud_ligand_parse": ([C.c_char_p, C.c_size_t, C.POINTER(vp)], C.c_int),
+        "ud_ligand_counts": ([vp, ip], C.c_int),
+        "ud_ligand_export": ([vp, fp, fp, ip, ip, ip, fp, ip, ip, ip, ip, fp, ip, ip], C.c_int),
+        "ud_ligand_initial_pose": ([vp, fp], C.c_int),
+        "ud_ligand_coords": ([vp, fp, fp], C.c_int),
+        "ud_ligand_conf_indep": ([vp, fp], C.c_int),
+        "ud_ligand_destroy": ([vp], C.c_int),
+        "ud_batch_create": ([vp, C.POINTER(vp), C.c_int, vp, C.POINTER(vp)], C.c_int),
+        "ud_batch_destroy": ([vp], C.c_int),
+        "ud_score_grad": ([vp, ip, fp, C.c_int, C.c_int, C.c_float, C.c_float, fp, fp, C.c_int, vp], C.c_int),
+        "ud_score_grad_device": ([vp, vp, vp, C.c_int, C.c_int, C.c_float, C.c_float, vp, vp, C.c_int, vp],
+                                 C.c_int),
+        "ud_score": ([vp, ip, fp, C.c_int, C.c_int, C.c_float, fp, vp], C.c_int),
+        "ud_search": ([vp, C.POINTER(SearchParams), vp], C.c_int),
+        "ud_search_launch": ([vp, C.POINTER(SearchParams), vp], C.c_int),
+        "ud_search_collect": ([vp, vp], C.c_int),
+        "ud_search_chains": ([vp, fp, C.c_int, fp, ip], C.c_int),
+        "ud_result_count": ([vp, C.c_int, ip], C.c_int),
+        "ud_result_mode": ([vp, C.c_int, C.c_int, fp, fp], C.c_int),
+        "ud_result_write": ([vp, C.c_int, C.c_int, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
+        "ud_search_stats": ([vp, C.POINTER(C.c_longlong), fp], C.c_int),
+        "ud_optimize": ([vp, ip, fp, C.c_int, C.c_int, C.c_int, C.c_float, fp, ip, vp], C.c_int),
+        "ud_device_fp32_peak": ([fp], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def exported_symbols():
+    """Names declared in include/unidock_b200.h."""
+    hdr = PKG_ROOT.parent / "include" / "unidock_b200.h"
+    import re
+    return sorted(set(re.findall(r"\bint\s+(ud_\w+)\s*\(", hdr.read_text())) |
+                  set(re.findall(r"const char\*\s+(ud_\w+)\s*\(", hdr.read_text())))
+
+
+def _check(code):
+    if code != UD_OK:
+        raise UdError(code, lib().ud_last_error().decode())
+
+
+def _f(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _i(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def fp32_peak_tflops() -> float:
+    v = C.c_float()
+    _check(lib().ud_device_fp32_peak(C.byref(v)))
+    return float(v.value)
+
+
+def parse_receptor(pdbqt: str):
+    b = pdbqt.encode()
+    n = C.c_int()
+    _check(lib().ud_receptor_parse(b, len(b), None, None, 0, C.byref(n)))
+    xyz = np.zeros((n.value, 3), np.float32)
+    xs = np.zeros(n.value, np.int32)
+    _check(lib().ud_receptor_parse(b, len(b), _f(xyz), _i(xs), n.value, C.byref(n)))
+    return xyz, xs
+
+
+class Maps:
+    """Receptor grid maps on the GPU (ud_maps_create)."""
+
+    def __init__(self, rec_xyz, rec_xs, center, size, spacing=0.375, sf=SF_VINA, weights=None,
+                 types=None):
+        rec_xyz = np.ascontiguousarray(rec_xyz, np.float32)
+        rec_xs = np.ascontiguousarray(rec_xs, np.int32)
+        center = np.ascontiguousarray(center, np.float32)
+        size = np.ascontiguousarray(size, np.float32)
+        w = None if weights is None else np.ascontiguousarray(weights, np.float32)
+        t = None if types is None else np.ascontiguousarray(types, np.int32)
+        h = C.c_void_p()
+        _check(lib().ud_maps_create(sf, None if w is None else _f(w), 0 if w is None else len(w),
+                                    _f(rec_xyz), _i(rec_xs), len(rec_xs), _f(center), _f(size),
+                                    float(spacing), None if t is None else _i(t), 0 if t is None else len(t),
+                                    None, C.byref(h)))
+        self.h = h
+        self.sf = sf
+
+    def info(self):
+        d = np.zeros(3, np.int32)
+        init = np.zeros(3, np.float32)
+        fac = np.zeros(3, np.float32)
+        n = C.c_int()
+        _check(lib().ud_maps_info(self.h, _i(d), _f(init), _f(fac), C.byref(n)))
+        return d, init, fac, n.value
+
+    def read(self, xs):
+        d, _, _, _ = self.info()
+        out = np.zeros(int(d.prod()), np.float32)
+        _check(lib().ud_maps_read(self.h, int(xs), _f(out), out.size))
+        return out.reshape(d[2], d[1], d[0])  # [z][y][x]
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.ud_maps_destroy(self.h)
+            self.h = None
+
+
+class Ligand:
+    """Host-side torsion-tree model parsed from PDBQT (ud_ligand_parse)."""
+
+    def __init__(self, pdbqt: str):
+        b = pdbqt.encode()
+        h = C.c_void_p()
+        _check(lib().ud_ligand_parse(b, len(b), C.byref(h)))
+        self.h = h
+        c = np.zeros(8, np.int32)
+        _check(lib().ud_ligand_counts(h, _i(c)))
+        (self.n_atoms, self.n_heavy, self.n_torsions, self.n_nodes, self.n_pairs, self.torsdof,
+         self.n_glue, self.local_steps) = [int(v) for v in c]
+
+    def export(self):
+        n, R, P = self.n_atoms, self.n_nodes, self.n_pairs
+        out = dict(lab=np.zeros((n, 3), np.float32), local=np.zeros((n, 3), np.float32),
+                   xs=np.zeros(n, np.int32), ad=np.zeros(n, np.int32), el=np.zeros(n, np.int32),
+                   charge=np.zeros(n, np.float32), node=np.zeros(n, np.int32),
+                   parent=np.zeros(R, np.int32), begin=np.zeros(R, np.int32), end=np.zeros(R, np.int32),
+                   rel=np.zeros((R, 6), np.float32), pair_a=np.zeros(max(P, 1), np.int32),
+                   pair_b=np.zeros(max(P, 1), np.int32))
+        _check(lib().ud_ligand_export(self.h, _f(out["lab"]), _f(out["local"]), _i(out["xs"]), _i(out["ad"]),
+                                      _i(out["el"]), _f(out["charge"]), _i(out["node"]), _i(out["parent"]),
+                                      _i(out["begin"]), _i(out["end"]), _f(out["rel"]), _i(out["pair_a"]),
+                                      _i(out["pair_b"])))
+        out["pair_a"] = out["pair_a"][:P]
+        out["pair_b"] = out["pair_b"][:P]
+        return out
+
+    def initial_pose(self):
+        p = np.zeros(7 + self.n_torsions, np.float32)
+        _check(lib().ud_ligand_initial_pose(self.h, _f(p)))
+        return p
+
+    def coords(self, pose):
+        pose = np.ascontiguousarray(pose, np.float32)
+        xyz = np.zeros((self.n_atoms, 3), np.float32)
+        _check(lib().ud_ligand_coords(self.h, _f(pose), _f(xyz)))
+        return xyz
+
+    def conf_indep(self):
+        o = np.zeros(7, np.float32)
+        _check(lib().ud_ligand_conf_indep(self.h, _f(o)))
+        return o
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.ud_ligand_destroy(self.h)
+            self.h = None
+
+
+class Batch:
+    """Ligand topologies resident on the GPU (ud_batch_create)."""
+
+    def __init__(self, maps: Maps, ligands):
+        self.maps = maps
+        self.ligands = list(ligands)
+        arr = (C.c_void_p * len(self.ligands))(*[l.h.value for l in self.ligands])
+        h = C.c_void_p()
+        _check(lib().ud_batch_create(maps.h, arr, len(self.ligands), None, C.byref(h)))
+        self.h = h
+        self.max_torsions = max([l.n_torsions for l in self.ligands] + [0])
+
+    # ---- fixed poses
+    def score_grad(self, pose_ligand, poses, v_intra=1000.0, v_inter=1000.0):
+        pose_ligand = np.ascontiguousarray(pose_ligand, np.int32)
+        poses = np.ascontiguousarray(poses, np.float32)
+        n, stride = poses.shape
+        gs = 6 + self.max_torsions
+        e = np.zeros(n, np.float32)
+        g = np.zeros((n, gs), np.float32)
+        _check(lib().ud_score_grad(self.h, _i(pose_ligand), _f(poses), n, stride, float(v_intra),
+                                   float(v_inter), _f(e), _f(g), gs, None))
+        return e, g
+
+    def score_grad_device(self, pose_ligand_ptr, poses_ptr, n, stride, e_ptr, g_ptr, g_stride,
+                          v_intra=1000.0, v_inter=1000.0, stream=0):
+        _check(lib().ud_score_grad_device(self.h, C.c_void_p(pose_ligand_ptr), C.c_void_p(poses_ptr), n, stride,
+                                          float(v_intra), float(v_inter), C.c_void_p(e_ptr), C.c_void_p(g_ptr),
+                                          g_stride, C.c_void_p(stream) if stream else None))
+
+    def score(self, pose_ligand, poses, v=1000.0):
+        pose_ligand = np.ascontiguousarray(pose_ligand, np.int32)
+        poses = np.ascontiguousarray(poses, np.float32)
+        n, stride = poses.shape
+        out = np.zeros((n, 2), np.float32)
+        _check(lib().ud_score(self.h, _i(pose_ligand), _f(poses), n, stride, float(v), _f(out), None))
+        return out
+
+    # ---- search
+    def search(self, exhaustiveness=8, max_step=0, num_modes=9, min_rmsd=1.0, energy_range=3.0, seed=0,
+               form=1, chains_per_block=0, bfgs_cap=0, use_graph=0):
+        p = SearchParams(exhaustiveness, max_step, num_modes, min_rmsd, energy_range, seed, form,
+                         chains_per_block, bfgs_cap, use_graph)
+        _check(lib().ud_search(self.h, C.byref(p), None))
+        self.exhaustiveness = exhaustiveness
+
+    def search_launch(self, exhaustiveness=8, max_step=0, num_modes=9, min_rmsd=1.0, energy_range=3.0, seed=0,
+                      form=1, chains_per_block=0, bfgs_cap=0, use_graph=0):
+        """Enqueue the search kernels only (device-resident inputs, asynchronous)."""
+        self._p = SearchParams(exhaustiveness, max_step, num_modes, min_rmsd, energy_range, seed, form,
+                               chains_per_block, bfgs_cap, use_graph)
+        _check(lib().ud_search_launch(self.h, C.byref(self._p), None))
+        self.exhaustiveness = exhaustiveness
+
+    def search_collect(self):
+        _check(lib().ud_search_collect(self.h, None))
+
+    def optimize(self, pose_ligand, poses, v=1000.0, max_steps=0):
+        pose_ligand = np.ascontiguousarray(pose_ligand, np.int32)
+        poses = np.array(poses, np.float32, copy=True, order="C")
+        n, stride = poses.shape
+        e = np.zeros(n, np.float32)
+        ev = np.zeros(n, np.int32)
+        _check(lib().ud_optimize(self.h, _i(pose_ligand), _f(poses), n, stride, int(max_steps), float(v), _f(e),
+                                 _i(ev), None))
+        return poses, e, ev
+
+    def chains(self):
+        n = len(self.ligands) * self.exhaustiveness
+        stride = 7 + self.max_torsions
+        poses = np.zeros((n, stride), np.float32)
+        e = np.zeros(n, np.float32)
+        ev = np.zeros(n, np.int32)
+        _check(lib().ud_search_chains(self.h, _f(poses), stride, _f(e), _i(ev)))
+        return poses, e, ev
+
+    def modes(self, lig):
+        n = C.c_int()
+        _check(lib().ud_result_count(self.h, lig, C.byref(n)))
+        out = []
+        for k in range(n.value):
+            pose = np.zeros(7 + self.ligands[lig].n_torsions, np.float32)
+            en = np.zeros(8, np.float32)
+            _check(lib().ud_result_mode(self.h, lig, k, _f(pose), _f(en)))
+            out.append((pose, en))
+        return out
+
+    def write(self, lig, fmt=0):
+        ln = C.c_size_t()
+        _check(lib().ud_result_write(self.h, lig, fmt, None, 0, C.byref(ln)))
+        buf = C.create_string_buffer(ln.value + 1)
+        _check(lib().ud_result_write(self.h, lig, fmt, buf, ln.value + 1, C.byref(ln)))
+        return buf.value.decode()
+
+    def stats(self):
+        ev = C.c_longlong()
+        ms = C.c_float()
+        _check(lib().ud_search_stats(self.h, C.byref(ev), C.byref(ms)))
+        return ev.value, ms.value
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.ud_batch_destroy(self.h)
+            self.h = None
