@@ -46,24 +46,28 @@ def parse_args():
     ap.add_argument("--cpu-sample", type=int, default=16, help="ligands timed on the reference CPU path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chains-per-block", type=int, default=0)
+    ap.add_argument("--profile-case", type=int, default=0,
+                    help="profiling aid: search N ligands of the workload twice and exit (no JSON)")
     return ap.parse_args()
 
 
-# ------------------------------------------------------------------ workload
-def make_workload(seed=20261203):
-    from unidock_tools import synth
+def profile_case(args):
+    """Small case of the same kernel for ncu: the second search launch is the one to capture."""
+    import torch
+    from unidock_tools import engine, synth
     rec = synth.make_receptor(3000, seed=1)
-    ligs = synth.ligand_set(N_LIGANDS, seed=seed, heavy=(12, 48), torsions=(0, 10))
-    return rec, [l.to_pdbqt() for l in ligs]
-
-
-def _ligand_texts(n, start=0, seed=20261203):
-    from unidock_tools import synth
-    rng_ligs = []
-    for k in range(start, start + n):
-        # same per-ligand seeds as synth.ligand_set (sizes drawn from its stream)
-        rng_ligs.append(k)
-    return rng_ligs
+    maps = engine.Maps(rec.xyz, rec.xs, np.zeros(3, np.float32), np.full(3, BOX, np.float32), SPACING)
+    ligs = [engine.Ligand(l.to_pdbqt()) for l in
+            synth.ligand_set(args.profile_case, seed=20261203, heavy=(12, 48), torsions=(0, 10))]
+    b = engine.Batch(maps, ligs)
+    P = dict(exhaustiveness=EXHAUSTIVENESS, max_step=MAX_STEP, seed=42, form=1,
+             chains_per_block=args.chains_per_block)
+    for _ in range(2):
+        b.search_launch(**P)
+        torch.cuda.synchronize()
+    b.search_collect()
+    ev, ms = b.stats()
+    print(f"profile case: {len(ligs)} ligands, {ev} evals, {ms:.1f} ms", flush=True)
 
 
 class Clocks:
@@ -355,6 +359,9 @@ def main():
     args = parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus == 1 else 1)))
+    if args.profile_case > 0:
+        profile_case(args)
+        return
     if args.impl == "reference":
         res = run_reference(args, rank, world)
     else:

@@ -268,7 +268,22 @@ extern "C" int ud_maps_create(int sf, const float* weights, int n_weights, const
         m->n_bins = tab.n;
         m->factor = tab.factor;
         m->cutoff2 = m->sf.cutoff * m->sf.cutoff;
-        m->smooth.upload(tab.smooth.data(), tab.smooth.size(), s);
+        // lerp table with both bracketing bins in one 16-byte record:
+        // [tp][bin] = (e_bin, dor_bin, e_bin+1, dor_bin+1)
+        {
+            const size_t ntp = tab.smooth.size() / (2 * (size_t)tab.n);
+            std::vector<float> s4(ntp * tab.n * 4, 0.0f);
+            for (size_t tp = 0; tp < ntp; ++tp)
+                for (int k = 0; k < tab.n; ++k) {
+                    const float* row = &tab.smooth[tp * tab.n * 2];
+                    float* o = &s4[(tp * tab.n + k) * 4];
+                    o[0] = row[2 * k];
+                    o[1] = row[2 * k + 1];
+                    o[2] = (k + 1 < tab.n) ? row[2 * (k + 1)] : 0.0f;
+                    o[3] = (k + 1 < tab.n) ? row[2 * (k + 1) + 1] : 0.0f;
+                }
+            m->smooth.upload(s4.data(), s4.size(), s);
+        }
         m->fast.upload(tab.fast.data(), tab.fast.size(), s);
         // receptor-type-major table for the map kernel: [t1][bin][slot]
         const int nslot = d.n_maps, nslot_pad = std::max(4, (nslot + 3) & ~3);
@@ -431,6 +446,36 @@ extern "C" int ud_ligand_destroy(ud_ligand lig) {
 
 // ---------------------------------------------------------------- batches
 
+// Pair records in groups of 32 (one warp-wide step of the pair loop): slots
+// 0-15 and 16-31 are each a matching (no atom twice), so the two half-warps can
+// add their pair forces into shared memory one after the other without
+// atomics.  Unfilled slots hold kPairPad; the list length is a multiple of 32.
+static std::vector<uint32_t> pair_groups(const Ligand& L) {
+    std::vector<uint32_t> out;
+    std::vector<char> used(L.pairs.size(), 0);
+    std::vector<int> stamp(L.atoms.size(), -1);
+    size_t left = L.pairs.size(), start = 0;
+    int half_id = 0;
+    while (left > 0) {
+        for (int half = 0; half < 2; ++half, ++half_id) {
+            int filled = 0;
+            for (size_t k = start; k < L.pairs.size() && filled < 16; ++k) {
+                if (used[k]) continue;
+                const Pair& p = L.pairs[k];
+                if (stamp[p.a] == half_id || stamp[p.b] == half_id) continue;
+                stamp[p.a] = stamp[p.b] = half_id;
+                used[k] = 1;
+                --left;
+                ++filled;
+                out.push_back((uint32_t)p.a | ((uint32_t)p.b << 8) | ((uint32_t)p.tp << 16));
+            }
+            while (start < L.pairs.size() && used[start]) ++start;
+            while (filled++ < 16) out.push_back(kPairPad);
+        }
+    }
+    return out;
+}
+
 extern "C" int ud_batch_create(ud_maps maps, const ud_ligand* ligs, int n, void* stream, ud_batch* out) {
     return guarded([&] {
         if (!maps || !out || n < 0 || (n > 0 && !ligs)) throw Error(UD_ERR_ARG, "invalid batch arguments");
@@ -460,17 +505,21 @@ extern "C" int ud_batch_create(ud_maps maps, const ud_ligand* ligs, int n, void*
             std::vector<int> depth(L.nodes.size(), 0);
             for (size_t k = 1; k < L.nodes.size(); ++k) depth[k] = depth[L.nodes[k].parent] + 1;
             d.max_depth = *std::max_element(depth.begin(), depth.end());
+            std::vector<int> subtree_end(L.nodes.size());
+            for (size_t k = 0; k < L.nodes.size(); ++k) subtree_end[k] = (int)k + 1;
+            for (size_t k = L.nodes.size(); k-- > 1;)  // children have larger DFS indices
+                subtree_end[L.nodes[k].parent] = std::max(subtree_end[L.nodes[k].parent], subtree_end[k]);
             for (size_t k = 0; k < L.nodes.size(); ++k) {
                 const Node& nd = L.nodes[k];
                 NodeRec r{};
                 for (int q = 0; q < 3; ++q) {
                     r.rel_origin[q] = nd.rel_origin[q];
                     r.rel_axis[q] = nd.rel_axis[q];
-                    r.origin0[q] = nd.origin0[q];
                 }
                 r.parent = nd.parent < 0 ? 0 : nd.parent;
                 r.depth = depth[k];
                 r.begin_end = nd.begin | (nd.end << 16);
+                r.subtree_end = subtree_end[k];
                 nodes.push_back(r);
             }
             for (const Atom& a : L.atoms) {
@@ -487,7 +536,9 @@ extern "C" int ud_batch_create(ud_maps maps, const ud_ligand* ligs, int n, void*
                 r.packed = a.node | ((slot + 1) << 8) | (heavy << 16) | (xsp << 24);
                 atoms.push_back(r);
             }
-            for (const Pair& p : L.pairs) pairs.push_back((uint32_t)p.a | ((uint32_t)p.b << 8) | ((uint32_t)p.tp << 16));
+            std::vector<uint32_t> ordered = pair_groups(L);
+            pairs.insert(pairs.end(), ordered.begin(), ordered.end());
+            d.n_pairs = (int)ordered.size();
             b->desc.push_back(d);
             b->max_atoms = std::max(b->max_atoms, d.n_atoms);
             b->max_tors = std::max(b->max_tors, d.n_nodes - 1);

@@ -152,8 +152,10 @@ struct Batch {
     const uint32_t* pairs;
 };
 
+constexpr int kPairBatch = 4;  // pair groups whose table rows are in flight together
+
 struct Tables {
-    const float2* smooth;  // [tp][bin] (e, dE/dr / r)
+    const float4* smooth4; // [tp][bin] (e, dE/dr / r) of bin and bin + 1
     const float* fast;     // [tp][bin]
     int n_bins;
     float factor;
@@ -216,8 +218,21 @@ struct Chain {
 };
 
 // Forward kinematics: node frames by tree depth, then atom coordinates.
-__device__ void kinematics(const Chain& c, const float* conf) {
+// A branch's orientation is the parent's composed with the torsion rotation
+// about the branch axis; written in the parent's frame that rotation
+// (axis_angle(rel_axis, theta)) does not depend on the parent, so all torsion
+// quaternions are formed in one parallel pass and each tree level only
+// composes q_parent * t (equal to axis_angle(R_parent rel_axis, theta) * q_parent
+// of tree.h:116-128 for unit quaternions).
+__device__ __noinline__ void kinematics(const Chain& c, const float* conf) {
     float* fr = c.s + c.L.frames;
+    // frame layout (20 floats): origin[0..2] q[3..6] R[7..15] lab axis[16..18];
+    // [16..19] hold the local torsion quaternion until the node is composed
+    for (int n = 1 + c.lane; n < c.R; n += 32) {
+        const NodeRec* nr = c.nodes + n;
+        float ra[3] = {__ldg(&nr->rel_axis[0]), __ldg(&nr->rel_axis[1]), __ldg(&nr->rel_axis[2])};
+        axis_angle_q(ra, conf[7 + n - 1], fr + 20 * n + 16);
+    }
     if (c.lane == 0) {
         fr[0] = conf[0]; fr[1] = conf[1]; fr[2] = conf[2];
         fr[3] = conf[3]; fr[4] = conf[4]; fr[5] = conf[5]; fr[6] = conf[6];
@@ -233,19 +248,17 @@ __device__ void kinematics(const Chain& c, const float* conf) {
             const float* pm = pf + 7;
             float ro[3] = {__ldg(&nr->rel_origin[0]), __ldg(&nr->rel_origin[1]), __ldg(&nr->rel_origin[2])};
             float ra[3] = {__ldg(&nr->rel_axis[0]), __ldg(&nr->rel_axis[1]), __ldg(&nr->rel_axis[2])};
-            float ax[3];
+            float t[4] = {f[16], f[17], f[18], f[19]};
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
                 f[i] = pf[i] + (pm[3 * i] * ro[0] + pm[3 * i + 1] * ro[1] + pm[3 * i + 2] * ro[2]);
-                ax[i] = pm[3 * i] * ra[0] + pm[3 * i + 1] * ra[1] + pm[3 * i + 2] * ra[2];
+                f[16 + i] = pm[3 * i] * ra[0] + pm[3 * i + 1] * ra[1] + pm[3 * i + 2] * ra[2];
             }
-            float t[4], q[4];
-            axis_angle_q(ax, conf[7 + n - 1], t);
-            qmul(t, pf + 3, q);
+            float q[4];
+            qmul(pf + 3, t, q);
             qnormalize_approx(q);
             f[3] = q[0]; f[4] = q[1]; f[5] = q[2]; f[6] = q[3];
             q_to_r3(q, f + 7);
-            f[16] = ax[0]; f[17] = ax[1]; f[18] = ax[2];
         }
         __syncwarp();
     }
@@ -319,7 +332,7 @@ __device__ __forceinline__ float grid_eval(const Maps& M, int slot, const float*
 }
 
 // Energy and gradient (change layout: position, torque, torsions) of `conf`.
-__device__ float eval_deriv(const Chain& c, const Maps& M, const Tables& Tb, const float* conf,
+__device__ __noinline__ float eval_deriv(const Chain& c, const Maps& M, const Tables& Tb, const float* conf,
                             float* g, float v_intra, float v_inter) {
     kinematics(c, conf);
     const float* xyz = c.s + c.L.coords;
@@ -333,33 +346,65 @@ __device__ float eval_deriv(const Chain& c, const Maps& M, const Tables& Tb, con
         frc[3 * a] = gx; frc[3 * a + 1] = gy; frc[3 * a + 2] = gz;
     }
     __syncwarp();
-    for (int k = c.lane; k < c.lig.n_pairs; k += 32) {
-        uint32_t pr = __ldg(c.pairs + k);
-        int a = pr & 0xFF, b = (pr >> 8) & 0xFF, tp = pr >> 16;
-        float rx = xyz[3 * b] - xyz[3 * a], ry = xyz[3 * b + 1] - xyz[3 * a + 1],
-              rz = xyz[3 * b + 2] - xyz[3 * a + 2];
-        float r2 = rx * rx + ry * ry + rz * rz;
-        if (r2 < Tb.cutoff2) {
-            float rf = Tb.factor * r2;
-            int i1 = (int)rf;
-            float rem = rf - i1;
-            const float2* row = Tb.smooth + (size_t)tp * Tb.n_bins;
-            float2 p1 = __ldg(row + i1), p2 = __ldg(row + i1 + 1);
-            float ep = p1.x + rem * (p2.x - p1.x);
-            float dor = p1.y + rem * (p2.y - p1.y);
-            float fx = dor * rx, fy = dor * ry, fz = dor * rz;
-            if (ep > 0 && v_intra < 0.1f * kMaxFl) {
-                float tmp = (v_intra < kEps) ? 0 : (v_intra / (v_intra + ep));
-                ep *= tmp;
-                float t2 = tmp * tmp;
-                fx *= t2; fy *= t2; fz *= t2;
+    // Pairs in 32-slot groups whose two half-warps are matchings (no atom twice
+    // within a half): table rows of kPairBatch groups are loaded before any is
+    // consumed, then each half-warp adds its forces in turn (no atomics).
+    const int n_groups = c.lig.n_pairs >> 5;
+    for (int g0 = 0; g0 < n_groups; g0 += kPairBatch) {
+        float4 tv[kPairBatch];
+        float rv[kPairBatch][3];
+        float remv[kPairBatch];
+        uint32_t prv[kPairBatch];
+#pragma unroll
+        for (int u = 0; u < kPairBatch; ++u) {
+            prv[u] = kPairPad;
+            if (g0 + u < n_groups) {
+                uint32_t pr = __ldg(c.pairs + ((g0 + u) << 5) + c.lane);
+                if (pr != kPairPad) {
+                    int a = pr & 0xFF, b = (pr >> 8) & 0xFF, tp = pr >> 16;
+                    float rx = xyz[3 * b] - xyz[3 * a], ry = xyz[3 * b + 1] - xyz[3 * a + 1],
+                          rz = xyz[3 * b + 2] - xyz[3 * a + 2];
+                    float r2 = rx * rx + ry * ry + rz * rz;
+                    if (r2 < Tb.cutoff2) {
+                        float rf = Tb.factor * r2;
+                        int i1 = (int)rf;
+                        remv[u] = rf - i1;
+                        rv[u][0] = rx; rv[u][1] = ry; rv[u][2] = rz;
+                        tv[u] = __ldg(Tb.smooth4 + (size_t)tp * Tb.n_bins + i1);
+                        prv[u] = pr;
+                    }
+                }
             }
-            e += ep;
-            atomicAdd(frc + 3 * a, -fx); atomicAdd(frc + 3 * a + 1, -fy); atomicAdd(frc + 3 * a + 2, -fz);
-            atomicAdd(frc + 3 * b, fx); atomicAdd(frc + 3 * b + 1, fy); atomicAdd(frc + 3 * b + 2, fz);
+        }
+#pragma unroll
+        for (int u = 0; u < kPairBatch; ++u) {
+            float fx = 0, fy = 0, fz = 0;
+            const bool live = prv[u] != kPairPad;
+            if (live) {
+                const float4 t = tv[u];
+                const float rem = remv[u];
+                float ep = t.x + rem * (t.z - t.x);
+                float dor = t.y + rem * (t.w - t.y);
+                fx = dor * rv[u][0]; fy = dor * rv[u][1]; fz = dor * rv[u][2];
+                if (ep > 0 && v_intra < 0.1f * kMaxFl) {
+                    float tmp = (v_intra < kEps) ? 0 : (v_intra / (v_intra + ep));
+                    ep *= tmp;
+                    float t2 = tmp * tmp;
+                    fx *= t2; fy *= t2; fz *= t2;
+                }
+                e += ep;
+            }
+            const int a = prv[u] & 0xFF, b = (prv[u] >> 8) & 0xFF;
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                if (live && (c.lane >> 4) == half) {
+                    frc[3 * a] -= fx; frc[3 * a + 1] -= fy; frc[3 * a + 2] -= fz;
+                    frc[3 * b] += fx; frc[3 * b + 1] += fy; frc[3 * b + 2] += fz;
+                }
+                __syncwarp();
+            }
         }
     }
-    __syncwarp();
     e = warp_sum(e);
     // per-node force and torque of the node's own atoms about its origin
     const float* fr = c.s + c.L.frames;
@@ -381,22 +426,28 @@ __device__ float eval_deriv(const Chain& c, const Maps& M, const Tables& Tb, con
         acc[6 * n + 3] = T0; acc[6 * n + 4] = T1; acc[6 * n + 5] = T2;
     }
     __syncwarp();
-    if (c.lane == 0) {
-        for (int n = c.R - 1; n >= 1; --n) {
-            const float* an = acc + 6 * n;
-            const float* on = fr + 20 * n;
-            g[6 + n - 1] = an[3] * on[16] + an[4] * on[17] + an[5] * on[18];
-            int p = __ldg(&c.nodes[n].parent);
-            float* ap = acc + 6 * p;
-            const float* op = fr + 20 * p;
-            float r0 = on[0] - op[0], r1 = on[1] - op[1], r2 = on[2] - op[2];
-            ap[0] += an[0]; ap[1] += an[1]; ap[2] += an[2];
-            ap[3] += (r1 * an[2] - r2 * an[1]) + an[3];
-            ap[4] += (r2 * an[0] - r0 * an[2]) + an[4];
-            ap[5] += (r0 * an[1] - r1 * an[0]) + an[5];
+    // subtree sums: nodes are in DFS pre-order, so the subtree of n is
+    // [n, subtree_end(n)); torques are moved to the node's origin.
+    for (int n = c.lane; n < c.R; n += 32) {
+        const float* on = fr + 20 * n;
+        const float* an = acc + 6 * n;
+        float F0 = an[0], F1 = an[1], F2 = an[2], T0 = an[3], T1 = an[4], T2 = an[5];
+        const int se = __ldg(&c.nodes[n].subtree_end);
+        for (int m = n + 1; m < se; ++m) {
+            const float* am = acc + 6 * m;
+            const float* om = fr + 20 * m;
+            float r0 = om[0] - on[0], r1 = om[1] - on[1], r2 = om[2] - on[2];
+            F0 += am[0]; F1 += am[1]; F2 += am[2];
+            T0 += (r1 * am[2] - r2 * am[1]) + am[3];
+            T1 += (r2 * am[0] - r0 * am[2]) + am[4];
+            T2 += (r0 * am[1] - r1 * am[0]) + am[5];
         }
-        g[0] = acc[0]; g[1] = acc[1]; g[2] = acc[2];
-        g[3] = acc[3]; g[4] = acc[4]; g[5] = acc[5];
+        if (n == 0) {
+            g[0] = F0; g[1] = F1; g[2] = F2;
+            g[3] = T0; g[4] = T1; g[5] = T2;
+        } else {
+            g[6 + n - 1] = T0 * on[16] + T1 * on[17] + T2 * on[18];
+        }
     }
     __syncwarp();
     return e;
@@ -417,6 +468,7 @@ __device__ void eval_score(const Chain& c, const Maps& M, const Tables& Tb, cons
     }
     for (int k = c.lane; k < c.lig.n_pairs; k += 32) {
         uint32_t pr = __ldg(c.pairs + k);
+        if (pr == kPairPad) continue;
         int a = pr & 0xFF, b = (pr >> 8) & 0xFF, tp = pr >> 16;
         float dx = xyz[3 * a] - xyz[3 * b], dy = xyz[3 * a + 1] - xyz[3 * b + 1],
               dz = xyz[3 * a + 2] - xyz[3 * b + 2];
@@ -461,7 +513,7 @@ __device__ void conf_increment(const Chain& c, const float* x, const float* p, f
 
 // Vina BFGS with Armijo backtracking (bfgs.h:27-146); x and g updated in
 // place, returns the final energy.
-__device__ float bfgs(Chain& c, const Maps& M, const Tables& Tb, float* x, int max_steps,
+__device__ __noinline__ float bfgs(Chain& c, const Maps& M, const Tables& Tb, float* x, int max_steps,
                       float v, int& evals) {
     const int n = c.L.gs - (c.L.gs - 6 - c.T);  // 6 + T
     float* s = c.s;
@@ -647,6 +699,7 @@ __device__ void run_chain(Chain& c, const Maps& M, const Tables& Tb, const Searc
     int steps = c.lig.local_steps;
     if (P.bfgs_cap > 0 && P.bfgs_cap < steps) steps = P.bfgs_cap;
     random_conf(c, rng, box_lo, box_hi, tmp);
+    kinematics(c, tmp);  // coordinates of the start pose (gyration radius of the first mutation)
     copyw(c, best, tmp, cs);
     float tmp_e = kMaxFl, best_e = kMaxFl;
     int evals = 0;
@@ -699,7 +752,7 @@ __device__ __forceinline__ void bind_chain(Chain& c, const Batch& B, const Layou
 
 // Search: plain form (grid covers the chains of `first_lig` .. with a fixed
 // tiling) or persistent form (warps pull (ligand, chain) items from a queue).
-__global__ void __launch_bounds__(128) search_kernel(Batch B, Maps M, Tables Tb, SearchParams P,
+__global__ void __launch_bounds__(128, 6) search_kernel(Batch B, Maps M, Tables Tb, SearchParams P,
                                                      Layout L, const int* order, int n_items,
                                                      int first_item, unsigned int* queue,
                                                      float box_lo0, float box_lo1, float box_lo2,
@@ -951,7 +1004,7 @@ static dev::Maps to_maps(const DeviceMapsView& m) {
 
 static dev::Tables to_tables(const DeviceTablesView& t) {
     dev::Tables T;
-    T.smooth = reinterpret_cast<const float2*>(t.smooth);
+    T.smooth4 = reinterpret_cast<const float4*>(t.smooth);
     T.fast = t.fast;
     T.n_bins = t.n_bins;
     T.factor = t.factor;

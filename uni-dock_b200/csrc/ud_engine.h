@@ -38,14 +38,18 @@ struct LigDesc {
     int pad[3];
 };
 
-struct NodeRec {            // 48 bytes
+struct NodeRec {            // 40 bytes
     float rel_origin[3];
     float rel_axis[3];
-    float origin0[3];      // input-frame origin (root: initial position)
     int parent;
     int depth;
-    int begin_end;         // begin | end << 16
+    int begin_end;         // atom range: begin | end << 16
+    int subtree_end;       // one past the last node of this node's subtree
 };
+
+// Pair records are a | b << 8 | type_pair << 16; this value pads a 32-pair
+// group of the conflict-free pair order and is skipped.
+constexpr uint32_t kPairPad = 0xFFFF0000u;
 
 // Atom record: local xyz and packed fields (node | (map slot + 1) << 8 |
 // heavy << 16 | (xs + 1) << 24).

@@ -14,7 +14,8 @@ from pathlib import Path
 import numpy as np
 
 PKG_ROOT = Path(__file__).resolve().parent.parent      # uni-dock_b200/
-LIB_PATH = PKG_ROOT / "lib" / "libunidock_b200.so"
+# UNIDOCK_B200_LIB selects another build of the same library (e.g. a tuning variant)
+LIB_PATH = Path(os.environ.get("UNIDOCK_B200_LIB", PKG_ROOT / "lib" / "libunidock_b200.so"))
 
 SF_VINA, SF_AD4, SF_VINARDO = 0, 1, 2
 UD_OK = 0
