@@ -1,25 +1,30 @@
 // Docking engine kernels for sm_100a.
 //
-//  * ud_maps_kernel      receptor grid maps (one thread per grid point, all
-//                        requested types at once, receptor atoms of the tile
-//                        staged in shared memory in index order)
-//  * ud_score_kernel     energy + pose gradient at fixed poses (one warp per pose)
-//  * ud_search_kernel    Monte-Carlo + BFGS chains (one warp per chain), plain
-//                        fixed tiling or a persistent queue over (ligand, chain)
+//  * maps_kernel      receptor grid maps (one thread per grid point, all
+//                     requested types at once, receptor atoms of the tile staged
+//                     in shared memory in index order)
+//  * score_kernel     energy + pose gradient at fixed poses (one warp per pose)
+//  * optimize_kernel  BFGS local optimisation from given poses (one warp per pose)
+//  * search_kernel    Monte-Carlo + BFGS chains (one warp per chain), plain fixed
+//                     tiling or a persistent queue over (ligand, chain) items
 //
-// Chain state (conformations, gradients, inverse Hessian, atom coordinates,
-// forces and node frames) lives in shared memory; ligand topology is read
-// through the read-only cache; grid maps and pair tables stay L2-resident.
-// Per-evaluation arithmetic follows the reference's model::eval_deriv
-// (unidock/src/lib/model.cpp:935-962): forward kinematics (tree.h:89-128),
-// trilinear grid energy/gradient with out-of-box penalty (grid.cpp:40-129),
-// lerped pair tables (precalculate.h:48-65), curl (curl.h:28-43) and the
-// force/torque reverse sweep up the torsion tree (tree.h:75-84,164-192).
+// A chain's state (conformations, gradients, inverse Hessian, atom
+// coordinates, forces, node frames) lives in shared memory; ligand topology is
+// read through the read-only cache; grid maps and pair tables stay L2-resident.
+// The search kernel is one flat loop around a single energy evaluation with a
+// warp-uniform state machine for the BFGS line search and the Monte-Carlo
+// steps, so the evaluation code exists once and the chain context stays in
+// registers.  Per-evaluation arithmetic follows the reference's
+// model::eval_deriv (unidock/src/lib/model.cpp:935-962): forward kinematics
+// (tree.h:89-128), trilinear grid energy/gradient with out-of-box penalty
+// (grid.cpp:40-129), lerped pair tables (precalculate.h:48-65), curl
+// (curl.h:28-43) and the force/torque sums up the torsion tree
+// (tree.h:75-84,164-192).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include <cmath>
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 
 #include "ud_engine.h"
@@ -43,7 +48,9 @@ struct Philox {
         k1 = (uint32_t)(seed >> 32);
         c0 = 0; c1 = 0; c2 = stream; c3 = sub;
     }
-    __device__ uint4 next() {
+    // out of line: only lane 0 draws, and inlining 10 rounds at every call
+    // site would grow the hot loop's code footprint
+    __device__ __noinline__ uint4 next() {
         uint32_t x0 = c0, x1 = c1, x2 = c2, x3 = c3, a = k0, b = k1;
 #pragma unroll
         for (int r = 0; r < 10; ++r) {
@@ -61,25 +68,13 @@ struct Philox {
 __device__ __forceinline__ float u01(uint32_t u) { return (u >> 8) * (1.0f / 16777216.0f); }
 
 // ---------------------------------------------------------------- math
+// normalize_angle of unidock/src/lib/common.h:252-270 (values within
+// [-3 pi, 3 pi] take one step; larger ones the ceil formula first).
 __device__ __forceinline__ float normalized_angle(float x) {
-    // normalize_angle of unidock/src/lib/common.h:252-270
-    for (int it = 0; it < 64; ++it) {
-        if (x > 3 * kPi) {
-            float n = (x - kPi) / (2 * kPi);
-            x -= 2 * kPi * ceilf(n);
-        } else if (x < -3 * kPi) {
-            float n = (-x - kPi) / (2 * kPi);
-            x += 2 * kPi * ceilf(n);
-        } else if (x > kPi) {
-            x -= 2 * kPi;
-            break;
-        } else if (x < -kPi) {
-            x += 2 * kPi;
-            break;
-        } else {
-            break;
-        }
-    }
+    if (x > 3 * kPi) x -= 2 * kPi * ceilf((x - kPi) / (2 * kPi));
+    else if (x < -3 * kPi) x += 2 * kPi * ceilf((-x - kPi) / (2 * kPi));
+    if (x > kPi) x -= 2 * kPi;
+    else if (x < -kPi) x += 2 * kPi;
     return x;
 }
 
@@ -94,16 +89,39 @@ __device__ __forceinline__ void qmul(const float* a, const float* b, float* o) {
 __device__ __forceinline__ void qnormalize_approx(float* q) {
     float s = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
     if (fabsf(s - 1) >= 1e-6f) {
-        float a = sqrtf(s);
-        float inv = 1 / a;
+        float inv = rsqrtf(s);
         q[0] *= inv; q[1] *= inv; q[2] *= inv; q[3] *= inv;
     }
+}
+
+// sin and cos of h in [-pi/2, pi/2] by their Taylor series to the x^15 / x^14
+// terms (truncation error below 1e-9 at |h| = pi/2), evaluated with Horner's
+// rule; no range reduction is needed because callers pass half angles of
+// normalised angles.
+__device__ __forceinline__ void sincos_half(float h, float* s, float* c) {
+    const float x2 = h * h;
+    float ps = -1.0f / 1307674368000.0f;              // -1/15!
+    ps = fmaf(ps, x2, 1.0f / 6227020800.0f);          //  1/13!
+    ps = fmaf(ps, x2, -1.0f / 39916800.0f);           // -1/11!
+    ps = fmaf(ps, x2, 1.0f / 362880.0f);              //  1/9!
+    ps = fmaf(ps, x2, -1.0f / 5040.0f);               // -1/7!
+    ps = fmaf(ps, x2, 1.0f / 120.0f);                 //  1/5!
+    ps = fmaf(ps, x2, -1.0f / 6.0f);                  // -1/3!
+    *s = fmaf(ps * x2, h, h);
+    float pc = -1.0f / 87178291200.0f;                // -1/14!
+    pc = fmaf(pc, x2, 1.0f / 479001600.0f);           //  1/12!
+    pc = fmaf(pc, x2, -1.0f / 3628800.0f);            // -1/10!
+    pc = fmaf(pc, x2, 1.0f / 40320.0f);               //  1/8!
+    pc = fmaf(pc, x2, -1.0f / 720.0f);                // -1/6!
+    pc = fmaf(pc, x2, 1.0f / 24.0f);                  //  1/4!
+    pc = fmaf(pc, x2, -0.5f);                         // -1/2!
+    *c = fmaf(pc, x2, 1.0f);
 }
 
 __device__ __forceinline__ void axis_angle_q(const float* axis, float angle, float* q) {
     angle = normalized_angle(angle);
     float s, c;
-    sincosf(angle / 2, &s, &c);
+    sincos_half(0.5f * angle, &s, &c);
     q[0] = c; q[1] = s * axis[0]; q[2] = s * axis[1]; q[3] = s * axis[2];
 }
 
@@ -112,7 +130,8 @@ __device__ __forceinline__ void quaternion_increment(float* q, const float* rot)
     float angle = sqrtf(rot[0] * rot[0] + rot[1] * rot[1] + rot[2] * rot[2]);
     float t[4] = {1, 0, 0, 0};
     if (angle > kEps) {
-        float ax[3] = {rot[0] / angle, rot[1] / angle, rot[2] / angle};
+        const float inv = __frcp_rn(angle);
+        float ax[3] = {rot[0] * inv, rot[1] * inv, rot[2] * inv};
         axis_angle_q(ax, angle, t);
     }
     float o[4];
@@ -144,7 +163,11 @@ __device__ __forceinline__ int tri_j(int k) {  // column of packed index k (i <=
     return j;
 }
 
-// ---------------------------------------------------------------- batch views
+__device__ __forceinline__ int tri(int i, int j) {  // packed upper-triangular index
+    return i <= j ? i + j * (j + 1) / 2 : j + i * (i + 1) / 2;
+}
+
+// ---------------------------------------------------------------- data views
 struct Batch {
     const LigDesc* ligs;
     const AtomRec* atoms;
@@ -152,7 +175,13 @@ struct Batch {
     const uint32_t* pairs;
 };
 
-constexpr int kPairBatch = 4;  // pair groups whose table rows are in flight together
+#ifndef UD_PAIR_BATCH
+#define UD_PAIR_BATCH 1
+#endif
+// pair groups whose table rows are in flight together (larger values unroll
+// more code into the hot loop, which costs more in instruction fetch than the
+// extra loads in flight gain)
+constexpr int kPairBatch = UD_PAIR_BATCH;
 
 struct Tables {
     const float4* smooth4; // [tp][bin] (e, dE/dr / r) of bin and bin + 1
@@ -167,11 +196,11 @@ struct Maps {
     int nx, ny, nz;
     float init[3], factor[3], factor_inv[3], dim_m1[3];
     float slope;
+    float corner2[3];
 };
 
-// Shared-memory layout of one chain (floats).
+// Shared-memory layout of one chain (float offsets).
 struct Layout {
-    int cs, gs;            // conformation / gradient sizes of the largest ligand
     int x, xnew, xorig, tmp, cand, best;
     int g, gnew, gorig, p, y, mhy;
     int h;
@@ -186,8 +215,6 @@ __host__ __device__ inline int pad4(int v) { return (v + 3) & ~3; }
 __host__ inline Layout make_layout(int max_atoms, int max_tors) {
     Layout L;
     int cs = 7 + max_tors, gs = 6 + max_tors, R = max_tors + 1;
-    L.cs = cs;
-    L.gs = gs;
     int o = 0;
     auto take = [&](int n) { int r = o; o += pad4(n); return r; };
     L.x = take(cs); L.xnew = take(cs); L.xorig = take(cs); L.tmp = take(cs); L.cand = take(cs);
@@ -204,28 +231,43 @@ __host__ inline Layout make_layout(int max_atoms, int max_tors) {
     return L;
 }
 
-// Per-warp chain context.
-struct Chain {
-    float* s;              // shared-memory base of this chain
-    Layout L;
-    LigDesc lig;
+// Per-warp context of the ligand being worked on (kept in registers).
+struct Ctx {
+    float* s;              // shared memory of this warp
     const AtomRec* atoms;
     const NodeRec* nodes;
     const uint32_t* pairs;
+    int n_atoms, R, T, n_pairs, max_depth, local_steps;
     int lane;
-    int T;                 // torsions
-    int R;                 // nodes
 };
 
+__device__ __forceinline__ Ctx make_ctx(const Batch& B, int lig, float* s) {
+    Ctx c;
+    const LigDesc* d = B.ligs + lig;
+    c.s = s;
+    c.atoms = B.atoms + __ldg(&d->atom_off);
+    c.nodes = B.nodes + __ldg(&d->node_off);
+    c.pairs = B.pairs + __ldg(&d->pair_off);
+    c.n_atoms = __ldg(&d->n_atoms);
+    c.R = __ldg(&d->n_nodes);
+    c.T = c.R - 1;
+    c.n_pairs = __ldg(&d->n_pairs);
+    c.max_depth = __ldg(&d->max_depth);
+    c.local_steps = __ldg(&d->local_steps);
+    c.lane = threadIdx.x & 31;
+    return c;
+}
+
+// ---------------------------------------------------------------- evaluation
 // Forward kinematics: node frames by tree depth, then atom coordinates.
-// A branch's orientation is the parent's composed with the torsion rotation
+// A branch's orientation is its parent's composed with the torsion rotation
 // about the branch axis; written in the parent's frame that rotation
 // (axis_angle(rel_axis, theta)) does not depend on the parent, so all torsion
 // quaternions are formed in one parallel pass and each tree level only
 // composes q_parent * t (equal to axis_angle(R_parent rel_axis, theta) * q_parent
 // of tree.h:116-128 for unit quaternions).
-__device__ __noinline__ void kinematics(const Chain& c, const float* conf) {
-    float* fr = c.s + c.L.frames;
+__device__ __forceinline__ void kinematics(const Ctx& c, const Layout& L, const float* conf) {
+    float* fr = c.s + L.frames;
     // frame layout (20 floats): origin[0..2] q[3..6] R[7..15] lab axis[16..18];
     // [16..19] hold the local torsion quaternion until the node is composed
     for (int n = 1 + c.lane; n < c.R; n += 32) {
@@ -239,7 +281,7 @@ __device__ __noinline__ void kinematics(const Chain& c, const float* conf) {
         q_to_r3(fr + 3, fr + 7);
     }
     __syncwarp();
-    for (int d = 1; d <= c.lig.max_depth; ++d) {
+    for (int d = 1; d <= c.max_depth; ++d) {
         for (int n = 1 + c.lane; n < c.R; n += 32) {
             const NodeRec* nr = c.nodes + n;
             if (__ldg(&nr->depth) != d) continue;
@@ -262,8 +304,8 @@ __device__ __noinline__ void kinematics(const Chain& c, const float* conf) {
         }
         __syncwarp();
     }
-    float* xyz = c.s + c.L.coords;
-    for (int a = c.lane; a < c.lig.n_atoms; a += 32) {
+    float* xyz = c.s + L.coords;
+    for (int a = c.lane; a < c.n_atoms; a += 32) {
         AtomRec ar = c.atoms[a];
         int n = ar.packed & 0xFF;
         const float* f = fr + 20 * n;
@@ -296,12 +338,12 @@ __device__ __forceinline__ float grid_eval(const Maps& M, int slot, const float*
     const float penalty = M.slope * (miss[0] * M.factor_inv[0] + miss[1] * M.factor_inv[1] +
                                      miss[2] * M.factor_inv[2]);
     const float* g = M.data + (size_t)slot * M.nx * M.ny * M.nz;
-    const size_t sx = 1, sy = M.nx, sz = (size_t)M.nx * M.ny;
-    const size_t base = a[0] + sy * a[1] + sz * a[2];
-    const float f000 = __ldg(g + base), f100 = __ldg(g + base + sx);
-    const float f010 = __ldg(g + base + sy), f110 = __ldg(g + base + sx + sy);
-    const float f001 = __ldg(g + base + sz), f101 = __ldg(g + base + sx + sz);
-    const float f011 = __ldg(g + base + sy + sz), f111 = __ldg(g + base + sx + sy + sz);
+    const int sy = M.nx, sz = M.nx * M.ny;
+    const int base = a[0] + sy * a[1] + sz * a[2];
+    const float f000 = __ldg(g + base), f100 = __ldg(g + base + 1);
+    const float f010 = __ldg(g + base + sy), f110 = __ldg(g + base + 1 + sy);
+    const float f001 = __ldg(g + base + sz), f101 = __ldg(g + base + 1 + sz);
+    const float f011 = __ldg(g + base + sy + sz), f111 = __ldg(g + base + 1 + sy + sz);
     const float x = s[0], y = s[1], z = s[2];
     const float mx = 1 - x, my = 1 - y, mz = 1 - z;
     float f = f000 * mx * my * mz + f100 * x * my * mz + f010 * mx * y * mz + f110 * x * y * mz +
@@ -314,7 +356,7 @@ __device__ __forceinline__ float grid_eval(const Maps& M, int slot, const float*
         float zg = -f000 * mx * my - f100 * x * my - f010 * mx * y - f110 * x * y +
                    f001 * mx * my + f101 * x * my + f011 * mx * y + f111 * x * y;
         if (f > 0 && v < 0.1f * kMaxFl) {  // curl
-            float tmp = (v < kEps) ? 0 : (v / (v + f));
+            float tmp = (v < kEps) ? 0 : __fdividef(v, v + f);
             f *= tmp;
             float t2 = tmp * tmp;
             xg *= t2; yg *= t2; zg *= t2;
@@ -324,7 +366,7 @@ __device__ __forceinline__ float grid_eval(const Maps& M, int slot, const float*
         gz = M.factor[2] * (reg[2] == 0 ? zg : 0.0f) + M.slope * reg[2];
     } else {
         if (f > 0 && v < 0.1f * kMaxFl) {
-            float tmp = (v < kEps) ? 0 : (v / (v + f));
+            float tmp = (v < kEps) ? 0 : __fdividef(v, v + f);
             f *= tmp;
         }
     }
@@ -332,13 +374,14 @@ __device__ __forceinline__ float grid_eval(const Maps& M, int slot, const float*
 }
 
 // Energy and gradient (change layout: position, torque, torsions) of `conf`.
-__device__ __noinline__ float eval_deriv(const Chain& c, const Maps& M, const Tables& Tb, const float* conf,
-                            float* g, float v_intra, float v_inter) {
-    kinematics(c, conf);
-    const float* xyz = c.s + c.L.coords;
-    float* frc = c.s + c.L.forces;
+__device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const Maps& M,
+                                            const Tables& Tb, const float* conf, float* g,
+                                            float v_intra, float v_inter) {
+    kinematics(c, L, conf);
+    const float* xyz = c.s + L.coords;
+    float* frc = c.s + L.forces;
     float e = 0;
-    for (int a = c.lane; a < c.lig.n_atoms; a += 32) {
+    for (int a = c.lane; a < c.n_atoms; a += 32) {
         int packed = __ldg(&c.atoms[a].packed);
         int slot = ((packed >> 8) & 0xFF) - 1;
         float gx = 0, gy = 0, gz = 0;
@@ -349,7 +392,7 @@ __device__ __noinline__ float eval_deriv(const Chain& c, const Maps& M, const Ta
     // Pairs in 32-slot groups whose two half-warps are matchings (no atom twice
     // within a half): table rows of kPairBatch groups are loaded before any is
     // consumed, then each half-warp adds its forces in turn (no atomics).
-    const int n_groups = c.lig.n_pairs >> 5;
+    const int n_groups = c.n_pairs >> 5;
     for (int g0 = 0; g0 < n_groups; g0 += kPairBatch) {
         float4 tv[kPairBatch];
         float rv[kPairBatch][3];
@@ -387,7 +430,7 @@ __device__ __noinline__ float eval_deriv(const Chain& c, const Maps& M, const Ta
                 float dor = t.y + rem * (t.w - t.y);
                 fx = dor * rv[u][0]; fy = dor * rv[u][1]; fz = dor * rv[u][2];
                 if (ep > 0 && v_intra < 0.1f * kMaxFl) {
-                    float tmp = (v_intra < kEps) ? 0 : (v_intra / (v_intra + ep));
+                    float tmp = (v_intra < kEps) ? 0 : __fdividef(v_intra, v_intra + ep);
                     ep *= tmp;
                     float t2 = tmp * tmp;
                     fx *= t2; fy *= t2; fz *= t2;
@@ -407,8 +450,8 @@ __device__ __noinline__ float eval_deriv(const Chain& c, const Maps& M, const Ta
     }
     e = warp_sum(e);
     // per-node force and torque of the node's own atoms about its origin
-    const float* fr = c.s + c.L.frames;
-    float* acc = c.s + c.L.accum;
+    const float* fr = c.s + L.frames;
+    float* acc = c.s + L.accum;
     for (int n = c.lane; n < c.R; n += 32) {
         int be = __ldg(&c.nodes[n].begin_end);
         int b0 = be & 0xFFFF, b1 = be >> 16;
@@ -455,18 +498,19 @@ __device__ __noinline__ float eval_deriv(const Chain& c, const Maps& M, const Ta
 
 // Scoring-path energy (no gradient): grid with curl cap v, intramolecular
 // pairs from the nearest-bin `fast` table (model.cpp:867-886, cache.cpp:84-120).
-__device__ void eval_score(const Chain& c, const Maps& M, const Tables& Tb, const float* conf,
-                           float v, float& e_grid, float& e_intra) {
-    kinematics(c, conf);
-    const float* xyz = c.s + c.L.coords;
+__device__ __forceinline__ void eval_score(const Ctx& c, const Layout& L, const Maps& M,
+                                           const Tables& Tb, const float* conf, float v,
+                                           float& e_grid, float& e_intra) {
+    kinematics(c, L, conf);
+    const float* xyz = c.s + L.coords;
     float eg = 0, ei = 0;
-    for (int a = c.lane; a < c.lig.n_atoms; a += 32) {
+    for (int a = c.lane; a < c.n_atoms; a += 32) {
         int packed = __ldg(&c.atoms[a].packed);
         int slot = ((packed >> 8) & 0xFF) - 1;
         float gx, gy, gz;
         if (slot >= 0) eg += grid_eval(M, slot, xyz + 3 * a, v, gx, gy, gz, false);
     }
-    for (int k = c.lane; k < c.lig.n_pairs; k += 32) {
+    for (int k = c.lane; k < c.n_pairs; k += 32) {
         uint32_t pr = __ldg(c.pairs + k);
         if (pr == kPairPad) continue;
         int a = pr & 0xFF, b = (pr >> 8) & 0xFF, tp = pr >> 16;
@@ -475,7 +519,7 @@ __device__ void eval_score(const Chain& c, const Maps& M, const Tables& Tb, cons
         float r2 = dx * dx + dy * dy + dz * dz;
         if (r2 < Tb.cutoff2) {
             float t = __ldg(Tb.fast + (size_t)tp * Tb.n_bins + (int)(Tb.factor * r2));
-            if (t > 0 && v < 0.1f * kMaxFl) t *= (v < kEps) ? 0 : (v / (v + t));
+            if (t > 0 && v < 0.1f * kMaxFl) t *= (v < kEps) ? 0 : __fdividef(v, v + t);
             ei += t;
         }
     }
@@ -483,20 +527,21 @@ __device__ void eval_score(const Chain& c, const Maps& M, const Tables& Tb, cons
     e_intra = warp_sum(ei);
 }
 
-__device__ __forceinline__ float dotw(const Chain& c, const float* a, const float* b, int n) {
+// ---------------------------------------------------------------- BFGS pieces
+__device__ __forceinline__ float dotw(const Ctx& c, const float* a, const float* b, int n) {
     float s = 0;
     for (int i = c.lane; i < n; i += 32) s += a[i] * b[i];
     return warp_sum(s);
 }
 
-__device__ __forceinline__ void copyw(const Chain& c, float* dst, const float* src, int n) {
+__device__ __forceinline__ void copyw(const Ctx& c, float* dst, const float* src, int n) {
     for (int i = c.lane; i < n; i += 32) dst[i] = src[i];
     __syncwarp();
 }
 
 // x_new = x + alpha * p in conformation space (conf.h:98-104, 146-150).
-__device__ void conf_increment(const Chain& c, const float* x, const float* p, float alpha,
-                               float* out) {
+__device__ __forceinline__ void conf_increment(const Ctx& c, const float* x, const float* p,
+                                               float alpha, float* out) {
     if (c.lane < 3) out[c.lane] = x[c.lane] + alpha * p[c.lane];
     if (c.lane == 3) {
         float rot[3] = {alpha * p[3], alpha * p[4], alpha * p[5]};
@@ -511,89 +556,43 @@ __device__ void conf_increment(const Chain& c, const float* x, const float* p, f
     __syncwarp();
 }
 
-// Vina BFGS with Armijo backtracking (bfgs.h:27-146); x and g updated in
-// place, returns the final energy.
-__device__ __noinline__ float bfgs(Chain& c, const Maps& M, const Tables& Tb, float* x, int max_steps,
-                      float v, int& evals) {
-    const int n = c.L.gs - (c.L.gs - 6 - c.T);  // 6 + T
-    float* s = c.s;
-    float* g = s + c.L.g;
-    float* gnew = s + c.L.gnew;
-    float* gorig = s + c.L.gorig;
-    float* p = s + c.L.p;
-    float* y = s + c.L.y;
-    float* mhy = s + c.L.mhy;
-    float* H = s + c.L.h;
-    float* xnew = s + c.L.xnew;
-    float* xorig = s + c.L.xorig;
-    const int cs = 7 + c.T;
+// out = -H v (packed symmetric inverse Hessian, one row per lane)
+__device__ __forceinline__ void minus_hv(const Ctx& c, const float* H, const float* v, float* out, int n) {
+    for (int i = c.lane; i < n; i += 32) {
+        float sum = 0;
+        const int ri = i * (i + 1) / 2;
+        for (int j = 0; j < i; ++j) sum += H[j + ri] * v[j];
+        for (int j = i; j < n; ++j) sum += H[i + j * (j + 1) / 2] * v[j];
+        out[i] = -sum;
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void h_identity(const Ctx& c, float* H, int n) {
     const int nh = n * (n + 1) / 2;
     for (int k = c.lane; k < nh; k += 32) H[k] = 0;
     __syncwarp();
     for (int i = c.lane; i < n; i += 32) H[i + i * (i + 1) / 2] = 1;
-    float f0 = eval_deriv(c, M, Tb, x, g, v, v);
-    ++evals;
-    const float f_orig = f0;
-    copyw(c, gorig, g, n);
-    copyw(c, xorig, x, cs);
-    for (int step = 0; step < max_steps; ++step) {
-        for (int i = c.lane; i < n; i += 32) {
-            float sum = 0;
-            for (int j = 0; j < n; ++j) sum += H[i < j ? i + j * (j + 1) / 2 : j + i * (i + 1) / 2] * g[j];
-            p[i] = -sum;
-        }
-        __syncwarp();
-        // line search
-        const float pg = dotw(c, p, g, n);
-        float alpha = 1.0f, f1 = 0;
-        for (int trial = 0; trial < 10; ++trial) {
-            conf_increment(c, x, p, alpha, xnew);
-            f1 = eval_deriv(c, M, Tb, xnew, gnew, v, v);
-            ++evals;
-            if (f1 - f0 < 0.0001f * alpha * pg) break;
-            alpha *= 0.5f;
-        }
-        for (int i = c.lane; i < n; i += 32) y[i] = gnew[i] - g[i];
-        __syncwarp();
-        f0 = f1;
-        copyw(c, x, xnew, cs);
-        const float gg = dotw(c, g, g, n);
-        if (!(sqrtf(gg) >= 1e-5f)) break;
-        copyw(c, g, gnew, n);
-        if (step == 0) {
-            float yy = dotw(c, y, y, n);
-            if (fabsf(yy) > kEps) {
-                float yp = dotw(c, y, p, n);
-                for (int i = c.lane; i < n; i += 32) H[i + i * (i + 1) / 2] = alpha * yp / yy;
-                __syncwarp();
-            }
-        }
-        // BFGS update of the inverse Hessian
-        const float yp = dotw(c, y, p, n);
-        if (alpha * yp < kEps) continue;
-        for (int i = c.lane; i < n; i += 32) {
-            float sum = 0;
-            for (int j = 0; j < n; ++j) sum += H[i < j ? i + j * (j + 1) / 2 : j + i * (i + 1) / 2] * y[j];
-            mhy[i] = -sum;
-        }
-        __syncwarp();
-        const float yhy = -dotw(c, y, mhy, n);
-        const float r = 1 / (alpha * yp);
-        for (int k = c.lane; k < nh; k += 32) {
-            int j = tri_j(k), i = k - j * (j + 1) / 2;
-            H[k] += alpha * r * (mhy[i] * p[j] + mhy[j] * p[i]) +
-                    alpha * alpha * (r * r * yhy + r) * p[i] * p[j];
-        }
-        __syncwarp();
-    }
-    if (!(f0 <= f_orig)) {
-        f0 = f_orig;
-        copyw(c, x, xorig, cs);
-        copyw(c, g, gorig, n);
-    }
-    return f0;
+    __syncwarp();
 }
 
+// BFGS update of the inverse Hessian (bfgs.h:40-58)
+__device__ __forceinline__ void h_update(const Ctx& c, float* H, const float* p, const float* y,
+                                         float* mhy, float alpha, int n) {
+    const float yp = dotw(c, y, p, n);
+    if (alpha * yp < kEps) return;
+    minus_hv(c, H, y, mhy, n);
+    const float yhy = -dotw(c, y, mhy, n);
+    const float r = __frcp_rn(alpha * yp);
+    const int nh = n * (n + 1) / 2;
+    for (int k = c.lane; k < nh; k += 32) {
+        int j = tri_j(k), i = k - j * (j + 1) / 2;
+        H[k] += alpha * r * (mhy[i] * p[j] + mhy[j] * p[i]) + alpha * alpha * (r * r * yhy + r) * p[i] * p[j];
+    }
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------- MC pieces
 __device__ void random_inside_sphere(Philox& rng, float* v) {
     for (int it = 0; it < 64; ++it) {
         uint4 u = rng.next();
@@ -609,23 +608,28 @@ __device__ void random_inside_sphere(Philox& rng, float* v) {
 
 // Initial chain conformation: position uniform in the box, orientation a
 // normalised 4-D Gaussian, torsions uniform (conf.h:105-108,173-176; quaternion.cpp:116-126).
-__device__ void random_conf(Chain& c, Philox& rng, const float* lo, const float* hi, float* x) {
+__device__ void random_conf(const Ctx& c, Philox& rng, const Maps& M, float* x) {
     if (c.lane == 0) {
         uint4 u = rng.next();
-        x[0] = lo[0] + (hi[0] - lo[0]) * u01(u.x);
-        x[1] = lo[1] + (hi[1] - lo[1]) * u01(u.y);
-        x[2] = lo[2] + (hi[2] - lo[2]) * u01(u.z);
+        x[0] = M.init[0] + (M.corner2[0] - M.init[0]) * u01(u.x);
+        x[1] = M.init[1] + (M.corner2[1] - M.init[1]) * u01(u.y);
+        x[2] = M.init[2] + (M.corner2[2] - M.init[2]) * u01(u.z);
+        x[3] = 1; x[4] = x[5] = x[6] = 0;
         for (int it = 0; it < 16; ++it) {
             uint4 a = rng.next();
-            float r1 = sqrtf(-2.0f * logf(fmaxf(u01(a.x), 1e-12f))), t1 = 2 * kPi * u01(a.y);
-            float r2 = sqrtf(-2.0f * logf(fmaxf(u01(a.z), 1e-12f))), t2 = 2 * kPi * u01(a.w);
-            float q[4] = {r1 * cosf(t1), r1 * sinf(t1), r2 * cosf(t2), r2 * sinf(t2)};
+            // Box-Muller with angles in [-pi, pi): sin/cos from the half angle
+            float r1 = sqrtf(-2.0f * __logf(fmaxf(u01(a.x), 1e-12f)));
+            float r2 = sqrtf(-2.0f * __logf(fmaxf(u01(a.z), 1e-12f)));
+            float s1, c1, s2, c2;
+            sincos_half(0.5f * (2 * kPi * u01(a.y) - kPi), &s1, &c1);
+            sincos_half(0.5f * (2 * kPi * u01(a.w) - kPi), &s2, &c2);
+            float q[4] = {r1 * (c1 * c1 - s1 * s1), r1 * (2 * s1 * c1), r2 * (c2 * c2 - s2 * s2),
+                          r2 * (2 * s2 * c2)};
             float nrm = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
             if (nrm > kEps) {
                 x[3] = q[0] / nrm; x[4] = q[1] / nrm; x[5] = q[2] / nrm; x[6] = q[3] / nrm;
                 break;
             }
-            x[3] = 1; x[4] = x[5] = x[6] = 0;
         }
         for (int t = 0; t < c.T; t += 4) {
             uint4 a = rng.next();
@@ -636,9 +640,10 @@ __device__ void random_conf(Chain& c, Philox& rng, const float* lo, const float*
     __syncwarp();
 }
 
-// Mutation of one of {position, orientation, one torsion} (mutate.cpp:36-80).
-__device__ void mutate(Chain& c, Philox& rng, float amplitude, float* x) {
-    float* misc = c.s + c.L.misc;
+// Mutation of one of {position, orientation, one torsion} (mutate.cpp:36-80);
+// the gyration radius uses the coordinates of the last evaluation.
+__device__ void mutate(const Ctx& c, const Layout& L, Philox& rng, float amplitude, float* x) {
+    float* misc = c.s + L.misc;
     if (c.lane == 0) {
         uint4 u = rng.next();
         int which = (int)(u.x % (uint32_t)(2 + c.T));
@@ -652,10 +657,10 @@ __device__ void mutate(Chain& c, Philox& rng, float amplitude, float* x) {
     const int which = __float_as_int(misc[0]);
     if (which == 1) {
         // gyration radius of heavy atoms about the root origin (model.cpp:853-865)
-        const float* xyz = c.s + c.L.coords;
-        const float* o = c.s + c.L.frames;
+        const float* xyz = c.s + L.coords;
+        const float* o = c.s + L.frames;
         float acc = 0, cnt = 0;
-        for (int a = c.lane; a < c.lig.n_atoms; a += 32) {
+        for (int a = c.lane; a < c.n_atoms; a += 32) {
             int packed = __ldg(&c.atoms[a].packed);
             if ((packed >> 16) & 1) {
                 float dx = xyz[3 * a] - o[0], dy = xyz[3 * a + 1] - o[1], dz = xyz[3 * a + 2] - o[2];
@@ -684,167 +689,316 @@ __device__ void mutate(Chain& c, Philox& rng, float amplitude, float* x) {
     __syncwarp();
 }
 
-// One Monte-Carlo chain (monte_carlo.cu:237-356 semantics): mutate, local
-// BFGS at the hunt cap, Metropolis at temperature T, refine improving poses
-// at the authentic cap and keep the best.
-__device__ void run_chain(Chain& c, const Maps& M, const Tables& Tb, const SearchParams& P,
-                          const float* box_lo, const float* box_hi, int lig_index, int chain,
-                          float* out_pose, int pose_stride, ChainResult* out_res) {
+// ---------------------------------------------------------------- chain driver
+// States of the per-warp machine.  Everything between two evaluations is
+// warp-uniform control; each pass through the loop performs exactly one
+// evaluation (eval_x, eval_g) unless the chain or the work runs out.
+enum : int {
+    S_FETCH = 0,     // take the next (ligand, chain) item
+    S_MC_STEP,       // mutate and start the search BFGS, or finish the chain
+    S_BFGS_BEGIN,    // identity inverse Hessian, evaluate the start point
+    S_BFGS_INIT,     // consume the start-point evaluation
+    S_BFGS_ITER,     // new search direction, first line-search trial
+    S_LS_DONE,       // consume a line-search evaluation
+    S_BFGS_END,      // restore if no improvement, hand the energy back
+    S_AFTER_SEARCH,  // Metropolis test of a locally optimised candidate
+    S_AFTER_REFINE,  // record the refined pose
+    S_DONE,          // write the chain's result
+    S_EXIT
+};
+
+struct Machine {
+    // chain
+    int item, lig, chain, step, evals, steps_cap;
+    float tmp_e, best_e;
+    // BFGS
+    int mode;          // 0 candidate search, 1 refinement, 2 standalone optimisation
+    int bx_off;        // shared-memory offset of the conformation being optimised
+    float v;
+    int iter, trial;
+    float alpha, f0, f_orig, pg, last_e;
+};
+
+// The MC chain of monte_carlo.cu:237-356 (mutate, BFGS at the hunt cap,
+// Metropolis at temperature T, refine improvements at the authentic cap, keep
+// the best) with the line search and BFGS iterations of bfgs.h:63-146.
+template <bool kSearch>
+__device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const Tables& Tb,
+                                            const SearchParams& P, const Layout& L, float* sw,
+                                            const int* order, int n_items, int first_item,
+                                            unsigned int* queue, float* poses, int pose_stride,
+                                            ChainResult* results, const int* opt_lig, int opt_steps,
+                                            float opt_v, float* opt_e, int* opt_evals) {
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    Machine m;
+    Ctx c;
     Philox rng;
-    rng.init(P.seed, (uint32_t)lig_index, (uint32_t)chain);
-    float* tmp = c.s + c.L.tmp;
-    float* cand = c.s + c.L.cand;
-    float* best = c.s + c.L.best;
-    const int cs = 7 + c.T;
-    int steps = c.lig.local_steps;
-    if (P.bfgs_cap > 0 && P.bfgs_cap < steps) steps = P.bfgs_cap;
-    random_conf(c, rng, box_lo, box_hi, tmp);
-    kinematics(c, tmp);  // coordinates of the start pose (gyration radius of the first mutation)
-    copyw(c, best, tmp, cs);
-    float tmp_e = kMaxFl, best_e = kMaxFl;
-    int evals = 0;
-    for (int step = 0; step < P.global_steps; ++step) {
-        copyw(c, cand, tmp, cs);
-        mutate(c, rng, P.mutation_amplitude, cand);
-        float cand_e = bfgs(c, M, Tb, cand, steps, P.hunt_cap, evals);
-        int accept = 0;
-        if (c.lane == 0) {
-            uint4 u = rng.next();
-            accept = (step == 0) || (cand_e < tmp_e) ||
-                     (u01(u.x) < expf((tmp_e - cand_e) / P.temperature));
-        }
-        accept = __shfl_sync(kFull, accept, 0);
-        if (accept) {
-            copyw(c, tmp, cand, cs);
-            tmp_e = cand_e;
-            if (tmp_e < best_e) {
-                tmp_e = bfgs(c, M, Tb, tmp, steps, P.authentic_v, evals);
-                if (tmp_e < best_e) {
-                    copyw(c, best, tmp, cs);
-                    best_e = tmp_e;
+    int st = S_FETCH;
+    m.item = -1;
+    m.evals = 0;
+    bool first = true;
+    for (;;) {
+        const float* eval_x = nullptr;
+        float* eval_g = nullptr;
+        // ---- warp-uniform control until the next evaluation is needed
+        while (eval_x == nullptr) {
+            if (st == S_FETCH) {
+                int it;
+                if (!kSearch) {
+                    it = first ? blockIdx.x * (blockDim.x >> 5) + warp : n_items;
+                } else if (P.persistent) {
+                    unsigned int v = 0;
+                    if (lane == 0) v = atomicAdd(queue, 1u);
+                    it = (int)__shfl_sync(kFull, v, 0);
+                } else {
+                    it = first ? first_item + blockIdx.x * (blockDim.x >> 5) + warp : n_items + first_item;
+                    if (it >= first_item + n_items) it = -1;
+                    else it -= first_item;
                 }
+                first = false;
+                if (it < 0 || it >= n_items) {
+                    st = S_EXIT;
+                    break;
+                }
+                m.item = it;
+                if (kSearch) {
+                    const int gi = P.persistent ? it : it + first_item;
+                    m.lig = order[gi / P.exhaustiveness];
+                    m.chain = gi % P.exhaustiveness;
+                    c = make_ctx(B, m.lig, sw);
+                    rng.init(P.seed, (uint32_t)m.lig, (uint32_t)m.chain);
+                    m.steps_cap = c.local_steps;
+                    if (P.bfgs_cap > 0 && P.bfgs_cap < m.steps_cap) m.steps_cap = P.bfgs_cap;
+                    float* tmp = c.s + L.tmp;
+                    random_conf(c, rng, M, tmp);
+                    copyw(c, c.s + L.best, tmp, 7 + c.T);
+                    m.tmp_e = kMaxFl;
+                    m.best_e = kMaxFl;
+                    m.step = 0;
+                    m.evals = 0;
+                    // one evaluation of the start pose (result unused) leaves its
+                    // coordinates for the first mutation's gyration radius
+                    m.v = P.hunt_cap;
+                    eval_x = tmp;
+                    eval_g = c.s + L.gnew;
+                    st = S_MC_STEP;
+                } else {
+                    m.lig = opt_lig[it];
+                    c = make_ctx(B, m.lig, sw);
+                    float* x = c.s + L.x;
+                    for (int i = lane; i < 7 + c.T; i += 32) x[i] = poses[(size_t)it * pose_stride + i];
+                    __syncwarp();
+                    m.steps_cap = opt_steps > 0 ? opt_steps : c.local_steps;
+                    m.mode = 2;
+                    m.bx_off = L.x;
+                    m.v = opt_v;
+                    m.evals = 0;
+                    st = S_BFGS_BEGIN;
+                }
+            } else if (st == S_MC_STEP) {
+                if (m.step >= P.global_steps) {
+                    st = S_DONE;
+                    continue;
+                }
+                float* cand = c.s + L.cand;
+                copyw(c, cand, c.s + L.tmp, 7 + c.T);
+                mutate(c, L, rng, P.mutation_amplitude, cand);
+                m.mode = 0;
+                m.bx_off = L.cand;
+                m.v = P.hunt_cap;
+                st = S_BFGS_BEGIN;
+            } else if (st == S_BFGS_BEGIN) {
+                h_identity(c, c.s + L.h, 6 + c.T);
+                eval_x = c.s + m.bx_off;
+                eval_g = c.s + L.g;
+                st = S_BFGS_INIT;
+            } else if (st == S_BFGS_INIT) {
+                m.f0 = m.last_e;
+                m.f_orig = m.last_e;
+                copyw(c, c.s + L.gorig, c.s + L.g, 6 + c.T);
+                copyw(c, c.s + L.xorig, c.s + m.bx_off, 7 + c.T);
+                m.iter = 0;
+                st = S_BFGS_ITER;
+            } else if (st == S_BFGS_ITER) {
+                if (m.iter >= m.steps_cap) {
+                    st = S_BFGS_END;
+                    continue;
+                }
+                const int n = 6 + c.T;
+                float* p = c.s + L.p;
+                minus_hv(c, c.s + L.h, c.s + L.g, p, n);
+                m.pg = dotw(c, p, c.s + L.g, n);
+                m.alpha = 1.0f;
+                m.trial = 0;
+                conf_increment(c, c.s + m.bx_off, p, m.alpha, c.s + L.xnew);
+                eval_x = c.s + L.xnew;
+                eval_g = c.s + L.gnew;
+                st = S_LS_DONE;
+            } else if (st == S_LS_DONE) {
+                const float f1 = m.last_e;
+                bool accept = (f1 - m.f0 < 0.0001f * m.alpha * m.pg);
+                if (!accept) {
+                    m.alpha *= 0.5f;
+                    if (++m.trial < 10) {
+                        conf_increment(c, c.s + m.bx_off, c.s + L.p, m.alpha, c.s + L.xnew);
+                        eval_x = c.s + L.xnew;
+                        eval_g = c.s + L.gnew;
+                        continue;
+                    }
+                }
+                // line search done (bfgs.h:120-141)
+                const int n = 6 + c.T;
+                float* g = c.s + L.g;
+                float* gnew = c.s + L.gnew;
+                float* y = c.s + L.y;
+                for (int i = lane; i < n; i += 32) y[i] = gnew[i] - g[i];
+                __syncwarp();
+                m.f0 = f1;
+                copyw(c, c.s + m.bx_off, c.s + L.xnew, 7 + c.T);
+                const float gg = dotw(c, g, g, n);
+                if (!(sqrtf(gg) >= 1e-5f)) {
+                    st = S_BFGS_END;
+                    continue;
+                }
+                copyw(c, g, gnew, n);
+                float* H = c.s + L.h;
+                float* p = c.s + L.p;
+                if (m.iter == 0) {
+                    float yy = dotw(c, y, y, n);
+                    if (fabsf(yy) > kEps) {
+                        float yp = dotw(c, y, p, n);
+                        const float d = __fdividef(m.alpha * yp, yy);
+                        for (int i = lane; i < n; i += 32) H[i + i * (i + 1) / 2] = d;
+                        __syncwarp();
+                    }
+                }
+                h_update(c, H, p, y, c.s + L.mhy, m.alpha, n);
+                ++m.iter;
+                st = S_BFGS_ITER;
+            } else if (st == S_BFGS_END) {
+                if (!(m.f0 <= m.f_orig)) {
+                    m.f0 = m.f_orig;
+                    copyw(c, c.s + m.bx_off, c.s + L.xorig, 7 + c.T);
+                    copyw(c, c.s + L.g, c.s + L.gorig, 6 + c.T);
+                }
+                st = (m.mode == 0) ? S_AFTER_SEARCH : (m.mode == 1 ? S_AFTER_REFINE : S_DONE);
+            } else if (st == S_AFTER_SEARCH) {
+                const float cand_e = m.f0;
+                int accept = 0;
+                if (lane == 0) {
+                    uint4 u = rng.next();
+                    accept = (m.step == 0) || (cand_e < m.tmp_e) ||
+                             (u01(u.x) < __expf(__fdividef(m.tmp_e - cand_e, P.temperature)));
+                }
+                accept = __shfl_sync(kFull, accept, 0);
+                if (accept) {
+                    copyw(c, c.s + L.tmp, c.s + L.cand, 7 + c.T);
+                    m.tmp_e = cand_e;
+                    if (m.tmp_e < m.best_e) {
+                        m.mode = 1;
+                        m.bx_off = L.tmp;
+                        m.v = P.authentic_v;
+                        st = S_BFGS_BEGIN;
+                        continue;
+                    }
+                }
+                ++m.step;
+                st = S_MC_STEP;
+            } else if (st == S_AFTER_REFINE) {
+                m.tmp_e = m.f0;
+                if (m.tmp_e < m.best_e) {
+                    copyw(c, c.s + L.best, c.s + L.tmp, 7 + c.T);
+                    m.best_e = m.tmp_e;
+                }
+                ++m.step;
+                st = S_MC_STEP;
+            } else if (st == S_DONE) {
+                if (kSearch) {
+                    const int slot = m.lig * P.exhaustiveness + m.chain;
+                    const float* best = c.s + L.best;
+                    for (int i = lane; i < 7 + c.T; i += 32) poses[(size_t)slot * pose_stride + i] = best[i];
+                    if (lane == 0) {
+                        results[slot].e = m.best_e;
+                        results[slot].evals = m.evals;
+                        results[slot].ligand = m.lig;
+                        results[slot].chain = m.chain;
+                    }
+                } else {
+                    const float* x = c.s + L.x;
+                    for (int i = lane; i < 7 + c.T; i += 32) poses[(size_t)m.item * pose_stride + i] = x[i];
+                    if (lane == 0) {
+                        opt_e[m.item] = m.f0;
+                        if (opt_evals) opt_evals[m.item] = m.evals;
+                    }
+                }
+                __syncwarp();
+                st = S_FETCH;
+            } else {  // S_EXIT
+                break;
             }
         }
+        if (st == S_EXIT) return;
+        // ---- the single evaluation site
+        m.last_e = eval_deriv(c, L, M, Tb, eval_x, eval_g, m.v, m.v);
+        ++m.evals;
     }
-    for (int i = c.lane; i < cs; i += 32) out_pose[i] = best[i];
-    if (c.lane == 0) {
-        out_res->e = best_e;
-        out_res->evals = evals;
-        out_res->ligand = lig_index;
-        out_res->chain = chain;
-    }
-}
-
-__device__ __forceinline__ void bind_chain(Chain& c, const Batch& B, const Layout& L, int lig,
-                                           float* smem_warp) {
-    c.s = smem_warp;
-    c.L = L;
-    c.lig = B.ligs[lig];
-    c.atoms = B.atoms + c.lig.atom_off;
-    c.nodes = B.nodes + c.lig.node_off;
-    c.pairs = B.pairs + c.lig.pair_off;
-    c.T = c.lig.n_nodes - 1;
-    c.R = c.lig.n_nodes;
-    c.lane = threadIdx.x & 31;
 }
 
 // ---------------------------------------------------------------- kernels
-
-// Search: plain form (grid covers the chains of `first_lig` .. with a fixed
-// tiling) or persistent form (warps pull (ligand, chain) items from a queue).
-__global__ void __launch_bounds__(128, 6) search_kernel(Batch B, Maps M, Tables Tb, SearchParams P,
-                                                     Layout L, const int* order, int n_items,
-                                                     int first_item, unsigned int* queue,
-                                                     float box_lo0, float box_lo1, float box_lo2,
-                                                     float box_hi0, float box_hi1, float box_hi2,
-                                                     float* poses, int pose_stride,
-                                                     ChainResult* results) {
+#ifndef UD_SEARCH_MIN_BLOCKS
+#define UD_SEARCH_MIN_BLOCKS 8
+#endif
+__global__ void __launch_bounds__(128, UD_SEARCH_MIN_BLOCKS) search_kernel(
+    const __grid_constant__ Batch B, const __grid_constant__ Maps M, const __grid_constant__ Tables Tb,
+    const __grid_constant__ SearchParams P, const __grid_constant__ Layout L, const int* order, int n_items,
+    int first_item, unsigned int* queue, float* poses, int pose_stride, ChainResult* results) {
     extern __shared__ float smem[];
-    const int warp = threadIdx.x >> 5;
-    float* sw = smem + (size_t)warp * L.total;
-    const float lo[3] = {box_lo0, box_lo1, box_lo2}, hi[3] = {box_hi0, box_hi1, box_hi2};
-    const int lane = threadIdx.x & 31;
-    int item;
-    if (!P.persistent) {
-        item = first_item + blockIdx.x * (blockDim.x >> 5) + warp;
-        if (item >= first_item + n_items) return;
-    }
-    for (;;) {
-        if (P.persistent) {
-            unsigned int it = 0;
-            if (lane == 0) it = atomicAdd(queue, 1u);
-            it = __shfl_sync(kFull, it, 0);
-            if ((int)it >= n_items) return;
-            item = (int)it;
-        }
-        const int lig = order[item / P.exhaustiveness];
-        const int chain = item % P.exhaustiveness;
-        const int slot = lig * P.exhaustiveness + chain;
-        Chain c;
-        bind_chain(c, B, L, lig, sw);
-        run_chain(c, M, Tb, P, lo, hi, lig, chain, poses + (size_t)slot * pose_stride, pose_stride,
-                  results + slot);
-        if (!P.persistent) return;
-    }
+    float* sw = smem + (size_t)(threadIdx.x >> 5) * L.total;
+    run_machine<true>(B, M, Tb, P, L, sw, order, n_items, first_item, queue, poses, pose_stride, results,
+                      nullptr, 0, 0.f, nullptr, nullptr);
+}
+
+// Local optimisation from given poses (quasi_newton, quasi_newton.cpp:42-53):
+// one warp per pose, BFGS at curl cap v; poses updated in place.
+__global__ void __launch_bounds__(128) optimize_kernel(
+    const __grid_constant__ Batch B, const __grid_constant__ Maps M, const __grid_constant__ Tables Tb,
+    const __grid_constant__ SearchParams P, const __grid_constant__ Layout L, const int* pose_lig,
+    float* poses, int pose_stride, int n_poses, int max_steps, float v, float* e_out, int* evals_out) {
+    extern __shared__ float smem[];
+    float* sw = smem + (size_t)(threadIdx.x >> 5) * L.total;
+    run_machine<false>(B, M, Tb, P, L, sw, nullptr, n_poses, 0, nullptr, poses, pose_stride, nullptr,
+                       pose_lig, max_steps, v, e_out, evals_out);
 }
 
 // Fixed poses: energy (search form, caps v_intra / v_inter) and gradient per pose.
-__global__ void __launch_bounds__(128) score_kernel(Batch B, Maps M, Tables Tb, Layout L,
-                                                    const int* pose_lig, const float* poses,
-                                                    int pose_stride, int n_poses, float v_intra,
-                                                    float v_inter, float* e_out, float* g_out,
-                                                    int g_stride, float* score_out) {
+__global__ void __launch_bounds__(128) score_kernel(
+    const __grid_constant__ Batch B, const __grid_constant__ Maps M, const __grid_constant__ Tables Tb,
+    const __grid_constant__ Layout L, const int* pose_lig, const float* poses, int pose_stride, int n_poses,
+    float v_intra, float v_inter, float* e_out, float* g_out, int g_stride, float* score_out) {
     extern __shared__ float smem[];
     const int warp = threadIdx.x >> 5;
     const int pose = blockIdx.x * (blockDim.x >> 5) + warp;
     if (pose >= n_poses) return;
     float* sw = smem + (size_t)warp * L.total;
-    Chain c;
-    bind_chain(c, B, L, pose_lig[pose], sw);
+    const Ctx c = make_ctx(B, pose_lig[pose], sw);
     float* x = sw + L.x;
     const int cs = 7 + c.T;
     for (int i = c.lane; i < cs; i += 32) x[i] = poses[(size_t)pose * pose_stride + i];
     __syncwarp();
     if (g_out) {
         float* g = sw + L.g;
-        float e = eval_deriv(c, M, Tb, x, g, v_intra, v_inter);
+        float e = eval_deriv(c, L, M, Tb, x, g, v_intra, v_inter);
         for (int i = c.lane; i < 6 + c.T; i += 32) g_out[(size_t)pose * g_stride + i] = g[i];
         if (c.lane == 0) e_out[pose] = e;
     }
     if (score_out) {
         float eg, ei;
-        eval_score(c, M, Tb, x, v_inter, eg, ei);
+        eval_score(c, L, M, Tb, x, v_inter, eg, ei);
         if (c.lane == 0) {
             score_out[2 * pose] = eg;
             score_out[2 * pose + 1] = ei;
         }
-    }
-}
-
-// Local optimisation from given poses (quasi_newton, quasi_newton.cpp:42-53):
-// one warp per pose, BFGS at curl cap v; poses updated in place.
-__global__ void __launch_bounds__(128) optimize_kernel(Batch B, Maps M, Tables Tb, Layout L,
-                                                       const int* pose_lig, float* poses,
-                                                       int pose_stride, int n_poses, int max_steps,
-                                                       float v, float* e_out, int* evals_out) {
-    extern __shared__ float smem[];
-    const int warp = threadIdx.x >> 5;
-    const int pose = blockIdx.x * (blockDim.x >> 5) + warp;
-    if (pose >= n_poses) return;
-    float* sw = smem + (size_t)warp * L.total;
-    Chain c;
-    bind_chain(c, B, L, pose_lig[pose], sw);
-    float* x = sw + L.x;
-    const int cs = 7 + c.T;
-    for (int i = c.lane; i < cs; i += 32) x[i] = poses[(size_t)pose * pose_stride + i];
-    __syncwarp();
-    int evals = 0;
-    const int steps = max_steps > 0 ? max_steps : c.lig.local_steps;
-    float e = bfgs(c, M, Tb, x, steps, v, evals);
-    for (int i = c.lane; i < cs; i += 32) poses[(size_t)pose * pose_stride + i] = x[i];
-    if (c.lane == 0) {
-        e_out[pose] = e;
-        if (evals_out) evals_out[pose] = evals;
     }
 }
 
@@ -873,16 +1027,14 @@ __global__ void fp32_peak_kernel(float* out, int iters) {
 constexpr int kMapTX = 8, kMapTY = 4, kMapTZ = 4;
 constexpr int kMapThreads = kMapTX * kMapTY * kMapTZ;
 constexpr int kMaxSlots = 36;
-constexpr int kMapStage = 1024;
 
 __global__ void __launch_bounds__(kMapThreads) maps_kernel(
     const float4* __restrict__ rec, int n_rec, const float* __restrict__ fastT, int n_bins,
     int n_slots_pad, int n_slots, float factor, float cutoff2, int nx, int ny, int nz,
     float init0, float init1, float init2, float finv0, float finv1, float finv2,
     float* __restrict__ out) {
-    __shared__ float4 stage[kMapStage];
+    __shared__ float4 stage[kMapThreads];
     __shared__ int warp_cnt[kMapThreads / 32];
-    __shared__ int total;
     const int tx = threadIdx.x % kMapTX, ty = (threadIdx.x / kMapTX) % kMapTY,
               tz = threadIdx.x / (kMapTX * kMapTY);
     const int gx0 = blockIdx.x * kMapTX, gy0 = blockIdx.y * kMapTY, gz0 = blockIdx.z * kMapTZ;
@@ -907,23 +1059,23 @@ __global__ void __launch_bounds__(kMapThreads) maps_kernel(
         if (i < n_rec) {
             a = rec[i];
             float d2 = 0;
-            float c[3] = {a.x, a.y, a.z};
+            float cc[3] = {a.x, a.y, a.z};
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                float d = fmaxf(fmaxf(lo[k] - c[k], c[k] - hi[k]), 0.0f);
+                float d = fmaxf(fmaxf(lo[k] - cc[k], cc[k] - hi[k]), 0.0f);
                 d2 += d * d;
             }
             take = d2 <= reach2;
         }
-        unsigned m = __ballot_sync(kFull, take);
-        if (lane == 0) warp_cnt[wid] = __popc(m);
+        unsigned msk = __ballot_sync(kFull, take);
+        if (lane == 0) warp_cnt[wid] = __popc(msk);
         __syncthreads();
         int off = 0, tot = 0;
         for (int w = 0; w < kMapThreads / 32; ++w) {
             if (w < wid) off += warp_cnt[w];
             tot += warp_cnt[w];
         }
-        if (take) stage[off + __popc(m & ((1u << lane) - 1))] = a;
+        if (take) stage[off + __popc(msk & ((1u << lane) - 1))] = a;
         __syncthreads();
         if (x < nx && y < ny && z < nz) {
             for (int k = 0; k < tot; ++k) {
@@ -949,7 +1101,6 @@ __global__ void __launch_bounds__(kMapThreads) maps_kernel(
             }
         }
         __syncthreads();
-        (void)total;
     }
     if (x < nx && y < ny && z < nz) {
         const size_t plane = (size_t)nx * ny * nz;
@@ -979,7 +1130,7 @@ struct DeviceMapsView {
 };
 
 struct DeviceTablesView {
-    const float* smooth;   // float2 per bin
+    const float* smooth;   // float4 per bin
     const float* fast;
     int n_bins;
     float factor;
@@ -997,6 +1148,7 @@ static dev::Maps to_maps(const DeviceMapsView& m) {
         M.factor[i] = m.desc.factor[i];
         M.factor_inv[i] = m.desc.factor_inv[i];
         M.dim_m1[i] = m.desc.dim_m1[i];
+        M.corner2[i] = m.desc.corner2[i];
     }
     M.slope = m.desc.slope;
     return M;
@@ -1038,6 +1190,10 @@ cudaError_t launch_maps(const float* rec_xyzt, int n_rec, const float* fastT, in
     return cudaGetLastError();
 }
 
+static cudaError_t smem_attr(const void* fn, size_t smem) {
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
 cudaError_t launch_score(const DeviceBatchView& b, const DeviceMapsView& m,
                          const DeviceTablesView& t, const int* pose_lig, const float* poses,
                          int pose_stride, int n_poses, float v_intra, float v_inter, float* e_out,
@@ -1045,11 +1201,8 @@ cudaError_t launch_score(const DeviceBatchView& b, const DeviceMapsView& m,
     dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
     const int warps = 4;
     size_t smem = (size_t)warps * L.total * sizeof(float);
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(dev::score_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-    }
+    cudaError_t e = smem_attr((const void*)dev::score_kernel, smem);
+    if (e != cudaSuccess) return e;
     dim3 grid((n_poses + warps - 1) / warps);
     dev::score_kernel<<<grid, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t), L,
                                                           pose_lig, poses, pose_stride, n_poses,
@@ -1064,19 +1217,16 @@ cudaError_t launch_search(const DeviceBatchView& b, const DeviceMapsView& m,
                           int pose_stride, ChainResult* results, int grid_blocks,
                           cudaStream_t stream) {
     dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
-    const int warps = P.chains_per_block > 0 ? P.chains_per_block : 4;
+    const int warps = 4;
     size_t smem = (size_t)warps * L.total * sizeof(float);
-    cudaError_t e = cudaFuncSetAttribute(dev::search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = smem_attr((const void*)dev::search_kernel, smem);
     if (e != cudaSuccess) return e;
     dim3 grid;
     if (P.persistent) grid = dim3(grid_blocks);
     else grid = dim3((n_items + warps - 1) / warps);
-    const float* lo = m.desc.init;
-    const float* hi = m.desc.corner2;
-    dev::search_kernel<<<grid, warps * 32, smem, stream>>>(
-        to_batch(b), to_maps(m), to_tables(t), P, L, order, n_items, first_item, queue, lo[0], lo[1],
-        lo[2], hi[0], hi[1], hi[2], poses, pose_stride, results);
+    dev::search_kernel<<<grid, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t), P, L,
+                                                           order, n_items, first_item, queue, poses,
+                                                           pose_stride, results);
     return cudaGetLastError();
 }
 
@@ -1087,14 +1237,13 @@ cudaError_t launch_optimize(const DeviceBatchView& b, const DeviceMapsView& m,
     dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
     const int warps = 4;
     size_t smem = (size_t)warps * L.total * sizeof(float);
-    cudaError_t e = cudaFuncSetAttribute(dev::optimize_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = smem_attr((const void*)dev::optimize_kernel, smem);
     if (e != cudaSuccess) return e;
+    SearchParams P{};
     dim3 grid((n_poses + warps - 1) / warps);
-    dev::optimize_kernel<<<grid, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t),
-                                                             L, pose_lig, poses, pose_stride,
-                                                             n_poses, max_steps, v, e_out,
-                                                             evals_out);
+    dev::optimize_kernel<<<grid, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t), P, L,
+                                                             pose_lig, poses, pose_stride, n_poses,
+                                                             max_steps, v, e_out, evals_out);
     return cudaGetLastError();
 }
 
@@ -1130,7 +1279,7 @@ float measure_fp32_peak_tflops() {
 int search_blocks_per_sm(const DeviceBatchView& b, int warps) {
     dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
     size_t smem = (size_t)warps * L.total * sizeof(float);
-    cudaFuncSetAttribute(dev::search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    smem_attr((const void*)dev::search_kernel, smem);
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, dev::search_kernel, warps * 32, smem) !=
         cudaSuccess)
