@@ -27,6 +27,7 @@ struct DeviceBatchView {
     const AtomRec* atoms;
     const NodeRec* nodes;
     const uint32_t* pairs;
+    const uint32_t* grid_list;
     int max_atoms, max_torsions;
 };
 struct DeviceMapsView {
@@ -145,6 +146,7 @@ struct ud_batch_s {
     DevBuf<AtomRec> d_atoms;
     DevBuf<NodeRec> d_nodes;
     DevBuf<uint32_t> d_pairs;
+    DevBuf<uint32_t> d_grid;
     int max_atoms = 0, max_tors = 0;
     // search state
     DevBuf<int> d_order;
@@ -172,7 +174,7 @@ struct ud_batch_s {
         if (ev1) cudaEventDestroy(ev1);
     }
     DeviceBatchView view() const {
-        return DeviceBatchView{d_desc.p, d_atoms.p, d_nodes.p, d_pairs.p, max_atoms, max_tors};
+        return DeviceBatchView{d_desc.p, d_atoms.p, d_nodes.p, d_pairs.p, d_grid.p, max_atoms, max_tors};
     }
 };
 
@@ -485,6 +487,7 @@ extern "C" int ud_batch_create(ud_maps maps, const ud_ligand* ligs, int n, void*
         std::vector<AtomRec> atoms;
         std::vector<NodeRec> nodes;
         std::vector<uint32_t> pairs;
+        std::vector<uint32_t> grid_list;
         for (int i = 0; i < n; ++i) {
             if (!ligs[i]) throw Error(UD_ERR_ARG, "null ligand in batch");
             const Ligand& L = ligs[i]->lig;
@@ -518,10 +521,12 @@ extern "C" int ud_batch_create(ud_maps maps, const ud_ligand* ligs, int n, void*
                 }
                 r.parent = nd.parent < 0 ? 0 : nd.parent;
                 r.depth = depth[k];
-                r.begin_end = nd.begin | (nd.end << 16);
+                // a subtree's atoms are contiguous in DFS order: [own begin, last descendant's end)
+                r.atoms = nd.begin | (L.nodes[subtree_end[k] - 1].end << 16);
                 r.subtree_end = subtree_end[k];
                 nodes.push_back(r);
             }
+            d.grid_off = (int)grid_list.size();
             for (const Atom& a : L.atoms) {
                 AtomRec r;
                 r.x = a.local[0];
@@ -534,8 +539,10 @@ extern "C" int ud_batch_create(ud_maps maps, const ud_ligand* ligs, int n, void*
                 int heavy = (a.el != EL_H) ? 1 : 0;
                 int xsp = (a.xs < XS_SIZE) ? a.xs + 1 : 0;
                 r.packed = a.node | ((slot + 1) << 8) | (heavy << 16) | (xsp << 24);
+                if (slot >= 0) grid_list.push_back((uint32_t)(atoms.size() - d.atom_off) | ((uint32_t)slot << 8));
                 atoms.push_back(r);
             }
+            d.n_grid = (int)grid_list.size() - d.grid_off;
             std::vector<uint32_t> ordered = pair_groups(L);
             pairs.insert(pairs.end(), ordered.begin(), ordered.end());
             d.n_pairs = (int)ordered.size();
@@ -547,6 +554,7 @@ extern "C" int ud_batch_create(ud_maps maps, const ud_ligand* ligs, int n, void*
         b->d_atoms.upload(atoms.data(), atoms.size(), s);
         b->d_nodes.upload(nodes.data(), nodes.size(), s);
         b->d_pairs.upload(pairs.data(), pairs.size(), s);
+        b->d_grid.upload(grid_list.data(), grid_list.size(), s);
         cuda_check(cudaStreamSynchronize(s), "batch upload");
         *out = b.release();
     });

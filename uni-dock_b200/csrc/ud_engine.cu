@@ -156,23 +156,13 @@ __device__ __forceinline__ float warp_sum(float v) {
     return v;
 }
 
-__device__ __forceinline__ int tri_j(int k) {  // column of packed index k (i <= j)
-    int j = (int)((sqrtf(8.0f * k + 1.0f) - 1.0f) * 0.5f);
-    while (j * (j + 1) / 2 > k) --j;
-    while ((j + 1) * (j + 2) / 2 <= k) ++j;
-    return j;
-}
-
-__device__ __forceinline__ int tri(int i, int j) {  // packed upper-triangular index
-    return i <= j ? i + j * (j + 1) / 2 : j + i * (i + 1) / 2;
-}
-
 // ---------------------------------------------------------------- data views
 struct Batch {
     const LigDesc* ligs;
     const AtomRec* atoms;
     const NodeRec* nodes;
     const uint32_t* pairs;
+    const uint32_t* grid_list;
 };
 
 #ifndef UD_PAIR_BATCH
@@ -203,9 +193,10 @@ struct Maps {
 struct Layout {
     int x, xnew, xorig, tmp, cand, best;
     int g, gnew, gorig, p, y, mhy;
-    int h;
+    int h;                 // inverse Hessian, full symmetric n x n (n = 6 + T)
     int coords, forces;
-    int frames, accum;
+    int frames;
+    int prefix;            // per-atom prefix sums of force and moment (6 floats)
     int misc;
     int total;
 };
@@ -221,11 +212,11 @@ __host__ inline Layout make_layout(int max_atoms, int max_tors) {
     L.best = take(cs);
     L.g = take(gs); L.gnew = take(gs); L.gorig = take(gs); L.p = take(gs); L.y = take(gs);
     L.mhy = take(gs);
-    L.h = take(gs * (gs + 1) / 2);
+    L.h = take(gs * gs);
     L.coords = take(3 * max_atoms);
     L.forces = take(3 * max_atoms);
     L.frames = take(20 * R);
-    L.accum = take(6 * R);
+    L.prefix = take(6 * max_atoms);
     L.misc = take(32);
     L.total = o;
     return L;
@@ -237,7 +228,8 @@ struct Ctx {
     const AtomRec* atoms;
     const NodeRec* nodes;
     const uint32_t* pairs;
-    int n_atoms, R, T, n_pairs, max_depth, local_steps;
+    const uint32_t* grid;  // atom | slot << 8 of the atoms with a grid map
+    int n_atoms, R, T, n_pairs, max_depth, local_steps, n_grid;
     int lane;
 };
 
@@ -248,6 +240,8 @@ __device__ __forceinline__ Ctx make_ctx(const Batch& B, int lig, float* s) {
     c.atoms = B.atoms + __ldg(&d->atom_off);
     c.nodes = B.nodes + __ldg(&d->node_off);
     c.pairs = B.pairs + __ldg(&d->pair_off);
+    c.grid = B.grid_list + __ldg(&d->grid_off);
+    c.n_grid = __ldg(&d->n_grid);
     c.n_atoms = __ldg(&d->n_atoms);
     c.R = __ldg(&d->n_nodes);
     c.T = c.R - 1;
@@ -381,11 +375,13 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
     const float* xyz = c.s + L.coords;
     float* frc = c.s + L.forces;
     float e = 0;
-    for (int a = c.lane; a < c.n_atoms; a += 32) {
-        int packed = __ldg(&c.atoms[a].packed);
-        int slot = ((packed >> 8) & 0xFF) - 1;
-        float gx = 0, gy = 0, gz = 0;
-        if (slot >= 0) e += grid_eval(M, slot, xyz + 3 * a, v_inter, gx, gy, gz, true);
+    for (int k = c.lane; k < 3 * c.n_atoms; k += 32) frc[k] = 0;
+    __syncwarp();
+    for (int k = c.lane; k < c.n_grid; k += 32) {
+        const uint32_t ga = __ldg(c.grid + k);
+        const int a = ga & 0xFF, slot = ga >> 8;
+        float gx, gy, gz;
+        e += grid_eval(M, slot, xyz + 3 * a, v_inter, gx, gy, gz, true);
         frc[3 * a] = gx; frc[3 * a + 1] = gy; frc[3 * a + 2] = gz;
     }
     __syncwarp();
@@ -449,44 +445,57 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
         }
     }
     e = warp_sum(e);
-    // per-node force and torque of the node's own atoms about its origin
+    // Force and torque of every subtree.  A subtree's atoms are contiguous in
+    // DFS order, so inclusive prefix sums over atoms of f and of the moment
+    // (x - o_root) x f give each subtree's sums as a difference of two
+    // prefixes; the torque about the subtree's own origin o is then
+    // M - (o - o_root) x F (tree.h:75-84,164-192 sum the same terms node by node).
     const float* fr = c.s + L.frames;
-    float* acc = c.s + L.accum;
-    for (int n = c.lane; n < c.R; n += 32) {
-        int be = __ldg(&c.nodes[n].begin_end);
-        int b0 = be & 0xFFFF, b1 = be >> 16;
-        const float* o = fr + 20 * n;
-        float F0 = 0, F1 = 0, F2 = 0, T0 = 0, T1 = 0, T2 = 0;
-        for (int a = b0; a < b1; ++a) {
-            float f0 = frc[3 * a], f1 = frc[3 * a + 1], f2 = frc[3 * a + 2];
-            float r0 = xyz[3 * a] - o[0], r1 = xyz[3 * a + 1] - o[1], r2 = xyz[3 * a + 2] - o[2];
-            F0 += f0; F1 += f1; F2 += f2;
-            T0 += r1 * f2 - r2 * f1;
-            T1 += r2 * f0 - r0 * f2;
-            T2 += r0 * f1 - r1 * f0;
+    float* pre = c.s + L.prefix;
+    float carry[6] = {0, 0, 0, 0, 0, 0};
+    for (int base = 0; base < c.n_atoms; base += 32) {
+        const int a = base + c.lane;
+        float v[6] = {0, 0, 0, 0, 0, 0};
+        if (a < c.n_atoms) {
+            const float f0 = frc[3 * a], f1 = frc[3 * a + 1], f2 = frc[3 * a + 2];
+            const float r0 = xyz[3 * a] - fr[0], r1 = xyz[3 * a + 1] - fr[1], r2 = xyz[3 * a + 2] - fr[2];
+            v[0] = f0; v[1] = f1; v[2] = f2;
+            v[3] = r1 * f2 - r2 * f1;
+            v[4] = r2 * f0 - r0 * f2;
+            v[5] = r0 * f1 - r1 * f0;
         }
-        acc[6 * n] = F0; acc[6 * n + 1] = F1; acc[6 * n + 2] = F2;
-        acc[6 * n + 3] = T0; acc[6 * n + 4] = T1; acc[6 * n + 5] = T2;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                const float t = __shfl_up_sync(kFull, v[q], off);
+                if (c.lane >= off) v[q] += t;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            v[q] += carry[q];
+            carry[q] = __shfl_sync(kFull, v[q], 31);
+        }
+        if (a < c.n_atoms)
+#pragma unroll
+            for (int q = 0; q < 6; ++q) pre[6 * a + q] = v[q];
     }
     __syncwarp();
-    // subtree sums: nodes are in DFS pre-order, so the subtree of n is
-    // [n, subtree_end(n)); torques are moved to the node's origin.
     for (int n = c.lane; n < c.R; n += 32) {
+        const int span = __ldg(&c.nodes[n].atoms);
+        const int b0 = span & 0xFFFF, b1 = span >> 16;
+        const float* hi = pre + 6 * (b1 - 1);
+        float sm[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) sm[q] = hi[q] - (b0 > 0 ? pre[6 * (b0 - 1) + q] : 0.0f);
         const float* on = fr + 20 * n;
-        const float* an = acc + 6 * n;
-        float F0 = an[0], F1 = an[1], F2 = an[2], T0 = an[3], T1 = an[4], T2 = an[5];
-        const int se = __ldg(&c.nodes[n].subtree_end);
-        for (int m = n + 1; m < se; ++m) {
-            const float* am = acc + 6 * m;
-            const float* om = fr + 20 * m;
-            float r0 = om[0] - on[0], r1 = om[1] - on[1], r2 = om[2] - on[2];
-            F0 += am[0]; F1 += am[1]; F2 += am[2];
-            T0 += (r1 * am[2] - r2 * am[1]) + am[3];
-            T1 += (r2 * am[0] - r0 * am[2]) + am[4];
-            T2 += (r0 * am[1] - r1 * am[0]) + am[5];
-        }
+        const float d0 = on[0] - fr[0], d1 = on[1] - fr[1], d2 = on[2] - fr[2];
+        const float T0 = sm[3] - (d1 * sm[2] - d2 * sm[1]);
+        const float T1 = sm[4] - (d2 * sm[0] - d0 * sm[2]);
+        const float T2 = sm[5] - (d0 * sm[1] - d1 * sm[0]);
         if (n == 0) {
-            g[0] = F0; g[1] = F1; g[2] = F2;
+            g[0] = sm[0]; g[1] = sm[1]; g[2] = sm[2];
             g[3] = T0; g[4] = T1; g[5] = T2;
         } else {
             g[6 + n - 1] = T0 * on[16] + T1 * on[17] + T2 * on[18];
@@ -504,11 +513,10 @@ __device__ __forceinline__ void eval_score(const Ctx& c, const Layout& L, const 
     kinematics(c, L, conf);
     const float* xyz = c.s + L.coords;
     float eg = 0, ei = 0;
-    for (int a = c.lane; a < c.n_atoms; a += 32) {
-        int packed = __ldg(&c.atoms[a].packed);
-        int slot = ((packed >> 8) & 0xFF) - 1;
+    for (int k = c.lane; k < c.n_grid; k += 32) {
+        const uint32_t ga = __ldg(c.grid + k);
         float gx, gy, gz;
-        if (slot >= 0) eg += grid_eval(M, slot, xyz + 3 * a, v, gx, gy, gz, false);
+        eg += grid_eval(M, ga >> 8, xyz + 3 * (ga & 0xFF), v, gx, gy, gz, false);
     }
     for (int k = c.lane; k < c.n_pairs; k += 32) {
         uint32_t pr = __ldg(c.pairs + k);
@@ -556,27 +564,27 @@ __device__ __forceinline__ void conf_increment(const Ctx& c, const float* x, con
     __syncwarp();
 }
 
-// out = -H v (packed symmetric inverse Hessian, one row per lane)
+// The inverse Hessian is kept as a full symmetric n x n matrix (the reference
+// stores the upper triangle, bfgs.h:27-58): lane i owns row/column i, so both
+// products and the update are one contiguous loop per lane.
+// out = -H v
 __device__ __forceinline__ void minus_hv(const Ctx& c, const float* H, const float* v, float* out, int n) {
     for (int i = c.lane; i < n; i += 32) {
         float sum = 0;
-        const int ri = i * (i + 1) / 2;
-        for (int j = 0; j < i; ++j) sum += H[j + ri] * v[j];
-        for (int j = i; j < n; ++j) sum += H[i + j * (j + 1) / 2] * v[j];
+        for (int j = 0; j < n; ++j) sum += H[j * n + i] * v[j];
         out[i] = -sum;
     }
     __syncwarp();
 }
 
 __device__ __forceinline__ void h_identity(const Ctx& c, float* H, int n) {
-    const int nh = n * (n + 1) / 2;
-    for (int k = c.lane; k < nh; k += 32) H[k] = 0;
+    for (int k = c.lane; k < n * n; k += 32) H[k] = 0;
     __syncwarp();
-    for (int i = c.lane; i < n; i += 32) H[i + i * (i + 1) / 2] = 1;
+    for (int i = c.lane; i < n; i += 32) H[i * n + i] = 1;
     __syncwarp();
 }
 
-// BFGS update of the inverse Hessian (bfgs.h:40-58)
+// BFGS update of the inverse Hessian (bfgs.h:40-58), applied to both triangles
 __device__ __forceinline__ void h_update(const Ctx& c, float* H, const float* p, const float* y,
                                          float* mhy, float alpha, int n) {
     const float yp = dotw(c, y, p, n);
@@ -584,10 +592,10 @@ __device__ __forceinline__ void h_update(const Ctx& c, float* H, const float* p,
     minus_hv(c, H, y, mhy, n);
     const float yhy = -dotw(c, y, mhy, n);
     const float r = __frcp_rn(alpha * yp);
-    const int nh = n * (n + 1) / 2;
-    for (int k = c.lane; k < nh; k += 32) {
-        int j = tri_j(k), i = k - j * (j + 1) / 2;
-        H[k] += alpha * r * (mhy[i] * p[j] + mhy[j] * p[i]) + alpha * alpha * (r * r * yhy + r) * p[i] * p[j];
+    const float a1 = alpha * r, a2 = alpha * alpha * (r * r * yhy + r);
+    for (int i = c.lane; i < n; i += 32) {
+        const float mi = mhy[i], pi = p[i];
+        for (int j = 0; j < n; ++j) H[j * n + i] += a1 * (mi * p[j] + mhy[j] * pi) + a2 * pi * p[j];
     }
     __syncwarp();
 }
@@ -869,7 +877,7 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                     if (fabsf(yy) > kEps) {
                         float yp = dotw(c, y, p, n);
                         const float d = __fdividef(m.alpha * yp, yy);
-                        for (int i = lane; i < n; i += 32) H[i + i * (i + 1) / 2] = d;
+                        for (int i = lane; i < n; i += 32) H[i * n + i] = d;
                         __syncwarp();
                     }
                 }
@@ -1121,6 +1129,7 @@ struct DeviceBatchView {
     const AtomRec* atoms;
     const NodeRec* nodes;
     const uint32_t* pairs;
+    const uint32_t* grid_list;
     int max_atoms, max_torsions;
 };
 
@@ -1170,6 +1179,7 @@ static dev::Batch to_batch(const DeviceBatchView& b) {
     B.atoms = b.atoms;
     B.nodes = b.nodes;
     B.pairs = b.pairs;
+    B.grid_list = b.grid_list;
     return B;
 }
 

@@ -35,7 +35,8 @@ struct LigDesc {
     int n_heavy;
     int max_depth;
     int local_steps;       // BFGS iteration cap of this ligand
-    int pad[3];
+    int grid_off, n_grid;  // atoms with a grid map: list of atom | slot << 8
+    int pad;
 };
 
 struct NodeRec {            // 40 bytes
@@ -43,7 +44,7 @@ struct NodeRec {            // 40 bytes
     float rel_axis[3];
     int parent;
     int depth;
-    int begin_end;         // atom range: begin | end << 16
+    int atoms;             // atoms of the node's subtree (DFS order): begin | end << 16
     int subtree_end;       // one past the last node of this node's subtree
 };
 
