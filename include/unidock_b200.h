@@ -144,6 +144,38 @@ int ud_search_collect(ud_batch batch, void* stream);
 /* Raw per-chain results of the last search: best pose (pose_stride floats
  * per chain, chain-major per ligand), best energy and evaluations spent. */
 int ud_search_chains(ud_batch batch, float* poses, int pose_stride, float* e, int* evals);
+/* Allocation-free batched search.  No counterpart in the reference: added
+ * for callers that cannot let the library allocate device memory while they
+ * search -- applications whose device memory belongs to their own pool
+ * allocator (a cudaMalloc behind its back fragments or overcommits the pool),
+ * and latency-critical loops where an allocation's implicit device-wide
+ * synchronisation is not acceptable.
+ *
+ * Runs the batched persistent search (form 1; params->form, chains_per_block
+ * and use_graph are ignored) on `stream` and returns without waiting.  The
+ * caller owns every output, all in device memory of the current device:
+ *   d_poses     [n_ligands * exhaustiveness][pose_stride] best pose per chain
+ *               (chain-major per ligand, as ud_search_chains), pose_stride >=
+ *               7 + the batch's largest torsion count; only the first 7 + T
+ *               floats of a row (T = that ligand's torsions) are written;
+ *   d_energies  [n_ligands * exhaustiveness] best energy per chain;
+ *   d_evals     [n_ligands * exhaustiveness] evaluations per chain, or NULL.
+ * Results equal those of ud_search_launch + ud_search_chains with the same
+ * params.  No clustering or rescoring is done (that host part allocates).
+ *
+ * Scratch (work-queue counter, ligand order, per-chain records) lives in one
+ * static device array of about 2.1 MB that each GPU using the library holds
+ * until the process exits; the call clears what must start at zero.  Limits:
+ * at most 8192 ligands and 131072 chains (ligands x exhaustiveness) per call,
+ * beyond which it returns UD_ERR_CAPACITY without launching anything.  All
+ * calls on one device share that scratch, so calls whose work overlaps on
+ * that device (issued on two streams, or from two threads) race: order them
+ * on one stream or synchronise between them.  Each device has its own copy,
+ * so calls on different devices do not interfere.  The first call on each
+ * device looks up the scratch's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture. */
+int ud_search_device_noalloc(ud_batch batch, const ud_search_params* params, float* d_poses, int pose_stride,
+                             float* d_energies, int* d_evals, void* stream);
 /* Number of modes kept for ligand `lig` after clustering and rescoring. */
 int ud_result_count(ud_batch batch, int lig, int* n_modes);
 /* Mode k of ligand `lig`: pose (7+T floats) and

@@ -57,6 +57,10 @@ cudaError_t launch_optimize(const DeviceBatchView& b, const DeviceMapsView& m, c
                             const int* pose_lig, float* poses, int pose_stride, int n_poses, int max_steps,
                             float v, float* e_out, int* evals_out, cudaStream_t stream);
 float measure_fp32_peak_tflops();
+cudaError_t launch_search_noalloc(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
+                                  const SearchParams& P, const int* h_order, int n_ligands, int grid_blocks,
+                                  float* poses, int pose_stride, float* e_out, int* evals_out,
+                                  cudaStream_t stream);
 int engine_chain_smem_bytes(int max_atoms, int max_torsions);
 }  // namespace ud
 
@@ -1020,5 +1024,55 @@ extern "C" int ud_device_fp32_peak(float* tflops) {
         if (!tflops) throw Error(UD_ERR_ARG, "null argument");
         *tflops = measure_fp32_peak_tflops();
         if (!(*tflops > 0)) throw Error(UD_ERR_CUDA, "fp32 probe failed");
+    });
+}
+
+// Persistent search with caller-provided device outputs and the library's
+// static device scratch instead of device allocations (see the header).
+extern "C" int ud_search_device_noalloc(ud_batch b, const ud_search_params* params, float* d_poses,
+                                        int pose_stride, float* d_energies, int* d_evals, void* stream) {
+    return guarded([&] {
+        if (!b || !params || !d_poses || !d_energies) throw Error(UD_ERR_ARG, "null argument");
+        const ud_search_params& P = *params;
+        if (P.exhaustiveness < 1) throw Error(UD_ERR_ARG, "exhaustiveness must be >= 1");
+        if (pose_stride < 7 + b->max_tors) throw Error(UD_ERR_ARG, "pose_stride smaller than 7 + max torsions");
+        const int n_lig = (int)b->ligs.size();
+        const long long n_chain = (long long)n_lig * P.exhaustiveness;
+        if (n_lig > kNoAllocMaxLigands)
+            throw Error(UD_ERR_CAPACITY, "ud_search_device_noalloc: batch of " + std::to_string(n_lig) +
+                                             " ligands exceeds the maximum of " + std::to_string(kNoAllocMaxLigands));
+        if (n_chain > kNoAllocMaxChains)
+            throw Error(UD_ERR_CAPACITY, "ud_search_device_noalloc: " + std::to_string(n_chain) +
+                                             " chains (ligands x exhaustiveness) exceed the maximum of " +
+                                             std::to_string(kNoAllocMaxChains));
+        if (n_lig == 0) return;
+        std::vector<int> order(n_lig);
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            long long cx = (long long)b->desc[x].local_steps * (b->desc[x].n_atoms + b->desc[x].n_pairs);
+            long long cy = (long long)b->desc[y].local_steps * (b->desc[y].n_atoms + b->desc[y].n_pairs);
+            return cx > cy;
+        });
+        SearchParams sp{};
+        sp.global_steps = global_steps_for(b->ligs, P.max_step);
+        sp.exhaustiveness = P.exhaustiveness;
+        sp.seed = P.seed;
+        sp.hunt_cap = 10.0f;
+        sp.authentic_v = 1000.0f;
+        sp.temperature = 1.2f;
+        sp.mutation_amplitude = 2.0f;
+        sp.lanes_per_chain = 32;
+        sp.chains_per_block = 4;
+        sp.persistent = 1;
+        sp.bfgs_cap = P.bfgs_cap;
+        int dev = 0, n_sm = 148;
+        cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+        cuda_check(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev), "device attribute");
+        const int per_sm = search_blocks_per_sm(b->view(), sp.chains_per_block);
+        const int needed = (int)((n_chain + sp.chains_per_block - 1) / sp.chains_per_block);
+        const int blocks = std::max(1, std::min(per_sm * n_sm, needed));
+        cuda_check(launch_search_noalloc(b->view(), maps_view(b->maps), tables_view(b->maps), sp, order.data(), n_lig,
+                                         blocks, d_poses, pose_stride, d_energies, d_evals, (cudaStream_t)stream),
+                   "allocation-free search");
     });
 }

@@ -1297,4 +1297,69 @@ int search_blocks_per_sm(const DeviceBatchView& b, int warps) {
     return nb > 0 ? nb : 1;
 }
 
+// ---------------------------------------------------------------- allocation-free search
+// Scratch of the persistent search for callers that cannot allocate device
+// memory when they search: a file-scope device array that every GPU loading
+// the library holds until the process exits.  Layout: the work-queue counter
+// (256 bytes), the ligand order (kNoAllocMaxLigands ints), then one
+// ChainResult per chain (kNoAllocMaxChains).  Every call shares it: the
+// counter is cleared and the order rewritten on each call, and calls that
+// overlap on the GPU race on it.
+constexpr size_t kNoAllocOrderOff = 256;
+constexpr size_t kNoAllocResultsOff =
+    kNoAllocOrderOff + ((kNoAllocMaxLigands * sizeof(int) + 255) / 256) * 256;
+constexpr size_t kNoAllocBytes = kNoAllocResultsOff + kNoAllocMaxChains * sizeof(ChainResult);
+static __device__ __align__(256) unsigned char g_search_scratch[kNoAllocBytes];
+
+namespace dev {
+__global__ void chain_results_out(const ChainResult* r, int n, float* e, int* evals) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (e) e[i] = r[i].e;
+    if (evals) evals[i] = r[i].evals;
+}
+}  // namespace dev
+
+// Device address of g_search_scratch on the current device, looked up once per
+// device (host code only holds a stand-in for the array, not its address).
+static cudaError_t noalloc_scratch(unsigned char** out) {
+    constexpr int kMaxDevices = 64;
+    static unsigned char* addr[kMaxDevices] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    if (!addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_search_scratch);
+        if (e != cudaSuccess) return e;
+        addr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = addr[dev];
+    return cudaSuccess;
+}
+
+cudaError_t launch_search_noalloc(const DeviceBatchView& b, const DeviceMapsView& m,
+                                  const DeviceTablesView& t, const SearchParams& P,
+                                  const int* h_order, int n_ligands, int grid_blocks, float* poses,
+                                  int pose_stride, float* e_out, int* evals_out, cudaStream_t stream) {
+    unsigned char* base = nullptr;
+    cudaError_t e = noalloc_scratch(&base);
+    if (e != cudaSuccess) return e;
+    unsigned int* queue = reinterpret_cast<unsigned int*>(base);
+    int* order = reinterpret_cast<int*>(base + kNoAllocOrderOff);
+    ChainResult* results = reinterpret_cast<ChainResult*>(base + kNoAllocResultsOff);
+    const int n_items = n_ligands * P.exhaustiveness;
+    e = cudaMemsetAsync(queue, 0, sizeof(unsigned int), stream);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(order, h_order, (size_t)n_ligands * sizeof(int), cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return e;
+    SearchParams sp = P;
+    sp.persistent = 1;
+    e = launch_search(b, m, t, sp, order, n_items, 0, queue, poses, pose_stride, results, grid_blocks, stream);
+    if (e != cudaSuccess) return e;
+    dev::chain_results_out<<<(n_items + 255) / 256, 256, 0, stream>>>(results, n_items, e_out, evals_out);
+    return cudaGetLastError();
+}
+
 }  // namespace ud

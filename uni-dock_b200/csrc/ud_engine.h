@@ -73,6 +73,10 @@ struct SearchParams {
     int bfgs_cap;          // 0: per-ligand local_steps; >0: min(local_steps, cap)
 };
 
+// Capacity of the allocation-free search (ud_search_device_noalloc).
+constexpr int kNoAllocMaxLigands = 8192;
+constexpr int kNoAllocMaxChains = 131072;
+
 // Result record of one chain.
 struct ChainResult {
     float e;               // best energy (refined, authentic cap)

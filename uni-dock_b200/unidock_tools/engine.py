@@ -19,6 +19,7 @@ LIB_PATH = Path(os.environ.get("UNIDOCK_B200_LIB", PKG_ROOT / "lib" / "libunidoc
 
 SF_VINA, SF_AD4, SF_VINARDO = 0, 1, 2
 UD_OK = 0
+UD_ERR_ARG, UD_ERR_PARSE, UD_ERR_CUDA, UD_ERR_CAPACITY, UD_ERR_STATE = 1, 2, 3, 4, 5
 
 _lib = None
 
@@ -80,6 +81,7 @@ def lib():
         "ud_search_launch": ([vp, C.POINTER(SearchParams), vp], C.c_int),
         "ud_search_collect": ([vp, vp], C.c_int),
         "ud_search_chains": ([vp, fp, C.c_int, fp, ip], C.c_int),
+        "ud_search_device_noalloc": ([vp, C.POINTER(SearchParams), vp, C.c_int, vp, vp, vp], C.c_int),
         "ud_result_count": ([vp, C.c_int, ip], C.c_int),
         "ud_result_mode": ([vp, C.c_int, C.c_int, fp, fp], C.c_int),
         "ud_result_write": ([vp, C.c_int, C.c_int, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
@@ -275,6 +277,18 @@ class Batch:
                                chains_per_block, bfgs_cap, use_graph)
         _check(lib().ud_search_launch(self.h, C.byref(self._p), None))
         self.exhaustiveness = exhaustiveness
+
+    def search_device_noalloc(self, d_poses, pose_stride, d_energies, d_evals=None, stream=None, exhaustiveness=8,
+                              max_step=0, seed=0, bfgs_cap=0):
+        """Batched search into caller-owned device buffers (raw device
+        addresses as ints), using the library's static scratch instead of
+        device allocations; asynchronous on `stream` (a raw cudaStream_t or
+        None for the legacy default stream).  Returns per-chain results only:
+        no clustering, and the batch's own result state is left untouched."""
+        p = SearchParams(exhaustiveness, max_step, 9, 1.0, 3.0, seed, 1, 0, bfgs_cap, 0)
+        _check(lib().ud_search_device_noalloc(self.h, C.byref(p), C.c_void_p(d_poses), int(pose_stride),
+                                              C.c_void_p(d_energies), C.c_void_p(d_evals) if d_evals else None,
+                                              C.c_void_p(stream) if stream else None))
 
     def search_collect(self):
         _check(lib().ud_search_collect(self.h, None))
