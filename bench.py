@@ -33,6 +33,7 @@ MAX_STEP = 20
 N_LIGANDS = 4096
 BOX = 22.5
 SPACING = 0.375
+ADJOINT_POSES = 65536
 
 
 def parse_args():
@@ -46,6 +47,8 @@ def parse_args():
     ap.add_argument("--cpu-sample", type=int, default=16, help="ligands timed on the reference CPU path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chains-per-block", type=int, default=0)
+    ap.add_argument("--adjoint-poses", type=int, default=ADJOINT_POSES,
+                    help="fixed poses of the adjoint leg (0 = skip)")
     ap.add_argument("--profile-case", type=int, default=0,
                     help="profiling aid: search N ligands of the workload twice and exit (no JSON)")
     return ap.parse_args()
@@ -157,7 +160,7 @@ def run_ours(args, rank, world):
 
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     P = dict(exhaustiveness=EXHAUSTIVENESS, max_step=MAX_STEP, num_modes=9, min_rmsd=1.0, seed=42, form=1,
-             chains_per_block=args.chains_per_block)
+             chains_per_block=args.chains_per_block, use_graph=1)
 
     # ---- device-resident form: topology uploaded before the timed region
     batches = []
@@ -249,16 +252,18 @@ def run_ours(args, rank, world):
         ligs, b = batches[args.warmup]
         sub = ligs[:args.plain_sample]
         bp = engine.Batch(maps, sub)
-        bp.search_launch(**dict(P, form=0))
+        bp.search_launch(**dict(P, form=0, use_graph=0))
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        bp.search_launch(**dict(P, form=0))
+        bp.search_launch(**dict(P, form=0, use_graph=0))
         e1.record()
         torch.cuda.synchronize()
         bp.search_collect()
         plain = len(sub) / (e0.elapsed_time(e1) / 1e3)
+
+    adjoint = adjoint_leg(maps) if rank == 0 and args.adjoint_poses > 0 else None
 
     result = None
     if rank == 0:
@@ -294,11 +299,57 @@ def run_ours(args, rank, world):
                     "d2h_bytes_per_step": int(d2h)},
             "clocks": clk,
             "gpu_launches": args.steps * 1,
+            "adjoint": adjoint,
         }
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     return result
+
+
+def adjoint_leg(maps, n_ligands=256, reps=5):
+    """Differentiation workload: 65,536 fixed poses over 256 ligands of the
+    screen's size distribution (centre uniform in the box, uniform random unit
+    quaternion, torsions U(-pi, pi)); energy + pose-layout gradient + the 6
+    term-weight gradients per pose in one adjoint launch (exact pair
+    derivative).  Device-resident inputs, CUDA-event time of the launch."""
+    import torch
+    from unidock_tools import engine, synth
+    ligs = [engine.Ligand(l.to_pdbqt()) for l in
+            synth.ligand_set(n_ligands, seed=7, heavy=(12, 48), torsions=(0, 10))]
+    B = engine.Batch(maps, ligs)
+    per = ADJOINT_POSES // n_ligands
+    stride = 7 + B.max_torsions
+    P = np.zeros((n_ligands * per, stride), np.float32)
+    for i, L in enumerate(ligs):
+        P[i * per:(i + 1) * per, :7 + L.n_torsions] = synth.random_poses(per, L.n_torsions, -BOX / 2, BOX / 2,
+                                                                          seed=1000 + i)
+    n = len(P)
+    nt = maps.n_terms
+    d_p = torch.from_numpy(P).cuda()
+    d_l = torch.from_numpy(np.repeat(np.arange(n_ligands, dtype=np.int32), per)).cuda()
+    d_e = torch.empty(n, device="cuda")
+    d_g = torch.empty((n, stride), device="cuda")
+    d_w = torch.empty((n, nt), device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+
+    def run():
+        B.score_adjoint_device(d_l.data_ptr(), d_p.data_ptr(), n, stride, d_e.data_ptr(), d_g.data_ptr(), stride,
+                               d_w.data_ptr(), nt, exact=True, stream=s)
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        run()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    return {"workload": f"{n} fixed poses over {n_ligands} ligands, Vina, energy + pose gradient + "
+                        f"{nt} term-weight gradients (exact), FP32", "poses_per_s": round(n / (ms / 1e3), 1),
+            "ms_per_launch": round(ms, 3)}
 
 
 # ------------------------------------------------------------------ reference CPU path

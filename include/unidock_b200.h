@@ -117,6 +117,45 @@ int ud_score_grad_device(ud_batch batch, const int* pose_ligand, const float* po
 int ud_score(ud_batch batch, const int* pose_ligand, const float* poses, int n_poses,
              int pose_stride, float v, float* out, void* stream);
 
+/* ---------------------------------------------------------------- differentiation
+ * No counterpart in the reference (its gradient is internal to BFGS).
+ *
+ * Term weights of the maps' scoring function, in the reference's order
+ * (Vina: gauss1, gauss2, repulsion, hydrophobic, hbond, glue; Vinardo:
+ * gauss1, repulsion, hydrophobic, hbond, glue); the rotatable-bond weight is
+ * not a term (it enters only the final conf-independent score). */
+int ud_maps_term_count(ud_maps maps, int* n_terms);
+int ud_maps_get_weights(ud_maps maps, float* w, int n);
+/* Replace the term weights: maps and pair tables become the weight-sum of
+ * per-term maps and tables (built on the GPU on first use, about
+ * n_terms x (maps + 27 MB) of device memory), so searches and scores that
+ * follow use the new weights.  Equal to maps built with those weights up to
+ * FP32 rounding of the sum. */
+int ud_maps_set_weights(ud_maps maps, const float* w, int n, void* stream);
+
+#define UD_ADJOINT_EXACT 1  /* pair forces: exact derivative of the lerped energy */
+/* Energy at fixed poses with its gradient in the POSE layout and its weight
+ * gradient (the adjoint of the energy; conformer coordinates recomputed from
+ * the pose, not stored).
+ *   g_out  (optional) 7 + T floats per pose, stride g_stride:
+ *          d/dposition[3], d/dq[4], d/dtorsions[T]; d/dq is tangent to the
+ *          unit sphere at q (the orientation is meant as q/|q|, and the
+ *          poses are expected to carry unit quaternions);
+ *   dw_out (optional) n_terms floats per pose, stride dw_stride: d/d(term
+ *          weight), with the maps' current weights.
+ * Pair forces follow the reference (model::eval_deriv, the table's dE/dr / r
+ * column, model.cpp:935-962) unless flags has UD_ADJOINT_EXACT, which takes the
+ * exact derivative of the computed (lerped) energy -- the gradient that
+ * finite differences of the energy converge to.  Poses whose pose_ligand is
+ * out of range get a NaN energy (device form) or UD_ERR_ARG (host form). */
+int ud_score_adjoint(ud_batch batch, const int* pose_ligand, const float* poses, int n_poses, int pose_stride,
+                     float v_intra, float v_inter, int flags, float* e_out, float* g_out, int g_stride,
+                     float* dw_out, int dw_stride, void* stream);
+/* Same with device pointers; asynchronous on `stream`. */
+int ud_score_adjoint_device(ud_batch batch, const int* pose_ligand, const float* poses, int n_poses,
+                            int pose_stride, float v_intra, float v_inter, int flags, float* e_out, float* g_out,
+                            int g_stride, float* dw_out, int dw_stride, void* stream);
+
 /* ---------------------------------------------------------------- search */
 typedef struct {
     int exhaustiveness;     /* MC chains per ligand (--exhaustiveness) */
@@ -126,10 +165,34 @@ typedef struct {
     float energy_range;     /* output energy window (--energy_range) */
     unsigned long long seed;/* --seed */
     int form;               /* 0 = plain (one launch per ligand), 1 = batched persistent */
-    int chains_per_block;   /* warps (chains) per CTA, 0 = autotuned/default */
-    int bfgs_cap;           /* 0 = per-ligand (25 + atoms)/3 BFGS steps; >0 caps it */
-    int use_graph;          /* batched form: replay the per-batch sequence as a CUDA graph */
+    int chains_per_block;   /* chains (warps) per CTA, 1..4; 0 = the batch's autotuned value, else 4 */
+    int bfgs_cap;           /* 0 = per-ligand (25 + atoms)/3 BFGS steps; >0 caps it;
+                               <0 = the batch's autotuned cap (per-ligand when not tuned) */
+    int use_graph;          /* batched form: the per-batch sequence (queue reset, search
+                               kernel, result copies) captured once as a CUDA graph and
+                               replayed while parameters and buffers are unchanged */
 } ud_search_params;
+
+/* Launch configuration picked by ud_autotune. */
+typedef struct {
+    int chains_per_block;      /* chains (warps) per CTA */
+    int lanes_per_chain;       /* lanes per chain (32: one warp per chain in this build) */
+    int bfgs_cap;              /* BFGS iteration cap, 0 = per-ligand */
+    int n_sample;              /* ligands of the batch in the tuning sample */
+    int n_tried;               /* configurations timed */
+    float ligands_per_s;       /* sample throughput of the picked configuration */
+    float base_ligands_per_s;  /* sample throughput of the default (4 chains/CTA, no cap) */
+    float energy_shift;        /* mean best-energy change against the default (<= 0.1) */
+} ud_tune_result;
+
+/* Autotuner (no counterpart in the reference): times the batched search on a
+ * sample of the batch (ligands spread over its size order, enough chains to
+ * fill the GPU twice, the caller's exhaustiveness, at most 40 MC steps) for
+ * chains-per-CTA in {4, 2, 1} and BFGS caps in {per-ligand, 16, 10, 6}, and
+ * keeps the fastest configuration whose mean best energy is within 0.1
+ * kcal/mol of the default's.  Searches of this batch with chains_per_block = 0
+ * and bfgs_cap < 0 then use it.  Synchronous; takes about 12 short searches. */
+int ud_autotune(ud_batch batch, const ud_search_params* params, ud_tune_result* out, void* stream);
 
 /* Run the Monte-Carlo + BFGS search of every ligand of the batch.
  * Replaces Vina::global_search_gpu (unidock/src/lib/vina.h:154-354) and

@@ -18,6 +18,11 @@ VINA_W = np.array([-0.035579, -0.005156, 0.840245, -0.035069, -0.587439, 50, 5 *
 VINARDO_W = np.array([-0.045, 0.8, -0.035, -0.600, 50, 5 * 0.05846 / 0.1 - 1], np.float32).astype(np.float64)
 
 
+def default_weights(sf):
+    """Default weights of the scoring function (unidock/src/main/main.cpp:373-395)."""
+    return {0: VINA_W, 2: VINARDO_W}[sf]
+
+
 class _Lig(C.Structure):
     _fields_ = [("n_atoms", C.c_int), ("n_nodes", C.c_int), ("n_pairs", C.c_int),
                 ("local", C.c_void_p), ("node", C.c_void_p), ("gtype", C.c_void_p), ("heavy", C.c_void_p),
@@ -61,7 +66,7 @@ class Oracle:
 
     # ---- tables
     def tables(self, sf=0, weights=None):
-        w = np.ascontiguousarray(VINA_W if weights is None else weights, np.float64)
+        w = np.ascontiguousarray(default_weights(sf) if weights is None else weights, np.float64)
         nb = self.L.orc_table_bins(sf)
         ntp = 36 * 37 // 2
         fast = np.zeros((ntp, nb), self.real)
@@ -75,7 +80,7 @@ class Oracle:
 
     # ---- maps
     def maps(self, rec_xyz, rec_xs, dims, init, factor_inv, types, sf=0, weights=None):
-        w = np.ascontiguousarray(VINA_W if weights is None else weights, np.float64)
+        w = np.ascontiguousarray(default_weights(sf) if weights is None else weights, np.float64)
         xyz = self._a(rec_xyz)
         xs = np.ascontiguousarray(rec_xs, np.int32)
         d = np.ascontiguousarray(dims, np.int32)

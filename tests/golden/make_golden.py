@@ -3,12 +3,14 @@ code (oracle/_ref/libudref.so, built by oracle/Makefile from the reference
 sources).  The reference's tests pin no energies, gradients or maps, so these
 vectors are produced here on seeded synthetic inputs:
 
-  ref_vina_small.npz   receptor + 12 A box maps (sampled points), 4 ligands
-                       (PDBQT text), 8 poses each, reference eval_deriv energies
-                       and gradients at curl caps 1000 and 10, scoring energies,
-                       and sampled type-pair table values.
+  ref_vina_small.npz     receptor + 12 A box maps (sampled points), 4 ligands
+                         (PDBQT text), 8 poses each, reference eval_deriv
+                         energies and gradients at curl caps 1000 and 10,
+                         scoring energies, and sampled type-pair table values,
+                         Vina scoring function with its default weights.
+  ref_vinardo_small.npz  the same inputs scored with Vinardo.
 
-Run:  python tests/golden/make_golden.py
+Run:  python tests/golden/make_golden.py [vina|vinardo|all]
 """
 import sys
 import tempfile
@@ -26,12 +28,16 @@ from unidock_tools import synth  # noqa: E402
 TYPES = [0, 1, 2, 3, 4, 5, 8, 9, 10, 12, 13]
 
 
-def main():
+SF_NAMES = {"vina": 0, "vinardo": 2}
+
+
+def make(name):
+    sf = SF_NAMES[name]
     rng = np.random.default_rng(2026)
     rec = synth.make_receptor(1200, radius=30.0, seed=11)
     center = np.zeros(3, np.float32)
     size = np.full(3, 12.0, np.float32)
-    R = ref.RefMaps(rec.xyz, rec.xs, center, size, 0.375, types=TYPES)
+    R = ref.RefMaps(rec.xyz, rec.xs, center, size, 0.375, sf=sf, types=TYPES)
     dims = R.dims.copy()
     npts = int(dims.prod())
     sample_idx = np.sort(rng.choice(npts, 3000, replace=False)).astype(np.int64)
@@ -45,7 +51,7 @@ def main():
             p = Path(d) / f"l{k}.pdbqt"
             p.write_text(txt)
             texts.append(txt)
-            ligs.append(ref.RefLigand(p))
+            ligs.append(ref.RefLigand(p, sf=sf))
         poses, e1000, g1000, e10, g10, score = [], [], [], [], [], []
         for k, RL in enumerate(ligs):
             P = synth.random_poses(8, RL.n_torsions, -3.0, 3.0, seed=77 + k)
@@ -67,16 +73,18 @@ def main():
         fast = np.array([ref.lib().udref_table_fast(R.h, int(a), int(b), float(c)) for a, b, c in zip(t1, t2, r2)],
                         np.float32)
         ntors = np.array([RL.n_torsions for RL in ligs], np.int32)
-    out = ROOT / "tests" / "golden" / "ref_vina_small.npz"
+    out = ROOT / "tests" / "golden" / f"ref_{name}_small.npz"
     np.savez_compressed(
         out, rec_xyz=rec.xyz, rec_xs=rec.xs, center=center, size=size, spacing=np.float32(0.375),
         types=np.array(TYPES, np.int32), dims=dims, init=R.init, factor=R.factor, factor_inv=R.factor_inv,
         sample_idx=sample_idx, map_samples=map_samples, ligand_pdbqt=np.array(texts), n_torsions=ntors,
         poses=np.array(poses, np.float32), e1000=np.array(e1000, np.float32), g1000=np.array(g1000, np.float32),
         e10=np.array(e10, np.float32), g10=np.array(g10, np.float32), score=np.array(score, np.float32),
-        tab_t1=t1.astype(np.int32), tab_t2=t2.astype(np.int32), tab_r2=r2, tab_fast=fast)
+        sf=np.int32(sf), tab_t1=t1.astype(np.int32), tab_t2=t2.astype(np.int32), tab_r2=r2, tab_fast=fast)
     print("wrote", out, out.stat().st_size, "bytes")
 
 
 if __name__ == "__main__":
-    main()
+    which = sys.argv[1] if len(sys.argv) > 1 else "all"
+    for nm in (SF_NAMES if which == "all" else [which]):
+        make(nm)

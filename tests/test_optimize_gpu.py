@@ -1,6 +1,7 @@
 """GPU local optimisation (ud_optimize, the quasi_newton path) against the
 oracle's BFGS restatement from the same starting poses, and fixed-pose
-energies/gradients against the committed reference golden vectors."""
+energies/gradients against the committed reference golden vectors, for the
+Vina and Vinardo scoring functions."""
 from pathlib import Path
 
 import numpy as np
@@ -10,14 +11,15 @@ from oracle.oracle import Oracle
 from unidock_tools import engine
 
 pytestmark = pytest.mark.gpu
-GOLD = Path(__file__).resolve().parent / "golden" / "ref_vina_small.npz"
+GOLDEN = Path(__file__).resolve().parent / "golden"
 
 
-@pytest.fixture(scope="module")
-def setup():
-    gold = dict(np.load(GOLD))
+@pytest.fixture(scope="module", params=["vina", "vinardo"])
+def setup(request):
+    gold = dict(np.load(GOLDEN / f"ref_{request.param}_small.npz"))
+    gold["sf"] = int(gold["sf"])
     maps = engine.Maps(gold["rec_xyz"], gold["rec_xs"], gold["center"], gold["size"], float(gold["spacing"]),
-                       types=gold["types"])
+                       types=gold["types"], sf=gold["sf"])
     ligs = [engine.Ligand(str(t)) for t in gold["ligand_pdbqt"]]
     batch = engine.Batch(maps, ligs)
     return gold, maps, ligs, batch
@@ -41,8 +43,9 @@ def test_energies_match_golden(setup):
 def test_bfgs_matches_oracle_from_same_start(setup):
     gold, maps, ligs, batch = setup
     o = Oracle(np.float32)
-    fast, smooth = o.tables()
-    om = o.maps(gold["rec_xyz"], gold["rec_xs"], gold["dims"], gold["init"], gold["factor_inv"], gold["types"])
+    fast, smooth = o.tables(sf=gold["sf"])
+    om = o.maps(gold["rec_xyz"], gold["rec_xs"], gold["dims"], gold["init"], gold["factor_inv"], gold["types"],
+                sf=gold["sf"])
     grid = o.grid(om, gold["dims"], gold["init"], gold["factor"], gold["factor_inv"])
     sm = {int(t): k for k, t in enumerate(gold["types"])}
     stride = 7 + batch.max_torsions

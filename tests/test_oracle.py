@@ -11,12 +11,14 @@ from oracle import ref
 from oracle.oracle import Oracle
 from unidock_tools import engine
 
-GOLD = Path(__file__).resolve().parent / "golden" / "ref_vina_small.npz"
+GOLDEN = Path(__file__).resolve().parent / "golden"
 
 
-@pytest.fixture(scope="module")
-def gold():
-    return dict(np.load(GOLD))
+@pytest.fixture(scope="module", params=["vina", "vinardo"])
+def gold(request):
+    g = dict(np.load(GOLDEN / f"ref_{request.param}_small.npz"))
+    g["sf"] = int(g["sf"])
+    return g
 
 
 @pytest.fixture(scope="module")
@@ -31,8 +33,9 @@ def o64():
 
 @pytest.fixture(scope="module")
 def setup32(gold, o32):
-    fast, smooth = o32.tables()
-    maps = o32.maps(gold["rec_xyz"], gold["rec_xs"], gold["dims"], gold["init"], gold["factor_inv"], gold["types"])
+    fast, smooth = o32.tables(sf=gold["sf"])
+    maps = o32.maps(gold["rec_xyz"], gold["rec_xs"], gold["dims"], gold["init"], gold["factor_inv"], gold["types"],
+                    sf=gold["sf"])
     grid = o32.grid(maps, gold["dims"], gold["init"], gold["factor"], gold["factor_inv"])
     return fast, smooth, maps, grid
 
@@ -42,7 +45,7 @@ def slot_map(gold):
 
 
 def test_table_samples_match_reference(gold, o32):
-    fast, _ = o32.tables()
+    fast, _ = o32.tables(sf=gold["sf"])
     t1, t2, r2 = gold["tab_t1"], gold["tab_t2"], gold["tab_r2"]
     tp = np.minimum(t1, t2) + np.maximum(t1, t2) * (np.maximum(t1, t2) + 1) // 2
     got = fast[tp, (np.float32(32) * r2).astype(np.int64)]
@@ -91,8 +94,9 @@ def test_scoring_energies_match_reference(gold, o32, setup32):
 def test_fp32_error_against_fp64_oracle(gold, o64):
     """FP32 reference energies/gradients vs the FP64 restatement: the FP32
     rounding error of the reference path itself (stated in DESIGN.md)."""
-    fast, smooth = o64.tables()
-    maps = o64.maps(gold["rec_xyz"], gold["rec_xs"], gold["dims"], gold["init"], gold["factor_inv"], gold["types"])
+    fast, smooth = o64.tables(sf=gold["sf"])
+    maps = o64.maps(gold["rec_xyz"], gold["rec_xs"], gold["dims"], gold["init"], gold["factor_inv"], gold["types"],
+                    sf=gold["sf"])
     grid = o64.grid(maps, gold["dims"], gold["init"], gold["factor"], gold["factor_inv"])
     sm = slot_map(gold)
     errs_e, errs_g = [], []
@@ -111,13 +115,13 @@ def test_bfgs_matches_reference_from_same_start(gold, o32, setup32, tmp_path):
     fast, smooth, maps, grid = setup32
     sm = slot_map(gold)
     R = ref.RefMaps(gold["rec_xyz"], gold["rec_xs"], gold["center"], gold["size"], float(gold["spacing"]),
-                    types=gold["types"])
+                    sf=gold["sf"], types=gold["types"])
     agree = 0
     total = 0
     for li, txt in enumerate(gold["ligand_pdbqt"]):
         p = tmp_path / f"l{li}.pdbqt"
         p.write_text(str(txt))
-        RL = ref.RefLigand(p)
+        RL = ref.RefLigand(p, sf=gold["sf"])
         L = o32.ligand(engine.Ligand(str(txt)).export(), sm)
         T = int(gold["n_torsions"][li])
         for k in range(4):

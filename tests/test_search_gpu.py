@@ -53,3 +53,47 @@ def test_modes_and_output(small):
         txt = B.write(li)
         assert txt.startswith("MODEL 1\nREMARK VINA RESULT:")
         assert txt.count("ENDMDL") >= 1
+
+
+def test_vinardo_search_chain_energy_is_pose_energy(receptor):
+    M = engine.Maps(receptor.xyz, receptor.xs, BOX_CENTER, BOX_SIZE, 0.375, sf=engine.SF_VINARDO)
+    ligs = [engine.Ligand(synth.make_ligand(16 + 8 * k, 2 * k + 1, seed=1700 + k).to_pdbqt()) for k in range(3)]
+    B = engine.Batch(M, ligs)
+    B.search(exhaustiveness=8, max_step=10, seed=4, form=1)
+    poses, e, ev = B.chains()
+    assert np.all(np.isfinite(e)) and np.all(ev > 0)
+    e2, _ = B.score_grad(np.repeat(np.arange(len(ligs)), 8), poses, 1000.0, 1000.0)
+    np.testing.assert_allclose(e2, e, rtol=1e-4, atol=1e-4)
+    for li in range(len(ligs)):
+        assert B.write(li).startswith("MODEL 1\nREMARK VINA RESULT:")
+
+
+def test_graph_form_equals_persistent_form(small):
+    M, ligs = small
+    B = engine.Batch(M, ligs)
+    B.search(exhaustiveness=8, max_step=8, seed=13, form=1, use_graph=0)
+    p0, e0, ev0 = B.chains()
+    for _ in range(2):  # captured once, replayed
+        B.search(exhaustiveness=8, max_step=8, seed=13, form=1, use_graph=1)
+        p1, e1, ev1 = B.chains()
+        np.testing.assert_array_equal(e1, e0)
+        np.testing.assert_array_equal(ev1, ev0)
+    B.search(exhaustiveness=8, max_step=8, seed=14, form=1, use_graph=1)   # new parameters: recaptured
+    _, e2, _ = B.chains()
+    B.search(exhaustiveness=8, max_step=8, seed=14, form=1, use_graph=0)
+    _, e3, _ = B.chains()
+    np.testing.assert_array_equal(e2, e3)
+    assert B.write(0).startswith("MODEL 1\nREMARK VINA RESULT:")
+
+
+def test_autotune_picks_valid_configuration(small):
+    M, ligs = small
+    B = engine.Batch(M, ligs * 8)
+    r = B.autotune(exhaustiveness=16, max_step=6, seed=1)
+    assert r["chains_per_block"] in (1, 2, 4)
+    assert r["bfgs_cap"] in (0, 16, 10, 6)
+    assert r["lanes_per_chain"] == 32 and r["n_tried"] == 12
+    assert r["energy_shift"] <= 0.1 and r["ligands_per_s"] >= r["base_ligands_per_s"] > 0
+    B.search(exhaustiveness=16, max_step=6, seed=1, form=1, chains_per_block=0, bfgs_cap=-1)
+    _, e, ev = B.chains()
+    assert np.all(np.isfinite(e)) and np.all(ev > 0)

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <iomanip>
+#include <limits>
 #include <memory>
 #include <numeric>
 #include <sstream>
@@ -20,49 +21,6 @@
 #include "ud_engine.h"
 #include "ud_model.h"
 
-namespace ud {
-// ud_engine.cu
-struct DeviceBatchView {
-    const LigDesc* ligs;
-    const AtomRec* atoms;
-    const NodeRec* nodes;
-    const uint32_t* pairs;
-    const uint32_t* grid_list;
-    int max_atoms, max_torsions;
-};
-struct DeviceMapsView {
-    const float* data;
-    MapsDesc desc;
-};
-struct DeviceTablesView {
-    const float* smooth;
-    const float* fast;
-    int n_bins;
-    float factor;
-    float cutoff2;
-};
-cudaError_t launch_maps(const float* rec_xyzt, int n_rec, const float* fastT, int n_bins, int n_slots,
-                        int n_slots_pad, float factor, float cutoff2, const MapsDesc& d, float* out,
-                        cudaStream_t stream);
-cudaError_t launch_score(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
-                         const int* pose_lig, const float* poses, int pose_stride, int n_poses,
-                         float v_intra, float v_inter, float* e_out, float* g_out, int g_stride,
-                         float* score_out, cudaStream_t stream);
-cudaError_t launch_search(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
-                          const SearchParams& P, const int* order, int n_items, int first_item,
-                          unsigned int* queue, float* poses, int pose_stride, ChainResult* results,
-                          int grid_blocks, cudaStream_t stream);
-int search_blocks_per_sm(const DeviceBatchView& b, int warps);
-cudaError_t launch_optimize(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
-                            const int* pose_lig, float* poses, int pose_stride, int n_poses, int max_steps,
-                            float v, float* e_out, int* evals_out, cudaStream_t stream);
-float measure_fp32_peak_tflops();
-cudaError_t launch_search_noalloc(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
-                                  const SearchParams& P, const int* h_order, int n_ligands, int grid_blocks,
-                                  float* poses, int pose_stride, float* e_out, int* evals_out,
-                                  cudaStream_t stream);
-int engine_chain_smem_bytes(int max_atoms, int max_torsions);
-}  // namespace ud
 
 using namespace ud;
 
@@ -104,6 +62,26 @@ template <class T> struct DevBuf {
     }
 };
 
+// Page-locked host buffer (device-to-host copies of a captured search graph).
+template <class T> struct PinnedBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    PinnedBuf() = default;
+    PinnedBuf(const PinnedBuf&) = delete;
+    PinnedBuf& operator=(const PinnedBuf&) = delete;
+    ~PinnedBuf() {
+        if (p) cudaFreeHost(p);
+    }
+    void alloc(size_t count) {
+        if (count <= n && p) return;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+        cuda_check(cudaMallocHost((void**)&p, std::max<size_t>(count, 1) * sizeof(T)), "cudaMallocHost");
+        n = count;
+    }
+};
+
 template <class F> int guarded(F&& f) {
     try {
         f();
@@ -132,6 +110,13 @@ struct ud_maps_s {
     int n_bins = 0;
     float factor = 32.0f;
     float cutoff2 = 64.0f;
+    // typed receptor atoms (x, y, z, xs as int bits), kept to build term maps
+    std::vector<float> rec_xyzt;
+    // per-term data of weight gradients, built on first use
+    DevBuf<float> term_maps;         // [term][slot][z][y][x]
+    DevBuf<float> term_rows;         // [term][tp][bin][4], as `smooth`
+    DevBuf<float> term_fast;         // [term][tp][bin], as `fast`
+    bool terms_built = false;
 };
 
 struct LigandPost {
@@ -171,9 +156,32 @@ struct ud_batch_s {
     // scoring scratch
     DevBuf<int> d_pose_lig;
     DevBuf<float> d_pose;
-    DevBuf<float> d_e, d_g, d_score;
+    DevBuf<float> d_e, d_g, d_score, d_dw;
 
+    // captured per-batch search sequence (use_graph): queue reset, persistent
+    // search kernel and the copies of its results into page-locked memory
+    cudaStream_t capture_stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    std::string graph_key;
+    PinnedBuf<float> hp_poses;
+    PinnedBuf<ChainResult> hp_results;
+    bool graph_results = false;
+    // launch configuration picked by ud_autotune for this batch
+    bool tuned = false;
+    int tuned_chains_per_block = 4;
+    int tuned_bfgs_cap = 0;
+
+    void drop_graph() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        if (graph) cudaGraphDestroy(graph);
+        graph_exec = nullptr;
+        graph = nullptr;
+        graph_key.clear();
+    }
     ~ud_batch_s() {
+        drop_graph();
+        if (capture_stream) cudaStreamDestroy(capture_stream);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
     }
@@ -220,6 +228,32 @@ static std::vector<int> default_map_types() {
         if (g >= 0 && std::find(t.begin(), t.end(), g) == t.end()) t.push_back(g);
     }
     return t;
+}
+
+static size_t round4(size_t n) { return (n + 3) & ~(size_t)3; }
+
+// Lerp rows with both bracketing bins in one 16-byte record:
+// [tp][bin] = (e_bin, dor_bin, e_bin+1, dor_bin+1).
+static void pack_smooth4(const PairTable& tab, float* s4) {
+    const size_t ntp = tab.smooth.size() / (2 * (size_t)tab.n);
+    for (size_t tp = 0; tp < ntp; ++tp)
+        for (int k = 0; k < tab.n; ++k) {
+            const float* row = &tab.smooth[tp * tab.n * 2];
+            float* o = &s4[(tp * tab.n + k) * 4];
+            o[0] = row[2 * k];
+            o[1] = row[2 * k + 1];
+            o[2] = (k + 1 < tab.n) ? row[2 * (k + 1)] : 0.0f;
+            o[3] = (k + 1 < tab.n) ? row[2 * (k + 1) + 1] : 0.0f;
+        }
+}
+
+// Receptor-type-major table of the map kernel: [t1][bin][slot].
+static void pack_fastT(const PairTable& tab, const std::vector<int>& slot_types, int nslot_pad, float* fastT) {
+    for (int t1 = 0; t1 < XS_SIZE; ++t1)
+        for (size_t k = 0; k < slot_types.size(); ++k) {
+            const float* row = &tab.fast[(size_t)tri_index(t1, slot_types[k]) * tab.n];
+            for (int b = 0; b < tab.n; ++b) fastT[((size_t)t1 * tab.n + b) * nslot_pad + k] = row[b];
+        }
 }
 
 extern "C" int ud_maps_create(int sf, const float* weights, int n_weights, const float* rec_xyz,
@@ -274,31 +308,17 @@ extern "C" int ud_maps_create(int sf, const float* weights, int n_weights, const
         m->n_bins = tab.n;
         m->factor = tab.factor;
         m->cutoff2 = m->sf.cutoff * m->sf.cutoff;
-        // lerp table with both bracketing bins in one 16-byte record:
-        // [tp][bin] = (e_bin, dor_bin, e_bin+1, dor_bin+1)
         {
-            const size_t ntp = tab.smooth.size() / (2 * (size_t)tab.n);
-            std::vector<float> s4(ntp * tab.n * 4, 0.0f);
-            for (size_t tp = 0; tp < ntp; ++tp)
-                for (int k = 0; k < tab.n; ++k) {
-                    const float* row = &tab.smooth[tp * tab.n * 2];
-                    float* o = &s4[(tp * tab.n + k) * 4];
-                    o[0] = row[2 * k];
-                    o[1] = row[2 * k + 1];
-                    o[2] = (k + 1 < tab.n) ? row[2 * (k + 1)] : 0.0f;
-                    o[3] = (k + 1 < tab.n) ? row[2 * (k + 1) + 1] : 0.0f;
-                }
+            std::vector<float> s4(tab.smooth.size() * 2, 0.0f);
+            pack_smooth4(tab, s4.data());
             m->smooth.upload(s4.data(), s4.size(), s);
         }
+        // padded to whole float4s: ud_maps_set_weights rewrites these in place
+        m->fast.alloc(round4(tab.fast.size()));
         m->fast.upload(tab.fast.data(), tab.fast.size(), s);
-        // receptor-type-major table for the map kernel: [t1][bin][slot]
         const int nslot = d.n_maps, nslot_pad = std::max(4, (nslot + 3) & ~3);
         std::vector<float> fastT((size_t)XS_SIZE * tab.n * nslot_pad, 0.0f);
-        for (int t1 = 0; t1 < XS_SIZE; ++t1)
-            for (int k = 0; k < nslot; ++k) {
-                const float* row = &tab.fast[(size_t)tri_index(t1, m->slot_types[k]) * tab.n];
-                for (int b = 0; b < tab.n; ++b) fastT[((size_t)t1 * tab.n + b) * nslot_pad + k] = row[b];
-            }
+        pack_fastT(tab, m->slot_types, nslot_pad, fastT.data());
         DevBuf<float> d_fastT;
         d_fastT.upload(fastT.data(), fastT.size(), s);
         std::vector<float> rec;
@@ -315,8 +335,9 @@ extern "C" int ud_maps_create(int sf, const float* weights, int n_weights, const
         }
         DevBuf<float> d_rec;
         d_rec.upload(rec.data(), rec.size(), s);
+        m->rec_xyzt = rec;
         const size_t plane = (size_t)d.dims[0] * d.dims[1] * d.dims[2];
-        m->maps.alloc(plane * std::max(1, nslot));
+        m->maps.alloc(round4(plane * std::max(1, nslot)));
         if (nslot > 0) {
             cuda_check(launch_maps(d_rec.p, (int)(rec.size() / 4), d_fastT.p, tab.n, nslot, nslot_pad,
                                    tab.factor, m->cutoff2, d, m->maps.p, s),
@@ -482,10 +503,11 @@ static std::vector<uint32_t> pair_groups(const Ligand& L) {
     return out;
 }
 
-extern "C" int ud_batch_create(ud_maps maps, const ud_ligand* ligs, int n, void* stream, ud_batch* out) {
-    return guarded([&] {
-        if (!maps || !out || n < 0 || (n > 0 && !ligs)) throw Error(UD_ERR_ARG, "invalid batch arguments");
-        cudaStream_t s = (cudaStream_t)stream;
+// Device topology of `ligs` against `maps` (the body of ud_batch_create; the
+// autotuner builds its sample batches with it too).
+static std::unique_ptr<ud_batch_s> build_batch(ud_maps maps, const std::vector<const Ligand*>& ligs,
+                                               cudaStream_t s) {
+        const int n = (int)ligs.size();
         auto b = std::make_unique<ud_batch_s>();
         b->maps = maps;
         std::vector<AtomRec> atoms;
@@ -493,8 +515,7 @@ extern "C" int ud_batch_create(ud_maps maps, const ud_ligand* ligs, int n, void*
         std::vector<uint32_t> pairs;
         std::vector<uint32_t> grid_list;
         for (int i = 0; i < n; ++i) {
-            if (!ligs[i]) throw Error(UD_ERR_ARG, "null ligand in batch");
-            const Ligand& L = ligs[i]->lig;
+            const Ligand& L = *ligs[i];
             if ((int)L.atoms.size() > kMaxLigAtoms)
                 throw Error(UD_ERR_CAPACITY, "ligand " + std::to_string(i) + " has more than 256 atoms");
             if (L.n_torsions() > kMaxLigTorsions)
@@ -560,7 +581,18 @@ extern "C" int ud_batch_create(ud_maps maps, const ud_ligand* ligs, int n, void*
         b->d_pairs.upload(pairs.data(), pairs.size(), s);
         b->d_grid.upload(grid_list.data(), grid_list.size(), s);
         cuda_check(cudaStreamSynchronize(s), "batch upload");
-        *out = b.release();
+        return b;
+}
+
+extern "C" int ud_batch_create(ud_maps maps, const ud_ligand* ligs, int n, void* stream, ud_batch* out) {
+    return guarded([&] {
+        if (!maps || !out || n < 0 || (n > 0 && !ligs)) throw Error(UD_ERR_ARG, "invalid batch arguments");
+        std::vector<const Ligand*> v;
+        for (int i = 0; i < n; ++i) {
+            if (!ligs[i]) throw Error(UD_ERR_ARG, "null ligand in batch");
+            v.push_back(&ligs[i]->lig);
+        }
+        *out = build_batch(maps, v, (cudaStream_t)stream).release();
     });
 }
 
@@ -645,6 +677,153 @@ extern "C" int ud_score(ud_batch b, const int* pose_ligand, const float* poses, 
         std::vector<float> p(poses, poses + (size_t)n_poses * pose_stride), o;
         score_poses_device(b, l, p, pose_stride, v, o, (cudaStream_t)stream);
         std::copy(o.begin(), o.end(), out);
+    });
+}
+
+// ---------------------------------------------------------------- adjoint
+
+// Unweighted per-term maps and tables of the maps' scoring function: the
+// same construction as the weighted ones (ud_maps_create) with one term at
+// weight 1.  Maps and tables are linear in the term weights, so a weighted
+// map or table is the weight-sum of these (up to FP32 rounding).
+static size_t term_map_block(const ud_maps_s* m) {
+    const size_t plane = (size_t)m->desc.dims[0] * m->desc.dims[1] * m->desc.dims[2];
+    return round4(plane * std::max(1, m->desc.n_maps));
+}
+static size_t n_type_pairs() { return (size_t)XS_SIZE * (XS_SIZE + 1) / 2; }
+
+static void ensure_terms(ud_maps_s* m, cudaStream_t s) {
+    if (m->terms_built) return;
+    const MapsDesc& d = m->desc;
+    const int nt = m->sf.n_terms;
+    const int nslot = d.n_maps, nslot_pad = std::max(4, (nslot + 3) & ~3);
+    const size_t mblock = term_map_block(m);
+    const size_t rblock = n_type_pairs() * m->n_bins * 4;
+    const size_t fblock = round4(n_type_pairs() * m->n_bins);
+    m->term_maps.alloc((size_t)nt * mblock);
+    m->term_rows.alloc((size_t)nt * rblock);
+    m->term_fast.alloc((size_t)nt * fblock);
+    cuda_check(cudaMemsetAsync(m->term_maps.p, 0, (size_t)nt * mblock * sizeof(float), s), "memset");
+    cuda_check(cudaMemsetAsync(m->term_fast.p, 0, (size_t)nt * fblock * sizeof(float), s), "memset");
+    DevBuf<float> d_rec;
+    d_rec.upload(m->rec_xyzt.data(), m->rec_xyzt.size(), s);
+    DevBuf<float> d_fastT;
+    std::vector<float> rows(rblock), fastT((size_t)XS_SIZE * m->n_bins * nslot_pad, 0.0f);
+    for (int t = 0; t < nt; ++t) {
+        PairTable tab;
+        tab.build(m->sf, t);
+        if (tab.n != m->n_bins) throw Error(UD_ERR_ARG, "term table size mismatch");
+        pack_smooth4(tab, rows.data());
+        cuda_check(cudaMemcpyAsync(m->term_rows.p + (size_t)t * rblock, rows.data(), rblock * sizeof(float),
+                                   cudaMemcpyHostToDevice, s),
+                   "H2D");
+        cuda_check(cudaMemcpyAsync(m->term_fast.p + (size_t)t * fblock, tab.fast.data(), tab.fast.size() * sizeof(float),
+                                   cudaMemcpyHostToDevice, s),
+                   "H2D");
+        pack_fastT(tab, m->slot_types, nslot_pad, fastT.data());
+        d_fastT.upload(fastT.data(), fastT.size(), s);
+        if (nslot > 0)
+            cuda_check(launch_maps(d_rec.p, (int)(m->rec_xyzt.size() / 4), d_fastT.p, tab.n, nslot, nslot_pad,
+                                   tab.factor, m->cutoff2, d, m->term_maps.p + (size_t)t * mblock, s),
+                       "term maps kernel");
+        // host rows / fastT and the table are reused or freed next round: wait for their copies
+        cuda_check(cudaStreamSynchronize(s), "term maps sync");
+    }
+    m->terms_built = true;
+}
+
+static DeviceTermsView terms_view(const ud_maps_s* m) {
+    return DeviceTermsView{m->term_maps.p, m->term_rows.p, m->sf.n_terms, (long long)term_map_block(m),
+                           (long long)(n_type_pairs() * m->n_bins)};
+}
+
+extern "C" int ud_maps_term_count(ud_maps maps, int* n_terms) {
+    return guarded([&] {
+        if (!maps || !n_terms) throw Error(UD_ERR_ARG, "null argument");
+        *n_terms = maps->sf.n_terms;
+    });
+}
+
+extern "C" int ud_maps_get_weights(ud_maps maps, float* w, int n) {
+    return guarded([&] {
+        if (!maps || !w || n < maps->sf.n_terms) throw Error(UD_ERR_ARG, "invalid weights buffer");
+        for (int t = 0; t < maps->sf.n_terms; ++t) w[t] = maps->sf.weights[t];
+    });
+}
+
+extern "C" int ud_maps_set_weights(ud_maps maps, const float* w, int n, void* stream) {
+    return guarded([&] {
+        if (!maps || !w || n != maps->sf.n_terms) throw Error(UD_ERR_ARG, "expected one weight per scoring term");
+        for (int t = 0; t < n; ++t)
+            if (!std::isfinite(w[t])) throw Error(UD_ERR_ARG, "weights must be finite");
+        cudaStream_t s = (cudaStream_t)stream;
+        ensure_terms(maps, s);
+        const size_t rblock = n_type_pairs() * maps->n_bins * 4;
+        const size_t fblock = round4(n_type_pairs() * maps->n_bins);
+        cuda_check(launch_combine_terms(maps->term_maps.p, (long long)term_map_block(maps), n, w, maps->maps.p, s),
+                   "combine maps");
+        cuda_check(launch_combine_terms(maps->term_rows.p, (long long)rblock, n, w, maps->smooth.p, s), "combine rows");
+        cuda_check(launch_combine_terms(maps->term_fast.p, (long long)fblock, n, w, maps->fast.p, s), "combine fast");
+        for (int t = 0; t < n; ++t) maps->sf.weights[t] = w[t];
+    });
+}
+
+extern "C" int ud_score_adjoint_device(ud_batch b, const int* pose_ligand, const float* poses, int n_poses,
+                                       int pose_stride, float v_intra, float v_inter, int flags, float* e_out,
+                                       float* g_out, int g_stride, float* dw_out, int dw_stride, void* stream) {
+    return guarded([&] {
+        if (!b || n_poses < 0 || (n_poses > 0 && (!pose_ligand || !poses || !e_out)))
+            throw Error(UD_ERR_ARG, "invalid adjoint arguments");
+        if (pose_stride < 7 + b->max_tors) throw Error(UD_ERR_ARG, "pose_stride smaller than 7 + max torsions");
+        if (g_out && g_stride < 7 + b->max_tors) throw Error(UD_ERR_ARG, "g_stride smaller than 7 + max torsions");
+        if (dw_out && dw_stride < b->maps->sf.n_terms) throw Error(UD_ERR_ARG, "dw_stride smaller than term count");
+        if (n_poses == 0) return;
+        cudaStream_t s = (cudaStream_t)stream;
+        if (dw_out) ensure_terms(b->maps, s);
+        DeviceTermsView tv = b->maps->terms_built ? terms_view(b->maps) : DeviceTermsView{nullptr, nullptr, 0, 0, 0};
+        cuda_check(launch_adjoint(b->view(), maps_view(b->maps), tables_view(b->maps), tv, (int)b->desc.size(),
+                                  pose_ligand, poses, pose_stride, n_poses, v_intra, v_inter,
+                                  (flags & UD_ADJOINT_EXACT) ? 1 : 0, e_out, g_out, g_stride, dw_out, dw_stride, s),
+                   "adjoint kernel");
+    });
+}
+
+extern "C" int ud_score_adjoint(ud_batch b, const int* pose_ligand, const float* poses, int n_poses,
+                                int pose_stride, float v_intra, float v_inter, int flags, float* e_out, float* g_out,
+                                int g_stride, float* dw_out, int dw_stride, void* stream) {
+    return guarded([&] {
+        check_poses(b, pose_ligand, n_poses, pose_stride);
+        if (!poses || !e_out) throw Error(UD_ERR_ARG, "null buffer");
+        if (g_out && g_stride < 7 + b->max_tors) throw Error(UD_ERR_ARG, "g_stride smaller than 7 + max torsions");
+        const int nt = b->maps->sf.n_terms;
+        if (dw_out && dw_stride < nt) throw Error(UD_ERR_ARG, "dw_stride smaller than term count");
+        for (int i = 0; i < n_poses; ++i)
+            if (pose_ligand[i] < 0 || pose_ligand[i] >= (int)b->desc.size())
+                throw Error(UD_ERR_ARG, "pose_ligand out of range");
+        if (n_poses == 0) return;
+        cudaStream_t s = (cudaStream_t)stream;
+        if (dw_out) ensure_terms(b->maps, s);
+        b->d_pose_lig.upload(pose_ligand, n_poses, s);
+        b->d_pose.upload(poses, (size_t)n_poses * pose_stride, s);
+        b->d_e.alloc(n_poses);
+        if (g_out) b->d_g.alloc((size_t)n_poses * g_stride);
+        if (dw_out) b->d_dw.alloc((size_t)n_poses * dw_stride);
+        DeviceTermsView tv = b->maps->terms_built ? terms_view(b->maps) : DeviceTermsView{nullptr, nullptr, 0, 0, 0};
+        cuda_check(launch_adjoint(b->view(), maps_view(b->maps), tables_view(b->maps), tv, (int)b->desc.size(),
+                                  b->d_pose_lig.p, b->d_pose.p, pose_stride, n_poses, v_intra, v_inter,
+                                  (flags & UD_ADJOINT_EXACT) ? 1 : 0, b->d_e.p, g_out ? b->d_g.p : nullptr, g_stride,
+                                  dw_out ? b->d_dw.p : nullptr, dw_stride, s),
+                   "adjoint kernel");
+        cuda_check(cudaMemcpyAsync(e_out, b->d_e.p, n_poses * sizeof(float), cudaMemcpyDeviceToHost, s), "D2H");
+        if (g_out)
+            cuda_check(cudaMemcpyAsync(g_out, b->d_g.p, (size_t)n_poses * g_stride * sizeof(float),
+                                       cudaMemcpyDeviceToHost, s),
+                       "D2H");
+        if (dw_out)
+            cuda_check(cudaMemcpyAsync(dw_out, b->d_dw.p, (size_t)n_poses * dw_stride * sizeof(float),
+                                       cudaMemcpyDeviceToHost, s),
+                       "D2H");
+        cuda_check(cudaStreamSynchronize(s), "adjoint sync");
     });
 }
 
@@ -813,11 +992,54 @@ static void post_process(ud_batch b, cudaStream_t s) {
     });
 }
 
+// Capture (or reuse) the per-batch sequence of the persistent search as a
+// CUDA graph: queue reset, search kernel, results into page-locked memory.
+// Captured on the batch's own stream (capture is not allowed on the legacy
+// default stream); the instantiated graph is then launched on any stream.
+// Reused while the launch parameters and buffers are unchanged.
+static void search_graph(ud_batch b, const SearchParams& sp, int n_chain, int blocks) {
+    b->hp_poses.alloc((size_t)n_chain * b->pose_stride);
+    b->hp_results.alloc((size_t)n_chain);
+    std::ostringstream k;
+    k << n_chain << ' ' << blocks << ' ' << sp.global_steps << ' ' << sp.exhaustiveness << ' ' << sp.seed << ' '
+      << sp.chains_per_block << ' ' << sp.bfgs_cap << ' ' << (const void*)b->d_poses.p << ' '
+      << (const void*)b->d_results.p << ' ' << (const void*)b->d_queue.p << ' ' << (const void*)b->d_order.p << ' '
+      << (const void*)b->hp_poses.p << ' ' << (const void*)b->hp_results.p << ' ' << (const void*)b->maps->maps.p
+      << ' ' << (const void*)b->maps->smooth.p;
+    if (b->graph_exec && b->graph_key == k.str()) return;
+    b->drop_graph();
+    if (!b->capture_stream)
+        cuda_check(cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking), "capture stream");
+    cudaStream_t cs = b->capture_stream;
+    cuda_check(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");
+    cudaError_t e = cudaMemsetAsync(b->d_queue.p, 0, sizeof(unsigned int), cs);
+    if (e == cudaSuccess)
+        e = launch_search(b->view(), maps_view(b->maps), tables_view(b->maps), sp, b->d_order.p, n_chain, 0,
+                          b->d_queue.p, b->d_poses.p, b->pose_stride, b->d_results.p, blocks, cs);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->hp_poses.p, b->d_poses.p, (size_t)n_chain * b->pose_stride * sizeof(float),
+                            cudaMemcpyDeviceToHost, cs);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->hp_results.p, b->d_results.p, (size_t)n_chain * sizeof(ChainResult),
+                            cudaMemcpyDeviceToHost, cs);
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cuda_check(e != cudaSuccess ? e : e2, "search graph capture");
+    }
+    b->graph = g;
+    cuda_check(cudaGraphInstantiate(&b->graph_exec, g, 0), "graph instantiate");
+    b->graph_key = k.str();
+}
+
 // Launch the search kernels of the batch asynchronously on `s`.
 static void search_launch(ud_batch b, const ud_search_params* params, cudaStream_t s) {
         if (!b || !params) throw Error(UD_ERR_ARG, "null argument");
         const ud_search_params& P = *params;
         if (P.exhaustiveness < 1) throw Error(UD_ERR_ARG, "exhaustiveness must be >= 1");
+        if (P.chains_per_block < 0 || P.chains_per_block > 4)
+            throw Error(UD_ERR_ARG, "chains_per_block must be 0 (default / autotuned) or 1..4");
         b->params = P;
         b->searched = false;
         const int n_lig = (int)b->ligs.size();
@@ -846,15 +1068,28 @@ static void search_launch(ud_batch b, const ud_search_params* params, cudaStream
         sp.temperature = 1.2f;
         sp.mutation_amplitude = 2.0f;
         sp.lanes_per_chain = 32;
-        sp.chains_per_block = P.chains_per_block > 0 ? P.chains_per_block : 4;
+        sp.chains_per_block = P.chains_per_block > 0 ? P.chains_per_block : (b->tuned ? b->tuned_chains_per_block : 4);
         sp.persistent = P.form == 1 ? 1 : 0;
-        sp.bfgs_cap = P.bfgs_cap;
+        sp.bfgs_cap = P.bfgs_cap >= 0 ? P.bfgs_cap : (b->tuned ? b->tuned_bfgs_cap : 0);
         int dev = 0, n_sm = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
         if (!b->ev0) {
             cuda_check(cudaEventCreate(&b->ev0), "event");
             cuda_check(cudaEventCreate(&b->ev1), "event");
+        }
+        b->graph_results = false;
+        if (sp.persistent && P.use_graph) {
+            int per_sm = search_blocks_per_sm(b->view(), sp.chains_per_block);
+            int blocks = std::max(1, std::min(per_sm * n_sm, (int)((n_chain + sp.chains_per_block - 1) /
+                                                                    sp.chains_per_block)));
+            search_graph(b, sp, (int)n_chain, blocks);
+            cudaEventRecord(b->ev0, s);
+            cuda_check(cudaGraphLaunch(b->graph_exec, s), "graph launch");
+            cudaEventRecord(b->ev1, s);
+            b->graph_results = true;
+            b->launched = true;
+            return;
         }
         cudaEventRecord(b->ev0, s);
         if (sp.persistent) {
@@ -884,19 +1119,114 @@ static void search_collect(ud_batch b, cudaStream_t s) {
         const size_t n_chain = (size_t)b->ligs.size() * b->exhaustiveness;
         b->h_poses.resize(n_chain * b->pose_stride);
         b->h_results.resize(n_chain);
-        cuda_check(cudaMemcpyAsync(b->h_poses.data(), b->d_poses.p, b->h_poses.size() * sizeof(float),
-                                   cudaMemcpyDeviceToHost, s),
-                   "D2H poses");
-        cuda_check(cudaMemcpyAsync(b->h_results.data(), b->d_results.p, n_chain * sizeof(ChainResult),
-                                   cudaMemcpyDeviceToHost, s),
-                   "D2H results");
-        cuda_check(cudaStreamSynchronize(s), "search sync");
+        if (b->graph_results) {  // the graph copied them into page-locked memory
+            cuda_check(cudaStreamSynchronize(s), "search sync");
+            std::memcpy(b->h_poses.data(), b->hp_poses.p, b->h_poses.size() * sizeof(float));
+            std::memcpy(b->h_results.data(), b->hp_results.p, n_chain * sizeof(ChainResult));
+        } else {
+            cuda_check(cudaMemcpyAsync(b->h_poses.data(), b->d_poses.p, b->h_poses.size() * sizeof(float),
+                                       cudaMemcpyDeviceToHost, s),
+                       "D2H poses");
+            cuda_check(cudaMemcpyAsync(b->h_results.data(), b->d_results.p, n_chain * sizeof(ChainResult),
+                                       cudaMemcpyDeviceToHost, s),
+                       "D2H results");
+            cuda_check(cudaStreamSynchronize(s), "search sync");
+        }
         cudaEventElapsedTime(&b->kernel_ms, b->ev0, b->ev1);
         b->evals = 0;
         for (auto& r : b->h_results) b->evals += r.evals;
         post_process(b, s);
         b->launched = false;
         b->searched = true;
+}
+
+// ---------------------------------------------------------------- autotuner
+
+// Per-ligand best chain energy and device time of one search of `tb`.
+static float trial_search(ud_batch tb, const ud_search_params& tp, cudaStream_t s, std::vector<float>& best) {
+    search_launch(tb, &tp, s);
+    const size_t n_lig = tb->ligs.size(), E = (size_t)tp.exhaustiveness;
+    std::vector<ChainResult> r(n_lig * E);
+    cuda_check(cudaMemcpyAsync(r.data(), tb->d_results.p, r.size() * sizeof(ChainResult), cudaMemcpyDeviceToHost, s),
+               "D2H results");
+    cuda_check(cudaStreamSynchronize(s), "trial sync");
+    tb->launched = false;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, tb->ev0, tb->ev1);
+    best.assign(n_lig, std::numeric_limits<float>::max());
+    for (size_t i = 0; i < r.size(); ++i) best[i / E] = std::min(best[i / E], r[i].e);
+    return ms;
+}
+
+extern "C" int ud_autotune(ud_batch b, const ud_search_params* params, ud_tune_result* out, void* stream) {
+    return guarded([&] {
+        if (!b || !params || !out) throw Error(UD_ERR_ARG, "null argument");
+        if (params->exhaustiveness < 1) throw Error(UD_ERR_ARG, "exhaustiveness must be >= 1");
+        cudaStream_t s = (cudaStream_t)stream;
+        const int n_lig = (int)b->ligs.size();
+        if (n_lig == 0) throw Error(UD_ERR_ARG, "empty batch");
+        const int E = params->exhaustiveness;
+        // sample: ligands spread evenly over the cost order, enough chains to
+        // fill every SM's resident warps about twice
+        std::vector<int> order(n_lig);
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            long long cx = (long long)b->desc[x].local_steps * (b->desc[x].n_atoms + b->desc[x].n_pairs);
+            long long cy = (long long)b->desc[y].local_steps * (b->desc[y].n_atoms + b->desc[y].n_pairs);
+            return cx > cy;
+        });
+        int dev = 0, n_sm = 148;
+        cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+        cuda_check(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev), "device attribute");
+        const long long resident = (long long)search_blocks_per_sm(b->view(), 4) * n_sm * 4;
+        const int S = (int)std::max<long long>(1, std::min<long long>({(2 * resident + E - 1) / E, n_lig, 512}));
+        std::vector<const Ligand*> sample;
+        for (int i = 0; i < S; ++i) sample.push_back(b->ligs[order[(size_t)i * n_lig / S]]);
+        auto tb = build_batch(b->maps, sample, s);
+        ud_search_params tp = *params;
+        tp.form = 1;
+        tp.use_graph = 0;
+        // tuning budget: the caller's MC step cap, or at most 40 steps per chain
+        if (tp.max_step <= 0 || tp.max_step > 40) tp.max_step = 40;
+        const int cpbs[] = {4, 2, 1};
+        const int caps[] = {0, 16, 10, 6};
+        std::vector<float> base, cur;
+        tp.chains_per_block = 4;
+        tp.bfgs_cap = 0;
+        trial_search(tb.get(), tp, s, cur);                 // warm-up (module load, caches)
+        float base_ms = trial_search(tb.get(), tp, s, base);
+        int best_cpb = 4, best_cap = 0, tried = 1;
+        float best_ms = base_ms, best_shift = 0.0f;
+        for (int cap : caps)
+            for (int cpb : cpbs) {
+                if (cap == 0 && cpb == 4) continue;
+                tp.chains_per_block = cpb;
+                tp.bfgs_cap = cap;
+                const float ms = trial_search(tb.get(), tp, s, cur);
+                ++tried;
+                double shift = 0;
+                for (int i = 0; i < S; ++i) shift += (double)cur[i] - (double)base[i];
+                shift /= S;
+                // accept only configurations whose search quality holds
+                if (shift <= 0.1 && ms < best_ms) {
+                    best_ms = ms;
+                    best_cpb = cpb;
+                    best_cap = cap;
+                    best_shift = (float)shift;
+                }
+            }
+        b->tuned = true;
+        b->tuned_chains_per_block = best_cpb;
+        b->tuned_bfgs_cap = best_cap;
+        out->chains_per_block = best_cpb;
+        out->lanes_per_chain = 32;
+        out->bfgs_cap = best_cap;
+        out->n_sample = S;
+        out->n_tried = tried;
+        out->ligands_per_s = best_ms > 0 ? 1e3f * S / best_ms : 0.0f;
+        out->base_ligands_per_s = base_ms > 0 ? 1e3f * S / base_ms : 0.0f;
+        out->energy_shift = best_shift;
+    });
 }
 
 extern "C" int ud_search(ud_batch b, const ud_search_params* params, void* stream) {

@@ -368,6 +368,10 @@ __device__ __forceinline__ float grid_eval(const Maps& M, int slot, const float*
 }
 
 // Energy and gradient (change layout: position, torque, torsions) of `conf`.
+// Pair forces use the table's dE/dr / r column (precalculate.h:48-65) or, with
+// kExactPairs, the slope of the lerped energy itself (the exact derivative of
+// the computed energy, 2 factor (e_bin+1 - e_bin) per unit r^2).
+template <bool kExactPairs = false>
 __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const Maps& M,
                                             const Tables& Tb, const float* conf, float* g,
                                             float v_intra, float v_inter) {
@@ -423,7 +427,7 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
                 const float4 t = tv[u];
                 const float rem = remv[u];
                 float ep = t.x + rem * (t.z - t.x);
-                float dor = t.y + rem * (t.w - t.y);
+                float dor = kExactPairs ? 2.0f * Tb.factor * (t.z - t.x) : t.y + rem * (t.w - t.y);
                 fx = dor * rv[u][0]; fy = dor * rv[u][1]; fz = dor * rv[u][2];
                 if (ep > 0 && v_intra < 0.1f * kMaxFl) {
                     float tmp = (v_intra < kEps) ? 0 : __fdividef(v_intra, v_intra + ep);
@@ -1010,6 +1014,168 @@ __global__ void __launch_bounds__(128) score_kernel(
     }
 }
 
+// ---------------------------------------------------------------- adjoint
+// Per-term data of the scoring function for weight gradients: the maps and the
+// lerp rows of each unweighted term, laid out like the weighted ones.  Maps
+// and tables are linear in the term weights, so a weighted map is the sum of
+// the term maps times their weights.
+constexpr int kMaxTerms = 6;
+struct TermData {
+    const float* maps;     // [term][slot][z][y][x]
+    const float4* rows;    // [term][tp][bin] = (e, dor) of the bin and the next, as Tables::smooth4
+    int n_terms;
+    long long map_block;   // floats per term in `maps`
+    long long row_block;   // float4 per term in `rows`
+};
+
+// Trilinear interpolation of one map at p, clamped to the box like grid_eval
+// (grid.cpp:40-129) but without curl or out-of-box penalty; `cell` and `frac`
+// cache the corner index and fractions for further maps of the same point.
+__device__ __forceinline__ void grid_cell(const Maps& M, const float* p, int& cell, float* frac) {
+    const int dims[3] = {M.nx, M.ny, M.nz};
+    int a[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float si = (p[i] - M.init[i]) * M.factor[i];
+        if (si < 0) {
+            a[i] = 0; si = 0;
+        } else if (si >= M.dim_m1[i]) {
+            a[i] = dims[i] - 2; si = 1;
+        } else {
+            a[i] = (int)si; si -= a[i];
+        }
+        frac[i] = si;
+    }
+    cell = a[0] + M.nx * (a[1] + M.ny * a[2]);
+}
+
+__device__ __forceinline__ float trilinear(const Maps& M, const float* g, int cell, const float* frac) {
+    const int sy = M.nx, sz = M.nx * M.ny;
+    const float x = frac[0], y = frac[1], z = frac[2];
+    const float mx = 1 - x, my = 1 - y, mz = 1 - z;
+    return __ldg(g + cell) * mx * my * mz + __ldg(g + cell + 1) * x * my * mz +
+           __ldg(g + cell + sy) * mx * y * mz + __ldg(g + cell + 1 + sy) * x * y * mz +
+           __ldg(g + cell + sz) * mx * my * z + __ldg(g + cell + 1 + sz) * x * my * z +
+           __ldg(g + cell + sy + sz) * mx * y * z + __ldg(g + cell + 1 + sy + sz) * x * y * z;
+}
+
+// d curl(e) / d e for curl(e) = e v / (v + e) when e > 0 (curl.h:28-43)
+__device__ __forceinline__ float curl_slope(float e, float v) {
+    if (!(e > 0) || !(v < 0.1f * kMaxFl)) return 1.0f;
+    const float t = (v < kEps) ? 0.0f : v / (v + e);
+    return t * t;
+}
+
+// Fixed poses, differentiation form: energy (caps v_intra / v_inter), its
+// gradient in the pose layout (d/dposition, d/dq, d/dtorsions; pair forces
+// exact or as the reference's tables give them, see eval_deriv) and, when
+// dw_out is set, its derivative with respect to each term weight.  The
+// conformer is recomputed from the pose (forward kinematics) rather than
+// stored.  The orientation gradient is 2 (0, tau) (x) q for the torque tau
+// of a rotation applied on the left (quaternion_increment, quaternion.h), the
+// gradient tangent to the unit sphere at a unit q.
+__global__ void __launch_bounds__(128) adjoint_kernel(
+    const __grid_constant__ Batch B, const __grid_constant__ Maps M, const __grid_constant__ Tables Tb,
+    const __grid_constant__ Layout L, const __grid_constant__ TermData TD, int n_ligands, const int* pose_lig,
+    const float* poses, int pose_stride, int n_poses, float v_intra, float v_inter, int exact, float* e_out,
+    float* g_out, int g_stride, float* dw_out, int dw_stride) {
+    extern __shared__ float smem[];
+    const int warp = threadIdx.x >> 5;
+    const int pose = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (pose >= n_poses) return;
+    const int lig = pose_lig[pose];
+    const int lane = threadIdx.x & 31;
+    if (lig < 0 || lig >= n_ligands) {  // refused pose: NaN outputs, no reads
+        if (lane == 0) e_out[pose] = __int_as_float(0x7fc00000);
+        return;
+    }
+    float* sw = smem + (size_t)warp * L.total;
+    const Ctx c = make_ctx(B, lig, sw);
+    float* x = sw + L.x;
+    const int cs = 7 + c.T;
+    for (int i = c.lane; i < cs; i += 32) x[i] = poses[(size_t)pose * pose_stride + i];
+    __syncwarp();
+    float* g = sw + L.g;
+    const float e = exact ? eval_deriv<true>(c, L, M, Tb, x, g, v_intra, v_inter)
+                          : eval_deriv<false>(c, L, M, Tb, x, g, v_intra, v_inter);
+    if (c.lane == 0) e_out[pose] = e;
+    if (g_out) {
+        float* go = g_out + (size_t)pose * g_stride;
+        if (c.lane == 0) {
+            const float t0 = g[3], t1 = g[4], t2 = g[5];
+            const float q0 = x[3], q1 = x[4], q2 = x[5], q3 = x[6];
+            go[0] = g[0]; go[1] = g[1]; go[2] = g[2];
+            go[3] = -2.0f * (t0 * q1 + t1 * q2 + t2 * q3);
+            go[4] = 2.0f * (q0 * t0 + (t1 * q3 - t2 * q2));
+            go[5] = 2.0f * (q0 * t1 + (t2 * q1 - t0 * q3));
+            go[6] = 2.0f * (q0 * t2 + (t0 * q2 - t1 * q1));
+        }
+        for (int i = c.lane; i < c.T; i += 32) go[7 + i] = g[6 + i];
+    }
+    if (dw_out) {
+        float acc[kMaxTerms];
+#pragma unroll
+        for (int t = 0; t < kMaxTerms; ++t) acc[t] = 0;
+        const float* xyz = sw + L.coords;  // conformer of the evaluation above
+        const size_t plane = (size_t)M.nx * M.ny * M.nz;
+        for (int k = c.lane; k < c.n_grid; k += 32) {
+            const uint32_t ga = __ldg(c.grid + k);
+            const int a = ga & 0xFF, slot = ga >> 8;
+            int cell;
+            float frac[3];
+            grid_cell(M, xyz + 3 * a, cell, frac);
+            const float w = curl_slope(trilinear(M, M.data + slot * plane, cell, frac), v_inter);
+#pragma unroll
+            for (int t = 0; t < kMaxTerms; ++t)
+                if (t < TD.n_terms) acc[t] += w * trilinear(M, TD.maps + t * TD.map_block + slot * plane, cell, frac);
+        }
+        for (int k = c.lane; k < c.n_pairs; k += 32) {
+            const uint32_t pr = __ldg(c.pairs + k);
+            if (pr == kPairPad) continue;
+            const int a = pr & 0xFF, b = (pr >> 8) & 0xFF, tp = pr >> 16;
+            const float rx = xyz[3 * b] - xyz[3 * a], ry = xyz[3 * b + 1] - xyz[3 * a + 1],
+                        rz = xyz[3 * b + 2] - xyz[3 * a + 2];
+            const float r2 = rx * rx + ry * ry + rz * rz;
+            if (!(r2 < Tb.cutoff2)) continue;
+            const float rf = Tb.factor * r2;
+            const int i1 = (int)rf;
+            const float rem = rf - i1;
+            const float4 row = __ldg(Tb.smooth4 + (size_t)tp * Tb.n_bins + i1);
+            const float w = curl_slope(row.x + rem * (row.z - row.x), v_intra);
+#pragma unroll
+            for (int t = 0; t < kMaxTerms; ++t)
+                if (t < TD.n_terms) {
+                    const float4 rt = __ldg(TD.rows + t * TD.row_block + (size_t)tp * Tb.n_bins + i1);
+                    acc[t] += w * (rt.x + rem * (rt.z - rt.x));
+                }
+        }
+#pragma unroll
+        for (int t = 0; t < kMaxTerms; ++t) acc[t] = warp_sum(acc[t]);
+        if (c.lane == 0)
+            for (int t = 0; t < TD.n_terms; ++t) dw_out[(size_t)pose * dw_stride + t] = acc[t];
+    }
+}
+
+// Weighted sum of per-term blocks: out[i] = sum_t w[t] * in[t * block + i]
+// (maps and tables from their unweighted terms, ud_maps_set_weights).
+struct TermWeights {
+    float w[kMaxTerms];
+};
+__global__ void combine_terms_kernel(const float4* __restrict__ in, long long block4, int n_terms,
+                                     const __grid_constant__ TermWeights W, float4* __restrict__ out,
+                                     long long n4) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4;
+         i += (long long)gridDim.x * blockDim.x) {
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int t = 0; t < n_terms; ++t) {
+            const float4 v = __ldg(in + t * block4 + i);
+            const float wt = W.w[t];
+            acc.x += wt * v.x; acc.y += wt * v.y; acc.z += wt * v.z; acc.w += wt * v.w;
+        }
+        out[i] = acc;
+    }
+}
+
 // FP32 issue-rate probe: independent FMA chains, used to report the FP32
 // roofline denominator measured on the running GPU.
 __global__ void fp32_peak_kernel(float* out, int iters) {
@@ -1122,29 +1288,8 @@ __global__ void __launch_bounds__(kMapThreads) maps_kernel(
 }  // namespace dev
 
 // ---------------------------------------------------------------- host side
-// Launch helpers called from the C-ABI layer (ud_capi.cpp).
-
-struct DeviceBatchView {
-    const LigDesc* ligs;
-    const AtomRec* atoms;
-    const NodeRec* nodes;
-    const uint32_t* pairs;
-    const uint32_t* grid_list;
-    int max_atoms, max_torsions;
-};
-
-struct DeviceMapsView {
-    const float* data;
-    MapsDesc desc;
-};
-
-struct DeviceTablesView {
-    const float* smooth;   // float4 per bin
-    const float* fast;
-    int n_bins;
-    float factor;
-    float cutoff2;
-};
+// Launch helpers called from the C-ABI layer (ud_capi.cpp), declared in
+// ud_engine.h with the device views they take.
 
 static dev::Maps to_maps(const DeviceMapsView& m) {
     dev::Maps M;
@@ -1218,6 +1363,48 @@ cudaError_t launch_score(const DeviceBatchView& b, const DeviceMapsView& m,
                                                           pose_lig, poses, pose_stride, n_poses,
                                                           v_intra, v_inter, e_out, g_out, g_stride,
                                                           score_out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
+                           const DeviceTermsView& terms, int n_ligands, const int* pose_lig, const float* poses,
+                           int pose_stride, int n_poses, float v_intra, float v_inter, int exact, float* e_out,
+                           float* g_out, int g_stride, float* dw_out, int dw_stride, cudaStream_t stream) {
+    if (terms.n_terms > dev::kMaxTerms) return cudaErrorInvalidValue;
+    dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
+    const int warps = 4;
+    size_t smem = (size_t)warps * L.total * sizeof(float);
+    cudaError_t e = smem_attr((const void*)dev::adjoint_kernel, smem);
+    if (e != cudaSuccess) return e;
+    dev::TermData TD;
+    TD.maps = terms.maps;
+    TD.rows = reinterpret_cast<const float4*>(terms.rows);
+    TD.n_terms = terms.n_terms;
+    TD.map_block = terms.map_block;
+    TD.row_block = terms.row_block;
+    dim3 grid((n_poses + warps - 1) / warps);
+    dev::adjoint_kernel<<<grid, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t), L, TD,
+                                                            n_ligands, pose_lig, poses, pose_stride, n_poses,
+                                                            v_intra, v_inter, exact, e_out, g_out, g_stride, dw_out,
+                                                            dw_stride);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_combine_terms(const float* in, long long block, int n_terms, const float* w, float* out,
+                                 cudaStream_t stream) {
+    if (n_terms < 1 || n_terms > dev::kMaxTerms || (block & 3) != 0) return cudaErrorInvalidValue;
+    if ((reinterpret_cast<uintptr_t>(in) & 15) != 0 || (reinterpret_cast<uintptr_t>(out) & 15) != 0)
+        return cudaErrorMisalignedAddress;
+    dev::TermWeights W{};
+    for (int t = 0; t < n_terms; ++t) W.w[t] = w[t];
+    const long long n4 = block / 4;
+    int dev_id = 0, n_sm = 148;
+    cudaGetDevice(&dev_id);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev_id);
+    const long long want = (n4 + 255) / 256;
+    const int blocks = (int)std::max<long long>(1, std::min<long long>(want, (long long)n_sm * 8));
+    dev::combine_terms_kernel<<<blocks, 256, 0, stream>>>(reinterpret_cast<const float4*>(in), n4, n_terms, W,
+                                                         reinterpret_cast<float4*>(out), n4);
     return cudaGetLastError();
 }
 

@@ -1,7 +1,9 @@
 // Device-side data layout of the docking engine and the host entry points
-// into ud_engine.cu.  Plain C++ (no CUDA types) so the C-ABI layer and the
-// host model code can include it.
+// into ud_engine.cu.  Host C++ (CUDA runtime types only) so the C-ABI layer
+// and the host model code can include it.
 #pragma once
+#include <cuda_runtime.h>
+
 #include <cstddef>
 #include <cstdint>
 #include <vector>
@@ -84,5 +86,68 @@ struct ChainResult {
     int ligand;
     int chain;
 };
+
+// ---------------------------------------------------------------- device views
+// Device pointers of one batch, one set of maps, the scoring tables and the
+// per-term data of weight gradients, as handed to the launchers below.
+struct DeviceBatchView {
+    const LigDesc* ligs;
+    const AtomRec* atoms;
+    const NodeRec* nodes;
+    const uint32_t* pairs;
+    const uint32_t* grid_list;
+    int max_atoms, max_torsions;
+};
+
+struct DeviceMapsView {
+    const float* data;
+    MapsDesc desc;
+};
+
+struct DeviceTablesView {
+    const float* smooth;   // float4 per bin: (e, dor) of the bin and the next
+    const float* fast;
+    int n_bins;
+    float factor;
+    float cutoff2;
+};
+
+struct DeviceTermsView {
+    const float* maps;     // [term][slot][z][y][x], unweighted term maps
+    const float* rows;     // float4 per bin: [term][tp][bin], laid out as DeviceTablesView::smooth
+    int n_terms;
+    long long map_block;   // floats per term in `maps`
+    long long row_block;   // float4 per term in `rows`
+};
+
+// ---------------------------------------------------------------- launchers (ud_engine.cu)
+cudaError_t launch_maps(const float* rec_xyzt, int n_rec, const float* fastT, int n_bins, int n_slots,
+                        int n_slots_pad, float factor, float cutoff2, const MapsDesc& d, float* out,
+                        cudaStream_t stream);
+cudaError_t launch_score(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
+                         const int* pose_lig, const float* poses, int pose_stride, int n_poses,
+                         float v_intra, float v_inter, float* e_out, float* g_out, int g_stride,
+                         float* score_out, cudaStream_t stream);
+cudaError_t launch_adjoint(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
+                           const DeviceTermsView& terms, int n_ligands, const int* pose_lig, const float* poses,
+                           int pose_stride, int n_poses, float v_intra, float v_inter, int exact, float* e_out,
+                           float* g_out, int g_stride, float* dw_out, int dw_stride, cudaStream_t stream);
+// out[i] = sum_t w[t] * in[t * block + i], i < block (a multiple of 4, 16-byte aligned buffers)
+cudaError_t launch_combine_terms(const float* in, long long block, int n_terms, const float* w, float* out,
+                                 cudaStream_t stream);
+cudaError_t launch_search(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
+                          const SearchParams& P, const int* order, int n_items, int first_item,
+                          unsigned int* queue, float* poses, int pose_stride, ChainResult* results,
+                          int grid_blocks, cudaStream_t stream);
+int search_blocks_per_sm(const DeviceBatchView& b, int warps);
+cudaError_t launch_optimize(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
+                            const int* pose_lig, float* poses, int pose_stride, int n_poses, int max_steps,
+                            float v, float* e_out, int* evals_out, cudaStream_t stream);
+float measure_fp32_peak_tflops();
+cudaError_t launch_search_noalloc(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
+                                  const SearchParams& P, const int* h_order, int n_ligands, int grid_blocks,
+                                  float* poses, int pose_stride, float* e_out, int* evals_out,
+                                  cudaStream_t stream);
+int engine_chain_smem_bytes(int max_atoms, int max_torsions);
 
 }  // namespace ud

@@ -19,9 +19,19 @@ LIB_PATH = Path(os.environ.get("UNIDOCK_B200_LIB", PKG_ROOT / "lib" / "libunidoc
 
 SF_VINA, SF_AD4, SF_VINARDO = 0, 1, 2
 UD_OK = 0
+UD_ADJOINT_EXACT = 1
 UD_ERR_ARG, UD_ERR_PARSE, UD_ERR_CUDA, UD_ERR_CAPACITY, UD_ERR_STATE = 1, 2, 3, 4, 5
 
 _lib = None
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("chains_per_block", C.c_int), ("lanes_per_chain", C.c_int), ("bfgs_cap", C.c_int),
+                ("n_sample", C.c_int), ("n_tried", C.c_int), ("ligands_per_s", C.c_float),
+                ("base_ligands_per_s", C.c_float), ("energy_shift", C.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class UdError(RuntimeError):
@@ -88,6 +98,14 @@ def lib():
         "ud_search_stats": ([vp, C.POINTER(C.c_longlong), fp], C.c_int),
         "ud_optimize": ([vp, ip, fp, C.c_int, C.c_int, C.c_int, C.c_float, fp, ip, vp], C.c_int),
         "ud_device_fp32_peak": ([fp], C.c_int),
+        "ud_maps_term_count": ([vp, ip], C.c_int),
+        "ud_autotune": ([vp, C.POINTER(SearchParams), C.POINTER(TuneResult), vp], C.c_int),
+        "ud_maps_get_weights": ([vp, fp, C.c_int], C.c_int),
+        "ud_maps_set_weights": ([vp, fp, C.c_int, vp], C.c_int),
+        "ud_score_adjoint": ([vp, ip, fp, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, fp, fp, C.c_int, fp,
+                              C.c_int, vp], C.c_int),
+        "ud_score_adjoint_device": ([vp, vp, vp, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, vp, vp, C.c_int,
+                                     vp, C.c_int, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -160,6 +178,23 @@ class Maps:
         n = C.c_int()
         _check(lib().ud_maps_info(self.h, _i(d), _f(init), _f(fac), C.byref(n)))
         return d, init, fac, n.value
+
+    @property
+    def n_terms(self):
+        n = C.c_int()
+        _check(lib().ud_maps_term_count(self.h, C.byref(n)))
+        return n.value
+
+    def weights(self):
+        """Current term weights (reference order; no rotatable weight)."""
+        w = np.zeros(self.n_terms, np.float32)
+        _check(lib().ud_maps_get_weights(self.h, _f(w), len(w)))
+        return w
+
+    def set_weights(self, w, stream=None):
+        """Recombine maps and tables for new term weights on the GPU (ud_maps_set_weights)."""
+        w = np.ascontiguousarray(w, np.float32)
+        _check(lib().ud_maps_set_weights(self.h, _f(w), len(w), C.c_void_p(stream) if stream else None))
 
     def read(self, xs):
         d, _, _, _ = self.info()
@@ -254,6 +289,31 @@ class Batch:
                                           float(v_intra), float(v_inter), C.c_void_p(e_ptr), C.c_void_p(g_ptr),
                                           g_stride, C.c_void_p(stream) if stream else None))
 
+    def score_adjoint(self, pose_ligand, poses, v_intra=1000.0, v_inter=1000.0, exact=True, weights_grad=True):
+        """Energy, pose-layout gradient (7 + T_max per pose) and term-weight
+        gradient at fixed poses (ud_score_adjoint), host arrays."""
+        pose_ligand = np.ascontiguousarray(pose_ligand, np.int32)
+        poses = np.ascontiguousarray(poses, np.float32)
+        n, stride = poses.shape
+        gs = 7 + self.max_torsions
+        nt = self.maps.n_terms
+        e = np.zeros(n, np.float32)
+        g = np.zeros((n, gs), np.float32)
+        dw = np.zeros((n, nt), np.float32) if weights_grad else None
+        _check(lib().ud_score_adjoint(self.h, _i(pose_ligand), _f(poses), n, stride, float(v_intra), float(v_inter),
+                                      UD_ADJOINT_EXACT if exact else 0, _f(e), _f(g), gs,
+                                      _f(dw) if weights_grad else None, nt, None))
+        return e, g, dw
+
+    def score_adjoint_device(self, pose_ligand_ptr, poses_ptr, n, stride, e_ptr, g_ptr=0, g_stride=0, dw_ptr=0,
+                             dw_stride=0, v_intra=1000.0, v_inter=1000.0, exact=True, stream=0):
+        """Device-pointer form of score_adjoint (raw addresses as ints; 0 = not wanted)."""
+        _check(lib().ud_score_adjoint_device(self.h, C.c_void_p(pose_ligand_ptr), C.c_void_p(poses_ptr), n, stride,
+                                             float(v_intra), float(v_inter), UD_ADJOINT_EXACT if exact else 0,
+                                             C.c_void_p(e_ptr), C.c_void_p(g_ptr) if g_ptr else None, g_stride,
+                                             C.c_void_p(dw_ptr) if dw_ptr else None, dw_stride,
+                                             C.c_void_p(stream) if stream else None))
+
     def score(self, pose_ligand, poses, v=1000.0):
         pose_ligand = np.ascontiguousarray(pose_ligand, np.int32)
         poses = np.ascontiguousarray(poses, np.float32)
@@ -289,6 +349,14 @@ class Batch:
         _check(lib().ud_search_device_noalloc(self.h, C.byref(p), C.c_void_p(d_poses), int(pose_stride),
                                               C.c_void_p(d_energies), C.c_void_p(d_evals) if d_evals else None,
                                               C.c_void_p(stream) if stream else None))
+
+    def autotune(self, exhaustiveness=8, max_step=0, seed=0):
+        """Pick chains-per-CTA and the BFGS cap for this batch (ud_autotune);
+        searches with chains_per_block=0 and bfgs_cap=-1 then use them."""
+        p = SearchParams(exhaustiveness, max_step, 9, 1.0, 3.0, seed, 1, 0, 0, 0)
+        r = TuneResult()
+        _check(lib().ud_autotune(self.h, C.byref(p), C.byref(r), None))
+        return r.as_dict()
 
     def search_collect(self):
         _check(lib().ud_search_collect(self.h, None))
