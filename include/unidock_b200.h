@@ -117,6 +117,15 @@ int ud_score_grad_device(ud_batch batch, const int* pose_ligand, const float* po
 int ud_score(ud_batch batch, const int* pose_ligand, const float* poses, int n_poses,
              int pose_stride, float v, float* out, void* stream);
 
+/* Score of fixed poses as Vina::score reports it (vina.cpp:1168-1240,
+ * rigid receptor): 8 floats per pose = {estimated free energy of binding,
+ * ligand-receptor, ligand-flex (0), flex-receptor (0), flex-flex (0), ligand
+ * intramolecular, torsional (conf-independent) term, unbound system's energy
+ * (the pose's own intramolecular energy)}.  Used by --score_only and
+ * --local_only. */
+int ud_score_terms(ud_batch batch, const int* pose_ligand, const float* poses, int n_poses, int pose_stride,
+                   float* out, void* stream);
+
 /* ---------------------------------------------------------------- differentiation
  * No counterpart in the reference (its gradient is internal to BFGS).
  *

@@ -14,6 +14,18 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200)")
 
 
+def pytest_sessionstart(session):
+    """Build the engine library, the CLI and the oracle libraries when a fresh
+    checkout lacks them (nvcc cross-compiles for sm_100a without a GPU)."""
+    import subprocess
+    need = [ROOT / "uni-dock_b200" / "lib" / "libunidock_b200.so", ROOT / "uni-dock_b200" / "bin" / "unidock",
+            ROOT / "oracle" / "_ref" / "liboracle32.so", ROOT / "oracle" / "_ref" / "liboracle64.so"]
+    if all(x.exists() for x in need):
+        return
+    for d in ("uni-dock_b200", "oracle"):
+        subprocess.run(["make", "-C", str(ROOT / d)], check=True, stdout=subprocess.DEVNULL)
+
+
 def has_gpu():
     try:
         import torch

@@ -1,0 +1,127 @@
+"""The unidock command-line host: the reference's option surface and argument
+checks (no GPU needed), and on the GPU a batch docking run that writes one
+`<ligand>_out.pdbqt` per input ligand in --dir, a single-ligand run with the
+default output name, and --score_only / --local_only."""
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from unidock_tools import synth
+
+ROOT = Path(__file__).resolve().parent.parent
+BIN = ROOT / "uni-dock_b200" / "bin" / "unidock"
+
+# option names of the reference CLI (unidock/src/main/main.cpp:421-575)
+REFERENCE_OPTIONS = [
+    "receptor", "flex", "ligand", "ligand_index", "paired_batch_size", "batch", "gpu_batch", "scoring", "maps",
+    "center_x", "center_y", "center_z", "size_x", "size_y", "size_z", "autobox", "out", "dir", "write_maps",
+    "device_id", "score_only", "score_file", "local_only", "no_refine", "force_even_voxels", "randomize_only",
+    "weight_gauss1", "weight_gauss2", "weight_repulsion", "weight_hydrophobic", "weight_hydrogen", "weight_rot",
+    "weight_vinardo_gauss1", "weight_vinardo_repulsion", "weight_vinardo_hydrophobic", "weight_vinardo_hydrogen",
+    "weight_vinardo_rot", "weight_ad4_vdw", "weight_ad4_hb", "weight_ad4_elec", "weight_ad4_dsolv",
+    "weight_ad4_rot", "weight_glue", "bias", "multi_bias", "keep_nonpolar_H", "cpu", "seed", "exhaustiveness",
+    "max_evals", "num_modes", "min_rmsd", "energy_range", "spacing", "verbosity", "max_step", "refine_step",
+    "max_gpu_memory", "search_mode", "config", "help", "help_advanced", "version"]
+
+
+def run(*args, cwd=None):
+    return subprocess.run([str(BIN), *map(str, args)], capture_output=True, text=True, cwd=cwd, timeout=600)
+
+
+def test_help_lists_every_reference_option():
+    r = run("--help_advanced")
+    assert r.returncode == 0
+    for name in REFERENCE_OPTIONS:
+        assert f"--{name} " in r.stdout, name
+
+
+@pytest.mark.parametrize("args,msg", [
+    (["--receptor", "r.pdbqt"], "Missing ligand(s)."),
+    (["--receptor", "r.pdbqt", "--gpu_batch", "a.pdbqt"], "Need to specify an output directory for batch mode."),
+    (["--receptor", "r.pdbqt", "--gpu_batch", "a.pdbqt", "--dir", "/nonexistent_dir_x"], "does not exist"),
+    (["--receptor", "r.pdbqt", "--ligand", "a.pdbqt", "--scoring", "xyz"], "Scoring function xyz unknown."),
+    (["--ligand", "a.pdbqt"], "The receptor or affinity maps must be specified."),
+    (["--bogus", "1"], "unrecognised option '--bogus'"),
+    (["--receptor", "r.pdbqt", "--ligand", "a.pdbqt", "--gpu_batch", "b.pdbqt", "--dir", "."],
+     "Can't use both --ligand and --batch arguments simultaneously."),
+    (["--receptor", "r.pdbqt", "--ligand", "a.pdbqt", "--search_mode", "slow"], "unknown search_mode"),
+])
+def test_argument_errors(args, msg):
+    r = run(*args)
+    assert r.returncode != 0
+    assert msg in r.stderr, r.stderr
+
+
+def box_args(size=22.5):
+    return ["--center_x", 0, "--center_y", 0, "--center_z", 0, "--size_x", size, "--size_y", size, "--size_z", size]
+
+
+@pytest.fixture(scope="module")
+def inputs(tmp_path_factory, receptor):
+    d = tmp_path_factory.mktemp("cli")
+    (d / "rec.pdbqt").write_text(receptor.to_pdbqt())
+    names = []
+    for k, L in enumerate(synth.ligand_set(6, seed=77, heavy=(12, 30), torsions=(0, 6))):
+        p = d / f"lig{k}.pdbqt"
+        p.write_text(L.to_pdbqt())
+        names.append(p)
+    (d / "out").mkdir()
+    return d, names
+
+
+@pytest.mark.gpu
+def test_batch_docking_writes_one_output_per_ligand(inputs):
+    d, names = inputs
+    idx = d / "index.txt"
+    idx.write_text("\n".join(str(p) for p in names[3:]) + "\n")
+    r = run("--receptor", d / "rec.pdbqt", "--gpu_batch", *names[:3], "--ligand_index", idx, "--dir", d / "out",
+            "--search_mode", "fast", "--seed", 3, "--num_modes", 5, "--batch_size", 4, *box_args())
+    assert r.returncode == 0, r.stderr
+    assert "Batch 1 size: 4" in r.stdout and "Batch 2 size: 2" in r.stdout
+    for p in names:
+        out = d / "out" / (p.stem + "_out.pdbqt")
+        text = out.read_text()
+        assert text.startswith("MODEL 1\nREMARK VINA RESULT:")
+        assert 1 <= text.count("ENDMDL") <= 5
+        e = [float(l.split()[3]) for l in text.splitlines() if l.startswith("REMARK VINA RESULT:")]
+        assert e == sorted(e) and e[-1] <= e[0] + 3.0 + 1e-6
+
+
+@pytest.mark.gpu
+def test_single_ligand_default_output_and_modes_table(inputs):
+    d, names = inputs
+    r = run("--receptor", d / "rec.pdbqt", "--ligand", names[0], "--exhaustiveness", 8, "--max_step", 10,
+            "--seed", 1, *box_args())
+    assert r.returncode == 0, r.stderr
+    assert "mode |   affinity | dist from best mode" in r.stdout
+    out = names[0].with_name(names[0].stem + "_out.pdbqt")
+    assert out.read_text().startswith("MODEL 1\nREMARK VINA RESULT:")
+
+
+@pytest.mark.gpu
+def test_score_only_and_local_only(inputs):
+    d, names = inputs
+    r = run("--receptor", d / "rec.pdbqt", "--ligand", names[1], "--score_only", *box_args())
+    assert r.returncode == 0, r.stderr
+    assert "Estimated Free Energy of Binding" in r.stdout
+    score = names[1].with_name(names[1].stem + "_score.txt").read_text()
+    assert score.startswith(f"REMARK {names[1].name} ")
+    assert np.isfinite(float(score.split()[2]))
+    out = d / "local.pdbqt"
+    r = run("--receptor", d / "rec.pdbqt", "--ligand", names[1], "--local_only", "--out", out, *box_args())
+    assert r.returncode == 0, r.stderr
+    # the input structure with new coordinates, line for line
+    src, dst = names[1].read_text().splitlines(), out.read_text().splitlines()
+    assert len(src) == len(dst)
+    moved = 0
+    for a, b in zip(src, dst):
+        if a.startswith(("ATOM", "HETATM")):
+            assert a[:30] == b[:30] and a[54:] == b[54:]
+            moved += a[30:54] != b[30:54]
+        else:
+            assert a == b
+    assert moved > 0
+    r = run("--receptor", d / "rec.pdbqt", "--ligand", names[1], "--score_only", "--autobox")
+    assert r.returncode == 0, r.stderr

@@ -680,6 +680,39 @@ extern "C" int ud_score(ud_batch b, const int* pose_ligand, const float* poses, 
     });
 }
 
+// Vina::score of fixed poses (vina.cpp:1168-1240) for a rigid receptor: per
+// pose {total, ligand-receptor, ligand-flex, flex-receptor, flex-flex intra,
+// ligand intra, conf-independent, unbound}; the unbound energy is the pose's
+// own intramolecular energy (Vina::score, vina.cpp:1329-1355).
+extern "C" int ud_score_terms(ud_batch b, const int* pose_ligand, const float* poses, int n_poses, int pose_stride,
+                              float* out, void* stream) {
+    return guarded([&] {
+        check_poses(b, pose_ligand, n_poses, pose_stride);
+        if (!poses || !out) throw Error(UD_ERR_ARG, "null buffer");
+        for (int i = 0; i < n_poses; ++i)
+            if (pose_ligand[i] < 0 || pose_ligand[i] >= (int)b->desc.size())
+                throw Error(UD_ERR_ARG, "pose_ligand out of range");
+        std::vector<int> l(pose_ligand, pose_ligand + n_poses);
+        std::vector<float> p(poses, poses + (size_t)n_poses * pose_stride), sc;
+        score_poses_device(b, l, p, pose_stride, 1000.0f, sc, (cudaStream_t)stream);
+        const Scoring& sf = b->maps->sf;
+        for (int i = 0; i < n_poses; ++i) {
+            const Ligand& L = *b->ligs[pose_ligand[i]];
+            const float grid = sc[2 * i], intra = sc[2 * i + 1];
+            const float total = sf.conf_independent(grid + intra - intra, L.conf_indep_inputs()[0], (float)L.torsdof);
+            float* o = out + 8 * (size_t)i;
+            o[0] = total;
+            o[1] = grid;
+            o[2] = 0.0f;
+            o[3] = 0.0f;
+            o[4] = 0.0f;
+            o[5] = intra;
+            o[6] = total - grid;
+            o[7] = intra;
+        }
+    });
+}
+
 // ---------------------------------------------------------------- adjoint
 
 // Unweighted per-term maps and tables of the maps' scoring function: the
