@@ -46,6 +46,11 @@ const char* ud_last_error(void);
 int ud_receptor_parse(const char* pdbqt, size_t len, float* xyz, int* xs, int capacity,
                       int* n_atoms);
 
+/* Receptor parse with AutoDock types and partial charges as well (the inputs
+ * of AD4 maps); any output pointer may be NULL.  Untyped atoms get ad = 35. */
+int ud_receptor_parse_ex(const char* pdbqt, size_t len, float* xyz, int* xs, int* ad, float* charge,
+                         int capacity, int* n_atoms);
+
 /* ---------------------------------------------------------------- grid maps
  * Build grid maps on the GPU for the listed XS types (all 24 Vina map types
  * when types == NULL) over the box center +- size/2 at `spacing`.
@@ -57,10 +62,35 @@ int ud_receptor_parse(const char* pdbqt, size_t len, float* xyz, int* xs, int ca
 int ud_maps_create(int sf, const float* weights, int n_weights, const float* rec_xyz,
                    const int* rec_xs, int n_rec, const float center[3], const float size[3],
                    float spacing, const int* types, int n_types, void* stream, ud_maps* out);
+/* AutoDock 4.2 maps built on the GPU (the reference reads them from AutoGrid
+ * files instead, ad4cache::read, unidock/src/lib/ad4cache.cpp:391-437): one
+ * map per AD type of `types` (NULL = every AD kind a ligand atom can read; CG
+ * carbons read C), then the electrostatic map (per unit ligand charge) and the
+ * desolvation map (per unit |ligand charge|), the three ad4cache::eval_deriv
+ * combines (ad4cache.cpp:227-269).  Map values are the reference's AD4.2 pair
+ * terms (potentials.h:346-486, scoring_function.h:74-86) summed over receptor
+ * atoms at the exact probe distances.  Weights in the reference's order
+ * (vdW, H-bond, electrostatics, desolvation, glue, torsional -- the last raw,
+ * as ad4_tors_add uses it); NULL = defaults.  The box has an even number of
+ * voxels per axis, as AutoGrid maps do.  Replaces the external autogrid4 step. */
+int ud_maps_create_ad4(const float* weights, int n_weights, const float* rec_xyz, const int* rec_ad,
+                       const float* rec_q, int n_rec, const float center[3], const float size[3], float spacing,
+                       const int* types, int n_types, void* stream, ud_maps* out);
+/* Write the maps as AutoGrid .map text files <prefix>.<type>.map (AD4 maps:
+ * AD type names plus <prefix>.e.map and <prefix>.d.map; Vina maps: X-Score type
+ * names), header as ad4cache::write (ad4cache.cpp:439-521), values at full
+ * float precision.  --write_maps of the reference CLI. */
+int ud_maps_write(ud_maps maps, const char* prefix);
+/* Maps read from AutoGrid .map files <prefix>.<type>.map (the reference's
+ * --maps: cache::read, cache.cpp:325-379, for Vina / Vinardo by X-Score type
+ * names; ad4cache::read, ad4cache.cpp:391-437, for AD4 by AD type names plus
+ * the required .e.map and .d.map).  Weights as ud_maps_create / _ad4. */
+int ud_maps_load(int sf, const float* weights, int n_weights, const char* prefix, void* stream, ud_maps* out);
 /* dims[3] sample points, init[3] box corner, factor[3] samples per Angstrom. */
 int ud_maps_info(ud_maps maps, int dims[3], float init[3], float factor[3], int* n_maps);
 /* Copy the map of XS type `xs` to host memory (dims[0]*dims[1]*dims[2] floats,
- * x fastest).  Replaces igrid::get_grids (unidock/src/lib/igrid.h:39). */
+ * x fastest); for AD4 maps `xs` is an AD type, 35 the electrostatic and 36 the
+ * desolvation map.  Replaces igrid::get_grids (unidock/src/lib/igrid.h:39). */
 int ud_maps_read(ud_maps maps, int xs, float* out, size_t n);
 int ud_maps_destroy(ud_maps maps);
 
@@ -102,12 +132,14 @@ int ud_batch_destroy(ud_batch batch);
  * layout of ud_ligand_initial_pose; g_out receives 6 + T floats per pose in
  * the reference's change layout (d/dposition, torque, d/dtorsions) with
  * stride g_stride.  v_intra / v_inter are the curl caps of the intramolecular
- * and grid terms (1000 = scoring, 10 = search).  Replaces model::eval_deriv
+ * and grid terms (1000 = scoring, 10 = search); entries of g_out past a
+ * pose's 6 + T are set to 0.  Replaces model::eval_deriv
  * (unidock/src/lib/model.cpp:935-962). */
 int ud_score_grad(ud_batch batch, const int* pose_ligand, const float* poses, int n_poses,
                   int pose_stride, float v_intra, float v_inter, float* e_out, float* g_out,
                   int g_stride, void* stream);
-/* Same with device pointers; asynchronous on `stream`. */
+/* Same with device pointers; asynchronous on `stream`; entries of g_out past
+ * a pose's 6 + T are left as they are. */
 int ud_score_grad_device(ud_batch batch, const int* pose_ligand, const float* poses, int n_poses,
                          int pose_stride, float v_intra, float v_inter, float* e_out,
                          float* g_out, int g_stride, void* stream);

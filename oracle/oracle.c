@@ -488,3 +488,94 @@ real orc_bfgs(const orc_ligand* L, const orc_grid* G, const real* smooth, int nb
     free(H); free(g); free(gn); free(g0); free(p); free(y); free(mhy); free(xn); free(x0);
     return f0;
 }
+
+/* ------------------------------------------------------------ AutoDock 4.2
+ * unidock/src/lib/atom_constants.h:158-194 (ad_type_property: radius, depth,
+ * hb_depth, hb_radius, solvation, volume) and potentials.h:346-486 (terms),
+ * scoring_function.h:74-86 (smoothing 0.5, caps 100000 / 100, cutoffs 8 /
+ * 20.48, desolvation sigma 3.6 and charge factor 0.01097). */
+static const float ad_par[35][6] = {
+    {2.00f, 0.150f, 0.0f, 0.0f, -0.00143f, 33.51030f}, {2.00f, 0.150f, 0.0f, 0.0f, -0.00052f, 33.51030f},
+    {1.75f, 0.160f, 0.0f, 0.0f, -0.00162f, 22.44930f}, {1.60f, 0.200f, 0.0f, 0.0f, -0.00251f, 17.15730f},
+    {2.10f, 0.200f, 0.0f, 0.0f, -0.00110f, 38.79240f}, {2.00f, 0.200f, 0.0f, 0.0f, -0.00214f, 33.51030f},
+    {1.00f, 0.020f, 0.0f, 0.0f, 0.00051f, 0.00000f},   {1.545f, 0.080f, 0.0f, 0.0f, -0.00110f, 15.44800f},
+    {2.36f, 0.550f, 0.0f, 0.0f, -0.00110f, 55.05850f}, {1.75f, 0.160f, -5.0f, 1.9f, -0.00162f, 22.44930f},
+    {1.60f, 0.200f, -5.0f, 1.9f, -0.00251f, 17.15730f}, {2.00f, 0.200f, -1.0f, 2.5f, -0.00214f, 33.51030f},
+    {1.00f, 0.020f, 1.0f, 0.0f, 0.00051f, 0.00000f},   {0.65f, 0.875f, 0.0f, 0.0f, -0.00110f, 1.56000f},
+    {0.65f, 0.875f, 0.0f, 0.0f, -0.00110f, 2.14000f},  {0.74f, 0.550f, 0.0f, 0.0f, -0.00110f, 1.70000f},
+    {0.99f, 0.550f, 0.0f, 0.0f, -0.00110f, 2.77000f},  {0.65f, 0.010f, 0.0f, 0.0f, -0.00110f, 1.84000f},
+    {2.045f, 0.276f, 0.0f, 0.0f, -0.00110f, 35.82350f}, {2.165f, 0.389f, 0.0f, 0.0f, -0.00110f, 42.56610f},
+    {2.30f, 0.200f, 0.0f, 0.0f, -0.00143f, 50.96500f}, {2.40f, 0.550f, 0.0f, 0.0f, -0.00110f, 57.90580f},
+    {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+    {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+    {2.00f, 0.150f, 0.0f, 0.0f, -0.00143f, 33.51030f}, {2.00f, 0.150f, 0.0f, 0.0f, -0.00143f, 33.51030f},
+    {2.00f, 0.150f, 0.0f, 0.0f, -0.00143f, 33.51030f}, {2.00f, 0.150f, 0.0f, 0.0f, -0.00143f, 33.51030f},
+    {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+    {1.60f, 0.200f, 0.0f, 0.0f, -0.00251f, 17.15730f}, {1.75f, 0.160f, 0.0f, 0.0f, -0.00162f, 22.44930f},
+    {1.60f, 0.200f, 0.0f, 0.0f, -0.00251f, 17.15730f}, {1.75f, 0.160f, 0.0f, 0.0f, -0.00162f, 22.44930f}};
+
+static real ipow_r(real x, int n) {
+    real p = 1;
+    for (int i = 0; i < n; ++i) p = p * x;
+    return p;
+}
+
+static real ad4_smooth(real r, real rij) {  /* potentials.h smoothen, smoothing 0.5 */
+    const real h = (real)0.25;
+    if (r > rij + h) return r - h;
+    if (r < rij - h) return r + h;
+    return rij;
+}
+
+real orc_ad4_pair(int t1, real q1, int t2, real q2, real r, const double* w) {
+    real e = 0;
+    const real cap = (real)100000;
+    /* vdW 12-6 / H-bond 12-10, cutoff 8 */
+    if (r < 8) {
+        const real hbd = (real)ad_par[t1][2] * (real)ad_par[t2][2];
+        if (hbd >= 0) {
+            const real rij = (real)ad_par[t1][0] + (real)ad_par[t2][0];
+            const real depth = RX(sqrt)((real)ad_par[t1][1] * (real)ad_par[t2][1]);
+            const real rs = ad4_smooth(r, rij);
+            const real c12 = ipow_r(rij, 12) * depth, c6 = ipow_r(rij, 6) * depth * 2;
+            const real r6 = ipow_r(rs, 6), r12 = ipow_r(rs, 12);
+            const real v = (r12 > EPS_R && r6 > EPS_R) ? (c12 / r12 - c6 / r6 < cap ? c12 / r12 - c6 / r6 : cap) : cap;
+            e += (real)(float)w[0] * v;
+        } else {
+            const real rij = (real)ad_par[t1][3] + (real)ad_par[t2][3];
+            const real rs = ad4_smooth(r, rij);
+            const real c12 = ipow_r(rij, 12) * -hbd * 10 / 2, c10 = ipow_r(rij, 10) * -hbd * 12 / 2;
+            const real r10 = ipow_r(rs, 10), r12 = ipow_r(rs, 12);
+            const real v = (r12 > EPS_R && r10 > EPS_R) ? (c12 / r12 - c10 / r10 < cap ? c12 / r12 - c10 / r10 : cap)
+                                                        : cap;
+            e += (real)(float)w[1] * v;
+        }
+    }
+    if (r < (real)20.48) {
+        /* electrostatics, distance-dependent dielectric, cap 100 */
+        const real B = (real)(78.4 + 8.5525);
+        const real lB = -B * (real)0.003627;
+        const real diel = (real)-8.5525 + B / (1 + (real)7.7839 * RX(exp)(lB * r));
+        const real inv = r < EPS_R ? (real)100 / diel : ((real)1 / (r * diel) < 100 ? (real)1 / (r * diel) : (real)100);
+        e += (real)(float)w[2] * (q1 * q2 * 332 * inv);
+        /* desolvation */
+        const real k = (real)0.01097, x = r / (real)3.6;
+        const real g = RX(exp)((real)-0.5 * x * x);
+        const real s1 = (real)ad_par[t1][4], s2 = (real)ad_par[t2][4], v1 = (real)ad_par[t1][5], v2 = (real)ad_par[t2][5];
+        const real aq1 = q1 < 0 ? -q1 : q1, aq2 = q2 < 0 ? -q2 : q2;
+        e += (real)(float)w[3] * (((s1 + k * aq1) * v2 + (s2 + k * aq2) * v1) * g);
+    }
+    return e;
+}
+
+real orc_ad4_probe(const real* rx, const int* rad, const real* rq, int n, const real* p, int probe_ad, real probe_q,
+                   const double* w) {
+    real acc = 0;
+    for (int i = 0; i < n; ++i) {
+        const real dx = rx[3 * i] - p[0], dy = rx[3 * i + 1] - p[1], dz = rx[3 * i + 2] - p[2];
+        const real r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 >= (real)20.48 * (real)20.48) continue;
+        acc += orc_ad4_pair(probe_ad, probe_q, rad[i], rq[i], RX(sqrt)(r2), w);
+    }
+    return acc;
+}

@@ -10,6 +10,13 @@
 
 #ifndef ORACLE_REAL
 #define ORACLE_REAL float
+/* AutoDock 4.2: weighted pair energy of two AD-typed atoms with charges
+ * (w = vdW, H-bond, electrostatics, desolvation, glue), and the energy of a
+ * probe atom against receptor atoms within the 20.48 A cutoff. */
+real orc_ad4_pair(int t1, real q1, int t2, real q2, real r, const double* w);
+real orc_ad4_probe(const real* rec_xyz, const int* rec_ad, const real* rec_q, int n_rec, const real* p,
+                   int probe_ad, real probe_q, const double* w);
+
 #endif
 typedef ORACLE_REAL real;
 
@@ -54,5 +61,12 @@ void orc_eval_score(const orc_ligand* L, const orc_grid* G, const real* fast, in
 /* BFGS local optimisation from `pose` (updated); returns the energy. */
 real orc_bfgs(const orc_ligand* L, const orc_grid* G, const real* smooth, int n_bins, real* pose,
               int max_steps, real v, int* evals);
+
+/* AutoDock 4.2: weighted pair energy of two AD-typed atoms with charges
+ * (w = vdW, H-bond, electrostatics, desolvation, glue), and the energy of a
+ * probe atom against receptor atoms within the 20.48 A cutoff. */
+real orc_ad4_pair(int t1, real q1, int t2, real q2, real r, const double* w);
+real orc_ad4_probe(const real* rec_xyz, const int* rec_ad, const real* rec_q, int n_rec, const real* p,
+                   int probe_ad, real probe_q, const double* w);
 
 #endif

@@ -18,9 +18,12 @@ VINA_W = np.array([-0.035579, -0.005156, 0.840245, -0.035069, -0.587439, 50, 5 *
 VINARDO_W = np.array([-0.045, 0.8, -0.035, -0.600, 50, 5 * 0.05846 / 0.1 - 1], np.float32).astype(np.float64)
 
 
+AD4_W = np.array([0.1662, 0.1209, 0.1406, 0.1322, 50, 0.2983], np.float32).astype(np.float64)
+
+
 def default_weights(sf):
     """Default weights of the scoring function (unidock/src/main/main.cpp:373-395)."""
-    return {0: VINA_W, 2: VINARDO_W}[sf]
+    return {0: VINA_W, 1: AD4_W, 2: VINARDO_W}[sf]
 
 
 class _Lig(C.Structure):
@@ -57,6 +60,10 @@ class Oracle:
             L.orc_eval_score.argtypes = [vp, vp, vp, C.c_int, vp, rt, vp]
             L.orc_bfgs.argtypes = [vp, vp, vp, C.c_int, vp, C.c_int, rt, ip]
             L.orc_bfgs.restype = rt
+            L.orc_ad4_pair.argtypes = [C.c_int, rt, C.c_int, rt, rt, dp]
+            L.orc_ad4_pair.restype = rt
+            L.orc_ad4_probe.argtypes = [vp, vp, vp, C.c_int, vp, C.c_int, rt, dp]
+            L.orc_ad4_probe.restype = rt
             _libs[name] = L
         self.L = _libs[name]
         self.Grid = _grid_struct(self.real)
@@ -156,3 +163,25 @@ class Oracle:
         e = self.L.orc_bfgs(C.byref(lig), C.byref(grid), smooth.ctypes.data, smooth.shape[1], x.ctypes.data,
                             max_steps, v, C.byref(ev))
         return float(e), x, ev.value
+
+
+def _ad4_weights(weights):
+    return np.ascontiguousarray(AD4_W if weights is None else weights, np.float64)
+
+
+def ad4_pair(oracle, t1, q1, t2, q2, r, weights=None):
+    """AD4.2 pair energy of two AD-typed atoms (weights: vdW, H-bond, elec, desolv, glue)."""
+    w = _ad4_weights(weights)
+    return float(oracle.L.orc_ad4_pair(int(t1), float(q1), int(t2), float(q2), float(r),
+                                       w.ctypes.data_as(C.POINTER(C.c_double))))
+
+
+def ad4_probe(oracle, rec_xyz, rec_ad, rec_q, p, probe_ad, probe_q, weights=None):
+    """Energy of a probe atom at p against every receptor atom within 20.48 A."""
+    w = _ad4_weights(weights)
+    xyz = oracle._a(rec_xyz)
+    ad = np.ascontiguousarray(rec_ad, np.int32)
+    q = oracle._a(rec_q)
+    pp = oracle._a(p)
+    return float(oracle.L.orc_ad4_probe(xyz.ctypes.data, ad.ctypes.data, q.ctypes.data, len(ad), pp.ctypes.data,
+                                        int(probe_ad), float(probe_q), w.ctypes.data_as(C.POINTER(C.c_double))))

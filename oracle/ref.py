@@ -44,6 +44,12 @@ def lib():
         L.udref_bfgs.restype = C.c_float
         L.udref_mc.argtypes = [vp, vp, C.c_uint, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, fp, fp, C.c_int,
                                C.POINTER(C.c_longlong)]
+        L.udref_ad4_maps_read.restype = vp
+        L.udref_ad4_maps_read.argtypes = [C.c_char_p, fp, C.c_int]
+        L.udref_ad4_pair.argtypes = [C.c_int, C.c_float, C.c_int, C.c_float, C.c_float, fp, C.c_int]
+        L.udref_ad4_pair.restype = C.c_float
+        L.udref_ad4_probe.argtypes = [fp, ip, fp, C.c_int, fp, C.c_int, C.c_float, fp, C.c_int]
+        L.udref_ad4_probe.restype = C.c_double
         _lib = L
     return _lib
 
@@ -60,8 +66,42 @@ VINA_W = np.array([-0.035579, -0.005156, 0.840245, -0.035069, -0.587439, 50, 5 *
 VINARDO_W = np.array([-0.045, 0.8, -0.035, -0.600, 50, 5 * 0.05846 / 0.1 - 1], np.float32)
 
 
+AD4_W = np.array([0.1662, 0.1209, 0.1406, 0.1322, 50, 0.2983], np.float32)
+
+
 def weights_for(sf):
-    return {0: VINA_W, 2: VINARDO_W}[sf]
+    return {0: VINA_W, 1: AD4_W, 2: VINARDO_W}[sf]
+
+
+def ad4_pair(t1, q1, t2, q2, r, weights=None):
+    """ScoringFunction(SF_AD42)::eval of two AD-typed atoms (the reference's own code)."""
+    w = np.ascontiguousarray(AD4_W if weights is None else weights, np.float32)
+    return float(lib().udref_ad4_pair(int(t1), float(q1), int(t2), float(q2), float(r), _f(w), len(w)))
+
+
+def ad4_probe(rec_xyz, rec_ad, rec_q, p, probe_ad, probe_q, weights=None):
+    """Sum of the reference's AD4 pair energies of a probe atom at p (its map value)."""
+    w = np.ascontiguousarray(AD4_W if weights is None else weights, np.float32)
+    xyz = np.ascontiguousarray(rec_xyz, np.float32)
+    ad = np.ascontiguousarray(rec_ad, np.int32)
+    q = np.ascontiguousarray(rec_q, np.float32)
+    pp = np.ascontiguousarray(p, np.float32)
+    return float(lib().udref_ad4_probe(_f(xyz), _i(ad), _f(q), len(ad), _f(pp), int(probe_ad), float(probe_q),
+                                       _f(w), len(w)))
+
+
+class RefAd4Maps:
+    """AD4 maps read by the reference's ad4cache from AutoGrid .map files."""
+
+    def __init__(self, prefix, weights=None):
+        w = np.ascontiguousarray(AD4_W if weights is None else weights, np.float32)
+        self.h = lib().udref_ad4_maps_read(str(prefix).encode(), _f(w), len(w))
+        if not self.h:
+            raise RuntimeError("reference could not read AD4 maps " + str(prefix))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().udref_maps_free(self.h)
 
 
 class RefMaps:

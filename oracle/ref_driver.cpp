@@ -15,6 +15,7 @@
 #include <thread>
 #include <vector>
 
+#include "ad4cache.h"
 #include "cache.h"
 #include "coords.h"
 #include "model.h"
@@ -33,7 +34,11 @@ struct RefMaps {
     std::unique_ptr<precalculate> pre;
     model rec;
     cache grid;
+    ad4cache ad4;               // AutoDock 4.2 maps read from .map files
+    const igrid* ig = &grid;    // the maps the model is scored against
     grid_dims gd;
+    vec corner1() const { return ig == &grid ? grid.corner1() : ad4.corner1(); }
+    vec corner2() const { return ig == &grid ? grid.corner2() : ad4.corner2(); }
 };
 
 struct RefLigand {
@@ -260,7 +265,7 @@ float udref_eval_deriv(void* lh, void* mh, const float* pos, const float* quat,
     L->m.set(c);
     change ch(L->m.get_size());
     vec v(v_intra, v_inter, v_inter);
-    fl e = L->m.eval_deriv(*L->pre, M->grid, v, ch);
+    fl e = L->m.eval_deriv(*L->pre, *M->ig, v, ch);
     for (sz i = 0; i < ch.num_floats(); ++i) g[i] = ch(i);
     if (coords_out)
         for (sz i = 0; i < L->m.num_atoms(); ++i)
@@ -279,9 +284,9 @@ int udref_score(void* lh, void* mh, const float* pos, const float* quat, const f
     conf c = make_conf(L->m, pos, quat, tors);
     L->m.set(c);
     vec vv(v, v, v);
-    fl grid_e = M->grid.eval(L->m, v);
+    fl grid_e = M->ig->eval(L->m, v);
     fl lig_intra = L->m.evali(*L->pre, vv);
-    fl intra_mol = L->m.eval_intramolecular(*L->pre, M->grid, vv);
+    fl intra_mol = L->m.eval_intramolecular(*L->pre, *M->ig, vv);
     out[0] = grid_e;
     out[1] = lig_intra;
     out[2] = intra_mol;
@@ -300,7 +305,7 @@ float udref_bfgs(void* lh, void* mh, float* pos, float* quat, float* tors, float
     quasi_newton qn;
     qn.max_steps = (unsigned)max_steps;
     int ec = 0;
-    qn(L->m, *L->pre, M->grid, out, g, vec(v, v, v), ec);
+    qn(L->m, *L->pre, *M->ig, out, g, vec(v, v, v), ec);
     read_conf(out.c, pos, quat, tors);
     if (evalcount) *evalcount = ec;
     return out.e;
@@ -317,7 +322,7 @@ int udref_mc(void* lh, void* mh, unsigned seed, int n_chains, int global_steps,
     if (threads < 1) threads = 1;
     std::atomic<int> next{0};
     std::atomic<long long> evals{0};
-    vec corner1 = M->grid.corner1(), corner2 = M->grid.corner2();
+    vec corner1 = M->corner1(), corner2 = M->corner2();
     auto worker = [&]() {
         model m = L->m;
         for (;;) {
@@ -338,12 +343,12 @@ int udref_mc(void* lh, void* mh, unsigned seed, int n_chains, int global_steps,
             for (int step = 0; step < global_steps; ++step) {
                 output_type candidate = tmp;
                 mutate_conf(candidate.c, m, 2.0, generator);
-                qn(m, *L->pre, M->grid, candidate, g, hunt, evalcount);
+                qn(m, *L->pre, *M->ig, candidate, g, hunt, evalcount);
                 if (step == 0 || metropolis(tmp.e, candidate.e, 1.2, generator)) {
                     tmp = candidate;
                     m.set(tmp.c);
                     if (tmp.e < best) {
-                        qn(m, *L->pre, M->grid, tmp, g, authentic_v, evalcount);
+                        qn(m, *L->pre, *M->ig, tmp, g, authentic_v, evalcount);
                         m.set(tmp.c);
                         if (tmp.e < best) {
                             best = tmp.e;
@@ -364,6 +369,62 @@ int udref_mc(void* lh, void* mh, unsigned seed, int n_chains, int global_steps,
     for (auto& t : ts) t.join();
     if (evals_out) *evals_out = evals.load();
     return 0;
+}
+
+// AutoDock 4.2 maps from AutoGrid .map files <prefix>.<type>.map, .e.map,
+// .d.map (ad4cache::read, ad4cache.cpp:391-437), scored with the AD4.2
+// scoring function of the given weights.
+void* udref_ad4_maps_read(const char* prefix, const float* weights, int n_weights) {
+    try {
+        auto h = new RefMaps();
+        h->sf = std::make_shared<ScoringFunction>(SF_AD42, to_flv(weights, n_weights));
+        h->ad4 = ad4cache(1e6);
+        h->ad4.read(prefix);
+        h->ig = &h->ad4;
+        return h;
+    } catch (...) {
+        g_err = "udref_ad4_maps_read failed";
+        return nullptr;
+    }
+}
+
+namespace {
+atom ad4_atom(int ad, float q) {
+    atom a;
+    a.ad = (sz)ad;
+    a.xs = XS_TYPE_SIZE;  // no X-Score type: no glue term
+    a.el = EL_TYPE_SIZE;
+    a.charge = q;
+    return a;
+}
+}  // namespace
+
+// ScoringFunction(SF_AD42)::eval of two AD-typed atoms at distance r
+// (scoring_function.h:113-117): the weighted sum of the AD4.2 terms.
+float udref_ad4_pair(int ad1, float q1, int ad2, float q2, float r, const float* weights, int n_weights) {
+    ScoringFunction sf(SF_AD42, to_flv(weights, n_weights));
+    atom a = ad4_atom(ad1, q1), b = ad4_atom(ad2, q2);
+    return sf.eval(a, b, r);
+}
+
+// Energy of a probe atom (AD type, charge) at point p against every receptor
+// atom within the AD4 cutoff: the sum of the reference's pairwise
+// ScoringFunction(SF_AD42)::eval, i.e. the value an AD4 grid map of that probe
+// holds at p (type map + q * electrostatic map + |q| * desolvation map).
+double udref_ad4_probe(const float* xyz, const int* ad, const float* q, int n, const float* p, int probe_ad,
+                       float probe_q, const float* weights, int n_weights) {
+    ScoringFunction sf(SF_AD42, to_flv(weights, n_weights));
+    atom pr = ad4_atom(probe_ad, probe_q);
+    const fl cut2 = sf.get_cutoff() * sf.get_cutoff();
+    double acc = 0;
+    for (int i = 0; i < n; ++i) {
+        vec d(xyz[3 * i] - p[0], xyz[3 * i + 1] - p[1], xyz[3 * i + 2] - p[2]);
+        fl r2 = d.norm_sqr();
+        if (r2 >= cut2) continue;
+        atom b = ad4_atom(ad[i], q[i]);
+        acc += sf.eval(pr, b, std::sqrt(r2));
+    }
+    return acc;
 }
 
 }  // extern "C"

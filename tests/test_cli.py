@@ -42,6 +42,7 @@ def test_help_lists_every_reference_option():
     (["--receptor", "r.pdbqt", "--gpu_batch", "a.pdbqt"], "Need to specify an output directory for batch mode."),
     (["--receptor", "r.pdbqt", "--gpu_batch", "a.pdbqt", "--dir", "/nonexistent_dir_x"], "does not exist"),
     (["--receptor", "r.pdbqt", "--ligand", "a.pdbqt", "--scoring", "xyz"], "Scoring function xyz unknown."),
+    (["--receptor", "r.pdbqt", "--ligand", "a.pdbqt", "--flex", "f.pdbqt"], "--flex is not supported by this build"),
     (["--ligand", "a.pdbqt"], "The receptor or affinity maps must be specified."),
     (["--bogus", "1"], "unrecognised option '--bogus'"),
     (["--receptor", "r.pdbqt", "--ligand", "a.pdbqt", "--gpu_batch", "b.pdbqt", "--dir", "."],
@@ -125,3 +126,28 @@ def test_score_only_and_local_only(inputs):
     assert moved > 0
     r = run("--receptor", d / "rec.pdbqt", "--ligand", names[1], "--score_only", "--autobox")
     assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.gpu
+def test_ad4_maps_written_then_read_back(inputs, tmp_path, receptor):
+    """--scoring ad4 builds AutoDock maps from the receptor (charges from its
+    PDBQT), --write_maps writes AutoGrid files, and --maps reads them back:
+    the docking from the files equals the docking from the receptor (the maps
+    are equal on the same grid, so the seeded search is too)."""
+    d, names = inputs
+    rec = synth.make_receptor(2000, seed=5, with_charges=True)
+    (tmp_path / "recq.pdbqt").write_text(rec.to_pdbqt())
+    lig = tmp_path / "lig.pdbqt"
+    lig.write_text(synth.make_ligand(18, 3, seed=808, with_charges=True).to_pdbqt())
+    common = ["--ligand", lig, "--scoring", "ad4", "--exhaustiveness", 8, "--max_step", 8, "--seed", 4]
+    r = run("--receptor", tmp_path / "recq.pdbqt", *common, "--out", tmp_path / "a.pdbqt",
+            "--write_maps", tmp_path / "maps", *box_args(16.0))
+    assert r.returncode == 0, r.stderr
+    for t in ("C", "OA", "HD", "e", "d"):
+        assert (tmp_path / f"maps.{t}.map").exists()
+    r = run("--maps", tmp_path / "maps", *common, "--out", tmp_path / "b.pdbqt")
+    assert r.returncode == 0, r.stderr
+    a, b = (tmp_path / "a.pdbqt").read_text(), (tmp_path / "b.pdbqt").read_text()
+    ea = [float(l.split()[3]) for l in a.splitlines() if l.startswith("REMARK VINA RESULT:")]
+    eb = [float(l.split()[3]) for l in b.splitlines() if l.startswith("REMARK VINA RESULT:")]
+    assert ea and ea == eb

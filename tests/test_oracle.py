@@ -132,3 +132,26 @@ def test_bfgs_matches_reference_from_same_start(gold, o32, setup32, tmp_path):
             agree += abs(eo - er) <= 1e-4 * max(1.0, abs(er))
     # trajectories can branch on last-bit differences in a line search; most must agree exactly
     assert agree >= total - 2, (agree, total)
+
+
+@pytest.mark.skipif(not ref.available(), reason="reference build missing")
+def test_ad4_pair_terms_match_reference():
+    """The AD4.2 pair energy (vdW / H-bond 12-6 / 12-10 with smoothing,
+    electrostatics with the distance-dependent dielectric, desolvation) of the
+    C restatement against the reference's ScoringFunction(SF_AD42)::eval on
+    random AD types, charges and distances; FP32 error against FP64 stated."""
+    from oracle.oracle import ad4_pair
+    o32, o64 = Oracle(np.float32), Oracle(np.float64)
+    rng = np.random.default_rng(0)
+    types = [t for t in range(35) if not (22 <= t <= 25) and t != 30]  # glue atoms and W carry no AD4 terms
+    err32, err64 = [], []
+    for _ in range(2000):
+        t1, t2 = rng.choice(types, 2)
+        q1, q2 = rng.normal(0, 0.3, 2).astype(np.float32)
+        r = np.float32(rng.uniform(0.2, 21.0))
+        er = ref.ad4_pair(t1, q1, t2, q2, r)
+        e64 = ad4_pair(o64, t1, q1, t2, q2, r)
+        err32.append(abs(ad4_pair(o32, t1, q1, t2, q2, r) - er) / max(1.0, abs(e64)))
+        err64.append(abs(er - e64) / max(1.0, abs(e64)))
+    assert max(err32) < 1e-6, max(err32)
+    assert max(err64) < 1e-5, max(err64)

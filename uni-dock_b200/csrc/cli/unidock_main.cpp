@@ -50,8 +50,9 @@ const OptSpec kOptions[] = {
     {"paired_batch_size", 0, "one-ligand-one-protein batching (not supported by this build)", "Input"},
     {"batch", 2, "batch ligand (PDBQT)", "Input"},
     {"gpu_batch", 2, "gpu batch ligand (PDBQT)", "Input"},
-    {"scoring", 0, "scoring function (vina or vinardo; ad4 maps are not supported by this build)", "Input"},
-    {"maps", 0, "affinity maps (not supported by this build)", "Search space"},
+    {"scoring", 0, "scoring function (ad4, vina or vinardo)", "Input"},
+    {"maps", 0, "affinity maps for the autodock4.2 (ad4) or vina scoring function (AutoGrid .map files "
+                "<prefix>.<type>.map)", "Search space"},
     {"center_x", 0, "X coordinate of the center (Angstrom)", "Search space"},
     {"center_y", 0, "Y coordinate of the center (Angstrom)", "Search space"},
     {"center_z", 0, "Z coordinate of the center (Angstrom)", "Search space"},
@@ -62,7 +63,7 @@ const OptSpec kOptions[] = {
      "Search space"},
     {"out", 0, "output models (PDBQT), the default is chosen based on the ligand file name", "Output"},
     {"dir", 0, "output directory for batch mode", "Output"},
-    {"write_maps", 0, "output maps (not supported by this build)", "Output"},
+    {"write_maps", 0, "output filename (directory + prefix name) for maps", "Output"},
     {"device_id", 0, "GPU device id to use (default 0)", "Advanced"},
     {"score_only", 1, "score only - search space can be omitted", "Advanced"},
     {"score_file", 0, "score only output file in batch mode, with 'score_only' option", "Advanced"},
@@ -348,14 +349,23 @@ struct Setup {
     bool autotune = false;
 };
 
+// Maps from the receptor: Vina / Vinardo maps, or AD4 maps (types and charges
+// from the receptor PDBQT) in place of the external autogrid4 step.
 ud_maps build_maps(const Setup& S, const std::string& receptor) {
     std::string text = read_file(receptor);
     int n = 0;
-    check(ud_receptor_parse(text.data(), text.size(), nullptr, nullptr, 0, &n), "receptor");
-    std::vector<float> xyz(3 * (size_t)n);
-    std::vector<int> xs(n);
-    check(ud_receptor_parse(text.data(), text.size(), xyz.data(), xs.data(), n, &n), "receptor");
+    check(ud_receptor_parse_ex(text.data(), text.size(), nullptr, nullptr, nullptr, nullptr, 0, &n), "receptor");
+    std::vector<float> xyz(3 * (size_t)n), q(n);
+    std::vector<int> xs(n), ad(n);
+    check(ud_receptor_parse_ex(text.data(), text.size(), xyz.data(), xs.data(), ad.data(), q.data(), n, &n),
+          "receptor");
     ud_maps maps = nullptr;
+    if (S.sf == UD_SF_AD4) {
+        check(ud_maps_create_ad4(S.weights.data(), (int)S.weights.size(), xyz.data(), ad.data(), q.data(), n,
+                                 S.center, S.size, S.spacing, nullptr, 0, nullptr, &maps),
+              "AD4 grid maps");
+        return maps;
+    }
     check(ud_maps_create(S.sf, S.weights.data(), (int)S.weights.size(), xyz.data(), xs.data(), n, S.center, S.size,
                          S.spacing, nullptr, 0, nullptr, &maps),
           "grid maps");
@@ -529,8 +539,7 @@ int run(int argc, char** argv) {
         std::cout << "unidock (B200 engine, C ABI version " << ud_version() << ")\n";
         return 0;
     }
-    for (const char* unsupported : {"flex", "maps", "paired_batch_size", "bias", "multi_bias", "write_maps",
-                                    "randomize_only"})
+    for (const char* unsupported : {"flex", "paired_batch_size", "bias", "multi_bias", "randomize_only"})
         if (o.has(unsupported))
             throw std::runtime_error(std::string("--") + unsupported + " is not supported by this build");
     Setup S;
@@ -548,11 +557,14 @@ int run(int argc, char** argv) {
                      (float)o.num("weight_vinardo_hydrogen", -0.6), (float)o.num("weight_glue", 50),
                      (float)o.num("weight_vinardo_rot", o.num("weight_rot", 0.05846))};
     } else if (sf_name == "ad4") {
-        throw std::runtime_error("the ad4 scoring function (AutoGrid maps) is not supported by this build");
+        S.sf = UD_SF_AD4;
+        S.weights = {(float)o.num("weight_ad4_vdw", 0.1662), (float)o.num("weight_ad4_hb", 0.1209),
+                     (float)o.num("weight_ad4_elec", 0.1406), (float)o.num("weight_ad4_dsolv", 0.1322),
+                     (float)o.num("weight_glue", 50), (float)o.num("weight_ad4_rot", 0.2983)};
     } else {
         throw std::runtime_error("Scoring function " + sf_name + " unknown.");
     }
-    if (!o.has("receptor")) throw std::runtime_error("The receptor or affinity maps must be specified.");
+    if (!o.has("receptor") && !o.has("maps")) throw std::runtime_error("The receptor or affinity maps must be specified.");
     const bool score_only = o.has("score_only"), local_only = o.has("local_only");
     S.verbosity = (int)o.num("verbosity", 1);
     const int cpu = (int)o.num("cpu", 0);
@@ -615,7 +627,7 @@ int run(int argc, char** argv) {
     for (int i = 0; i < 3; ++i) {
         const char* c[3] = {"center_x", "center_y", "center_z"};
         const char* z[3] = {"size_x", "size_y", "size_z"};
-        if (!autobox && (!o.has(c[i]) || !o.has(z[i])))
+        if (!autobox && !o.has("maps") && (!o.has(c[i]) || !o.has(z[i])))
             throw std::runtime_error("the search space (--center_x/y/z, --size_x/y/z) must be specified");
         S.center[i] = (float)o.num(c[i], 0);
         S.size[i] = (float)o.num(z[i], 0);
@@ -643,7 +655,7 @@ int run(int argc, char** argv) {
             S.size[i] = (float)std::ceil((m + 4.0) * 2);
         }
     }
-    for (int i = 0; i < 3; ++i) {
+    for (int i = 0; i < 3 && !o.has("maps"); ++i) {
         if (!(S.size[i] > 0)) throw std::runtime_error("Grid box dimensions must be greater than 0 Angstrom.");
         if (o.has("force_even_voxels")) {  // vina.cpp:529-534: odd voxel counts get one more voxel
             long nv = (long)std::ceil(S.size[i] / S.spacing);
@@ -654,7 +666,8 @@ int run(int argc, char** argv) {
         std::cerr << "WARNING: Search space volume is greater than 27000 Angstrom^3 (See FAQ)\n";
     if (S.verbosity > 0) {
         std::cout << "Scoring function : " << sf_name << "\n";
-        std::cout << "Rigid receptor: " << o.str("receptor") << "\n";
+        if (o.has("receptor")) std::cout << "Rigid receptor: " << o.str("receptor") << "\n";
+        if (o.has("maps")) std::cout << "Affinity maps: " << o.str("maps") << "\n";
         if (ligand_names.size() == 1) std::cout << "Ligand: " << ligand_names[0] << "\n";
         else std::cout << "Ligands (batch mode): " << batch_names.size() << " molecules\n";
         std::cout << std::setprecision(6) << "Grid center: X " << S.center[0] << " Y " << S.center[1] << " Z "
@@ -668,7 +681,14 @@ int run(int argc, char** argv) {
     }
     const int device = (int)o.num("device_id", 0);
     if (cudaSetDevice(device) != cudaSuccess) throw std::runtime_error("could not select GPU " + std::to_string(device));
-    ud_maps maps = build_maps(S, o.str("receptor"));
+    ud_maps maps = nullptr;
+    if (o.has("maps")) {
+        check(ud_maps_load(S.sf, S.weights.data(), (int)S.weights.size(), o.str("maps").c_str(), nullptr, &maps),
+              "maps");
+    } else {
+        maps = build_maps(S, o.str("receptor"));
+    }
+    if (o.has("write_maps")) check(ud_maps_write(maps, o.str("write_maps").c_str()), "write maps");
     if (!ligand_names.empty()) {
         std::string out_name = o.has("out") ? o.str("out") : default_output(ligand_names[0]);
         if (!score_only && S.verbosity > 0 && !o.has("out")) std::cout << "Output will be " << out_name << "\n";

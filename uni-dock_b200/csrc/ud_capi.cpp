@@ -7,6 +7,7 @@
 #include <thread>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <iomanip>
 #include <limits>
@@ -20,6 +21,10 @@
 #include "../../include/unidock_b200.h"
 #include "ud_engine.h"
 #include "ud_model.h"
+
+static_assert(ud::kAd4TableRowElec == ud::kAd4RowElec && ud::kAd4TableRowDesolv == ud::kAd4RowDesolv,
+              "AD4 table layout shared by host and device");
+static_assert(ud::kAdTypes == ud::AD_SIZE, "AD4 parameter arrays cover every AD type");
 
 
 using namespace ud;
@@ -112,11 +117,17 @@ struct ud_maps_s {
     float cutoff2 = 64.0f;
     // typed receptor atoms (x, y, z, xs as int bits), kept to build term maps
     std::vector<float> rec_xyzt;
+    // AD4: receptor atoms (x, y, z, charge) and AD types
+    std::vector<float> rec_xyzq;
+    std::vector<int> rec_ad;
     // per-term data of weight gradients, built on first use
     DevBuf<float> term_maps;         // [term][slot][z][y][x]
     DevBuf<float> term_rows;         // [term][tp][bin][4], as `smooth`
     DevBuf<float> term_fast;         // [term][tp][bin], as `fast`
     bool terms_built = false;
+    bool loaded = false;             // read from map files: no receptor to rebuild per-term maps from
+    float box_center[3] = {0, 0, 0}; // box as given (written to map file headers)
+    float box_spacing = 0;
 };
 
 struct LigandPost {
@@ -136,6 +147,8 @@ struct ud_batch_s {
     DevBuf<NodeRec> d_nodes;
     DevBuf<uint32_t> d_pairs;
     DevBuf<uint32_t> d_grid;
+    DevBuf<float> d_charge;          // AD4: atom charges
+    DevBuf<float> d_pair_coef;       // AD4: (q_a q_b, |q_a| V_b + |q_b| V_a) per pair slot
     int max_atoms = 0, max_tors = 0;
     // search state
     DevBuf<int> d_order;
@@ -186,7 +199,8 @@ struct ud_batch_s {
         if (ev1) cudaEventDestroy(ev1);
     }
     DeviceBatchView view() const {
-        return DeviceBatchView{d_desc.p, d_atoms.p, d_nodes.p, d_pairs.p, d_grid.p, max_atoms, max_tors};
+        return DeviceBatchView{d_desc.p, d_atoms.p, d_nodes.p, d_pairs.p, d_grid.p, max_atoms, max_tors,
+                               d_charge.p, d_pair_coef.p, maps && maps->desc.ad4 ? 1 : 0};
     }
 };
 
@@ -212,6 +226,25 @@ extern "C" int ud_receptor_parse(const char* pdbqt, size_t len, float* xyz, int*
                 if (xyz)
                     for (int k = 0; k < 3; ++k) xyz[3 * i + k] = R.xyz[i][k];
                 if (xs) xs[i] = R.xs[i];
+            }
+        }
+    });
+}
+
+extern "C" int ud_receptor_parse_ex(const char* pdbqt, size_t len, float* xyz, int* xs, int* ad, float* charge,
+                                    int capacity, int* n_atoms) {
+    return guarded([&] {
+        if (!pdbqt || !n_atoms) throw Error(UD_ERR_ARG, "null argument");
+        Receptor R = parse_receptor_pdbqt(std::string(pdbqt, len));
+        *n_atoms = (int)R.xyz.size();
+        if (xyz || xs || ad || charge) {
+            if (capacity < (int)R.xyz.size()) throw Error(UD_ERR_CAPACITY, "receptor capacity too small");
+            for (size_t i = 0; i < R.xyz.size(); ++i) {
+                if (xyz)
+                    for (int k = 0; k < 3; ++k) xyz[3 * i + k] = R.xyz[i][k];
+                if (xs) xs[i] = R.xs[i];
+                if (ad) ad[i] = R.ad[i];
+                if (charge) charge[i] = R.charge[i];
             }
         }
     });
@@ -277,6 +310,8 @@ extern "C" int ud_maps_create(int sf, const float* weights, int n_weights, const
         m->sf = Scoring::make(sf, w.empty() ? nullptr : w.data(), (int)w.size());
         // box (vina.cpp:528-539) and grid frame (grid.cpp:25-38)
         MapsDesc& d = m->desc;
+        for (int i = 0; i < 3; ++i) m->box_center[i] = center[i];
+        m->box_spacing = spacing;
         for (int i = 0; i < 3; ++i) {
             size_t nvox = (size_t)std::ceil((float)size[i] / (float)spacing);
             float real_span = (float)spacing * nvox;
@@ -348,6 +383,276 @@ extern "C" int ud_maps_create(int sf, const float* weights, int n_weights, const
     });
 }
 
+// ---------------------------------------------------------------- AD4 maps
+
+// AutoDock 4.2 atom-kind parameters for the map kernel (atom_constants.h).
+static Ad4Params ad4_params() {
+    Ad4Params P{};
+    for (int t = 0; t < AD_SIZE; ++t) {
+        const AdKind& k = ad_kind(t);
+        P.radius[t] = k.radius;
+        P.depth[t] = k.depth;
+        P.hb_depth[t] = k.hb_depth;
+        P.hb_radius[t] = k.hb_radius;
+        P.solvation[t] = ad4_solvation(t);
+        P.volume[t] = ad4_volume(t);
+    }
+    return P;
+}
+
+// Map set of AD4 maps `m` with the term weights (term >= 0: that term alone at weight 1).
+static Ad4MapSpec ad4_spec(const ud_maps_s* m, int term) {
+    Ad4MapSpec S{};
+    S.n_slots = m->desc.n_maps - 2;
+    for (int k = 0; k < S.n_slots; ++k) S.slot_ad[k] = m->slot_types[k];
+    auto w = [&](int t) { return term < 0 ? m->sf.weights[t] : (term == t ? 1.0f : 0.0f); };
+    S.w_vdw = w(0);
+    S.w_hb = w(1);
+    S.w_elec = w(2);
+    S.w_dsolv = w(3);
+    return S;
+}
+
+// AD types an AD4 map set covers by default: every AD kind an atom can read
+// (CG carbons read C, glue atoms none, W never occurs in ligands).
+static std::vector<int> default_ad4_types() {
+    std::vector<int> t;
+    for (int a = 0; a < AD_SIZE; ++a)
+        if ((a < AD_G0 || a > AD_CG3) && a != AD_W) t.push_back(a);
+    return t;
+}
+
+extern "C" int ud_maps_create_ad4(const float* weights, int n_weights, const float* rec_xyz, const int* rec_ad,
+                                  const float* rec_q, int n_rec, const float center[3], const float size[3],
+                                  float spacing, const int* types, int n_types, void* stream, ud_maps* out) {
+    return guarded([&] {
+        if (!out || !center || !size || (n_rec > 0 && (!rec_xyz || !rec_ad || !rec_q)) || spacing <= 0)
+            throw Error(UD_ERR_ARG, "invalid maps arguments");
+        for (int i = 0; i < 3; ++i)
+            if (!(size[i] > 0)) throw Error(UD_ERR_ARG, "box size must be positive");
+        cudaStream_t s = (cudaStream_t)stream;
+        auto m = std::make_unique<ud_maps_s>();
+        // AD4 weights: vdW, H-bond, electrostatics, desolvation, glue, torsional (raw, ad4_tors_add)
+        m->sf = Scoring::make(SF_AD42, (weights && n_weights > 0) ? weights : nullptr,
+                              (weights && n_weights > 0) ? n_weights : 0);
+        MapsDesc& d = m->desc;
+        for (int i = 0; i < 3; ++i) {
+            // AutoGrid maps have an even number of voxels per axis (ad4cache.cpp:355-364)
+            size_t nvox = (size_t)std::ceil((float)size[i] / (float)spacing);
+            if (nvox % 2 == 1) ++nvox;
+            // the frame the map reader derives from CENTER and SPACING, so that
+            // written maps read back onto the same grid
+            const float halfspan = (float)((double)((int)nvox * spacing) / 2.0);
+            float begin = (float)center[i] - halfspan;
+            float end = (float)center[i] + halfspan;
+            m->box_center[i] = center[i];
+            d.dims[i] = (int)nvox + 1;
+            d.init[i] = begin;
+            d.corner2[i] = end;
+            d.dim_m1[i] = (float)(d.dims[i] - 1);
+            d.factor[i] = d.dim_m1[i] / (end - begin);
+            d.factor_inv[i] = 1 / d.factor[i];
+        }
+        m->box_spacing = spacing;
+        d.slope = 1e6f;
+        d.ad4 = 1;
+        std::vector<int> req = types && n_types > 0 ? std::vector<int>(types, types + n_types) : default_ad4_types();
+        for (int t : req) {
+            if (t < 0 || t >= AD_SIZE) throw Error(UD_ERR_ARG, "AD type out of range");
+            int g = (t >= AD_CG0 && t <= AD_CG3) ? AD_C : t;
+            if (g >= AD_G0 && g <= AD_G3) continue;
+            if (std::find(m->slot_types.begin(), m->slot_types.end(), g) == m->slot_types.end())
+                m->slot_types.push_back(g);
+        }
+        if (m->slot_types.size() > 34) throw Error(UD_ERR_ARG, "too many map types");
+        std::fill(d.slot_of_xs, d.slot_of_xs + 36, (int8_t)-1);
+        for (size_t k = 0; k < m->slot_types.size(); ++k) d.slot_of_xs[m->slot_types[k]] = (int8_t)k;
+        d.e_slot = (int)m->slot_types.size();
+        d.d_slot = d.e_slot + 1;
+        d.n_maps = d.d_slot + 1;
+        // pair tables: AD type pairs + the shared electrostatic / desolvation rows
+        PairTable tab;
+        tab.build(m->sf);
+        m->n_bins = tab.n;
+        m->factor = tab.factor;
+        m->cutoff2 = m->sf.cutoff * m->sf.cutoff;
+        {
+            std::vector<float> s4(tab.smooth.size() * 2, 0.0f);
+            pack_smooth4(tab, s4.data());
+            m->smooth.upload(s4.data(), s4.size(), s);
+        }
+        m->fast.alloc(round4(tab.fast.size()));
+        m->fast.upload(tab.fast.data(), tab.fast.size(), s);
+        for (int i = 0; i < n_rec; ++i) {
+            if (rec_ad[i] < 0 || rec_ad[i] >= AD_SIZE) continue;  // untyped atoms contribute nothing
+            for (int k = 0; k < 3; ++k) m->rec_xyzq.push_back(rec_xyz[3 * i + k]);
+            m->rec_xyzq.push_back(rec_q[i]);
+            m->rec_ad.push_back(rec_ad[i]);
+        }
+        DevBuf<float> d_rec;
+        DevBuf<int> d_ad;
+        d_rec.upload(m->rec_xyzq.data(), m->rec_xyzq.size(), s);
+        d_ad.upload(m->rec_ad.data(), m->rec_ad.size(), s);
+        const size_t plane = (size_t)d.dims[0] * d.dims[1] * d.dims[2];
+        m->maps.alloc(round4(plane * d.n_maps));
+        cuda_check(launch_maps_ad4(d_rec.p, d_ad.p, (int)m->rec_ad.size(), ad4_params(), ad4_spec(m.get(), -1), d,
+                                   m->maps.p, s),
+                   "AD4 maps kernel");
+        cuda_check(cudaStreamSynchronize(s), "maps sync");
+        *out = m.release();
+    });
+}
+
+// AutoGrid .map files of the maps (header of ad4cache::write, ad4cache.cpp:439-521;
+// values at full float precision): AD4 maps as <prefix>.<AD type>.map,
+// <prefix>.e.map and <prefix>.d.map; Vina maps as <prefix>.<XS type>.map.
+extern "C" int ud_maps_write(ud_maps maps, const char* prefix) {
+    return guarded([&] {
+        if (!maps || !prefix) throw Error(UD_ERR_ARG, "null argument");
+        const MapsDesc& d = maps->desc;
+        const size_t plane = (size_t)d.dims[0] * d.dims[1] * d.dims[2];
+        std::vector<float> h(plane);
+        for (int k = 0; k < d.n_maps; ++k) {
+            std::string name;
+            if (d.ad4) name = k == d.e_slot ? "e" : k == d.d_slot ? "d" : ad_kind(maps->slot_types[k]).name;
+            else name = xs_name(maps->slot_types[k]);
+            cuda_check(cudaMemcpy(h.data(), maps->maps.p + plane * k, plane * sizeof(float), cudaMemcpyDeviceToHost),
+                       "map D2H");
+            std::string path = std::string(prefix) + "." + name + ".map";
+            FILE* f = std::fopen(path.c_str(), "w");
+            if (!f) throw Error(UD_ERR_ARG, "cannot write " + path);
+            std::fprintf(f, "GRID_PARAMETER_FILE NULL\nGRID_DATA_FILE NULL\nMACROMOLECULE NULL\n");
+            std::fprintf(f, "SPACING %.9g\n", maps->box_spacing);
+            std::fprintf(f, "NELEMENTS %d %d %d\n", d.dims[0] - 1, d.dims[1] - 1, d.dims[2] - 1);
+            std::fprintf(f, "CENTER %.9g %.9g %.9g\n", maps->box_center[0], maps->box_center[1], maps->box_center[2]);
+            for (size_t i = 0; i < plane; ++i) std::fprintf(f, "%.9g\n", h[i]);
+            std::fclose(f);
+        }
+    });
+}
+
+// One AutoGrid .map text file: six header lines (SPACING on the 4th,
+// NELEMENTS on the 5th, CENTER on the 6th) then one value per line, x
+// fastest (read_vina_map / read_ad4_map, cache.cpp:267-323, ad4cache.cpp:333-389).
+static bool read_map_file(const std::string& path, float& spacing, int nvox[3], float center[3],
+                          std::vector<float>& vals) {
+    FILE* f = std::fopen(path.c_str(), "r");
+    if (!f) return false;
+    char line[512];
+    int ln = 0;
+    vals.clear();
+    bool ok = true;
+    while (std::fgets(line, sizeof line, f)) {
+        ++ln;
+        if (ln == 4) ok &= std::sscanf(line, "%*s %f", &spacing) == 1;
+        else if (ln == 5) ok &= std::sscanf(line, "%*s %d %d %d", &nvox[0], &nvox[1], &nvox[2]) == 3;
+        else if (ln == 6) ok &= std::sscanf(line, "%*s %f %f %f", &center[0], &center[1], &center[2]) == 3;
+        else if (ln > 6) vals.push_back(std::strtof(line, nullptr));
+    }
+    std::fclose(f);
+    if (!ok) throw Error(UD_ERR_PARSE, "malformed map header in " + path);
+    for (int i = 0; i < 3; ++i)
+        if (nvox[i] < 2 || nvox[i] % 2 == 1)
+            throw Error(UD_ERR_PARSE, "number of voxels (NELEMENTS) must be even and positive in " + path);
+    const size_t want = (size_t)(nvox[0] + 1) * (nvox[1] + 1) * (nvox[2] + 1);
+    if (vals.size() != want)
+        throw Error(UD_ERR_PARSE, path + ": " + std::to_string(vals.size()) + " values, expected " +
+                                      std::to_string(want));
+    return true;
+}
+
+extern "C" int ud_maps_load(int sf, const float* weights, int n_weights, const char* prefix, void* stream,
+                            ud_maps* out) {
+    return guarded([&] {
+        if (!out || !prefix) throw Error(UD_ERR_ARG, "null argument");
+        if (sf != UD_SF_VINA && sf != UD_SF_VINARDO && sf != UD_SF_AD4) throw Error(UD_ERR_ARG, "unknown scoring function");
+        cudaStream_t s = (cudaStream_t)stream;
+        auto m = std::make_unique<ud_maps_s>();
+        std::vector<float> w;
+        if (weights && n_weights > 0) {
+            w.assign(weights, weights + n_weights);
+            if (sf != UD_SF_AD4) w.back() = (float)(5 * (double)w.back() / 0.1 - 1);  // as ud_maps_create
+        }
+        m->sf = Scoring::make(sf == UD_SF_AD4 ? SF_AD42 : sf, w.empty() ? nullptr : w.data(), (int)w.size());
+        MapsDesc& d = m->desc;
+        std::vector<std::pair<std::string, int>> files;  // (name, type)
+        if (sf == UD_SF_AD4) {
+            for (int t : default_ad4_types()) files.push_back({ad_kind(t).name, t});
+        } else {
+            for (int t : default_map_types()) files.push_back({xs_name(t), t});
+        }
+        std::vector<std::vector<float>> data;
+        float spacing0 = 0, center0[3] = {0, 0, 0};
+        int nvox0[3] = {0, 0, 0};
+        auto take = [&](const std::string& name, int type, bool required) {
+            float sp, c[3];
+            int nv[3];
+            std::vector<float> v;
+            const std::string path = std::string(prefix) + "." + name + ".map";
+            if (!read_map_file(path, sp, nv, c, v)) {
+                if (required) throw Error(UD_ERR_ARG, "missing map file " + path);
+                return;
+            }
+            if (data.empty()) {
+                spacing0 = sp;
+                for (int i = 0; i < 3; ++i) {
+                    nvox0[i] = nv[i];
+                    center0[i] = c[i];
+                }
+            } else if (sp != spacing0 || nv[0] != nvox0[0] || nv[1] != nvox0[1] || nv[2] != nvox0[2] ||
+                       c[0] != center0[0] || c[1] != center0[1] || c[2] != center0[2]) {
+                throw Error(UD_ERR_ARG, "map " + path + " has a different grid than the others");
+            }
+            data.push_back(std::move(v));
+            if (type >= 0) m->slot_types.push_back(type);
+        };
+        for (auto& f : files) take(f.first, f.second, false);
+        if (m->slot_types.empty()) throw Error(UD_ERR_ARG, std::string("no *.map files with prefix ") + prefix);
+        std::fill(d.slot_of_xs, d.slot_of_xs + 36, (int8_t)-1);
+        for (size_t k = 0; k < m->slot_types.size(); ++k) d.slot_of_xs[m->slot_types[k]] = (int8_t)k;
+        if (sf == UD_SF_AD4) {
+            d.ad4 = 1;
+            d.e_slot = (int)m->slot_types.size();
+            d.d_slot = d.e_slot + 1;
+            take("e", -1, true);
+            take("d", -1, true);
+        }
+        d.n_maps = (int)data.size();
+        for (int i = 0; i < 3; ++i) {  // grid frame of the map reader (read_ad4_map, ad4cache.cpp:365-376)
+            const float halfspan = (float)((double)(nvox0[i] * spacing0) / 2.0);
+            const float begin = center0[i] - halfspan, end = center0[i] + halfspan;
+            d.dims[i] = nvox0[i] + 1;
+            d.init[i] = begin;
+            d.corner2[i] = end;
+            d.dim_m1[i] = (float)nvox0[i];
+            d.factor[i] = d.dim_m1[i] / (end - begin);
+            d.factor_inv[i] = 1 / d.factor[i];
+        }
+        d.slope = 1e6f;
+        for (int i = 0; i < 3; ++i) m->box_center[i] = center0[i];
+        m->box_spacing = spacing0;
+        PairTable tab;
+        tab.build(m->sf);
+        m->n_bins = tab.n;
+        m->factor = tab.factor;
+        m->cutoff2 = m->sf.cutoff * m->sf.cutoff;
+        {
+            std::vector<float> s4(tab.smooth.size() * 2, 0.0f);
+            pack_smooth4(tab, s4.data());
+            m->smooth.upload(s4.data(), s4.size(), s);
+        }
+        m->fast.alloc(round4(tab.fast.size()));
+        m->fast.upload(tab.fast.data(), tab.fast.size(), s);
+        const size_t plane = (size_t)d.dims[0] * d.dims[1] * d.dims[2];
+        std::vector<float> all(round4(plane * d.n_maps), 0.0f);
+        for (int k = 0; k < d.n_maps; ++k) std::copy(data[k].begin(), data[k].end(), all.begin() + plane * k);
+        m->maps.upload(all.data(), all.size(), s);
+        cuda_check(cudaStreamSynchronize(s), "maps upload");
+        m->loaded = true;
+        *out = m.release();
+    });
+}
+
 extern "C" int ud_maps_info(ud_maps maps, int dims[3], float init[3], float factor[3], int* n_maps) {
     return guarded([&] {
         if (!maps) throw Error(UD_ERR_ARG, "null maps");
@@ -362,9 +667,18 @@ extern "C" int ud_maps_info(ud_maps maps, int dims[3], float init[3], float fact
 
 extern "C" int ud_maps_read(ud_maps maps, int xs, float* out, size_t n) {
     return guarded([&] {
-        if (!maps || !out || xs < 0 || xs >= XS_SIZE) throw Error(UD_ERR_ARG, "invalid argument");
-        int slot = maps->desc.slot_of_xs[xs];
-        if (slot < 0) throw Error(UD_ERR_ARG, std::string("no map for type ") + xs_name(xs));
+        if (!maps || !out || xs < 0) throw Error(UD_ERR_ARG, "invalid argument");
+        int slot = -1;
+        if (maps->desc.ad4) {  // AD type, AD_SIZE = electrostatic, AD_SIZE + 1 = desolvation
+            if (xs == AD_SIZE) slot = maps->desc.e_slot;
+            else if (xs == AD_SIZE + 1) slot = maps->desc.d_slot;
+            else if (xs < AD_SIZE) slot = maps->desc.slot_of_xs[xs];
+            if (slot < 0) throw Error(UD_ERR_ARG, "no AD4 map for type " + std::to_string(xs));
+        } else {
+            if (xs >= XS_SIZE) throw Error(UD_ERR_ARG, "invalid argument");
+            slot = maps->desc.slot_of_xs[xs];
+            if (slot < 0) throw Error(UD_ERR_ARG, std::string("no map for type ") + xs_name(xs));
+        }
         const size_t plane = (size_t)maps->desc.dims[0] * maps->desc.dims[1] * maps->desc.dims[2];
         if (n < plane) throw Error(UD_ERR_CAPACITY, "output buffer too small");
         cuda_check(cudaMemcpy(out, maps->maps.p + plane * slot, plane * sizeof(float), cudaMemcpyDeviceToHost),
@@ -477,27 +791,28 @@ extern "C" int ud_ligand_destroy(ud_ligand lig) {
 // 0-15 and 16-31 are each a matching (no atom twice), so the two half-warps can
 // add their pair forces into shared memory one after the other without
 // atomics.  Unfilled slots hold kPairPad; the list length is a multiple of 32.
-static std::vector<uint32_t> pair_groups(const Ligand& L) {
-    std::vector<uint32_t> out;
-    std::vector<char> used(L.pairs.size(), 0);
+// Index into `pairs` of every slot of the conflict-free 32-slot groups, -1 for padding.
+static std::vector<int> pair_group_slots(const Ligand& L, const std::vector<Pair>& pairs) {
+    std::vector<int> out;
+    std::vector<char> used(pairs.size(), 0);
     std::vector<int> stamp(L.atoms.size(), -1);
-    size_t left = L.pairs.size(), start = 0;
+    size_t left = pairs.size(), start = 0;
     int half_id = 0;
     while (left > 0) {
         for (int half = 0; half < 2; ++half, ++half_id) {
             int filled = 0;
-            for (size_t k = start; k < L.pairs.size() && filled < 16; ++k) {
+            for (size_t k = start; k < pairs.size() && filled < 16; ++k) {
                 if (used[k]) continue;
-                const Pair& p = L.pairs[k];
+                const Pair& p = pairs[k];
                 if (stamp[p.a] == half_id || stamp[p.b] == half_id) continue;
                 stamp[p.a] = stamp[p.b] = half_id;
                 used[k] = 1;
                 --left;
                 ++filled;
-                out.push_back((uint32_t)p.a | ((uint32_t)p.b << 8) | ((uint32_t)p.tp << 16));
+                out.push_back((int)k);
             }
-            while (start < L.pairs.size() && used[start]) ++start;
-            while (filled++ < 16) out.push_back(kPairPad);
+            while (start < pairs.size() && used[start]) ++start;
+            while (filled++ < 16) out.push_back(-1);
         }
     }
     return out;
@@ -514,6 +829,7 @@ static std::unique_ptr<ud_batch_s> build_batch(ud_maps maps, const std::vector<c
         std::vector<NodeRec> nodes;
         std::vector<uint32_t> pairs;
         std::vector<uint32_t> grid_list;
+        std::vector<float> charges, coef;  // AD4 only
         for (int i = 0; i < n; ++i) {
             const Ligand& L = *ligs[i];
             if ((int)L.atoms.size() > kMaxLigAtoms)
@@ -552,15 +868,26 @@ static std::unique_ptr<ud_batch_s> build_batch(ud_maps maps, const std::vector<c
                 nodes.push_back(r);
             }
             d.grid_off = (int)grid_list.size();
+            const bool ad4 = maps->desc.ad4 != 0;
             for (const Atom& a : L.atoms) {
                 AtomRec r;
                 r.x = a.local[0];
                 r.y = a.local[1];
                 r.z = a.local[2];
-                int g = (a.xs < XS_SIZE) ? xs_grid_type(a.xs) : -1;
-                int slot = (g >= 0) ? maps->desc.slot_of_xs[g] : -1;
-                if (g >= 0 && slot < 0)
-                    throw Error(UD_ERR_ARG, std::string("no grid map for ligand atom type ") + xs_name(g));
+                int g, slot;
+                if (ad4) {  // every AD-typed atom but glue atoms; CG carbons read the C map (ad4cache.cpp:227-269)
+                    g = (a.ad < AD_SIZE && (a.ad < AD_G0 || a.ad > AD_G3)) ? a.ad : -1;
+                    if (g >= AD_CG0 && g <= AD_CG3) g = AD_C;
+                    slot = (g >= 0) ? maps->desc.slot_of_xs[g] : -1;
+                    if (g >= 0 && slot < 0)
+                        throw Error(UD_ERR_ARG, std::string("no AD4 map for ligand atom type ") + ad_kind(g).name);
+                    charges.push_back(a.charge);
+                } else {
+                    g = (a.xs < XS_SIZE) ? xs_grid_type(a.xs) : -1;
+                    slot = (g >= 0) ? maps->desc.slot_of_xs[g] : -1;
+                    if (g >= 0 && slot < 0)
+                        throw Error(UD_ERR_ARG, std::string("no grid map for ligand atom type ") + xs_name(g));
+                }
                 int heavy = (a.el != EL_H) ? 1 : 0;
                 int xsp = (a.xs < XS_SIZE) ? a.xs + 1 : 0;
                 r.packed = a.node | ((slot + 1) << 8) | (heavy << 16) | (xsp << 24);
@@ -568,9 +895,25 @@ static std::unique_ptr<ud_batch_s> build_batch(ud_maps maps, const std::vector<c
                 atoms.push_back(r);
             }
             d.n_grid = (int)grid_list.size() - d.grid_off;
-            std::vector<uint32_t> ordered = pair_groups(L);
-            pairs.insert(pairs.end(), ordered.begin(), ordered.end());
-            d.n_pairs = (int)ordered.size();
+            const std::vector<Pair>& plist = ad4 ? L.pairs_ad : L.pairs;
+            for (int k : pair_group_slots(L, plist)) {
+                if (k < 0) {
+                    pairs.push_back(kPairPad);
+                    if (ad4) {
+                        coef.push_back(0.0f);
+                        coef.push_back(0.0f);
+                    }
+                    continue;
+                }
+                const Pair& p = plist[k];
+                pairs.push_back((uint32_t)p.a | ((uint32_t)p.b << 8) | ((uint32_t)p.tp << 16));
+                if (ad4) {  // per-pair scales of the shared electrostatic and desolvation rows
+                    const Atom &x = L.atoms[p.a], &y = L.atoms[p.b];
+                    coef.push_back(x.charge * y.charge);
+                    coef.push_back(std::fabs(x.charge) * ad4_volume(y.ad) + std::fabs(y.charge) * ad4_volume(x.ad));
+                }
+            }
+            d.n_pairs = (int)pairs.size() - d.pair_off;
             b->desc.push_back(d);
             b->max_atoms = std::max(b->max_atoms, d.n_atoms);
             b->max_tors = std::max(b->max_tors, d.n_nodes - 1);
@@ -580,6 +923,10 @@ static std::unique_ptr<ud_batch_s> build_batch(ud_maps maps, const std::vector<c
         b->d_nodes.upload(nodes.data(), nodes.size(), s);
         b->d_pairs.upload(pairs.data(), pairs.size(), s);
         b->d_grid.upload(grid_list.data(), grid_list.size(), s);
+        if (maps->desc.ad4) {
+            b->d_charge.upload(charges.data(), charges.size(), s);
+            b->d_pair_coef.upload(coef.data(), coef.size(), s);
+        }
         cuda_check(cudaStreamSynchronize(s), "batch upload");
         return b;
 }
@@ -638,6 +985,8 @@ extern "C" int ud_score_grad(ud_batch b, const int* pose_ligand, const float* po
         b->d_pose.upload(poses, (size_t)n_poses * pose_stride, s);
         b->d_e.alloc(n_poses);
         b->d_g.alloc((size_t)n_poses * g_stride);
+        // entries past a pose's 6 + T gradient floats come back as 0
+        cuda_check(cudaMemsetAsync(b->d_g.p, 0, (size_t)n_poses * g_stride * sizeof(float), s), "memset");
         cuda_check(launch_score(b->view(), maps_view(b->maps), tables_view(b->maps), b->d_pose_lig.p, b->d_pose.p,
                                 pose_stride, n_poses, v_intra, v_inter, b->d_e.p, b->d_g.p, g_stride, nullptr, s),
                    "score kernel");
@@ -723,25 +1072,35 @@ static size_t term_map_block(const ud_maps_s* m) {
     const size_t plane = (size_t)m->desc.dims[0] * m->desc.dims[1] * m->desc.dims[2];
     return round4(plane * std::max(1, m->desc.n_maps));
 }
-static size_t n_type_pairs() { return (size_t)XS_SIZE * (XS_SIZE + 1) / 2; }
+static size_t table_rows(const ud_maps_s* m) {
+    return m->desc.ad4 ? (size_t)kAd4Rows : (size_t)XS_SIZE * (XS_SIZE + 1) / 2;
+}
 
 static void ensure_terms(ud_maps_s* m, cudaStream_t s) {
     if (m->terms_built) return;
+    if (m->loaded)
+        throw Error(UD_ERR_STATE, "maps read from files have no per-term decomposition (build them from the receptor)");
     const MapsDesc& d = m->desc;
     const int nt = m->sf.n_terms;
     const int nslot = d.n_maps, nslot_pad = std::max(4, (nslot + 3) & ~3);
     const size_t mblock = term_map_block(m);
-    const size_t rblock = n_type_pairs() * m->n_bins * 4;
-    const size_t fblock = round4(n_type_pairs() * m->n_bins);
+    const size_t rblock = table_rows(m) * m->n_bins * 4;
+    const size_t fblock = round4(table_rows(m) * m->n_bins);
     m->term_maps.alloc((size_t)nt * mblock);
     m->term_rows.alloc((size_t)nt * rblock);
     m->term_fast.alloc((size_t)nt * fblock);
     cuda_check(cudaMemsetAsync(m->term_maps.p, 0, (size_t)nt * mblock * sizeof(float), s), "memset");
     cuda_check(cudaMemsetAsync(m->term_fast.p, 0, (size_t)nt * fblock * sizeof(float), s), "memset");
     DevBuf<float> d_rec;
-    d_rec.upload(m->rec_xyzt.data(), m->rec_xyzt.size(), s);
+    DevBuf<int> d_ad;
+    if (d.ad4) {
+        d_rec.upload(m->rec_xyzq.data(), m->rec_xyzq.size(), s);
+        d_ad.upload(m->rec_ad.data(), m->rec_ad.size(), s);
+    } else {
+        d_rec.upload(m->rec_xyzt.data(), m->rec_xyzt.size(), s);
+    }
     DevBuf<float> d_fastT;
-    std::vector<float> rows(rblock), fastT((size_t)XS_SIZE * m->n_bins * nslot_pad, 0.0f);
+    std::vector<float> rows(rblock), fastT(d.ad4 ? 0 : (size_t)XS_SIZE * m->n_bins * nslot_pad, 0.0f);
     for (int t = 0; t < nt; ++t) {
         PairTable tab;
         tab.build(m->sf, t);
@@ -753,12 +1112,19 @@ static void ensure_terms(ud_maps_s* m, cudaStream_t s) {
         cuda_check(cudaMemcpyAsync(m->term_fast.p + (size_t)t * fblock, tab.fast.data(), tab.fast.size() * sizeof(float),
                                    cudaMemcpyHostToDevice, s),
                    "H2D");
-        pack_fastT(tab, m->slot_types, nslot_pad, fastT.data());
-        d_fastT.upload(fastT.data(), fastT.size(), s);
-        if (nslot > 0)
-            cuda_check(launch_maps(d_rec.p, (int)(m->rec_xyzt.size() / 4), d_fastT.p, tab.n, nslot, nslot_pad,
-                                   tab.factor, m->cutoff2, d, m->term_maps.p + (size_t)t * mblock, s),
-                       "term maps kernel");
+        if (d.ad4) {
+            Ad4MapSpec spec = ad4_spec(m, t);
+            cuda_check(launch_maps_ad4(d_rec.p, d_ad.p, (int)m->rec_ad.size(), ad4_params(), spec, d,
+                                       m->term_maps.p + (size_t)t * mblock, s),
+                       "AD4 term maps kernel");
+        } else {
+            pack_fastT(tab, m->slot_types, nslot_pad, fastT.data());
+            d_fastT.upload(fastT.data(), fastT.size(), s);
+            if (nslot > 0)
+                cuda_check(launch_maps(d_rec.p, (int)(m->rec_xyzt.size() / 4), d_fastT.p, tab.n, nslot, nslot_pad,
+                                       tab.factor, m->cutoff2, d, m->term_maps.p + (size_t)t * mblock, s),
+                           "term maps kernel");
+        }
         // host rows / fastT and the table are reused or freed next round: wait for their copies
         cuda_check(cudaStreamSynchronize(s), "term maps sync");
     }
@@ -767,7 +1133,7 @@ static void ensure_terms(ud_maps_s* m, cudaStream_t s) {
 
 static DeviceTermsView terms_view(const ud_maps_s* m) {
     return DeviceTermsView{m->term_maps.p, m->term_rows.p, m->sf.n_terms, (long long)term_map_block(m),
-                           (long long)(n_type_pairs() * m->n_bins)};
+                           (long long)(table_rows(m) * m->n_bins)};
 }
 
 extern "C" int ud_maps_term_count(ud_maps maps, int* n_terms) {
@@ -791,8 +1157,8 @@ extern "C" int ud_maps_set_weights(ud_maps maps, const float* w, int n, void* st
             if (!std::isfinite(w[t])) throw Error(UD_ERR_ARG, "weights must be finite");
         cudaStream_t s = (cudaStream_t)stream;
         ensure_terms(maps, s);
-        const size_t rblock = n_type_pairs() * maps->n_bins * 4;
-        const size_t fblock = round4(n_type_pairs() * maps->n_bins);
+        const size_t rblock = table_rows(maps) * maps->n_bins * 4;
+        const size_t fblock = round4(table_rows(maps) * maps->n_bins);
         cuda_check(launch_combine_terms(maps->term_maps.p, (long long)term_map_block(maps), n, w, maps->maps.p, s),
                    "combine maps");
         cuda_check(launch_combine_terms(maps->term_rows.p, (long long)rblock, n, w, maps->smooth.p, s), "combine rows");
@@ -839,7 +1205,10 @@ extern "C" int ud_score_adjoint(ud_batch b, const int* pose_ligand, const float*
         b->d_pose_lig.upload(pose_ligand, n_poses, s);
         b->d_pose.upload(poses, (size_t)n_poses * pose_stride, s);
         b->d_e.alloc(n_poses);
-        if (g_out) b->d_g.alloc((size_t)n_poses * g_stride);
+        if (g_out) {  // entries past a pose's 7 + T gradient floats come back as 0
+            b->d_g.alloc((size_t)n_poses * g_stride);
+            cuda_check(cudaMemsetAsync(b->d_g.p, 0, (size_t)n_poses * g_stride * sizeof(float), s), "memset");
+        }
         if (dw_out) b->d_dw.alloc((size_t)n_poses * dw_stride);
         DeviceTermsView tv = b->maps->terms_built ? terms_view(b->maps) : DeviceTermsView{nullptr, nullptr, 0, 0, 0};
         cuda_check(launch_adjoint(b->view(), maps_view(b->maps), tables_view(b->maps), tv, (int)b->desc.size(),

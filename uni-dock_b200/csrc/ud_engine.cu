@@ -163,6 +163,8 @@ struct Batch {
     const NodeRec* nodes;
     const uint32_t* pairs;
     const uint32_t* grid_list;
+    const float* charges;    // AD4: per atom
+    const float2* pair_coef; // AD4: per pair slot (q_a q_b, |q_a| V_b + |q_b| V_a)
 };
 
 #ifndef UD_PAIR_BATCH
@@ -181,12 +183,17 @@ struct Tables {
     float cutoff2;
 };
 
+// AD4 pair-table rows scaled per pair: electrostatics and charge-dependent
+// desolvation (after the AD type-pair rows)
+constexpr int kAd4RowE = kAd4TableRowElec, kAd4RowG = kAd4TableRowDesolv;
+
 struct Maps {
     const float* data;     // [slot][z][y][x]
     int nx, ny, nz;
     float init[3], factor[3], factor_inv[3], dim_m1[3];
     float slope;
     float corner2[3];
+    int e_slot, d_slot;    // AD4: electrostatic and desolvation maps
 };
 
 // Shared-memory layout of one chain (float offsets).
@@ -229,6 +236,8 @@ struct Ctx {
     const NodeRec* nodes;
     const uint32_t* pairs;
     const uint32_t* grid;  // atom | slot << 8 of the atoms with a grid map
+    const float* q;        // AD4: atom charges
+    const float2* coef;    // AD4: per pair slot coefficients
     int n_atoms, R, T, n_pairs, max_depth, local_steps, n_grid;
     int lane;
 };
@@ -241,6 +250,8 @@ __device__ __forceinline__ Ctx make_ctx(const Batch& B, int lig, float* s) {
     c.nodes = B.nodes + __ldg(&d->node_off);
     c.pairs = B.pairs + __ldg(&d->pair_off);
     c.grid = B.grid_list + __ldg(&d->grid_off);
+    c.q = B.charges + __ldg(&d->atom_off);
+    c.coef = B.pair_coef + __ldg(&d->pair_off);
     c.n_grid = __ldg(&d->n_grid);
     c.n_atoms = __ldg(&d->n_atoms);
     c.R = __ldg(&d->n_nodes);
@@ -371,7 +382,7 @@ __device__ __forceinline__ float grid_eval(const Maps& M, int slot, const float*
 // Pair forces use the table's dE/dr / r column (precalculate.h:48-65) or, with
 // kExactPairs, the slope of the lerped energy itself (the exact derivative of
 // the computed energy, 2 factor (e_bin+1 - e_bin) per unit r^2).
-template <bool kExactPairs = false>
+template <bool kExactPairs = false, bool kAD4 = false>
 __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const Maps& M,
                                             const Tables& Tb, const float* conf, float* g,
                                             float v_intra, float v_inter) {
@@ -386,6 +397,14 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
         const int a = ga & 0xFF, slot = ga >> 8;
         float gx, gy, gz;
         e += grid_eval(M, slot, xyz + 3 * a, v_inter, gx, gy, gz, true);
+        if constexpr (kAD4) {  // electrostatic map x q, desolvation map x |q| (ad4cache.cpp:227-269)
+            const float q = __ldg(c.q + a), aq = fabsf(q);
+            float hx, hy, hz;
+            e += q * grid_eval(M, M.e_slot, xyz + 3 * a, v_inter, hx, hy, hz, true);
+            gx += q * hx; gy += q * hy; gz += q * hz;
+            e += aq * grid_eval(M, M.d_slot, xyz + 3 * a, v_inter, hx, hy, hz, true);
+            gx += aq * hx; gy += aq * hy; gz += aq * hz;
+        }
         frc[3 * a] = gx; frc[3 * a + 1] = gy; frc[3 * a + 2] = gz;
     }
     __syncwarp();
@@ -414,6 +433,15 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
                         remv[u] = rf - i1;
                         rv[u][0] = rx; rv[u][1] = ry; rv[u][2] = rz;
                         tv[u] = __ldg(Tb.smooth4 + (size_t)tp * Tb.n_bins + i1);
+                        if constexpr (kAD4) {  // + q_a q_b E(r) + (|q_a| V_b + |q_b| V_a) G(r)
+                            const float2 cf = __ldg(c.coef + ((g0 + u) << 5) + c.lane);
+                            const float4 te = __ldg(Tb.smooth4 + (size_t)kAd4RowE * Tb.n_bins + i1);
+                            const float4 tg = __ldg(Tb.smooth4 + (size_t)kAd4RowG * Tb.n_bins + i1);
+                            tv[u].x += cf.x * te.x + cf.y * tg.x;
+                            tv[u].y += cf.x * te.y + cf.y * tg.y;
+                            tv[u].z += cf.x * te.z + cf.y * tg.z;
+                            tv[u].w += cf.x * te.w + cf.y * tg.w;
+                        }
                         prv[u] = pr;
                     }
                 }
@@ -511,6 +539,7 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
 
 // Scoring-path energy (no gradient): grid with curl cap v, intramolecular
 // pairs from the nearest-bin `fast` table (model.cpp:867-886, cache.cpp:84-120).
+template <bool kAD4 = false>
 __device__ __forceinline__ void eval_score(const Ctx& c, const Layout& L, const Maps& M,
                                            const Tables& Tb, const float* conf, float v,
                                            float& e_grid, float& e_intra) {
@@ -521,6 +550,11 @@ __device__ __forceinline__ void eval_score(const Ctx& c, const Layout& L, const 
         const uint32_t ga = __ldg(c.grid + k);
         float gx, gy, gz;
         eg += grid_eval(M, ga >> 8, xyz + 3 * (ga & 0xFF), v, gx, gy, gz, false);
+        if constexpr (kAD4) {
+            const float q = __ldg(c.q + (ga & 0xFF));
+            eg += q * grid_eval(M, M.e_slot, xyz + 3 * (ga & 0xFF), v, gx, gy, gz, false);
+            eg += fabsf(q) * grid_eval(M, M.d_slot, xyz + 3 * (ga & 0xFF), v, gx, gy, gz, false);
+        }
     }
     for (int k = c.lane; k < c.n_pairs; k += 32) {
         uint32_t pr = __ldg(c.pairs + k);
@@ -530,7 +564,13 @@ __device__ __forceinline__ void eval_score(const Ctx& c, const Layout& L, const 
               dz = xyz[3 * a + 2] - xyz[3 * b + 2];
         float r2 = dx * dx + dy * dy + dz * dz;
         if (r2 < Tb.cutoff2) {
-            float t = __ldg(Tb.fast + (size_t)tp * Tb.n_bins + (int)(Tb.factor * r2));
+            const int bin = (int)(Tb.factor * r2);
+            float t = __ldg(Tb.fast + (size_t)tp * Tb.n_bins + bin);
+            if constexpr (kAD4) {
+                const float2 cf = __ldg(c.coef + k);
+                t += cf.x * __ldg(Tb.fast + (size_t)kAd4RowE * Tb.n_bins + bin) +
+                     cf.y * __ldg(Tb.fast + (size_t)kAd4RowG * Tb.n_bins + bin);
+            }
             if (t > 0 && v < 0.1f * kMaxFl) t *= (v < kEps) ? 0 : __fdividef(v, v + t);
             ei += t;
         }
@@ -734,7 +774,7 @@ struct Machine {
 // The MC chain of monte_carlo.cu:237-356 (mutate, BFGS at the hunt cap,
 // Metropolis at temperature T, refine improvements at the authentic cap, keep
 // the best) with the line search and BFGS iterations of bfgs.h:63-146.
-template <bool kSearch>
+template <bool kSearch, bool kAD4>
 __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const Tables& Tb,
                                             const SearchParams& P, const Layout& L, float* sw,
                                             const int* order, int n_items, int first_item,
@@ -952,7 +992,7 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
         }
         if (st == S_EXIT) return;
         // ---- the single evaluation site
-        m.last_e = eval_deriv(c, L, M, Tb, eval_x, eval_g, m.v, m.v);
+        m.last_e = eval_deriv<false, kAD4>(c, L, M, Tb, eval_x, eval_g, m.v, m.v);
         ++m.evals;
     }
 }
@@ -961,29 +1001,32 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
 #ifndef UD_SEARCH_MIN_BLOCKS
 #define UD_SEARCH_MIN_BLOCKS 8
 #endif
+template <bool kAD4>
 __global__ void __launch_bounds__(128, UD_SEARCH_MIN_BLOCKS) search_kernel(
     const __grid_constant__ Batch B, const __grid_constant__ Maps M, const __grid_constant__ Tables Tb,
     const __grid_constant__ SearchParams P, const __grid_constant__ Layout L, const int* order, int n_items,
     int first_item, unsigned int* queue, float* poses, int pose_stride, ChainResult* results) {
     extern __shared__ float smem[];
     float* sw = smem + (size_t)(threadIdx.x >> 5) * L.total;
-    run_machine<true>(B, M, Tb, P, L, sw, order, n_items, first_item, queue, poses, pose_stride, results,
-                      nullptr, 0, 0.f, nullptr, nullptr);
+    run_machine<true, kAD4>(B, M, Tb, P, L, sw, order, n_items, first_item, queue, poses, pose_stride, results,
+                            nullptr, 0, 0.f, nullptr, nullptr);
 }
 
 // Local optimisation from given poses (quasi_newton, quasi_newton.cpp:42-53):
 // one warp per pose, BFGS at curl cap v; poses updated in place.
+template <bool kAD4>
 __global__ void __launch_bounds__(128) optimize_kernel(
     const __grid_constant__ Batch B, const __grid_constant__ Maps M, const __grid_constant__ Tables Tb,
     const __grid_constant__ SearchParams P, const __grid_constant__ Layout L, const int* pose_lig,
     float* poses, int pose_stride, int n_poses, int max_steps, float v, float* e_out, int* evals_out) {
     extern __shared__ float smem[];
     float* sw = smem + (size_t)(threadIdx.x >> 5) * L.total;
-    run_machine<false>(B, M, Tb, P, L, sw, nullptr, n_poses, 0, nullptr, poses, pose_stride, nullptr,
-                       pose_lig, max_steps, v, e_out, evals_out);
+    run_machine<false, kAD4>(B, M, Tb, P, L, sw, nullptr, n_poses, 0, nullptr, poses, pose_stride, nullptr,
+                             pose_lig, max_steps, v, e_out, evals_out);
 }
 
 // Fixed poses: energy (search form, caps v_intra / v_inter) and gradient per pose.
+template <bool kAD4>
 __global__ void __launch_bounds__(128) score_kernel(
     const __grid_constant__ Batch B, const __grid_constant__ Maps M, const __grid_constant__ Tables Tb,
     const __grid_constant__ Layout L, const int* pose_lig, const float* poses, int pose_stride, int n_poses,
@@ -1000,13 +1043,13 @@ __global__ void __launch_bounds__(128) score_kernel(
     __syncwarp();
     if (g_out) {
         float* g = sw + L.g;
-        float e = eval_deriv(c, L, M, Tb, x, g, v_intra, v_inter);
+        float e = eval_deriv<false, kAD4>(c, L, M, Tb, x, g, v_intra, v_inter);
         for (int i = c.lane; i < 6 + c.T; i += 32) g_out[(size_t)pose * g_stride + i] = g[i];
         if (c.lane == 0) e_out[pose] = e;
     }
     if (score_out) {
         float eg, ei;
-        eval_score(c, L, M, Tb, x, v_inter, eg, ei);
+        eval_score<kAD4>(c, L, M, Tb, x, v_inter, eg, ei);
         if (c.lane == 0) {
             score_out[2 * pose] = eg;
             score_out[2 * pose + 1] = ei;
@@ -1074,6 +1117,7 @@ __device__ __forceinline__ float curl_slope(float e, float v) {
 // stored.  The orientation gradient is 2 (0, tau) (x) q for the torque tau
 // of a rotation applied on the left (quaternion_increment, quaternion.h), the
 // gradient tangent to the unit sphere at a unit q.
+template <bool kAD4>
 __global__ void __launch_bounds__(128) adjoint_kernel(
     const __grid_constant__ Batch B, const __grid_constant__ Maps M, const __grid_constant__ Tables Tb,
     const __grid_constant__ Layout L, const __grid_constant__ TermData TD, int n_ligands, const int* pose_lig,
@@ -1096,8 +1140,8 @@ __global__ void __launch_bounds__(128) adjoint_kernel(
     for (int i = c.lane; i < cs; i += 32) x[i] = poses[(size_t)pose * pose_stride + i];
     __syncwarp();
     float* g = sw + L.g;
-    const float e = exact ? eval_deriv<true>(c, L, M, Tb, x, g, v_intra, v_inter)
-                          : eval_deriv<false>(c, L, M, Tb, x, g, v_intra, v_inter);
+    const float e = exact ? eval_deriv<true, kAD4>(c, L, M, Tb, x, g, v_intra, v_inter)
+                          : eval_deriv<false, kAD4>(c, L, M, Tb, x, g, v_intra, v_inter);
     if (c.lane == 0) e_out[pose] = e;
     if (g_out) {
         float* go = g_out + (size_t)pose * g_stride;
@@ -1128,6 +1172,18 @@ __global__ void __launch_bounds__(128) adjoint_kernel(
 #pragma unroll
             for (int t = 0; t < kMaxTerms; ++t)
                 if (t < TD.n_terms) acc[t] += w * trilinear(M, TD.maps + t * TD.map_block + slot * plane, cell, frac);
+            if constexpr (kAD4) {
+                const float q = __ldg(c.q + a), aq = fabsf(q);
+                const float we = q * curl_slope(trilinear(M, M.data + M.e_slot * plane, cell, frac), v_inter);
+                const float wd = aq * curl_slope(trilinear(M, M.data + M.d_slot * plane, cell, frac), v_inter);
+#pragma unroll
+                for (int t = 0; t < kMaxTerms; ++t)
+                    if (t < TD.n_terms) {
+                        const float* tm = TD.maps + t * TD.map_block;
+                        acc[t] += we * trilinear(M, tm + M.e_slot * plane, cell, frac) +
+                                  wd * trilinear(M, tm + M.d_slot * plane, cell, frac);
+                    }
+            }
         }
         for (int k = c.lane; k < c.n_pairs; k += 32) {
             const uint32_t pr = __ldg(c.pairs + k);
@@ -1140,12 +1196,27 @@ __global__ void __launch_bounds__(128) adjoint_kernel(
             const float rf = Tb.factor * r2;
             const int i1 = (int)rf;
             const float rem = rf - i1;
-            const float4 row = __ldg(Tb.smooth4 + (size_t)tp * Tb.n_bins + i1);
+            float4 row = __ldg(Tb.smooth4 + (size_t)tp * Tb.n_bins + i1);
+            float2 cf = make_float2(0.f, 0.f);
+            if constexpr (kAD4) {
+                cf = __ldg(c.coef + k);
+                const float4 te = __ldg(Tb.smooth4 + (size_t)kAd4RowE * Tb.n_bins + i1);
+                const float4 tg = __ldg(Tb.smooth4 + (size_t)kAd4RowG * Tb.n_bins + i1);
+                row.x += cf.x * te.x + cf.y * tg.x;
+                row.z += cf.x * te.z + cf.y * tg.z;
+            }
             const float w = curl_slope(row.x + rem * (row.z - row.x), v_intra);
 #pragma unroll
             for (int t = 0; t < kMaxTerms; ++t)
                 if (t < TD.n_terms) {
-                    const float4 rt = __ldg(TD.rows + t * TD.row_block + (size_t)tp * Tb.n_bins + i1);
+                    const float4* tr = TD.rows + t * TD.row_block;
+                    float4 rt = __ldg(tr + (size_t)tp * Tb.n_bins + i1);
+                    if constexpr (kAD4) {
+                        const float4 te = __ldg(tr + (size_t)kAd4RowE * Tb.n_bins + i1);
+                        const float4 tg = __ldg(tr + (size_t)kAd4RowG * Tb.n_bins + i1);
+                        rt.x += cf.x * te.x + cf.y * tg.x;
+                        rt.z += cf.x * te.z + cf.y * tg.z;
+                    }
                     acc[t] += w * (rt.x + rem * (rt.z - rt.x));
                 }
         }
@@ -1201,6 +1272,14 @@ __global__ void fp32_peak_kernel(float* out, int iters) {
 constexpr int kMapTX = 8, kMapTY = 4, kMapTZ = 4;
 constexpr int kMapThreads = kMapTX * kMapTY * kMapTZ;
 constexpr int kMaxSlots = 36;
+constexpr float kAd4ShortCut = 8.0f, kAd4LongCut = 20.48f, kAd4QsolvDev = 0.01097f;
+
+// x^n by repeated multiplication from 1 (int_pow, int_pow.h)
+__device__ __forceinline__ float ipow(float x, int n) {
+    float p = 1.0f;
+    for (int i = 0; i < n; ++i) p *= x;
+    return p;
+}
 
 __global__ void __launch_bounds__(kMapThreads) maps_kernel(
     const float4* __restrict__ rec, int n_rec, const float* __restrict__ fastT, int n_bins,
@@ -1285,6 +1364,135 @@ __global__ void __launch_bounds__(kMapThreads) maps_kernel(
     }
 }
 
+// ---------------------------------------------------------------- AD4 maps
+// AutoDock 4.2 grid maps computed from the AD4 pair terms
+// (potentials.h:346-486) at the exact probe-atom distances: one map per
+// requested AD type (vdW + H-bond within 8 A, the charge-independent part of
+// desolvation within 20.48 A), the electrostatic map per unit ligand charge
+// and the desolvation map per unit |ligand charge| -- the three maps
+// ad4cache::eval_deriv combines (ad4cache.cpp:227-269).  Receptor atoms of
+// the tile are staged in shared memory; one thread per grid point.
+__global__ void __launch_bounds__(kMapThreads) maps_ad4_kernel(
+    const float4* __restrict__ rec, const int* __restrict__ rec_ad, int n_rec, const __grid_constant__ Ad4Params P,
+    const __grid_constant__ Ad4MapSpec S, int nx, int ny, int nz, float init0, float init1, float init2,
+    float finv0, float finv1, float finv2, float* __restrict__ out) {
+    __shared__ float4 stage[kMapThreads];
+    __shared__ int stage_ad[kMapThreads];
+    __shared__ int warp_cnt[kMapThreads / 32];
+    const int tx = threadIdx.x % kMapTX, ty = (threadIdx.x / kMapTX) % kMapTY,
+              tz = threadIdx.x / (kMapTX * kMapTY);
+    const int gx0 = blockIdx.x * kMapTX, gy0 = blockIdx.y * kMapTY, gz0 = blockIdx.z * kMapTZ;
+    const int x = gx0 + tx, y = gy0 + ty, z = gz0 + tz;
+    const float lo[3] = {init0 + finv0 * gx0, init1 + finv1 * gy0, init2 + finv2 * gz0};
+    const float hi[3] = {init0 + finv0 * (gx0 + kMapTX - 1), init1 + finv1 * (gy0 + kMapTY - 1),
+                         init2 + finv2 * (gz0 + kMapTZ - 1)};
+    const float long2 = kAd4LongCut * kAd4LongCut, short2 = kAd4ShortCut * kAd4ShortCut;
+    const float reach2 = long2 * 1.0001f + 1e-3f;
+    const float px = init0 + finv0 * (float)x, py = init1 + finv1 * (float)y, pz = init2 + finv2 * (float)z;
+    float vh[kMaxSlots];
+#pragma unroll
+    for (int k = 0; k < kMaxSlots; ++k) vh[k] = 0.0f;
+    float sum_vg = 0.0f, sum_sg = 0.0f, sum_qe = 0.0f;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int base = 0; base < n_rec; base += kMapThreads) {
+        const int i = base + threadIdx.x;
+        bool take = false;
+        float4 a = make_float4(0, 0, 0, 0);
+        int aad = 0;
+        if (i < n_rec) {
+            a = rec[i];
+            aad = rec_ad[i];
+            float d2 = 0;
+            const float cc[3] = {a.x, a.y, a.z};
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float d = fmaxf(fmaxf(lo[k] - cc[k], cc[k] - hi[k]), 0.0f);
+                d2 += d * d;
+            }
+            take = d2 <= reach2;
+        }
+        const unsigned msk = __ballot_sync(kFull, take);
+        if (lane == 0) warp_cnt[wid] = __popc(msk);
+        __syncthreads();
+        int off = 0, tot = 0;
+        for (int w = 0; w < kMapThreads / 32; ++w) {
+            if (w < wid) off += warp_cnt[w];
+            tot += warp_cnt[w];
+        }
+        if (take) {
+            const int at = off + __popc(msk & ((1u << lane) - 1));
+            stage[at] = a;
+            stage_ad[at] = aad;
+        }
+        __syncthreads();
+        if (x < nx && y < ny && z < nz) {
+            for (int k = 0; k < tot; ++k) {
+                const float4 r = stage[k];
+                const float dx = r.x - px, dy = r.y - py, dz = r.z - pz;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                if (!(r2 < long2)) continue;
+                const float d = sqrtf(r2);
+                const int ra = stage_ad[k];
+                const float q = r.w;
+                // desolvation distance factor and electrostatics (cutoff 20.48 A)
+                const float xg = d / 3.6f;
+                const float g = expf(-0.5f * (xg * xg));
+                sum_vg += P.volume[ra] * g;
+                sum_sg += (P.solvation[ra] + kAd4QsolvDev * fabsf(q)) * g;
+                const float B = 78.4f + 8.5525f;
+                const float diel = -8.5525f + B / (1.0f + 7.7839f * expf(-B * 0.003627f * d));
+                const float einv = d < kEps ? 100.0f / diel : fminf(100.0f, 1.0f / (d * diel));
+                sum_qe += q * 332.0f * einv;
+                if (!(r2 < short2)) continue;
+#pragma unroll
+                for (int s = 0; s < kMaxSlots; ++s) {
+                    if (s >= S.n_slots) break;
+                    const int t = S.slot_ad[s];
+                    const float hbd = P.hb_depth[t] * P.hb_depth[ra];
+                    float rij, c_a, c_b;
+                    int pa, pb;
+                    if (hbd < 0) {  // H-bond 12-10
+                        rij = P.hb_radius[t] + P.hb_radius[ra];
+                        const float r10 = ipow(rij, 10);
+                        c_a = ipow(rij, 12) * -hbd * 10.0f / 2.0f;
+                        c_b = r10 * -hbd * 12.0f / 2.0f;
+                        pa = 12;
+                        pb = 10;
+                    } else {  // vdW 12-6
+                        rij = P.radius[t] + P.radius[ra];
+                        const float depth = sqrtf(P.depth[t] * P.depth[ra]);
+                        c_a = ipow(rij, 12) * depth;
+                        c_b = ipow(rij, 6) * depth * 2.0f;
+                        pa = 12;
+                        pb = 6;
+                    }
+                    float rs = d;  // smoothing 0.5
+                    if (rs > rij + 0.25f) rs -= 0.25f;
+                    else if (rs < rij - 0.25f) rs += 0.25f;
+                    else rs = rij;
+                    const float ra_ = ipow(rs, pa), rb_ = ipow(rs, pb);
+                    const float w = hbd < 0 ? S.w_hb : S.w_vdw;
+                    const float e = (ra_ > kEps && rb_ > kEps) ? fminf(100000.0f, c_a / ra_ - c_b / rb_) : 100000.0f;
+                    vh[s] += w * e;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (x < nx && y < ny && z < nz) {
+        const size_t plane = (size_t)nx * ny * nz;
+        const size_t idx = x + (size_t)nx * (y + (size_t)ny * z);
+#pragma unroll
+        for (int s = 0; s < kMaxSlots; ++s)
+            if (s < S.n_slots) {
+                const int t = S.slot_ad[s];
+                out[s * plane + idx] = vh[s] + S.w_dsolv * (P.solvation[t] * sum_vg + P.volume[t] * sum_sg);
+            }
+        out[S.n_slots * plane + idx] = S.w_elec * sum_qe;
+        out[(S.n_slots + 1) * plane + idx] = S.w_dsolv * kAd4QsolvDev * sum_vg;
+    }
+}
+
 }  // namespace dev
 
 // ---------------------------------------------------------------- host side
@@ -1305,6 +1513,8 @@ static dev::Maps to_maps(const DeviceMapsView& m) {
         M.corner2[i] = m.desc.corner2[i];
     }
     M.slope = m.desc.slope;
+    M.e_slot = m.desc.e_slot;
+    M.d_slot = m.desc.d_slot;
     return M;
 }
 
@@ -1325,6 +1535,8 @@ static dev::Batch to_batch(const DeviceBatchView& b) {
     B.nodes = b.nodes;
     B.pairs = b.pairs;
     B.grid_list = b.grid_list;
+    B.charges = b.charges;
+    B.pair_coef = reinterpret_cast<const float2*>(b.pair_coef);
     return B;
 }
 
@@ -1345,6 +1557,18 @@ cudaError_t launch_maps(const float* rec_xyzt, int n_rec, const float* fastT, in
     return cudaGetLastError();
 }
 
+cudaError_t launch_maps_ad4(const float* rec_xyzq, const int* rec_ad, int n_rec, const Ad4Params& params,
+                            const Ad4MapSpec& spec, const MapsDesc& d, float* out, cudaStream_t stream) {
+    if (spec.n_slots < 0 || spec.n_slots > dev::kMaxSlots) return cudaErrorInvalidValue;
+    dim3 block(dev::kMapThreads);
+    dim3 grid((d.dims[0] + dev::kMapTX - 1) / dev::kMapTX, (d.dims[1] + dev::kMapTY - 1) / dev::kMapTY,
+              (d.dims[2] + dev::kMapTZ - 1) / dev::kMapTZ);
+    dev::maps_ad4_kernel<<<grid, block, 0, stream>>>(reinterpret_cast<const float4*>(rec_xyzq), rec_ad, n_rec, params,
+                                                     spec, d.dims[0], d.dims[1], d.dims[2], d.init[0], d.init[1],
+                                                     d.init[2], d.factor_inv[0], d.factor_inv[1], d.factor_inv[2], out);
+    return cudaGetLastError();
+}
+
 static cudaError_t smem_attr(const void* fn, size_t smem) {
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
@@ -1356,10 +1580,11 @@ cudaError_t launch_score(const DeviceBatchView& b, const DeviceMapsView& m,
     dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
     const int warps = 4;
     size_t smem = (size_t)warps * L.total * sizeof(float);
-    cudaError_t e = smem_attr((const void*)dev::score_kernel, smem);
+    const auto kern = m.desc.ad4 ? dev::score_kernel<true> : dev::score_kernel<false>;
+    cudaError_t e = smem_attr((const void*)kern, smem);
     if (e != cudaSuccess) return e;
     dim3 grid((n_poses + warps - 1) / warps);
-    dev::score_kernel<<<grid, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t), L,
+    kern<<<grid, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t), L,
                                                           pose_lig, poses, pose_stride, n_poses,
                                                           v_intra, v_inter, e_out, g_out, g_stride,
                                                           score_out);
@@ -1374,7 +1599,8 @@ cudaError_t launch_adjoint(const DeviceBatchView& b, const DeviceMapsView& m, co
     dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
     const int warps = 4;
     size_t smem = (size_t)warps * L.total * sizeof(float);
-    cudaError_t e = smem_attr((const void*)dev::adjoint_kernel, smem);
+    const auto kern = m.desc.ad4 ? dev::adjoint_kernel<true> : dev::adjoint_kernel<false>;
+    cudaError_t e = smem_attr((const void*)kern, smem);
     if (e != cudaSuccess) return e;
     dev::TermData TD;
     TD.maps = terms.maps;
@@ -1383,7 +1609,7 @@ cudaError_t launch_adjoint(const DeviceBatchView& b, const DeviceMapsView& m, co
     TD.map_block = terms.map_block;
     TD.row_block = terms.row_block;
     dim3 grid((n_poses + warps - 1) / warps);
-    dev::adjoint_kernel<<<grid, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t), L, TD,
+    kern<<<grid, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t), L, TD,
                                                             n_ligands, pose_lig, poses, pose_stride, n_poses,
                                                             v_intra, v_inter, exact, e_out, g_out, g_stride, dw_out,
                                                             dw_stride);
@@ -1416,12 +1642,13 @@ cudaError_t launch_search(const DeviceBatchView& b, const DeviceMapsView& m,
     dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
     const int warps = 4;
     size_t smem = (size_t)warps * L.total * sizeof(float);
-    cudaError_t e = smem_attr((const void*)dev::search_kernel, smem);
+    const auto kern = m.desc.ad4 ? dev::search_kernel<true> : dev::search_kernel<false>;
+    cudaError_t e = smem_attr((const void*)kern, smem);
     if (e != cudaSuccess) return e;
     dim3 grid;
     if (P.persistent) grid = dim3(grid_blocks);
     else grid = dim3((n_items + warps - 1) / warps);
-    dev::search_kernel<<<grid, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t), P, L,
+    kern<<<grid, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t), P, L,
                                                            order, n_items, first_item, queue, poses,
                                                            pose_stride, results);
     return cudaGetLastError();
@@ -1434,11 +1661,12 @@ cudaError_t launch_optimize(const DeviceBatchView& b, const DeviceMapsView& m,
     dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
     const int warps = 4;
     size_t smem = (size_t)warps * L.total * sizeof(float);
-    cudaError_t e = smem_attr((const void*)dev::optimize_kernel, smem);
+    const auto kern = m.desc.ad4 ? dev::optimize_kernel<true> : dev::optimize_kernel<false>;
+    cudaError_t e = smem_attr((const void*)kern, smem);
     if (e != cudaSuccess) return e;
     SearchParams P{};
     dim3 grid((n_poses + warps - 1) / warps);
-    dev::optimize_kernel<<<grid, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t), P, L,
+    kern<<<grid, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t), P, L,
                                                              pose_lig, poses, pose_stride, n_poses,
                                                              max_steps, v, e_out, evals_out);
     return cudaGetLastError();
@@ -1476,10 +1704,10 @@ float measure_fp32_peak_tflops() {
 int search_blocks_per_sm(const DeviceBatchView& b, int warps) {
     dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
     size_t smem = (size_t)warps * L.total * sizeof(float);
-    smem_attr((const void*)dev::search_kernel, smem);
+    const auto kern = b.ad4 ? dev::search_kernel<true> : dev::search_kernel<false>;
+    smem_attr((const void*)kern, smem);
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, dev::search_kernel, warps * 32, smem) !=
-        cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, warps * 32, smem) != cudaSuccess)
         return 1;
     return nb > 0 ? nb : 1;
 }

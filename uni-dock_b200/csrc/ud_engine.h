@@ -25,8 +25,14 @@ struct MapsDesc {
     float corner2[3];      // box end
     float slope;           // out-of-box penalty slope
     int n_maps;
-    int8_t slot_of_xs[36]; // map slot per XS grid type, -1 when absent
+    int8_t slot_of_xs[36]; // map slot per XS grid type (per AD type for AD4), -1 when absent
+    int ad4;               // AutoDock 4.2 maps: type maps, then the electrostatic and desolvation maps
+    int e_slot, d_slot;    // AD4: slots of the electrostatic and desolvation maps
 };
+
+// AD4 pair-table rows scaled per pair (after the AD type-pair rows)
+constexpr int kAd4TableRowElec = 35 * 36 / 2;
+constexpr int kAd4TableRowDesolv = kAd4TableRowElec + 1;
 
 // One ligand's topology as it sits in device memory (offsets into the batch
 // arrays).  Nodes are in DFS pre-order: node k >= 1 owns torsion k - 1.
@@ -75,6 +81,19 @@ struct SearchParams {
     int bfgs_cap;          // 0: per-ligand local_steps; >0: min(local_steps, cap)
 };
 
+// AutoDock 4.2 atom-kind parameters indexed by AD type (atom_constants.h
+// ad_type_property) and the set of maps an AD4 map build computes.
+constexpr int kAdTypes = 35;
+struct Ad4Params {
+    float radius[kAdTypes], depth[kAdTypes], hb_depth[kAdTypes], hb_radius[kAdTypes];
+    float solvation[kAdTypes], volume[kAdTypes];
+};
+struct Ad4MapSpec {
+    int n_slots;           // type maps; the electrostatic and desolvation maps follow them
+    int slot_ad[36];       // AD type of each type map
+    float w_vdw, w_hb, w_elec, w_dsolv;
+};
+
 // Capacity of the allocation-free search (ud_search_device_noalloc).
 constexpr int kNoAllocMaxLigands = 8192;
 constexpr int kNoAllocMaxChains = 131072;
@@ -97,6 +116,9 @@ struct DeviceBatchView {
     const uint32_t* pairs;
     const uint32_t* grid_list;
     int max_atoms, max_torsions;
+    const float* charges;    // AD4: per atom
+    const float* pair_coef;  // AD4: float2 per pair slot
+    int ad4;
 };
 
 struct DeviceMapsView {
@@ -132,6 +154,10 @@ cudaError_t launch_adjoint(const DeviceBatchView& b, const DeviceMapsView& m, co
                            const DeviceTermsView& terms, int n_ligands, const int* pose_lig, const float* poses,
                            int pose_stride, int n_poses, float v_intra, float v_inter, int exact, float* e_out,
                            float* g_out, int g_stride, float* dw_out, int dw_stride, cudaStream_t stream);
+// AD4 maps: type maps of spec.slot_ad, then the electrostatic and desolvation
+// maps; receptor atoms as (x, y, z, charge) plus their AD types
+cudaError_t launch_maps_ad4(const float* rec_xyzq, const int* rec_ad, int n_rec, const Ad4Params& params,
+                            const Ad4MapSpec& spec, const MapsDesc& d, float* out, cudaStream_t stream);
 // out[i] = sum_t w[t] * in[t * block + i], i < block (a multiple of 4, 16-byte aligned buffers)
 cudaError_t launch_combine_terms(const float* in, long long block, int n_terms, const float* w, float* out,
                                  cudaStream_t stream);

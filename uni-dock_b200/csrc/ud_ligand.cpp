@@ -378,8 +378,9 @@ struct Builder {
                 int t2 = xs_typing ? lig.atoms[j].xs : lig.atoms[j].ad;
                 if (t1 < nt && t2 < nt) {
                     Pair p{i, j, tri_index(t1, t2)};
-                    if (glue_pair(i, j)) lig.glue_pairs.push_back(p);
-                    else lig.pairs.push_back(p);
+                    auto& dst = glue_pair(i, j) ? (xs_typing ? lig.glue_pairs : lig.glue_pairs_ad)
+                                                : (xs_typing ? lig.pairs : lig.pairs_ad);
+                    dst.push_back(p);
                 }
             }
         }
@@ -570,7 +571,13 @@ Ligand parse_ligand_pdbqt(const std::string& text, int atom_typing_xs) {
         for (int i = lig.nodes[k].begin; i < lig.nodes[k].end; ++i) lig.atoms[i].node = (int)k;
     B.assign_bonds();
     assign_types(lig.atoms);
-    B.make_pairs(atom_typing_xs != 0);
+    // both typings: the pair list of a batch follows its maps' scoring function
+    B.make_pairs(true);
+    B.make_pairs(false);
+    if (!atom_typing_xs) {
+        lig.pairs = lig.pairs_ad;
+        lig.glue_pairs = lig.glue_pairs_ad;
+    }
     return lig;
 }
 

@@ -70,6 +70,25 @@ struct Scoring {
     float conf_independent(float e, float num_tors, float torsdof) const;
 };
 
+// AutoDock 4.2 terms between AD-typed atoms, unweighted (potentials.h:346-486
+// with the parameters of scoring_function.h:74-86).
+constexpr float kAd4ShortCutoff = 8.0f;   // vdW and H-bond
+constexpr float kAd4LongCutoff = 20.48f;  // electrostatics and desolvation
+constexpr float kAd4Qsolv = 0.01097f;     // charge-dependent solvation factor
+float ad4_vdw(int t1, int t2, float r);
+float ad4_hb(int t1, int t2, float r);
+float ad4_elec_unit(float r);      // electrostatic energy of two unit charges
+float ad4_desolv_gauss(float r);   // distance factor exp(-r^2 / (2 sigma^2)) of desolvation
+float ad4_solvation(int ad);
+float ad4_volume(int ad);
+// AD4 pair-table rows: AD type pairs tri_index(t1, t2), then two rows shared by
+// all pairs and scaled per pair: electrostatics (times q1 q2) and the
+// charge-dependent desolvation (times |q1| V2 + |q2| V1).
+constexpr int kAd4TypePairs = AD_SIZE * (AD_SIZE + 1) / 2;
+constexpr int kAd4RowElec = kAd4TypePairs;
+constexpr int kAd4RowDesolv = kAd4TypePairs + 1;
+constexpr int kAd4Rows = kAd4TypePairs + 2;
+
 // r^2-binned tables with factor 32 (points per A^2): `fast` is the midpoint
 // average used for maps/scoring, `smooth` the (e, dE/dr / r) pairs for lerp.
 struct PairTable {
@@ -111,8 +130,10 @@ struct Ligand {
     std::string name;
     std::vector<Atom> atoms;
     std::vector<Node> nodes;           // DFS pre-order; node k >= 1 owns torsion k-1
-    std::vector<Pair> pairs;           // intramolecular pairs (1-4 and beyond)
+    std::vector<Pair> pairs;           // intramolecular pairs (1-4 and beyond), XS typing
     std::vector<Pair> glue_pairs;
+    std::vector<Pair> pairs_ad;        // the same with AutoDock typing (hydrogens included)
+    std::vector<Pair> glue_pairs_ad;
     std::vector<std::pair<std::string, int>> context;  // input lines; atom index or -1
     int torsdof = 0;
     bool sdf = false;

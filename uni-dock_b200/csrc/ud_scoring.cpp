@@ -6,7 +6,9 @@
 // unidock/src/lib/potentials.h:27-509.  Arithmetic is FP32 with the same
 // operation order as the reference so that the tables match bit for bit.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <limits>
 #include <stdexcept>
 
 #include "ud_model.h"
@@ -216,6 +218,97 @@ float Scoring::term_types(int k, int t1, int t2, float r) const {
     return 0.0f;
 }
 
+// ---------------------------------------------------------------- AutoDock 4.2
+// potentials.h:346-486.  The reference computes in float (fl) with double
+// literals promoting some subexpressions; the same promotions are kept.
+static float int_pow_f(float x, int n) {
+    float p = 1.0f;
+    for (int i = 0; i < n; ++i) p = p * x;
+    return p;
+}
+
+static float ad4_smoothen(float r, float rij, float smoothing) {  // potentials.h:66-77
+    smoothing *= 0.5f;
+    if (r > rij + smoothing) return r - smoothing;
+    if (r < rij - smoothing) return r + smoothing;
+    return rij;
+}
+
+float ad4_vdw(int t1, int t2, float r) {
+    const float cap = 100000.0f, smoothing = 0.5f;
+    if (r >= kAd4ShortCutoff) return 0.0f;
+    const AdKind &a = ad_kind(t1), &b = ad_kind(t2);
+    const float hb_depth = a.hb_depth * b.hb_depth;
+    const float vdw_rij = a.radius + b.radius;
+    const float vdw_depth = std::sqrt(a.depth * b.depth);
+    if (hb_depth < 0) return 0.0f;  // an H-bond pair, not vdW
+    r = ad4_smoothen(r, vdw_rij, smoothing);
+    const float c_12 = int_pow_f(vdw_rij, 12) * vdw_depth;
+    const float c_6 = (float)((double)(int_pow_f(vdw_rij, 6) * vdw_depth) * 2.0);
+    const float r6 = int_pow_f(r, 6), r12 = int_pow_f(r, 12);
+    const float eps = std::numeric_limits<float>::epsilon();
+    if (r12 > eps && r6 > eps) return std::min(cap, c_12 / r12 - c_6 / r6);
+    return cap;
+}
+
+float ad4_hb(int t1, int t2, float r) {
+    const float cap = 100000.0f, smoothing = 0.5f;
+    if (r >= kAd4ShortCutoff) return 0.0f;
+    const AdKind &a = ad_kind(t1), &b = ad_kind(t2);
+    const float hb_rij = a.hb_radius + b.hb_radius;
+    const float hb_depth = a.hb_depth * b.hb_depth;
+    if (hb_depth >= 0) return 0.0f;  // a vdW pair, not H-bond
+    r = ad4_smoothen(r, hb_rij, smoothing);
+    const float c_12 = (float)((double)(int_pow_f(hb_rij, 12) * -hb_depth * 10) / 2.0);
+    const float c_10 = (float)((double)(int_pow_f(hb_rij, 10) * -hb_depth * 12) / 2.0);
+    const float r10 = int_pow_f(r, 10), r12 = int_pow_f(r, 12);
+    const float eps = std::numeric_limits<float>::epsilon();
+    if (r12 > eps && r10 > eps) return std::min(cap, c_12 / r12 - c_10 / r10);
+    return cap;
+}
+
+float ad4_elec_unit(float r) {
+    const float cap = 100.0f;
+    if (r >= kAd4LongCutoff) return 0.0f;
+    const float q1q2 = (float)(1.0 * 332.0);
+    const float B = (float)(78.4 + 8.5525);
+    const float lB = (float)(-(double)B * 0.003627);
+    const float diel = (float)(-8.5525 + ((double)B / (1 + 7.7839 * (double)std::exp(lB * r))));
+    if (r < std::numeric_limits<float>::epsilon()) return q1q2 * cap / diel;
+    return q1q2 * std::min(cap, 1.0f / (r * diel));
+}
+
+float ad4_desolv_gauss(float r) {
+    const float sigma = 3.6f;
+    if (r >= kAd4LongCutoff) return 0.0f;
+    const float x = r / sigma;
+    return (float)std::exp(-0.5 * (double)(x * x));
+}
+
+float ad4_solvation(int ad) { return ad < AD_SIZE ? ad_kind(ad).solvation : -0.00110f; }
+float ad4_volume(int ad) { return ad < AD_SIZE ? ad_kind(ad).volume : 0.0f; }
+
+// AD4 row `row` (kAd4Rows layout) at r for term k (< 0: weighted sum of all).
+static float ad4_row_value(const Scoring& sf, int row, int k, float r) {
+    auto w = [&](int t) { return k < 0 ? sf.weights[t] : (k == t ? 1.0f : 0.0f); };
+    if (row == kAd4RowElec) return w(2) * ad4_elec_unit(r);
+    if (row == kAd4RowDesolv) return w(3) * (float)((double)kAd4Qsolv * ad4_desolv_gauss(r));
+    int t1 = 0, t2 = 0;  // invert tri_index
+    while ((t2 + 1) * (t2 + 2) / 2 <= row) ++t2;
+    t1 = row - t2 * (t2 + 1) / 2;
+    float acc = 0.0f;
+    acc += w(0) * ad4_vdw(t1, t2, r);
+    acc += w(1) * ad4_hb(t1, t2, r);
+    const float s1 = ad4_solvation(t1), s2 = ad4_solvation(t2), v1 = ad4_volume(t1), v2 = ad4_volume(t2);
+    acc += w(3) * ((s1 * v2 + s2 * v1) * ad4_desolv_gauss(r));
+    const bool glued = (t1 == AD_G0 && t2 == AD_CG0) || (t1 == AD_G1 && t2 == AD_CG1) ||
+                       (t1 == AD_G2 && t2 == AD_CG2) || (t1 == AD_G3 && t2 == AD_CG3) ||
+                       (t2 == AD_G0 && t1 == AD_CG0) || (t2 == AD_G1 && t1 == AD_CG1) ||
+                       (t2 == AD_G2 && t1 == AD_CG2) || (t2 == AD_G3 && t1 == AD_CG3);
+    if (glued && r < 20.0f) acc += w(4) * r;
+    return acc;
+}
+
 float Scoring::eval_types(int t1, int t2, float r) const {
     float acc = 0;
     for (int k = 0; k < n_terms; ++k) acc += weights[k] * term_types(k, t1, t2, r);
@@ -284,6 +377,20 @@ void PairTable::build(const Scoring& sf, int term) {
     factor = 32.0f;
     const float cut2 = sf.max_cutoff * sf.max_cutoff;
     n = (int)(std::size_t)(factor * cut2) + 3;
+    if (sf.choice == SF_AD42) {  // AD type pairs + the two per-pair scaled rows
+        n_types = AD_SIZE;
+        const int rows = kAd4Rows;
+        fast.assign((std::size_t)rows * n, 0.0f);
+        smooth.assign((std::size_t)rows * n * 2, 0.0f);
+        std::vector<float> rs(n), e(n);
+        for (int i = 0; i < n; ++i) rs[i] = std::sqrt((float)i / factor);
+        for (int row = 0; row < rows; ++row) {
+            for (int i = 0; i < n; ++i) e[i] = ad4_row_value(sf, row, term, rs[i]);
+            table_row_from_energies(e.data(), rs.data(), n, &fast[(std::size_t)row * n],
+                                    &smooth[(std::size_t)row * n * 2]);
+        }
+        return;
+    }
     n_types = XS_SIZE;
     const int ntp = n_types * (n_types + 1) / 2;
     fast.assign((std::size_t)ntp * n, 0.0f);

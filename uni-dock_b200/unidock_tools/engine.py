@@ -99,6 +99,11 @@ def lib():
         "ud_optimize": ([vp, ip, fp, C.c_int, C.c_int, C.c_int, C.c_float, fp, ip, vp], C.c_int),
         "ud_device_fp32_peak": ([fp], C.c_int),
         "ud_maps_term_count": ([vp, ip], C.c_int),
+        "ud_receptor_parse_ex": ([C.c_char_p, C.c_size_t, fp, ip, ip, fp, C.c_int, ip], C.c_int),
+        "ud_maps_create_ad4": ([fp, C.c_int, fp, ip, fp, C.c_int, fp, fp, C.c_float, ip, C.c_int, vp,
+                                C.POINTER(vp)], C.c_int),
+        "ud_maps_write": ([vp, C.c_char_p], C.c_int),
+        "ud_maps_load": ([C.c_int, fp, C.c_int, C.c_char_p, vp, C.POINTER(vp)], C.c_int),
         "ud_autotune": ([vp, C.POINTER(SearchParams), C.POINTER(TuneResult), vp], C.c_int),
         "ud_maps_get_weights": ([vp, fp, C.c_int], C.c_int),
         "ud_maps_set_weights": ([vp, fp, C.c_int, vp], C.c_int),
@@ -113,6 +118,19 @@ def lib():
         f.restype = res
     _lib = L
     return L
+
+
+def parse_receptor_ex(text: str):
+    """(xyz, xs, ad, charge) of a receptor PDBQT (ud_receptor_parse_ex)."""
+    b = text.encode()
+    n = C.c_int()
+    _check(lib().ud_receptor_parse_ex(b, len(b), None, None, None, None, 0, C.byref(n)))
+    xyz = np.zeros((n.value, 3), np.float32)
+    xs = np.zeros(n.value, np.int32)
+    ad = np.zeros(n.value, np.int32)
+    q = np.zeros(n.value, np.float32)
+    _check(lib().ud_receptor_parse_ex(b, len(b), _f(xyz), _i(xs), _i(ad), _f(q), n.value, C.byref(n)))
+    return xyz, xs, ad, q
 
 
 def exported_symbols():
@@ -153,10 +171,14 @@ def parse_receptor(pdbqt: str):
 
 
 class Maps:
-    """Receptor grid maps on the GPU (ud_maps_create)."""
+    """Receptor grid maps on the GPU (ud_maps_create; ud_maps_create_ad4 for
+    sf=SF_AD4, where `rec_xs` holds AD types and `charges` the receptor charges)."""
 
     def __init__(self, rec_xyz, rec_xs, center, size, spacing=0.375, sf=SF_VINA, weights=None,
-                 types=None):
+                 types=None, charges=None):
+        if sf == SF_AD4:
+            self._init_ad4(rec_xyz, rec_xs, charges, center, size, spacing, weights, types)
+            return
         rec_xyz = np.ascontiguousarray(rec_xyz, np.float32)
         rec_xs = np.ascontiguousarray(rec_xs, np.int32)
         center = np.ascontiguousarray(center, np.float32)
@@ -178,6 +200,38 @@ class Maps:
         n = C.c_int()
         _check(lib().ud_maps_info(self.h, _i(d), _f(init), _f(fac), C.byref(n)))
         return d, init, fac, n.value
+
+    def _init_ad4(self, rec_xyz, rec_ad, charges, center, size, spacing, weights, types):
+        rec_xyz = np.ascontiguousarray(rec_xyz, np.float32)
+        rec_ad = np.ascontiguousarray(rec_ad, np.int32)
+        q = np.ascontiguousarray(charges, np.float32)
+        center = np.ascontiguousarray(center, np.float32)
+        size = np.ascontiguousarray(size, np.float32)
+        w = None if weights is None else np.ascontiguousarray(weights, np.float32)
+        t = None if types is None else np.ascontiguousarray(types, np.int32)
+        h = C.c_void_p()
+        _check(lib().ud_maps_create_ad4(None if w is None else _f(w), 0 if w is None else len(w), _f(rec_xyz),
+                                        _i(rec_ad), _f(q), len(rec_ad), _f(center), _f(size), float(spacing),
+                                        None if t is None else _i(t), 0 if t is None else len(t), None,
+                                        C.byref(h)))
+        self.h = h
+        self.sf = SF_AD4
+
+    @classmethod
+    def load(cls, prefix, sf=SF_VINA, weights=None):
+        """Maps read from AutoGrid .map files (ud_maps_load, the reference's --maps)."""
+        self = cls.__new__(cls)
+        w = None if weights is None else np.ascontiguousarray(weights, np.float32)
+        h = C.c_void_p()
+        _check(lib().ud_maps_load(sf, None if w is None else _f(w), 0 if w is None else len(w),
+                                  str(prefix).encode(), None, C.byref(h)))
+        self.h = h
+        self.sf = sf
+        return self
+
+    def write(self, prefix):
+        """AutoGrid .map files <prefix>.<type>.map (ud_maps_write)."""
+        _check(lib().ud_maps_write(self.h, str(prefix).encode()))
 
     @property
     def n_terms(self):
