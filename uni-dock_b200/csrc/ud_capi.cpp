@@ -791,28 +791,31 @@ extern "C" int ud_ligand_destroy(ud_ligand lig) {
 // 0-15 and 16-31 are each a matching (no atom twice), so the two half-warps can
 // add their pair forces into shared memory one after the other without
 // atomics.  Unfilled slots hold kPairPad; the list length is a multiple of 32.
-// Index into `pairs` of every slot of the conflict-free 32-slot groups, -1 for padding.
+// Index into `pairs` of every slot of the conflict-free 32-slot groups, -1 for
+// padding: each group is kPairPasses lane ranges of kPairPassWidth slots, and
+// no atom occurs twice within a range (the kernel adds one range's forces at a
+// time).  Ranges are filled greedily in pair order.
 static std::vector<int> pair_group_slots(const Ligand& L, const std::vector<Pair>& pairs) {
     std::vector<int> out;
     std::vector<char> used(pairs.size(), 0);
     std::vector<int> stamp(L.atoms.size(), -1);
     size_t left = pairs.size(), start = 0;
-    int half_id = 0;
+    int range_id = 0;
     while (left > 0) {
-        for (int half = 0; half < 2; ++half, ++half_id) {
+        for (int r = 0; r < kPairPasses; ++r, ++range_id) {
             int filled = 0;
-            for (size_t k = start; k < pairs.size() && filled < 16; ++k) {
+            for (size_t k = start; k < pairs.size() && filled < kPairPassWidth; ++k) {
                 if (used[k]) continue;
                 const Pair& p = pairs[k];
-                if (stamp[p.a] == half_id || stamp[p.b] == half_id) continue;
-                stamp[p.a] = stamp[p.b] = half_id;
+                if (stamp[p.a] == range_id || stamp[p.b] == range_id) continue;
+                stamp[p.a] = stamp[p.b] = range_id;
                 used[k] = 1;
                 --left;
                 ++filled;
                 out.push_back((int)k);
             }
             while (start < pairs.size() && used[start]) ++start;
-            while (filled++ < 16) out.push_back(-1);
+            while (filled++ < kPairPassWidth) out.push_back(-1);
         }
     }
     return out;

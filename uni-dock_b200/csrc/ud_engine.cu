@@ -220,8 +220,8 @@ __host__ inline Layout make_layout(int max_atoms, int max_tors) {
     L.g = take(gs); L.gnew = take(gs); L.gorig = take(gs); L.p = take(gs); L.y = take(gs);
     L.mhy = take(gs);
     L.h = take(gs * gs);
-    L.coords = take(3 * max_atoms);
-    L.forces = take(3 * max_atoms);
+    L.coords = take(4 * max_atoms);   // float4 per atom (x, y, z, unused)
+    L.forces = take(4 * max_atoms);
     L.frames = take(20 * R);
     L.prefix = take(6 * max_atoms);
     L.misc = take(32);
@@ -309,25 +309,27 @@ __device__ __forceinline__ void kinematics(const Ctx& c, const Layout& L, const 
         }
         __syncwarp();
     }
-    float* xyz = c.s + L.coords;
+    float4* xyz = reinterpret_cast<float4*>(c.s + L.coords);
     for (int a = c.lane; a < c.n_atoms; a += 32) {
         AtomRec ar = c.atoms[a];
         int n = ar.packed & 0xFF;
         const float* f = fr + 20 * n;
         const float* m = f + 7;
+        float o[3];
 #pragma unroll
-        for (int i = 0; i < 3; ++i)
-            xyz[3 * a + i] = f[i] + (m[3 * i] * ar.x + m[3 * i + 1] * ar.y + m[3 * i + 2] * ar.z);
+        for (int i = 0; i < 3; ++i) o[i] = f[i] + (m[3 * i] * ar.x + m[3 * i + 1] * ar.y + m[3 * i + 2] * ar.z);
+        xyz[a] = make_float4(o[0], o[1], o[2], 0.0f);
     }
     __syncwarp();
 }
 
 // Trilinear map energy, gradient and out-of-box penalty of one atom.
-__device__ __forceinline__ float grid_eval(const Maps& M, int slot, const float* p, float v,
+__device__ __forceinline__ float grid_eval(const Maps& M, int slot, const float4 pos, float v,
                                            float& gx, float& gy, float& gz, bool want_deriv) {
     float s[3], miss[3];
     int reg[3], a[3];
     const int dims[3] = {M.nx, M.ny, M.nz};
+    const float p[3] = {pos.x, pos.y, pos.z};
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
         float si = (p[i] - M.init[i]) * M.factor[i];
@@ -387,30 +389,32 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
                                             const Tables& Tb, const float* conf, float* g,
                                             float v_intra, float v_inter) {
     kinematics(c, L, conf);
-    const float* xyz = c.s + L.coords;
-    float* frc = c.s + L.forces;
+    const float4* xyz = reinterpret_cast<const float4*>(c.s + L.coords);
+    float4* frc = reinterpret_cast<float4*>(c.s + L.forces);
     float e = 0;
-    for (int k = c.lane; k < 3 * c.n_atoms; k += 32) frc[k] = 0;
+    for (int k = c.lane; k < c.n_atoms; k += 32) frc[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     __syncwarp();
     for (int k = c.lane; k < c.n_grid; k += 32) {
         const uint32_t ga = __ldg(c.grid + k);
         const int a = ga & 0xFF, slot = ga >> 8;
         float gx, gy, gz;
-        e += grid_eval(M, slot, xyz + 3 * a, v_inter, gx, gy, gz, true);
+        const float4 pa = xyz[a];
+        e += grid_eval(M, slot, pa, v_inter, gx, gy, gz, true);
         if constexpr (kAD4) {  // electrostatic map x q, desolvation map x |q| (ad4cache.cpp:227-269)
             const float q = __ldg(c.q + a), aq = fabsf(q);
             float hx, hy, hz;
-            e += q * grid_eval(M, M.e_slot, xyz + 3 * a, v_inter, hx, hy, hz, true);
+            e += q * grid_eval(M, M.e_slot, pa, v_inter, hx, hy, hz, true);
             gx += q * hx; gy += q * hy; gz += q * hz;
-            e += aq * grid_eval(M, M.d_slot, xyz + 3 * a, v_inter, hx, hy, hz, true);
+            e += aq * grid_eval(M, M.d_slot, pa, v_inter, hx, hy, hz, true);
             gx += aq * hx; gy += aq * hy; gz += aq * hz;
         }
-        frc[3 * a] = gx; frc[3 * a + 1] = gy; frc[3 * a + 2] = gz;
+        frc[a] = make_float4(gx, gy, gz, 0.0f);
     }
     __syncwarp();
-    // Pairs in 32-slot groups whose two half-warps are matchings (no atom twice
-    // within a half): table rows of kPairBatch groups are loaded before any is
-    // consumed, then each half-warp adds its forces in turn (no atomics).
+    // Pairs in 32-slot groups made of kPairPasses lane ranges that are each a
+    // matching (no atom twice within a range): table rows of kPairBatch groups
+    // are loaded before any is consumed, then each range adds its forces in
+    // turn (no atomics, a fixed summation order).
     const int n_groups = c.n_pairs >> 5;
     for (int g0 = 0; g0 < n_groups; g0 += kPairBatch) {
         float4 tv[kPairBatch];
@@ -424,8 +428,8 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
                 uint32_t pr = __ldg(c.pairs + ((g0 + u) << 5) + c.lane);
                 if (pr != kPairPad) {
                     int a = pr & 0xFF, b = (pr >> 8) & 0xFF, tp = pr >> 16;
-                    float rx = xyz[3 * b] - xyz[3 * a], ry = xyz[3 * b + 1] - xyz[3 * a + 1],
-                          rz = xyz[3 * b + 2] - xyz[3 * a + 2];
+                    const float4 pa = xyz[a], pb = xyz[b];
+                    float rx = pb.x - pa.x, ry = pb.y - pa.y, rz = pb.z - pa.z;
                     float r2 = rx * rx + ry * ry + rz * rz;
                     if (r2 < Tb.cutoff2) {
                         float rf = Tb.factor * r2;
@@ -467,10 +471,13 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
             }
             const int a = prv[u] & 0xFF, b = (prv[u] >> 8) & 0xFF;
 #pragma unroll
-            for (int half = 0; half < 2; ++half) {
-                if (live && (c.lane >> 4) == half) {
-                    frc[3 * a] -= fx; frc[3 * a + 1] -= fy; frc[3 * a + 2] -= fz;
-                    frc[3 * b] += fx; frc[3 * b + 1] += fy; frc[3 * b + 2] += fz;
+            for (int pass = 0; pass < kPairPasses; ++pass) {
+                if (live && c.lane / kPairPassWidth == pass) {
+                    float4 fa = frc[a], fb = frc[b];
+                    fa.x -= fx; fa.y -= fy; fa.z -= fz;
+                    fb.x += fx; fb.y += fy; fb.z += fz;
+                    frc[a] = fa;
+                    frc[b] = fb;
                 }
                 __syncwarp();
             }
@@ -489,8 +496,9 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
         const int a = base + c.lane;
         float v[6] = {0, 0, 0, 0, 0, 0};
         if (a < c.n_atoms) {
-            const float f0 = frc[3 * a], f1 = frc[3 * a + 1], f2 = frc[3 * a + 2];
-            const float r0 = xyz[3 * a] - fr[0], r1 = xyz[3 * a + 1] - fr[1], r2 = xyz[3 * a + 2] - fr[2];
+            const float4 fa = frc[a], xa = xyz[a];
+            const float f0 = fa.x, f1 = fa.y, f2 = fa.z;
+            const float r0 = xa.x - fr[0], r1 = xa.y - fr[1], r2 = xa.z - fr[2];
             v[0] = f0; v[1] = f1; v[2] = f2;
             v[3] = r1 * f2 - r2 * f1;
             v[4] = r2 * f0 - r0 * f2;
@@ -544,24 +552,25 @@ __device__ __forceinline__ void eval_score(const Ctx& c, const Layout& L, const 
                                            const Tables& Tb, const float* conf, float v,
                                            float& e_grid, float& e_intra) {
     kinematics(c, L, conf);
-    const float* xyz = c.s + L.coords;
+    const float4* xyz = reinterpret_cast<const float4*>(c.s + L.coords);
     float eg = 0, ei = 0;
     for (int k = c.lane; k < c.n_grid; k += 32) {
         const uint32_t ga = __ldg(c.grid + k);
         float gx, gy, gz;
-        eg += grid_eval(M, ga >> 8, xyz + 3 * (ga & 0xFF), v, gx, gy, gz, false);
+        const float4 pa = xyz[ga & 0xFF];
+        eg += grid_eval(M, ga >> 8, pa, v, gx, gy, gz, false);
         if constexpr (kAD4) {
             const float q = __ldg(c.q + (ga & 0xFF));
-            eg += q * grid_eval(M, M.e_slot, xyz + 3 * (ga & 0xFF), v, gx, gy, gz, false);
-            eg += fabsf(q) * grid_eval(M, M.d_slot, xyz + 3 * (ga & 0xFF), v, gx, gy, gz, false);
+            eg += q * grid_eval(M, M.e_slot, pa, v, gx, gy, gz, false);
+            eg += fabsf(q) * grid_eval(M, M.d_slot, pa, v, gx, gy, gz, false);
         }
     }
     for (int k = c.lane; k < c.n_pairs; k += 32) {
         uint32_t pr = __ldg(c.pairs + k);
         if (pr == kPairPad) continue;
         int a = pr & 0xFF, b = (pr >> 8) & 0xFF, tp = pr >> 16;
-        float dx = xyz[3 * a] - xyz[3 * b], dy = xyz[3 * a + 1] - xyz[3 * b + 1],
-              dz = xyz[3 * a + 2] - xyz[3 * b + 2];
+        const float4 pa = xyz[a], pb = xyz[b];
+        float dx = pa.x - pb.x, dy = pa.y - pb.y, dz = pa.z - pb.z;
         float r2 = dx * dx + dy * dy + dz * dz;
         if (r2 < Tb.cutoff2) {
             const int bin = (int)(Tb.factor * r2);
@@ -709,13 +718,14 @@ __device__ void mutate(const Ctx& c, const Layout& L, Philox& rng, float amplitu
     const int which = __float_as_int(misc[0]);
     if (which == 1) {
         // gyration radius of heavy atoms about the root origin (model.cpp:853-865)
-        const float* xyz = c.s + L.coords;
+        const float4* xyz = reinterpret_cast<const float4*>(c.s + L.coords);
         const float* o = c.s + L.frames;
         float acc = 0, cnt = 0;
         for (int a = c.lane; a < c.n_atoms; a += 32) {
             int packed = __ldg(&c.atoms[a].packed);
             if ((packed >> 16) & 1) {
-                float dx = xyz[3 * a] - o[0], dy = xyz[3 * a + 1] - o[1], dz = xyz[3 * a + 2] - o[2];
+                const float4 pa = xyz[a];
+                float dx = pa.x - o[0], dy = pa.y - o[1], dz = pa.z - o[2];
                 acc += dx * dx + dy * dy + dz * dz;
                 cnt += 1;
             }
@@ -1006,7 +1016,7 @@ __global__ void __launch_bounds__(128, UD_SEARCH_MIN_BLOCKS) search_kernel(
     const __grid_constant__ Batch B, const __grid_constant__ Maps M, const __grid_constant__ Tables Tb,
     const __grid_constant__ SearchParams P, const __grid_constant__ Layout L, const int* order, int n_items,
     int first_item, unsigned int* queue, float* poses, int pose_stride, ChainResult* results) {
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) float smem[];
     float* sw = smem + (size_t)(threadIdx.x >> 5) * L.total;
     run_machine<true, kAD4>(B, M, Tb, P, L, sw, order, n_items, first_item, queue, poses, pose_stride, results,
                             nullptr, 0, 0.f, nullptr, nullptr);
@@ -1019,7 +1029,7 @@ __global__ void __launch_bounds__(128) optimize_kernel(
     const __grid_constant__ Batch B, const __grid_constant__ Maps M, const __grid_constant__ Tables Tb,
     const __grid_constant__ SearchParams P, const __grid_constant__ Layout L, const int* pose_lig,
     float* poses, int pose_stride, int n_poses, int max_steps, float v, float* e_out, int* evals_out) {
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) float smem[];
     float* sw = smem + (size_t)(threadIdx.x >> 5) * L.total;
     run_machine<false, kAD4>(B, M, Tb, P, L, sw, nullptr, n_poses, 0, nullptr, poses, pose_stride, nullptr,
                              pose_lig, max_steps, v, e_out, evals_out);
@@ -1031,7 +1041,7 @@ __global__ void __launch_bounds__(128) score_kernel(
     const __grid_constant__ Batch B, const __grid_constant__ Maps M, const __grid_constant__ Tables Tb,
     const __grid_constant__ Layout L, const int* pose_lig, const float* poses, int pose_stride, int n_poses,
     float v_intra, float v_inter, float* e_out, float* g_out, int g_stride, float* score_out) {
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5;
     const int pose = blockIdx.x * (blockDim.x >> 5) + warp;
     if (pose >= n_poses) return;
@@ -1074,8 +1084,9 @@ struct TermData {
 // Trilinear interpolation of one map at p, clamped to the box like grid_eval
 // (grid.cpp:40-129) but without curl or out-of-box penalty; `cell` and `frac`
 // cache the corner index and fractions for further maps of the same point.
-__device__ __forceinline__ void grid_cell(const Maps& M, const float* p, int& cell, float* frac) {
+__device__ __forceinline__ void grid_cell(const Maps& M, const float4 pos, int& cell, float* frac) {
     const int dims[3] = {M.nx, M.ny, M.nz};
+    const float p[3] = {pos.x, pos.y, pos.z};
     int a[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
@@ -1123,7 +1134,7 @@ __global__ void __launch_bounds__(128) adjoint_kernel(
     const __grid_constant__ Layout L, const __grid_constant__ TermData TD, int n_ligands, const int* pose_lig,
     const float* poses, int pose_stride, int n_poses, float v_intra, float v_inter, int exact, float* e_out,
     float* g_out, int g_stride, float* dw_out, int dw_stride) {
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5;
     const int pose = blockIdx.x * (blockDim.x >> 5) + warp;
     if (pose >= n_poses) return;
@@ -1160,14 +1171,14 @@ __global__ void __launch_bounds__(128) adjoint_kernel(
         float acc[kMaxTerms];
 #pragma unroll
         for (int t = 0; t < kMaxTerms; ++t) acc[t] = 0;
-        const float* xyz = sw + L.coords;  // conformer of the evaluation above
+        const float4* xyz = reinterpret_cast<const float4*>(sw + L.coords);  // conformer of the evaluation above
         const size_t plane = (size_t)M.nx * M.ny * M.nz;
         for (int k = c.lane; k < c.n_grid; k += 32) {
             const uint32_t ga = __ldg(c.grid + k);
             const int a = ga & 0xFF, slot = ga >> 8;
             int cell;
             float frac[3];
-            grid_cell(M, xyz + 3 * a, cell, frac);
+            grid_cell(M, xyz[a], cell, frac);
             const float w = curl_slope(trilinear(M, M.data + slot * plane, cell, frac), v_inter);
 #pragma unroll
             for (int t = 0; t < kMaxTerms; ++t)
@@ -1189,8 +1200,8 @@ __global__ void __launch_bounds__(128) adjoint_kernel(
             const uint32_t pr = __ldg(c.pairs + k);
             if (pr == kPairPad) continue;
             const int a = pr & 0xFF, b = (pr >> 8) & 0xFF, tp = pr >> 16;
-            const float rx = xyz[3 * b] - xyz[3 * a], ry = xyz[3 * b + 1] - xyz[3 * a + 1],
-                        rz = xyz[3 * b + 2] - xyz[3 * a + 2];
+            const float4 pa = xyz[a], pb = xyz[b];
+            const float rx = pb.x - pa.x, ry = pb.y - pa.y, rz = pb.z - pa.z;
             const float r2 = rx * rx + ry * ry + rz * rz;
             if (!(r2 < Tb.cutoff2)) continue;
             const float rf = Tb.factor * r2;

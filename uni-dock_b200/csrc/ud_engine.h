@@ -59,6 +59,13 @@ struct NodeRec {            // 40 bytes
 // Pair records are a | b << 8 | type_pair << 16; this value pads a 32-pair
 // group of the conflict-free pair order and is skipped.
 constexpr uint32_t kPairPad = 0xFFFF0000u;
+// A 32-slot pair group is kPairPasses lane ranges of 32 / kPairPasses slots,
+// each a matching (no atom twice), whose forces are added one range at a time.
+#ifndef UD_PAIR_PASSES
+#define UD_PAIR_PASSES 4
+#endif
+constexpr int kPairPasses = UD_PAIR_PASSES;
+constexpr int kPairPassWidth = 32 / kPairPasses;
 
 // Atom record: local xyz and packed fields (node | (map slot + 1) << 8 |
 // heavy << 16 | (xs + 1) << 24).
