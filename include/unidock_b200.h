@@ -100,6 +100,12 @@ int ud_maps_destroy(ud_maps maps);
  * (unidock/src/lib/parse_pdbqt.cpp:1089-1122) + model::initialize
  * (unidock/src/lib/model.cpp:613-619). */
 int ud_ligand_parse(const char* pdbqt, size_t len, ud_ligand* out);
+/* Parse n ligands on `threads` host threads (0 = all): out[i] is the handle
+ * or NULL, status[i] its error code (may be NULL: then any failure makes the
+ * call return UD_ERR_PARSE, the successful handles still set).  The batch form
+ * of the OpenMP-parallel parse of the reference CLI (main.cpp:975-983). */
+int ud_ligand_parse_many(const char* const* texts, const size_t* lens, int n, int threads, ud_ligand* out,
+                         int* status);
 /* counts[0] atoms, [1] heavy atoms, [2] torsions, [3] rigid nodes,
  * [4] intramolecular pairs, [5] TORSDOF, [6] glue pairs, [7] BFGS steps. */
 int ud_ligand_counts(ud_ligand lig, int counts[8]);
@@ -244,6 +250,10 @@ int ud_search(ud_batch batch, const ud_search_params* params, void* stream);
  * `stream`, inputs already resident) and the host part (device-to-host copy,
  * clustering, rescoring).  ud_search == ud_search_launch + ud_search_collect. */
 int ud_search_launch(ud_batch batch, const ud_search_params* params, void* stream);
+/* The set-up of ud_search_launch without the launch: result buffers (device
+ * and page-locked host), the ligand order and, with use_graph, the captured
+ * graph.  A following ud_search_launch with the same params only launches. */
+int ud_search_prepare(ud_batch batch, const ud_search_params* params, void* stream);
 int ud_search_collect(ud_batch batch, void* stream);
 /* Raw per-chain results of the last search: best pose (pose_stride floats
  * per chain, chain-major per ligand), best energy and evaluations spent. */

@@ -97,3 +97,18 @@ def test_autotune_picks_valid_configuration(small):
     B.search(exhaustiveness=16, max_step=6, seed=1, form=1, chains_per_block=0, bfgs_cap=-1)
     _, e, ev = B.chains()
     assert np.all(np.isfinite(e)) and np.all(ev > 0)
+
+
+def test_prepare_then_launch_equals_search(small):
+    M, ligs = small
+    B = engine.Batch(M, ligs)
+    B.search_prepare(exhaustiveness=8, max_step=6, seed=21, form=1, use_graph=1)
+    B.search_launch(exhaustiveness=8, max_step=6, seed=21, form=1, use_graph=1)
+    B.search_collect()
+    _, e1, ev1 = B.chains()
+    B2 = engine.Batch(M, ligs)
+    B2.search(exhaustiveness=8, max_step=6, seed=21, form=1, use_graph=0)
+    _, e2, ev2 = B2.chains()
+    np.testing.assert_array_equal(e1, e2)
+    np.testing.assert_array_equal(ev1, ev2)
+    assert [m[1][0] for m in B.modes(0)] == [m[1][0] for m in B2.modes(0)]

@@ -704,6 +704,38 @@ extern "C" int ud_ligand_parse(const char* pdbqt, size_t len, ud_ligand* out) {
     });
 }
 
+extern "C" int ud_ligand_parse_many(const char* const* texts, const size_t* lens, int n, int threads,
+                                    ud_ligand* out, int* status) {
+    return guarded([&] {
+        if (n < 0 || (n > 0 && (!texts || !lens || !out))) throw Error(UD_ERR_ARG, "invalid arguments");
+        for (int i = 0; i < n; ++i) out[i] = nullptr;
+        std::atomic<int> next{0}, failed{0};
+        const int nt = std::max(1, std::min(threads > 0 ? threads : (int)std::thread::hardware_concurrency(), n));
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nt; ++t)
+            pool.emplace_back([&] {
+                for (int i; (i = next.fetch_add(1)) < n;) {
+                    int code = UD_OK;
+                    try {
+                        if (!texts[i]) throw Error(UD_ERR_ARG, "null text");
+                        auto h = std::make_unique<ud_ligand_s>();
+                        h->lig = parse_ligand_pdbqt(std::string(texts[i], lens[i]));
+                        out[i] = h.release();
+                    } catch (const Error& e) {
+                        code = e.code;
+                    } catch (const std::exception&) {
+                        code = UD_ERR_PARSE;
+                    }
+                    if (status) status[i] = code;
+                    if (code != UD_OK) failed.fetch_add(1);
+                }
+            });
+        for (auto& th : pool) th.join();
+        if (failed.load() > 0 && !status)
+            throw Error(UD_ERR_PARSE, std::to_string(failed.load()) + " of " + std::to_string(n) + " ligands failed to parse");
+    });
+}
+
 extern "C" int ud_ligand_counts(ud_ligand lig, int counts[8]) {
     return guarded([&] {
         if (!lig || !counts) throw Error(UD_ERR_ARG, "null argument");
@@ -1341,6 +1373,8 @@ static void post_process(ud_batch b, cudaStream_t s) {
             const float* p = &b->h_poses[(size_t)slot * b->pose_stride];
             r.pose.assign(p, p + 7 + L.n_torsions());
             r.e = b->h_results[slot].e;
+            r.inter = b->h_results[slot].e_grid;   // rescoring values computed with the chain
+            r.intra = b->h_results[slot].e_intra;
             ligand_coords(L, r.pose.data(), xyz.data());
             r.heavy_xyz = heavy_coords(L, xyz);
             add_to_container(out, r, P.min_rmsd, (size_t)std::max(1, P.num_modes));
@@ -1349,34 +1383,17 @@ static void post_process(ud_batch b, cudaStream_t s) {
         for (auto& r : out) add_to_container(red, r, P.min_rmsd, out.size());
         cont[l] = std::move(red);
     });
-    // rescoring: grid + intramolecular (fast table) energies at the authentic cap, one launch
-    const int stride = 7 + b->max_tors;
-    std::vector<int> lig;
-    std::vector<float> poses;
-    std::vector<int> first(n_lig + 1, 0);
-    for (int l = 0; l < n_lig; ++l) {
-        first[l] = (int)lig.size();
-        for (auto& r : cont[l]) {
-            lig.push_back(l);
-            size_t off = poses.size();
-            poses.resize(off + stride, 0.0f);
-            std::copy(r.pose.begin(), r.pose.end(), poses.begin() + off);
-        }
-    }
-    first[n_lig] = (int)lig.size();
-    std::vector<float> sc;
-    score_poses_device(b, lig, poses, stride, 1000.0f, sc, s);
     const Scoring& sf = b->maps->sf;
     parallel_for(n_lig, [&](int l) {
         auto& v = cont[l];
         if (v.empty()) return;
         const Ligand& L = *b->ligs[l];
         auto ci = L.conf_indep_inputs();
-        const int f = first[l];
-        const float intramolecular = sc[2 * f + 1];  // best pose by search energy
+        // final scores (vina.h:241-300): grid + intramolecular energies at the
+        // authentic cap; the unbound energy is that of the best pose by search energy
+        const float intramolecular = v[0].intra;
         for (size_t i = 0; i < v.size(); ++i) {
-            float grid = sc[2 * (f + i)], intra = sc[2 * (f + i) + 1];
-            float inter = grid;
+            const float inter = v[i].inter, intra = v[i].intra;
             float total = sf.conf_independent(inter + intra - intramolecular, ci[0], (float)L.torsdof);
             v[i].e = total;
             v[i].inter = inter;
@@ -1439,7 +1456,8 @@ static void search_graph(ud_batch b, const SearchParams& sp, int n_chain, int bl
 }
 
 // Launch the search kernels of the batch asynchronously on `s`.
-static void search_launch(ud_batch b, const ud_search_params* params, cudaStream_t s) {
+// `launch` false: only the set-up (buffers, ligand order, graph capture).
+static void search_launch(ud_batch b, const ud_search_params* params, cudaStream_t s, bool launch = true) {
         if (!b || !params) throw Error(UD_ERR_ARG, "null argument");
         const ud_search_params& P = *params;
         if (P.exhaustiveness < 1) throw Error(UD_ERR_ARG, "exhaustiveness must be >= 1");
@@ -1489,6 +1507,7 @@ static void search_launch(ud_batch b, const ud_search_params* params, cudaStream
             int blocks = std::max(1, std::min(per_sm * n_sm, (int)((n_chain + sp.chains_per_block - 1) /
                                                                     sp.chains_per_block)));
             search_graph(b, sp, (int)n_chain, blocks);
+            if (!launch) return;
             cudaEventRecord(b->ev0, s);
             cuda_check(cudaGraphLaunch(b->graph_exec, s), "graph launch");
             cudaEventRecord(b->ev1, s);
@@ -1496,6 +1515,7 @@ static void search_launch(ud_batch b, const ud_search_params* params, cudaStream
             b->launched = true;
             return;
         }
+        if (!launch) return;
         cudaEventRecord(b->ev0, s);
         if (sp.persistent) {
             cuda_check(cudaMemsetAsync(b->d_queue.p, 0, sizeof(unsigned int), s), "queue reset");
@@ -1638,6 +1658,13 @@ extern "C" int ud_search(ud_batch b, const ud_search_params* params, void* strea
     return guarded([&] {
         search_launch(b, params, (cudaStream_t)stream);
         search_collect(b, (cudaStream_t)stream);
+    });
+}
+
+extern "C" int ud_search_prepare(ud_batch b, const ud_search_params* params, void* stream) {
+    return guarded([&] {
+        search_launch(b, params, (cudaStream_t)stream, false);
+        cuda_check(cudaStreamSynchronize((cudaStream_t)stream), "prepare sync");
     });
 }
 

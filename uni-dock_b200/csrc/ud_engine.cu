@@ -980,11 +980,17 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                     const int slot = m.lig * P.exhaustiveness + m.chain;
                     const float* best = c.s + L.best;
                     for (int i = lane; i < 7 + c.T; i += 32) poses[(size_t)slot * pose_stride + i] = best[i];
+                    // scoring-path energies of the best pose for the final rescoring
+                    // (vina.h:241-300), so that post-processing needs no device work
+                    float eg, ei;
+                    eval_score<kAD4>(c, L, M, Tb, best, P.authentic_v, eg, ei);
                     if (lane == 0) {
                         results[slot].e = m.best_e;
                         results[slot].evals = m.evals;
                         results[slot].ligand = m.lig;
                         results[slot].chain = m.chain;
+                        results[slot].e_grid = eg;
+                        results[slot].e_intra = ei;
                     }
                 } else {
                     const float* x = c.s + L.x;

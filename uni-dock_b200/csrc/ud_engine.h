@@ -111,6 +111,8 @@ struct ChainResult {
     int evals;             // energy+gradient evaluations spent
     int ligand;
     int chain;
+    float e_grid;          // scoring-path energies of the best pose at the authentic cap:
+    float e_intra;         // grid (cache::eval) and intramolecular (nearest-bin table)
 };
 
 // ---------------------------------------------------------------- device views

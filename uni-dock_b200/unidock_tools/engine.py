@@ -89,6 +89,7 @@ def lib():
         "ud_score": ([vp, ip, fp, C.c_int, C.c_int, C.c_float, fp, vp], C.c_int),
         "ud_search": ([vp, C.POINTER(SearchParams), vp], C.c_int),
         "ud_search_launch": ([vp, C.POINTER(SearchParams), vp], C.c_int),
+        "ud_search_prepare": ([vp, C.POINTER(SearchParams), vp], C.c_int),
         "ud_search_collect": ([vp, vp], C.c_int),
         "ud_search_chains": ([vp, fp, C.c_int, fp, ip], C.c_int),
         "ud_search_device_noalloc": ([vp, C.POINTER(SearchParams), vp, C.c_int, vp, vp, vp], C.c_int),
@@ -99,6 +100,8 @@ def lib():
         "ud_optimize": ([vp, ip, fp, C.c_int, C.c_int, C.c_int, C.c_float, fp, ip, vp], C.c_int),
         "ud_device_fp32_peak": ([fp], C.c_int),
         "ud_maps_term_count": ([vp, ip], C.c_int),
+        "ud_ligand_parse_many": ([C.POINTER(C.c_char_p), C.POINTER(C.c_size_t), C.c_int, C.c_int, C.POINTER(vp),
+                                  ip], C.c_int),
         "ud_receptor_parse_ex": ([C.c_char_p, C.c_size_t, fp, ip, ip, fp, C.c_int, ip], C.c_int),
         "ud_maps_create_ad4": ([fp, C.c_int, fp, ip, fp, C.c_int, fp, fp, C.c_float, ip, C.c_int, vp,
                                 C.POINTER(vp)], C.c_int),
@@ -118,6 +121,24 @@ def lib():
         f.restype = res
     _lib = L
     return L
+
+
+def parse_ligands(texts, threads=0):
+    """Ligands parsed on all host threads (ud_ligand_parse_many); raises on any failure."""
+    bs = [t.encode() for t in texts]
+    n = len(bs)
+    arr = (C.c_char_p * n)(*bs)
+    lens = (C.c_size_t * n)(*[len(b) for b in bs])
+    out = (C.c_void_p * n)()
+    status = np.zeros(n, np.int32)
+    _check(lib().ud_ligand_parse_many(arr, lens, n, int(threads), out, _i(status)))
+    bad = np.nonzero(status)[0]
+    if len(bad):
+        for h in out:
+            if h:
+                lib().ud_ligand_destroy(C.c_void_p(h))
+        raise UdError(int(status[bad[0]]), f"{len(bad)} of {n} ligands failed to parse (first: {int(bad[0])})")
+    return [Ligand("", _handle=h) for h in out]
 
 
 def parse_receptor_ex(text: str):
@@ -265,10 +286,13 @@ class Maps:
 class Ligand:
     """Host-side torsion-tree model parsed from PDBQT (ud_ligand_parse)."""
 
-    def __init__(self, pdbqt: str):
-        b = pdbqt.encode()
-        h = C.c_void_p()
-        _check(lib().ud_ligand_parse(b, len(b), C.byref(h)))
+    def __init__(self, pdbqt: str, _handle=None):
+        if _handle is None:
+            b = pdbqt.encode()
+            h = C.c_void_p()
+            _check(lib().ud_ligand_parse(b, len(b), C.byref(h)))
+        else:
+            h = C.c_void_p(_handle)
         self.h = h
         c = np.zeros(8, np.int32)
         _check(lib().ud_ligand_counts(h, _i(c)))
@@ -385,11 +409,12 @@ class Batch:
         self.exhaustiveness = exhaustiveness
 
     def search_launch(self, exhaustiveness=8, max_step=0, num_modes=9, min_rmsd=1.0, energy_range=3.0, seed=0,
-                      form=1, chains_per_block=0, bfgs_cap=0, use_graph=0):
-        """Enqueue the search kernels only (device-resident inputs, asynchronous)."""
+                      form=1, chains_per_block=0, bfgs_cap=0, use_graph=0, stream=None):
+        """Enqueue the search kernels only (device-resident inputs, asynchronous
+        on `stream`, a raw cudaStream_t or None for the default stream)."""
         self._p = SearchParams(exhaustiveness, max_step, num_modes, min_rmsd, energy_range, seed, form,
                                chains_per_block, bfgs_cap, use_graph)
-        _check(lib().ud_search_launch(self.h, C.byref(self._p), None))
+        _check(lib().ud_search_launch(self.h, C.byref(self._p), C.c_void_p(stream) if stream else None))
         self.exhaustiveness = exhaustiveness
 
     def search_device_noalloc(self, d_poses, pose_stride, d_energies, d_evals=None, stream=None, exhaustiveness=8,
@@ -412,8 +437,16 @@ class Batch:
         _check(lib().ud_autotune(self.h, C.byref(p), C.byref(r), None))
         return r.as_dict()
 
-    def search_collect(self):
-        _check(lib().ud_search_collect(self.h, None))
+    def search_prepare(self, exhaustiveness=8, max_step=0, num_modes=9, min_rmsd=1.0, energy_range=3.0, seed=0,
+                       form=1, chains_per_block=0, bfgs_cap=0, use_graph=0, stream=None):
+        """Set up a search (buffers, order, graph) without launching it (ud_search_prepare)."""
+        p = SearchParams(exhaustiveness, max_step, num_modes, min_rmsd, energy_range, seed, form,
+                         chains_per_block, bfgs_cap, use_graph)
+        _check(lib().ud_search_prepare(self.h, C.byref(p), C.c_void_p(stream) if stream else None))
+
+    def search_collect(self, stream=None):
+        """Wait for the launched search, then cluster, rescore and keep the modes."""
+        _check(lib().ud_search_collect(self.h, C.c_void_p(stream) if stream else None))
 
     def optimize(self, pose_ligand, poses, v=1000.0, max_steps=0):
         pose_ligand = np.ascontiguousarray(pose_ligand, np.int32)
