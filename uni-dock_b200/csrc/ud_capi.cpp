@@ -165,6 +165,8 @@ struct ud_batch_s {
     long long evals = 0;
     float kernel_ms = 0;
     std::vector<LigandPost> post;
+    std::vector<std::string> text[2];  // rendered output per ligand (PDBQT, SDF), filled on first request
+    bool text_ready[2] = {false, false};
     ud_search_params params{};
     // scoring scratch
     DevBuf<int> d_pose_lig;
@@ -1465,6 +1467,7 @@ static void search_launch(ud_batch b, const ud_search_params* params, cudaStream
             throw Error(UD_ERR_ARG, "chains_per_block must be 0 (default / autotuned) or 1..4");
         b->params = P;
         b->searched = false;
+        b->text_ready[0] = b->text_ready[1] = false;
         const int n_lig = (int)b->ligs.size();
         const int E = P.exhaustiveness;
         b->exhaustiveness = E;
@@ -1720,22 +1723,36 @@ extern "C" int ud_result_mode(ud_batch b, int lig, int k, float* pose, float ene
     });
 }
 
+// Output text of one ligand: the kept modes within num_modes and energy_range
+// of the best (Vina::get_poses_gpu, vina.cpp:872-923).
+static std::string render_result(const ud_batch_s* b, int lig, int format) {
+    const Ligand& L = *b->ligs[lig];
+    const auto& modes = b->post[lig].modes;
+    std::vector<PoseResult> sel;
+    if (!modes.empty()) {
+        const float best = modes[0].e;
+        for (auto& m : modes) {
+            if ((int)sel.size() >= b->params.num_modes) break;
+            if (!(m.e < 0.1f * std::numeric_limits<float>::max()) || m.e > best + b->params.energy_range) break;
+            sel.push_back(m);
+        }
+    }
+    const bool ad4 = b->maps->desc.ad4 != 0;
+    return format == 1 ? write_sdf_models(L, sel, ad4) : write_pdbqt_models(L, sel, ad4);
+}
+
 extern "C" int ud_result_write(ud_batch b, int lig, int format, char* buf, size_t cap, size_t* len) {
     return guarded([&] {
         if (!b || !b->searched) throw Error(UD_ERR_STATE, "no search results");
         if (lig < 0 || lig >= (int)b->post.size()) throw Error(UD_ERR_ARG, "ligand out of range");
-        const Ligand& L = *b->ligs[lig];
-        const auto& modes = b->post[lig].modes;
-        std::vector<PoseResult> sel;
-        if (!modes.empty()) {
-            const float best = modes[0].e;
-            for (auto& m : modes) {
-                if ((int)sel.size() >= b->params.num_modes) break;
-                if (!(m.e < 0.1f * std::numeric_limits<float>::max()) || m.e > best + b->params.energy_range) break;
-                sel.push_back(m);
-            }
+        if (format != 0 && format != 1) throw Error(UD_ERR_ARG, "format must be 0 (PDBQT) or 1 (SDF)");
+        if (!b->text_ready[format]) {  // every ligand's text at once, on all host threads
+            auto& t = b->text[format];
+            t.assign(b->post.size(), std::string());
+            parallel_for((int)t.size(), [&](int i) { t[i] = render_result(b, i, format); });
+            b->text_ready[format] = true;
         }
-        std::string s = format == 1 ? write_sdf_models(L, sel, false) : write_pdbqt_models(L, sel, false);
+        const std::string& s = b->text[format][lig];
         if (len) *len = s.size();
         if (buf && cap > 0) {
             size_t n = std::min(cap - 1, s.size());

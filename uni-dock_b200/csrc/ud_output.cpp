@@ -10,12 +10,11 @@
 
 namespace ud {
 
+// std::fixed with setw(width) and setprecision(prec), as the reference's streams format
 static std::string fixed(float v, int width, int prec) {
-    std::ostringstream o;
-    o.setf(std::ios::fixed, std::ios::floatfield);
-    o.setf(std::ios::showpoint);
-    o << std::setw(width) << std::setprecision(prec) << v;
-    return o.str();
+    char buf[64];
+    std::snprintf(buf, sizeof buf, "%*.*f", width, prec, (double)v);
+    return buf;
 }
 
 static void put_coord(std::string& line, std::size_t col, float v) {  // 1-based column, 8 wide
