@@ -34,6 +34,10 @@ N_LIGANDS = 4096
 BOX = 22.5
 SPACING = 0.375
 ADJOINT_POSES = 65536
+# DRAM bytes (read + write) of one search launch of this workload at 1024
+# ligands per step, from an ncu capture of dram__bytes_read.sum +
+# dram__bytes_write.sum (profiles/search_kernel_launch_list_bench_fast_1024lig.md)
+SEARCH_LAUNCH_DRAM_BYTES = 14.29e6 + 32.86e6
 
 
 def parse_args():
@@ -306,7 +310,10 @@ def run_ours(args, rank, world):
             "batched_over_plain": None if plain is None else round(value / plain, 2),
             "evals_per_s": round(evals_total / t_total, 1),
             "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 2), "peak": hbm_peak, "unit": "GB/s",
-                         "frac": round(achieved_gbs / hbm_peak, 4), "traffic": None,
+                         "frac": round(achieved_gbs / hbm_peak, 4),
+                         "traffic": SEARCH_LAUNCH_DRAM_BYTES if B == 1024 else None,
+                         "traffic_note": "DRAM bytes per launch from one ncu capture of this workload; the "
+                                         "achieved figure counts algorithmic L2 bytes (maps stay L2-resident)",
                          "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)",
                          "kernel": "ud::dev::search_kernel",
                          "fp32": {"achieved": round(achieved_tf, 3), "peak": round(fp32_peak, 2),
