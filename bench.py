@@ -35,8 +35,8 @@ BOX = 22.5
 SPACING = 0.375
 ADJOINT_POSES = 65536
 # DRAM bytes (read + write) of one search launch of this workload at 1024
-# ligands per step, from an ncu capture of dram__bytes_read.sum +
-# dram__bytes_write.sum (profiles/search_kernel_launch_list_bench_fast_1024lig.md)
+# ligands per step, measured with ncu (dram__bytes_read.sum 14.29 MB +
+# dram__bytes_write.sum 32.86 MB, one-pass capture of a timed launch)
 SEARCH_LAUNCH_DRAM_BYTES = 14.29e6 + 32.86e6
 
 
