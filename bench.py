@@ -150,17 +150,23 @@ def run_ours(args, rank, world):
 
     steps_total = args.warmup + args.steps
     B = args.batch
-    n_batches = max(1, N_LIGANDS // (B * world))
-    # ligand texts of this rank's batches (weak scaling: every rank searches B ligands per step)
+    # ligand texts of this rank's batches (weak scaling: every rank searches B
+    # ligands per step).  A step's global batch of B * world ligands is split
+    # by ligand (unidock_tools.shard, cost-balanced); there is no data-path
+    # collective, only the timing barrier and max.
+    from unidock_tools.shard import shard
     from unidock_tools.synth import ligand_set
-    all_ligs = ligand_set(min(N_LIGANDS, B * world * min(steps_total, n_batches)), seed=20261203,
+    n_global = max(N_LIGANDS, B * world) if world > 1 else N_LIGANDS
+    n_batches = max(1, n_global // (B * world))
+    all_ligs = ligand_set(min(n_global, B * world * min(steps_total, n_batches)), seed=20261203,
                           heavy=(12, 48), torsions=(0, 10))
     texts = [l.to_pdbqt() for l in all_ligs]
 
     def batch_texts(step):
         b = step % n_batches
-        lo = (b * world + rank) * B
-        return texts[lo:lo + B]
+        glob = texts[b * world * B:(b + 1) * world * B]
+        cost = [len(t) for t in glob]  # text length ~ atoms: a cheap cost proxy before parsing
+        return [glob[i] for i in shard(len(glob), rank, world, cost)]
 
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     P = dict(exhaustiveness=EXHAUSTIVENESS, max_step=MAX_STEP, num_modes=9, min_rmsd=1.0, seed=42, form=1,
