@@ -53,6 +53,11 @@ def parse_args():
     ap.add_argument("--chains-per-block", type=int, default=0)
     ap.add_argument("--adjoint-poses", type=int, default=ADJOINT_POSES,
                     help="fixed poses of the adjoint leg (0 = skip)")
+    ap.add_argument("--workload", default="screen-fast",
+                    choices=["screen-fast", "uneven-vinardo", "uneven-ad4", "stream"],
+                    help="screen-fast: the headline batched screen; the others are the uneven-size detail-mode "
+                         "screens (Vinardo, AD4, autotuned) and the three-receptor streaming screen, each on a "
+                         "sample, printed as their own JSON line")
     ap.add_argument("--profile-case", type=int, default=0,
                     help="profiling aid: search N ligands of the workload twice and exit (no JSON)")
     return ap.parse_args()
@@ -385,6 +390,106 @@ def adjoint_leg(maps, n_ligands=256, reps=5):
             "ms_per_launch": round(ms, 3)}
 
 
+# ------------------------------------------------------------------ other workloads
+def run_uneven(args, sf_name):
+    """Uneven-size screen: lognormal heavy-atom counts (median 28, 8..80), torsions
+    min(n/4, Poisson(6)) <= 20, search_mode detail (exhaustiveness 512, max_step 40),
+    Vinardo or AD4 (receptor and ligand charges N(0, 0.25 e), integer net charge),
+    chains-per-CTA and BFGS cap picked by the autotuner on each batch."""
+    import torch
+    from unidock_tools import engine, synth
+    per_step = args.batch if args.batch != 1024 else 512
+    rec = synth.make_receptor(3000, seed=1, with_charges=(sf_name == "ad4"))
+    center, size = np.zeros(3, np.float32), np.full(3, BOX, np.float32)
+    if sf_name == "ad4":
+        xyz, xs, ad, q = engine.parse_receptor_ex(rec.to_pdbqt())
+        maps = engine.Maps(xyz, ad, center, size, SPACING, sf=engine.SF_AD4, charges=q)
+    else:
+        maps = engine.Maps(rec.xyz, rec.xs, center, size, SPACING, sf=engine.SF_VINARDO)
+    steps_total = args.warmup + args.steps
+    texts = [l.to_pdbqt() for l in synth.ligand_set(per_step * steps_total, seed=8192, dist="lognormal",
+                                                      with_charges=(sf_name == "ad4"))]
+    P = dict(exhaustiveness=512, max_step=40, seed=42, form=1, use_graph=1, chains_per_block=0, bfgs_cap=-1)
+    batches, tunes = [], []
+    for s in range(steps_total):
+        ligs = engine.parse_ligands(texts[s * per_step:(s + 1) * per_step])
+        bt = engine.Batch(maps, ligs)
+        tunes.append(bt.autotune(exhaustiveness=512, max_step=40, seed=42))
+        bt.search_prepare(**P)
+        batches.append(bt)
+    for s in range(args.warmup):
+        batches[s].search_launch(**P)
+        torch.cuda.synchronize()
+    times, evals = [], 0
+    for s in range(args.warmup, steps_total):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        batches[s].search_launch(**P)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+        batches[s].search_collect()
+        evals += batches[s].stats()[0]
+    t = sum(times)
+    tune = tunes[args.warmup]
+    return {"metric": "ligands/s on 1 B200 (uneven-size screen)", "value": round(per_step * args.steps / t, 3),
+            "unit": "ligands/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * t / args.steps, 1), "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic", "evals_per_s": round(evals / t, 1),
+            "config": {"workload": f"uneven-size screen, {sf_name}, search_mode detail (exhaustiveness 512, "
+                                   "max_step 40), lognormal sizes (median 28 heavy, 8..80), 3000-atom receptor, "
+                                   "22.5 A box", "ligands_per_step": per_step,
+                       "autotuned": {k: tune[k] for k in ("chains_per_block", "bfgs_cap", "energy_shift",
+                                                          "ligands_per_s", "base_ligands_per_s")}}}
+
+
+def run_stream(args):
+    """Streaming screen: search_mode balance (exhaustiveness 384, max_step 40),
+    ligands with U{10..100} heavy atoms and U{0..30} torsions, through the
+    public API with batches pipelined on two streams (parse / post-process of
+    one batch overlapping the search of the next), against three receptors:
+    3000 atoms with a 22.5 A box, 6000 with 30 A, 12000 with 36 A (0.375 A)."""
+    import torch
+    from unidock_tools import engine, synth
+    per_batch = args.batch if args.batch != 1024 else 512
+    n_batches = max(2, args.steps)
+    out = []
+    for n_rec, box in ((3000, 22.5), (6000, 30.0), (12000, 36.0)):
+        rec = synth.make_receptor(n_rec, seed=1)
+        maps = engine.Maps(rec.xyz, rec.xs, np.zeros(3, np.float32), np.full(3, box, np.float32), SPACING)
+        dims, _, _, n_maps = maps.info()
+        texts = [l.to_pdbqt() for l in synth.ligand_set(per_batch * n_batches, seed=100000 + n_rec,
+                                                          heavy=(10, 100), torsions=(0, 30))]
+        P = dict(exhaustiveness=384, max_step=40, seed=42, form=1, use_graph=1)
+        streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pending = None
+        for k in range(n_batches):
+            st = streams[k % 2].cuda_stream
+            ligs = engine.parse_ligands(texts[k * per_batch:(k + 1) * per_batch])
+            bt = engine.Batch(maps, ligs)
+            bt.search_launch(**P, stream=st)
+            if pending is not None:
+                pending[0].search_collect(stream=pending[1])
+                [pending[0].write(i) for i in range(per_batch)]
+            pending = (bt, st)
+        pending[0].search_collect(stream=pending[1])
+        [pending[0].write(i) for i in range(per_batch)]
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+        map_bytes = int(dims.prod()) * n_maps * 4
+        out.append({"receptor_atoms": n_rec, "box": box, "grid": [int(d) for d in dims],
+                    "ligands": per_batch * n_batches, "ligands_per_s": round(per_batch * n_batches / t, 2),
+                    "map_mbytes": round(map_bytes / 1e6, 1), "maps_fit_l2_126mb": map_bytes < 126e6})
+    return {"metric": "sustained ligands/s on 1 B200 (streaming screen)", "unit": "ligands/s", "n_gpus": 1,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "value": round(min(r["ligands_per_s"] for r in out), 3),
+            "config": {"workload": "streaming screen, Vina, search_mode balance (exhaustiveness 384, max_step 40), "
+                                   "ligands U{10..100} heavy / U{0..30} torsions, batches pipelined on two streams, "
+                                   "wall clock", "ligands_per_batch": per_batch, "receptors": out}}
+
+
 # ------------------------------------------------------------------ reference CPU path
 def reference_cpu(sample, step_index, threads=None, seed=7):
     """Reference CPU Vina search (oracle/_ref, the reference's own sources) on
@@ -445,6 +550,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus == 1 else 1)))
     if args.profile_case > 0:
         profile_case(args)
+        return
+    if args.workload != "screen-fast" and args.impl != "reference":
+        res = run_stream(args) if args.workload == "stream" else run_uneven(args, args.workload.split("-")[1])
+        print(json.dumps(res), flush=True)
         return
     if args.impl == "reference":
         res = run_reference(args, rank, world)

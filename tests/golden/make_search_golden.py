@@ -1,10 +1,10 @@
-"""Generate tests/golden/ref_search_vina.npz: the reference's own CPU Monte-Carlo
+"""Generate tests/golden/ref_search_<sf>.npz: the reference's own CPU Monte-Carlo
 search (oracle/_ref/libudref.so, the reference's mutate_conf / quasi_newton /
 output container under the chain loop of monte_carlo.cu:2319-2356) run with
 32 seeds on seeded synthetic ligands, as the distribution the GPU search is
 compared against.
 
-Settings follow the plain single-docking case: Vina, exhaustiveness 8, the
+Settings follow the plain single-docking case: Vina (or Vinardo), exhaustiveness 8, the
 heuristic global step count min(70*3*(50 + N + 10*(6 + T))/2, max_step) with no
 max_step cap (unidock/src/lib/vina.h:191-204), per-ligand BFGS steps
 (25 + N)/3, curl cap 10 during the search and 1000 for the refinement of
@@ -13,7 +13,7 @@ improved poses.  Receptor: 3000 synthetic atoms, 22.5 A box at 0.375 A.
 Stored per ligand and seed: every chain's best energy (inter + intra at curl
 cap 1000, the quantity the search minimises) and best pose.
 
-Run:  python tests/golden/make_search_golden.py      (about 10 minutes on 8 threads)
+Run:  python tests/golden/make_search_golden.py [vina|vinardo]   (about 10 minutes on 8 threads)
 """
 import os
 import sys
@@ -43,12 +43,13 @@ def global_steps(n_atoms, n_torsions):
     return 70 * 3 * (50 + n_atoms + 10 * (6 + n_torsions)) // 2
 
 
-def main():
+def main(name="vina"):
+    sf = {"vina": 0, "vinardo": 2}[name]
     threads = os.cpu_count()
     rec = synth.make_receptor(3000, seed=1)
     center = np.zeros(3, np.float32)
     size = np.full(3, BOX, np.float32)
-    R = ref.RefMaps(rec.xyz, rec.xs, center, size, SPACING)
+    R = ref.RefMaps(rec.xyz, rec.xs, center, size, SPACING, sf=sf)
     texts, energies, poses, gsteps, n_tors = [], [], [], [], []
     max_t = max(t for _, t, _ in LIGANDS)
     with tempfile.TemporaryDirectory() as d:
@@ -56,7 +57,7 @@ def main():
             txt = synth.make_ligand(nh, nt, seed=s).to_pdbqt()
             p = Path(d) / f"l{k}.pdbqt"
             p.write_text(txt)
-            RL = ref.RefLigand(p)
+            RL = ref.RefLigand(p, sf=sf)
             gs = global_steps(RL.n_atoms, RL.n_torsions)
             t0 = time.perf_counter()
             e_l, p_l = [], []
@@ -71,8 +72,8 @@ def main():
             poses.append(p_l)
             gsteps.append(gs)
             n_tors.append(RL.n_torsions)
-    out = ROOT / "tests" / "golden" / "ref_search_vina.npz"
-    np.savez_compressed(out, rec_xyz=rec.xyz, rec_xs=rec.xs, center=center, size=size, spacing=np.float32(SPACING),
+    out = ROOT / "tests" / "golden" / f"ref_search_{name}.npz"
+    np.savez_compressed(out, sf=np.int32(sf), rec_xyz=rec.xyz, rec_xs=rec.xs, center=center, size=size, spacing=np.float32(SPACING),
                         ligand_pdbqt=np.array(texts), n_torsions=np.array(n_tors, np.int32),
                         global_steps=np.array(gsteps, np.int32), exhaustiveness=np.int32(EXHAUSTIVENESS),
                         chain_e=np.array(energies, np.float32), chain_pose=np.array(poses, np.float32),
@@ -81,4 +82,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1] if len(sys.argv) > 1 else "vina")

@@ -1,6 +1,6 @@
 """Distributional parity of the GPU Monte-Carlo search with the reference's CPU
-search (tests/golden/ref_search_vina.npz, made by make_search_golden.py from
-the reference's own mutate_conf / quasi_newton code).
+search (tests/golden/ref_search_{vina,vinardo}.npz, made by make_search_golden.py
+from the reference's own mutate_conf / quasi_newton code).
 
 The random streams cannot match (Philox on the device against the reference's
 host generator), so the comparison is over 32 independent runs per ligand:
@@ -19,7 +19,8 @@ import pytest
 from unidock_tools import engine
 
 pytestmark = pytest.mark.gpu
-GOLD = Path(__file__).resolve().parent / "golden" / "ref_search_vina.npz"
+GOLDEN = Path(__file__).resolve().parent / "golden"
+CASES = [sf for sf in ("vina", "vinardo") if (GOLDEN / f"ref_search_{sf}.npz").exists()]
 TOL = 0.1
 
 
@@ -28,10 +29,11 @@ def heavy_rmsd(L, heavy, pa, pb):
     return float(np.sqrt(np.mean(np.sum((a - b) ** 2, axis=1))))
 
 
-@pytest.fixture(scope="module")
-def gold():
-    g = dict(np.load(GOLD))
-    maps = engine.Maps(g["rec_xyz"], g["rec_xs"], g["center"], g["size"], float(g["spacing"]))
+@pytest.fixture(scope="module", params=CASES)
+def gold(request):
+    g = dict(np.load(GOLDEN / f"ref_search_{request.param}.npz"))
+    sf = int(g.get("sf", 0))
+    maps = engine.Maps(g["rec_xyz"], g["rec_xs"], g["center"], g["size"], float(g["spacing"]), sf=sf)
     return g, maps
 
 
