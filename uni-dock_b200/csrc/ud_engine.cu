@@ -619,7 +619,9 @@ __device__ __forceinline__ void conf_increment(const Ctx& c, const float* x, con
 
 // The inverse Hessian is kept as a full symmetric n x n matrix (the reference
 // stores the upper triangle, bfgs.h:27-58): lane i owns row/column i, so both
-// products and the update are one contiguous loop per lane.
+// products and the update are one contiguous loop per lane.  (Two lanes per
+// row for n <= 16 measured no faster: the combining shuffle costs what the
+// shorter loops save.)
 // out = -H v
 __device__ __forceinline__ void minus_hv(const Ctx& c, const float* H, const float* v, float* out, int n) {
     for (int i = c.lane; i < n; i += 32) {
@@ -1014,8 +1016,10 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
 }
 
 // ---------------------------------------------------------------- kernels
+// CTAs per SM the register budget is sized for: 7 x 128 threads leaves 72
+// registers a thread (measured faster than 8 CTAs at 64 registers, which spill)
 #ifndef UD_SEARCH_MIN_BLOCKS
-#define UD_SEARCH_MIN_BLOCKS 8
+#define UD_SEARCH_MIN_BLOCKS 7
 #endif
 template <bool kAD4>
 __global__ void __launch_bounds__(128, UD_SEARCH_MIN_BLOCKS) search_kernel(
