@@ -1021,8 +1021,13 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
 #ifndef UD_SEARCH_MIN_BLOCKS
 #define UD_SEARCH_MIN_BLOCKS 7
 #endif
+// the AD4 instantiation (three maps per atom, three pair-table rows) keeps more
+// values live: 6 CTAs, 80 registers a thread
+#ifndef UD_SEARCH_MIN_BLOCKS_AD4
+#define UD_SEARCH_MIN_BLOCKS_AD4 6
+#endif
 template <bool kAD4>
-__global__ void __launch_bounds__(128, UD_SEARCH_MIN_BLOCKS) search_kernel(
+__global__ void __launch_bounds__(128, kAD4 ? UD_SEARCH_MIN_BLOCKS_AD4 : UD_SEARCH_MIN_BLOCKS) search_kernel(
     const __grid_constant__ Batch B, const __grid_constant__ Maps M, const __grid_constant__ Tables Tb,
     const __grid_constant__ SearchParams P, const __grid_constant__ Layout L, const int* order, int n_items,
     int first_item, unsigned int* queue, float* poses, int pose_stride, ChainResult* results) {
