@@ -95,11 +95,24 @@ int ud_maps_read(ud_maps maps, int xs, float* out, size_t n);
 int ud_maps_destroy(ud_maps maps);
 
 /* ---------------------------------------------------------------- ligands
- * Parse a Vina PDBQT ligand into a torsion-tree model (host memory).
- * Replaces parse_ligand_pdbqt_from_file_no_failure
- * (unidock/src/lib/parse_pdbqt.cpp:1089-1122) + model::initialize
+ * Parse a ligand into a torsion-tree model (host memory): a V2000 SDF
+ * record (4th line ends in V2000) or else a Vina PDBQT.
+ * Replaces parse_ligand_from_file_no_failure with hydrogens kept, as the
+ * reference CLI calls it (unidock/src/lib/parse_pdbqt.cpp:1076-1140,
+ * unidock/src/main/main.cpp:858-863) + model::initialize
  * (unidock/src/lib/model.cpp:613-619). */
-int ud_ligand_parse(const char* pdbqt, size_t len, ud_ligand* out);
+int ud_ligand_parse(const char* text, size_t len, ud_ligand* out);
+/* SDF record with the fragInfo / torsionInfo / atomInfo properties of the
+ * reference's ligand preparation.  keep_h = 0 leaves atoms of AutoDock type H
+ * out of the model (parse_sdf_ligand's keep_H, parse_pdbqt.cpp:612-873).
+ * Results of such a ligand are written back as its own SDF record. */
+int ud_ligand_parse_sdf(const char* sdf, size_t len, int keep_h, ud_ligand* out);
+/* The ligand's own input record (SDF or PDBQT, as parsed) with the atom
+ * coordinates of `pose` ([x y z qw qx qy qz torsions...]) and no result block,
+ * into buf (cap bytes, NUL-terminated); *len = full length.  Replaces
+ * model::write_structure / write_sdf_structure (unidock/src/lib/model.h:125-144)
+ * as Vina::write_pose uses them for --local_only (vina.cpp:1018-1030). */
+int ud_ligand_write(ud_ligand lig, const float* pose, char* buf, size_t cap, size_t* len);
 /* Parse n ligands on `threads` host threads (0 = all): out[i] is the handle
  * or NULL, status[i] its error code (may be NULL: then any failure makes the
  * call return UD_ERR_PARSE, the successful handles still set).  The batch form

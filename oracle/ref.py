@@ -4,12 +4,24 @@ baseline leg and the smoke check call it."""
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
 
 LIB = Path(__file__).resolve().parent / "_ref" / "libudref.so"
+# the reference's source tree (oracle/Makefile's REF points into it); only the
+# checkers read its own test inputs, and only when it is present
+REFERENCE_TREE = Path(os.environ.get("UD_REFERENCE_TREE", "/root/reference"))
 _lib = None
+
+
+def reference_inputs(pattern: str) -> list[Path]:
+    """The reference's own test input files matching a glob under its tree
+    (empty when the tree is absent)."""
+    if not REFERENCE_TREE.is_dir():
+        return []
+    return sorted(REFERENCE_TREE.glob(pattern))
 
 
 def available() -> bool:

@@ -147,14 +147,16 @@ float udref_table_fast(void* hh, int t1, int t2, float r2) {
     return h->pre->eval_fast(triangular_matrix_index_permissive(n, t1, t2), r2);
 }
 
-// Ligand parsed by the reference parser (parse_pdbqt.cpp:1089), per-atom-pair tables
+// Ligand parsed by the reference parser (parse_pdbqt.cpp:1076-1140), per-atom-pair tables
 // precalculate_byatom (precalculate.h:206-241).
 void* udref_ligand_new(const char* path, int sf_choice, const float* weights, int n_weights) {
     try {
         auto h = new RefLigand();
         h->sf = std::make_shared<ScoringFunction>((scoring_function_choice)sf_choice,
                                                   to_flv(weights, n_weights));
-        h->m = parse_ligand_pdbqt_from_file_no_failure(path, h->sf->get_atom_typing(), true);
+        // .pdbqt / .sdf dispatch on the file name with hydrogens kept, as the
+        // reference CLI loads ligands (main.cpp:858-863, parse_pdbqt.cpp:1076-1087)
+        h->m = parse_ligand_from_file_no_failure(path, h->sf->get_atom_typing(), true);
         if (h->m.num_ligands() != 1) {
             delete h;
             g_err = "parse failed";

@@ -129,6 +129,40 @@ def test_score_only_and_local_only(inputs):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("scoring", ["vina", "vinardo"])
+def test_sdf_batch_docking(inputs, tmp_path, scoring):
+    """SDF ligands through --gpu_batch (the reference's test_unidock_sdf.py
+    case: --search_mode fast --num_modes 1 --seed 181129): <ligand>_out.sdf
+    holds the input record with new coordinates and the Uni-Dock RESULT block."""
+    d, _ = inputs
+    names = []
+    for k, L in enumerate(synth.ligand_set(3, seed=91, heavy=(20, 30), torsions=(2, 8))):
+        p = tmp_path / f"sdf{k}.sdf"
+        p.write_text(L.to_sdf())
+        names.append(p)
+    out = tmp_path / "out"
+    out.mkdir()
+    r = run("--receptor", d / "rec.pdbqt", "--gpu_batch", *names, "--dir", out, "--scoring", scoring,
+            "--search_mode", "fast", "--num_modes", 1, "--seed", 181129, *box_args())
+    assert r.returncode == 0, r.stderr
+    for p in names:
+        text = (out / (p.stem + "_out.sdf")).read_text()
+        assert text.count("$$$$") == 1 and text.endswith("$$$$\n")
+        lines = text.split("\n")
+        k = lines.index("> <Uni-Dock RESULT> ")
+        score = float(lines[k + 1][len("ENERGY="):].split()[0])
+        assert -20 <= score <= -1
+    # --local_only on an SDF ligand writes an SDF structure (coordinates in SDF columns)
+    lo = tmp_path / "local.sdf"
+    r = run("--receptor", d / "rec.pdbqt", "--ligand", names[0], "--local_only", "--out", lo, *box_args())
+    assert r.returncode == 0, r.stderr
+    src = [l for l in names[0].read_text().splitlines() if "$$$$" not in l]
+    dst = lo.read_text().splitlines()
+    assert len(src) == len(dst) and all(a[30:] == b[30:] for a, b in zip(src, dst))
+    assert sum(a[:30] != b[:30] for a, b in zip(src, dst)) > 0
+
+
+@pytest.mark.gpu
 def test_ad4_maps_written_then_read_back(inputs, tmp_path, receptor):
     """--scoring ad4 builds AutoDock maps from the receptor (charges from its
     PDBQT), --write_maps writes AutoGrid files, and --maps reads them back:

@@ -1,5 +1,7 @@
 """Host parsing/typing/torsion tree against the reference parser
-(unidock/src/lib/parse_pdbqt.cpp + model.cpp:initialize) on seeded ligands."""
+(unidock/src/lib/parse_pdbqt.cpp + model.cpp:initialize) on seeded ligands,
+PDBQT and SDF (fragInfo / torsionInfo / atomInfo), and on the reference's own
+prepared SDF test inputs when its tree is present."""
 import numpy as np
 import pytest
 
@@ -9,16 +11,7 @@ from unidock_tools import engine, synth
 pytestmark = pytest.mark.skipif(not ref.available(), reason="reference build (oracle/_ref) missing")
 
 
-@pytest.mark.parametrize("seed", range(24))
-def test_ligand_model_matches_reference(seed, workdir):
-    nh = 12 + (seed * 7) % 37
-    nt = seed % 11
-    lig = synth.make_ligand(nh, nt, seed=100 + seed)
-    text = lig.to_pdbqt()
-    path = workdir / f"lig{seed}.pdbqt"
-    path.write_text(text)
-    R = ref.RefLigand(path)
-    M = engine.Ligand(text)
+def assert_same_model(R, M):
     ra, ma = R.atoms(), M.export()
     assert (R.n_atoms, R.n_torsions, R.n_pairs) == (M.n_atoms, M.n_torsions, M.n_pairs)
     for k in ("xs", "ad", "el"):
@@ -34,6 +27,87 @@ def test_ligand_model_matches_reference(seed, workdir):
     np.testing.assert_array_equal(end, ma["end"])
     np.testing.assert_array_equal(rel, ma["rel"])
     np.testing.assert_array_equal(R.conf_indep()[:6], M.conf_indep()[:6])
+    np.testing.assert_array_equal(ra["charge"], ma["charge"])
+
+
+@pytest.mark.parametrize("seed", range(24))
+def test_ligand_model_matches_reference(seed, workdir):
+    nh = 12 + (seed * 7) % 37
+    nt = seed % 11
+    lig = synth.make_ligand(nh, nt, seed=100 + seed)
+    text = lig.to_pdbqt()
+    path = workdir / f"lig{seed}.pdbqt"
+    path.write_text(text)
+    assert_same_model(ref.RefLigand(path), engine.Ligand(text))
+
+
+@pytest.mark.parametrize("seed", range(16))
+def test_sdf_ligand_model_matches_reference(seed, workdir):
+    """SDF front end (parse_sdf_aux / parse_sdf_branch): same atoms in the same
+    order, frames, types, charges, tree and pairs as the reference."""
+    lig = synth.make_ligand(12 + (seed * 5) % 41, seed % 12, seed=300 + seed, with_charges=True)
+    text = lig.to_sdf()
+    path = workdir / f"lig{seed}.sdf"
+    path.write_text(text)
+    M = engine.Ligand(text)
+    assert M.torsdof == len(lig.rotatable)
+    assert_same_model(ref.RefLigand(path), M)
+    # explicit SDF entry point, hydrogens kept: the same model
+    assert M.export()["ad"].tolist() == engine.Ligand(text, keep_h=True).export()["ad"].tolist()
+
+
+@pytest.mark.parametrize("path", ref.reference_inputs("**/*.sdf"), ids=lambda p: p.name)
+def test_reference_sdf_inputs_match_reference(path):
+    """The reference's own SDF test inputs: prepared ligands (with fragInfo),
+    ligands without it (one rigid body) and multi-property records."""
+    text = path.read_text()
+    try:
+        R = ref.RefLigand(path)
+    except RuntimeError:
+        with pytest.raises(engine.UdError):
+            engine.Ligand(text, keep_h=True)
+        return
+    assert_same_model(R, engine.Ligand(text, keep_h=True))
+
+
+def test_sdf_without_fragments_is_rigid():
+    lig = synth.make_ligand(14, 3, seed=5, with_charges=True)
+    text = lig.to_sdf()
+    cut = text.index(">  <fragInfo>")
+    rigid = text[:cut] + text[text.index(">  <atomInfo>"):]
+    M = engine.Ligand(rigid)
+    assert (M.n_torsions, M.torsdof) == (0, 0)
+    assert M.n_atoms == int(text.split("\n")[3][:3])
+
+
+def test_sdf_keep_h_false_drops_nonpolar_hydrogens():
+    lig = synth.make_ligand(16, 2, seed=9, with_charges=True)
+    lines = lig.to_sdf().split("\n")
+    # make the last atom a non-polar hydrogen (AutoDock type H) in atomInfo
+    k = max(i for i, l in enumerate(lines) if l.rstrip().endswith("HD"))
+    lines[k] = lines[k].rstrip()[:-2] + "H "
+    text = "\n".join(lines)
+    kept, dropped = engine.Ligand(text, keep_h=True), engine.Ligand(text, keep_h=False)
+    assert dropped.n_atoms == kept.n_atoms - 1
+
+
+def test_ligand_write_reproduces_input_record():
+    """ud_ligand_write at the input pose: the input lines, with coordinates
+    rewritten in their own columns (SDF 1-30, PDBQT 31-54)."""
+    lig = synth.make_ligand(22, 4, seed=13, with_charges=True)
+    for text, cols in ((lig.to_sdf(), (0, 30)), (lig.to_pdbqt(), (30, 54))):
+        M = engine.Ligand(text)
+        out = M.write_structure(M.initial_pose())
+        src = [l for l in text.split("\n") if "$$$$" not in l]
+        dst = out.split("\n")
+        assert len(src) == len(dst)
+        for a, b in zip(src, dst):
+            assert a[:cols[0]] == b[:cols[0]] and a[cols[1]:] == b[cols[1]:]
+            if a[cols[0]:cols[1]] != b[cols[0]:cols[1]]:
+                w = 10 if cols[0] == 0 else 8
+                xa = [float(a[cols[0] + w * k:cols[0] + w * (k + 1)]) for k in range(3)]
+                xb = [float(b[cols[0] + w * k:cols[0] + w * (k + 1)]) for k in range(3)]
+                np.testing.assert_allclose(xa, xb, atol=1.5e-3)
 
 
 def test_initial_pose_reproduces_input_coordinates():

@@ -45,11 +45,11 @@ struct OptSpec {
 const OptSpec kOptions[] = {
     {"receptor", 0, "rigid part of the receptor (PDBQT)", "Input"},
     {"flex", 0, "flexible side chains (not supported by this build)", "Input"},
-    {"ligand", 2, "ligand (PDBQT)", "Input"},
-    {"ligand_index", 0, "file containing paths to ligands (PDBQT)", "Input"},
+    {"ligand", 2, "ligand (PDBQT or SDF)", "Input"},
+    {"ligand_index", 0, "file containing paths to ligands (PDBQT or SDF)", "Input"},
     {"paired_batch_size", 0, "one-ligand-one-protein batching (not supported by this build)", "Input"},
     {"batch", 2, "batch ligand (PDBQT)", "Input"},
-    {"gpu_batch", 2, "gpu batch ligand (PDBQT)", "Input"},
+    {"gpu_batch", 2, "gpu batch ligand (PDBQT or SDF)", "Input"},
     {"scoring", 0, "scoring function (ad4, vina or vinardo)", "Input"},
     {"maps", 0, "affinity maps for the autodock4.2 (ad4) or vina scoring function (AutoGrid .map files "
                 "<prefix>.<type>.map)", "Search space"},
@@ -290,9 +290,12 @@ std::vector<ParsedLigand> parse_ligands(const std::vector<std::string>& paths, i
     parallel_for((int)paths.size(), threads, [&](int i) {
         out[i].path = paths[i];
         try {
-            if (ends_with(paths[i], ".sdf")) throw std::runtime_error("SDF input is not supported by this build");
             std::string t = read_file(paths[i]);
-            if (ud_ligand_parse(t.data(), t.size(), &out[i].h) != UD_OK) {
+            // by file name, as parse_ligand_from_file_no_failure; hydrogens are
+            // always kept (--keep_nonpolar_H is a switch that defaults to on)
+            const int rc = ends_with(paths[i], ".sdf") ? ud_ligand_parse_sdf(t.data(), t.size(), 1, &out[i].h)
+                                                       : ud_ligand_parse(t.data(), t.size(), &out[i].h);
+            if (rc != UD_OK) {
                 out[i].h = nullptr;
                 throw std::runtime_error(ud_last_error());
             }
@@ -440,7 +443,8 @@ void run_batches(const Setup& S, ud_maps maps, const std::vector<std::string>& p
                 std::cerr << "WARNING: Could not find any poses. No poses were written.\n";
                 continue;
             }
-            write_text(default_output(get_filename(sl.ligs[i].path), dir), result_text(sl.b, (int)i, 0));
+            const std::string name = default_output(get_filename(sl.ligs[i].path), dir);
+            write_text(name, result_text(sl.b, (int)i, ends_with(name, ".sdf") ? 1 : 0));
         }
         done += (int)sl.ligs.size();
         if (S.verbosity > 0)
@@ -498,30 +502,19 @@ void run_single(const Setup& S, ud_maps maps, const std::string& path, const std
             write_text(default_score_output(path), f.str());
         } else {
             // Vina::write_pose with no remark: the input structure with the
-            // optimised coordinates (vina.cpp:1018-1030)
-            std::vector<float> xyz(3 * (size_t)counts[0]);
-            check(ud_ligand_coords(h, pose.data(), xyz.data()), "coords");
-            std::ostringstream o;
-            std::string text = read_file(path);
-            std::istringstream in(text);
-            std::string line;
-            int a = 0;
-            while (std::getline(in, line)) {
-                if ((line.rfind("ATOM", 0) == 0 || line.rfind("HETATM", 0) == 0) && line.size() >= 54 &&
-                    a < counts[0]) {
-                    char buf[32];
-                    std::snprintf(buf, sizeof buf, "%8.3f%8.3f%8.3f", xyz[3 * a], xyz[3 * a + 1], xyz[3 * a + 2]);
-                    line.replace(30, 24, buf);
-                    ++a;
-                }
-                o << line << "\n";
-            }
-            write_text(out_name, o.str());
+            // optimised coordinates (vina.cpp:1018-1030); an SDF ligand keeps
+            // SDF coordinate columns
+            size_t len = 0;
+            check(ud_ligand_write(h, pose.data(), nullptr, 0, &len), "write");
+            std::string o(len + 1, '\0');
+            check(ud_ligand_write(h, pose.data(), &o[0], o.size(), &len), "write");
+            o.resize(len);
+            write_text(out_name, o);
         }
     } else {
         check(ud_search(b, &S.params, nullptr), "search");
         if (S.verbosity > 0) print_modes(b, 0, S.params.num_modes, S.params.energy_range);
-        write_text(out_name, result_text(b, 0, 0));
+        write_text(out_name, result_text(b, 0, ends_with(out_name, ".sdf") ? 1 : 0));
     }
     ud_batch_destroy(b);
     ud_ligand_destroy(h);

@@ -697,11 +697,20 @@ extern "C" int ud_maps_destroy(ud_maps maps) {
 
 static int ligand_local_steps(const Ligand& L) { return (25 + (int)L.atoms.size()) / 3; }
 
-extern "C" int ud_ligand_parse(const char* pdbqt, size_t len, ud_ligand* out) {
+extern "C" int ud_ligand_parse(const char* text, size_t len, ud_ligand* out) {
     return guarded([&] {
-        if (!pdbqt || !out) throw Error(UD_ERR_ARG, "null argument");
+        if (!text || !out) throw Error(UD_ERR_ARG, "null argument");
         auto h = std::make_unique<ud_ligand_s>();
-        h->lig = parse_ligand_pdbqt(std::string(pdbqt, len));
+        h->lig = parse_ligand(std::string(text, len));
+        *out = h.release();
+    });
+}
+
+extern "C" int ud_ligand_parse_sdf(const char* sdf, size_t len, int keep_h, ud_ligand* out) {
+    return guarded([&] {
+        if (!sdf || !out) throw Error(UD_ERR_ARG, "null argument");
+        auto h = std::make_unique<ud_ligand_s>();
+        h->lig = parse_ligand_sdf(std::string(sdf, len), keep_h != 0);
         *out = h.release();
     });
 }
@@ -721,7 +730,7 @@ extern "C" int ud_ligand_parse_many(const char* const* texts, const size_t* lens
                     try {
                         if (!texts[i]) throw Error(UD_ERR_ARG, "null text");
                         auto h = std::make_unique<ud_ligand_s>();
-                        h->lig = parse_ligand_pdbqt(std::string(texts[i], lens[i]));
+                        h->lig = parse_ligand(std::string(texts[i], lens[i]));
                         out[i] = h.release();
                     } catch (const Error& e) {
                         code = e.code;
@@ -735,6 +744,19 @@ extern "C" int ud_ligand_parse_many(const char* const* texts, const size_t* lens
         for (auto& th : pool) th.join();
         if (failed.load() > 0 && !status)
             throw Error(UD_ERR_PARSE, std::to_string(failed.load()) + " of " + std::to_string(n) + " ligands failed to parse");
+    });
+}
+
+extern "C" int ud_ligand_write(ud_ligand lig, const float* pose, char* buf, size_t cap, size_t* len) {
+    return guarded([&] {
+        if (!lig || !pose) throw Error(UD_ERR_ARG, "null argument");
+        const std::string s = write_structure(lig->lig, pose);
+        if (len) *len = s.size();
+        if (buf && cap > 0) {
+            size_t n = std::min(cap - 1, s.size());
+            std::memcpy(buf, s.data(), n);
+            buf[n] = 0;
+        }
     });
 }
 

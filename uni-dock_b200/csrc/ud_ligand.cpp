@@ -1,4 +1,4 @@
-// Ligand and receptor input: PDBQT parsing, torsion tree, covalent bonds,
+// Ligand and receptor input: PDBQT and SDF parsing, torsion tree, covalent bonds,
 // X-Score typing and the intramolecular pair list.
 //
 // The result has to be the model the reference builds from the same file,
@@ -10,9 +10,11 @@
 //   bonds:           unidock/src/lib/model.cpp:288-390 (assign_bonds, atom_exists_between)
 //   typing:          unidock/src/lib/model.cpp:408-506 (assign_types)
 //   pairs:           unidock/src/lib/model.cpp:508-611 (bonded_to, initialize_pairs)
+//   SDF input:       unidock/src/lib/parse_pdbqt.cpp:129-144, 400-420, 612-873, 962-1000
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <sstream>
 #include <stdexcept>
@@ -455,6 +457,42 @@ void assign_types(std::vector<Atom>& atoms) {
     }
 }
 
+// Rigid-body frames, bonds, X-Score types and intramolecular pairs from the
+// parsed ROOT block (postprocess_ligand, parse_pdbqt.cpp:525-542, then
+// model.cpp:initialize); shared by the PDBQT and SDF front ends.
+void finish_ligand(Builder& B, Block& root, int atom_typing_xs) {
+    Ligand& lig = B.lig;
+    Node r;
+    for (int k = 0; k < 3; ++k) r.origin0[k] = root.atoms[0].a.xyz[k];
+    lig.nodes.push_back(r);
+    B.postprocess(root, 0);
+    B.grow_mob();
+    for (std::size_t k = 0; k < lig.nodes.size(); ++k)
+        for (int i = lig.nodes[k].begin; i < lig.nodes[k].end; ++i) lig.atoms[i].node = (int)k;
+    B.assign_bonds();
+    assign_types(lig.atoms);
+    // both typings: the pair list of a batch follows its maps' scoring function
+    B.make_pairs(true);
+    B.make_pairs(false);
+    if (!atom_typing_xs) {
+        lig.pairs = lig.pairs_ad;
+        lig.glue_pairs = lig.glue_pairs_ad;
+    }
+}
+
+// Whitespace-separated unsigned integers of an SDF property line.
+std::vector<int> sdf_ints(const std::string& line) {
+    std::vector<int> v;
+    std::istringstream in(line);
+    std::string tok;
+    while (in >> tok) {
+        for (char c : tok)
+            if (!std::isdigit((unsigned char)c)) throw std::runtime_error("Invalid SDF property line: " + line);
+        v.push_back(std::stoi(tok));
+    }
+    return v;
+}
+
 }  // namespace
 
 int Ligand::n_heavy() const {
@@ -561,24 +599,177 @@ Ligand parse_ligand_pdbqt(const std::string& text, int atom_typing_xs) {
     }
     if (root.atoms.empty()) throw std::runtime_error("No atoms in this ligand.");
     if (!have_torsdof) throw std::runtime_error("Missing TORSDOF keyword in this ligand.");
-
-    Node r;
-    for (int k = 0; k < 3; ++k) r.origin0[k] = root.atoms[0].a.xyz[k];
-    lig.nodes.push_back(r);
-    B.postprocess(root, 0);
-    B.grow_mob();
-    for (std::size_t k = 0; k < lig.nodes.size(); ++k)
-        for (int i = lig.nodes[k].begin; i < lig.nodes[k].end; ++i) lig.atoms[i].node = (int)k;
-    B.assign_bonds();
-    assign_types(lig.atoms);
-    // both typings: the pair list of a batch follows its maps' scoring function
-    B.make_pairs(true);
-    B.make_pairs(false);
-    if (!atom_typing_xs) {
-        lig.pairs = lig.pairs_ad;
-        lig.glue_pairs = lig.glue_pairs_ad;
-    }
+    finish_ligand(B, root, atom_typing_xs);
     return lig;
+}
+
+bool looks_like_sdf(const std::string& text) {
+    // a V2000 molfile: the counts line (4th line) ends in "V2000"
+    std::size_t pos = 0;
+    for (int k = 0; k < 3; ++k) {
+        pos = text.find('\n', pos);
+        if (pos == std::string::npos) return false;
+        ++pos;
+    }
+    std::size_t end = text.find('\n', pos);
+    std::string counts = text.substr(pos, end == std::string::npos ? std::string::npos : end - pos);
+    return counts.find("V2000") != std::string::npos || counts.find("V3000") != std::string::npos;
+}
+
+// SDF (V2000) ligand with the torsion tree written by the reference's ligand
+// preparation (unidock_tools torsion_tree.py): the property blocks "fragInfo"
+// (the SDF atom numbers of each rigid fragment; fragment 0 is the root),
+// "torsionInfo" (lines "a b fa fb": rotatable bond a-b with a in fragment fa
+// and b in fragment fb) and "atomInfo" (atom number, partial charge in columns
+// 4-13, AutoDock type from column 14).  Followed:
+//   atom lines       parse_pdbqt.cpp:129-144 (x/y/z in columns 1-30, element at 32-33)
+//   property blocks  parse_pdbqt.cpp:612-733 (a block runs to the next empty line;
+//                    "$$$$" lines are dropped; every other line is kept as context)
+//   tree             parse_pdbqt.cpp:735-859 and :400-420, :962-1000: root = fragment 0
+//                    in listed order; for each atom of a fragment in order and each
+//                    torsion naming it, the fragment on the other side becomes a branch
+//                    of that atom unless already placed; the branch's immobile atom is
+//                    the torsion's other atom.
+// Without keep_h, atoms of AutoDock type H are left out of every fragment (their
+// lines stay in the context with the input coordinates).  Without fragInfo the
+// ligand is one rigid body of all atoms and TORSDOF 0.  TORSDOF is the number of
+// torsionInfo lines.
+Ligand parse_ligand_sdf(const std::string& text, bool keep_h, int atom_typing_xs) {
+    Ligand lig;
+    lig.sdf = true;
+    LineReader in;
+    {
+        std::istringstream ss(text);
+        std::string s;
+        while (std::getline(ss, s)) {
+            if (!s.empty() && s.back() == '\r') s.pop_back();
+            in.lines.push_back(s);
+        }
+    }
+    Builder B(lig);
+    std::string s;
+    for (int k = 0; k < 3; ++k) {
+        if (!in.next(s)) throw std::runtime_error("SDF record ends inside its header.");
+        B.add_context(s);
+        if (k == 0) lig.name = trim(s);
+    }
+    if (!in.next(s)) throw std::runtime_error("SDF record has no counts line.");
+    B.add_context(s);
+    if (s.find("V3000") != std::string::npos) throw std::runtime_error("V3000 molfiles are not supported.");
+    const int n_atoms = (int)convert<float>(column(s, 1, 3, true, "atom count"), s, "Atom num");
+    const int n_bonds = (int)convert<float>(column(s, 4, 6, true, "bond count"), s, "Bond num");
+    if (n_atoms <= 0) throw std::runtime_error("No atoms in this ligand.");
+    std::vector<ParsedAtom> atoms(n_atoms);
+    for (int i = 0; i < n_atoms; ++i) {
+        if (!in.next(s)) throw std::runtime_error("SDF record ends inside its atom block.");
+        B.add_context(s);
+        ParsedAtom& a = atoms[i];
+        for (int k = 0; k < 3; ++k)
+            a.xyz[k] = convert<float>(column(s, 1 + 10 * k, 10 + 10 * k, true, "coordinate"), s, "Coordinate");
+        if (s.size() < 32) throw std::runtime_error("line too short for the element: " + s);
+        std::string name = s.substr(31, 2);
+        if (name.size() == 2 && name[1] == ' ') name = name.substr(0, 1);
+        a.ad = ad_type_from_name(name);
+        a.number = (unsigned)(i + 1);
+        a.context = (int)lig.context.size() - 1;
+    }
+    for (int i = 0; i < n_bonds; ++i) {
+        if (!in.next(s)) throw std::runtime_error("SDF record ends inside its bond block.");
+        B.add_context(s);
+    }
+    while (in.next(s)) {
+        B.add_context(s);
+        if (s.find("M  END") != std::string::npos) break;
+    }
+    std::vector<std::vector<int>> frags, torsions;
+    while (in.next(s)) {
+        if (s.find("$$$$") != std::string::npos) continue;
+        B.add_context(s);
+        if (s.empty() || s[0] != '>') continue;
+        const bool atom_info = s.find("atomInfo") != std::string::npos || s.find("atom_info") != std::string::npos;
+        const bool torsion = !atom_info && s.find("torsion") != std::string::npos;
+        const bool frag = !atom_info && !torsion && s.find("frag") != std::string::npos;
+        while (in.next(s)) {
+            B.add_context(s);
+            if (s.empty()) break;
+            if (atom_info) {
+                std::size_t sp = s.find(' ');
+                std::size_t idlen = std::min<std::size_t>(sp == std::string::npos ? 3 : sp, 3);
+                if (idlen == 0 || s.size() < 14) throw std::runtime_error("Invalid atomInfo line: " + s);
+                int id = convert<int>(column(s, 1, idlen, true, "atom id"), s, "AtomId");
+                float q = convert<float>(column(s, 4, 13, true, "partial charge"), s, "Partial Charge");
+                if (id < 1 || id > n_atoms) throw std::runtime_error("atomInfo names a missing atom: " + s);
+                atoms[id - 1].charge = q;
+                atoms[id - 1].ad = ad_type_from_name(trim(s.substr(13)));
+            } else if (torsion) {
+                std::vector<int> t = sdf_ints(s);
+                if (t.size() < 4) throw std::runtime_error("Invalid torsionInfo line: " + s);
+                torsions.push_back(t);
+            } else if (frag) {
+                frags.push_back(sdf_ints(s));
+            }
+        }
+    }
+    for (auto& a : atoms)
+        if (a.ad >= AD_SIZE)
+            throw std::runtime_error("SDF atom " + std::to_string(a.number) + " has no valid AutoDock type.");
+    for (auto& f : frags)
+        for (int id : f)
+            if (id < 1 || id > n_atoms) throw std::runtime_error("fragInfo names a missing atom.");
+    for (auto& t : torsions)
+        if (t[2] < 0 || t[3] < 0 || (frags.size() && (t[2] >= (int)frags.size() || t[3] >= (int)frags.size())))
+            throw std::runtime_error("torsionInfo names a missing fragment.");
+    lig.torsdof = (int)torsions.size();
+    if (!keep_h)
+        for (auto& f : frags)
+            f.erase(std::remove_if(f.begin(), f.end(), [&](int id) { return atoms[id - 1].ad == AD_H; }), f.end());
+
+    Block root;
+    if (frags.empty()) {
+        lig.torsdof = 0;
+        for (auto& a : atoms) root.atoms.push_back(Block::Entry{a, {}});
+    } else {
+        std::vector<char> placed(frags.size(), 0);
+        placed[0] = 1;
+        // fill block `b` with fragment f (immobile atom `to`, 0 for the root) and its branches
+        std::function<void(Block&, int, int)> fill = [&](Block& b, int f, int to) {
+            for (int id : frags[f]) {
+                if (id == to) b.immobile = (int)b.atoms.size();
+                b.atoms.push_back(Block::Entry{atoms[id - 1], {}});
+            }
+            for (int id : frags[f]) {
+                for (const auto& t : torsions) {
+                    int from, next_to, nf;
+                    if (t[0] == id) {
+                        from = t[0], next_to = t[1], nf = t[3];
+                    } else if (t[1] == id) {
+                        from = t[1], next_to = t[0], nf = t[2];
+                    } else {
+                        continue;
+                    }
+                    if (placed[nf]) continue;
+                    for (auto& e : b.atoms) {
+                        if ((int)e.a.number != from) continue;
+                        placed[nf] = 1;
+                        e.children.emplace_back(new Block());
+                        fill(*e.children.back(), nf, next_to);
+                        break;
+                    }
+                }
+            }
+            if (to > 0 && b.immobile < 0)
+                throw std::runtime_error("Atom " + std::to_string(to) + " has not been found in this branch.");
+        };
+        fill(root, 0, 0);
+    }
+    if (root.atoms.empty()) throw std::runtime_error("No atoms in this ligand.");
+    finish_ligand(B, root, atom_typing_xs);
+    return lig;
+}
+
+Ligand parse_ligand(const std::string& text, bool keep_h, int atom_typing_xs) {
+    return looks_like_sdf(text) ? parse_ligand_sdf(text, keep_h, atom_typing_xs)
+                                : parse_ligand_pdbqt(text, atom_typing_xs);
 }
 
 // Rigid receptor: atoms in file order, bonds from distances (all receptor

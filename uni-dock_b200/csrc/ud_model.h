@@ -147,6 +147,13 @@ struct Ligand {
 // bonds, types and pairs.  Throws std::runtime_error on malformed input.
 Ligand parse_ligand_pdbqt(const std::string& text, int atom_typing_xs = 1);
 
+// SDF (V2000) ligand carrying fragInfo / torsionInfo / atomInfo properties;
+// keep_h keeps AutoDock type H atoms in the fragments (the reference CLI always does).
+Ligand parse_ligand_sdf(const std::string& text, bool keep_h = true, int atom_typing_xs = 1);
+bool looks_like_sdf(const std::string& text);
+// SDF when the text is a V2000 molfile, PDBQT otherwise.
+Ligand parse_ligand(const std::string& text, bool keep_h = true, int atom_typing_xs = 1);
+
 // Receptor atoms with types assigned from bonds (rigid receptor).
 struct Receptor {
     std::vector<std::array<float, 3>> xyz;
@@ -165,6 +172,8 @@ struct PoseResult {
     float e = 0, inter = 0, intra = 0, total = 0, conf_indep = 0, unbound = 0, lb = 0, ub = 0;
     std::vector<float> heavy_xyz;
 };
+// Input record of the ligand with the coordinates of one pose, no remarks.
+std::string write_structure(const Ligand& lig, const float* pose);
 std::string write_pdbqt_models(const Ligand& lig, const std::vector<PoseResult>& poses,
                                bool ad4);
 std::string write_sdf_models(const Ligand& lig, const std::vector<PoseResult>& poses, bool ad4);

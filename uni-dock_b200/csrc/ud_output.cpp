@@ -1,6 +1,7 @@
 // Pose output in the reference's formats: PDBQT MODEL blocks with the
 // "REMARK VINA RESULT" header (unidock/src/lib/vina.cpp:725-748, model.cpp:726-846)
-// and SDF records with the "> <Uni-Dock RESULT>" block (vina.cpp:750-770).
+// and SDF records with the "> <Uni-Dock RESULT>" block (vina.cpp:750-770,
+// model.cpp:850-866).
 #include <cstdio>
 #include <iomanip>
 #include <sstream>
@@ -72,9 +73,70 @@ std::string write_pdbqt_models(const Ligand& lig, const std::vector<PoseResult>&
     return out.str();
 }
 
+static void put_sdf_coord(std::string& line, std::size_t col, float v) {  // 1-based column, 10 wide
+    std::string s = fixed(v, 10, 4);
+    if (s.size() != 10) throw std::runtime_error("coordinate does not fit SDF columns");
+    if (line.size() < col - 1 + 10) line.resize(col - 1 + 10, ' ');
+    line.replace(col - 1, 10, s);
+}
+
+// A ligand read from SDF is written back as its own record, each atom line
+// with the pose's coordinates (model.cpp:779-785, 822-863): the input lines in
+// order ("$$$$" lines were dropped at parse time), then the result block and
+// "$$$$".
+static std::string write_sdf_context(const Ligand& lig, const std::vector<PoseResult>& poses, bool ad4) {
+    std::ostringstream out;
+    std::vector<float> xyz(3 * lig.atoms.size());
+    for (std::size_t m = 0; m < poses.size(); ++m) {
+        ligand_coords(lig, poses[m].pose.data(), xyz.data());
+        for (const auto& c : lig.context) {
+            if (c.second >= 0) {
+                std::string line = c.first;
+                put_sdf_coord(line, 1, xyz[3 * c.second]);
+                put_sdf_coord(line, 11, xyz[3 * c.second + 1]);
+                put_sdf_coord(line, 21, xyz[3 * c.second + 2]);
+                out << line << '\n';
+            } else {
+                out << c.first << '\n';
+            }
+        }
+        out << sdf_remarks(poses[m], ad4);
+        out << "$$$$\n";
+    }
+    return out.str();
+}
+
+// The ligand's input record at one pose with no result block: an SDF
+// ligand in SDF columns, a PDBQT one in PDBQT columns (model.h:125-144,
+// write_structure / write_sdf_structure).
+std::string write_structure(const Ligand& lig, const float* pose) {
+    std::vector<float> xyz(3 * lig.atoms.size());
+    ligand_coords(lig, pose, xyz.data());
+    std::ostringstream out;
+    for (const auto& c : lig.context) {
+        if (c.second < 0) {
+            out << c.first << '\n';
+            continue;
+        }
+        std::string line = c.first;
+        const float* x = &xyz[3 * c.second];
+        if (lig.sdf) {
+            put_sdf_coord(line, 1, x[0]);
+            put_sdf_coord(line, 11, x[1]);
+            put_sdf_coord(line, 21, x[2]);
+        } else {
+            put_coord(line, 31, x[0]);
+            put_coord(line, 39, x[1]);
+            put_coord(line, 47, x[2]);
+        }
+        out << line << '\n';
+    }
+    return out.str();
+}
+
 std::string write_sdf_models(const Ligand& lig, const std::vector<PoseResult>& poses, bool ad4) {
-    // SDF records are written for ligands that came from SDF input; PDBQT
-    // input is written as a minimal V2000 block of its atoms.
+    if (lig.sdf) return write_sdf_context(lig, poses, ad4);
+    // PDBQT input is written as a minimal V2000 block of its atoms.
     std::ostringstream out;
     std::vector<float> xyz(3 * lig.atoms.size());
     static const char* el_name[] = {"H", "C", "N", "O", "S", "P", "F", "Cl", "Br", "I", "Si", "At", "X", "X"};

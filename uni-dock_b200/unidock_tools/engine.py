@@ -75,6 +75,8 @@ def lib():
         "ud_maps_read": ([vp, C.c_int, fp, C.c_size_t], C.c_int),
         "ud_maps_destroy": ([vp], C.c_int),
         "ud_ligand_parse": ([C.c_char_p, C.c_size_t, C.POINTER(vp)], C.c_int),
+        "ud_ligand_parse_sdf": ([C.c_char_p, C.c_size_t, C.c_int, C.POINTER(vp)], C.c_int),
+        "ud_ligand_write": ([vp, fp, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
         "ud_ligand_counts": ([vp, ip], C.c_int),
         "ud_ligand_export": ([vp, fp, fp, ip, ip, ip, fp, ip, ip, ip, ip, fp, ip, ip], C.c_int),
         "ud_ligand_initial_pose": ([vp, fp], C.c_int),
@@ -284,13 +286,17 @@ class Maps:
 
 
 class Ligand:
-    """Host-side torsion-tree model parsed from PDBQT (ud_ligand_parse)."""
+    """Host-side torsion-tree model parsed from PDBQT or SDF text
+    (ud_ligand_parse; ud_ligand_parse_sdf when keep_h is given)."""
 
-    def __init__(self, pdbqt: str, _handle=None):
+    def __init__(self, text: str, _handle=None, keep_h=None):
         if _handle is None:
-            b = pdbqt.encode()
+            b = text.encode()
             h = C.c_void_p()
-            _check(lib().ud_ligand_parse(b, len(b), C.byref(h)))
+            if keep_h is None:
+                _check(lib().ud_ligand_parse(b, len(b), C.byref(h)))
+            else:
+                _check(lib().ud_ligand_parse_sdf(b, len(b), int(bool(keep_h)), C.byref(h)))
         else:
             h = C.c_void_p(_handle)
         self.h = h
@@ -330,6 +336,15 @@ class Ligand:
         o = np.zeros(7, np.float32)
         _check(lib().ud_ligand_conf_indep(self.h, _f(o)))
         return o
+
+    def write_structure(self, pose) -> str:
+        """The input record (SDF or PDBQT) with the coordinates of `pose` (ud_ligand_write)."""
+        pose = np.ascontiguousarray(pose, np.float32)
+        n = C.c_size_t()
+        _check(lib().ud_ligand_write(self.h, _f(pose), None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value + 1)
+        _check(lib().ud_ligand_write(self.h, _f(pose), buf, n.value + 1, C.byref(n)))
+        return buf.value.decode()
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:

@@ -253,6 +253,86 @@ class Ligand:
         return "\n".join(lines) + "\n"
 
 
+    def to_sdf(self) -> str:
+        """SDF (V2000) with the torsion-tree properties of the reference's ligand
+        preparation (fragInfo, torsionInfo, atomInfo: unidock_tools
+        torsion_tree.py get_sdf_torsion_tree_info): heavy atoms first, then the
+        polar hydrogens; fragment 0 (the root) is the most central fragment."""
+        n = self.n_heavy
+        adj = [[] for _ in range(n)]
+        for bi, (a, b) in enumerate(self.bonds):
+            adj[a].append((b, bi))
+            adj[b].append((a, bi))
+        rot = set(self.rotatable)
+        frag = [-1] * n
+        nf = 0
+        for s0 in range(n):
+            if frag[s0] >= 0:
+                continue
+            stack = [s0]
+            frag[s0] = nf
+            while stack:
+                u = stack.pop()
+                for v, bi in adj[u]:
+                    if bi not in rot and frag[v] < 0:
+                        frag[v] = nf
+                        stack.append(v)
+            nf += 1
+        fadj = [[] for _ in range(nf)]
+        for bi in rot:
+            a, b = self.bonds[bi]
+            fadj[frag[a]].append(frag[b])
+            fadj[frag[b]].append(frag[a])
+
+        def height(root):
+            seen, best, stack = {root}, 0, [(root, 0)]
+            while stack:
+                u, d = stack.pop()
+                best = max(best, d)
+                for v in fadj[u]:
+                    if v not in seen:
+                        seen.add(v)
+                        stack.append((v, d + 1))
+            return best
+
+        sizes = [frag.count(f) for f in range(nf)]
+        root = min(range(nf), key=lambda f: (height(f), -sizes[f], f))
+        renum = {root: 0}
+        for f in range(nf):
+            if f != root:
+                renum[f] = len(renum)
+        charges = self.charge if self.charge is not None else np.zeros(n)
+        xyz = [np.asarray(x, float) for x in self.heavy_xyz] + [np.asarray(h, float) for _, h in self.h_xyz]
+        elem = list(self.element) + ["H"] * len(self.h_xyz)
+        adt = [self.ad_type(i) for i in range(n)] + ["HD"] * len(self.h_xyz)
+        q = [float(c) for c in charges] + [0.0] * len(self.h_xyz)
+        atom_frag = [renum[frag[i]] for i in range(n)] + [renum[frag[p]] for p, _ in self.h_xyz]
+        bonds = [(a, b) for a, b in self.bonds] + [(p, n + k) for k, (p, _) in enumerate(self.h_xyz)]
+        out = [self.name, "  unidock_b200 synth", ""]
+        out.append("%3d%3d  0  0  0  0  0  0  0  0999 V2000" % (len(xyz), len(bonds)))
+        for i in range(len(xyz)):
+            out.append("%10.4f%10.4f%10.4f %-3s 0  0  0  0  0  0  0  0  0  0  0  0"
+                       % (xyz[i][0], xyz[i][1], xyz[i][2], elem[i]))
+        for a, b in bonds:
+            out.append("%3d%3d  1  0" % (a + 1, b + 1))
+        out.append("M  END")
+        out.append(">  <fragInfo>  (1) ")
+        for f in range(nf):
+            out.append(" ".join(str(i + 1) for i in range(len(xyz)) if atom_frag[i] == f))
+        out.append("")
+        out.append(">  <torsionInfo>  (1) ")
+        for bi in sorted(rot):
+            a, b = self.bonds[bi]
+            out.append("%d %d %d %d" % (a + 1, b + 1, renum[frag[a]], renum[frag[b]]))
+        out.append("")
+        out.append(">  <atomInfo>  (1) ")
+        for i in range(len(xyz)):
+            out.append(str(i + 1).ljust(3) + str(q[i])[:10].ljust(10) + adt[i].ljust(2))
+        out.append("")
+        out.append("$$$$")
+        return "\n".join(out) + "\n"
+
+
 def _pdbqt_atom(rec, serial, name, resname, resseq, xyz, charge, adtype):
     nm = name if len(name) >= 4 else " " + name.ljust(3)
     return "%-6s%5d %-4s %3s A%4d    %8.3f%8.3f%8.3f%6.2f%6.2f    %6.3f %-2s" % (
