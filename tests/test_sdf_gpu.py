@@ -20,6 +20,9 @@ REL = 1e-4
 def setup(receptor, tmp_path_factory):
     d = tmp_path_factory.mktemp("sdf")
     mols = [synth.make_ligand(14 + 6 * k, min(2 * k, 10), seed=700 + k, with_charges=True) for k in range(6)]
+    for L in mols:  # PDBQT keeps 3 decimals, SDF 4: give both files the same coordinates
+        L.heavy_xyz = np.round(L.heavy_xyz, 3)
+        L.h_xyz = [(a, np.round(h, 3)) for a, h in L.h_xyz]
     paths, sdf, pdbqt = [], [], []
     for k, L in enumerate(mols):
         p = d / f"l{k}.sdf"
@@ -52,13 +55,14 @@ def test_sdf_model_energy_and_gradient_match_reference(setup, receptor):
 
 def test_sdf_and_pdbqt_of_one_molecule_score_alike(setup):
     """Atom order and torsion tree differ between the two files of one
-    molecule; the energy at the input coordinates does not."""
+    molecule; the energy at the input coordinates does not (up to FP32
+    summation order)."""
     _, _, sdf, pdbqt, M = setup
     for a, b in zip(sdf, pdbqt):
         assert (a.n_atoms, a.n_torsions, a.n_pairs) == (b.n_atoms, b.n_torsions, b.n_pairs)
         ea, _ = engine.Batch(M, [a]).score_grad(np.zeros(1, np.int32), a.initial_pose()[None, :])
         eb, _ = engine.Batch(M, [b]).score_grad(np.zeros(1, np.int32), b.initial_pose()[None, :])
-        assert abs(ea[0] - eb[0]) <= 2e-4 * max(1.0, abs(eb[0])), (ea, eb)
+        assert abs(ea[0] - eb[0]) <= 1e-4 * max(1.0, abs(eb[0])), (ea, eb)
 
 
 def test_search_results_written_as_sdf_records(setup):
