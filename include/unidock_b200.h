@@ -231,6 +231,12 @@ typedef struct {
     int use_graph;          /* batched form: the per-batch sequence (queue reset, search
                                kernel, result copies) captured once as a CUDA graph and
                                replayed while parameters and buffers are unchanged */
+    int refine_step;        /* > 0: each mode is refined against the receptor atoms in up
+                               to refine_step rounds and scored against them, as the
+                               reference does unless --no_refine (--refine_step, CLI
+                               default 3; vina.h:251-272).  Vina / Vinardo maps built
+                               from a receptor only; otherwise, and at 0, the modes keep
+                               their grid energies (--no_refine). */
 } ud_search_params;
 
 /* Launch configuration picked by ud_autotune. */
@@ -259,9 +265,11 @@ int ud_autotune(ud_batch batch, const ud_search_params* params, ud_tune_result* 
  * monte_carlo_template::do_docking (unidock/src/cuda/monte_carlo.cu:2975-3010).
  * Synchronous: returns after the results are on the host. */
 int ud_search(ud_batch batch, const ud_search_params* params, void* stream);
-/* ud_search split in two: the asynchronous device part (kernels enqueued on
- * `stream`, inputs already resident) and the host part (device-to-host copy,
- * clustering, rescoring).  ud_search == ud_search_launch + ud_search_collect. */
+/* ud_search split in two: the asynchronous device part (search kernel, then
+ * the clustering of every ligand's chains into modes and, with refine_step,
+ * their refinement against the receptor atoms, all enqueued on `stream` with
+ * inputs already resident) and the host part (final scores, ordering, RMSD
+ * bounds).  ud_search == ud_search_launch + ud_search_collect. */
 int ud_search_launch(ud_batch batch, const ud_search_params* params, void* stream);
 /* The set-up of ud_search_launch without the launch: result buffers (device
  * and page-locked host), the ligand order and, with use_graph, the captured
@@ -320,6 +328,32 @@ int ud_result_write(ud_batch batch, int lig, int format, char* buf, size_t cap, 
  * the --local_only path of Vina::optimize (unidock/src/lib/vina.cpp:1385-1428). */
 int ud_optimize(ud_batch batch, const int* pose_ligand, float* poses, int n_poses, int pose_stride,
                 int max_steps, float v, float* e_out, int* evals_out, void* stream);
+/* ---------------------------------------------------------------- receptor atoms
+ * Scoring against the receptor atoms the maps were built from, instead of the
+ * maps: the reference's non_cache (unidock/src/lib/non_cache.cpp), which it
+ * uses after the search and for --score_only / --local_only scores unless
+ * --no_refine.  An atom outside the box is scored at its position clamped into
+ * the box plus a penalty of slope per Angstrom.  Vina / Vinardo maps built
+ * from a receptor (ud_maps_create) only; others give UD_ERR_STATE.
+ *
+ * Energy and gradient (change layout, 6 + T floats per pose) at fixed poses:
+ * model::eval_deriv with non_cache::eval_deriv (non_cache.cpp:420-500) at
+ * out-of-box slope `slope` and curl cap v. */
+int ud_score_grad_receptor(ud_batch batch, const int* pose_ligand, const float* poses, int n_poses, int pose_stride,
+                           float slope, float v, float* e_out, float* g_out, int g_stride, void* stream);
+/* Refinement of poses (updated in place), as the reference refines each mode
+ * after its search (vina.h:251-272): up to refine_step rounds of BFGS
+ * ((25 + atoms)/3 steps, curl cap 1000) against the receptor atoms at slope
+ * 100, 1e4, 1e6, ..., stopping once every heavy atom is inside the box; then
+ * the scoring energies.  out4 per pose: {last BFGS energy, inter (receptor
+ * atoms, slope 1e6, curl cap 1000, nearest-bin table), intra (model::evali),
+ * 1 if inside the box else 0}. */
+int ud_refine(ud_batch batch, const int* pose_ligand, float* poses, int n_poses, int pose_stride, int refine_step,
+              float* out4, void* stream);
+/* ud_score_terms with the inter energy from the receptor atoms: Vina::score
+ * without --no_refine (vina.cpp:1168-1243). */
+int ud_score_terms_receptor(ud_batch batch, const int* pose_ligand, const float* poses, int n_poses, int pose_stride,
+                            float* out, void* stream);
 /* Measured FP32 FMA throughput of the current device in TFLOP/s (roofline
  * denominator of the search kernels).  No counterpart in the reference. */
 int ud_device_fp32_peak(float* tflops);

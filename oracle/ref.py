@@ -56,6 +56,11 @@ def lib():
         L.udref_bfgs.restype = C.c_float
         L.udref_mc.argtypes = [vp, vp, C.c_uint, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, fp, fp, C.c_int,
                                C.POINTER(C.c_longlong)]
+        L.udref_nc_eval_deriv.argtypes = [vp, vp, fp, fp, fp, C.c_float, C.c_float, fp]
+        L.udref_nc_eval_deriv.restype = C.c_float
+        L.udref_refine.argtypes = [vp, vp, fp, fp, fp, C.c_int, fp]
+        L.udref_nc_score.argtypes = [vp, vp, fp, fp, fp, C.c_float, fp]
+        L.udref_cluster.argtypes = [vp, C.c_int, fp, C.c_int, fp, C.c_float, C.c_int, ip]
         L.udref_ad4_maps_read.restype = vp
         L.udref_ad4_maps_read.argtypes = [C.c_char_p, fp, C.c_int]
         L.udref_ad4_pair.argtypes = [C.c_int, C.c_float, C.c_int, C.c_float, C.c_float, fp, C.c_int]
@@ -216,6 +221,41 @@ class RefLigand:
         ec = C.c_int()
         e = lib().udref_bfgs(self.h, maps.h, _f(p), _f(q), _f(t), v, steps, C.byref(ec))
         return float(e), np.concatenate([p, q, t[:self.n_torsions]]), ec.value
+
+    def _split(self, pose):
+        pose = np.array(pose, np.float32)
+        t = pose[7:7 + self.n_torsions].copy() if self.n_torsions else np.zeros(1, np.float32)
+        return pose[0:3].copy(), pose[3:7].copy(), np.ascontiguousarray(t)
+
+    def nc_eval_deriv(self, maps, pose, slope=1e6, v=1000.0):
+        """model::eval_deriv against the receptor atoms (non_cache)."""
+        p, q, t = self._split(pose)
+        g = np.zeros(6 + self.n_torsions, np.float32)
+        e = lib().udref_nc_eval_deriv(self.h, maps.h, _f(p), _f(q), _f(t), slope, v, _f(g))
+        return float(e), g
+
+    def refine(self, maps, pose, refine_step=3):
+        """The per-pose refinement of the reference's GPU search post-processing:
+        (refined pose, last BFGS energy, inter against receptor atoms, intra, inside box)."""
+        p, q, t = self._split(pose)
+        out = np.zeros(3, np.float32)
+        within = lib().udref_refine(self.h, maps.h, _f(p), _f(q), _f(t), refine_step, _f(out))
+        return np.concatenate([p, q, t[:self.n_torsions]]), float(out[0]), float(out[1]), float(out[2]), bool(within)
+
+    def nc_score(self, maps, pose, v=1000.0):
+        """(inter against receptor atoms at slope 1e6, intra, intramolecular)."""
+        p, q, t = self._split(pose)
+        out = np.zeros(3, np.float32)
+        lib().udref_nc_score(self.h, maps.h, _f(p), _f(q), _f(t), v, _f(out))
+        return out
+
+    def cluster(self, poses, energies, min_rmsd=1.0, max_modes=9):
+        """Chain indices of the modes, in order, as the reference clusters chain results."""
+        poses = np.ascontiguousarray(poses, np.float32)
+        e = np.ascontiguousarray(energies, np.float32)
+        out = np.zeros(max(len(e), 1), np.int32)
+        n = lib().udref_cluster(self.h, len(e), _f(poses), poses.shape[1], _f(e), min_rmsd, max_modes, _i(out))
+        return out[:n]
 
     def mc(self, maps, seed, n_chains, global_steps, local_steps=None, threads=1, hunt_cap=10.0):
         steps = (25 + self.n_atoms) // 3 if local_steps is None else local_steps

@@ -20,6 +20,7 @@
 #include "coords.h"
 #include "model.h"
 #include "mutate.h"
+#include "non_cache.h"
 #include "parse_pdbqt.h"
 #include "precalculate.h"
 #include "quasi_newton.h"
@@ -37,6 +38,7 @@ struct RefMaps {
     ad4cache ad4;               // AutoDock 4.2 maps read from .map files
     const igrid* ig = &grid;    // the maps the model is scored against
     grid_dims gd;
+    std::unique_ptr<non_cache> nc;  // explicit receptor atoms, built on first use
     vec corner1() const { return ig == &grid ? grid.corner1() : ad4.corner1(); }
     vec corner2() const { return ig == &grid ? grid.corner2() : ad4.corner2(); }
 };
@@ -311,6 +313,114 @@ float udref_bfgs(void* lh, void* mh, float* pos, float* quat, float* tors, float
     read_conf(out.c, pos, quat, tors);
     if (evalcount) *evalcount = ec;
     return out.e;
+}
+
+// The receptor-atom scorer Vina::compute_vina_maps keeps unless --no_refine
+// (vina.cpp:557-562), and the docking model it scores: the receptor with the
+// ligand appended, as set_ligand_from_object_gpu builds each ligand's model.
+static non_cache& nc_of(RefMaps* M) {
+    if (!M->nc) M->nc.reset(new non_cache(M->rec, M->gd, M->pre.get(), 1e6, std::vector<bias_element>()));
+    return *M->nc;
+}
+static model docking_model(RefMaps* M, RefLigand* L) {
+    model mm = M->rec;
+    mm.append(L->m);
+    return mm;
+}
+
+// model::eval_deriv against the receptor atoms (non_cache::eval_deriv,
+// non_cache.cpp:420-500) at out-of-box slope `slope`, curl caps v.
+float udref_nc_eval_deriv(void* lh, void* mh, const float* pos, const float* quat, const float* tors, float slope,
+                          float v, float* g) {
+    auto L = (RefLigand*)lh;
+    auto M = (RefMaps*)mh;
+    non_cache& nc = nc_of(M);
+    nc.slope = slope;
+    model mm = docking_model(M, L);
+    conf c = make_conf(mm, pos, quat, tors);
+    mm.set(c);
+    change ch(mm.get_size());
+    fl e = mm.eval_deriv(*L->pre, nc, vec(v, v, v), ch);
+    for (sz i = 0; i < ch.num_floats(); ++i) g[i] = ch(i);
+    nc.slope = 1e6;
+    return e;
+}
+
+// The refinement of one pose in Vina::global_search_gpu (vina.h:251-272): up to
+// refine_step rounds of quasi_newton against the receptor atoms at slope
+// 100 * 10^(2p), stopping once the heavy atoms are inside the box; then
+// non_cache::eval at slope 1e6 and model::evali at the authentic cap
+// (score_gpu, vina.cpp:1245-1283).  Pose updated in place; out[0] = the last
+// quasi_newton energy, out[1] = inter (receptor atoms), out[2] = intra;
+// returns 1 when the pose ended inside the box.
+int udref_refine(void* lh, void* mh, float* pos, float* quat, float* tors, int refine_step, float* out) {
+    auto L = (RefLigand*)lh;
+    auto M = (RefMaps*)mh;
+    non_cache& nc = nc_of(M);
+    model mm = docking_model(M, L);
+    conf c = make_conf(mm, pos, quat, tors);
+    output_type o(c, 0);
+    change g(mm.get_size());
+    quasi_newton qn;
+    qn.max_steps = unsigned((25 + mm.num_movable_atoms()) / 3);
+    const vec authentic_v(1000, 1000, 1000);
+    int evalcount = 0;
+    VINA_FOR(p, refine_step) {
+        nc.slope = 100 * std::pow(10.0, 2.0 * p);
+        qn(mm, *L->pre, nc, o, g, authentic_v, evalcount);
+        if (nc.within(mm)) break;
+    }
+    const int within = nc.within(mm) ? 1 : 0;
+    nc.slope = 1e6;
+    read_conf(o.c, pos, quat, tors);
+    mm.set(o.c);
+    out[0] = o.e;
+    out[1] = nc.eval(mm, authentic_v[1]);
+    out[2] = mm.evali(*L->pre, authentic_v);
+    return within;
+}
+
+// Scoring-path energies against the receptor atoms at a fixed pose (Vina::score
+// without --no_refine, vina.cpp:1168-1243): out[0] = non_cache::eval (slope 1e6,
+// cap v), out[1] = model::evali, out[2] = model::eval_intramolecular.
+int udref_nc_score(void* lh, void* mh, const float* pos, const float* quat, const float* tors, float v, float* out) {
+    auto L = (RefLigand*)lh;
+    auto M = (RefMaps*)mh;
+    non_cache& nc = nc_of(M);
+    nc.slope = 1e6;
+    model mm = docking_model(M, L);
+    conf c = make_conf(mm, pos, quat, tors);
+    mm.set(c);
+    vec vv(v, v, v);
+    out[0] = nc.eval(mm, v);
+    out[1] = mm.evali(*L->pre, vv);
+    out[2] = mm.eval_intramolecular(*L->pre, nc, vv);
+    return 0;
+}
+
+// Clustering of one ligand's chain results as the reference's GPU path does
+// it: each chain's best pose through add_to_output_container (coords.cpp:44-68)
+// with num_saved_mins = max_modes, then Vina::remove_redundant (vina.cpp:
+// 1465-1470).  Writes the chain indices of the modes in their final order and
+// returns their count.
+int udref_cluster(void* lh, int n_chains, const float* poses, int pose_stride, const float* energies, float min_rmsd,
+                  int max_modes, int* out_chain) {
+    auto L = (RefLigand*)lh;
+    model& m = L->m;
+    output_container out;
+    for (int k = 0; k < n_chains; ++k) {
+        const float* p = poses + (size_t)k * pose_stride;
+        conf c = make_conf(m, p, p + 3, p + 7);
+        m.set(c);
+        output_type t(c, energies[k]);
+        t.coords = m.get_heavy_atom_movable_coords();
+        t.lb = (fl)k;  // the chain index travels in a field clustering does not read
+        add_to_output_container(out, t, min_rmsd, (sz)max_modes);
+    }
+    output_container tmp;
+    VINA_FOR_IN(i, out) add_to_output_container(tmp, out[i], min_rmsd, out.size());
+    for (sz i = 0; i < tmp.size(); ++i) out_chain[i] = (int)tmp[i].lb;
+    return (int)tmp.size();
 }
 
 // Monte-Carlo chains of the CPU search (monte_carlo.cu:2319-2356): chains run on

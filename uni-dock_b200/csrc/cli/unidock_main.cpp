@@ -68,8 +68,9 @@ const OptSpec kOptions[] = {
     {"score_only", 1, "score only - search space can be omitted", "Advanced"},
     {"score_file", 0, "score only output file in batch mode, with 'score_only' option", "Advanced"},
     {"local_only", 1, "do local search only", "Advanced"},
-    {"no_refine", 1, "do not use explicit receptor atoms after docking (this build always uses the grids)",
-     "Advanced"},
+    {"no_refine", 1, "when --receptor is provided, do not use explicit receptor atoms (instead of precalculated "
+                     "grids) for: (1) local optimization and scoring after docking, (2) --local_only and "
+                     "--score_only", "Advanced"},
     {"force_even_voxels", 1, "calculated grid maps will have an even number of voxels in each dimension",
      "Advanced"},
     {"randomize_only", 1, "randomize input (not supported by this build)", "Advanced"},
@@ -105,7 +106,7 @@ const OptSpec kOptions[] = {
     {"verbosity", 0, "verbosity (0=no output, 1=normal, 2=verbose)", "Misc"},
     {"max_step", 0, "maximum number of steps in each MC run (if zero, the number of MC steps is based on "
                     "heuristics)", "Misc"},
-    {"refine_step", 0, "number of steps in refinement (accepted; refinement uses the grids)", "Misc"},
+    {"refine_step", 0, "number of steps in refinement, default=3", "Misc"},
     {"max_gpu_memory", 0, "maximum gpu memory to use in MiB (default=0, use the available memory)", "Misc"},
     {"search_mode", 0, "search mode of vina (fast, balance, detail)", "Misc"},
     {"batch_size", 0, "ligands per GPU batch (default 4096)", "Misc"},
@@ -350,7 +351,52 @@ struct Setup {
     int verbosity = 1;
     int threads = 1;
     bool autotune = false;
+    // scores after docking, --score_only and --local_only against the receptor
+    // atoms (the reference unless --no_refine; Vina / Vinardo with --receptor)
+    bool receptor_scoring = false;
 };
+
+// --score_only / --local_only energy vector of one pose (Vina::score, vina.cpp:1168-1243).
+void score_pose(const Setup& S, ud_batch b, std::vector<float>& pose, float* en) {
+    int lig = 0;
+    if (S.receptor_scoring)
+        check(ud_score_terms_receptor(b, &lig, pose.data(), 1, (int)pose.size(), en, nullptr), "score");
+    else
+        check(ud_score_terms(b, &lig, pose.data(), 1, (int)pose.size(), en, nullptr), "score");
+}
+
+// Vina::optimize (vina.cpp:1385-1428): up to five rounds of BFGS on the maps at
+// curl cap 1000, until the heavy atoms are inside the box (cache::is_in_grid,
+// margin 1e-4).
+void local_optimize(ud_maps maps, ud_batch b, ud_ligand h, std::vector<float>& pose) {
+    int counts[8];
+    check(ud_ligand_counts(h, counts), "ligand");
+    const int n = counts[0];
+    std::vector<int> el(n);
+    check(ud_ligand_export(h, nullptr, nullptr, nullptr, nullptr, el.data(), nullptr, nullptr, nullptr, nullptr,
+                           nullptr, nullptr, nullptr, nullptr),
+          "ligand");
+    int dims[3], n_maps = 0;
+    float init[3], factor[3];
+    check(ud_maps_info(maps, dims, init, factor, &n_maps), "maps");
+    std::vector<float> xyz(3 * (size_t)n);
+    const float margin = 1e-4f;
+    for (int round = 0; round < 5; ++round) {
+        int lig = 0, ev = 0;
+        float e = 0;
+        check(ud_optimize(b, &lig, pose.data(), 1, (int)pose.size(), 0, 1000.0f, &e, &ev, nullptr), "optimize");
+        check(ud_ligand_coords(h, pose.data(), xyz.data()), "coords");
+        bool inside = true;
+        for (int a = 0; a < n && inside; ++a) {
+            if (el[a] == 0) continue;  // hydrogen
+            for (int k = 0; k < 3; ++k) {
+                const float end = init[k] + (dims[k] - 1) / factor[k];
+                if (xyz[3 * a + k] < init[k] - margin || xyz[3 * a + k] > end + margin) inside = false;
+            }
+        }
+        if (inside) break;
+    }
+}
 
 // Maps from the receptor: Vina / Vinardo maps, or AD4 maps (types and charges
 // from the receptor PDBQT) in place of the external autogrid4 step.
@@ -484,15 +530,10 @@ void run_single(const Setup& S, ud_maps maps, const std::string& path, const std
     const int stride = 7 + counts[2];
     std::vector<float> pose(stride);
     check(ud_ligand_initial_pose(h, pose.data()), "ligand");
-    int lig = 0;
     float en[8];
     if (score_only || local_only) {
-        if (local_only) {
-            float e = 0;
-            int ev = 0;
-            check(ud_optimize(b, &lig, pose.data(), 1, stride, 0, 1000.0f, &e, &ev, nullptr), "optimize");
-        }
-        check(ud_score_terms(b, &lig, pose.data(), 1, stride, en, nullptr), "score");
+        if (local_only) local_optimize(maps, b, h, pose);
+        score_pose(S, b, pose, en);
         print_energies(std::cout, en);
         if (score_only) {
             std::ostringstream f;
@@ -598,6 +639,8 @@ int run(int argc, char** argv) {
     p.chains_per_block = 0;
     p.bfgs_cap = 0;
     p.use_graph = 1;
+    const bool no_refine = o.has("no_refine");
+    p.refine_step = no_refine ? 0 : (int)o.num("refine_step", 3);
     // ligands
     std::vector<std::string> ligand_names = o.list("ligand");
     std::vector<std::string> batch_names = o.list("gpu_batch");
@@ -680,6 +723,7 @@ int run(int argc, char** argv) {
               "maps");
     } else {
         maps = build_maps(S, o.str("receptor"));
+        S.receptor_scoring = !no_refine && S.sf != UD_SF_AD4;
     }
     if (o.has("write_maps")) check(ud_maps_write(maps, o.str("write_maps").c_str()), "write maps");
     if (!ligand_names.empty()) {
@@ -698,14 +742,9 @@ int run(int argc, char** argv) {
             check(ud_ligand_counts(L.h, counts), "ligand");
             std::vector<float> pose(7 + counts[2]);
             check(ud_ligand_initial_pose(L.h, pose.data()), "ligand");
-            int lig = 0;
             float en[8];
-            if (local_only) {
-                float e;
-                int ev;
-                check(ud_optimize(b, &lig, pose.data(), 1, (int)pose.size(), 0, 1000.0f, &e, &ev, nullptr), "optimize");
-            }
-            check(ud_score_terms(b, &lig, pose.data(), 1, (int)pose.size(), en, nullptr), "score");
+            if (local_only) local_optimize(maps, b, L.h, pose);
+            score_pose(S, b, pose, en);
             if (score_only)
                 sfile << get_filename(L.path) << " " << std::fixed << std::setprecision(3) << en[0] << "\n";
             if (S.verbosity > 0) print_energies(std::cout, en);

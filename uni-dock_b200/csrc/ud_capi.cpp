@@ -128,6 +128,11 @@ struct ud_maps_s {
     bool loaded = false;             // read from map files: no receptor to rebuild per-term maps from
     float box_center[3] = {0, 0, 0}; // box as given (written to map file headers)
     float box_spacing = 0;
+    // receptor atoms in box cells for scoring without the maps, built on first use
+    DevBuf<float> rc_atoms;
+    DevBuf<int> rc_start;
+    DeviceReceptorView rc{};
+    bool rc_built = false;
 };
 
 struct LigandPost {
@@ -182,6 +187,14 @@ struct ud_batch_s {
     PinnedBuf<float> hp_poses;
     PinnedBuf<ChainResult> hp_results;
     bool graph_results = false;
+    // modes of the last search: clustered (and refined) on the device
+    int mode_cap = 0;
+    bool refined = false;
+    DevBuf<float> d_cluster_scratch;
+    DevBuf<int> d_n_modes, d_mode_chain, d_mode_lig;
+    DevBuf<float> d_mode_pose, d_mode_e;
+    PinnedBuf<int> hp_n_modes, hp_mode_chain;
+    PinnedBuf<float> hp_mode_pose, hp_mode_e;
     // launch configuration picked by ud_autotune for this batch
     bool tuned = false;
     int tuned_chains_per_block = 4;
@@ -1313,28 +1326,6 @@ static float rmsd_ub(const std::vector<float>& a, const std::vector<float>& b) {
 }
 
 // add_to_output_container (unidock/src/lib/coords.cpp:44-68)
-static void add_to_container(std::vector<PoseResult>& out, const PoseResult& t, float min_rmsd, size_t max_size) {
-    if (!out.empty() && t.heavy_xyz.size() != out[0].heavy_xyz.size()) return;
-    const float eps = std::numeric_limits<float>::epsilon();
-    if (t.e < eps && t.e > -eps) return;
-    size_t best_i = out.size();
-    float best_r = std::numeric_limits<float>::max();
-    for (size_t i = 0; i < out.size(); ++i) {
-        float r = rmsd_ub(t.heavy_xyz, out[i].heavy_xyz);
-        if (i == 0 || r < best_r) {
-            best_i = i;
-            best_r = r;
-        }
-    }
-    if (best_i < out.size() && best_r < min_rmsd) {
-        if (t.e < out[best_i].e) out[best_i] = t;
-    } else {
-        if (out.size() < max_size) out.push_back(t);
-        else if (!out.empty() && t.e < out.back().e) out.back() = t;
-    }
-    std::stable_sort(out.begin(), out.end(), [](const PoseResult& x, const PoseResult& y) { return x.e < y.e; });
-}
-
 static std::vector<float> heavy_coords(const Ligand& L, const std::vector<float>& all) {
     std::vector<float> h;
     for (size_t i = 0; i < L.atoms.size(); ++i)
@@ -1379,42 +1370,159 @@ template <class F> static void parallel_for(int n, F&& body) {
     for (auto& t : ts) t.join();
 }
 
-// Clustering and rescoring of the chain results of every ligand
-// (monte_carlo.cu:2939-2942, vina.h:236-343 without explicit-receptor refinement).
-static void post_process(ud_batch b, cudaStream_t s) {
-    const int n_lig = (int)b->ligs.size();
-    const int E = b->exhaustiveness;
-    const ud_search_params& P = b->params;
-    b->post.assign(n_lig, LigandPost{});
-    std::vector<std::vector<PoseResult>> cont(n_lig);
-    parallel_for(n_lig, [&](int l) {
-        const Ligand& L = *b->ligs[l];
-        std::vector<float> xyz(3 * L.atoms.size());
-        std::vector<PoseResult> out;
-        for (int c = 0; c < E; ++c) {
-            const int slot = l * E + c;
-            PoseResult r;
-            const float* p = &b->h_poses[(size_t)slot * b->pose_stride];
-            r.pose.assign(p, p + 7 + L.n_torsions());
-            r.e = b->h_results[slot].e;
-            r.inter = b->h_results[slot].e_grid;   // rescoring values computed with the chain
-            r.intra = b->h_results[slot].e_intra;
-            ligand_coords(L, r.pose.data(), xyz.data());
-            r.heavy_xyz = heavy_coords(L, xyz);
-            add_to_container(out, r, P.min_rmsd, (size_t)std::max(1, P.num_modes));
+// Receptor atoms of the maps in box cells (DeviceReceptorView): the scoring
+// without maps that the reference keeps unless --no_refine (non_cache,
+// non_cache.cpp:23-30; its szv_grid lists, per cell, the receptor atoms within
+// the cutoff of the cell).  2 A cells over the box; atoms listed in receptor
+// order.
+static bool has_receptor(const ud_maps_s* m) { return !m->desc.ad4 && !m->loaded && !m->rec_xyzt.empty(); }
+
+static void ensure_receptor(ud_maps_s* m, cudaStream_t s) {
+    if (m->rc_built) return;
+    if (!has_receptor(m))
+        throw Error(UD_ERR_STATE, "receptor-atom scoring needs Vina / Vinardo maps built from a receptor");
+    const MapsDesc& d = m->desc;
+    const float cell = 2.0f;
+    DeviceReceptorView& R = m->rc;
+    for (int i = 0; i < 3; ++i) {
+        R.begin[i] = d.init[i];
+        R.end[i] = d.corner2[i];
+        R.n[i] = std::max(1, (int)std::ceil((R.end[i] - R.begin[i]) / cell));
+    }
+    R.inv_cell = 1.0f / cell;
+    // margin over the cutoff: a query point on a cell face must not miss an atom by rounding
+    const float cut = std::sqrt(m->cutoff2) + 1e-3f, cut2 = cut * cut;
+    const int n_rec = (int)(m->rec_xyzt.size() / 4);
+    const float* X = m->rec_xyzt.data();
+    auto box_d2 = [&](const float* p, const float* lo, const float* hi) {
+        float d2 = 0;
+        for (int k = 0; k < 3; ++k) {
+            const float t = p[k] < lo[k] ? lo[k] - p[k] : (p[k] > hi[k] ? p[k] - hi[k] : 0.0f);
+            d2 += t * t;
         }
-        std::vector<PoseResult> red;
-        for (auto& r : out) add_to_container(red, r, P.min_rmsd, out.size());
-        cont[l] = std::move(red);
+        return d2;
+    };
+    const int nx = R.n[0], ny = R.n[1], nz = R.n[2];
+    std::vector<std::vector<int>> lists((size_t)nx * ny * nz);
+    parallel_for(ny * nz, [&](int row) {
+        const int iy = row % ny, iz = row / ny;
+        const float lo[3] = {R.begin[0], R.begin[1] + iy * cell, R.begin[2] + iz * cell};
+        const float hi[3] = {R.begin[0] + nx * cell, lo[1] + cell, lo[2] + cell};
+        std::vector<int> cand;
+        for (int a = 0; a < n_rec; ++a)
+            if (box_d2(X + 4 * a, lo, hi) < cut2) cand.push_back(a);
+        for (int ix = 0; ix < nx; ++ix) {
+            const float clo[3] = {R.begin[0] + ix * cell, lo[1], lo[2]};
+            const float chi[3] = {clo[0] + cell, hi[1], hi[2]};
+            auto& L = lists[((size_t)iz * ny + iy) * nx + ix];
+            for (int a : cand)
+                if (box_d2(X + 4 * a, clo, chi) < cut2) L.push_back(a);
+        }
     });
+    std::vector<int> start(lists.size() + 1, 0);
+    for (size_t c = 0; c < lists.size(); ++c) start[c + 1] = start[c] + (int)lists[c].size();
+    std::vector<float> atoms(4 * (size_t)start.back());
+    for (size_t c = 0; c < lists.size(); ++c)
+        for (size_t k = 0; k < lists[c].size(); ++k)
+            std::memcpy(&atoms[4 * ((size_t)start[c] + k)], X + 4 * (size_t)lists[c][k], 4 * sizeof(float));
+    m->rc_atoms.upload(atoms.data(), atoms.size(), s);
+    m->rc_start.upload(start.data(), start.size(), s);
+    cuda_check(cudaStreamSynchronize(s), "receptor cells");
+    R.atoms = m->rc_atoms.p;
+    R.start = m->rc_start.p;
+    m->rc_built = true;
+}
+
+// Whether a search with these parameters refines its modes against the
+// receptor atoms (Vina / Vinardo with a receptor, refine_step > 0: the
+// reference's default, vina.h:251-272).
+static bool refines(const ud_batch b, const ud_search_params& P) {
+    return P.refine_step > 0 && has_receptor(b->maps);
+}
+
+// The device part after the search kernel: clustering of every ligand's
+// chains into modes, their refinement against the receptor atoms and final
+// scoring energies when `b->refined`, and the copies of the modes into
+// page-locked memory.  Enqueued on `s` (also inside a graph capture).
+static cudaError_t enqueue_modes(ud_batch b, cudaStream_t s) {
+    const int n_lig = (int)b->ligs.size(), cap = b->mode_cap;
+    const size_t n_slot = (size_t)n_lig * cap;
+    cudaError_t e = launch_cluster(b->view(), b->d_poses.p, b->pose_stride, b->d_results.p, n_lig, b->exhaustiveness,
+                                   cap, b->params.min_rmsd, b->d_cluster_scratch.p, b->d_n_modes.p,
+                                   b->d_mode_chain.p, b->d_mode_lig.p, b->d_mode_pose.p, s);
+    if (e == cudaSuccess && b->refined)
+        e = launch_receptor(kRecRefine, b->view(), tables_view(b->maps), b->maps->rc, b->d_mode_lig.p,
+                            b->d_mode_pose.p, b->pose_stride, (int)n_slot, b->params.refine_step, 0.0f, 1000.0f,
+                            nullptr, nullptr, 0, b->d_mode_e.p, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->hp_n_modes.p, b->d_n_modes.p, n_lig * sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->hp_mode_chain.p, b->d_mode_chain.p, n_slot * sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->hp_mode_pose.p, b->d_mode_pose.p, n_slot * b->pose_stride * sizeof(float),
+                            cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && b->refined)
+        e = cudaMemcpyAsync(b->hp_mode_e.p, b->d_mode_e.p, n_slot * 4 * sizeof(float), cudaMemcpyDeviceToHost, s);
+    return e;
+}
+
+// Buffers of enqueue_modes for the batch's current parameters.
+static void alloc_modes(ud_batch b, cudaStream_t s) {
+    const int n_lig = (int)b->ligs.size();
+    b->mode_cap = std::max(1, b->params.num_modes);
+    b->refined = refines(b, b->params);
+    if (b->refined) ensure_receptor(b->maps, s);
+    const size_t n_slot = (size_t)n_lig * b->mode_cap;
+    b->d_cluster_scratch.alloc(n_slot * 3 * std::max(1, b->max_atoms));
+    b->d_n_modes.alloc(n_lig);
+    b->d_mode_chain.alloc(n_slot);
+    b->d_mode_lig.alloc(n_slot);
+    b->d_mode_pose.alloc(n_slot * b->pose_stride);
+    b->d_mode_e.alloc(n_slot * 4);
+    b->hp_n_modes.alloc(n_lig);
+    b->hp_mode_chain.alloc(n_slot);
+    b->hp_mode_pose.alloc(n_slot * b->pose_stride);
+    b->hp_mode_e.alloc(n_slot * 4);
+}
+
+// Final scores of every ligand's modes (vina.h:232-343) from the device
+// clustering (and refinement): without refinement the modes keep their search
+// order and their grid / intramolecular energies at the authentic cap; with
+// it they are ordered by refined energy (max when outside the box), and the
+// inter energies come from the receptor atoms.  The unbound energy is the
+// intramolecular energy of the first mode.
+static void post_process(ud_batch b) {
+    const int n_lig = (int)b->ligs.size();
+    const int E = b->exhaustiveness, cap = b->mode_cap;
+    b->post.assign(n_lig, LigandPost{});
     const Scoring& sf = b->maps->sf;
     parallel_for(n_lig, [&](int l) {
-        auto& v = cont[l];
-        if (v.empty()) return;
         const Ligand& L = *b->ligs[l];
+        const int nm = b->hp_n_modes.p[l];
+        std::vector<PoseResult> v;
+        for (int k = 0; k < nm; ++k) {
+            const size_t o = (size_t)l * cap + k;
+            const int ch = b->hp_mode_chain.p[o];
+            const ChainResult& cr = b->h_results[(size_t)l * E + ch];
+            PoseResult r;
+            const float* p = b->hp_mode_pose.p + o * b->pose_stride;
+            r.pose.assign(p, p + 7 + L.n_torsions());
+            if (b->refined) {
+                const float* me = b->hp_mode_e.p + 4 * o;
+                r.e = me[3] > 0.5f ? me[0] : std::numeric_limits<float>::max();
+                r.inter = me[1];
+                r.intra = me[2];
+            } else {
+                r.e = cr.e;
+                r.inter = cr.e_grid;
+                r.intra = cr.e_intra;
+            }
+            v.push_back(r);
+        }
+        if (v.empty()) return;
+        if (b->refined)
+            std::stable_sort(v.begin(), v.end(), [](const PoseResult& x, const PoseResult& y) { return x.e < y.e; });
         auto ci = L.conf_indep_inputs();
-        // final scores (vina.h:241-300): grid + intramolecular energies at the
-        // authentic cap; the unbound energy is that of the best pose by search energy
         const float intramolecular = v[0].intra;
         for (size_t i = 0; i < v.size(); ++i) {
             const float inter = v[i].inter, intra = v[i].intra;
@@ -1439,7 +1547,8 @@ static void post_process(ud_batch b, cudaStream_t s) {
 }
 
 // Capture (or reuse) the per-batch sequence of the persistent search as a
-// CUDA graph: queue reset, search kernel, results into page-locked memory.
+// CUDA graph: queue reset, search kernel, results into page-locked memory,
+// clustering (and refinement) of the modes and their copies.
 // Captured on the batch's own stream (capture is not allowed on the legacy
 // default stream); the instantiated graph is then launched on any stream.
 // Reused while the launch parameters and buffers are unchanged.
@@ -1451,7 +1560,11 @@ static void search_graph(ud_batch b, const SearchParams& sp, int n_chain, int bl
       << sp.chains_per_block << ' ' << sp.bfgs_cap << ' ' << (const void*)b->d_poses.p << ' '
       << (const void*)b->d_results.p << ' ' << (const void*)b->d_queue.p << ' ' << (const void*)b->d_order.p << ' '
       << (const void*)b->hp_poses.p << ' ' << (const void*)b->hp_results.p << ' ' << (const void*)b->maps->maps.p
-      << ' ' << (const void*)b->maps->smooth.p;
+      << ' ' << (const void*)b->maps->smooth.p << ' ' << b->mode_cap << ' ' << b->refined << ' '
+      << b->params.refine_step << ' ' << b->params.min_rmsd << ' ' << (const void*)b->d_mode_pose.p << ' '
+      << (const void*)b->d_mode_e.p << ' ' << (const void*)b->d_cluster_scratch.p << ' '
+      << (const void*)b->hp_mode_pose.p << ' ' << (const void*)b->hp_mode_e.p << ' ' << (const void*)b->hp_n_modes.p
+      << ' ' << (const void*)b->hp_mode_chain.p << ' ' << (const void*)b->maps->rc.atoms;
     if (b->graph_exec && b->graph_key == k.str()) return;
     b->drop_graph();
     if (!b->capture_stream)
@@ -1468,6 +1581,7 @@ static void search_graph(ud_batch b, const SearchParams& sp, int n_chain, int bl
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(b->hp_results.p, b->d_results.p, (size_t)n_chain * sizeof(ChainResult),
                             cudaMemcpyDeviceToHost, cs);
+    if (e == cudaSuccess) e = enqueue_modes(b, cs);
     cudaGraph_t g = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(cs, &g);
     if (e != cudaSuccess || e2 != cudaSuccess) {
@@ -1479,9 +1593,11 @@ static void search_graph(ud_batch b, const SearchParams& sp, int n_chain, int bl
     b->graph_key = k.str();
 }
 
-// Launch the search kernels of the batch asynchronously on `s`.
+// Launch the search kernels of the batch asynchronously on `s`, followed by the
+// clustering (and refinement) of the modes unless `modes` is false.
 // `launch` false: only the set-up (buffers, ligand order, graph capture).
-static void search_launch(ud_batch b, const ud_search_params* params, cudaStream_t s, bool launch = true) {
+static void search_launch(ud_batch b, const ud_search_params* params, cudaStream_t s, bool launch = true,
+                          bool modes = true) {
         if (!b || !params) throw Error(UD_ERR_ARG, "null argument");
         const ud_search_params& P = *params;
         if (P.exhaustiveness < 1) throw Error(UD_ERR_ARG, "exhaustiveness must be >= 1");
@@ -1498,6 +1614,8 @@ static void search_launch(ud_batch b, const ud_search_params* params, cudaStream
         b->d_poses.alloc(n_chain * b->pose_stride);
         b->d_results.alloc(n_chain);
         b->d_queue.alloc(1);
+        if (P.num_modes < 1) throw Error(UD_ERR_ARG, "num_modes must be >= 1");
+        if (modes) alloc_modes(b, s);
         // most expensive ligands first (atoms x pairs as the cost proxy)
         std::vector<int> order(n_lig);
         std::iota(order.begin(), order.end(), 0);
@@ -1527,7 +1645,7 @@ static void search_launch(ud_batch b, const ud_search_params* params, cudaStream
             cuda_check(cudaEventCreate(&b->ev1), "event");
         }
         b->graph_results = false;
-        if (sp.persistent && P.use_graph) {
+        if (sp.persistent && P.use_graph && modes) {
             int per_sm = search_blocks_per_sm(b->view(), sp.chains_per_block);
             int blocks = std::max(1, std::min(per_sm * n_sm, (int)((n_chain + sp.chains_per_block - 1) /
                                                                     sp.chains_per_block)));
@@ -1560,10 +1678,11 @@ static void search_launch(ud_batch b, const ud_search_params* params, cudaStream
             }
         }
         cudaEventRecord(b->ev1, s);
+        if (modes) cuda_check(enqueue_modes(b, s), "modes");
         b->launched = true;
 }
 
-// Copy the chain results of the launched search to the host, cluster and rescore.
+// Copy the results of the launched search to the host and finish the modes.
 static void search_collect(ud_batch b, cudaStream_t s) {
         if (!b || !b->launched) throw Error(UD_ERR_STATE, "no search launched");
         const size_t n_chain = (size_t)b->ligs.size() * b->exhaustiveness;
@@ -1585,16 +1704,111 @@ static void search_collect(ud_batch b, cudaStream_t s) {
         cudaEventElapsedTime(&b->kernel_ms, b->ev0, b->ev1);
         b->evals = 0;
         for (auto& r : b->h_results) b->evals += r.evals;
-        post_process(b, s);
+        post_process(b);
         b->launched = false;
         b->searched = true;
+}
+
+// ---------------------------------------------------------------- receptor atoms
+
+static void check_receptor_poses(ud_batch b, const int* pose_ligand, const float* poses, int n_poses,
+                                 int pose_stride) {
+    check_poses(b, pose_ligand, n_poses, pose_stride);
+    if (!poses) throw Error(UD_ERR_ARG, "null buffer");
+    for (int i = 0; i < n_poses; ++i)
+        if (pose_ligand[i] < 0 || pose_ligand[i] >= (int)b->desc.size())
+            throw Error(UD_ERR_ARG, "pose_ligand out of range");
+}
+
+// Receptor-atom kernel of `mode` over host poses; out4 (4 floats per pose) read back.
+static void receptor_poses(ud_batch b, int mode, const int* pose_ligand, float* poses, int n_poses, int pose_stride,
+                           int refine_step, std::vector<float>& out4, cudaStream_t s) {
+    ensure_receptor(b->maps, s);
+    out4.assign(4 * (size_t)n_poses, 0.0f);
+    if (n_poses == 0) return;
+    b->d_pose_lig.upload(pose_ligand, n_poses, s);
+    b->d_pose.upload(poses, (size_t)n_poses * pose_stride, s);
+    b->d_score.alloc(4 * (size_t)n_poses);
+    cuda_check(launch_receptor(mode, b->view(), tables_view(b->maps), b->maps->rc, b->d_pose_lig.p, b->d_pose.p,
+                               pose_stride, n_poses, refine_step, 0.0f, 1000.0f, nullptr, nullptr, 0, b->d_score.p, s),
+               "receptor kernel");
+    if (mode == kRecRefine)
+        cuda_check(cudaMemcpyAsync(poses, b->d_pose.p, (size_t)n_poses * pose_stride * sizeof(float),
+                                   cudaMemcpyDeviceToHost, s),
+                   "D2H");
+    cuda_check(cudaMemcpyAsync(out4.data(), b->d_score.p, 4 * (size_t)n_poses * sizeof(float),
+                               cudaMemcpyDeviceToHost, s),
+               "D2H");
+    cuda_check(cudaStreamSynchronize(s), "receptor sync");
+}
+
+extern "C" int ud_score_grad_receptor(ud_batch b, const int* pose_ligand, const float* poses, int n_poses,
+                                      int pose_stride, float slope, float v, float* e_out, float* g_out, int g_stride,
+                                      void* stream) {
+    return guarded([&] {
+        check_receptor_poses(b, pose_ligand, poses, n_poses, pose_stride);
+        if (!e_out || !g_out || g_stride < 6 + b->max_tors) throw Error(UD_ERR_ARG, "invalid buffers");
+        cudaStream_t s = (cudaStream_t)stream;
+        ensure_receptor(b->maps, s);
+        if (n_poses == 0) return;
+        b->d_pose_lig.upload(pose_ligand, n_poses, s);
+        b->d_pose.upload(poses, (size_t)n_poses * pose_stride, s);
+        b->d_e.alloc(n_poses);
+        b->d_g.alloc((size_t)n_poses * g_stride);
+        cuda_check(cudaMemsetAsync(b->d_g.p, 0, (size_t)n_poses * g_stride * sizeof(float), s), "memset");
+        cuda_check(launch_receptor(kRecEnergyGrad, b->view(), tables_view(b->maps), b->maps->rc, b->d_pose_lig.p,
+                                   b->d_pose.p, pose_stride, n_poses, 0, slope, v, b->d_e.p, b->d_g.p, g_stride,
+                                   nullptr, s),
+                   "receptor kernel");
+        cuda_check(cudaMemcpyAsync(e_out, b->d_e.p, n_poses * sizeof(float), cudaMemcpyDeviceToHost, s), "D2H");
+        cuda_check(cudaMemcpyAsync(g_out, b->d_g.p, (size_t)n_poses * g_stride * sizeof(float),
+                                   cudaMemcpyDeviceToHost, s),
+                   "D2H");
+        cuda_check(cudaStreamSynchronize(s), "receptor sync");
+    });
+}
+
+extern "C" int ud_refine(ud_batch b, const int* pose_ligand, float* poses, int n_poses, int pose_stride,
+                         int refine_step, float* out4, void* stream) {
+    return guarded([&] {
+        check_receptor_poses(b, pose_ligand, poses, n_poses, pose_stride);
+        if (!out4 || refine_step < 0) throw Error(UD_ERR_ARG, "invalid refinement arguments");
+        std::vector<float> o;
+        receptor_poses(b, kRecRefine, pose_ligand, poses, n_poses, pose_stride, refine_step, o, (cudaStream_t)stream);
+        std::copy(o.begin(), o.end(), out4);
+    });
+}
+
+extern "C" int ud_score_terms_receptor(ud_batch b, const int* pose_ligand, const float* poses, int n_poses,
+                                       int pose_stride, float* out, void* stream) {
+    return guarded([&] {
+        check_receptor_poses(b, pose_ligand, poses, n_poses, pose_stride);
+        if (!out) throw Error(UD_ERR_ARG, "null buffer");
+        std::vector<float> p(poses, poses + (size_t)n_poses * pose_stride), o;
+        receptor_poses(b, kRecScore, pose_ligand, p.data(), n_poses, pose_stride, 0, o, (cudaStream_t)stream);
+        const Scoring& sf = b->maps->sf;
+        for (int i = 0; i < n_poses; ++i) {
+            const Ligand& L = *b->ligs[pose_ligand[i]];
+            const float inter = o[4 * i + 1], intra = o[4 * i + 2];
+            const float total = sf.conf_independent(inter + intra - intra, L.conf_indep_inputs()[0], (float)L.torsdof);
+            float* r = out + 8 * (size_t)i;
+            r[0] = total;
+            r[1] = inter;
+            r[2] = 0.0f;
+            r[3] = 0.0f;
+            r[4] = 0.0f;
+            r[5] = intra;
+            r[6] = total - inter;
+            r[7] = intra;
+        }
+    });
 }
 
 // ---------------------------------------------------------------- autotuner
 
 // Per-ligand best chain energy and device time of one search of `tb`.
 static float trial_search(ud_batch tb, const ud_search_params& tp, cudaStream_t s, std::vector<float>& best) {
-    search_launch(tb, &tp, s);
+    search_launch(tb, &tp, s, true, false);
     const size_t n_lig = tb->ligs.size(), E = (size_t)tp.exhaustiveness;
     std::vector<ChainResult> r(n_lig * E);
     cuda_check(cudaMemcpyAsync(r.data(), tb->d_results.p, r.size() * sizeof(ChainResult), cudaMemcpyDeviceToHost, s),

@@ -196,6 +196,15 @@ struct Maps {
     int e_slot, d_slot;    // AD4: electrostatic and desolvation maps
 };
 
+// Receptor atoms in box cells (the device form of DeviceReceptorView).
+struct Receptor {
+    const float4* atoms;
+    const int* start;
+    int n[3];
+    float begin[3], end[3];
+    float inv_cell;
+};
+
 // Shared-memory layout of one chain (float offsets).
 struct Layout {
     int x, xnew, xorig, tmp, cand, best;
@@ -380,35 +389,123 @@ __device__ __forceinline__ float grid_eval(const Maps& M, int slot, const float4
     return f + penalty;
 }
 
+// Interaction of one ligand atom (XS type t1, position pa) with the receptor
+// atoms, all lanes of the warp together (non_cache::eval_deriv / eval,
+// non_cache.cpp:35-110, 420-500): the position is clamped into the box at a
+// penalty of slope x the distance moved (derivative +-slope per axis), the
+// pair terms of the receptor atoms within the cutoff of the clamped position
+// are summed (lerped (e, dE/dr / r) table rows with kDeriv, the nearest-bin
+// `fast` table without), and the sum is curled at cap v.  Every lane returns
+// the same energy and gradient.
+template <bool kDeriv>
+__device__ __forceinline__ float receptor_term(const Receptor& R, const Tables& Tb, int t1, const float4 pa, float v,
+                                               float slope, float& gx, float& gy, float& gz) {
+    const int lane = threadIdx.x & 31;
+    float p[3] = {pa.x, pa.y, pa.z};
+    float pen = 0, od[3] = {0, 0, 0};
+    int ci[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        if (p[i] < R.begin[i]) {
+            pen += R.begin[i] - p[i];
+            p[i] = R.begin[i];
+            od[i] = -1;
+        } else if (p[i] > R.end[i]) {
+            pen += p[i] - R.end[i];
+            p[i] = R.end[i];
+            od[i] = 1;
+        }
+        int k = (int)((p[i] - R.begin[i]) * R.inv_cell);
+        ci[i] = k < 0 ? 0 : (k >= R.n[i] ? R.n[i] - 1 : k);
+    }
+    const int cell = (ci[2] * R.n[1] + ci[1]) * R.n[0] + ci[0];
+    const int j0 = __ldg(R.start + cell), j1 = __ldg(R.start + cell + 1);
+    float e = 0, dx = 0, dy = 0, dz = 0;
+    for (int j = j0 + lane; j < j1; j += 32) {
+        const float4 r = __ldg(R.atoms + j);
+        const float rx = p[0] - r.x, ry = p[1] - r.y, rz = p[2] - r.z;
+        const float r2 = rx * rx + ry * ry + rz * rz;
+        if (r2 < Tb.cutoff2) {
+            const int t2 = __float_as_int(r.w);
+            const int tp = t1 <= t2 ? t1 + t2 * (t2 + 1) / 2 : t2 + t1 * (t1 + 1) / 2;
+            const float rf = Tb.factor * r2;
+            const int i1 = (int)rf;
+            if constexpr (kDeriv) {
+                const float4 t = __ldg(Tb.smooth4 + (size_t)tp * Tb.n_bins + i1);
+                const float rem = rf - i1;
+                e += t.x + rem * (t.z - t.x);
+                const float dor = t.y + rem * (t.w - t.y);
+                dx += dor * rx;
+                dy += dor * ry;
+                dz += dor * rz;
+            } else {
+                e += __ldg(Tb.fast + (size_t)tp * Tb.n_bins + i1);
+            }
+        }
+    }
+    e = warp_sum(e);
+    if constexpr (kDeriv) {
+        dx = warp_sum(dx);
+        dy = warp_sum(dy);
+        dz = warp_sum(dz);
+    }
+    if (e > 0 && v < 0.1f * kMaxFl) {  // curl
+        const float tmp = (v < kEps) ? 0 : v / (v + e);
+        e *= tmp;
+        const float t2 = tmp * tmp;
+        dx *= t2; dy *= t2; dz *= t2;
+    }
+    gx = dx + od[0] * slope;
+    gy = dy + od[1] * slope;
+    gz = dz + od[2] * slope;
+    return e + pen * slope;
+}
+
 // Energy and gradient (change layout: position, torque, torsions) of `conf`.
 // Pair forces use the table's dE/dr / r column (precalculate.h:48-65) or, with
 // kExactPairs, the slope of the lerped energy itself (the exact derivative of
 // the computed energy, 2 factor (e_bin+1 - e_bin) per unit r^2).
-template <bool kExactPairs = false, bool kAD4 = false>
+// With kReceptor the receptor term comes from the receptor atoms (`Rc`,
+// out-of-box slope `rslope`) instead of the maps.
+template <bool kExactPairs = false, bool kAD4 = false, bool kReceptor = false>
 __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const Maps& M,
                                             const Tables& Tb, const float* conf, float* g,
-                                            float v_intra, float v_inter) {
+                                            float v_intra, float v_inter, const Receptor* Rc = nullptr,
+                                            float rslope = 0.0f) {
     kinematics(c, L, conf);
     const float4* xyz = reinterpret_cast<const float4*>(c.s + L.coords);
     float4* frc = reinterpret_cast<float4*>(c.s + L.forces);
     float e = 0;
     for (int k = c.lane; k < c.n_atoms; k += 32) frc[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     __syncwarp();
-    for (int k = c.lane; k < c.n_grid; k += 32) {
-        const uint32_t ga = __ldg(c.grid + k);
-        const int a = ga & 0xFF, slot = ga >> 8;
-        float gx, gy, gz;
-        const float4 pa = xyz[a];
-        e += grid_eval(M, slot, pa, v_inter, gx, gy, gz, true);
-        if constexpr (kAD4) {  // electrostatic map x q, desolvation map x |q| (ad4cache.cpp:227-269)
-            const float q = __ldg(c.q + a), aq = fabsf(q);
-            float hx, hy, hz;
-            e += q * grid_eval(M, M.e_slot, pa, v_inter, hx, hy, hz, true);
-            gx += q * hx; gy += q * hy; gz += q * hz;
-            e += aq * grid_eval(M, M.d_slot, pa, v_inter, hx, hy, hz, true);
-            gx += aq * hx; gy += aq * hy; gz += aq * hz;
+    if constexpr (kReceptor) {
+        for (int k = 0; k < c.n_grid; ++k) {  // one atom at a time, lanes over its receptor atoms
+            const int a = __ldg(c.grid + k) & 0xFF;
+            const int t1 = ((__ldg(&c.atoms[a].packed) >> 24) & 0xFF) - 1;
+            float gx, gy, gz;
+            const float ea = receptor_term<true>(*Rc, Tb, t1, xyz[a], v_inter, rslope, gx, gy, gz);
+            if (c.lane == 0) {
+                frc[a] = make_float4(gx, gy, gz, 0.0f);
+                e += ea;
+            }
         }
-        frc[a] = make_float4(gx, gy, gz, 0.0f);
+    } else {
+        for (int k = c.lane; k < c.n_grid; k += 32) {
+            const uint32_t ga = __ldg(c.grid + k);
+            const int a = ga & 0xFF, slot = ga >> 8;
+            float gx, gy, gz;
+            const float4 pa = xyz[a];
+            e += grid_eval(M, slot, pa, v_inter, gx, gy, gz, true);
+            if constexpr (kAD4) {  // electrostatic map x q, desolvation map x |q| (ad4cache.cpp:227-269)
+                const float q = __ldg(c.q + a), aq = fabsf(q);
+                float hx, hy, hz;
+                e += q * grid_eval(M, M.e_slot, pa, v_inter, hx, hy, hz, true);
+                gx += q * hx; gy += q * hy; gz += q * hz;
+                e += aq * grid_eval(M, M.d_slot, pa, v_inter, hx, hy, hz, true);
+                gx += aq * hx; gy += aq * hy; gz += aq * hz;
+            }
+            frc[a] = make_float4(gx, gy, gz, 0.0f);
+        }
     }
     __syncwarp();
     // Pairs in 32-slot groups made of kPairPasses lane ranges that are each a
@@ -545,26 +642,11 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
     return e;
 }
 
-// Scoring-path energy (no gradient): grid with curl cap v, intramolecular
-// pairs from the nearest-bin `fast` table (model.cpp:867-886, cache.cpp:84-120).
+// Intramolecular energy from the nearest-bin `fast` table at curl cap v
+// (model::evali, model.cpp:927-933), summed over the warp.
 template <bool kAD4 = false>
-__device__ __forceinline__ void eval_score(const Ctx& c, const Layout& L, const Maps& M,
-                                           const Tables& Tb, const float* conf, float v,
-                                           float& e_grid, float& e_intra) {
-    kinematics(c, L, conf);
-    const float4* xyz = reinterpret_cast<const float4*>(c.s + L.coords);
-    float eg = 0, ei = 0;
-    for (int k = c.lane; k < c.n_grid; k += 32) {
-        const uint32_t ga = __ldg(c.grid + k);
-        float gx, gy, gz;
-        const float4 pa = xyz[ga & 0xFF];
-        eg += grid_eval(M, ga >> 8, pa, v, gx, gy, gz, false);
-        if constexpr (kAD4) {
-            const float q = __ldg(c.q + (ga & 0xFF));
-            eg += q * grid_eval(M, M.e_slot, pa, v, gx, gy, gz, false);
-            eg += fabsf(q) * grid_eval(M, M.d_slot, pa, v, gx, gy, gz, false);
-        }
-    }
+__device__ __forceinline__ float intra_fast(const Ctx& c, const Tables& Tb, const float4* xyz, float v) {
+    float ei = 0;
     for (int k = c.lane; k < c.n_pairs; k += 32) {
         uint32_t pr = __ldg(c.pairs + k);
         if (pr == kPairPad) continue;
@@ -584,8 +666,31 @@ __device__ __forceinline__ void eval_score(const Ctx& c, const Layout& L, const 
             ei += t;
         }
     }
+    return warp_sum(ei);
+}
+
+// Scoring-path energy (no gradient): grid with curl cap v, intramolecular
+// pairs from the nearest-bin `fast` table (model.cpp:867-886, cache.cpp:84-120).
+template <bool kAD4 = false>
+__device__ __forceinline__ void eval_score(const Ctx& c, const Layout& L, const Maps& M,
+                                           const Tables& Tb, const float* conf, float v,
+                                           float& e_grid, float& e_intra) {
+    kinematics(c, L, conf);
+    const float4* xyz = reinterpret_cast<const float4*>(c.s + L.coords);
+    float eg = 0;
+    for (int k = c.lane; k < c.n_grid; k += 32) {
+        const uint32_t ga = __ldg(c.grid + k);
+        float gx, gy, gz;
+        const float4 pa = xyz[ga & 0xFF];
+        eg += grid_eval(M, ga >> 8, pa, v, gx, gy, gz, false);
+        if constexpr (kAD4) {
+            const float q = __ldg(c.q + (ga & 0xFF));
+            eg += q * grid_eval(M, M.e_slot, pa, v, gx, gy, gz, false);
+            eg += fabsf(q) * grid_eval(M, M.d_slot, pa, v, gx, gy, gz, false);
+        }
+    }
     e_grid = warp_sum(eg);
-    e_intra = warp_sum(ei);
+    e_intra = intra_fast<kAD4>(c, Tb, xyz, v);
 }
 
 // ---------------------------------------------------------------- BFGS pieces
@@ -1082,6 +1187,285 @@ __global__ void __launch_bounds__(128) score_kernel(
     }
 }
 
+// ---------------------------------------------------------------- receptor atoms
+// Scoring against the receptor atoms instead of the maps, as the reference
+// does after its search unless --no_refine (vina.h:232-300, vina.cpp:1168-1283).
+
+// non_cache::within (non_cache.cpp:408-418): the heavy atoms of the last
+// kinematics lie inside the box, with a margin of 1e-4.
+__device__ __forceinline__ bool heavy_within(const Ctx& c, const Layout& L, const Receptor& R) {
+    const float4* xyz = reinterpret_cast<const float4*>(c.s + L.coords);
+    const float m = 1e-4f;
+    bool ok = true;
+    for (int a = c.lane; a < c.n_atoms; a += 32) {
+        if (!((__ldg(&c.atoms[a].packed) >> 16) & 1)) continue;
+        const float4 x = xyz[a];
+        if (x.x < R.begin[0] - m || x.x > R.end[0] + m || x.y < R.begin[1] - m || x.y > R.end[1] + m ||
+            x.z < R.begin[2] - m || x.z > R.end[2] + m)
+            ok = false;
+    }
+    return __all_sync(kFull, ok);
+}
+
+// Scoring-path energies: inter = non_cache::eval at slope 1e6 and cap v
+// (non_cache.cpp:35-110), intra = model::evali at cap v.
+__device__ __forceinline__ void eval_score_receptor(const Ctx& c, const Layout& L, const Receptor& R,
+                                                    const Tables& Tb, const float* conf, float v, float& e_inter,
+                                                    float& e_intra) {
+    kinematics(c, L, conf);
+    const float4* xyz = reinterpret_cast<const float4*>(c.s + L.coords);
+    float ei = 0;
+    for (int k = 0; k < c.n_grid; ++k) {
+        const int a = __ldg(c.grid + k) & 0xFF;
+        const int t1 = ((__ldg(&c.atoms[a].packed) >> 24) & 0xFF) - 1;
+        float gx, gy, gz;
+        ei += receptor_term<false>(R, Tb, t1, xyz[a], v, 1e6f, gx, gy, gz);
+    }
+    e_inter = ei;
+    e_intra = intra_fast<false>(c, Tb, xyz, v);
+}
+
+// quasi_newton against the receptor atoms at out-of-box slope `slope`, curl
+// caps v, from the conformation at L.x (updated in place): the iterations and
+// line search of bfgs.h:63-146, as run_machine performs them.
+__device__ float bfgs_receptor(const Ctx& c, const Layout& L, const Tables& Tb, const Receptor& R, int steps, float v,
+                               float slope) {
+    const Maps M{};
+    const int n = 6 + c.T, cs = 7 + c.T;
+    float* x = c.s + L.x;
+    float* xnew = c.s + L.xnew;
+    float* xorig = c.s + L.xorig;
+    float* g = c.s + L.g;
+    float* gnew = c.s + L.gnew;
+    float* gorig = c.s + L.gorig;
+    float* p = c.s + L.p;
+    float* y = c.s + L.y;
+    float* H = c.s + L.h;
+    h_identity(c, H, n);
+    float f0 = eval_deriv<false, false, true>(c, L, M, Tb, x, g, v, v, &R, slope);
+    const float f_orig = f0;
+    copyw(c, gorig, g, n);
+    copyw(c, xorig, x, cs);
+    for (int iter = 0; iter < steps; ++iter) {
+        minus_hv(c, H, g, p, n);
+        const float pg = dotw(c, p, g, n);
+        float alpha = 1.0f, f1 = 0.0f;
+        for (int trial = 0;;) {
+            conf_increment(c, x, p, alpha, xnew);
+            f1 = eval_deriv<false, false, true>(c, L, M, Tb, xnew, gnew, v, v, &R, slope);
+            if (f1 - f0 < 0.0001f * alpha * pg) break;
+            alpha *= 0.5f;
+            if (++trial >= 10) break;
+        }
+        for (int i = c.lane; i < n; i += 32) y[i] = gnew[i] - g[i];
+        __syncwarp();
+        f0 = f1;
+        copyw(c, x, xnew, cs);
+        const float gg = dotw(c, g, g, n);
+        if (!(sqrtf(gg) >= 1e-5f)) break;
+        copyw(c, g, gnew, n);
+        if (iter == 0) {
+            const float yy = dotw(c, y, y, n);
+            if (fabsf(yy) > kEps) {
+                const float d = __fdividef(alpha * dotw(c, y, p, n), yy);
+                for (int i = c.lane; i < n; i += 32) H[i * n + i] = d;
+                __syncwarp();
+            }
+        }
+        h_update(c, H, p, y, c.s + L.mhy, alpha, n);
+    }
+    if (!(f0 <= f_orig)) {
+        f0 = f_orig;
+        copyw(c, x, xorig, cs);
+        copyw(c, g, gorig, n);
+    }
+    return f0;
+}
+
+// One warp per pose (pose_lig < 0: skipped); the modes of ReceptorMode.
+// Refinement follows vina.h:251-272: up to refine_step rounds of quasi_newton
+// (per-ligand (25 + atoms)/3 steps) at slopes 100, 1e4, 1e6, ..., stopping once
+// the heavy atoms are inside the box.
+template <int kMode>
+__global__ void __launch_bounds__(128) receptor_kernel(
+    const __grid_constant__ Batch B, const __grid_constant__ Tables Tb, const __grid_constant__ Receptor R,
+    const __grid_constant__ Layout L, const int* pose_lig, float* poses, int pose_stride, int n_poses,
+    int refine_step, float slope, float v, float* e_out, float* g_out, int g_stride, float4* out4) {
+    extern __shared__ __align__(16) float smem[];
+    const int warp = threadIdx.x >> 5;
+    const int pose = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (pose >= n_poses) return;
+    const int lig = pose_lig[pose];
+    if (lig < 0) return;
+    float* sw = smem + (size_t)warp * L.total;
+    const Ctx c = make_ctx(B, lig, sw);
+    float* x = sw + L.x;
+    const int cs = 7 + c.T;
+    for (int i = c.lane; i < cs; i += 32) x[i] = poses[(size_t)pose * pose_stride + i];
+    __syncwarp();
+    if constexpr (kMode == kRecEnergyGrad) {
+        const Maps M{};
+        float* g = sw + L.g;
+        const float e = eval_deriv<false, false, true>(c, L, M, Tb, x, g, v, v, &R, slope);
+        for (int i = c.lane; i < 6 + c.T; i += 32) g_out[(size_t)pose * g_stride + i] = g[i];
+        if (c.lane == 0) e_out[pose] = e;
+    } else {
+        float e_last = 0.0f;
+        if constexpr (kMode == kRecRefine) {
+            float sl = 100.0f;
+            for (int r = 0; r < refine_step; ++r) {
+                e_last = bfgs_receptor(c, L, Tb, R, c.local_steps, v, sl);
+                kinematics(c, L, x);
+                if (heavy_within(c, L, R)) break;
+                sl *= 100.0f;
+            }
+            for (int i = c.lane; i < cs; i += 32) poses[(size_t)pose * pose_stride + i] = x[i];
+        }
+        float ei, ea;
+        eval_score_receptor(c, L, R, Tb, x, v, ei, ea);
+        const bool within = heavy_within(c, L, R);
+        if (c.lane == 0) out4[pose] = make_float4(e_last, ei, ea, within ? 1.0f : 0.0f);
+    }
+}
+
+// ---------------------------------------------------------------- clustering
+// Heavy-atom RMSD (rmsd_upper_bound, coords.cpp:28-35) between the current
+// kinematics (or scratch slot `a`) and scratch slot `b`.
+__device__ __forceinline__ float heavy_rmsd(const Ctx& c, const float4* xyz, const float* a, const float* b,
+                                            int n_heavy) {
+    float sum = 0;
+    for (int i = c.lane; i < c.n_atoms; i += 32) {
+        if (!((__ldg(&c.atoms[i].packed) >> 16) & 1)) continue;
+        float dx, dy, dz;
+        if (a) {
+            dx = a[3 * i] - b[3 * i]; dy = a[3 * i + 1] - b[3 * i + 1]; dz = a[3 * i + 2] - b[3 * i + 2];
+        } else {
+            const float4 p = xyz[i];
+            dx = p.x - b[3 * i]; dy = p.y - b[3 * i + 1]; dz = p.z - b[3 * i + 2];
+        }
+        sum += dx * dx + dy * dy + dz * dz;
+    }
+    return sqrtf(warp_sum(sum) / (float)n_heavy);
+}
+
+// Stable insertion sort of slot ids by energy (lane 0).
+__device__ __forceinline__ void sort_slots(int* ids, const float* e, int n) {
+    if ((threadIdx.x & 31) == 0)
+        for (int i = 1; i < n; ++i) {
+            const int v = ids[i];
+            int j = i - 1;
+            while (j >= 0 && e[ids[j]] > e[v]) {
+                ids[j + 1] = ids[j];
+                --j;
+            }
+            ids[j + 1] = v;
+        }
+    __syncwarp();
+}
+
+// The modes of one ligand from its chains (warp per ligand): each chain's best
+// pose goes through add_to_output_container (coords.cpp:44-68) in chain order
+// with at most `cap` modes, then the modes through Vina::remove_redundant
+// (vina.cpp:1465-1470).  The coordinates of the modes are kept in `scratch`.
+__global__ void __launch_bounds__(128) cluster_kernel(
+    const __grid_constant__ Batch B, const __grid_constant__ Layout L, const float* poses, int pose_stride,
+    const ChainResult* results, int n_lig, int E, int cap, float min_rmsd, float* scratch, int max_atoms,
+    int* n_modes, int* mode_chain, int* mode_lig, float* mode_pose) {
+    extern __shared__ __align__(16) float smem[];
+    const int warp = threadIdx.x >> 5;
+    const int lig = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (lig >= n_lig) return;
+    const int cap4 = pad4(cap);
+    float* sw = smem + (size_t)warp * (L.total + 4 * cap4);
+    int* ord = reinterpret_cast<int*>(sw + L.total);
+    float* ent_e = sw + L.total + cap4;
+    int* ent_chain = reinterpret_cast<int*>(sw + L.total + 2 * cap4);
+    int* keep = reinterpret_cast<int*>(sw + L.total + 3 * cap4);
+    const Ctx c = make_ctx(B, lig, sw);
+    const int n_heavy = __ldg(&B.ligs[lig].n_heavy);
+    const float4* xyz = reinterpret_cast<const float4*>(c.s + L.coords);
+    float* S = scratch + (size_t)lig * cap * 3 * max_atoms;
+    const int cs = 7 + c.T;
+    const float eps = 1.1920929e-7f;  // FLT_EPSILON
+    int n = 0;
+    for (int ch = 0; ch < E; ++ch) {
+        const size_t item = (size_t)lig * E + ch;
+        const float e = __ldg(&results[item].e);
+        if (e < eps && e > -eps) continue;  // an energy of exactly 0 marks a failed chain
+        float* x = c.s + L.x;
+        for (int i = c.lane; i < cs; i += 32) x[i] = __ldg(poses + item * pose_stride + i);
+        __syncwarp();
+        kinematics(c, L, x);
+        int best = n;
+        float best_r = kMaxFl;
+        for (int k = 0; k < n; ++k) {
+            const float r = heavy_rmsd(c, xyz, nullptr, S + (size_t)ord[k] * 3 * max_atoms, n_heavy);
+            if (k == 0 || r < best_r) {
+                best = k;
+                best_r = r;
+            }
+        }
+        int slot = -1;
+        if (best < n && best_r < min_rmsd) {
+            if (e < ent_e[ord[best]]) slot = ord[best];
+        } else if (n < cap) {
+            slot = n;
+            if (c.lane == 0) ord[n] = n;
+            ++n;
+        } else if (e < ent_e[ord[n - 1]]) {
+            slot = ord[n - 1];
+        }
+        if (slot >= 0) {
+            float* Sd = S + (size_t)slot * 3 * max_atoms;
+            for (int a = c.lane; a < c.n_atoms; a += 32) {
+                const float4 p = xyz[a];
+                Sd[3 * a] = p.x; Sd[3 * a + 1] = p.y; Sd[3 * a + 2] = p.z;
+            }
+            if (c.lane == 0) {
+                ent_e[slot] = e;
+                ent_chain[slot] = ch;
+            }
+            __syncwarp();
+            sort_slots(ord, ent_e, n);
+        }
+    }
+    // remove_redundant: the modes in energy order into a fresh container
+    int m = 0;
+    for (int k = 0; k < n; ++k) {
+        const int sl = ord[k];
+        const float* Sa = S + (size_t)sl * 3 * max_atoms;
+        int best = m;
+        float best_r = kMaxFl;
+        for (int j = 0; j < m; ++j) {
+            const float r = heavy_rmsd(c, xyz, Sa, S + (size_t)keep[j] * 3 * max_atoms, n_heavy);
+            if (j == 0 || r < best_r) {
+                best = j;
+                best_r = r;
+            }
+        }
+        if (best < m && best_r < min_rmsd) {
+            if (ent_e[sl] < ent_e[keep[best]] && c.lane == 0) keep[best] = sl;
+        } else {
+            if (c.lane == 0) keep[m] = sl;
+            ++m;
+        }
+        __syncwarp();
+        sort_slots(keep, ent_e, m);
+    }
+    if (c.lane == 0) n_modes[lig] = m;
+    for (int k = 0; k < cap; ++k) {
+        const size_t o = (size_t)lig * cap + k;
+        const int ch = k < m ? ent_chain[keep[k]] : -1;
+        if (c.lane == 0) {
+            mode_chain[o] = ch;
+            mode_lig[o] = k < m ? lig : -1;
+        }
+        if (k < m)
+            for (int i = c.lane; i < cs; i += 32)
+                mode_pose[o * pose_stride + i] = __ldg(poses + ((size_t)lig * E + ch) * pose_stride + i);
+    }
+}
+
 // ---------------------------------------------------------------- adjoint
 // Per-term data of the scoring function for weight gradients: the maps and the
 // lerp rows of each unweighted term, laid out like the weighted ones.  Maps
@@ -1566,6 +1950,19 @@ static dev::Batch to_batch(const DeviceBatchView& b) {
     return B;
 }
 
+static dev::Receptor to_receptor(const DeviceReceptorView& r) {
+    dev::Receptor R;
+    R.atoms = reinterpret_cast<const float4*>(r.atoms);
+    R.start = r.start;
+    for (int i = 0; i < 3; ++i) {
+        R.n[i] = r.n[i];
+        R.begin[i] = r.begin[i];
+        R.end[i] = r.end[i];
+    }
+    R.inv_cell = r.inv_cell;
+    return R;
+}
+
 int engine_chain_smem_bytes(int max_atoms, int max_torsions) {
     return dev::make_layout(max_atoms, max_torsions).total * (int)sizeof(float);
 }
@@ -1695,6 +2092,54 @@ cudaError_t launch_optimize(const DeviceBatchView& b, const DeviceMapsView& m,
     kern<<<grid, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t), P, L,
                                                              pose_lig, poses, pose_stride, n_poses,
                                                              max_steps, v, e_out, evals_out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cluster(const DeviceBatchView& b, const float* poses, int pose_stride, const ChainResult* results,
+                           int n_ligands, int exhaustiveness, int cap, float min_rmsd, float* scratch, int* n_modes,
+                           int* mode_chain, int* mode_lig, float* mode_pose, cudaStream_t stream) {
+    if (n_ligands <= 0) return cudaSuccess;
+    if (cap < 1) return cudaErrorInvalidValue;
+    dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
+    const int warps = 4;
+    size_t smem = (size_t)warps * (L.total + 4 * dev::pad4(cap)) * sizeof(float);
+    cudaError_t e = smem_attr((const void*)dev::cluster_kernel, smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid((n_ligands + warps - 1) / warps);
+    dev::cluster_kernel<<<grid, warps * 32, smem, stream>>>(to_batch(b), L, poses, pose_stride, results, n_ligands,
+                                                            exhaustiveness, cap, min_rmsd, scratch, b.max_atoms,
+                                                            n_modes, mode_chain, mode_lig, mode_pose);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_receptor(int mode, const DeviceBatchView& b, const DeviceTablesView& t,
+                            const DeviceReceptorView& r, const int* pose_lig, float* poses, int pose_stride,
+                            int n_poses, int refine_step, float slope, float v, float* e_out, float* g_out,
+                            int g_stride, float* out4, cudaStream_t stream) {
+    if (n_poses <= 0) return cudaSuccess;
+    if (b.ad4) return cudaErrorInvalidValue;  // receptor-atom scoring is for Vina / Vinardo maps
+    dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
+    const int warps = 4;
+    size_t smem = (size_t)warps * L.total * sizeof(float);
+    const void* fn = mode == kRecEnergyGrad ? (const void*)dev::receptor_kernel<kRecEnergyGrad>
+                     : mode == kRecRefine   ? (const void*)dev::receptor_kernel<kRecRefine>
+                                            : (const void*)dev::receptor_kernel<kRecScore>;
+    cudaError_t e = smem_attr(fn, smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid((n_poses + warps - 1) / warps);
+    const dev::Batch B = to_batch(b);
+    const dev::Tables T = to_tables(t);
+    const dev::Receptor R = to_receptor(r);
+    float4* o4 = reinterpret_cast<float4*>(out4);
+    if (mode == kRecEnergyGrad)
+        dev::receptor_kernel<kRecEnergyGrad><<<grid, warps * 32, smem, stream>>>(
+            B, T, R, L, pose_lig, poses, pose_stride, n_poses, refine_step, slope, v, e_out, g_out, g_stride, o4);
+    else if (mode == kRecRefine)
+        dev::receptor_kernel<kRecRefine><<<grid, warps * 32, smem, stream>>>(
+            B, T, R, L, pose_lig, poses, pose_stride, n_poses, refine_step, slope, v, e_out, g_out, g_stride, o4);
+    else
+        dev::receptor_kernel<kRecScore><<<grid, warps * 32, smem, stream>>>(
+            B, T, R, L, pose_lig, poses, pose_stride, n_poses, refine_step, slope, v, e_out, g_out, g_stride, o4);
     return cudaGetLastError();
 }
 

@@ -151,6 +151,26 @@ struct DeviceTermsView {
     long long row_block;   // float4 per term in `rows`
 };
 
+// Receptor atoms for scoring without maps (the reference's non_cache, used to
+// refine and rescore poses): a uniform grid of cubic cells over the box; cell c
+// lists, in receptor order, every typed receptor atom within the cutoff of some
+// point of the cell, as (x, y, z, XS type as int bits).  Positions are clamped
+// into the box before the lookup, so every query lands in a cell.
+struct DeviceReceptorView {
+    const float* atoms;    // float4 per entry, grouped by cell
+    const int* start;      // [cells + 1] entry offsets
+    int n[3];              // cells per axis
+    float begin[3], end[3];// the box (grid_dims begin / end)
+    float inv_cell;        // 1 / cell edge
+};
+
+// Modes of the receptor-atom kernel.
+enum ReceptorMode : int {
+    kRecEnergyGrad = 0,    // energy and gradient at fixed poses (model::eval_deriv with non_cache)
+    kRecRefine = 1,        // refinement rounds, then the final scoring energies
+    kRecScore = 2          // scoring energies only (non_cache::eval, model::evali)
+};
+
 // ---------------------------------------------------------------- launchers (ud_engine.cu)
 cudaError_t launch_maps(const float* rec_xyzt, int n_rec, const float* fastT, int n_bins, int n_slots,
                         int n_slots_pad, float factor, float cutoff2, const MapsDesc& d, float* out,
@@ -184,5 +204,21 @@ cudaError_t launch_search_noalloc(const DeviceBatchView& b, const DeviceMapsView
                                   float* poses, int pose_stride, float* e_out, int* evals_out,
                                   cudaStream_t stream);
 int engine_chain_smem_bytes(int max_atoms, int max_torsions);
+// Per-ligand clustering of the chain results (warp per ligand) into at most
+// `cap` modes: n_modes[lig], and per mode slot lig * cap + k its chain, its
+// ligand (-1 for an unused slot) and a copy of the chain's pose.
+// scratch: n_ligands * cap * 3 * max_atoms floats.
+cudaError_t launch_cluster(const DeviceBatchView& b, const float* poses, int pose_stride, const ChainResult* results,
+                           int n_ligands, int exhaustiveness, int cap, float min_rmsd, float* scratch, int* n_modes,
+                           int* mode_chain, int* mode_lig, float* mode_pose, cudaStream_t stream);
+// Receptor-atom scoring of poses (one warp per pose, pose_lig < 0 skipped):
+//   kRecEnergyGrad: e_out[i] and g_out (6 + T per pose, stride g_stride) at slope / cap v;
+//   kRecRefine:     refinement rounds (slope 100 * 100^p, curl cap v) updating poses in place,
+//                   out4[i] = (last BFGS energy, inter at slope 1e6, intra, inside box 1/0);
+//   kRecScore:      out4[i] = (0, inter at slope 1e6, intra, inside box 1/0), caps v.
+cudaError_t launch_receptor(int mode, const DeviceBatchView& b, const DeviceTablesView& t,
+                            const DeviceReceptorView& r, const int* pose_lig, float* poses, int pose_stride,
+                            int n_poses, int refine_step, float slope, float v, float* e_out, float* g_out,
+                            int g_stride, float* out4, cudaStream_t stream);
 
 }  // namespace ud

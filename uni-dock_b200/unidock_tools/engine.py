@@ -52,6 +52,7 @@ class SearchParams(C.Structure):
         ("chains_per_block", C.c_int),
         ("bfgs_cap", C.c_int),
         ("use_graph", C.c_int),
+        ("refine_step", C.c_int),
     ]
 
 
@@ -76,6 +77,10 @@ def lib():
         "ud_maps_destroy": ([vp], C.c_int),
         "ud_ligand_parse": ([C.c_char_p, C.c_size_t, C.POINTER(vp)], C.c_int),
         "ud_ligand_parse_sdf": ([C.c_char_p, C.c_size_t, C.c_int, C.POINTER(vp)], C.c_int),
+        "ud_score_grad_receptor": ([vp, ip, fp, C.c_int, C.c_int, C.c_float, C.c_float, fp, fp, C.c_int, vp],
+                                   C.c_int),
+        "ud_refine": ([vp, ip, fp, C.c_int, C.c_int, C.c_int, fp, vp], C.c_int),
+        "ud_score_terms_receptor": ([vp, ip, fp, C.c_int, C.c_int, fp, vp], C.c_int),
         "ud_ligand_write": ([vp, fp, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
         "ud_ligand_counts": ([vp, ip], C.c_int),
         "ud_ligand_export": ([vp, fp, fp, ip, ip, ip, fp, ip, ip, ip, ip, fp, ip, ip], C.c_int),
@@ -407,6 +412,37 @@ class Batch:
                                              C.c_void_p(dw_ptr) if dw_ptr else None, dw_stride,
                                              C.c_void_p(stream) if stream else None))
 
+    # ---- receptor atoms (the reference's non_cache)
+    def score_grad_receptor(self, pose_ligand, poses, slope=1e6, v=1000.0):
+        """Energy and gradient against the receptor atoms (ud_score_grad_receptor)."""
+        pose_ligand = np.ascontiguousarray(pose_ligand, np.int32)
+        poses = np.ascontiguousarray(poses, np.float32)
+        n, stride = poses.shape
+        gs = 6 + self.max_torsions
+        e = np.zeros(n, np.float32)
+        g = np.zeros((n, gs), np.float32)
+        _check(lib().ud_score_grad_receptor(self.h, _i(pose_ligand), _f(poses), n, stride, float(slope), float(v),
+                                            _f(e), _f(g), gs, None))
+        return e, g
+
+    def refine(self, pose_ligand, poses, refine_step=3):
+        """Refined poses and (last BFGS energy, inter, intra, inside box) per pose (ud_refine)."""
+        pose_ligand = np.ascontiguousarray(pose_ligand, np.int32)
+        poses = np.array(poses, np.float32, copy=True, order="C")
+        n, stride = poses.shape
+        out = np.zeros((n, 4), np.float32)
+        _check(lib().ud_refine(self.h, _i(pose_ligand), _f(poses), n, stride, int(refine_step), _f(out), None))
+        return poses, out
+
+    def score_terms_receptor(self, pose_ligand, poses):
+        """--score_only energy vector with receptor atoms (ud_score_terms_receptor)."""
+        pose_ligand = np.ascontiguousarray(pose_ligand, np.int32)
+        poses = np.ascontiguousarray(poses, np.float32)
+        n, stride = poses.shape
+        out = np.zeros((n, 8), np.float32)
+        _check(lib().ud_score_terms_receptor(self.h, _i(pose_ligand), _f(poses), n, stride, _f(out), None))
+        return out
+
     def score(self, pose_ligand, poses, v=1000.0):
         pose_ligand = np.ascontiguousarray(pose_ligand, np.int32)
         poses = np.ascontiguousarray(poses, np.float32)
@@ -417,18 +453,22 @@ class Batch:
 
     # ---- search
     def search(self, exhaustiveness=8, max_step=0, num_modes=9, min_rmsd=1.0, energy_range=3.0, seed=0,
-               form=1, chains_per_block=0, bfgs_cap=0, use_graph=0):
+               form=1, chains_per_block=0, bfgs_cap=0, use_graph=0, refine_step=0):
+        """Search, cluster and score (ud_search).  refine_step > 0 refines the
+        modes against the receptor atoms, as the reference CLI does by default
+        (refine_step 3); 0 keeps the grid energies (--no_refine)."""
         p = SearchParams(exhaustiveness, max_step, num_modes, min_rmsd, energy_range, seed, form,
-                         chains_per_block, bfgs_cap, use_graph)
+                         chains_per_block, bfgs_cap, use_graph, refine_step)
         _check(lib().ud_search(self.h, C.byref(p), None))
         self.exhaustiveness = exhaustiveness
 
     def search_launch(self, exhaustiveness=8, max_step=0, num_modes=9, min_rmsd=1.0, energy_range=3.0, seed=0,
-                      form=1, chains_per_block=0, bfgs_cap=0, use_graph=0, stream=None):
-        """Enqueue the search kernels only (device-resident inputs, asynchronous
-        on `stream`, a raw cudaStream_t or None for the default stream)."""
+                      form=1, chains_per_block=0, bfgs_cap=0, use_graph=0, stream=None, refine_step=0):
+        """Enqueue the device part only (search, clustering, refinement;
+        device-resident inputs, asynchronous on `stream`, a raw cudaStream_t or
+        None for the default stream)."""
         self._p = SearchParams(exhaustiveness, max_step, num_modes, min_rmsd, energy_range, seed, form,
-                               chains_per_block, bfgs_cap, use_graph)
+                               chains_per_block, bfgs_cap, use_graph, refine_step)
         _check(lib().ud_search_launch(self.h, C.byref(self._p), C.c_void_p(stream) if stream else None))
         self.exhaustiveness = exhaustiveness
 
@@ -453,14 +493,14 @@ class Batch:
         return r.as_dict()
 
     def search_prepare(self, exhaustiveness=8, max_step=0, num_modes=9, min_rmsd=1.0, energy_range=3.0, seed=0,
-                       form=1, chains_per_block=0, bfgs_cap=0, use_graph=0, stream=None):
+                       form=1, chains_per_block=0, bfgs_cap=0, use_graph=0, stream=None, refine_step=0):
         """Set up a search (buffers, order, graph) without launching it (ud_search_prepare)."""
         p = SearchParams(exhaustiveness, max_step, num_modes, min_rmsd, energy_range, seed, form,
-                         chains_per_block, bfgs_cap, use_graph)
+                         chains_per_block, bfgs_cap, use_graph, refine_step)
         _check(lib().ud_search_prepare(self.h, C.byref(p), C.c_void_p(stream) if stream else None))
 
     def search_collect(self, stream=None):
-        """Wait for the launched search, then cluster, rescore and keep the modes."""
+        """Wait for the launched search, then finish and keep the modes."""
         _check(lib().ud_search_collect(self.h, C.c_void_p(stream) if stream else None))
 
     def optimize(self, pose_ligand, poses, v=1000.0, max_steps=0):
