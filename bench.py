@@ -51,6 +51,8 @@ def parse_args():
     ap.add_argument("--cpu-sample", type=int, default=16, help="ligands timed on the reference CPU path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chains-per-block", type=int, default=0)
+    ap.add_argument("--refine-step", type=int, default=3,
+                    help="rounds of refinement against the receptor atoms per mode (0: grid energies only)")
     ap.add_argument("--adjoint-poses", type=int, default=ADJOINT_POSES,
                     help="fixed poses of the adjoint leg (0 = skip)")
     ap.add_argument("--workload", default="screen-fast",
@@ -174,8 +176,10 @@ def run_ours(args, rank, world):
         return [glob[i] for i in shard(len(glob), rank, world, cost)]
 
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    # refine_step 3: the modes are refined and rescored against the receptor
+    # atoms, as the reference's CLI does by default
     P = dict(exhaustiveness=EXHAUSTIVENESS, max_step=MAX_STEP, num_modes=9, min_rmsd=1.0, seed=42, form=1,
-             chains_per_block=args.chains_per_block, use_graph=1)
+             chains_per_block=args.chains_per_block, use_graph=1, refine_step=args.refine_step)
 
     # ---- device-resident form: topology uploaded and the search set up (result
     # buffers, ligand order, captured graph) before the timed region
@@ -232,19 +236,30 @@ def run_ours(args, rank, world):
 
     # ---- end-to-end through the public API with host buffers: PDBQT text ->
     # parallel parse -> topology upload -> search (graph: queue reset, kernel,
-    # result copies) -> clustering / final scores -> output text.  Consecutive
+    # clustering and refinement of the modes, result copies) -> final scores ->
+    # output text.  Consecutive
     # batches alternate between two streams, as the CLI runs a screen: the host
     # work of one batch overlaps the search of the next.  Wall-clock time of
     # the whole pipelined loop, device synchronised at both ends.
+    # Two batch handles, one per stream, are reused (ud_batch_reset): once they
+    # have held the largest batch, nothing is allocated or freed (a device
+    # free would wait for the search running on the other stream).
     streams = [torch.cuda.Stream(), torch.cuda.Stream()]
     h2d = d2h = 0
-    for s in range(args.warmup):  # warm the pipeline's code paths
+    pool = []
+    for s in range(args.warmup):  # warm the pipeline's code paths and the two handles
         ligs = engine.parse_ligands(batch_texts(s))
-        bb = engine.Batch(maps, ligs)
-        bb.search_launch(**P, stream=streams[0].cuda_stream)
-        bb.search_collect(stream=streams[0].cuda_stream)
+        st = streams[s % 2].cuda_stream
+        if len(pool) < 2:
+            pool.append(engine.Batch(maps, ligs))
+        else:
+            pool[s % 2].reset(ligs, stream=st)
+        bb = pool[s % 2]
+        bb.search_launch(**P, stream=st)
+        bb.search_collect(stream=st)
         [bb.write(i) for i in range(len(ligs))]
-        del bb, ligs
+    while len(pool) < 2:
+        pool.append(engine.Batch(maps, engine.parse_ligands(batch_texts(0))))
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
@@ -253,7 +268,8 @@ def run_ours(args, rank, world):
     for k, s in enumerate(range(args.warmup, steps_total)):
         st = streams[k % 2].cuda_stream
         ligs = engine.parse_ligands(batch_texts(s))
-        bb = engine.Batch(maps, ligs)
+        bb = pool[k % 2]
+        bb.reset(ligs, stream=st)
         bb.search_launch(**P, stream=st)
         if k == 0:
             n_atoms = sum(L.n_atoms for L in ligs)
@@ -261,7 +277,9 @@ def run_ours(args, rank, world):
             n_pairs = sum(L.n_pairs for L in ligs)
             h2d = 16 * n_atoms + 40 * n_nodes + 4 * n_pairs + 48 * len(ligs) + 4 * len(ligs)
             stride = 7 + bb.max_torsions
-            d2h = len(ligs) * EXHAUSTIVENESS * (4 * stride + 24)
+            # chain results, then per ligand the mode count and nine mode slots
+            # (chain, pose, refined energies)
+            d2h = len(ligs) * EXHAUSTIVENESS * (4 * stride + 24) + len(ligs) * (4 + 9 * (4 + 4 * stride + 16))
         if pending is not None:
             pb, pligs, pst = pending
             pb.search_collect(stream=pst)
@@ -272,7 +290,7 @@ def run_ours(args, rank, world):
     outs = [pb.write(i) for i in range(len(pligs))]
     torch.cuda.synchronize()
     e2e_t = time.perf_counter() - t_e2e0
-    del pending, pb, pligs, bb, ligs
+    del pending, pb, pligs, bb, ligs, pool
     if world > 1:
         tt = torch.tensor([e2e_t], device="cuda")
         torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
@@ -315,6 +333,7 @@ def run_ours(args, rank, world):
                                    "max_step 20), 4096 ligands U{12..48} heavy / U{0..10} torsions, "
                                    "3000-atom receptor, 22.5 A box at 0.375 A (61^3)",
                        "ligands_per_step": B * world, "exhaustiveness": EXHAUSTIVENESS, "max_step": MAX_STEP,
+                       "refine_step": args.refine_step,
                        "form": "batched persistent", "l2": "flushed between timed steps (256 MB write)",
                        "parallelism": f"ligand shards x{world}" if world > 1 else "1 GPU"},
             "plain_form_ligands_per_s": None if plain is None else round(plain, 3),
@@ -333,10 +352,12 @@ def run_ours(args, rank, world):
                          "ms_per_launch": round(ms_launch, 3)},
             "e2e": {"value": round(e2e_value, 3), "unit": "ligands/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h),
-                    "path": "PDBQT text -> parse (all host threads) -> upload -> graph search -> clustering "
-                            "and final scores -> output text; batches pipelined on two streams, wall clock"},
+                    "path": "PDBQT text -> parse (all host threads) -> upload into a reused batch handle -> "
+                            "graph (search kernel, clustering and refinement of the modes on the device, result "
+                            "copies) -> final scores -> output text; batches pipelined on two streams, wall clock"},
             "clocks": clk,
-            "gpu_launches": args.steps * 1,
+            # per step: the search kernel, the clustering kernel and (refine_step > 0) the refinement kernel
+            "gpu_launches": args.steps * (3 if args.refine_step > 0 else 2),
             "adjoint": adjoint,
         }
     if world > 1:
@@ -409,7 +430,8 @@ def run_uneven(args, sf_name):
     steps_total = args.warmup + args.steps
     texts = [l.to_pdbqt() for l in synth.ligand_set(per_step * steps_total, seed=8192, dist="lognormal",
                                                       with_charges=(sf_name == "ad4"))]
-    P = dict(exhaustiveness=512, max_step=40, seed=42, form=1, use_graph=1, chains_per_block=0, bfgs_cap=-1)
+    P = dict(exhaustiveness=512, max_step=40, seed=42, form=1, use_graph=1, chains_per_block=0, bfgs_cap=-1,
+             refine_step=args.refine_step)
     batches, tunes = [], []
     for s in range(steps_total):
         ligs = engine.parse_ligands(texts[s * per_step:(s + 1) * per_step])
@@ -460,7 +482,7 @@ def run_stream(args):
         dims, _, _, n_maps = maps.info()
         texts = [l.to_pdbqt() for l in synth.ligand_set(per_batch * n_batches, seed=100000 + n_rec,
                                                           heavy=(10, 100), torsions=(0, 30))]
-        P = dict(exhaustiveness=384, max_step=40, seed=42, form=1, use_graph=1)
+        P = dict(exhaustiveness=384, max_step=40, seed=42, form=1, use_graph=1, refine_step=args.refine_step)
         streams = [torch.cuda.Stream(), torch.cuda.Stream()]
         torch.cuda.synchronize()
         t0 = time.perf_counter()

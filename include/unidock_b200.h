@@ -144,6 +144,13 @@ int ud_ligand_destroy(ud_ligand lig);
  * (unidock/src/cuda/precalculate.cu:169-326): type-pair tables of the
  * scoring function are shared by all ligands. */
 int ud_batch_create(ud_maps maps, const ud_ligand* ligs, int n, void* stream, ud_batch* out);
+/* The batch's handle and device buffers reused for n other ligands (no
+ * counterpart in the reference): buffers grow to the largest batch seen and
+ * are never freed in between, so a streaming screen that cycles a few batch
+ * handles makes no device allocation or free -- which would synchronise the
+ * device -- once warm.  A launched search must have been collected first
+ * (UD_ERR_STATE otherwise); the results of the previous ligands are dropped. */
+int ud_batch_reset(ud_batch batch, const ud_ligand* ligs, int n, void* stream);
 int ud_batch_destroy(ud_batch batch);
 
 /* Energy and pose gradient at fixed poses, host buffers.  pose_ligand[i]

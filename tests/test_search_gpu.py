@@ -112,3 +112,26 @@ def test_prepare_then_launch_equals_search(small):
     np.testing.assert_array_equal(e1, e2)
     np.testing.assert_array_equal(ev1, ev2)
     assert [m[1][0] for m in B.modes(0)] == [m[1][0] for m in B2.modes(0)]
+
+
+def test_reset_batch_equals_fresh_batch(small):
+    """A batch handle reused for other ligands (ud_batch_reset, smaller and
+    then larger than before) searches exactly as a fresh batch of them."""
+    M, ligs = small
+    B = engine.Batch(M, ligs[:3])
+    P = dict(exhaustiveness=8, max_step=6, seed=21, use_graph=1, refine_step=3)
+    B.search(**P)
+    for sub in (ligs[3:], ligs[1:]):
+        B.reset(sub)
+        B.search(**P)
+        F = engine.Batch(M, sub)
+        F.search(**P)
+        _, e_reset, _ = B.chains()
+        _, e_fresh, _ = F.chains()
+        np.testing.assert_array_equal(e_reset, e_fresh)
+        for li in range(len(sub)):
+            a, b = B.modes(li), F.modes(li)
+            assert len(a) == len(b)
+            for (pa, ea), (pb, eb) in zip(a, b):
+                np.testing.assert_array_equal(pa, pb)
+                np.testing.assert_array_equal(ea, eb)

@@ -461,7 +461,12 @@ void run_batches(const Setup& S, ud_maps maps, const std::vector<std::string>& p
             if (sl.ligs.empty()) continue;
             std::vector<ud_ligand> hs;
             for (auto& p : sl.ligs) hs.push_back(p.h);
-            check(ud_batch_create(maps, hs.data(), (int)hs.size(), sl.s, &sl.b), "batch");
+            // each slot keeps its batch handle: reused, it allocates (and frees,
+            // which would wait for the other slot's search) nothing once warm
+            if (sl.b)
+                check(ud_batch_reset(sl.b, hs.data(), (int)hs.size(), sl.s), "batch");
+            else
+                check(ud_batch_create(maps, hs.data(), (int)hs.size(), sl.s, &sl.b), "batch");
             sl.id = ++batch_id;
             sl.t0 = std::chrono::steady_clock::now();
             ud_search_params p = S.params;
@@ -499,9 +504,7 @@ void run_batches(const Setup& S, ud_maps maps, const std::vector<std::string>& p
                                                                                sl.t0)
                              .count()
                       << "ms" << std::endl;
-        ud_batch_destroy(sl.b);
         for (auto& p : sl.ligs) ud_ligand_destroy(p.h);
-        sl.b = nullptr;
         sl.ligs.clear();
     };
     bool live[2] = {start_batch(slots[0]), false};
@@ -513,6 +516,8 @@ void run_batches(const Setup& S, ud_maps maps, const std::vector<std::string>& p
         live[cur] = false;
         cur = other;
     }
+    for (auto& sl : slots)
+        if (sl.b) ud_batch_destroy(sl.b);
     for (auto& sl : slots) cudaStreamDestroy(sl.s);
     if (S.verbosity > 0) std::cout << "Docked ligands: " << done << std::endl;
 }

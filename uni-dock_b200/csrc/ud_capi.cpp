@@ -892,11 +892,16 @@ static std::vector<int> pair_group_slots(const Ligand& L, const std::vector<Pair
 
 // Device topology of `ligs` against `maps` (the body of ud_batch_create; the
 // autotuner builds its sample batches with it too).
-static std::unique_ptr<ud_batch_s> build_batch(ud_maps maps, const std::vector<const Ligand*>& ligs,
-                                               cudaStream_t s) {
+// Topology of `ligs` into the batch's device arrays (grown, never shrunk, so a
+// batch reused for the next ligands allocates nothing once it has seen the
+// largest batch).
+static void fill_batch(ud_batch_s* b, const std::vector<const Ligand*>& ligs, cudaStream_t s) {
         const int n = (int)ligs.size();
-        auto b = std::make_unique<ud_batch_s>();
-        b->maps = maps;
+        const ud_maps maps = b->maps;
+        b->ligs.clear();
+        b->desc.clear();
+        b->max_atoms = 0;
+        b->max_tors = 0;
         std::vector<AtomRec> atoms;
         std::vector<NodeRec> nodes;
         std::vector<uint32_t> pairs;
@@ -1000,7 +1005,14 @@ static std::unique_ptr<ud_batch_s> build_batch(ud_maps maps, const std::vector<c
             b->d_pair_coef.upload(coef.data(), coef.size(), s);
         }
         cuda_check(cudaStreamSynchronize(s), "batch upload");
-        return b;
+}
+
+static std::unique_ptr<ud_batch_s> build_batch(ud_maps maps, const std::vector<const Ligand*>& ligs,
+                                               cudaStream_t s) {
+    auto b = std::make_unique<ud_batch_s>();
+    b->maps = maps;
+    fill_batch(b.get(), ligs, s);
+    return b;
 }
 
 extern "C" int ud_batch_create(ud_maps maps, const ud_ligand* ligs, int n, void* stream, ud_batch* out) {
@@ -1012,6 +1024,25 @@ extern "C" int ud_batch_create(ud_maps maps, const ud_ligand* ligs, int n, void*
             v.push_back(&ligs[i]->lig);
         }
         *out = build_batch(maps, v, (cudaStream_t)stream).release();
+    });
+}
+
+extern "C" int ud_batch_reset(ud_batch b, const ud_ligand* ligs, int n, void* stream) {
+    return guarded([&] {
+        if (!b || n < 0 || (n > 0 && !ligs)) throw Error(UD_ERR_ARG, "invalid batch arguments");
+        if (b->launched) throw Error(UD_ERR_STATE, "the batch's launched search has not been collected");
+        std::vector<const Ligand*> v;
+        for (int i = 0; i < n; ++i) {
+            if (!ligs[i]) throw Error(UD_ERR_ARG, "null ligand in batch");
+            v.push_back(&ligs[i]->lig);
+        }
+        b->searched = false;
+        b->post.clear();
+        b->text[0].clear();
+        b->text[1].clear();
+        b->text_ready[0] = b->text_ready[1] = false;
+        b->tuned = false;
+        fill_batch(b, v, (cudaStream_t)stream);
     });
 }
 

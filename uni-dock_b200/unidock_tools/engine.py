@@ -80,6 +80,7 @@ def lib():
         "ud_score_grad_receptor": ([vp, ip, fp, C.c_int, C.c_int, C.c_float, C.c_float, fp, fp, C.c_int, vp],
                                    C.c_int),
         "ud_refine": ([vp, ip, fp, C.c_int, C.c_int, C.c_int, fp, vp], C.c_int),
+        "ud_batch_reset": ([vp, C.POINTER(vp), C.c_int, vp], C.c_int),
         "ud_score_terms_receptor": ([vp, ip, fp, C.c_int, C.c_int, fp, vp], C.c_int),
         "ud_ligand_write": ([vp, fp, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
         "ud_ligand_counts": ([vp, ip], C.c_int),
@@ -367,6 +368,15 @@ class Batch:
         h = C.c_void_p()
         _check(lib().ud_batch_create(maps.h, arr, len(self.ligands), None, C.byref(h)))
         self.h = h
+        self.max_torsions = max([l.n_torsions for l in self.ligands] + [0])
+
+    def reset(self, ligands, stream=None):
+        """Reuse this batch's handle and device buffers for other ligands
+        (ud_batch_reset; the previous search must have been collected)."""
+        ligands = list(ligands)
+        arr = (C.c_void_p * len(ligands))(*[l.h.value for l in ligands])
+        _check(lib().ud_batch_reset(self.h, arr, len(ligands), C.c_void_p(stream) if stream else None))
+        self.ligands = ligands
         self.max_torsions = max([l.n_torsions for l in self.ligands] + [0])
 
     # ---- fixed poses
