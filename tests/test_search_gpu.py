@@ -115,13 +115,15 @@ def test_prepare_then_launch_equals_search(small):
 
 
 def test_reset_batch_equals_fresh_batch(small):
-    """A batch handle reused for other ligands (ud_batch_reset, smaller and
-    then larger than before) searches exactly as a fresh batch of them."""
+    """A batch handle reused for other ligands (ud_batch_reset) searches
+    exactly as a fresh batch of them: a smaller batch, a larger one, and one
+    with the same ligand count, largest ligand and step count but more atoms in
+    total (topology arrays reallocated under an otherwise unchanged graph)."""
     M, ligs = small
-    B = engine.Batch(M, ligs[:3])
+    B = engine.Batch(M, [ligs[3], ligs[0]])
     P = dict(exhaustiveness=8, max_step=6, seed=21, use_graph=1, refine_step=3)
     B.search(**P)
-    for sub in (ligs[3:], ligs[1:]):
+    for sub in ([ligs[3], ligs[2]], ligs[:1], ligs):
         B.reset(sub)
         B.search(**P)
         F = engine.Batch(M, sub)

@@ -1595,7 +1595,16 @@ static void search_graph(ud_batch b, const SearchParams& sp, int n_chain, int bl
       << b->params.refine_step << ' ' << b->params.min_rmsd << ' ' << (const void*)b->d_mode_pose.p << ' '
       << (const void*)b->d_mode_e.p << ' ' << (const void*)b->d_cluster_scratch.p << ' '
       << (const void*)b->hp_mode_pose.p << ' ' << (const void*)b->hp_mode_e.p << ' ' << (const void*)b->hp_n_modes.p
-      << ' ' << (const void*)b->hp_mode_chain.p << ' ' << (const void*)b->maps->rc.atoms;
+      << ' ' << (const void*)b->hp_mode_chain.p << ' ' << (const void*)b->maps->rc.atoms << ' '
+      << (const void*)b->maps->rc.start << ' ' << (const void*)b->maps->fast.p << ' '
+      << (const void*)b->d_n_modes.p << ' ' << (const void*)b->d_mode_chain.p << ' ' << (const void*)b->d_mode_lig.p;
+    // the topology (reallocated when a reused handle gets a larger batch) and
+    // the per-warp shared-memory layout it sizes
+    const DeviceBatchView v = b->view();
+    k << ' ' << (const void*)v.ligs << ' ' << (const void*)v.atoms << ' ' << (const void*)v.nodes << ' '
+      << (const void*)v.pairs << ' ' << (const void*)v.grid_list << ' ' << (const void*)v.charges << ' '
+      << (const void*)v.pair_coef << ' ' << v.max_atoms << ' ' << v.max_torsions << ' ' << b->ligs.size() << ' '
+      << b->pose_stride;
     if (b->graph_exec && b->graph_key == k.str()) return;
     b->drop_graph();
     if (!b->capture_stream)
