@@ -35,9 +35,9 @@ BOX = 22.5
 SPACING = 0.375
 ADJOINT_POSES = 65536
 # DRAM bytes (read + write) of one search launch of this workload at 1024
-# ligands per step, measured with ncu (dram__bytes_read.sum 14.29 MB +
-# dram__bytes_write.sum 32.86 MB, one-pass capture of a timed launch)
-SEARCH_LAUNCH_DRAM_BYTES = 14.29e6 + 32.86e6
+# ligands per step, measured with ncu (dram__bytes_read.sum 13.36 MB +
+# dram__bytes_write.sum 3.98 MB, one-pass capture of a timed launch)
+SEARCH_LAUNCH_DRAM_BYTES = 13.36e6 + 3.98e6
 
 
 def parse_args():
@@ -75,7 +75,7 @@ def profile_case(args):
             synth.ligand_set(args.profile_case, seed=20261203, heavy=(12, 48), torsions=(0, 10))]
     b = engine.Batch(maps, ligs)
     P = dict(exhaustiveness=EXHAUSTIVENESS, max_step=MAX_STEP, seed=42, form=1,
-             chains_per_block=args.chains_per_block)
+             chains_per_block=args.chains_per_block, refine_step=args.refine_step)
     for _ in range(2):
         b.search_launch(**P)
         torch.cuda.synchronize()

@@ -26,6 +26,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <mutex>
+#include <unordered_map>
 
 #include "ud_engine.h"
 
@@ -1992,8 +1994,21 @@ cudaError_t launch_maps_ad4(const float* rec_xyzq, const int* rec_ad, int n_rec,
     return cudaGetLastError();
 }
 
+// Dynamic shared memory allowed for kernel `fn` on the current device, raised
+// to `smem` when below it and never lowered: a kernel launch captured in a graph earlier may need
+// more than the launch at hand (another batch's layout), and the attribute is
+// a per-kernel limit that later launches of the graph are checked against.
 static cudaError_t smem_attr(const void* fn, size_t smem) {
-    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    static std::mutex mu;
+    static std::unordered_map<uint64_t, size_t> allowed;  // (kernel, device) -> bytes
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& cur = allowed[(uint64_t)(uintptr_t)fn * 64u + (uint64_t)dev];
+    if (smem <= cur) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) cur = smem;
+    return e;
 }
 
 cudaError_t launch_score(const DeviceBatchView& b, const DeviceMapsView& m,
