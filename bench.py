@@ -270,6 +270,10 @@ def run_ours(args, rank, world):
         ligs = engine.parse_ligands(batch_texts(s))
         bb = pool[k % 2]
         bb.reset(ligs, stream=st)
+        # this batch's search starts when the previous batch's graph (search,
+        # clustering, refinement) is done: queued behind it on the device, it
+        # neither starves that batch's last kernels nor waits for the host
+        streams[k % 2].wait_stream(streams[(k + 1) % 2])
         bb.search_launch(**P, stream=st)
         if k == 0:
             n_atoms = sum(L.n_atoms for L in ligs)

@@ -450,6 +450,15 @@ void run_batches(const Setup& S, ud_maps maps, const std::vector<std::string>& p
     for (auto& sl : slots)
         if (cudaStreamCreateWithFlags(&sl.s, cudaStreamNonBlocking) != cudaSuccess)
             throw std::runtime_error("could not create a CUDA stream");
+    // end of each slot's last launched batch on the device: the other slot's
+    // next search is queued behind it, so that the persistent search of the
+    // next batch does not take the SMs from this batch's clustering and
+    // refinement kernels
+    cudaEvent_t slot_done[2];
+    for (auto& e : slot_done)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+            throw std::runtime_error("could not create a CUDA event");
+    bool has_done[2] = {false, false};
     size_t next = 0;
     int batch_id = 0, done = 0;
     auto start_batch = [&](Slot& sl) -> bool {
@@ -480,7 +489,11 @@ void run_batches(const Setup& S, ud_maps maps, const std::vector<std::string>& p
                               << r.bfgs_cap << "\n";
             }
             if (S.verbosity > 0) std::cout << "Batch " << sl.id << " size: " << sl.ligs.size() << std::endl;
+            const int me = (int)(&sl - slots), other = me ^ 1;
+            if (has_done[other]) cudaStreamWaitEvent(sl.s, slot_done[other], 0);
             check(ud_search_launch(sl.b, &p, sl.s), "search");
+            cudaEventRecord(slot_done[me], sl.s);
+            has_done[me] = true;
             return true;
         }
         return false;
@@ -518,6 +531,7 @@ void run_batches(const Setup& S, ud_maps maps, const std::vector<std::string>& p
     }
     for (auto& sl : slots)
         if (sl.b) ud_batch_destroy(sl.b);
+    for (auto& e : slot_done) cudaEventDestroy(e);
     for (auto& sl : slots) cudaStreamDestroy(sl.s);
     if (S.verbosity > 0) std::cout << "Docked ligands: " << done << std::endl;
 }

@@ -55,11 +55,15 @@ template <class T> struct DevBuf {
         p = nullptr;
         n = 0;
     }
+    // Grows with a quarter of headroom: a batch handle reused for batches of
+    // similar size then never reallocates, and a free (cudaFree synchronises
+    // the whole device) never stalls the host behind another stream's search.
     void alloc(size_t count) {
         if (count <= n && p) return;
         release();
-        cuda_check(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)), "cudaMalloc");
-        n = count;
+        const size_t cap = std::max<size_t>(count + count / 4, 1);
+        cuda_check(cudaMalloc(&p, cap * sizeof(T)), "cudaMalloc");
+        n = cap;
     }
     void upload(const T* src, size_t count, cudaStream_t s) {
         alloc(count);
@@ -77,13 +81,14 @@ template <class T> struct PinnedBuf {
     ~PinnedBuf() {
         if (p) cudaFreeHost(p);
     }
-    void alloc(size_t count) {
+    void alloc(size_t count) {  // with headroom, as DevBuf::alloc (cudaFreeHost synchronises too)
         if (count <= n && p) return;
         if (p) cudaFreeHost(p);
         p = nullptr;
         n = 0;
-        cuda_check(cudaMallocHost((void**)&p, std::max<size_t>(count, 1) * sizeof(T)), "cudaMallocHost");
-        n = count;
+        const size_t cap = std::max<size_t>(count + count / 4, 1);
+        cuda_check(cudaMallocHost((void**)&p, cap * sizeof(T)), "cudaMallocHost");
+        n = cap;
     }
 };
 
@@ -1004,6 +1009,18 @@ static void fill_batch(ud_batch_s* b, const std::vector<const Ligand*>& ligs, cu
             b->d_charge.upload(charges.data(), charges.size(), s);
             b->d_pair_coef.upload(coef.data(), coef.size(), s);
         }
+        // work order of the persistent search: most expensive ligands first
+        // (BFGS steps x (atoms + pairs) as the cost proxy).  Uploaded here, with
+        // the topology, so that a search launch does no host-to-device copy
+        // (a copy from pageable memory would wait for the stream's prior work)
+        std::vector<int> order(n);
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            long long cx = (long long)b->desc[x].local_steps * (b->desc[x].n_atoms + b->desc[x].n_pairs);
+            long long cy = (long long)b->desc[y].local_steps * (b->desc[y].n_atoms + b->desc[y].n_pairs);
+            return cx > cy;
+        });
+        b->d_order.upload(order.data(), order.size(), s);
         cuda_check(cudaStreamSynchronize(s), "batch upload");
 }
 
@@ -1656,15 +1673,6 @@ static void search_launch(ud_batch b, const ud_search_params* params, cudaStream
         b->d_queue.alloc(1);
         if (P.num_modes < 1) throw Error(UD_ERR_ARG, "num_modes must be >= 1");
         if (modes) alloc_modes(b, s);
-        // most expensive ligands first (atoms x pairs as the cost proxy)
-        std::vector<int> order(n_lig);
-        std::iota(order.begin(), order.end(), 0);
-        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-            long long cx = (long long)b->desc[x].local_steps * (b->desc[x].n_atoms + b->desc[x].n_pairs);
-            long long cy = (long long)b->desc[y].local_steps * (b->desc[y].n_atoms + b->desc[y].n_pairs);
-            return cx > cy;
-        });
-        b->d_order.upload(order.data(), order.size(), s);
         SearchParams sp{};
         sp.global_steps = global_steps_for(b->ligs, P.max_step);
         sp.exhaustiveness = E;
