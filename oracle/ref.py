@@ -16,6 +16,46 @@ REFERENCE_TREE = Path(os.environ.get("UD_REFERENCE_TREE", "/root/reference"))
 _lib = None
 
 
+GPU_LIB = Path(__file__).resolve().parent / "_ref" / "libudref_gpu.so"
+_gpu_lib = None
+
+
+def gpu_available() -> bool:
+    return LIB.exists() and GPU_LIB.exists()
+
+
+def gpu_lib():
+    """The reference's own GPU search (monte_carlo.cu, precalculate.cu) built for this GPU."""
+    global _gpu_lib
+    if _gpu_lib is None:
+        lib()  # the GPU library resolves the reference's CPU code from libudref.so
+        L = C.CDLL(str(GPU_LIB))
+        L.udref_gpu_config.argtypes = [C.POINTER(C.c_void_p), C.c_int]
+        L.udref_gpu_dock.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int, C.c_ulonglong,
+                                     C.POINTER(C.c_float), C.POINTER(C.c_double)]
+        L.udref_gpu_last_error.restype = C.c_char_p
+        _gpu_lib = L
+    return _gpu_lib
+
+
+def gpu_bucket(ligand) -> int:
+    """Size bucket (0 Small .. 4 Max) of the reference kernel that holds the ligand, or -1."""
+    arr = (C.c_void_p * 1)(ligand.h)
+    return gpu_lib().udref_gpu_config(arr, 1)
+
+
+def gpu_dock(maps, ligands, exhaustiveness, max_step, seed):
+    """The reference's GPU batched search of `ligands` (one size bucket):
+    (best energy per ligand, seconds of the pair tables, seconds of do_docking, bucket)."""
+    arr = (C.c_void_p * len(ligands))(*[l.h for l in ligands])
+    best = np.zeros(len(ligands), np.float32)
+    t = (C.c_double * 2)()
+    cfg = gpu_lib().udref_gpu_dock(maps.h, arr, len(ligands), exhaustiveness, max_step, seed, _f(best), t)
+    if cfg < 0:
+        raise RuntimeError("reference GPU search: " + gpu_lib().udref_gpu_last_error().decode())
+    return best, t[0], t[1], cfg
+
+
 def reference_inputs(pattern: str) -> list[Path]:
     """The reference's own test input files matching a glob under its tree
     (empty when the tree is absent)."""

@@ -24,30 +24,12 @@
 #include "parse_pdbqt.h"
 #include "precalculate.h"
 #include "quasi_newton.h"
+#include "ref_driver.h"
 #include "scoring_function.h"
 
 namespace {
 
 thread_local std::string g_err;
-
-struct RefMaps {
-    std::shared_ptr<ScoringFunction> sf;
-    std::unique_ptr<precalculate> pre;
-    model rec;
-    cache grid;
-    ad4cache ad4;               // AutoDock 4.2 maps read from .map files
-    const igrid* ig = &grid;    // the maps the model is scored against
-    grid_dims gd;
-    std::unique_ptr<non_cache> nc;  // explicit receptor atoms, built on first use
-    vec corner1() const { return ig == &grid ? grid.corner1() : ad4.corner1(); }
-    vec corner2() const { return ig == &grid ? grid.corner2() : ad4.corner2(); }
-};
-
-struct RefLigand {
-    std::shared_ptr<ScoringFunction> sf;
-    model m;
-    std::unique_ptr<precalculate_byatom> pre;
-};
 
 flv to_flv(const float* w, int n) { return flv(w, w + n); }
 
