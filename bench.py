@@ -56,10 +56,10 @@ def parse_args():
     ap.add_argument("--adjoint-poses", type=int, default=ADJOINT_POSES,
                     help="fixed poses of the adjoint leg (0 = skip)")
     ap.add_argument("--workload", default="screen-fast",
-                    choices=["screen-fast", "uneven-vinardo", "uneven-ad4", "stream"],
+                    choices=["screen-fast", "uneven-vinardo", "uneven-ad4", "stream", "paired"],
                     help="screen-fast: the headline batched screen; the others are the uneven-size detail-mode "
-                         "screens (Vinardo, AD4, autotuned) and the three-receptor streaming screen, each on a "
-                         "sample, printed as their own JSON line")
+                         "screens (Vinardo, AD4, autotuned), the three-receptor streaming screen and the paired "
+                         "one-ligand-one-receptor batches (CLI), each on a sample, printed as their own JSON line")
     ap.add_argument("--profile-case", type=int, default=0,
                     help="profiling aid: search N ligands of the workload twice and exit (no JSON)")
     return ap.parse_args()
@@ -469,6 +469,51 @@ def run_uneven(args, sf_name):
                                                           "ligands_per_s", "base_ligands_per_s")}}}
 
 
+def run_paired(args):
+    """Paired 1:1 batches through the CLI (--paired_batch_size): 64 complexes,
+    each its own synthetic receptor (8 receptors of 3000 atoms, boxes
+    centred on their pockets) and ligand, search_mode fast settings, batches
+    of 16; wall clock of the whole command, files in and out."""
+    import json
+    import subprocess
+    import tempfile
+    from unidock_tools import synth
+    n_rec, n_cplx, batch = 8, 64, 16
+    with tempfile.TemporaryDirectory() as d:
+        d = Path(d)
+        cfg = {}
+        for r in range(n_rec):
+            (d / f"rec{r}.pdbqt").write_text(synth.make_receptor(3000, seed=500 + r).to_pdbqt())
+        ligs = synth.ligand_set(n_cplx, seed=777, heavy=(12, 48), torsions=(0, 10))
+        for k, L in enumerate(ligs):
+            (d / f"lig{k}.pdbqt").write_text(L.to_pdbqt())
+            (d / f"lig{k}_config.json").write_text(json.dumps(
+                {"center_x": 0.0, "center_y": 0.0, "center_z": 0.0, "size_x": BOX, "size_y": BOX, "size_z": BOX}))
+            cfg[f"c{k}"] = {"protein": str(d / f"rec{k % n_rec}.pdbqt"), "ligand": str(d / f"lig{k}.pdbqt"),
+                            "ligand_config": str(d / f"lig{k}_config.json")}
+        (d / "pairs.json").write_text(json.dumps(cfg))
+        (d / "out").mkdir()
+        cmd = [str(ROOT / "uni-dock_b200" / "bin" / "unidock"), "--paired_batch_size", str(batch), "--ligand_index",
+               str(d / "pairs.json"), "--dir", str(d / "out"), "--size_x", str(BOX), "--size_y", str(BOX),
+               "--size_z", str(BOX), "--exhaustiveness", str(EXHAUSTIVENESS), "--max_step", str(MAX_STEP),
+               "--seed", "5"]
+        t0 = time.perf_counter()
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        t = time.perf_counter() - t0
+        if r.returncode != 0:
+            raise RuntimeError(r.stdout + r.stderr)
+        done = len(list((d / "out").glob("*_out.pdbqt")))
+    return {"metric": "complexes/s (paired one-ligand-one-receptor batches)", "value": round(done / t, 3),
+            "unit": "complexes/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic (seeded receptors and random-tree ligands)",
+            "config": {"workload": f"paired batches: {n_cplx} complexes over {n_rec} receptors (3000 atoms each), "
+                                   f"box {BOX} A at {SPACING} A, exhaustiveness {EXHAUSTIVENESS}, max_step "
+                                   f"{MAX_STEP}, refine_step 3, --paired_batch_size {batch}",
+                       "timing": "wall clock of the CLI command: receptor parsing, one map build per complex, "
+                                 "searches queued on 16 streams, refinement, output files"},
+            "complexes_done": done, "seconds": round(t, 3)}
+
+
 def run_stream(args):
     """Streaming screen: search_mode balance (exhaustiveness 384, max_step 40),
     ligands with U{10..100} heavy atoms and U{0..30} torsions, through the
@@ -578,7 +623,8 @@ def main():
         profile_case(args)
         return
     if args.workload != "screen-fast" and args.impl != "reference":
-        res = run_stream(args) if args.workload == "stream" else run_uneven(args, args.workload.split("-")[1])
+        res = (run_stream(args) if args.workload == "stream" else
+               run_paired(args) if args.workload == "paired" else run_uneven(args, args.workload.split("-")[1]))
         print(json.dumps(res), flush=True)
         return
     if args.impl == "reference":

@@ -48,11 +48,13 @@ def test_help_lists_every_reference_option():
     (["--receptor", "r.pdbqt", "--ligand", "a.pdbqt", "--gpu_batch", "b.pdbqt", "--dir", "."],
      "Can't use both --ligand and --batch arguments simultaneously."),
     (["--receptor", "r.pdbqt", "--ligand", "a.pdbqt", "--search_mode", "slow"], "unknown search_mode"),
+    (["--paired_batch_size", "2"], "ERROR: Paired batch size set, but no config json specified via --ligand_index"),
+    (["--paired_batch_size", "2", "--ligand_index", "c.json"], "ERROR: Need to specify an output directory for batch mode."),
 ])
 def test_argument_errors(args, msg):
     r = run(*args)
     assert r.returncode != 0
-    assert msg in r.stderr, r.stderr
+    assert msg in r.stderr + r.stdout, (r.stdout, r.stderr)
 
 
 def box_args(size=22.5):
@@ -185,3 +187,52 @@ def test_ad4_maps_written_then_read_back(inputs, tmp_path, receptor):
     ea = [float(l.split()[3]) for l in a.splitlines() if l.startswith("REMARK VINA RESULT:")]
     eb = [float(l.split()[3]) for l in b.splitlines() if l.startswith("REMARK VINA RESULT:")]
     assert ea and ea == eb
+
+
+@pytest.mark.gpu
+def test_paired_batch_mode(tmp_path):
+    """--paired_batch_size with a JSON configuration (the reference's
+    paired_batching.schema.json): every complex is its own receptor, box and
+    ligand.  Each output equals a single-ligand run of that complex with the
+    paired mode's settings (min_rmsd 0, energy range 3), and the score file
+    holds its best affinity."""
+    import json
+    recs = [synth.make_receptor(1500, radius=28.0, seed=s) for s in (11, 12)]
+    centers = [(0.0, 0.0, 0.0), (1.5, -1.0, 0.5)]
+    cfg = {}
+    for k in range(3):
+        rec_path = tmp_path / f"rec{k % 2}.pdbqt"
+        rec_path.write_text(recs[k % 2].to_pdbqt())
+        lig_path = tmp_path / f"lig{k}.pdbqt"
+        lig_path.write_text(synth.make_ligand(16 + 4 * k, 2 + k, seed=40 + k).to_pdbqt())
+        c = centers[k % 2]
+        if k < 2:  # .json ligand config with the box, and a key=value text config
+            lc = tmp_path / f"lig{k}_config.json"
+            lc.write_text(json.dumps({"center_x": c[0], "center_y": c[1], "center_z": c[2],
+                                      "size_x": 20.0, "size_y": 20.0, "size_z": 20.0}))
+        else:
+            lc = tmp_path / f"lig{k}_config.txt"
+            lc.write_text(f"center_x={c[0]}\ncenter_y={c[1]}\ncenter_z={c[2]}\n")
+        cfg[f"complex{k}"] = {"protein": str(rec_path), "ligand": str(lig_path), "ligand_config": str(lc)}
+    (tmp_path / "pairs.json").write_text(json.dumps(cfg))
+    out = tmp_path / "out"
+    out.mkdir()
+    common = ["--exhaustiveness", 16, "--max_step", 8, "--seed", 5, "--num_modes", 4]
+    r = run("--paired_batch_size", 2, "--ligand_index", tmp_path / "pairs.json", "--dir", out,
+            "--size_x", 20, "--size_y", 20, "--size_z", 20, *common)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "Found 3 to be primed." in r.stdout and "To do [2] batches" in r.stdout
+    for k in range(3):
+        text = (out / f"lig{k}_out.pdbqt").read_text()
+        assert text.startswith("MODEL 1\nREMARK VINA RESULT:")
+        best = float(text.split("\n")[1].split()[3])
+        score = (out / f"lig{k}_score.txt").read_text()
+        assert score.startswith("affinity(kcal/mol)[0]=")
+        assert abs(float(score.split("=")[1]) - best) < 1e-3
+        c = centers[k % 2]
+        single = tmp_path / f"single{k}.pdbqt"
+        r = run("--receptor", tmp_path / f"rec{k % 2}.pdbqt", "--ligand", tmp_path / f"lig{k}.pdbqt",
+                "--center_x", c[0], "--center_y", c[1], "--center_z", c[2], "--size_x", 20, "--size_y", 20,
+                "--size_z", 20, "--min_rmsd", 0, "--out", single, *common)
+        assert r.returncode == 0, r.stderr
+        assert single.read_text() == text

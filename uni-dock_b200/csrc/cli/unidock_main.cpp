@@ -47,7 +47,8 @@ const OptSpec kOptions[] = {
     {"flex", 0, "flexible side chains (not supported by this build)", "Input"},
     {"ligand", 2, "ligand (PDBQT or SDF)", "Input"},
     {"ligand_index", 0, "file containing paths to ligands (PDBQT or SDF)", "Input"},
-    {"paired_batch_size", 0, "one-ligand-one-protein batching (not supported by this build)", "Input"},
+    {"paired_batch_size", 0, "If > 0, uses batching for one-ligand-one-protein docking, with json config in "
+                             "ligand_index following paired_batching.schema.json", "Input"},
     {"batch", 2, "batch ligand (PDBQT)", "Input"},
     {"gpu_batch", 2, "gpu batch ligand (PDBQT or SDF)", "Input"},
     {"scoring", 0, "scoring function (ad4, vina or vinardo)", "Input"},
@@ -257,6 +258,11 @@ std::string default_output(const std::string& name, const std::string& dir) {
     return dir + "/" + default_output(name);
 }
 std::string default_score_output(const std::string& name) { return strip_ext(name) + "_score.txt"; }
+
+bool file_exists(const std::string& p) {
+    struct stat st;
+    return stat(p.c_str(), &st) == 0 && S_ISREG(st.st_mode);
+}
 
 bool is_directory(const std::string& p) {
     struct stat st;
@@ -580,6 +586,292 @@ void run_single(const Setup& S, ud_maps maps, const std::string& path, const std
     ud_ligand_destroy(h);
 }
 
+// ---------------------------------------------------------------- paired batches
+// A small JSON reader for the paired-batch configuration: objects, strings,
+// numbers, true/false/null and arrays (only objects, strings and numbers are
+// used).  Object members keep their file order, as the reference's
+// property tree does.
+struct Json {
+    enum Kind { Null, Bool, Number, String, Array, Object } kind = Null;
+    double num = 0;
+    std::string str;
+    std::vector<Json> items;                           // array elements
+    std::vector<std::pair<std::string, Json>> members;  // object members in order
+    const Json* get(const std::string& k) const {
+        for (auto& m : members)
+            if (m.first == k) return &m.second;
+        return nullptr;
+    }
+};
+
+struct JsonReader {
+    const std::string& t;
+    size_t i = 0;
+    explicit JsonReader(const std::string& text) : t(text) {}
+    [[noreturn]] void fail(const std::string& what) {
+        throw std::runtime_error("JSON: " + what + " at offset " + std::to_string(i));
+    }
+    void ws() {
+        while (i < t.size() && std::isspace((unsigned char)t[i])) ++i;
+    }
+    std::string string() {
+        if (t[i] != '"') fail("expected a string");
+        std::string out;
+        for (++i; i < t.size() && t[i] != '"'; ++i) {
+            if (t[i] != '\\') {
+                out += t[i];
+                continue;
+            }
+            if (++i >= t.size()) break;
+            const char e = t[i];
+            if (e == 'n') out += '\n';
+            else if (e == 't') out += '\t';
+            else if (e == 'r') out += '\r';
+            else if (e == 'b') out += '\b';
+            else if (e == 'f') out += '\f';
+            else if (e == 'u') {
+                if (i + 4 >= t.size()) fail("bad escape");
+                const unsigned cp = (unsigned)std::stoul(t.substr(i + 1, 4), nullptr, 16);
+                i += 4;
+                if (cp < 0x80) out += (char)cp;  // paths and numbers only need ASCII
+                else fail("non-ASCII escape");
+            } else out += e;
+        }
+        if (i >= t.size()) fail("unterminated string");
+        ++i;
+        return out;
+    }
+    Json value() {
+        ws();
+        if (i >= t.size()) fail("unexpected end");
+        Json v;
+        const char c = t[i];
+        if (c == '{') {
+            v.kind = Json::Object;
+            ++i;
+            ws();
+            if (i < t.size() && t[i] == '}') { ++i; return v; }
+            for (;;) {
+                ws();
+                std::string k = string();
+                ws();
+                if (i >= t.size() || t[i] != ':') fail("expected ':'");
+                ++i;
+                v.members.emplace_back(k, value());
+                ws();
+                if (i < t.size() && t[i] == ',') { ++i; continue; }
+                if (i < t.size() && t[i] == '}') { ++i; return v; }
+                fail("expected ',' or '}'");
+            }
+        }
+        if (c == '[') {
+            v.kind = Json::Array;
+            ++i;
+            ws();
+            if (i < t.size() && t[i] == ']') { ++i; return v; }
+            for (;;) {
+                v.items.push_back(value());
+                ws();
+                if (i < t.size() && t[i] == ',') { ++i; continue; }
+                if (i < t.size() && t[i] == ']') { ++i; return v; }
+                fail("expected ',' or ']'");
+            }
+        }
+        if (c == '"') {
+            v.kind = Json::String;
+            v.str = string();
+            return v;
+        }
+        if (t.compare(i, 4, "true") == 0) { v.kind = Json::Bool; v.num = 1; i += 4; return v; }
+        if (t.compare(i, 5, "false") == 0) { v.kind = Json::Bool; i += 5; return v; }
+        if (t.compare(i, 4, "null") == 0) { i += 4; return v; }
+        size_t used = 0;
+        try {
+            v.num = std::stod(t.substr(i, 64), &used);
+        } catch (...) {
+            fail("unexpected character");
+        }
+        v.kind = Json::Number;
+        i += used;
+        return v;
+    }
+};
+
+Json read_json(const std::string& path) {
+    const std::string text = read_file(path);
+    JsonReader r(text);
+    Json v = r.value();
+    r.ws();
+    if (r.i != text.size()) r.fail("trailing characters");
+    return v;
+}
+
+struct PairedComplex {
+    std::string protein, ligand;
+    float center[3], size[3];
+};
+
+// One complex's box (simulation_container.h fill_config_from_json /
+// fill_config): a .json ligand config needs center_x/y/z and size_x/y/z; any
+// other file holds "key=value" lines, the centre first, then optionally the
+// size.  The box given on the command line is the default size.
+bool read_ligand_config(const std::string& path, const float* box, PairedComplex& c) {
+    for (int k = 0; k < 3; ++k) c.size[k] = box[k];
+    if (ends_with(path, ".json")) {
+        Json v = read_json(path);
+        const char* keys[6] = {"center_x", "center_y", "center_z", "size_x", "size_y", "size_z"};
+        float vals[6];
+        for (int k = 0; k < 6; ++k) {
+            const Json* f = v.get(keys[k]);
+            if (!f || f->kind != Json::Number) {
+                std::cout << "Error parsing config json " << path << "\n";
+                return false;
+            }
+            vals[k] = (float)f->num;
+        }
+        for (int k = 0; k < 3; ++k) {
+            c.center[k] = vals[k];
+            c.size[k] = vals[3 + k];
+        }
+        return true;
+    }
+    std::ifstream in(path);
+    if (!in) return false;
+    std::vector<double> vals;
+    for (std::string line; std::getline(in, line);) {
+        line.erase(std::remove(line.begin(), line.end(), '\r'), line.end());
+        const size_t eq = line.find('=');
+        if (eq == std::string::npos) continue;
+        vals.push_back(std::stod(line.substr(eq + 1)));
+    }
+    if (vals.size() < 3) return false;
+    for (int k = 0; k < 3; ++k) c.center[k] = (float)vals[k];
+    if (vals.size() >= 6)
+        for (int k = 0; k < 3; ++k) c.size[k] = (float)vals[3 + k];
+    return true;
+}
+
+// Paired batches (simulation_container.h, vina_cuda_worker.h): every complex
+// of the configuration is its own receptor, box and ligand.  The reference
+// runs one host thread and CUDA stream per complex; here each batch of
+// complexes is set up (maps, ligand, batch) and all its searches are queued on
+// a pool of streams, so the GPU runs them side by side, then collected.
+// Per complex: <dir>/<ligand>_out.pdbqt and <dir>/<ligand>_score.txt with the
+// best affinity.  As the reference's worker: Vina weights, min_rmsd 0, energy
+// range 3, the command line's exhaustiveness, max_step, num_modes,
+// refine_step and seed.
+int run_paired(const Setup& S0, const std::string& config, const std::string& dir, int batch_size, const float* box,
+               bool local_only) {
+    if (local_only) throw std::runtime_error("--local_only with --paired_batch_size is not supported by this build");
+    Setup S = S0;
+    S.sf = UD_SF_VINA;
+    S.weights = {-0.035579f, -0.005156f, 0.840245f, -0.035069f, -0.587439f, 50.0f, 0.05846f};
+    S.params.min_rmsd = 0.0f;
+    S.params.energy_range = 3.0f;
+    S.params.use_graph = 0;  // each batch is searched once
+    const Json cfg = read_json(config);
+    if (cfg.kind != Json::Object) throw std::runtime_error("paired batch config " + config + " is not a JSON object");
+    std::vector<PairedComplex> complexes;
+    for (auto& m : cfg.members) {
+        const Json *pr = m.second.get("protein"), *lg = m.second.get("ligand"), *lc = m.second.get("ligand_config");
+        if (!pr || !lg || !lc) continue;
+        PairedComplex c;
+        c.protein = pr->str;
+        c.ligand = lg->str;
+        if (read_ligand_config(lc->str, box, c)) complexes.push_back(c);
+        if (complexes.size() >= 5000) {
+            std::cout << "Limiting number of ranked samples to max limits 5000\n";
+            break;
+        }
+    }
+    std::cout << "Found " << complexes.size() << " to be primed.\n";
+    if (complexes.empty()) {
+        std::cout << "m_successful_property_count = 0\n";
+        return -1;
+    }
+    const int n_batches = (int)((complexes.size() + batch_size - 1) / batch_size);
+    std::cout << "Parameters: exh = " << S.params.exhaustiveness << ", box[0] = " << box[0]
+              << ", max_eval_steps global = " << S.params.max_step << ", num_modes = " << S.params.num_modes
+              << ", refine_steps = " << S.params.refine_step << "\n";
+    std::cout << "To do [" << n_batches << "] batches\n";
+    const int n_streams = std::min(batch_size, 16);
+    std::vector<cudaStream_t> streams(n_streams);
+    for (auto& st : streams)
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+            throw std::runtime_error("could not create a CUDA stream");
+    int errors = 0;
+    for (int bi = 0; bi < n_batches; ++bi) {
+        struct Job {
+            const PairedComplex* c = nullptr;
+            ud_maps maps = nullptr;
+            ud_ligand lig = nullptr;
+            ud_batch b = nullptr;
+            cudaStream_t s = nullptr;
+            bool ok = false;
+        };
+        std::vector<Job> jobs;
+        int batch_errors = 0;
+        for (size_t k = (size_t)bi * batch_size; k < std::min(complexes.size(), (size_t)(bi + 1) * batch_size); ++k) {
+            Job j;
+            j.c = &complexes[k];
+            j.s = streams[jobs.size() % n_streams];
+            std::cout << "Processing " << j.c->ligand << "\n";
+            try {
+                if (!file_exists(j.c->ligand)) throw std::runtime_error("Input ligand file does not exist (" + j.c->ligand + ")");
+                if (!file_exists(j.c->protein))
+                    throw std::runtime_error("Input (rigid) protein file does not exist (" + j.c->protein + ")");
+                Setup Sk = S;
+                for (int q = 0; q < 3; ++q) {
+                    Sk.center[q] = j.c->center[q];
+                    Sk.size[q] = j.c->size[q];
+                }
+                j.maps = build_maps(Sk, j.c->protein);
+                auto parsed = parse_ligands({j.c->ligand}, 1, 1);
+                if (parsed.empty()) throw std::runtime_error("could not parse " + j.c->ligand);
+                j.lig = parsed[0].h;
+                check(ud_batch_create(j.maps, &j.lig, 1, j.s, &j.b), "batch");
+                check(ud_search_launch(j.b, &S.params, j.s), "search");
+                j.ok = true;
+            } catch (const std::exception& e) {
+                std::cerr << "Exception processing " << j.c->ligand << ", " << e.what() << "\n";
+                ++batch_errors;
+            }
+            jobs.push_back(j);
+        }
+        for (auto& j : jobs) {
+            if (j.ok) {
+                try {
+                    check(ud_search_collect(j.b, j.s), "search");
+                    int n = 0;
+                    check(ud_result_count(j.b, 0, &n), "results");
+                    if (n == 0) {
+                        std::cerr << "WARNING: Could not find any poses. No poses were written.\n";
+                    } else {
+                        const std::string name = default_output(get_filename(j.c->ligand), dir + "/");
+                        write_text(name, result_text(j.b, 0, ends_with(name, ".sdf") ? 1 : 0));
+                        float pose[7 + 64], en[8];
+                        check(ud_result_mode(j.b, 0, 0, pose, en), "results");
+                        std::ostringstream sc;
+                        sc << "affinity(kcal/mol)[0]=" << en[0] << "\n";
+                        write_text(dir + "/" + default_score_output(get_filename(j.c->ligand)), sc.str());
+                    }
+                } catch (const std::exception& e) {
+                    std::cerr << "Exception processing " << j.c->ligand << ", " << e.what() << "\n";
+                    ++batch_errors;
+                }
+            }
+            if (j.b) ud_batch_destroy(j.b);
+            if (j.lig) ud_ligand_destroy(j.lig);
+            if (j.maps) ud_maps_destroy(j.maps);
+        }
+        errors += batch_errors;
+        std::cout << "Batch [" << bi + 1 << "/" << n_batches << "] completed. " << batch_errors << " errors.\n";
+    }
+    for (auto& st : streams) cudaStreamDestroy(st);
+    std::cout << errors << " Total errors\n";
+    return errors;
+}
+
 int run(int argc, char** argv) {
     Options o;
     parse_args(argc, argv, o);
@@ -592,7 +884,7 @@ int run(int argc, char** argv) {
         std::cout << "unidock (B200 engine, C ABI version " << ud_version() << ")\n";
         return 0;
     }
-    for (const char* unsupported : {"flex", "paired_batch_size", "bias", "multi_bias", "randomize_only"})
+    for (const char* unsupported : {"flex", "bias", "multi_bias", "randomize_only"})
         if (o.has(unsupported))
             throw std::runtime_error(std::string("--") + unsupported + " is not supported by this build");
     Setup S;
@@ -617,7 +909,6 @@ int run(int argc, char** argv) {
     } else {
         throw std::runtime_error("Scoring function " + sf_name + " unknown.");
     }
-    if (!o.has("receptor") && !o.has("maps")) throw std::runtime_error("The receptor or affinity maps must be specified.");
     const bool score_only = o.has("score_only"), local_only = o.has("local_only");
     S.verbosity = (int)o.num("verbosity", 1);
     const int cpu = (int)o.num("cpu", 0);
@@ -660,6 +951,28 @@ int run(int argc, char** argv) {
     p.use_graph = 1;
     const bool no_refine = o.has("no_refine");
     p.refine_step = no_refine ? 0 : (int)o.num("refine_step", 3);
+    // one-ligand-one-protein batches (main.cpp:663-700)
+    const int paired_batch_size = (int)o.num("paired_batch_size", 0);
+    if (paired_batch_size > 0) {
+        if (!o.has("ligand_index")) {
+            std::cout << "ERROR: Paired batch size set, but no config json specified via --ligand_index\n";
+            return -1;
+        }
+        float box[3] = {25, 25, 25};
+        if (!o.has("size_x") || !o.has("size_y") || !o.has("size_z"))
+            std::cout << "WARN: Paired batch size set, but size_x/size_y/size_z not specified, using 25\n";
+        else
+            box[0] = (float)o.num("size_x", 25), box[1] = (float)o.num("size_y", 25), box[2] = (float)o.num("size_z", 25);
+        if (!o.has("dir")) {
+            std::cout << "ERROR: Need to specify an output directory for batch mode.\n";
+            return -1;
+        }
+        std::cout << "Entering paired batch mode\n";
+        const int device = (int)o.num("device_id", 0);
+        if (cudaSetDevice(device) != cudaSuccess) throw std::runtime_error("could not select GPU " + std::to_string(device));
+        return run_paired(S, o.str("ligand_index"), o.str("dir"), paired_batch_size, box, local_only);
+    }
+    if (!o.has("receptor") && !o.has("maps")) throw std::runtime_error("The receptor or affinity maps must be specified.");
     // ligands
     std::vector<std::string> ligand_names = o.list("ligand");
     std::vector<std::string> batch_names = o.list("gpu_batch");
