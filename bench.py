@@ -509,8 +509,9 @@ def run_paired(args):
             "config": {"workload": f"paired batches: {n_cplx} complexes over {n_rec} receptors (3000 atoms each), "
                                    f"box {BOX} A at {SPACING} A, exhaustiveness {EXHAUSTIVENESS}, max_step "
                                    f"{MAX_STEP}, refine_step 3, --paired_batch_size {batch}",
-                       "timing": "wall clock of the CLI command: receptor parsing, one map build per complex, "
-                                 "searches queued on 16 streams, refinement, output files"},
+                       "timing": "wall clock of the CLI command: receptor parsing, map builds (complexes of a "
+                                 "batch with the same receptor and box share one), searches queued on 16 streams, "
+                                 "refinement, output files"},
             "complexes_done": done, "seconds": round(t, 3)}
 
 

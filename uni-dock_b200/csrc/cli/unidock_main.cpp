@@ -811,6 +811,8 @@ int run_paired(const Setup& S0, const std::string& config, const std::string& di
         };
         std::vector<Job> jobs;
         int batch_errors = 0;
+        // complexes of the batch with the same receptor file and box share one set of maps
+        std::map<std::string, ud_maps> maps_of;
         for (size_t k = (size_t)bi * batch_size; k < std::min(complexes.size(), (size_t)(bi + 1) * batch_size); ++k) {
             Job j;
             j.c = &complexes[k];
@@ -825,7 +827,12 @@ int run_paired(const Setup& S0, const std::string& config, const std::string& di
                     Sk.center[q] = j.c->center[q];
                     Sk.size[q] = j.c->size[q];
                 }
-                j.maps = build_maps(Sk, j.c->protein);
+                std::ostringstream key;
+                key << j.c->protein << ' ' << Sk.center[0] << ' ' << Sk.center[1] << ' ' << Sk.center[2] << ' '
+                    << Sk.size[0] << ' ' << Sk.size[1] << ' ' << Sk.size[2];
+                auto it = maps_of.find(key.str());
+                if (it == maps_of.end()) it = maps_of.emplace(key.str(), build_maps(Sk, j.c->protein)).first;
+                j.maps = it->second;
                 auto parsed = parse_ligands({j.c->ligand}, 1, 1);
                 if (parsed.empty()) throw std::runtime_error("could not parse " + j.c->ligand);
                 j.lig = parsed[0].h;
@@ -862,8 +869,8 @@ int run_paired(const Setup& S0, const std::string& config, const std::string& di
             }
             if (j.b) ud_batch_destroy(j.b);
             if (j.lig) ud_ligand_destroy(j.lig);
-            if (j.maps) ud_maps_destroy(j.maps);
         }
+        for (auto& m : maps_of) ud_maps_destroy(m.second);
         errors += batch_errors;
         std::cout << "Batch [" << bi + 1 << "/" << n_batches << "] completed. " << batch_errors << " errors.\n";
     }

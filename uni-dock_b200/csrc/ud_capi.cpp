@@ -11,7 +11,9 @@
 #include <cstring>
 #include <iomanip>
 #include <limits>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <sstream>
 #include <stdexcept>
@@ -109,6 +111,26 @@ template <class F> int guarded(F&& f) {
 }
 
 }  // namespace
+
+// Pair tables of a scoring function (all terms weighted, or one term
+// unweighted), built once per process for each (function, weights, term):
+// building one takes tens of milliseconds of host time, and screens with
+// many receptors (paired batches) create many maps with the same function.
+static std::shared_ptr<const PairTable> cached_table(const Scoring& sf, int term = -1) {
+    static std::mutex mu;
+    static std::map<std::string, std::shared_ptr<const PairTable>> cache;
+    std::string key = std::to_string(sf.choice) + ' ' + std::to_string(term) + ' ' + std::to_string(sf.cutoff);
+    for (float w : sf.weights) key += ' ' + std::to_string(w);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    auto t = std::make_shared<PairTable>();
+    t->build(sf, term);
+    std::lock_guard<std::mutex> lock(mu);
+    return cache.emplace(key, std::move(t)).first->second;
+}
 
 struct ud_maps_s {
     Scoring sf;
@@ -358,8 +380,7 @@ extern "C" int ud_maps_create(int sf, const float* weights, int n_weights, const
         for (size_t k = 0; k < m->slot_types.size(); ++k) d.slot_of_xs[m->slot_types[k]] = (int8_t)k;
         d.n_maps = (int)m->slot_types.size();
         // pair tables of the scoring function
-        PairTable tab;
-        tab.build(m->sf);
+        const PairTable& tab = *cached_table(m->sf);
         m->n_bins = tab.n;
         m->factor = tab.factor;
         m->cutoff2 = m->sf.cutoff * m->sf.cutoff;
@@ -491,8 +512,7 @@ extern "C" int ud_maps_create_ad4(const float* weights, int n_weights, const flo
         d.d_slot = d.e_slot + 1;
         d.n_maps = d.d_slot + 1;
         // pair tables: AD type pairs + the shared electrostatic / desolvation rows
-        PairTable tab;
-        tab.build(m->sf);
+        const PairTable& tab = *cached_table(m->sf);
         m->n_bins = tab.n;
         m->factor = tab.factor;
         m->cutoff2 = m->sf.cutoff * m->sf.cutoff;
@@ -651,8 +671,7 @@ extern "C" int ud_maps_load(int sf, const float* weights, int n_weights, const c
         d.slope = 1e6f;
         for (int i = 0; i < 3; ++i) m->box_center[i] = center0[i];
         m->box_spacing = spacing0;
-        PairTable tab;
-        tab.build(m->sf);
+        const PairTable& tab = *cached_table(m->sf);
         m->n_bins = tab.n;
         m->factor = tab.factor;
         m->cutoff2 = m->sf.cutoff * m->sf.cutoff;
@@ -1222,8 +1241,7 @@ static void ensure_terms(ud_maps_s* m, cudaStream_t s) {
     DevBuf<float> d_fastT;
     std::vector<float> rows(rblock), fastT(d.ad4 ? 0 : (size_t)XS_SIZE * m->n_bins * nslot_pad, 0.0f);
     for (int t = 0; t < nt; ++t) {
-        PairTable tab;
-        tab.build(m->sf, t);
+        const PairTable& tab = *cached_table(m->sf, t);
         if (tab.n != m->n_bins) throw Error(UD_ERR_ARG, "term table size mismatch");
         pack_smooth4(tab, rows.data());
         cuda_check(cudaMemcpyAsync(m->term_rows.p + (size_t)t * rblock, rows.data(), rblock * sizeof(float),
