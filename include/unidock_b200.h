@@ -335,6 +335,24 @@ int ud_result_write(ud_batch batch, int lig, int format, char* buf, size_t cap, 
  * the --local_only path of Vina::optimize (unidock/src/lib/vina.cpp:1385-1428). */
 int ud_optimize(ud_batch batch, const int* pose_ligand, float* poses, int n_poses, int pose_stride,
                 int max_steps, float v, float* e_out, int* evals_out, void* stream);
+/* ---------------------------------------------------------------- bias wells
+ * AutoDock-bias style wells (BPF text, unidock/src/lib/bias.h: a header line,
+ * then "x y z Vset r type [AD types]" with type don, acc, aro or map).
+ * Added to Vina / Vinardo maps built from a receptor, as --bias does
+ * (Vina::set_bias + cache::compute_bias, vina.cpp:1472-1480, cache.cpp:789-957):
+ * every map point gets Vset exp(-d^2/r^2) on the maps the well reaches when it
+ * is below -0.01; the wells also enter the scoring against the receptor atoms
+ * (refinement, ud_score_terms_receptor).  Wells accumulate over calls.  The
+ * maps then have no term decomposition (ud_maps_set_weights, weight
+ * gradients: UD_ERR_STATE). */
+int ud_maps_add_bias(ud_maps maps, const char* bpf, size_t len, void* stream);
+/* Ligand `lig`'s own wells (--multi_bias, Vina::set_batch_bias,
+ * vina.cpp:1482-1493), used instead of the maps' when it is scored against
+ * the receptor atoms, as model::bias_list is.  As in the reference's GPU
+ * search, they do not change the maps the search uses.  Empty text clears
+ * them; ud_batch_reset clears all. */
+int ud_batch_set_bias(ud_batch batch, int lig, const char* bpf, size_t len);
+
 /* ---------------------------------------------------------------- receptor atoms
  * Scoring against the receptor atoms the maps were built from, instead of the
  * maps: the reference's non_cache (unidock/src/lib/non_cache.cpp), which it

@@ -101,6 +101,8 @@ def lib():
         L.udref_refine.argtypes = [vp, vp, fp, fp, fp, C.c_int, fp]
         L.udref_nc_score.argtypes = [vp, vp, fp, fp, fp, C.c_float, fp]
         L.udref_cluster.argtypes = [vp, C.c_int, fp, C.c_int, fp, C.c_float, C.c_int, ip]
+        L.udref_maps_bias.argtypes = [vp, C.c_char_p]
+        L.udref_ligand_bias.argtypes = [vp, C.c_char_p]
         L.udref_ad4_maps_read.restype = vp
         L.udref_ad4_maps_read.argtypes = [C.c_char_p, fp, C.c_int]
         L.udref_ad4_pair.argtypes = [C.c_int, C.c_float, C.c_int, C.c_float, C.c_float, fp, C.c_int]
@@ -177,6 +179,10 @@ class RefMaps:
         self.factor = np.zeros(3, np.float32)
         self.factor_inv = np.zeros(3, np.float32)
         lib().udref_maps_dims(self.h, _i(self.dims), _f(self.init), _f(self.factor), _f(self.factor_inv))
+
+    def add_bias(self, bpf: str):
+        """Bias wells added to the maps and to receptor-atom scoring (--bias)."""
+        return lib().udref_maps_bias(self.h, bpf.encode())
 
     def get(self, xs):
         out = np.zeros(int(self.dims.prod()), np.float32)
@@ -266,6 +272,10 @@ class RefLigand:
         pose = np.array(pose, np.float32)
         t = pose[7:7 + self.n_torsions].copy() if self.n_torsions else np.zeros(1, np.float32)
         return pose[0:3].copy(), pose[3:7].copy(), np.ascontiguousarray(t)
+
+    def set_bias(self, bpf: str):
+        """The ligand's own wells (--multi_bias)."""
+        return lib().udref_ligand_bias(self.h, bpf.encode())
 
     def nc_eval_deriv(self, maps, pose, slope=1e6, v=1000.0):
         """model::eval_deriv against the receptor atoms (non_cache)."""

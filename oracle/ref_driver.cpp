@@ -12,6 +12,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <sstream>
 #include <thread>
 #include <vector>
 
@@ -301,13 +302,45 @@ float udref_bfgs(void* lh, void* mh, float* pos, float* quat, float* tors, float
 // (vina.cpp:557-562), and the docking model it scores: the receptor with the
 // ligand appended, as set_ligand_from_object_gpu builds each ligand's model.
 static non_cache& nc_of(RefMaps* M) {
-    if (!M->nc) M->nc.reset(new non_cache(M->rec, M->gd, M->pre.get(), 1e6, std::vector<bias_element>()));
+    if (!M->nc) M->nc.reset(new non_cache(M->rec, M->gd, M->pre.get(), 1e6, M->bias));
     return *M->nc;
 }
 static model docking_model(RefMaps* M, RefLigand* L) {
     model mm = M->rec;
     mm.append(L->m);
+    mm.bias_list = L->bias;  // as set_ligand_from_object_gpu sets it for --multi_bias
     return mm;
+}
+
+// Bias wells of a BPF text: header line, then one well per line (Vina::set_bias, vina.cpp:1472-1480).
+static std::vector<bias_element> parse_bpf(const char* text) {
+    std::vector<bias_element> out;
+    std::istringstream in(text);
+    std::string line;
+    std::getline(in, line);
+    while (std::getline(in, line)) {
+        if (line.find_first_not_of(" \t\r") == std::string::npos) continue;
+        std::istringstream l(line);
+        out.emplace_back(l);
+    }
+    return out;
+}
+
+// --bias: the wells added to the maps (cache::compute_bias) and kept for non_cache.
+int udref_maps_bias(void* mh, const char* text) {
+    auto M = (RefMaps*)mh;
+    std::vector<bias_element> wells = parse_bpf(text);
+    M->grid.compute_bias(M->rec, wells);
+    M->bias.insert(M->bias.end(), wells.begin(), wells.end());
+    M->nc.reset();
+    return (int)M->bias.size();
+}
+
+// --multi_bias: the ligand's own wells.
+int udref_ligand_bias(void* lh, const char* text) {
+    auto L = (RefLigand*)lh;
+    L->bias = parse_bpf(text);
+    return (int)L->bias.size();
 }
 
 // model::eval_deriv against the receptor atoms (non_cache::eval_deriv,

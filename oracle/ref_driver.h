@@ -5,6 +5,7 @@
 #include <memory>
 
 #include "ad4cache.h"
+#include "bias.h"
 #include "cache.h"
 #include "model.h"
 #include "non_cache.h"
@@ -20,6 +21,7 @@ struct RefMaps {
     const igrid* ig = &grid;    // the maps the model is scored against
     grid_dims gd;
     std::unique_ptr<non_cache> nc;  // explicit receptor atoms, built on first use
+    std::vector<bias_element> bias; // wells added to the maps and to non_cache
     vec corner1() const { return ig == &grid ? grid.corner1() : ad4.corner1(); }
     vec corner2() const { return ig == &grid ? grid.corner2() : ad4.corner2(); }
 };
@@ -28,5 +30,6 @@ struct RefLigand {
     std::shared_ptr<ScoringFunction> sf;
     model m;
     std::unique_ptr<precalculate_byatom> pre;
+    std::vector<bias_element> bias; // the ligand's own wells (model::bias_list of its docking model)
 };
 

@@ -236,3 +236,32 @@ def test_paired_batch_mode(tmp_path):
                 "--size_z", 20, "--min_rmsd", 0, "--out", single, *common)
         assert r.returncode == 0, r.stderr
         assert single.read_text() == text
+
+
+@pytest.mark.gpu
+def test_bias_and_multi_bias(inputs, tmp_path):
+    """--bias adds wells to the maps; --multi_bias reads <ligand>.bpf beside every
+    batch ligand (and fails when one is missing)."""
+    d, names = inputs
+    bpf = "x y z Vset r type\n1.0 0.0 0.0 -3.0 1.2 acc\n-2.0 1.0 0.5 -2.0 1.5 map C\n"
+    (tmp_path / "b.bpf").write_text(bpf)
+    out = tmp_path / "biased"
+    out.mkdir()
+    search = ["--exhaustiveness", 16, "--max_step", 8, "--seed", 2, *box_args()]
+    r = run("--receptor", d / "rec.pdbqt", "--gpu_batch", *names[:2], "--dir", out, *search, "--bias", tmp_path / "b.bpf")
+    assert r.returncode == 0, r.stderr
+    assert all((out / (p.stem + "_out.pdbqt")).exists() for p in names[:2])
+    ligs = []
+    for k, p in enumerate(names[:2]):  # copies with a .bpf beside each
+        q = tmp_path / p.name
+        q.write_text(p.read_text())
+        q.with_suffix(".bpf").write_text(bpf)
+        ligs.append(q)
+    out2 = tmp_path / "multi"
+    out2.mkdir()
+    r = run("--receptor", d / "rec.pdbqt", "--gpu_batch", *ligs, "--dir", out2, *search, "--multi_bias")
+    assert r.returncode == 0, r.stderr
+    assert all((out2 / (p.stem + "_out.pdbqt")).exists() for p in ligs)
+    ligs[1].with_suffix(".bpf").unlink()
+    r = run("--receptor", d / "rec.pdbqt", "--gpu_batch", *ligs, "--dir", out2, *search, "--multi_bias")
+    assert r.returncode != 0

@@ -92,8 +92,9 @@ const OptSpec kOptions[] = {
     {"weight_ad4_dsolv", 0, "ad4_dsolv weight", "Advanced"},
     {"weight_ad4_rot", 0, "ad4_rot weight", "Advanced"},
     {"weight_glue", 0, "macrocycle glue weight", "Advanced"},
-    {"bias", 0, "bias configuration file (not supported by this build)", "Advanced"},
-    {"multi_bias", 1, "per-ligand bias files (not supported by this build)", "Advanced"},
+    {"bias", 0, "bias configuration file name, content similar to BPF in AutoDock-bias", "Advanced"},
+    {"multi_bias", 1, "add ligand bias {ligand_name}.bpf for every input ligand, content similar to BPF in "
+                      "AutoDock-bias", "Advanced"},
     {"keep_nonpolar_H", 1, "keep non polar H in sdf", "Advanced"},
     {"cpu", 0, "the number of CPUs to use for parsing and post-processing (0 = all)", "Misc"},
     {"seed", 0, "explicit random seed", "Misc"},
@@ -360,7 +361,16 @@ struct Setup {
     // scores after docking, --score_only and --local_only against the receptor
     // atoms (the reference unless --no_refine; Vina / Vinardo with --receptor)
     bool receptor_scoring = false;
+    bool multi_bias = false;  // --multi_bias: each batch ligand's own {name}.bpf
 };
+
+// get_biasname (utils.cpp:103-111): the ligand file name without .pdbqt / .sdf, plus .bpf
+std::string bias_name(const std::string& path) {
+    std::string t = path;
+    if (t.size() >= 6 && t.compare(t.size() - 6, 6, ".pdbqt") == 0) t.resize(t.size() - 6);
+    else if (t.size() >= 4 && t.compare(t.size() - 4, 4, ".sdf") == 0) t.resize(t.size() - 4);
+    return t + ".bpf";
+}
 
 // --score_only / --local_only energy vector of one pose (Vina::score, vina.cpp:1168-1243).
 void score_pose(const Setup& S, ud_batch b, std::vector<float>& pose, float* en) {
@@ -482,6 +492,11 @@ void run_batches(const Setup& S, ud_maps maps, const std::vector<std::string>& p
                 check(ud_batch_reset(sl.b, hs.data(), (int)hs.size(), sl.s), "batch");
             else
                 check(ud_batch_create(maps, hs.data(), (int)hs.size(), sl.s, &sl.b), "batch");
+            if (S.multi_bias)  // each ligand's {name}.bpf (main.cpp:255-265, utils.cpp:103-111)
+                for (size_t i = 0; i < sl.ligs.size(); ++i) {
+                    const std::string bpf = read_file(bias_name(sl.ligs[i].path));
+                    check(ud_batch_set_bias(sl.b, (int)i, bpf.data(), bpf.size()), "bias");
+                }
             sl.id = ++batch_id;
             sl.t0 = std::chrono::steady_clock::now();
             ud_search_params p = S.params;
@@ -891,7 +906,7 @@ int run(int argc, char** argv) {
         std::cout << "unidock (B200 engine, C ABI version " << ud_version() << ")\n";
         return 0;
     }
-    for (const char* unsupported : {"flex", "bias", "multi_bias", "randomize_only"})
+    for (const char* unsupported : {"flex", "randomize_only"})
         if (o.has(unsupported))
             throw std::runtime_error(std::string("--") + unsupported + " is not supported by this build");
     Setup S;
@@ -922,6 +937,9 @@ int run(int argc, char** argv) {
     S.threads = cpu > 0 ? cpu : (int)std::max(1u, std::thread::hardware_concurrency());
     S.spacing = (float)o.num("spacing", 0.375);
     S.autotune = o.has("autotune");
+    S.multi_bias = o.has("multi_bias");
+    if ((o.has("bias") || S.multi_bias) && S.sf == UD_SF_AD4)
+        throw std::runtime_error("bias wells with --scoring ad4 are not supported by this build");
     // search parameters and search_mode presets (main.cpp:644-661)
     const bool batch_mode = o.has("gpu_batch") || o.has("batch") || o.has("ligand_index");
     int exhaustiveness = (int)o.num("exhaustiveness", 8);
@@ -1063,6 +1081,10 @@ int run(int argc, char** argv) {
     } else {
         maps = build_maps(S, o.str("receptor"));
         S.receptor_scoring = !no_refine && S.sf != UD_SF_AD4;
+        if (o.has("bias")) {  // Vina::set_bias, then the wells go into the maps (vina.cpp:547-553)
+            const std::string bpf = read_file(o.str("bias"));
+            check(ud_maps_add_bias(maps, bpf.data(), bpf.size(), nullptr), "bias");
+        }
     }
     if (o.has("write_maps")) check(ud_maps_write(maps, o.str("write_maps").c_str()), "write maps");
     if (!ligand_names.empty()) {

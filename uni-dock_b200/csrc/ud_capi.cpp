@@ -155,6 +155,9 @@ struct ud_maps_s {
     bool loaded = false;             // read from map files: no receptor to rebuild per-term maps from
     float box_center[3] = {0, 0, 0}; // box as given (written to map file headers)
     float box_spacing = 0;
+    // bias wells added to the maps (and to receptor-atom scoring)
+    std::vector<BiasElement> bias;
+    DevBuf<BiasRec> d_bias;
     // receptor atoms in box cells for scoring without the maps, built on first use
     DevBuf<float> rc_atoms;
     DevBuf<int> rc_start;
@@ -214,6 +217,12 @@ struct ud_batch_s {
     PinnedBuf<float> hp_poses;
     PinnedBuf<ChainResult> hp_results;
     bool graph_results = false;
+    // per-ligand bias wells for receptor-atom scoring (multi-bias), all lists
+    // back to back; span per ligand: offset | count << 16
+    std::vector<std::vector<BiasRec>> lig_bias;
+    DevBuf<BiasRec> d_lig_bias;
+    DevBuf<int> d_lig_bias_span;
+    bool lig_bias_dirty = false;
     // modes of the last search: clustered (and refined) on the device
     int mode_cap = 0;
     bool refined = false;
@@ -1078,6 +1087,8 @@ extern "C" int ud_batch_reset(ud_batch b, const ud_ligand* ligs, int n, void* st
         b->text[1].clear();
         b->text_ready[0] = b->text_ready[1] = false;
         b->tuned = false;
+        b->lig_bias.clear();
+        b->lig_bias_dirty = true;
         fill_batch(b, v, (cudaStream_t)stream);
     });
 }
@@ -1201,6 +1212,96 @@ extern "C" int ud_score_terms(ud_batch b, const int* pose_ligand, const float* p
     });
 }
 
+// ---------------------------------------------------------------- bias wells
+
+static BiasRec bias_rec(const BiasElement& e) {
+    BiasRec r{};
+    r.x = e.xyz[0];
+    r.y = e.xyz[1];
+    r.z = e.xyz[2];
+    r.vset = e.vset;
+    r.r = e.r;
+    bias_atom_multiplicity(e, r.mult);
+    return r;
+}
+
+extern "C" int ud_maps_add_bias(ud_maps m, const char* text, size_t len, void* stream) {
+    return guarded([&] {
+        if (!m || !text) throw Error(UD_ERR_ARG, "null argument");
+        if (m->desc.ad4) throw Error(UD_ERR_STATE, "bias wells on AutoDock 4.2 maps are not supported by this build");
+        if (m->terms_built)
+            throw Error(UD_ERR_STATE, "add bias wells before the maps' term decomposition is first used");
+        cudaStream_t s = (cudaStream_t)stream;
+        const std::vector<BiasElement> wells = parse_bias(std::string(text, len));
+        std::vector<BiasMapRec> recs;
+        for (const BiasElement& e : wells) {
+            BiasMapRec r{};
+            r.x = e.xyz[0];
+            r.y = e.xyz[1];
+            r.z = e.xyz[2];
+            r.vset = e.vset;
+            r.r = e.r;
+            const uint64_t types = bias_map_types(e);
+            for (size_t k = 0; k < m->slot_types.size(); ++k)
+                if ((types >> m->slot_types[k]) & 1u) {
+                    if (k < 32) r.slots_lo |= 1u << k;
+                    else r.slots_hi |= 1u << (k - 32);
+                }
+            recs.push_back(r);
+        }
+        DevBuf<BiasMapRec> d;
+        d.upload(recs.data(), recs.size(), s);
+        cuda_check(launch_bias_maps(d.p, (int)recs.size(), m->desc, m->maps.p, s), "bias maps kernel");
+        cuda_check(cudaStreamSynchronize(s), "bias maps");
+        m->bias.insert(m->bias.end(), wells.begin(), wells.end());
+        std::vector<BiasRec> all;
+        for (const BiasElement& e : m->bias) all.push_back(bias_rec(e));
+        m->d_bias.upload(all.data(), all.size(), s);
+        cuda_check(cudaStreamSynchronize(s), "bias upload");
+        m->rc.bias = m->d_bias.p;
+        m->rc.n_bias = (int)all.size();
+    });
+}
+
+extern "C" int ud_batch_set_bias(ud_batch b, int lig, const char* text, size_t len) {
+    return guarded([&] {
+        if (!b || (len > 0 && !text)) throw Error(UD_ERR_ARG, "null argument");
+        if (lig < 0 || lig >= (int)b->ligs.size()) throw Error(UD_ERR_ARG, "ligand out of range");
+        if (b->maps->desc.ad4) throw Error(UD_ERR_STATE, "bias wells with AutoDock 4.2 maps are not supported by this build");
+        b->lig_bias.resize(b->ligs.size());
+        b->lig_bias[lig].clear();
+        for (const BiasElement& e : parse_bias(std::string(text ? text : "", len))) b->lig_bias[lig].push_back(bias_rec(e));
+        if (b->lig_bias[lig].size() > 0xFFFF) throw Error(UD_ERR_CAPACITY, "too many bias wells for one ligand");
+        b->lig_bias_dirty = true;
+    });
+}
+
+// Per-ligand wells to the device before a receptor-atom launch that needs them.
+static void upload_lig_bias(ud_batch b, cudaStream_t s) {
+    if (!b->lig_bias_dirty) return;
+    std::vector<BiasRec> all;
+    std::vector<int> span(b->ligs.size(), 0);
+    for (size_t l = 0; l < b->lig_bias.size() && l < b->ligs.size(); ++l) {
+        if (b->lig_bias[l].empty()) continue;
+        if (all.size() > 0xFFFF) throw Error(UD_ERR_CAPACITY, "too many bias wells in one batch");
+        span[l] = (int)all.size() | ((int)b->lig_bias[l].size() << 16);
+        all.insert(all.end(), b->lig_bias[l].begin(), b->lig_bias[l].end());
+    }
+    b->d_lig_bias.upload(all.data(), all.size(), s);
+    b->d_lig_bias_span.upload(span.data(), span.size(), s);
+    cuda_check(cudaStreamSynchronize(s), "bias upload");
+    b->lig_bias_dirty = false;
+}
+
+// The receptor view of a batch: the maps' receptor and wells, the batch's per-ligand wells.
+static DeviceReceptorView receptor_view(ud_batch b) {
+    DeviceReceptorView r = b->maps->rc;
+    const bool any = !b->lig_bias.empty();
+    r.lig_bias = any ? b->d_lig_bias.p : nullptr;
+    r.lig_bias_span = any ? b->d_lig_bias_span.p : nullptr;
+    return r;
+}
+
 // ---------------------------------------------------------------- adjoint
 
 // Unweighted per-term maps and tables of the maps' scoring function: the
@@ -1219,6 +1320,8 @@ static void ensure_terms(ud_maps_s* m, cudaStream_t s) {
     if (m->terms_built) return;
     if (m->loaded)
         throw Error(UD_ERR_STATE, "maps read from files have no per-term decomposition (build them from the receptor)");
+    if (!m->bias.empty())
+        throw Error(UD_ERR_STATE, "maps with bias wells have no per-term decomposition (the wells are no weighted term)");
     const MapsDesc& d = m->desc;
     const int nt = m->sf.n_terms;
     const int nslot = d.n_maps, nslot_pad = std::max(4, (nslot + 3) & ~3);
@@ -1517,7 +1620,7 @@ static cudaError_t enqueue_modes(ud_batch b, cudaStream_t s) {
                                    cap, b->params.min_rmsd, b->d_cluster_scratch.p, b->d_n_modes.p,
                                    b->d_mode_chain.p, b->d_mode_lig.p, b->d_mode_pose.p, s);
     if (e == cudaSuccess && b->refined)
-        e = launch_receptor(kRecRefine, b->view(), tables_view(b->maps), b->maps->rc, b->d_mode_lig.p,
+        e = launch_receptor(kRecRefine, b->view(), tables_view(b->maps), receptor_view(b), b->d_mode_lig.p,
                             b->d_mode_pose.p, b->pose_stride, (int)n_slot, b->params.refine_step, 0.0f, 1000.0f,
                             nullptr, nullptr, 0, b->d_mode_e.p, s);
     if (e == cudaSuccess)
@@ -1537,7 +1640,10 @@ static void alloc_modes(ud_batch b, cudaStream_t s) {
     const int n_lig = (int)b->ligs.size();
     b->mode_cap = std::max(1, b->params.num_modes);
     b->refined = refines(b, b->params);
-    if (b->refined) ensure_receptor(b->maps, s);
+    if (b->refined) {
+        ensure_receptor(b->maps, s);
+        upload_lig_bias(b, s);
+    }
     const size_t n_slot = (size_t)n_lig * b->mode_cap;
     b->d_cluster_scratch.alloc(n_slot * 3 * std::max(1, b->max_atoms));
     b->d_n_modes.alloc(n_lig);
@@ -1631,7 +1737,9 @@ static void search_graph(ud_batch b, const SearchParams& sp, int n_chain, int bl
       << (const void*)b->d_mode_e.p << ' ' << (const void*)b->d_cluster_scratch.p << ' '
       << (const void*)b->hp_mode_pose.p << ' ' << (const void*)b->hp_mode_e.p << ' ' << (const void*)b->hp_n_modes.p
       << ' ' << (const void*)b->hp_mode_chain.p << ' ' << (const void*)b->maps->rc.atoms << ' '
-      << (const void*)b->maps->rc.start << ' ' << (const void*)b->maps->fast.p << ' '
+      << (const void*)b->maps->rc.start << ' ' << (const void*)b->maps->rc.bias << ' ' << b->maps->rc.n_bias << ' '
+      << (const void*)receptor_view(b).lig_bias << ' ' << (const void*)receptor_view(b).lig_bias_span << ' '
+      << (const void*)b->maps->fast.p << ' '
       << (const void*)b->d_n_modes.p << ' ' << (const void*)b->d_mode_chain.p << ' ' << (const void*)b->d_mode_lig.p;
     // the topology (reallocated when a reused handle gets a larger batch) and
     // the per-warp shared-memory layout it sizes
@@ -1790,12 +1898,13 @@ static void check_receptor_poses(ud_batch b, const int* pose_ligand, const float
 static void receptor_poses(ud_batch b, int mode, const int* pose_ligand, float* poses, int n_poses, int pose_stride,
                            int refine_step, std::vector<float>& out4, cudaStream_t s) {
     ensure_receptor(b->maps, s);
+    upload_lig_bias(b, s);
     out4.assign(4 * (size_t)n_poses, 0.0f);
     if (n_poses == 0) return;
     b->d_pose_lig.upload(pose_ligand, n_poses, s);
     b->d_pose.upload(poses, (size_t)n_poses * pose_stride, s);
     b->d_score.alloc(4 * (size_t)n_poses);
-    cuda_check(launch_receptor(mode, b->view(), tables_view(b->maps), b->maps->rc, b->d_pose_lig.p, b->d_pose.p,
+    cuda_check(launch_receptor(mode, b->view(), tables_view(b->maps), receptor_view(b), b->d_pose_lig.p, b->d_pose.p,
                                pose_stride, n_poses, refine_step, 0.0f, 1000.0f, nullptr, nullptr, 0, b->d_score.p, s),
                "receptor kernel");
     if (mode == kRecRefine)
@@ -1816,13 +1925,14 @@ extern "C" int ud_score_grad_receptor(ud_batch b, const int* pose_ligand, const 
         if (!e_out || !g_out || g_stride < 6 + b->max_tors) throw Error(UD_ERR_ARG, "invalid buffers");
         cudaStream_t s = (cudaStream_t)stream;
         ensure_receptor(b->maps, s);
+        upload_lig_bias(b, s);
         if (n_poses == 0) return;
         b->d_pose_lig.upload(pose_ligand, n_poses, s);
         b->d_pose.upload(poses, (size_t)n_poses * pose_stride, s);
         b->d_e.alloc(n_poses);
         b->d_g.alloc((size_t)n_poses * g_stride);
         cuda_check(cudaMemsetAsync(b->d_g.p, 0, (size_t)n_poses * g_stride * sizeof(float), s), "memset");
-        cuda_check(launch_receptor(kRecEnergyGrad, b->view(), tables_view(b->maps), b->maps->rc, b->d_pose_lig.p,
+        cuda_check(launch_receptor(kRecEnergyGrad, b->view(), tables_view(b->maps), receptor_view(b), b->d_pose_lig.p,
                                    b->d_pose.p, pose_stride, n_poses, 0, slope, v, b->d_e.p, b->d_g.p, g_stride,
                                    nullptr, s),
                    "receptor kernel");

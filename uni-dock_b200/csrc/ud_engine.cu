@@ -205,6 +205,10 @@ struct Receptor {
     int n[3];
     float begin[3], end[3];
     float inv_cell;
+    const BiasRec* bias;
+    int n_bias;
+    const BiasRec* lig_bias;
+    const int* lig_bias_span;
 };
 
 // Shared-memory layout of one chain (float offsets).
@@ -251,6 +255,7 @@ struct Ctx {
     const float2* coef;    // AD4: per pair slot coefficients
     int n_atoms, R, T, n_pairs, max_depth, local_steps, n_grid;
     int lane;
+    int lig;
 };
 
 __device__ __forceinline__ Ctx make_ctx(const Batch& B, int lig, float* s) {
@@ -271,6 +276,7 @@ __device__ __forceinline__ Ctx make_ctx(const Batch& B, int lig, float* s) {
     c.max_depth = __ldg(&d->max_depth);
     c.local_steps = __ldg(&d->local_steps);
     c.lane = threadIdx.x & 31;
+    c.lig = lig;
     return c;
 }
 
@@ -391,6 +397,19 @@ __device__ __forceinline__ float grid_eval(const Maps& M, int slot, const float4
     return f + penalty;
 }
 
+// The bias wells a ligand is scored with against the receptor atoms: its own
+// list when it has one (model::bias_list), else the maps' (non_cache::bias_list).
+__device__ __forceinline__ void bias_of(const Receptor& R, int lig, const BiasRec*& bias, int& n) {
+    const int span = R.lig_bias_span ? __ldg(R.lig_bias_span + lig) : 0;
+    if (span >> 16) {
+        bias = R.lig_bias + (span & 0xFFFF);
+        n = span >> 16;
+    } else {
+        bias = R.bias;
+        n = R.n_bias;
+    }
+}
+
 // Interaction of one ligand atom (XS type t1, position pa) with the receptor
 // atoms, all lanes of the warp together (non_cache::eval_deriv / eval,
 // non_cache.cpp:35-110, 420-500): the position is clamped into the box at a
@@ -401,7 +420,8 @@ __device__ __forceinline__ float grid_eval(const Maps& M, int slot, const float4
 // the same energy and gradient.
 template <bool kDeriv>
 __device__ __forceinline__ float receptor_term(const Receptor& R, const Tables& Tb, int t1, const float4 pa, float v,
-                                               float slope, float& gx, float& gy, float& gz) {
+                                               float slope, const BiasRec* bias, int n_bias, float& gx, float& gy,
+                                               float& gz) {
     const int lane = threadIdx.x & 31;
     float p[3] = {pa.x, pa.y, pa.z};
     float pen = 0, od[3] = {0, 0, 0};
@@ -451,6 +471,28 @@ __device__ __forceinline__ float receptor_term(const Receptor& R, const Tables& 
         dy = warp_sum(dy);
         dz = warp_sum(dz);
     }
+    if (n_bias > 0) {  // bias wells at the unclamped position, before the curl (non_cache.cpp:112-400)
+        for (int k = 0; k < n_bias; ++k) {
+            const BiasRec* b = bias + k;
+            const int m = __ldg(&b->mult[t1]);
+            if (m == 0) continue;
+            const float bx = pa.x - __ldg(&b->x), by = pa.y - __ldg(&b->y), bz = pa.z - __ldg(&b->z);
+            const float rb2 = bx * bx + by * by + bz * bz;
+            if (rb2 > Tb.cutoff2) continue;
+            const float r = __ldg(&b->r);
+            const float dE = __ldg(&b->vset) * expf(-rb2 / r / r);
+            if (dE >= -0.01f) continue;
+            const float f = dE / (-r * r);
+            for (int q = 0; q < m; ++q) {
+                e += dE;
+                if constexpr (kDeriv) {
+                    dx += f * bx;
+                    dy += f * by;
+                    dz += f * bz;
+                }
+            }
+        }
+    }
     if (e > 0 && v < 0.1f * kMaxFl) {  // curl
         const float tmp = (v < kEps) ? 0 : v / (v + e);
         e *= tmp;
@@ -481,11 +523,14 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
     for (int k = c.lane; k < c.n_atoms; k += 32) frc[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     __syncwarp();
     if constexpr (kReceptor) {
+        const BiasRec* bias;
+        int n_bias;
+        bias_of(*Rc, c.lig, bias, n_bias);
         for (int k = 0; k < c.n_grid; ++k) {  // one atom at a time, lanes over its receptor atoms
             const int a = __ldg(c.grid + k) & 0xFF;
             const int t1 = ((__ldg(&c.atoms[a].packed) >> 24) & 0xFF) - 1;
             float gx, gy, gz;
-            const float ea = receptor_term<true>(*Rc, Tb, t1, xyz[a], v_inter, rslope, gx, gy, gz);
+            const float ea = receptor_term<true>(*Rc, Tb, t1, xyz[a], v_inter, rslope, bias, n_bias, gx, gy, gz);
             if (c.lane == 0) {
                 frc[a] = make_float4(gx, gy, gz, 0.0f);
                 e += ea;
@@ -1216,12 +1261,15 @@ __device__ __forceinline__ void eval_score_receptor(const Ctx& c, const Layout& 
                                                     float& e_intra) {
     kinematics(c, L, conf);
     const float4* xyz = reinterpret_cast<const float4*>(c.s + L.coords);
+    const BiasRec* bias;
+    int n_bias;
+    bias_of(R, c.lig, bias, n_bias);
     float ei = 0;
     for (int k = 0; k < c.n_grid; ++k) {
         const int a = __ldg(c.grid + k) & 0xFF;
         const int t1 = ((__ldg(&c.atoms[a].packed) >> 24) & 0xFF) - 1;
         float gx, gy, gz;
-        ei += receptor_term<false>(R, Tb, t1, xyz[a], v, 1e6f, gx, gy, gz);
+        ei += receptor_term<false>(R, Tb, t1, xyz[a], v, 1e6f, bias, n_bias, gx, gy, gz);
     }
     e_inter = ei;
     e_intra = intra_fast<false>(c, Tb, xyz, v);
@@ -1327,6 +1375,34 @@ __global__ void __launch_bounds__(128) receptor_kernel(
         eval_score_receptor(c, L, R, Tb, x, v, ei, ea);
         const bool within = heavy_within(c, L, R);
         if (c.lane == 0) out4[pose] = make_float4(e_last, ei, ea, within ? 1.0f : 0.0f);
+    }
+}
+
+// ---------------------------------------------------------------- bias wells on the maps
+// cache::compute_bias (cache.cpp:789-957): at every map point, in list order,
+// each well adds Vset exp(-d^2 / r^2) to the maps of the slots it reaches when
+// that is below -0.01.  Probe points as the map build places them.
+__global__ void __launch_bounds__(256) bias_maps_kernel(const BiasMapRec* __restrict__ bias, int n_bias, int nx, int ny,
+                                                        int nz, int n_slots, float init0, float init1, float init2,
+                                                        float finv0, float finv1, float finv2,
+                                                        float* __restrict__ maps) {
+    const size_t plane = (size_t)nx * ny * nz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < plane; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((size_t)nx * ny));
+        const float px = __fadd_rn(init0, __fmul_rn(finv0, (float)x));
+        const float py = __fadd_rn(init1, __fmul_rn(finv1, (float)y));
+        const float pz = __fadd_rn(init2, __fmul_rn(finv2, (float)z));
+        for (int k = 0; k < n_bias; ++k) {
+            const BiasMapRec b = bias[k];
+            const float dx = __fsub_rn(b.x, px), dy = __fsub_rn(b.y, py), dz = __fsub_rn(b.z, pz);
+            const float rb2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+            const float dE = __fmul_rn(b.vset, expf(__fdiv_rn(__fdiv_rn(-rb2, b.r), b.r)));
+            if (dE >= -0.01f) continue;
+            for (int s = 0; s < n_slots; ++s) {
+                const unsigned int word = s < 32 ? b.slots_lo : b.slots_hi;
+                if ((word >> (s & 31)) & 1u) maps[(size_t)s * plane + i] = __fadd_rn(maps[(size_t)s * plane + i], dE);
+            }
+        }
     }
 }
 
@@ -1962,6 +2038,10 @@ static dev::Receptor to_receptor(const DeviceReceptorView& r) {
         R.end[i] = r.end[i];
     }
     R.inv_cell = r.inv_cell;
+    R.bias = r.bias;
+    R.n_bias = r.n_bias;
+    R.lig_bias = r.lig_bias;
+    R.lig_bias_span = r.lig_bias_span;
     return R;
 }
 
@@ -2107,6 +2187,18 @@ cudaError_t launch_optimize(const DeviceBatchView& b, const DeviceMapsView& m,
     kern<<<grid, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t), P, L,
                                                              pose_lig, poses, pose_stride, n_poses,
                                                              max_steps, v, e_out, evals_out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bias_maps(const BiasMapRec* bias, int n_bias, const MapsDesc& d, float* maps,
+                             cudaStream_t stream) {
+    if (n_bias <= 0) return cudaSuccess;
+    const size_t plane = (size_t)d.dims[0] * d.dims[1] * d.dims[2];
+    const int threads = 256;
+    const int blocks = (int)std::min<size_t>((plane + threads - 1) / threads, 148 * 16);
+    dev::bias_maps_kernel<<<blocks, threads, 0, stream>>>(bias, n_bias, d.dims[0], d.dims[1], d.dims[2], d.n_maps,
+                                                          d.init[0], d.init[1], d.init[2], d.factor_inv[0],
+                                                          d.factor_inv[1], d.factor_inv[2], maps);
     return cudaGetLastError();
 }
 

@@ -151,6 +151,25 @@ struct DeviceTermsView {
     long long row_block;   // float4 per term in `rows`
 };
 
+// A bias well as the receptor-atom scoring adds it to a ligand atom: the well
+// (x, y, z, Vset, r) and, per XS type of the atom, how many times it counts
+// (a CG carbon counts as its C_H / C_P type).
+struct BiasRec {
+    float x, y, z, vset;
+    float r;
+    float pad[3];
+    unsigned char mult[36];
+    unsigned char pad2[12];
+};
+static_assert(sizeof(BiasRec) == 80, "BiasRec layout");
+
+// A bias well as a map build adds it: the well and the map slots it reaches.
+struct BiasMapRec {
+    float x, y, z, vset, r;
+    unsigned int slots_lo, slots_hi;  // bit s: map slot s
+    float pad;
+};
+
 // Receptor atoms for scoring without maps (the reference's non_cache, used to
 // refine and rescore poses): a uniform grid of cubic cells over the box; cell c
 // lists, in receptor order, every typed receptor atom within the cutoff of some
@@ -162,6 +181,10 @@ struct DeviceReceptorView {
     int n[3];              // cells per axis
     float begin[3], end[3];// the box (grid_dims begin / end)
     float inv_cell;        // 1 / cell edge
+    const BiasRec* bias;   // bias wells of the maps (used for ligands without their own)
+    int n_bias;
+    const BiasRec* lig_bias;       // per-ligand bias wells, all ligands' lists back to back
+    const int* lig_bias_span;      // per ligand: offset | count << 16 into lig_bias (0: none)
 };
 
 // Modes of the receptor-atom kernel.
@@ -204,6 +227,11 @@ cudaError_t launch_search_noalloc(const DeviceBatchView& b, const DeviceMapsView
                                   float* poses, int pose_stride, float* e_out, int* evals_out,
                                   cudaStream_t stream);
 int engine_chain_smem_bytes(int max_atoms, int max_torsions);
+// Bias wells added to the maps (cache::compute_bias): every map point of every
+// slot a well reaches gets Vset exp(-d^2 / r^2) when that is below -0.01,
+// wells in list order.
+cudaError_t launch_bias_maps(const BiasMapRec* bias, int n_bias, const MapsDesc& d, float* maps,
+                             cudaStream_t stream);
 // Per-ligand clustering of the chain results (warp per ligand) into at most
 // `cap` modes: n_modes[lig], and per mode slot lig * cap + k its chain, its
 // ligand (-1 for an unused slot) and a copy of the chain's pose.

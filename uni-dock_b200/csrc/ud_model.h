@@ -102,6 +102,29 @@ struct PairTable {
 // smooth/fast construction of one row from the tabulated energies at r = sqrt(i/factor)
 void table_row_from_energies(const float* e, const float* rs, int n, float* fast, float* smooth);
 
+// ---------------------------------------------------------------- bias
+// One entry of an AutoDock-bias style file (BPF; unidock/src/lib/bias.h):
+// "x y z Vset r type [AD types...]", a Gaussian well Vset exp(-d^2 / r^2)
+// around (x, y, z) for the atoms its type selects.
+enum BiasType { BIAS_DON = 0, BIAS_ACC, BIAS_ARO, BIAS_MAP, BIAS_UNKNOWN };
+struct BiasElement {
+    float xyz[3] = {0, 0, 0};
+    float vset = 0, r = 1;
+    int type = BIAS_UNKNOWN;
+    std::vector<int> ad_list;  // BIAS_MAP: the AD types named (empty: every type)
+};
+// The entries of a bias file (its first line is a header; blank lines skipped).
+std::vector<BiasElement> parse_bias(const std::string& text);
+// XS types whose maps get the well (cache::compute_bias, cache.cpp:789-957):
+// acceptor wells the acceptor maps, map wells every map or the types of the
+// named AD types' elements; donor and aromatic wells none.
+uint64_t bias_map_types(const BiasElement& b);
+// Times the well is added to a ligand atom of XS type t when it is scored
+// against the receptor atoms (non_cache::eval / eval_deriv, non_cache.cpp:
+// 112-400): a CG carbon counts as its C_H / C_P type; a map well counts once
+// per named AD type that selects t.
+void bias_atom_multiplicity(const BiasElement& b, unsigned char mult[XS_SIZE]);
+
 // ---------------------------------------------------------------- ligand model
 struct Atom {
     float lab[3];      // coordinates as read (lab frame of the input pose)

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <sstream>
 #include <stdexcept>
 
 #include "ud_model.h"
@@ -408,6 +409,114 @@ void PairTable::build(const Scoring& sf, int term) {
             table_row_from_energies(e.data(), rs.data(), n, &fast[(std::size_t)tp * n],
                                     &smooth[(std::size_t)tp * n * 2]);
         }
+}
+
+}  // namespace ud
+
+// ---------------------------------------------------------------- bias
+
+namespace ud {
+
+std::vector<BiasElement> parse_bias(const std::string& text) {
+    std::vector<BiasElement> out;
+    std::istringstream in(text);
+    std::string line;
+    std::getline(in, line);  // header
+    while (std::getline(in, line)) {
+        std::istringstream l(line);
+        BiasElement b;
+        if (!(l >> b.xyz[0] >> b.xyz[1] >> b.xyz[2] >> b.vset >> b.r)) continue;
+        std::string t;
+        l >> t;
+        if (t == "don") b.type = BIAS_DON;
+        else if (t == "acc") b.type = BIAS_ACC;
+        else if (t == "aro") b.type = BIAS_ARO;
+        else if (t == "map") {
+            b.type = BIAS_MAP;
+            for (std::string a; l >> a;) {  // AD types; metals and unknown names are not kept (bias.h)
+                const int ad = ad_type_from_name(a);
+                if (ad < AD_SIZE) b.ad_list.push_back(ad);
+            }
+        } else b.type = BIAS_UNKNOWN;
+        out.push_back(b);
+    }
+    return out;
+}
+
+uint64_t bias_map_types(const BiasElement& b) {
+    auto bit = [](int t) { return (uint64_t)1 << t; };
+    uint64_t m = 0;
+    if (b.type == BIAS_ACC) return bit(XS_O_A) | bit(XS_N_A) | bit(XS_O_DA) | bit(XS_N_DA);
+    if (b.type != BIAS_MAP) return 0;
+    if (b.ad_list.empty()) return (bit(XS_SIZE) - 1);
+    for (int ad : b.ad_list) {
+        switch (ad_to_el(ad)) {
+            case EL_C:
+                if (ad == AD_CG0) m |= bit(XS_C_P_CG0) | bit(XS_C_H_CG0);
+                else if (ad == AD_CG1) m |= bit(XS_C_P_CG1) | bit(XS_C_H_CG1);
+                else if (ad == AD_CG2) m |= bit(XS_C_P_CG2) | bit(XS_C_H_CG2);
+                else if (ad == AD_CG3) m |= bit(XS_C_P_CG3) | bit(XS_C_H_CG3);
+                else if (ad == AD_C)
+                    m |= bit(XS_C_P_CG0) | bit(XS_C_H_CG0) | bit(XS_C_P_CG1) | bit(XS_C_H_CG1) | bit(XS_C_P_CG2) |
+                         bit(XS_C_H_CG2) | bit(XS_C_P_CG3) | bit(XS_C_H_CG3) | bit(XS_C_P) | bit(XS_C_H);
+                else m |= bit(XS_C_P) | bit(XS_C_H);
+                break;
+            case EL_N: m |= bit(XS_N_DA) | bit(XS_N_A) | bit(XS_N_D) | bit(XS_N_P); break;
+            case EL_O: m |= bit(XS_O_DA) | bit(XS_O_A) | bit(XS_O_D) | bit(XS_O_P); break;
+            case EL_S: m |= bit(XS_S_P); break;
+            case EL_P: m |= bit(XS_P_P); break;
+            case EL_F: m |= bit(XS_F_H); break;
+            case EL_Cl: m |= bit(XS_Cl_H); break;
+            case EL_Br: m |= bit(XS_Br_H); break;
+            case EL_I: m |= bit(XS_I_H); break;
+            case EL_Si: m |= bit(XS_Si); break;
+            case EL_At: m |= bit(XS_At); break;
+            case EL_Met: m |= bit(XS_Met_D); break;
+            case EL_Dummy:
+                if (ad == AD_G0) m |= bit(XS_G0);
+                else if (ad == AD_G1) m |= bit(XS_G1);
+                else if (ad == AD_G2) m |= bit(XS_G2);
+                else if (ad == AD_G3) m |= bit(XS_G3);
+                break;  // W: no XS type
+            default: break;
+        }
+    }
+    return m;
+}
+
+void bias_atom_multiplicity(const BiasElement& b, unsigned char mult[XS_SIZE]) {
+    for (int t = 0; t < XS_SIZE; ++t) mult[t] = 0;
+    auto add = [&](int t) {
+        if (mult[t] < 255) ++mult[t];
+    };
+    if (b.type == BIAS_ACC) {
+        for (int t : {XS_O_A, XS_N_A, XS_O_DA, XS_N_DA}) add(t);
+        return;
+    }
+    if (b.type != BIAS_MAP) return;  // donor: no polar H in XS scoring; aromatic: CG types never remain
+    if (b.ad_list.empty()) {  // every scored atom (glue atoms are not scored)
+        for (int t = 0; t < XS_SIZE; ++t) add(t);
+        return;
+    }
+    for (int ad : b.ad_list) {
+        switch (ad_to_el(ad)) {
+            case EL_C: add(XS_C_P); add(XS_C_H); break;  // atoms' CG types were folded into C_H / C_P
+            case EL_N: for (int t : {XS_N_DA, XS_N_A, XS_N_D, XS_N_P}) add(t); break;
+            case EL_O: for (int t : {XS_O_DA, XS_O_A, XS_O_D, XS_O_P}) add(t); break;
+            case EL_S: add(XS_S_P); break;
+            case EL_P: add(XS_P_P); break;
+            case EL_F: add(XS_F_H); break;
+            case EL_Cl: add(XS_Cl_H); break;
+            case EL_Br: add(XS_Br_H); break;
+            case EL_I: add(XS_I_H); break;
+            case EL_Si: add(XS_Si); break;
+            case EL_At: add(XS_At); break;
+            case EL_Met: add(XS_Met_D); break;
+            default: break;  // hydrogen, glue and W select no scored atom
+        }
+    }
+    for (int t : {XS_C_H_CG0, XS_C_H_CG1, XS_C_H_CG2, XS_C_H_CG3}) mult[t] = mult[XS_C_H];
+    for (int t : {XS_C_P_CG0, XS_C_P_CG1, XS_C_P_CG2, XS_C_P_CG3}) mult[t] = mult[XS_C_P];
 }
 
 }  // namespace ud

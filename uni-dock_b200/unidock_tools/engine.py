@@ -81,6 +81,8 @@ def lib():
                                    C.c_int),
         "ud_refine": ([vp, ip, fp, C.c_int, C.c_int, C.c_int, fp, vp], C.c_int),
         "ud_batch_reset": ([vp, C.POINTER(vp), C.c_int, vp], C.c_int),
+        "ud_maps_add_bias": ([vp, C.c_char_p, C.c_size_t, vp], C.c_int),
+        "ud_batch_set_bias": ([vp, C.c_int, C.c_char_p, C.c_size_t], C.c_int),
         "ud_score_terms_receptor": ([vp, ip, fp, C.c_int, C.c_int, fp, vp], C.c_int),
         "ud_ligand_write": ([vp, fp, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
         "ud_ligand_counts": ([vp, ip], C.c_int),
@@ -258,6 +260,11 @@ class Maps:
         self.sf = sf
         return self
 
+    def add_bias(self, bpf: str):
+        """Add AutoDock-bias style wells (BPF text) to the maps (ud_maps_add_bias, --bias)."""
+        b = bpf.encode()
+        _check(lib().ud_maps_add_bias(self.h, b, len(b), None))
+
     def write(self, prefix):
         """AutoGrid .map files <prefix>.<type>.map (ud_maps_write)."""
         _check(lib().ud_maps_write(self.h, str(prefix).encode()))
@@ -369,6 +376,11 @@ class Batch:
         _check(lib().ud_batch_create(maps.h, arr, len(self.ligands), None, C.byref(h)))
         self.h = h
         self.max_torsions = max([l.n_torsions for l in self.ligands] + [0])
+
+    def set_bias(self, lig, bpf: str):
+        """Ligand `lig`'s own bias wells for receptor-atom scoring (ud_batch_set_bias, --multi_bias)."""
+        b = bpf.encode()
+        _check(lib().ud_batch_set_bias(self.h, int(lig), b, len(b)))
 
     def reset(self, ligands, stream=None):
         """Reuse this batch's handle and device buffers for other ligands
