@@ -100,7 +100,10 @@ int ud_maps_destroy(ud_maps maps);
  * Replaces parse_ligand_from_file_no_failure with hydrogens kept, as the
  * reference CLI calls it (unidock/src/lib/parse_pdbqt.cpp:1076-1140,
  * unidock/src/main/main.cpp:858-863) + model::initialize
- * (unidock/src/lib/model.cpp:613-619). */
+ * (unidock/src/lib/model.cpp:613-619).  A ligand with more than 48 torsions
+ * or 256 atoms returns UD_ERR_CAPACITY, as the reference refuses more than
+ * MAX_NUM_OF_LIG_TORSION torsions and MAX_NUM_OF_ATOMS (150) atoms
+ * (parse_pdbqt.cpp:1107-1120); the same holds for the two calls below. */
 int ud_ligand_parse(const char* text, size_t len, ud_ligand* out);
 /* SDF record with the fragInfo / torsionInfo / atomInfo properties of the
  * reference's ligand preparation.  keep_h = 0 leaves atoms of AutoDock type H

@@ -93,6 +93,24 @@ def test_batch_docking_writes_one_output_per_ligand(inputs):
 
 
 @pytest.mark.gpu
+def test_oversized_ligand_is_skipped_alone(inputs, tmp_path):
+    """A ligand over the torsion limit is reported and skipped; the rest of the
+    screen is docked (parse_ligand_from_file_no_failure, parse_pdbqt.cpp:1107-1113)."""
+    d, names = inputs
+    big = tmp_path / "big.pdbqt"
+    big.write_text(synth.make_ligand(200, 49, seed=8).to_pdbqt())
+    out = tmp_path / "out"
+    out.mkdir()
+    r = run("--receptor", d / "rec.pdbqt", "--gpu_batch", names[0], big, names[1], "--dir", out,
+            "--exhaustiveness", 8, "--max_step", 5, "--seed", 2, *box_args())
+    assert r.returncode == 0, r.stderr
+    assert "skipping ligand" in r.stderr and "exceeds max torsion counts" in r.stderr
+    assert not (out / "big_out.pdbqt").exists()
+    for p in names[:2]:
+        assert (out / (p.stem + "_out.pdbqt")).read_text().startswith("MODEL 1\nREMARK VINA RESULT:")
+
+
+@pytest.mark.gpu
 def test_single_ligand_default_output_and_modes_table(inputs):
     d, names = inputs
     r = run("--receptor", d / "rec.pdbqt", "--ligand", names[0], "--exhaustiveness", 8, "--max_step", 10,

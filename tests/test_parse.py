@@ -125,3 +125,29 @@ def test_malformed_inputs_raise():
         engine.Ligand(good.replace("TORSDOF", "REMARK"))      # missing TORSDOF
     with pytest.raises(engine.UdError):
         engine.Ligand(good.replace("ENDBRANCH", "ENDBRANCH 99", 1))
+
+
+def test_size_limits_refused_at_parse(tmp_path):
+    """48 torsions is the largest ligand the reference takes
+    (parse_pdbqt.cpp:1107-1113); one more is refused at parse, by both, so a
+    screen skips that ligand alone.  Atoms: the engine takes up to 256 (the
+    reference 150)."""
+    ok = synth.make_ligand(140, 48, seed=7)
+    L = engine.Ligand(ok.to_pdbqt())
+    assert L.n_torsions == 48 and L.n_atoms <= 256
+    over = synth.make_ligand(200, 49, seed=8).to_pdbqt()
+    with pytest.raises(engine.UdError) as e:
+        engine.Ligand(over)
+    assert e.value.code == engine.UD_ERR_CAPACITY and "torsion" in str(e.value)
+    big = synth.make_ligand(250, 10, seed=9).to_pdbqt()   # 277 atoms with polar H
+    with pytest.raises(engine.UdError) as e:
+        engine.Ligand(big)
+    assert e.value.code == engine.UD_ERR_CAPACITY and "atom" in str(e.value)
+    with pytest.raises(engine.UdError) as e:
+        engine.parse_ligands([ok.to_pdbqt(), over, big])
+    assert e.value.code == engine.UD_ERR_CAPACITY and "2 of 3" in str(e.value)
+    if ref.available():
+        p = tmp_path / "over.pdbqt"
+        p.write_text(over)
+        with pytest.raises(RuntimeError):
+            ref.RefLigand(p)

@@ -743,11 +743,25 @@ extern "C" int ud_maps_destroy(ud_maps maps) {
 
 static int ligand_local_steps(const Ligand& L) { return (25 + (int)L.atoms.size()) / 3; }
 
+// A ligand beyond the search's limits is refused when it is parsed, so that a
+// screen skips it alone (parse_ligand_from_file_no_failure refuses more than
+// MAX_NUM_OF_LIG_TORSION torsions and MAX_NUM_OF_ATOMS atoms the same way,
+// parse_pdbqt.cpp:1107-1120; the atom limit here is 256, the reference's 150).
+static Ligand within_limits(Ligand L) {
+    if (L.n_torsions() > kMaxLigTorsions)
+        throw Error(UD_ERR_CAPACITY, "ligand exceeds max torsion counts: " + std::to_string(L.n_torsions()) +
+                                         " > " + std::to_string(kMaxLigTorsions));
+    if ((int)L.atoms.size() > kMaxLigAtoms)
+        throw Error(UD_ERR_CAPACITY, "ligand exceeds max atom counts: " + std::to_string(L.atoms.size()) + " > " +
+                                         std::to_string(kMaxLigAtoms));
+    return L;
+}
+
 extern "C" int ud_ligand_parse(const char* text, size_t len, ud_ligand* out) {
     return guarded([&] {
         if (!text || !out) throw Error(UD_ERR_ARG, "null argument");
         auto h = std::make_unique<ud_ligand_s>();
-        h->lig = parse_ligand(std::string(text, len));
+        h->lig = within_limits(parse_ligand(std::string(text, len)));
         *out = h.release();
     });
 }
@@ -756,7 +770,7 @@ extern "C" int ud_ligand_parse_sdf(const char* sdf, size_t len, int keep_h, ud_l
     return guarded([&] {
         if (!sdf || !out) throw Error(UD_ERR_ARG, "null argument");
         auto h = std::make_unique<ud_ligand_s>();
-        h->lig = parse_ligand_sdf(std::string(sdf, len), keep_h != 0);
+        h->lig = within_limits(parse_ligand_sdf(std::string(sdf, len), keep_h != 0));
         *out = h.release();
     });
 }
@@ -776,7 +790,7 @@ extern "C" int ud_ligand_parse_many(const char* const* texts, const size_t* lens
                     try {
                         if (!texts[i]) throw Error(UD_ERR_ARG, "null text");
                         auto h = std::make_unique<ud_ligand_s>();
-                        h->lig = parse_ligand(std::string(texts[i], lens[i]));
+                        h->lig = within_limits(parse_ligand(std::string(texts[i], lens[i])));
                         out[i] = h.release();
                     } catch (const Error& e) {
                         code = e.code;
@@ -1786,10 +1800,11 @@ static void search_launch(ud_batch b, const ud_search_params* params, cudaStream
         if (P.exhaustiveness < 1) throw Error(UD_ERR_ARG, "exhaustiveness must be >= 1");
         if (P.chains_per_block < 0 || P.chains_per_block > 4)
             throw Error(UD_ERR_ARG, "chains_per_block must be 0 (default / autotuned) or 1..4");
+        const int n_lig = (int)b->ligs.size();
+        if (n_lig == 0) throw Error(UD_ERR_ARG, "empty batch");
         b->params = P;
         b->searched = false;
         b->text_ready[0] = b->text_ready[1] = false;
-        const int n_lig = (int)b->ligs.size();
         const int E = P.exhaustiveness;
         b->exhaustiveness = E;
         b->pose_stride = 7 + b->max_tors;
