@@ -50,7 +50,9 @@ def parse_args():
     ap.add_argument("--plain-sample", type=int, default=32, help="ligands timed in the plain form")
     ap.add_argument("--cpu-sample", type=int, default=16, help="ligands timed on the reference CPU path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--chains-per-block", type=int, default=0)
+    ap.add_argument("--chains-per-block", type=int, default=0, help="warps per CTA (0 = 4)")
+    ap.add_argument("--lanes-per-chain", type=int, default=0, choices=[0, 16, 32],
+                    help="32 = a warp per chain, 16 = two chains per warp (0 = 32)")
     ap.add_argument("--refine-step", type=int, default=3,
                     help="rounds of refinement against the receptor atoms per mode (0: grid energies only)")
     ap.add_argument("--adjoint-poses", type=int, default=ADJOINT_POSES,
@@ -75,7 +77,8 @@ def profile_case(args):
             synth.ligand_set(args.profile_case, seed=20261203, heavy=(12, 48), torsions=(0, 10))]
     b = engine.Batch(maps, ligs)
     P = dict(exhaustiveness=EXHAUSTIVENESS, max_step=MAX_STEP, seed=42, form=1,
-             chains_per_block=args.chains_per_block, refine_step=args.refine_step)
+             chains_per_block=args.chains_per_block, lanes_per_chain=args.lanes_per_chain,
+             refine_step=args.refine_step)
     for _ in range(2):
         b.search_launch(**P)
         torch.cuda.synchronize()
@@ -179,7 +182,8 @@ def run_ours(args, rank, world):
     # refine_step 3: the modes are refined and rescored against the receptor
     # atoms, as the reference's CLI does by default
     P = dict(exhaustiveness=EXHAUSTIVENESS, max_step=MAX_STEP, num_modes=9, min_rmsd=1.0, seed=42, form=1,
-             chains_per_block=args.chains_per_block, use_graph=1, refine_step=args.refine_step)
+             chains_per_block=args.chains_per_block, lanes_per_chain=args.lanes_per_chain, use_graph=1,
+             refine_step=args.refine_step)
 
     # ---- device-resident form: topology uploaded and the search set up (result
     # buffers, ligand order, captured graph) before the timed region
@@ -338,6 +342,7 @@ def run_ours(args, rank, world):
                                    "3000-atom receptor, 22.5 A box at 0.375 A (61^3)",
                        "ligands_per_step": B * world, "exhaustiveness": EXHAUSTIVENESS, "max_step": MAX_STEP,
                        "refine_step": args.refine_step,
+                       "warps_per_cta": args.chains_per_block or 4, "lanes_per_chain": args.lanes_per_chain or 32,
                        "form": "batched persistent", "l2": "flushed between timed steps (256 MB write)",
                        "parallelism": f"ligand shards x{world}" if world > 1 else "1 GPU"},
             "plain_form_ligands_per_s": None if plain is None else round(plain, 3),
@@ -435,7 +440,7 @@ def run_uneven(args, sf_name):
     texts = [l.to_pdbqt() for l in synth.ligand_set(per_step * steps_total, seed=8192, dist="lognormal",
                                                       with_charges=(sf_name == "ad4"))]
     P = dict(exhaustiveness=512, max_step=40, seed=42, form=1, use_graph=1, chains_per_block=0, bfgs_cap=-1,
-             refine_step=args.refine_step)
+             lanes_per_chain=0, refine_step=args.refine_step)
     batches, tunes = [], []
     for s in range(steps_total):
         ligs = engine.parse_ligands(texts[s * per_step:(s + 1) * per_step])
@@ -465,7 +470,8 @@ def run_uneven(args, sf_name):
             "config": {"workload": f"uneven-size screen, {sf_name}, search_mode detail (exhaustiveness 512, "
                                    "max_step 40), lognormal sizes (median 28 heavy, 8..80), 3000-atom receptor, "
                                    "22.5 A box", "ligands_per_step": per_step,
-                       "autotuned": {k: tune[k] for k in ("chains_per_block", "bfgs_cap", "energy_shift",
+                       "autotuned": {k: tune[k] for k in ("chains_per_block", "lanes_per_chain", "bfgs_cap",
+                                                          "energy_shift",
                                                           "ligands_per_s", "base_ligands_per_s")}}}
 
 

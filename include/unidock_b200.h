@@ -235,7 +235,7 @@ typedef struct {
     float energy_range;     /* output energy window (--energy_range) */
     unsigned long long seed;/* --seed */
     int form;               /* 0 = plain (one launch per ligand), 1 = batched persistent */
-    int chains_per_block;   /* chains (warps) per CTA, 1..4; 0 = the batch's autotuned value, else 4 */
+    int chains_per_block;   /* warps per CTA, 1..4; 0 = the batch's autotuned value, else 4 */
     int bfgs_cap;           /* 0 = per-ligand (25 + atoms)/3 BFGS steps; >0 caps it;
                                <0 = the batch's autotuned cap (per-ligand when not tuned) */
     int use_graph;          /* batched form: the per-batch sequence (queue reset, search
@@ -247,12 +247,15 @@ typedef struct {
                                default 3; vina.h:251-272).  Vina / Vinardo maps built
                                from a receptor only; otherwise, and at 0, the modes keep
                                their grid energies (--no_refine). */
+    int lanes_per_chain;    /* batched form: 32 = one chain per warp, 16 = two chains per
+                               warp (half a warp each); 0 = the batch's autotuned value,
+                               else 32.  The plain form ignores it. */
 } ud_search_params;
 
 /* Launch configuration picked by ud_autotune. */
 typedef struct {
-    int chains_per_block;      /* chains (warps) per CTA */
-    int lanes_per_chain;       /* lanes per chain (32: one warp per chain in this build) */
+    int chains_per_block;      /* warps per CTA */
+    int lanes_per_chain;       /* lanes per chain: 32 (a warp) or 16 (half a warp) */
     int bfgs_cap;              /* BFGS iteration cap, 0 = per-ligand */
     int n_sample;              /* ligands of the batch in the tuning sample */
     int n_tried;               /* configurations timed */
@@ -263,11 +266,13 @@ typedef struct {
 
 /* Autotuner (no counterpart in the reference): times the batched search on a
  * sample of the batch (ligands spread over its size order, enough chains to
- * fill the GPU twice, the caller's exhaustiveness, at most 40 MC steps) for
- * chains-per-CTA in {4, 2, 1} and BFGS caps in {per-ligand, 16, 10, 6}, and
+ * fill the GPU twice, the caller's exhaustiveness, at most 40 MC steps):
+ * first the launch shape, warps per CTA in {4, 2, 1} x lanes per chain in
+ * {32, 16}, uncapped; then BFGS caps in {16, 10, 6} on the shape picked.  It
  * keeps the fastest configuration whose mean best energy is within 0.1
- * kcal/mol of the default's.  Searches of this batch with chains_per_block = 0
- * and bfgs_cap < 0 then use it.  Synchronous; takes about 12 short searches. */
+ * kcal/mol of the default's (4 warps, 32 lanes, no cap).  Searches of this
+ * batch with chains_per_block = 0, lanes_per_chain = 0 and bfgs_cap < 0 then
+ * use it.  Synchronous; takes about 10 short searches. */
 int ud_autotune(ud_batch batch, const ud_search_params* params, ud_tune_result* out, void* stream);
 
 /* Run the Monte-Carlo + BFGS search of every ligand of the batch.

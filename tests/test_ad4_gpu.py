@@ -96,9 +96,10 @@ def test_ad4_energy_and_gradient_match_reference(ad4, v):
     assert not errs["clash"] or max(errs["clash"]) <= CLASH_REL
 
 
-def test_ad4_search_chain_energy_is_pose_energy(ad4):
+@pytest.mark.parametrize("lanes", [32, 16])
+def test_ad4_search_chain_energy_is_pose_energy(ad4, lanes):
     B, ligs = ad4["B"], ad4["ligs"]
-    B.search(exhaustiveness=8, max_step=10, seed=2, form=1)
+    B.search(exhaustiveness=8, max_step=10, seed=2, form=1, lanes_per_chain=lanes)
     poses, e, ev = B.chains()
     assert np.all(np.isfinite(e)) and np.all(ev > 0)
     e2, _ = B.score_grad(np.repeat(np.arange(len(ligs)), 8), poses, 1000.0, 1000.0)

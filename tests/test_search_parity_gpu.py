@@ -37,8 +37,10 @@ def gold(request):
     return g, maps
 
 
-@pytest.mark.parametrize("li", [0, 1, 2, 3])
-def test_best_energy_median_matches_reference(gold, li):
+# every ligand with one chain per warp; two of them with two chains per warp
+# (16 lanes a chain: the same random streams, another FP32 summation order)
+@pytest.mark.parametrize("li,lanes", [(0, 32), (1, 32), (2, 32), (3, 32), (0, 16), (2, 16)])
+def test_best_energy_median_matches_reference(gold, li, lanes):
     g, maps = gold
     runs, E = g["chain_e"].shape[1], int(g["exhaustiveness"])
     L = engine.Ligand(str(g["ligand_pdbqt"][li]))
@@ -47,7 +49,7 @@ def test_best_energy_median_matches_reference(gold, li):
     # same MC budget as the reference run (vina.h:191-204 heuristic, no max_step cap)
     assert 70 * 3 * (50 + L.n_atoms + 10 * (6 + T)) // 2 == int(g["global_steps"][li])
     B = engine.Batch(maps, [L] * runs)
-    B.search(exhaustiveness=E, max_step=0, seed=2024 + li, form=1)
+    B.search(exhaustiveness=E, max_step=0, seed=2024 + li, form=1, lanes_per_chain=lanes)
     poses, e, _ = B.chains()
     e = e.reshape(runs, E)
     ours = e.min(axis=1)
@@ -61,7 +63,7 @@ def test_best_energy_median_matches_reference(gold, li):
     theirs_best = g["chain_pose"][li][np.arange(runs), g["chain_e"][li].argmin(axis=1), :7 + T]
     r_ours = [heavy_rmsd(L, heavy, p, ref_best) for p in ours_best]
     r_theirs = [heavy_rmsd(L, heavy, p, ref_best) for p in theirs_best]
-    print(f"ligand {li}: {L.n_atoms} atoms {T} torsions; median best GPU {np.median(ours):.3f} "
+    print(f"ligand {li} ({lanes} lanes a chain): {L.n_atoms} atoms {T} torsions; median best GPU {np.median(ours):.3f} "
           f"reference {np.median(theirs):.3f} (diff {d:+.3f}); min GPU {ours.min():.3f} ref {theirs.min():.3f}; "
           f"median RMSD to reference best: GPU {np.median(r_ours):.2f} A, reference runs {np.median(r_theirs):.2f} A")
     assert abs(d) <= TOL, (np.sort(ours), np.sort(theirs))

@@ -234,6 +234,7 @@ struct ud_batch_s {
     // launch configuration picked by ud_autotune for this batch
     bool tuned = false;
     int tuned_chains_per_block = 4;
+    int tuned_lanes_per_chain = 32;
     int tuned_bfgs_cap = 0;
 
     void drop_graph() {
@@ -1743,7 +1744,7 @@ static void search_graph(ud_batch b, const SearchParams& sp, int n_chain, int bl
     b->hp_results.alloc((size_t)n_chain);
     std::ostringstream k;
     k << n_chain << ' ' << blocks << ' ' << sp.global_steps << ' ' << sp.exhaustiveness << ' ' << sp.seed << ' '
-      << sp.chains_per_block << ' ' << sp.bfgs_cap << ' ' << (const void*)b->d_poses.p << ' '
+      << sp.chains_per_block << ' ' << sp.lanes_per_chain << ' ' << sp.bfgs_cap << ' ' << (const void*)b->d_poses.p << ' '
       << (const void*)b->d_results.p << ' ' << (const void*)b->d_queue.p << ' ' << (const void*)b->d_order.p << ' '
       << (const void*)b->hp_poses.p << ' ' << (const void*)b->hp_results.p << ' ' << (const void*)b->maps->maps.p
       << ' ' << (const void*)b->maps->smooth.p << ' ' << b->mode_cap << ' ' << b->refined << ' '
@@ -1800,6 +1801,8 @@ static void search_launch(ud_batch b, const ud_search_params* params, cudaStream
         if (P.exhaustiveness < 1) throw Error(UD_ERR_ARG, "exhaustiveness must be >= 1");
         if (P.chains_per_block < 0 || P.chains_per_block > 4)
             throw Error(UD_ERR_ARG, "chains_per_block must be 0 (default / autotuned) or 1..4");
+        if (P.lanes_per_chain != 0 && P.lanes_per_chain != 16 && P.lanes_per_chain != 32)
+            throw Error(UD_ERR_ARG, "lanes_per_chain must be 0 (default / autotuned), 16 or 32");
         const int n_lig = (int)b->ligs.size();
         if (n_lig == 0) throw Error(UD_ERR_ARG, "empty batch");
         b->params = P;
@@ -1822,8 +1825,11 @@ static void search_launch(ud_batch b, const ud_search_params* params, cudaStream
         sp.authentic_v = 1000.0f;
         sp.temperature = 1.2f;
         sp.mutation_amplitude = 2.0f;
-        sp.lanes_per_chain = 32;
+        // the plain form keeps one chain per warp (the fixed tiling it stands for)
+        sp.lanes_per_chain = P.form != 1 ? 32
+                             : P.lanes_per_chain > 0 ? P.lanes_per_chain : (b->tuned ? b->tuned_lanes_per_chain : 32);
         sp.chains_per_block = P.chains_per_block > 0 ? P.chains_per_block : (b->tuned ? b->tuned_chains_per_block : 4);
+        const int chains_per_cta = sp.chains_per_block * (32 / sp.lanes_per_chain);
         sp.persistent = P.form == 1 ? 1 : 0;
         sp.bfgs_cap = P.bfgs_cap >= 0 ? P.bfgs_cap : (b->tuned ? b->tuned_bfgs_cap : 0);
         int dev = 0, n_sm = 148;
@@ -1835,9 +1841,8 @@ static void search_launch(ud_batch b, const ud_search_params* params, cudaStream
         }
         b->graph_results = false;
         if (sp.persistent && P.use_graph && modes) {
-            int per_sm = search_blocks_per_sm(b->view(), sp.chains_per_block);
-            int blocks = std::max(1, std::min(per_sm * n_sm, (int)((n_chain + sp.chains_per_block - 1) /
-                                                                    sp.chains_per_block)));
+            int per_sm = search_blocks_per_sm(b->view(), sp.chains_per_block, sp.lanes_per_chain);
+            int blocks = std::max(1, std::min(per_sm * n_sm, (int)((n_chain + chains_per_cta - 1) / chains_per_cta)));
             search_graph(b, sp, (int)n_chain, blocks);
             if (!launch) return;
             cudaEventRecord(b->ev0, s);
@@ -1851,9 +1856,9 @@ static void search_launch(ud_batch b, const ud_search_params* params, cudaStream
         cudaEventRecord(b->ev0, s);
         if (sp.persistent) {
             cuda_check(cudaMemsetAsync(b->d_queue.p, 0, sizeof(unsigned int), s), "queue reset");
-            int per_sm = search_blocks_per_sm(b->view(), sp.chains_per_block);
+            int per_sm = search_blocks_per_sm(b->view(), sp.chains_per_block, sp.lanes_per_chain);
             int blocks = per_sm * n_sm;
-            int needed = (int)((n_chain + sp.chains_per_block - 1) / sp.chains_per_block);
+            int needed = (int)((n_chain + chains_per_cta - 1) / chains_per_cta);
             blocks = std::max(1, std::min(blocks, needed));
             cuda_check(launch_search(b->view(), maps_view(b->maps), tables_view(b->maps), sp, b->d_order.p,
                                      (int)n_chain, 0, b->d_queue.p, b->d_poses.p, b->pose_stride, b->d_results.p,
@@ -2033,7 +2038,8 @@ extern "C" int ud_autotune(ud_batch b, const ud_search_params* params, ud_tune_r
         int dev = 0, n_sm = 148;
         cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
         cuda_check(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev), "device attribute");
-        const long long resident = (long long)search_blocks_per_sm(b->view(), 4) * n_sm * 4;
+        // chains resident at once with two chains per warp (the larger count)
+        const long long resident = (long long)search_blocks_per_sm(b->view(), 4, 16) * n_sm * 8;
         const int S = (int)std::max<long long>(1, std::min<long long>({(2 * resident + E - 1) / E, n_lig, 512}));
         std::vector<const Ligand*> sample;
         for (int i = 0; i < S; ++i) sample.push_back(b->ligs[order[(size_t)i * n_lig / S]]);
@@ -2044,37 +2050,47 @@ extern "C" int ud_autotune(ud_batch b, const ud_search_params* params, ud_tune_r
         // tuning budget: the caller's MC step cap, or at most 40 steps per chain
         if (tp.max_step <= 0 || tp.max_step > 40) tp.max_step = 40;
         const int cpbs[] = {4, 2, 1};
-        const int caps[] = {0, 16, 10, 6};
+        const int lanes[] = {32, 16};
+        const int caps[] = {16, 10, 6};
         std::vector<float> base, cur;
         tp.chains_per_block = 4;
+        tp.lanes_per_chain = 32;
         tp.bfgs_cap = 0;
         trial_search(tb.get(), tp, s, cur);                 // warm-up (module load, caches)
         float base_ms = trial_search(tb.get(), tp, s, base);
-        int best_cpb = 4, best_cap = 0, tried = 1;
+        int best_cpb = 4, best_lanes = 32, best_cap = 0, tried = 1;
         float best_ms = base_ms, best_shift = 0.0f;
-        for (int cap : caps)
-            for (int cpb : cpbs) {
-                if (cap == 0 && cpb == 4) continue;
-                tp.chains_per_block = cpb;
-                tp.bfgs_cap = cap;
-                const float ms = trial_search(tb.get(), tp, s, cur);
-                ++tried;
-                double shift = 0;
-                for (int i = 0; i < S; ++i) shift += (double)cur[i] - (double)base[i];
-                shift /= S;
-                // accept only configurations whose search quality holds
-                if (shift <= 0.1 && ms < best_ms) {
-                    best_ms = ms;
-                    best_cpb = cpb;
-                    best_cap = cap;
-                    best_shift = (float)shift;
-                }
+        auto trial = [&](int cpb, int ln, int cap) {
+            tp.chains_per_block = cpb;
+            tp.lanes_per_chain = ln;
+            tp.bfgs_cap = cap;
+            const float ms = trial_search(tb.get(), tp, s, cur);
+            ++tried;
+            double shift = 0;
+            for (int i = 0; i < S; ++i) shift += (double)cur[i] - (double)base[i];
+            shift /= S;
+            // accept only configurations whose search quality holds
+            if (shift <= 0.1 && ms < best_ms) {
+                best_ms = ms;
+                best_cpb = cpb;
+                best_lanes = ln;
+                best_cap = cap;
+                best_shift = (float)shift;
             }
+        };
+        // launch shape first (warps per CTA x lanes per chain), uncapped; then
+        // the BFGS caps on the shape picked
+        for (int ln : lanes)
+            for (int cpb : cpbs)
+                if (!(cpb == 4 && ln == 32)) trial(cpb, ln, 0);
+        const int shape_cpb = best_cpb, shape_lanes = best_lanes;
+        for (int cap : caps) trial(shape_cpb, shape_lanes, cap);
         b->tuned = true;
         b->tuned_chains_per_block = best_cpb;
+        b->tuned_lanes_per_chain = best_lanes;
         b->tuned_bfgs_cap = best_cap;
         out->chains_per_block = best_cpb;
-        out->lanes_per_chain = 32;
+        out->lanes_per_chain = best_lanes;
         out->bfgs_cap = best_cap;
         out->n_sample = S;
         out->n_tried = tried;

@@ -158,6 +158,27 @@ __device__ __forceinline__ float warp_sum(float v) {
     return v;
 }
 
+// A chain runs on kW lanes: the whole warp (32) or one half of it (16), the
+// two halves of a warp then being two independent chains.  Masks, sums and
+// barriers below involve only the calling chain's lanes.
+template <int kW>
+__device__ __forceinline__ unsigned lanes_mask() {
+    static_assert(kW == 32 || kW == 16, "a chain spans a warp or half a warp");
+    if constexpr (kW == 32) return kFull;
+    else return 0xFFFFu << (threadIdx.x & 16);
+}
+
+template <int kW>
+__device__ __forceinline__ float lanes_sum(float v) {
+    const unsigned m = lanes_mask<kW>();
+#pragma unroll
+    for (int o = kW / 2; o > 0; o >>= 1) v += __shfl_xor_sync(m, v, o);
+    return v;
+}
+
+template <int kW>
+__device__ __forceinline__ void lanes_sync() { __syncwarp(lanes_mask<kW>()); }
+
 // ---------------------------------------------------------------- data views
 struct Batch {
     const LigDesc* ligs;
@@ -258,6 +279,7 @@ struct Ctx {
     int lig;
 };
 
+template <int kW = 32>
 __device__ __forceinline__ Ctx make_ctx(const Batch& B, int lig, float* s) {
     Ctx c;
     const LigDesc* d = B.ligs + lig;
@@ -275,7 +297,7 @@ __device__ __forceinline__ Ctx make_ctx(const Batch& B, int lig, float* s) {
     c.n_pairs = __ldg(&d->n_pairs);
     c.max_depth = __ldg(&d->max_depth);
     c.local_steps = __ldg(&d->local_steps);
-    c.lane = threadIdx.x & 31;
+    c.lane = threadIdx.x & (kW - 1);
     c.lig = lig;
     return c;
 }
@@ -288,11 +310,12 @@ __device__ __forceinline__ Ctx make_ctx(const Batch& B, int lig, float* s) {
 // quaternions are formed in one parallel pass and each tree level only
 // composes q_parent * t (equal to axis_angle(R_parent rel_axis, theta) * q_parent
 // of tree.h:116-128 for unit quaternions).
+template <int kW = 32>
 __device__ __forceinline__ void kinematics(const Ctx& c, const Layout& L, const float* conf) {
     float* fr = c.s + L.frames;
     // frame layout (20 floats): origin[0..2] q[3..6] R[7..15] lab axis[16..18];
     // [16..19] hold the local torsion quaternion until the node is composed
-    for (int n = 1 + c.lane; n < c.R; n += 32) {
+    for (int n = 1 + c.lane; n < c.R; n += kW) {
         const NodeRec* nr = c.nodes + n;
         float ra[3] = {__ldg(&nr->rel_axis[0]), __ldg(&nr->rel_axis[1]), __ldg(&nr->rel_axis[2])};
         axis_angle_q(ra, conf[7 + n - 1], fr + 20 * n + 16);
@@ -302,9 +325,9 @@ __device__ __forceinline__ void kinematics(const Ctx& c, const Layout& L, const 
         fr[3] = conf[3]; fr[4] = conf[4]; fr[5] = conf[5]; fr[6] = conf[6];
         q_to_r3(fr + 3, fr + 7);
     }
-    __syncwarp();
+    lanes_sync<kW>();
     for (int d = 1; d <= c.max_depth; ++d) {
-        for (int n = 1 + c.lane; n < c.R; n += 32) {
+        for (int n = 1 + c.lane; n < c.R; n += kW) {
             const NodeRec* nr = c.nodes + n;
             if (__ldg(&nr->depth) != d) continue;
             const float* pf = fr + 20 * __ldg(&nr->parent);
@@ -324,10 +347,10 @@ __device__ __forceinline__ void kinematics(const Ctx& c, const Layout& L, const 
             f[3] = q[0]; f[4] = q[1]; f[5] = q[2]; f[6] = q[3];
             q_to_r3(q, f + 7);
         }
-        __syncwarp();
+        lanes_sync<kW>();
     }
     float4* xyz = reinterpret_cast<float4*>(c.s + L.coords);
-    for (int a = c.lane; a < c.n_atoms; a += 32) {
+    for (int a = c.lane; a < c.n_atoms; a += kW) {
         AtomRec ar = c.atoms[a];
         int n = ar.packed & 0xFF;
         const float* f = fr + 20 * n;
@@ -337,7 +360,7 @@ __device__ __forceinline__ void kinematics(const Ctx& c, const Layout& L, const 
         for (int i = 0; i < 3; ++i) o[i] = f[i] + (m[3 * i] * ar.x + m[3 * i + 1] * ar.y + m[3 * i + 2] * ar.z);
         xyz[a] = make_float4(o[0], o[1], o[2], 0.0f);
     }
-    __syncwarp();
+    lanes_sync<kW>();
 }
 
 // Trilinear map energy, gradient and out-of-box penalty of one atom.
@@ -511,17 +534,18 @@ __device__ __forceinline__ float receptor_term(const Receptor& R, const Tables& 
 // the computed energy, 2 factor (e_bin+1 - e_bin) per unit r^2).
 // With kReceptor the receptor term comes from the receptor atoms (`Rc`,
 // out-of-box slope `rslope`) instead of the maps.
-template <bool kExactPairs = false, bool kAD4 = false, bool kReceptor = false>
+template <bool kExactPairs = false, bool kAD4 = false, bool kReceptor = false, int kW = 32>
 __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const Maps& M,
                                             const Tables& Tb, const float* conf, float* g,
                                             float v_intra, float v_inter, const Receptor* Rc = nullptr,
                                             float rslope = 0.0f) {
-    kinematics(c, L, conf);
+    static_assert(!kReceptor || kW == 32, "receptor-atom terms use the whole warp");
+    kinematics<kW>(c, L, conf);
     const float4* xyz = reinterpret_cast<const float4*>(c.s + L.coords);
     float4* frc = reinterpret_cast<float4*>(c.s + L.forces);
     float e = 0;
-    for (int k = c.lane; k < c.n_atoms; k += 32) frc[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    __syncwarp();
+    for (int k = c.lane; k < c.n_atoms; k += kW) frc[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    lanes_sync<kW>();
     if constexpr (kReceptor) {
         const BiasRec* bias;
         int n_bias;
@@ -537,7 +561,7 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
             }
         }
     } else {
-        for (int k = c.lane; k < c.n_grid; k += 32) {
+        for (int k = c.lane; k < c.n_grid; k += kW) {
             const uint32_t ga = __ldg(c.grid + k);
             const int a = ga & 0xFF, slot = ga >> 8;
             float gx, gy, gz;
@@ -554,12 +578,16 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
             frc[a] = make_float4(gx, gy, gz, 0.0f);
         }
     }
-    __syncwarp();
+    lanes_sync<kW>();
     // Pairs in 32-slot groups made of kPairPasses lane ranges that are each a
-    // matching (no atom twice within a range): table rows of kPairBatch groups
-    // are loaded before any is consumed, then each range adds its forces in
-    // turn (no atomics, a fixed summation order).
-    const int n_groups = c.n_pairs >> 5;
+    // matching (no atom twice within a range), taken kW slots (a window of
+    // whole ranges) at a time: table rows of kPairBatch windows are loaded
+    // before any is consumed, then each range adds its forces in turn (no
+    // atomics, a fixed summation order).
+    static_assert(kW % kPairPassWidth == 0, "a window holds whole lane ranges");
+    constexpr int kWinShift = kW == 32 ? 5 : 4;
+    constexpr int kWinPasses = kW / kPairPassWidth;
+    const int n_groups = c.n_pairs >> kWinShift;   // windows; n_pairs is a multiple of 32
     for (int g0 = 0; g0 < n_groups; g0 += kPairBatch) {
         float4 tv[kPairBatch];
         float rv[kPairBatch][3];
@@ -569,7 +597,7 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
         for (int u = 0; u < kPairBatch; ++u) {
             prv[u] = kPairPad;
             if (g0 + u < n_groups) {
-                uint32_t pr = __ldg(c.pairs + ((g0 + u) << 5) + c.lane);
+                uint32_t pr = __ldg(c.pairs + ((g0 + u) << kWinShift) + c.lane);
                 if (pr != kPairPad) {
                     int a = pr & 0xFF, b = (pr >> 8) & 0xFF, tp = pr >> 16;
                     const float4 pa = xyz[a], pb = xyz[b];
@@ -582,7 +610,7 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
                         rv[u][0] = rx; rv[u][1] = ry; rv[u][2] = rz;
                         tv[u] = __ldg(Tb.smooth4 + (size_t)tp * Tb.n_bins + i1);
                         if constexpr (kAD4) {  // + q_a q_b E(r) + (|q_a| V_b + |q_b| V_a) G(r)
-                            const float2 cf = __ldg(c.coef + ((g0 + u) << 5) + c.lane);
+                            const float2 cf = __ldg(c.coef + ((g0 + u) << kWinShift) + c.lane);
                             const float4 te = __ldg(Tb.smooth4 + (size_t)kAd4RowE * Tb.n_bins + i1);
                             const float4 tg = __ldg(Tb.smooth4 + (size_t)kAd4RowG * Tb.n_bins + i1);
                             tv[u].x += cf.x * te.x + cf.y * tg.x;
@@ -615,7 +643,7 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
             }
             const int a = prv[u] & 0xFF, b = (prv[u] >> 8) & 0xFF;
 #pragma unroll
-            for (int pass = 0; pass < kPairPasses; ++pass) {
+            for (int pass = 0; pass < kWinPasses; ++pass) {
                 if (live && c.lane / kPairPassWidth == pass) {
                     float4 fa = frc[a], fb = frc[b];
                     fa.x -= fx; fa.y -= fy; fa.z -= fz;
@@ -623,11 +651,11 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
                     frc[a] = fa;
                     frc[b] = fb;
                 }
-                __syncwarp();
+                lanes_sync<kW>();
             }
         }
     }
-    e = warp_sum(e);
+    e = lanes_sum<kW>(e);
     // Force and torque of every subtree.  A subtree's atoms are contiguous in
     // DFS order, so inclusive prefix sums over atoms of f and of the moment
     // (x - o_root) x f give each subtree's sums as a difference of two
@@ -636,7 +664,8 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
     const float* fr = c.s + L.frames;
     float* pre = c.s + L.prefix;
     float carry[6] = {0, 0, 0, 0, 0, 0};
-    for (int base = 0; base < c.n_atoms; base += 32) {
+    const unsigned lanes = lanes_mask<kW>();
+    for (int base = 0; base < c.n_atoms; base += kW) {
         const int a = base + c.lane;
         float v[6] = {0, 0, 0, 0, 0, 0};
         if (a < c.n_atoms) {
@@ -649,24 +678,24 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
             v[5] = r0 * f1 - r1 * f0;
         }
 #pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
+        for (int off = 1; off < kW; off <<= 1) {
 #pragma unroll
             for (int q = 0; q < 6; ++q) {
-                const float t = __shfl_up_sync(kFull, v[q], off);
+                const float t = __shfl_up_sync(lanes, v[q], off, kW);
                 if (c.lane >= off) v[q] += t;
             }
         }
 #pragma unroll
         for (int q = 0; q < 6; ++q) {
             v[q] += carry[q];
-            carry[q] = __shfl_sync(kFull, v[q], 31);
+            carry[q] = __shfl_sync(lanes, v[q], kW - 1, kW);
         }
         if (a < c.n_atoms)
 #pragma unroll
             for (int q = 0; q < 6; ++q) pre[6 * a + q] = v[q];
     }
-    __syncwarp();
-    for (int n = c.lane; n < c.R; n += 32) {
+    lanes_sync<kW>();
+    for (int n = c.lane; n < c.R; n += kW) {
         const int span = __ldg(&c.nodes[n].atoms);
         const int b0 = span & 0xFFFF, b1 = span >> 16;
         const float* hi = pre + 6 * (b1 - 1);
@@ -685,16 +714,16 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
             g[6 + n - 1] = T0 * on[16] + T1 * on[17] + T2 * on[18];
         }
     }
-    __syncwarp();
+    lanes_sync<kW>();
     return e;
 }
 
 // Intramolecular energy from the nearest-bin `fast` table at curl cap v
 // (model::evali, model.cpp:927-933), summed over the warp.
-template <bool kAD4 = false>
+template <bool kAD4 = false, int kW = 32>
 __device__ __forceinline__ float intra_fast(const Ctx& c, const Tables& Tb, const float4* xyz, float v) {
     float ei = 0;
-    for (int k = c.lane; k < c.n_pairs; k += 32) {
+    for (int k = c.lane; k < c.n_pairs; k += kW) {
         uint32_t pr = __ldg(c.pairs + k);
         if (pr == kPairPad) continue;
         int a = pr & 0xFF, b = (pr >> 8) & 0xFF, tp = pr >> 16;
@@ -713,19 +742,19 @@ __device__ __forceinline__ float intra_fast(const Ctx& c, const Tables& Tb, cons
             ei += t;
         }
     }
-    return warp_sum(ei);
+    return lanes_sum<kW>(ei);
 }
 
 // Scoring-path energy (no gradient): grid with curl cap v, intramolecular
 // pairs from the nearest-bin `fast` table (model.cpp:867-886, cache.cpp:84-120).
-template <bool kAD4 = false>
+template <bool kAD4 = false, int kW = 32>
 __device__ __forceinline__ void eval_score(const Ctx& c, const Layout& L, const Maps& M,
                                            const Tables& Tb, const float* conf, float v,
                                            float& e_grid, float& e_intra) {
-    kinematics(c, L, conf);
+    kinematics<kW>(c, L, conf);
     const float4* xyz = reinterpret_cast<const float4*>(c.s + L.coords);
     float eg = 0;
-    for (int k = c.lane; k < c.n_grid; k += 32) {
+    for (int k = c.lane; k < c.n_grid; k += kW) {
         const uint32_t ga = __ldg(c.grid + k);
         float gx, gy, gz;
         const float4 pa = xyz[ga & 0xFF];
@@ -736,23 +765,26 @@ __device__ __forceinline__ void eval_score(const Ctx& c, const Layout& L, const 
             eg += fabsf(q) * grid_eval(M, M.d_slot, pa, v, gx, gy, gz, false);
         }
     }
-    e_grid = warp_sum(eg);
-    e_intra = intra_fast<kAD4>(c, Tb, xyz, v);
+    e_grid = lanes_sum<kW>(eg);
+    e_intra = intra_fast<kAD4, kW>(c, Tb, xyz, v);
 }
 
 // ---------------------------------------------------------------- BFGS pieces
+template <int kW = 32>
 __device__ __forceinline__ float dotw(const Ctx& c, const float* a, const float* b, int n) {
     float s = 0;
-    for (int i = c.lane; i < n; i += 32) s += a[i] * b[i];
-    return warp_sum(s);
+    for (int i = c.lane; i < n; i += kW) s += a[i] * b[i];
+    return lanes_sum<kW>(s);
 }
 
+template <int kW = 32>
 __device__ __forceinline__ void copyw(const Ctx& c, float* dst, const float* src, int n) {
-    for (int i = c.lane; i < n; i += 32) dst[i] = src[i];
-    __syncwarp();
+    for (int i = c.lane; i < n; i += kW) dst[i] = src[i];
+    lanes_sync<kW>();
 }
 
 // x_new = x + alpha * p in conformation space (conf.h:98-104, 146-150).
+template <int kW = 32>
 __device__ __forceinline__ void conf_increment(const Ctx& c, const float* x, const float* p,
                                                float alpha, float* out) {
     if (c.lane < 3) out[c.lane] = x[c.lane] + alpha * p[c.lane];
@@ -762,11 +794,11 @@ __device__ __forceinline__ void conf_increment(const Ctx& c, const float* x, con
         quaternion_increment(q, rot);
         out[3] = q[0]; out[4] = q[1]; out[5] = q[2]; out[6] = q[3];
     }
-    for (int t = c.lane; t < c.T; t += 32) {
+    for (int t = c.lane; t < c.T; t += kW) {
         float v = x[7 + t] + normalized_angle(alpha * p[6 + t]);
         out[7 + t] = normalized_angle(v);
     }
-    __syncwarp();
+    lanes_sync<kW>();
 }
 
 // The inverse Hessian is kept as a full symmetric n x n matrix (the reference
@@ -775,36 +807,39 @@ __device__ __forceinline__ void conf_increment(const Ctx& c, const float* x, con
 // row for n <= 16 measured no faster: the combining shuffle costs what the
 // shorter loops save.)
 // out = -H v
+template <int kW = 32>
 __device__ __forceinline__ void minus_hv(const Ctx& c, const float* H, const float* v, float* out, int n) {
-    for (int i = c.lane; i < n; i += 32) {
+    for (int i = c.lane; i < n; i += kW) {
         float sum = 0;
         for (int j = 0; j < n; ++j) sum += H[j * n + i] * v[j];
         out[i] = -sum;
     }
-    __syncwarp();
+    lanes_sync<kW>();
 }
 
+template <int kW = 32>
 __device__ __forceinline__ void h_identity(const Ctx& c, float* H, int n) {
-    for (int k = c.lane; k < n * n; k += 32) H[k] = 0;
-    __syncwarp();
-    for (int i = c.lane; i < n; i += 32) H[i * n + i] = 1;
-    __syncwarp();
+    for (int k = c.lane; k < n * n; k += kW) H[k] = 0;
+    lanes_sync<kW>();
+    for (int i = c.lane; i < n; i += kW) H[i * n + i] = 1;
+    lanes_sync<kW>();
 }
 
 // BFGS update of the inverse Hessian (bfgs.h:40-58), applied to both triangles
+template <int kW = 32>
 __device__ __forceinline__ void h_update(const Ctx& c, float* H, const float* p, const float* y,
                                          float* mhy, float alpha, int n) {
-    const float yp = dotw(c, y, p, n);
+    const float yp = dotw<kW>(c, y, p, n);
     if (alpha * yp < kEps) return;
-    minus_hv(c, H, y, mhy, n);
-    const float yhy = -dotw(c, y, mhy, n);
+    minus_hv<kW>(c, H, y, mhy, n);
+    const float yhy = -dotw<kW>(c, y, mhy, n);
     const float r = __frcp_rn(alpha * yp);
     const float a1 = alpha * r, a2 = alpha * alpha * (r * r * yhy + r);
-    for (int i = c.lane; i < n; i += 32) {
+    for (int i = c.lane; i < n; i += kW) {
         const float mi = mhy[i], pi = p[i];
         for (int j = 0; j < n; ++j) H[j * n + i] += a1 * (mi * p[j] + mhy[j] * pi) + a2 * pi * p[j];
     }
-    __syncwarp();
+    lanes_sync<kW>();
 }
 
 // ---------------------------------------------------------------- MC pieces
@@ -823,6 +858,7 @@ __device__ void random_inside_sphere(Philox& rng, float* v) {
 
 // Initial chain conformation: position uniform in the box, orientation a
 // normalised 4-D Gaussian, torsions uniform (conf.h:105-108,173-176; quaternion.cpp:116-126).
+template <int kW = 32>
 __device__ void random_conf(const Ctx& c, Philox& rng, const Maps& M, float* x) {
     if (c.lane == 0) {
         uint4 u = rng.next();
@@ -852,11 +888,12 @@ __device__ void random_conf(const Ctx& c, Philox& rng, const Maps& M, float* x) 
             for (int k = 0; k < 4 && t + k < c.T; ++k) x[7 + t + k] = -kPi + 2 * kPi * u01(w[k]);
         }
     }
-    __syncwarp();
+    lanes_sync<kW>();
 }
 
 // Mutation of one of {position, orientation, one torsion} (mutate.cpp:36-80);
 // the gyration radius uses the coordinates of the last evaluation.
+template <int kW = 32>
 __device__ void mutate(const Ctx& c, const Layout& L, Philox& rng, float amplitude, float* x) {
     float* misc = c.s + L.misc;
     if (c.lane == 0) {
@@ -868,14 +905,14 @@ __device__ void mutate(const Ctx& c, const Layout& L, Philox& rng, float amplitu
         misc[1] = sph[0]; misc[2] = sph[1]; misc[3] = sph[2];
         misc[4] = -kPi + 2 * kPi * u01(u.y);
     }
-    __syncwarp();
+    lanes_sync<kW>();
     const int which = __float_as_int(misc[0]);
     if (which == 1) {
         // gyration radius of heavy atoms about the root origin (model.cpp:853-865)
         const float4* xyz = reinterpret_cast<const float4*>(c.s + L.coords);
         const float* o = c.s + L.frames;
         float acc = 0, cnt = 0;
-        for (int a = c.lane; a < c.n_atoms; a += 32) {
+        for (int a = c.lane; a < c.n_atoms; a += kW) {
             int packed = __ldg(&c.atoms[a].packed);
             if ((packed >> 16) & 1) {
                 const float4 pa = xyz[a];
@@ -884,8 +921,8 @@ __device__ void mutate(const Ctx& c, const Layout& L, Philox& rng, float amplitu
                 cnt += 1;
             }
         }
-        acc = warp_sum(acc);
-        cnt = warp_sum(cnt);
+        acc = lanes_sum<kW>(acc);
+        cnt = lanes_sum<kW>(cnt);
         float gr = cnt > 0 ? sqrtf(acc / cnt) : 0;
         if (c.lane == 0 && gr > kEps) {
             float rot[3] = {amplitude / gr * misc[1], amplitude / gr * misc[2], amplitude / gr * misc[3]};
@@ -902,7 +939,7 @@ __device__ void mutate(const Ctx& c, const Layout& L, Philox& rng, float amplitu
             x[7 + which - 2] = misc[4];
         }
     }
-    __syncwarp();
+    lanes_sync<kW>();
 }
 
 // ---------------------------------------------------------------- chain driver
@@ -938,15 +975,16 @@ struct Machine {
 // The MC chain of monte_carlo.cu:237-356 (mutate, BFGS at the hunt cap,
 // Metropolis at temperature T, refine improvements at the authentic cap, keep
 // the best) with the line search and BFGS iterations of bfgs.h:63-146.
-template <bool kSearch, bool kAD4>
+template <bool kSearch, bool kAD4, int kW>
 __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const Tables& Tb,
                                             const SearchParams& P, const Layout& L, float* sw,
                                             const int* order, int n_items, int first_item,
                                             unsigned int* queue, float* poses, int pose_stride,
                                             ChainResult* results, const int* opt_lig, int opt_steps,
                                             float opt_v, float* opt_e, int* opt_evals) {
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & (kW - 1);
+    const int slot_in_block = threadIdx.x / kW;    // this chain's index in the CTA
+    const int chains_in_block = blockDim.x / kW;
     Machine m;
     Ctx c;
     Philox rng;
@@ -962,13 +1000,13 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
             if (st == S_FETCH) {
                 int it;
                 if (!kSearch) {
-                    it = first ? blockIdx.x * (blockDim.x >> 5) + warp : n_items;
+                    it = first ? blockIdx.x * chains_in_block + slot_in_block : n_items;
                 } else if (P.persistent) {
                     unsigned int v = 0;
                     if (lane == 0) v = atomicAdd(queue, 1u);
-                    it = (int)__shfl_sync(kFull, v, 0);
+                    it = (int)__shfl_sync(lanes_mask<kW>(), v, 0, kW);
                 } else {
-                    it = first ? first_item + blockIdx.x * (blockDim.x >> 5) + warp : n_items + first_item;
+                    it = first ? first_item + blockIdx.x * chains_in_block + slot_in_block : n_items + first_item;
                     if (it >= first_item + n_items) it = -1;
                     else it -= first_item;
                 }
@@ -982,13 +1020,13 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                     const int gi = P.persistent ? it : it + first_item;
                     m.lig = order[gi / P.exhaustiveness];
                     m.chain = gi % P.exhaustiveness;
-                    c = make_ctx(B, m.lig, sw);
+                    c = make_ctx<kW>(B, m.lig, sw);
                     rng.init(P.seed, (uint32_t)m.lig, (uint32_t)m.chain);
                     m.steps_cap = c.local_steps;
                     if (P.bfgs_cap > 0 && P.bfgs_cap < m.steps_cap) m.steps_cap = P.bfgs_cap;
                     float* tmp = c.s + L.tmp;
-                    random_conf(c, rng, M, tmp);
-                    copyw(c, c.s + L.best, tmp, 7 + c.T);
+                    random_conf<kW>(c, rng, M, tmp);
+                    copyw<kW>(c, c.s + L.best, tmp, 7 + c.T);
                     m.tmp_e = kMaxFl;
                     m.best_e = kMaxFl;
                     m.step = 0;
@@ -1001,10 +1039,10 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                     st = S_MC_STEP;
                 } else {
                     m.lig = opt_lig[it];
-                    c = make_ctx(B, m.lig, sw);
+                    c = make_ctx<kW>(B, m.lig, sw);
                     float* x = c.s + L.x;
-                    for (int i = lane; i < 7 + c.T; i += 32) x[i] = poses[(size_t)it * pose_stride + i];
-                    __syncwarp();
+                    for (int i = lane; i < 7 + c.T; i += kW) x[i] = poses[(size_t)it * pose_stride + i];
+                    lanes_sync<kW>();
                     m.steps_cap = opt_steps > 0 ? opt_steps : c.local_steps;
                     m.mode = 2;
                     m.bx_off = L.x;
@@ -1018,22 +1056,22 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                     continue;
                 }
                 float* cand = c.s + L.cand;
-                copyw(c, cand, c.s + L.tmp, 7 + c.T);
-                mutate(c, L, rng, P.mutation_amplitude, cand);
+                copyw<kW>(c, cand, c.s + L.tmp, 7 + c.T);
+                mutate<kW>(c, L, rng, P.mutation_amplitude, cand);
                 m.mode = 0;
                 m.bx_off = L.cand;
                 m.v = P.hunt_cap;
                 st = S_BFGS_BEGIN;
             } else if (st == S_BFGS_BEGIN) {
-                h_identity(c, c.s + L.h, 6 + c.T);
+                h_identity<kW>(c, c.s + L.h, 6 + c.T);
                 eval_x = c.s + m.bx_off;
                 eval_g = c.s + L.g;
                 st = S_BFGS_INIT;
             } else if (st == S_BFGS_INIT) {
                 m.f0 = m.last_e;
                 m.f_orig = m.last_e;
-                copyw(c, c.s + L.gorig, c.s + L.g, 6 + c.T);
-                copyw(c, c.s + L.xorig, c.s + m.bx_off, 7 + c.T);
+                copyw<kW>(c, c.s + L.gorig, c.s + L.g, 6 + c.T);
+                copyw<kW>(c, c.s + L.xorig, c.s + m.bx_off, 7 + c.T);
                 m.iter = 0;
                 st = S_BFGS_ITER;
             } else if (st == S_BFGS_ITER) {
@@ -1043,11 +1081,11 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                 }
                 const int n = 6 + c.T;
                 float* p = c.s + L.p;
-                minus_hv(c, c.s + L.h, c.s + L.g, p, n);
-                m.pg = dotw(c, p, c.s + L.g, n);
+                minus_hv<kW>(c, c.s + L.h, c.s + L.g, p, n);
+                m.pg = dotw<kW>(c, p, c.s + L.g, n);
                 m.alpha = 1.0f;
                 m.trial = 0;
-                conf_increment(c, c.s + m.bx_off, p, m.alpha, c.s + L.xnew);
+                conf_increment<kW>(c, c.s + m.bx_off, p, m.alpha, c.s + L.xnew);
                 eval_x = c.s + L.xnew;
                 eval_g = c.s + L.gnew;
                 st = S_LS_DONE;
@@ -1057,7 +1095,7 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                 if (!accept) {
                     m.alpha *= 0.5f;
                     if (++m.trial < 10) {
-                        conf_increment(c, c.s + m.bx_off, c.s + L.p, m.alpha, c.s + L.xnew);
+                        conf_increment<kW>(c, c.s + m.bx_off, c.s + L.p, m.alpha, c.s + L.xnew);
                         eval_x = c.s + L.xnew;
                         eval_g = c.s + L.gnew;
                         continue;
@@ -1068,35 +1106,35 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                 float* g = c.s + L.g;
                 float* gnew = c.s + L.gnew;
                 float* y = c.s + L.y;
-                for (int i = lane; i < n; i += 32) y[i] = gnew[i] - g[i];
-                __syncwarp();
+                for (int i = lane; i < n; i += kW) y[i] = gnew[i] - g[i];
+                lanes_sync<kW>();
                 m.f0 = f1;
-                copyw(c, c.s + m.bx_off, c.s + L.xnew, 7 + c.T);
-                const float gg = dotw(c, g, g, n);
+                copyw<kW>(c, c.s + m.bx_off, c.s + L.xnew, 7 + c.T);
+                const float gg = dotw<kW>(c, g, g, n);
                 if (!(sqrtf(gg) >= 1e-5f)) {
                     st = S_BFGS_END;
                     continue;
                 }
-                copyw(c, g, gnew, n);
+                copyw<kW>(c, g, gnew, n);
                 float* H = c.s + L.h;
                 float* p = c.s + L.p;
                 if (m.iter == 0) {
-                    float yy = dotw(c, y, y, n);
+                    float yy = dotw<kW>(c, y, y, n);
                     if (fabsf(yy) > kEps) {
-                        float yp = dotw(c, y, p, n);
+                        float yp = dotw<kW>(c, y, p, n);
                         const float d = __fdividef(m.alpha * yp, yy);
-                        for (int i = lane; i < n; i += 32) H[i * n + i] = d;
-                        __syncwarp();
+                        for (int i = lane; i < n; i += kW) H[i * n + i] = d;
+                        lanes_sync<kW>();
                     }
                 }
-                h_update(c, H, p, y, c.s + L.mhy, m.alpha, n);
+                h_update<kW>(c, H, p, y, c.s + L.mhy, m.alpha, n);
                 ++m.iter;
                 st = S_BFGS_ITER;
             } else if (st == S_BFGS_END) {
                 if (!(m.f0 <= m.f_orig)) {
                     m.f0 = m.f_orig;
-                    copyw(c, c.s + m.bx_off, c.s + L.xorig, 7 + c.T);
-                    copyw(c, c.s + L.g, c.s + L.gorig, 6 + c.T);
+                    copyw<kW>(c, c.s + m.bx_off, c.s + L.xorig, 7 + c.T);
+                    copyw<kW>(c, c.s + L.g, c.s + L.gorig, 6 + c.T);
                 }
                 st = (m.mode == 0) ? S_AFTER_SEARCH : (m.mode == 1 ? S_AFTER_REFINE : S_DONE);
             } else if (st == S_AFTER_SEARCH) {
@@ -1107,9 +1145,9 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                     accept = (m.step == 0) || (cand_e < m.tmp_e) ||
                              (u01(u.x) < __expf(__fdividef(m.tmp_e - cand_e, P.temperature)));
                 }
-                accept = __shfl_sync(kFull, accept, 0);
+                accept = __shfl_sync(lanes_mask<kW>(), accept, 0, kW);
                 if (accept) {
-                    copyw(c, c.s + L.tmp, c.s + L.cand, 7 + c.T);
+                    copyw<kW>(c, c.s + L.tmp, c.s + L.cand, 7 + c.T);
                     m.tmp_e = cand_e;
                     if (m.tmp_e < m.best_e) {
                         m.mode = 1;
@@ -1124,7 +1162,7 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
             } else if (st == S_AFTER_REFINE) {
                 m.tmp_e = m.f0;
                 if (m.tmp_e < m.best_e) {
-                    copyw(c, c.s + L.best, c.s + L.tmp, 7 + c.T);
+                    copyw<kW>(c, c.s + L.best, c.s + L.tmp, 7 + c.T);
                     m.best_e = m.tmp_e;
                 }
                 ++m.step;
@@ -1133,11 +1171,11 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                 if (kSearch) {
                     const int slot = m.lig * P.exhaustiveness + m.chain;
                     const float* best = c.s + L.best;
-                    for (int i = lane; i < 7 + c.T; i += 32) poses[(size_t)slot * pose_stride + i] = best[i];
+                    for (int i = lane; i < 7 + c.T; i += kW) poses[(size_t)slot * pose_stride + i] = best[i];
                     // scoring-path energies of the best pose for the final rescoring
                     // (vina.h:241-300), so that post-processing needs no device work
                     float eg, ei;
-                    eval_score<kAD4>(c, L, M, Tb, best, P.authentic_v, eg, ei);
+                    eval_score<kAD4, kW>(c, L, M, Tb, best, P.authentic_v, eg, ei);
                     if (lane == 0) {
                         results[slot].e = m.best_e;
                         results[slot].evals = m.evals;
@@ -1148,13 +1186,13 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                     }
                 } else {
                     const float* x = c.s + L.x;
-                    for (int i = lane; i < 7 + c.T; i += 32) poses[(size_t)m.item * pose_stride + i] = x[i];
+                    for (int i = lane; i < 7 + c.T; i += kW) poses[(size_t)m.item * pose_stride + i] = x[i];
                     if (lane == 0) {
                         opt_e[m.item] = m.f0;
                         if (opt_evals) opt_evals[m.item] = m.evals;
                     }
                 }
-                __syncwarp();
+                lanes_sync<kW>();
                 st = S_FETCH;
             } else {  // S_EXIT
                 break;
@@ -1162,7 +1200,7 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
         }
         if (st == S_EXIT) return;
         // ---- the single evaluation site
-        m.last_e = eval_deriv<false, kAD4>(c, L, M, Tb, eval_x, eval_g, m.v, m.v);
+        m.last_e = eval_deriv<false, kAD4, false, kW>(c, L, M, Tb, eval_x, eval_g, m.v, m.v);
         ++m.evals;
     }
 }
@@ -1178,14 +1216,14 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
 #ifndef UD_SEARCH_MIN_BLOCKS_AD4
 #define UD_SEARCH_MIN_BLOCKS_AD4 6
 #endif
-template <bool kAD4>
+template <bool kAD4, int kW>
 __global__ void __launch_bounds__(128, kAD4 ? UD_SEARCH_MIN_BLOCKS_AD4 : UD_SEARCH_MIN_BLOCKS) search_kernel(
     const __grid_constant__ Batch B, const __grid_constant__ Maps M, const __grid_constant__ Tables Tb,
     const __grid_constant__ SearchParams P, const __grid_constant__ Layout L, const int* order, int n_items,
     int first_item, unsigned int* queue, float* poses, int pose_stride, ChainResult* results) {
     extern __shared__ __align__(16) float smem[];
-    float* sw = smem + (size_t)(threadIdx.x >> 5) * L.total;
-    run_machine<true, kAD4>(B, M, Tb, P, L, sw, order, n_items, first_item, queue, poses, pose_stride, results,
+    float* sw = smem + (size_t)(threadIdx.x / kW) * L.total;
+    run_machine<true, kAD4, kW>(B, M, Tb, P, L, sw, order, n_items, first_item, queue, poses, pose_stride, results,
                             nullptr, 0, 0.f, nullptr, nullptr);
 }
 
@@ -1198,7 +1236,7 @@ __global__ void __launch_bounds__(128) optimize_kernel(
     float* poses, int pose_stride, int n_poses, int max_steps, float v, float* e_out, int* evals_out) {
     extern __shared__ __align__(16) float smem[];
     float* sw = smem + (size_t)(threadIdx.x >> 5) * L.total;
-    run_machine<false, kAD4>(B, M, Tb, P, L, sw, nullptr, n_poses, 0, nullptr, poses, pose_stride, nullptr,
+    run_machine<false, kAD4, 32>(B, M, Tb, P, L, sw, nullptr, n_poses, 0, nullptr, poses, pose_stride, nullptr,
                              pose_lig, max_steps, v, e_out, evals_out);
 }
 
@@ -2152,20 +2190,32 @@ cudaError_t launch_combine_terms(const float* in, long long block, int n_terms, 
     return cudaGetLastError();
 }
 
+// The search kernel instantiation for the scoring function and the lanes a
+// chain runs on (a warp, or half a warp).
+using SearchKernel = void (*)(const dev::Batch, const dev::Maps, const dev::Tables, const SearchParams,
+                              const dev::Layout, const int*, int, int, unsigned int*, float*, int, ChainResult*);
+static SearchKernel search_kernel_for(bool ad4, int lanes) {
+    if (lanes == 16) return ad4 ? dev::search_kernel<true, 16> : dev::search_kernel<false, 16>;
+    return ad4 ? dev::search_kernel<true, 32> : dev::search_kernel<false, 32>;
+}
+
 cudaError_t launch_search(const DeviceBatchView& b, const DeviceMapsView& m,
                           const DeviceTablesView& t, const SearchParams& P, const int* order,
                           int n_items, int first_item, unsigned int* queue, float* poses,
                           int pose_stride, ChainResult* results, int grid_blocks,
                           cudaStream_t stream) {
     dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
-    const int warps = 4;
-    size_t smem = (size_t)warps * L.total * sizeof(float);
-    const auto kern = m.desc.ad4 ? dev::search_kernel<true> : dev::search_kernel<false>;
+    if (P.chains_per_block < 1 || P.chains_per_block > 4 || (P.lanes_per_chain != 32 && P.lanes_per_chain != 16))
+        return cudaErrorInvalidValue;
+    const int warps = P.chains_per_block;                        // warps per CTA
+    const int chains = warps * (32 / P.lanes_per_chain);         // chains per CTA
+    size_t smem = (size_t)chains * L.total * sizeof(float);
+    const auto kern = search_kernel_for(m.desc.ad4 != 0, P.lanes_per_chain);
     cudaError_t e = smem_attr((const void*)kern, smem);
     if (e != cudaSuccess) return e;
     dim3 grid;
     if (P.persistent) grid = dim3(grid_blocks);
-    else grid = dim3((n_items + warps - 1) / warps);
+    else grid = dim3((n_items + chains - 1) / chains);
     kern<<<grid, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t), P, L,
                                                            order, n_items, first_item, queue, poses,
                                                            pose_stride, results);
@@ -2279,10 +2329,11 @@ float measure_fp32_peak_tflops() {
     return best;
 }
 
-int search_blocks_per_sm(const DeviceBatchView& b, int warps) {
+int search_blocks_per_sm(const DeviceBatchView& b, int warps, int lanes_per_chain) {
     dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
-    size_t smem = (size_t)warps * L.total * sizeof(float);
-    const auto kern = b.ad4 ? dev::search_kernel<true> : dev::search_kernel<false>;
+    const int lanes = lanes_per_chain == 16 ? 16 : 32;
+    size_t smem = (size_t)warps * (32 / lanes) * L.total * sizeof(float);
+    const auto kern = search_kernel_for(b.ad4 != 0, lanes);
     smem_attr((const void*)kern, smem);
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, warps * 32, smem) != cudaSuccess)

@@ -82,8 +82,8 @@ struct SearchParams {
     float authentic_v;     // curl cap of the refinement (1000)
     float temperature;     // Metropolis temperature (1.2)
     float mutation_amplitude;
-    int lanes_per_chain;   // 32 (warp) or 16 / 8 (sub-warp)
-    int chains_per_block;
+    int lanes_per_chain;   // 32 (a warp per chain) or 16 (two chains per warp)
+    int chains_per_block;  // warps per CTA (1..4)
     int persistent;        // 0: plain fixed-tiling launch, 1: persistent queue
     int bfgs_cap;          // 0: per-ligand local_steps; >0: min(local_steps, cap)
 };
@@ -217,7 +217,8 @@ cudaError_t launch_search(const DeviceBatchView& b, const DeviceMapsView& m, con
                           const SearchParams& P, const int* order, int n_items, int first_item,
                           unsigned int* queue, float* poses, int pose_stride, ChainResult* results,
                           int grid_blocks, cudaStream_t stream);
-int search_blocks_per_sm(const DeviceBatchView& b, int warps);
+// CTAs of `warps` warps (chains of lanes_per_chain = 32 or 16 lanes) resident per SM
+int search_blocks_per_sm(const DeviceBatchView& b, int warps, int lanes_per_chain = 32);
 cudaError_t launch_optimize(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
                             const int* pose_lig, float* poses, int pose_stride, int n_poses, int max_steps,
                             float v, float* e_out, int* evals_out, cudaStream_t stream);

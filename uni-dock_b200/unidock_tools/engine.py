@@ -53,6 +53,7 @@ class SearchParams(C.Structure):
         ("bfgs_cap", C.c_int),
         ("use_graph", C.c_int),
         ("refine_step", C.c_int),
+        ("lanes_per_chain", C.c_int),
     ]
 
 
@@ -475,22 +476,23 @@ class Batch:
 
     # ---- search
     def search(self, exhaustiveness=8, max_step=0, num_modes=9, min_rmsd=1.0, energy_range=3.0, seed=0,
-               form=1, chains_per_block=0, bfgs_cap=0, use_graph=0, refine_step=0):
+               form=1, chains_per_block=0, bfgs_cap=0, use_graph=0, refine_step=0, lanes_per_chain=0):
         """Search, cluster and score (ud_search).  refine_step > 0 refines the
         modes against the receptor atoms, as the reference CLI does by default
         (refine_step 3); 0 keeps the grid energies (--no_refine)."""
         p = SearchParams(exhaustiveness, max_step, num_modes, min_rmsd, energy_range, seed, form,
-                         chains_per_block, bfgs_cap, use_graph, refine_step)
+                         chains_per_block, bfgs_cap, use_graph, refine_step, lanes_per_chain)
         _check(lib().ud_search(self.h, C.byref(p), None))
         self.exhaustiveness = exhaustiveness
 
     def search_launch(self, exhaustiveness=8, max_step=0, num_modes=9, min_rmsd=1.0, energy_range=3.0, seed=0,
-                      form=1, chains_per_block=0, bfgs_cap=0, use_graph=0, stream=None, refine_step=0):
+                      form=1, chains_per_block=0, bfgs_cap=0, use_graph=0, stream=None, refine_step=0,
+                      lanes_per_chain=0):
         """Enqueue the device part only (search, clustering, refinement;
         device-resident inputs, asynchronous on `stream`, a raw cudaStream_t or
         None for the default stream)."""
         self._p = SearchParams(exhaustiveness, max_step, num_modes, min_rmsd, energy_range, seed, form,
-                               chains_per_block, bfgs_cap, use_graph, refine_step)
+                               chains_per_block, bfgs_cap, use_graph, refine_step, lanes_per_chain)
         _check(lib().ud_search_launch(self.h, C.byref(self._p), C.c_void_p(stream) if stream else None))
         self.exhaustiveness = exhaustiveness
 
@@ -507,18 +509,20 @@ class Batch:
                                               C.c_void_p(stream) if stream else None))
 
     def autotune(self, exhaustiveness=8, max_step=0, seed=0):
-        """Pick chains-per-CTA and the BFGS cap for this batch (ud_autotune);
-        searches with chains_per_block=0 and bfgs_cap=-1 then use them."""
+        """Pick warps per CTA, lanes per chain and the BFGS cap for this batch
+        (ud_autotune); searches with chains_per_block=0, lanes_per_chain=0 and
+        bfgs_cap=-1 then use them."""
         p = SearchParams(exhaustiveness, max_step, 9, 1.0, 3.0, seed, 1, 0, 0, 0)
         r = TuneResult()
         _check(lib().ud_autotune(self.h, C.byref(p), C.byref(r), None))
         return r.as_dict()
 
     def search_prepare(self, exhaustiveness=8, max_step=0, num_modes=9, min_rmsd=1.0, energy_range=3.0, seed=0,
-                       form=1, chains_per_block=0, bfgs_cap=0, use_graph=0, stream=None, refine_step=0):
+                       form=1, chains_per_block=0, bfgs_cap=0, use_graph=0, stream=None, refine_step=0,
+                       lanes_per_chain=0):
         """Set up a search (buffers, order, graph) without launching it (ud_search_prepare)."""
         p = SearchParams(exhaustiveness, max_step, num_modes, min_rmsd, energy_range, seed, form,
-                         chains_per_block, bfgs_cap, use_graph, refine_step)
+                         chains_per_block, bfgs_cap, use_graph, refine_step, lanes_per_chain)
         _check(lib().ud_search_prepare(self.h, C.byref(p), C.c_void_p(stream) if stream else None))
 
     def search_collect(self, stream=None):
