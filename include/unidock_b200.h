@@ -252,6 +252,14 @@ typedef struct {
                                else 32.  The plain form ignores it. */
 } ud_search_params;
 
+/* Device bytes a batch of these n ligands holds through a search with
+ * `params` (exhaustiveness, num_modes) under scoring `sf`: topology, chain
+ * results and mode buffers, headroom included; the maps, pair tables and
+ * receptor cells belong to the maps handle and are not counted.  Host-only.
+ * The batch packing of the CLI's --max_gpu_memory uses it, as the reference
+ * packs batches by predict_peak_memory (unidock/src/main/main.cpp:139-206). */
+int ud_batch_device_bytes(const ud_ligand* ligs, int n, int sf, const ud_search_params* params, size_t* bytes);
+
 /* Launch configuration picked by ud_autotune. */
 typedef struct {
     int chains_per_block;      /* warps per CTA */

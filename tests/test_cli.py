@@ -111,6 +111,34 @@ def test_oversized_ligand_is_skipped_alone(inputs, tmp_path):
 
 
 @pytest.mark.gpu
+def test_max_gpu_memory_packs_smaller_batches(inputs, tmp_path):
+    """--max_gpu_memory caps the device memory of the batches in flight: a
+    budget of about a megabyte per batch splits six ligands over several
+    batches and still docks every one; a budget below the maps' own memory is
+    refused."""
+    import re
+    d, names = inputs
+    common = ["--receptor", d / "rec.pdbqt", "--gpu_batch", *names, "--exhaustiveness", 2048, "--max_step", 1,
+              "--seed", 4, *box_args()]
+    out1 = tmp_path / "o1"
+    out1.mkdir()
+    r = run(*common, "--dir", out1, "--verbosity", 2)
+    assert r.returncode == 0, r.stderr
+    used = int(re.search(r"GPU memory: maps (\d+) MiB", r.stdout).group(1))
+    assert "Batch 2 size" not in r.stdout
+    out2 = tmp_path / "o2"
+    out2.mkdir()
+    r = run(*common, "--dir", out2, "--max_gpu_memory", used + 66)   # 64 MiB reserve + about 1 MiB per batch
+    assert r.returncode == 0, r.stderr
+    sizes = [int(x) for x in re.findall(r"Batch \d+ size: (\d+)", r.stdout)]
+    assert len(sizes) >= 2 and sum(sizes) == len(names)
+    for p in names:
+        assert (out2 / (p.stem + "_out.pdbqt")).read_text().startswith("MODEL 1\nREMARK VINA RESULT:")
+    r = run(*common, "--dir", out2, "--max_gpu_memory", 1)
+    assert r.returncode != 0 and "max_gpu_memory" in r.stderr
+
+
+@pytest.mark.gpu
 def test_single_ligand_default_output_and_modes_table(inputs):
     d, names = inputs
     r = run("--receptor", d / "rec.pdbqt", "--ligand", names[0], "--exhaustiveness", 8, "--max_step", 10,

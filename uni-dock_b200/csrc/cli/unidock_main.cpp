@@ -453,8 +453,32 @@ std::string result_text(ud_batch b, int lig, int format) {
 }
 
 // ---------------------------------------------------------------- batch mode
+// Ligands of a batch kept within `budget` device bytes (ud_batch_device_bytes;
+// 0 = no limit): the largest leading count that fits, the rest returned for
+// the next batch, as the reference packs batches until its predicted peak
+// memory reaches --max_gpu_memory (main.cpp:139-206, 993-1070).
+std::vector<ParsedLigand> fit_budget(const Setup& S, std::vector<ParsedLigand>& ligs, size_t budget) {
+    std::vector<ParsedLigand> rest;
+    if (budget == 0 || ligs.empty()) return rest;
+    auto bytes_of = [&](size_t n) {
+        std::vector<ud_ligand> hs;
+        for (size_t i = 0; i < n; ++i) hs.push_back(ligs[i].h);
+        size_t b = 0;
+        check(ud_batch_device_bytes(hs.data(), (int)n, S.sf, &S.params, &b), "memory estimate");
+        return b;
+    };
+    if (bytes_of(1) > budget)
+        throw std::runtime_error("--max_gpu_memory leaves too little device memory for one ligand of " + ligs[0].path);
+    size_t n = ligs.size();
+    for (size_t b; n > 1 && (b = bytes_of(n)) > budget;)
+        n = std::max<size_t>(1, std::min(n - 1, (size_t)((double)n * (double)budget / (double)b)));
+    rest.assign(ligs.begin() + n, ligs.end());
+    ligs.resize(n);
+    return rest;
+}
+
 void run_batches(const Setup& S, ud_maps maps, const std::vector<std::string>& paths, const std::string& dir,
-                 int batch_size) {
+                 int batch_size, size_t slot_budget) {
     struct Slot {
         std::vector<ParsedLigand> ligs;
         ud_batch b = nullptr;
@@ -477,13 +501,19 @@ void run_batches(const Setup& S, ud_maps maps, const std::vector<std::string>& p
     bool has_done[2] = {false, false};
     size_t next = 0;
     int batch_id = 0, done = 0;
+    std::vector<ParsedLigand> carry;  // parsed, but over the previous batch's memory budget
     auto start_batch = [&](Slot& sl) -> bool {
-        while (next < paths.size()) {
-            std::vector<std::string> chunk(paths.begin() + next,
-                                           paths.begin() + std::min(paths.size(), next + (size_t)batch_size));
-            next += chunk.size();
-            sl.ligs = parse_ligands(chunk, S.threads, S.verbosity);
-            if (sl.ligs.empty()) continue;
+        {
+            sl.ligs.swap(carry);
+            carry.clear();
+            while (sl.ligs.size() < (size_t)batch_size && next < paths.size()) {
+                const size_t take = std::min(paths.size() - next, (size_t)batch_size - sl.ligs.size());
+                std::vector<std::string> chunk(paths.begin() + next, paths.begin() + next + take);
+                next += take;
+                for (auto& p : parse_ligands(chunk, S.threads, S.verbosity)) sl.ligs.push_back(p);
+            }
+            if (sl.ligs.empty()) return false;
+            carry = fit_budget(S, sl.ligs, slot_budget);
             std::vector<ud_ligand> hs;
             for (auto& p : sl.ligs) hs.push_back(p.h);
             // each slot keeps its batch handle: reused, it allocates (and frees,
@@ -504,10 +534,11 @@ void run_batches(const Setup& S, ud_maps maps, const std::vector<std::string>& p
                 ud_tune_result r;
                 check(ud_autotune(sl.b, &p, &r, sl.s), "autotune");
                 p.chains_per_block = 0;
+                p.lanes_per_chain = 0;
                 p.bfgs_cap = -1;
                 if (S.verbosity > 1)
-                    std::cout << "Batch " << sl.id << " autotuned: " << r.chains_per_block << " chains/CTA, BFGS cap "
-                              << r.bfgs_cap << "\n";
+                    std::cout << "Batch " << sl.id << " autotuned: " << r.chains_per_block << " warps/CTA, "
+                              << r.lanes_per_chain << " lanes/chain, BFGS cap " << r.bfgs_cap << "\n";
             }
             if (S.verbosity > 0) std::cout << "Batch " << sl.id << " size: " << sl.ligs.size() << std::endl;
             const int me = (int)(&sl - slots), other = me ^ 1;
@@ -517,7 +548,6 @@ void run_batches(const Setup& S, ud_maps maps, const std::vector<std::string>& p
             has_done[me] = true;
             return true;
         }
-        return false;
     };
     auto finish_batch = [&](Slot& sl) {
         check(ud_search_collect(sl.b, sl.s), "search");
@@ -1074,6 +1104,9 @@ int run(int argc, char** argv) {
     }
     const int device = (int)o.num("device_id", 0);
     if (cudaSetDevice(device) != cudaSuccess) throw std::runtime_error("could not select GPU " + std::to_string(device));
+    size_t free_start = 0, total_mem = 0;
+    cudaFree(nullptr);  // the context, so that its own memory is not counted below
+    cudaMemGetInfo(&free_start, &total_mem);
     ud_maps maps = nullptr;
     if (o.has("maps")) {
         check(ud_maps_load(S.sf, S.weights.data(), (int)S.weights.size(), o.str("maps").c_str(), nullptr, &maps),
@@ -1114,7 +1147,27 @@ int run(int argc, char** argv) {
         }
     } else {
         const int batch_size = std::max(1, (int)o.num("batch_size", 4096));
-        run_batches(S, maps, batch_names, dir, batch_size);
+        // --max_gpu_memory (MiB; 0 = 95% of the free memory, main.cpp:955-965):
+        // what the maps left, less a reserve for the receptor cells and the
+        // search set-up, is shared by the two batches in flight
+        size_t free_now = 0;
+        cudaMemGetInfo(&free_now, &total_mem);
+        const size_t used = free_start > free_now ? free_start - free_now : 0;
+        const double max_mib = o.num("max_gpu_memory", 0);
+        const size_t reserve = (size_t)64 << 20;
+        size_t slot_budget = 0;
+        if (max_mib > 0) {
+            const size_t cap = (size_t)(max_mib * 1048576.0);
+            if (cap <= used + reserve)
+                throw std::runtime_error("--max_gpu_memory " + std::to_string((long long)max_mib) +
+                                         " MiB is below the maps' own " + std::to_string(used >> 20) + " MiB");
+            slot_budget = (cap - used - reserve) / 2;
+        } else {
+            slot_budget = (size_t)(0.95 * (double)free_now) / 2;
+        }
+        if (S.verbosity > 1)
+            std::cout << "GPU memory: maps " << (used >> 20) << " MiB, per batch " << (slot_budget >> 20) << " MiB\n";
+        run_batches(S, maps, batch_names, dir, batch_size, slot_budget);
     }
     ud_maps_destroy(maps);
     return 0;

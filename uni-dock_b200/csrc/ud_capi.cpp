@@ -171,6 +171,9 @@ struct LigandPost {
 
 struct ud_ligand_s {
     Ligand lig;
+    // pair-group slots of the Vina / Vinardo and the AD4 pair lists (-1 until
+    // counted; memory estimates only)
+    mutable int pair_slots[2] = {-1, -1};
 };
 
 struct ud_batch_s {
@@ -1073,6 +1076,48 @@ static std::unique_ptr<ud_batch_s> build_batch(ud_maps maps, const std::vector<c
     b->maps = maps;
     fill_batch(b.get(), ligs, s);
     return b;
+}
+
+// Bytes of one DevBuf allocation of `count` elements of `size` bytes (its
+// quarter of headroom included).
+static size_t devbuf_bytes(size_t count, size_t size) { return std::max<size_t>(count + count / 4, 1) * size; }
+
+extern "C" int ud_batch_device_bytes(const ud_ligand* ligs, int n, int sf, const ud_search_params* params,
+                                     size_t* bytes) {
+    return guarded([&] {
+        if (!bytes || !params || n < 0 || (n > 0 && !ligs)) throw Error(UD_ERR_ARG, "invalid arguments");
+        if (sf != UD_SF_VINA && sf != UD_SF_VINARDO && sf != UD_SF_AD4) throw Error(UD_ERR_ARG, "unknown scoring");
+        const bool ad4 = sf == UD_SF_AD4;
+        size_t atoms = 0, nodes = 0, slots = 0;
+        int max_atoms = 0, max_tors = 0;
+        for (int i = 0; i < n; ++i) {
+            if (!ligs[i]) throw Error(UD_ERR_ARG, "null ligand");
+            const Ligand& L = ligs[i]->lig;
+            int& ps = ligs[i]->pair_slots[ad4 ? 1 : 0];
+            if (ps < 0) ps = (int)pair_group_slots(L, ad4 ? L.pairs_ad : L.pairs).size();
+            atoms += L.atoms.size();
+            nodes += L.nodes.size();
+            slots += (size_t)ps;
+            max_atoms = std::max(max_atoms, (int)L.atoms.size());
+            max_tors = std::max(max_tors, L.n_torsions());
+        }
+        const size_t E = (size_t)std::max(1, params->exhaustiveness), cap = (size_t)std::max(1, params->num_modes);
+        const size_t stride = 7 + (size_t)max_tors, chains = (size_t)n * E, mode_slots = (size_t)n * cap;
+        size_t b = 0;
+        // topology (fill_batch)
+        b += devbuf_bytes(n, sizeof(LigDesc)) + devbuf_bytes(atoms, sizeof(AtomRec)) +
+             devbuf_bytes(nodes, sizeof(NodeRec)) + devbuf_bytes(slots, sizeof(uint32_t)) +
+             devbuf_bytes(atoms, sizeof(uint32_t)) + devbuf_bytes(n, sizeof(int));
+        if (ad4) b += devbuf_bytes(atoms, sizeof(float)) + devbuf_bytes(slots, 2 * sizeof(float));
+        // search results (search_launch)
+        b += devbuf_bytes(chains * stride, sizeof(float)) + devbuf_bytes(chains, sizeof(ChainResult)) +
+             devbuf_bytes(1, sizeof(unsigned int));
+        // modes (alloc_modes)
+        b += devbuf_bytes(mode_slots * 3 * std::max(1, max_atoms), sizeof(float)) + devbuf_bytes(n, sizeof(int)) +
+             2 * devbuf_bytes(mode_slots, sizeof(int)) + devbuf_bytes(mode_slots * stride, sizeof(float)) +
+             devbuf_bytes(mode_slots * 4, sizeof(float));
+        *bytes = b;
+    });
 }
 
 extern "C" int ud_batch_create(ud_maps maps, const ud_ligand* ligs, int n, void* stream, ud_batch* out) {

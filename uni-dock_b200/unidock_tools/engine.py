@@ -111,6 +111,8 @@ def lib():
         "ud_optimize": ([vp, ip, fp, C.c_int, C.c_int, C.c_int, C.c_float, fp, ip, vp], C.c_int),
         "ud_device_fp32_peak": ([fp], C.c_int),
         "ud_maps_term_count": ([vp, ip], C.c_int),
+        "ud_batch_device_bytes": ([C.POINTER(vp), C.c_int, C.c_int, C.POINTER(SearchParams),
+                                   C.POINTER(C.c_size_t)], C.c_int),
         "ud_ligand_parse_many": ([C.POINTER(C.c_char_p), C.POINTER(C.c_size_t), C.c_int, C.c_int, C.POINTER(vp),
                                   ip], C.c_int),
         "ud_receptor_parse_ex": ([C.c_char_p, C.c_size_t, fp, ip, ip, fp, C.c_int, ip], C.c_int),
@@ -150,6 +152,16 @@ def parse_ligands(texts, threads=0):
                 lib().ud_ligand_destroy(C.c_void_p(h))
         raise UdError(int(status[bad[0]]), f"{len(bad)} of {n} ligands failed to parse (first: {int(bad[0])})")
     return [Ligand("", _handle=h) for h in out]
+
+
+def batch_device_bytes(ligands, sf=SF_VINA, exhaustiveness=8, num_modes=9):
+    """Device bytes a batch of these ligands holds through a search
+    (ud_batch_device_bytes; host-only, no GPU needed)."""
+    arr = (C.c_void_p * len(ligands))(*[l.h.value for l in ligands])
+    p = SearchParams(exhaustiveness, 0, num_modes, 1.0, 3.0, 0, 1, 0, 0, 0)
+    out = C.c_size_t()
+    _check(lib().ud_batch_device_bytes(arr, len(ligands), int(sf), C.byref(p), C.byref(out)))
+    return int(out.value)
 
 
 def parse_receptor_ex(text: str):
