@@ -503,51 +503,49 @@ void run_batches(const Setup& S, ud_maps maps, const std::vector<std::string>& p
     int batch_id = 0, done = 0;
     std::vector<ParsedLigand> carry;  // parsed, but over the previous batch's memory budget
     auto start_batch = [&](Slot& sl) -> bool {
-        {
-            sl.ligs.swap(carry);
-            carry.clear();
-            while (sl.ligs.size() < (size_t)batch_size && next < paths.size()) {
-                const size_t take = std::min(paths.size() - next, (size_t)batch_size - sl.ligs.size());
-                std::vector<std::string> chunk(paths.begin() + next, paths.begin() + next + take);
-                next += take;
-                for (auto& p : parse_ligands(chunk, S.threads, S.verbosity)) sl.ligs.push_back(p);
-            }
-            if (sl.ligs.empty()) return false;
-            carry = fit_budget(S, sl.ligs, slot_budget);
-            std::vector<ud_ligand> hs;
-            for (auto& p : sl.ligs) hs.push_back(p.h);
-            // each slot keeps its batch handle: reused, it allocates (and frees,
-            // which would wait for the other slot's search) nothing once warm
-            if (sl.b)
-                check(ud_batch_reset(sl.b, hs.data(), (int)hs.size(), sl.s), "batch");
-            else
-                check(ud_batch_create(maps, hs.data(), (int)hs.size(), sl.s, &sl.b), "batch");
-            if (S.multi_bias)  // each ligand's {name}.bpf (main.cpp:255-265, utils.cpp:103-111)
-                for (size_t i = 0; i < sl.ligs.size(); ++i) {
-                    const std::string bpf = read_file(bias_name(sl.ligs[i].path));
-                    check(ud_batch_set_bias(sl.b, (int)i, bpf.data(), bpf.size()), "bias");
-                }
-            sl.id = ++batch_id;
-            sl.t0 = std::chrono::steady_clock::now();
-            ud_search_params p = S.params;
-            if (S.autotune) {
-                ud_tune_result r;
-                check(ud_autotune(sl.b, &p, &r, sl.s), "autotune");
-                p.chains_per_block = 0;
-                p.lanes_per_chain = 0;
-                p.bfgs_cap = -1;
-                if (S.verbosity > 1)
-                    std::cout << "Batch " << sl.id << " autotuned: " << r.chains_per_block << " warps/CTA, "
-                              << r.lanes_per_chain << " lanes/chain, BFGS cap " << r.bfgs_cap << "\n";
-            }
-            if (S.verbosity > 0) std::cout << "Batch " << sl.id << " size: " << sl.ligs.size() << std::endl;
-            const int me = (int)(&sl - slots), other = me ^ 1;
-            if (has_done[other]) cudaStreamWaitEvent(sl.s, slot_done[other], 0);
-            check(ud_search_launch(sl.b, &p, sl.s), "search");
-            cudaEventRecord(slot_done[me], sl.s);
-            has_done[me] = true;
-            return true;
+        sl.ligs.swap(carry);
+        carry.clear();
+        while (sl.ligs.size() < (size_t)batch_size && next < paths.size()) {
+            const size_t take = std::min(paths.size() - next, (size_t)batch_size - sl.ligs.size());
+            std::vector<std::string> chunk(paths.begin() + next, paths.begin() + next + take);
+            next += take;
+            for (auto& p : parse_ligands(chunk, S.threads, S.verbosity)) sl.ligs.push_back(p);
         }
+        if (sl.ligs.empty()) return false;
+        carry = fit_budget(S, sl.ligs, slot_budget);
+        std::vector<ud_ligand> hs;
+        for (auto& p : sl.ligs) hs.push_back(p.h);
+        // each slot keeps its batch handle: reused, it allocates (and frees,
+        // which would wait for the other slot's search) nothing once warm
+        if (sl.b)
+            check(ud_batch_reset(sl.b, hs.data(), (int)hs.size(), sl.s), "batch");
+        else
+            check(ud_batch_create(maps, hs.data(), (int)hs.size(), sl.s, &sl.b), "batch");
+        if (S.multi_bias)  // each ligand's {name}.bpf (main.cpp:255-265, utils.cpp:103-111)
+            for (size_t i = 0; i < sl.ligs.size(); ++i) {
+                const std::string bpf = read_file(bias_name(sl.ligs[i].path));
+                check(ud_batch_set_bias(sl.b, (int)i, bpf.data(), bpf.size()), "bias");
+            }
+        sl.id = ++batch_id;
+        sl.t0 = std::chrono::steady_clock::now();
+        ud_search_params p = S.params;
+        if (S.autotune) {
+            ud_tune_result r;
+            check(ud_autotune(sl.b, &p, &r, sl.s), "autotune");
+            p.chains_per_block = 0;
+            p.lanes_per_chain = 0;
+            p.bfgs_cap = -1;
+            if (S.verbosity > 1)
+                std::cout << "Batch " << sl.id << " autotuned: " << r.chains_per_block << " warps/CTA, "
+                          << r.lanes_per_chain << " lanes/chain, BFGS cap " << r.bfgs_cap << "\n";
+        }
+        if (S.verbosity > 0) std::cout << "Batch " << sl.id << " size: " << sl.ligs.size() << std::endl;
+        const int me = (int)(&sl - slots), other = me ^ 1;
+        if (has_done[other]) cudaStreamWaitEvent(sl.s, slot_done[other], 0);
+        check(ud_search_launch(sl.b, &p, sl.s), "search");
+        cudaEventRecord(slot_done[me], sl.s);
+        has_done[me] = true;
+        return true;
     };
     auto finish_batch = [&](Slot& sl) {
         check(ud_search_collect(sl.b, sl.s), "search");
