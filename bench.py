@@ -64,6 +64,9 @@ def parse_args():
                          "one-ligand-one-receptor batches (CLI), each on a sample, printed as their own JSON line")
     ap.add_argument("--profile-case", type=int, default=0,
                     help="profiling aid: search N ligands of the workload twice and exit (no JSON)")
+    ap.add_argument("--profile-receptor", type=int, default=3000, choices=[3000, 6000, 12000],
+                    help="receptor of the profiling case: 3000 atoms in a 22.5 A box (61^3 maps), "
+                         "6000 in 30 A (81^3) or 12000 in 36 A (97^3), as the streaming screen")
     return ap.parse_args()
 
 
@@ -71,8 +74,9 @@ def profile_case(args):
     """Small case of the same kernel for ncu: the second search launch is the one to capture."""
     import torch
     from unidock_tools import engine, synth
-    rec = synth.make_receptor(3000, seed=1)
-    maps = engine.Maps(rec.xyz, rec.xs, np.zeros(3, np.float32), np.full(3, BOX, np.float32), SPACING)
+    box = {3000: BOX, 6000: 30.0, 12000: 36.0}[args.profile_receptor]
+    rec = synth.make_receptor(args.profile_receptor, seed=1)
+    maps = engine.Maps(rec.xyz, rec.xs, np.zeros(3, np.float32), np.full(3, box, np.float32), SPACING)
     ligs = [engine.Ligand(l.to_pdbqt()) for l in
             synth.ligand_set(args.profile_case, seed=20261203, heavy=(12, 48), torsions=(0, 10))]
     b = engine.Batch(maps, ligs)
@@ -84,7 +88,9 @@ def profile_case(args):
         torch.cuda.synchronize()
     b.search_collect()
     ev, ms = b.stats()
-    print(f"profile case: {len(ligs)} ligands, {ev} evals, {ms:.1f} ms", flush=True)
+    dims, _, _, n_maps = maps.info()
+    print(f"profile case: {len(ligs)} ligands, receptor {args.profile_receptor} atoms, maps {list(dims)} x {n_maps} "
+          f"({int(dims.prod()) * n_maps * 4 / 1e6:.1f} MB), {ev} evals, {ms:.1f} ms", flush=True)
 
 
 class Clocks:
