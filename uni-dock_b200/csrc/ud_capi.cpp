@@ -172,8 +172,8 @@ struct LigandPost {
 struct ud_ligand_s {
     Ligand lig;
     // pair-group slots of the Vina / Vinardo and the AD4 pair lists (-1 until
-    // counted; memory estimates only)
-    mutable int pair_slots[2] = {-1, -1};
+    // counted; memory estimates only, which may run on several threads)
+    mutable std::atomic<int> pair_slots[2] = {-1, -1};
 };
 
 struct ud_batch_s {
@@ -1093,8 +1093,12 @@ extern "C" int ud_batch_device_bytes(const ud_ligand* ligs, int n, int sf, const
         for (int i = 0; i < n; ++i) {
             if (!ligs[i]) throw Error(UD_ERR_ARG, "null ligand");
             const Ligand& L = ligs[i]->lig;
-            int& ps = ligs[i]->pair_slots[ad4 ? 1 : 0];
-            if (ps < 0) ps = (int)pair_group_slots(L, ad4 ? L.pairs_ad : L.pairs).size();
+            std::atomic<int>& cached = ligs[i]->pair_slots[ad4 ? 1 : 0];
+            int ps = cached.load(std::memory_order_relaxed);
+            if (ps < 0) {
+                ps = (int)pair_group_slots(L, ad4 ? L.pairs_ad : L.pairs).size();
+                cached.store(ps, std::memory_order_relaxed);
+            }
             atoms += L.atoms.size();
             nodes += L.nodes.size();
             slots += (size_t)ps;
