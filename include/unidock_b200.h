@@ -276,9 +276,10 @@ typedef struct {
  * sample of the batch (ligands spread over its size order, enough chains to
  * fill the GPU twice, the caller's exhaustiveness, at most 40 MC steps):
  * first the launch shape, warps per CTA in {4, 2, 1} x lanes per chain in
- * {32, 16}, uncapped; then BFGS caps in {16, 10, 6} on the shape picked.  It
- * keeps the fastest configuration whose mean best energy is within 0.1
- * kcal/mol of the default's (4 warps, 32 lanes, no cap).  Searches of this
+ * {32, 16}, uncapped; then BFGS caps in {16, 10, 6} on the shape picked.  A
+ * configuration replaces the best so far only when it is more than 3% faster
+ * and its mean best energy is within 0.1 kcal/mol of the default's (4 warps,
+ * 32 lanes, no cap).  Searches of this
  * batch with chains_per_block = 0, lanes_per_chain = 0 and bfgs_cap < 0 then
  * use it.  Synchronous; takes about 10 short searches. */
 int ud_autotune(ud_batch batch, const ud_search_params* params, ud_tune_result* out, void* stream);

@@ -2118,8 +2118,9 @@ extern "C" int ud_autotune(ud_batch b, const ud_search_params* params, ud_tune_r
             double shift = 0;
             for (int i = 0; i < S; ++i) shift += (double)cur[i] - (double)base[i];
             shift /= S;
-            // accept only configurations whose search quality holds
-            if (shift <= 0.1 && ms < best_ms) {
+            // accept only configurations whose search quality holds and that
+            // beat the best so far by more than the sample's timing noise
+            if (shift <= 0.1 && ms < 0.97f * best_ms) {
                 best_ms = ms;
                 best_cpb = cpb;
                 best_lanes = ln;
