@@ -93,7 +93,7 @@ def test_scoring_energies_match_reference(gold, o32, setup32):
 
 def test_fp32_error_against_fp64_oracle(gold, o64):
     """FP32 reference energies/gradients vs the FP64 restatement: the FP32
-    rounding error of the reference path itself (stated in DESIGN.md)."""
+    rounding error of the reference path itself."""
     fast, smooth = o64.tables(sf=gold["sf"])
     maps = o64.maps(gold["rec_xyz"], gold["rec_xs"], gold["dims"], gold["init"], gold["factor_inv"], gold["types"],
                     sf=gold["sf"])
