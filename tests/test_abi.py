@@ -43,3 +43,21 @@ def test_batch_device_bytes_estimate():
     assert engine.batch_device_bytes([one], exhaustiveness=1, num_modes=9) == expect
     with __import__("pytest").raises(engine.UdError):
         engine.batch_device_bytes(ligs, sf=7)
+
+
+def _header_struct_fields(name):
+    """Field names, in order, of `typedef struct { ... } name;` in include/unidock_b200.h."""
+    import re
+    from pathlib import Path
+    text = (Path(__file__).resolve().parent.parent / "include" / "unidock_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    body = re.search(r"typedef struct \{([^}]*)\}\s*" + name + r"\s*;", text).group(1)
+    return [re.match(r"\s*[\w\s]+?\b(\w+)\s*$", decl).group(1) for decl in body.split(";") if decl.strip()]
+
+
+def test_python_structs_match_the_header():
+    """The ctypes mirrors of the ABI's parameter structs list the header's
+    fields in the header's order (a field added on one side only would shift
+    every field after it)."""
+    assert [f for f, _ in engine.SearchParams._fields_] == _header_struct_fields("ud_search_params")
+    assert [f for f, _ in engine.TuneResult._fields_] == _header_struct_fields("ud_tune_result")
