@@ -41,6 +41,19 @@ def test_ligand_model_matches_reference(seed, workdir):
     assert_same_model(ref.RefLigand(path), engine.Ligand(text))
 
 
+@pytest.mark.parametrize("heavy,torsions,seed", [(1, 0, 41), (2, 0, 5), (3, 0, 6), (60, 30, 12), (130, 48, 7)])
+def test_ligand_model_matches_reference_at_size_limits(heavy, torsions, seed, workdir):
+    """A one-atom ligand, rigid two- and three-atom ones, and the largest the
+    reference parses (48 torsions, 145 atoms): the same model as the
+    reference's parser."""
+    text = synth.make_ligand(heavy, torsions, seed=seed).to_pdbqt()
+    path = workdir / f"limit{heavy}_{torsions}.pdbqt"
+    path.write_text(text)
+    M = engine.Ligand(text)
+    assert M.n_torsions == torsions
+    assert_same_model(ref.RefLigand(path), M)
+
+
 @pytest.mark.parametrize("seed", range(16))
 def test_sdf_ligand_model_matches_reference(seed, workdir):
     """SDF front end (parse_sdf_aux / parse_sdf_branch): same atoms in the same
