@@ -1,5 +1,5 @@
 """Ligands at the size limits on the GPU, mixed in one batch:
-- rigid two- and three-atom ligands (no torsions, no intramolecular pairs);
+- rigid one-, two- and three-atom ligands (no torsions, no intramolecular pairs);
 - the largest the reference parses: 48 torsions, 145 atoms and 7,798
   intramolecular pairs, more than the 4,096 pairs of the reference GPU
   search's largest size bucket (unidock/src/cuda/kernel.h MaxConfig);
@@ -19,7 +19,7 @@ from .conftest import BOX_CENTER, BOX_SIZE
 pytestmark = pytest.mark.gpu
 
 REL = 1e-4
-SIZES = [(2, 0, 5), (3, 0, 6), (130, 48, 7), (60, 30, 12)]   # heavy atoms, torsions, seed
+SIZES = [(2, 0, 5), (3, 0, 6), (130, 48, 7), (60, 30, 12), (1, 0, 41)]   # heavy atoms, torsions, seed
 
 
 @pytest.fixture(scope="module")
