@@ -1852,6 +1852,7 @@ static void search_launch(ud_batch b, const ud_search_params* params, cudaStream
             throw Error(UD_ERR_ARG, "chains_per_block must be 0 (default / autotuned) or 1..4");
         if (P.lanes_per_chain != 0 && P.lanes_per_chain != 16 && P.lanes_per_chain != 32)
             throw Error(UD_ERR_ARG, "lanes_per_chain must be 0 (default / autotuned), 16 or 32");
+        if (P.num_modes < 1) throw Error(UD_ERR_ARG, "num_modes must be >= 1");
         const int n_lig = (int)b->ligs.size();
         if (n_lig == 0) throw Error(UD_ERR_ARG, "empty batch");
         b->params = P;
@@ -1864,7 +1865,6 @@ static void search_launch(ud_batch b, const ud_search_params* params, cudaStream
         b->d_poses.alloc(n_chain * b->pose_stride);
         b->d_results.alloc(n_chain);
         b->d_queue.alloc(1);
-        if (P.num_modes < 1) throw Error(UD_ERR_ARG, "num_modes must be >= 1");
         if (modes) alloc_modes(b, s);
         SearchParams sp{};
         sp.global_steps = global_steps_for(b->ligs, P.max_step);
