@@ -9,7 +9,9 @@ refined energy, inter + intra at curl cap 1000, the quantity the search
 minimises) must match the reference's median within 0.1 kcal/mol.  The 32
 runs are 32 replicas of the ligand in one batch; every chain draws from its
 own Philox stream, as a separate seed would give.  Heavy-atom RMSD of each
-run's best pose to the reference's overall best pose is reported.
+run's best pose to the reference's overall best pose is reported.  Every
+ligand is searched with one chain per warp, two of them also with two chains
+per warp (16 lanes each).
 """
 from pathlib import Path
 
