@@ -62,6 +62,11 @@ def parse_args():
                     help="screen-fast: the headline batched screen; the others are the uneven-size detail-mode "
                          "screens (Vinardo, AD4, autotuned), the three-receptor streaming screen and the paired "
                          "one-ligand-one-receptor batches (CLI), each on a sample, printed as their own JSON line")
+    ap.add_argument("--stream-ligands", type=int, default=8192, help="ligands per receptor of the streaming screen")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="no GPU work: every rank builds its ligand shard of the first step and meets the others at "
+                         "the timing barrier and max-reduction (gloo), then rank 0 prints a JSON line; checks the "
+                         "multi-rank launch on a machine without GPUs")
     ap.add_argument("--profile-case", type=int, default=0,
                     help="profiling aid: search N ligands of the workload twice and exit (no JSON)")
     ap.add_argument("--profile-receptor", type=int, default=3000, choices=[3000, 6000, 12000],
@@ -158,7 +163,7 @@ def run_ours(args, rank, world):
     torch.cuda.set_device(dev)
     if world > 1:
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=180))
     rec = synth.make_receptor(3000, seed=1)
     center = np.zeros(3, np.float32)
     size = np.full(3, BOX, np.float32)
@@ -228,11 +233,14 @@ def run_ours(args, rank, world):
         tt = torch.tensor([t_total], device="cuda")
         torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
         t_total = float(tt.item())
-    # work accounting of the timed steps (algorithmic bytes and flops per evaluation)
-    evals_total, bytes_total, flops_total = 0, 0.0, 0.0
+    # work accounting of the timed steps (algorithmic bytes and flops per
+    # evaluation) and the search kernel's own device time in each of them (CUDA
+    # events recorded around the kernel inside the captured graph)
+    evals_total, bytes_total, flops_total, kernel_s = 0, 0.0, 0.0, 0.0
     for s in range(args.warmup, steps_total):
         ligs, b = batches[s]
         b.search_collect()
+        kernel_s += b.stats()[1] / 1e3
         _, e, ev = b.chains()
         ev = ev.reshape(len(ligs), EXHAUSTIVENESS).sum(axis=1)
         for L, n_ev in zip(ligs, ev):
@@ -328,16 +336,17 @@ def run_ours(args, rank, world):
         bp.search_collect()
         plain = len(sub) / (e0.elapsed_time(e1) / 1e3)
 
-    adjoint = adjoint_leg(maps) if rank == 0 and args.adjoint_poses > 0 else None
+    adjoint = adjoint_leg(maps, engine.l2_peak_gbs()) if rank == 0 and args.adjoint_poses > 0 else None
 
     result = None
     if rank == 0:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
         hbm_peak = peaks.get("hbm_gbs", 6650.0)
         fp32_peak = engine.fp32_peak_tflops()
-        ms_launch = t_total * 1e3 / args.steps
-        achieved_gbs = bytes_total / t_total / 1e9
-        achieved_tf = flops_total / t_total / 1e12
+        l2_peak = engine.l2_peak_gbs()
+        ms_launch = kernel_s * 1e3 / args.steps
+        achieved_gbs = bytes_total / kernel_s / 1e9
+        achieved_tf = flops_total / kernel_s / 1e12
         result = {
             "metric": METRIC, "value": round(value, 3), "unit": "ligands/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_total * 1e3 / args.steps, 3),
@@ -354,17 +363,26 @@ def run_ours(args, rank, world):
             "plain_form_ligands_per_s": None if plain is None else round(plain, 3),
             "batched_over_plain": None if plain is None else round(value / plain, 2),
             "evals_per_s": round(evals_total / t_total, 1),
-            "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 2), "peak": hbm_peak, "unit": "GB/s",
-                         "frac": round(achieved_gbs / hbm_peak, 4),
+            # the search reads L2-resident maps and pair tables: its memory
+            # ceiling is L2 read bandwidth (measured here), not HBM; DRAM
+            # traffic per launch stays at the maps' first load
+            "roofline": {"bound": "l2", "achieved": round(achieved_gbs, 2), "peak": round(l2_peak, 1),
+                         "unit": "GB/s", "frac": round(achieved_gbs / l2_peak, 4),
                          "traffic": SEARCH_LAUNCH_DRAM_BYTES if B == 1024 else None,
-                         "traffic_note": "DRAM bytes per launch from one ncu capture of this workload; the "
-                                         "achieved figure counts algorithmic L2 bytes (maps stay L2-resident)",
-                         "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)",
+                         "traffic_note": "DRAM bytes (read + write) per launch from one ncu capture of this "
+                                         "workload; the achieved figure counts algorithmic L2 bytes per "
+                                         "evaluation (32 per grid atom + 16 per intramolecular pair)",
+                         "peak_source": "measured L2 read probe on this GPU (ud_device_l2_peak: 32 MB buffer, "
+                                        "16-byte L2-only loads from every SM, best of 5, CUDA events)",
                          "kernel": "ud::dev::search_kernel",
+                         "ms_per_launch": round(ms_launch, 3),
+                         "timing": "CUDA events recorded around the search kernel inside each timed step's graph",
+                         "hbm": {"achieved": round(SEARCH_LAUNCH_DRAM_BYTES / (ms_launch / 1e3) / 1e9, 2)
+                                 if B == 1024 else None, "peak": hbm_peak, "unit": "GB/s",
+                                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)"},
                          "fp32": {"achieved": round(achieved_tf, 3), "peak": round(fp32_peak, 2),
                                   "unit": "TFLOP/s", "frac": round(achieved_tf / fp32_peak, 4),
-                                  "peak_source": "measured FMA probe (ud_device_fp32_peak)"},
-                         "ms_per_launch": round(ms_launch, 3)},
+                                  "peak_source": "measured FMA probe (ud_device_fp32_peak)"}},
             "e2e": {"value": round(e2e_value, 3), "unit": "ligands/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h),
                     "path": "PDBQT text -> parse (all host threads) -> upload into a reused batch handle -> "
@@ -381,7 +399,7 @@ def run_ours(args, rank, world):
     return result
 
 
-def adjoint_leg(maps, n_ligands=256, reps=5):
+def adjoint_leg(maps, l2_peak, n_ligands=256, reps=5):
     """Differentiation workload: 65,536 fixed poses over 256 ligands of the
     screen's size distribution (centre uniform in the box, uniform random unit
     quaternion, torsions U(-pi, pi)); energy + pose-layout gradient + the 6
@@ -421,9 +439,24 @@ def adjoint_leg(maps, n_ligands=256, reps=5):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / reps
+    # algorithmic bytes per launch: per pose the weighted maps and pair rows
+    # once for the energy / pose gradient and once per term for the weight
+    # gradient (32 B per grid atom and map set, 16 B per pair and table), plus
+    # the pose in and the energy, gradient and weight gradient out
+    per_lig = []
+    for L in ligs:
+        n_grid = int(np.sum(L.export()["xs"] < 36))
+        per_lig.append((1 + nt) * (32.0 * n_grid + 16.0 * L.n_pairs) + 4.0 * (stride + 1 + stride + nt))
+    bytes_launch = per * float(np.sum(per_lig))
+    gbs = bytes_launch / (ms / 1e3) / 1e9
     return {"workload": f"{n} fixed poses over {n_ligands} ligands, Vina, energy + pose gradient + "
                         f"{nt} term-weight gradients (exact), FP32", "poses_per_s": round(n / (ms / 1e3), 1),
-            "ms_per_launch": round(ms, 3)}
+            "ms_per_launch": round(ms, 3),
+            "roofline": {"bound": "l2", "kernel": "ud::dev::adjoint_kernel", "achieved": round(gbs, 1),
+                         "peak": round(l2_peak, 1), "unit": "GB/s", "frac": round(gbs / l2_peak, 4),
+                         "algorithmic_bytes_per_launch": round(bytes_launch),
+                         "note": "the 7 map sets (weighted + 6 term maps, 153 MB at 61^3) exceed the 126 MB L2, "
+                                 "so part of the reads come from HBM"}}
 
 
 # ------------------------------------------------------------------ other workloads
@@ -529,49 +562,68 @@ def run_paired(args):
 
 def run_stream(args):
     """Streaming screen: search_mode balance (exhaustiveness 384, max_step 40),
-    ligands with U{10..100} heavy atoms and U{0..30} torsions, through the
-    public API with batches pipelined on two streams (parse / post-process of
-    one batch overlapping the search of the next), against three receptors:
-    3000 atoms with a 22.5 A box, 6000 with 30 A, 12000 with 36 A (0.375 A)."""
+    ligands with U{10..100} heavy atoms and U{0..30} torsions, fed slot by slot
+    (64 ligands a slot, 4 result areas) into one persistent search kernel per
+    receptor (ud_stream_*), against three receptors: 3000 atoms with a 22.5 A
+    box, 6000 with 30 A, 12000 with 36 A (0.375 A).  The host parses each slot,
+    pushes it while the kernel works on earlier ones, and collects (clustering,
+    refinement, final scores) and writes each finished slot's results; the
+    wall clock from the first push to the kernel's end gives sustained
+    ligands/s."""
     import torch
     from unidock_tools import engine, synth
-    per_batch = args.batch if args.batch != 1024 else 512
-    n_batches = max(2, args.steps)
+    n_lig = args.stream_ligands
+    slot, ring = 64, 4
+    n_slots = (n_lig + slot - 1) // slot
     out = []
     for n_rec, box in ((3000, 22.5), (6000, 30.0), (12000, 36.0)):
         rec = synth.make_receptor(n_rec, seed=1)
         maps = engine.Maps(rec.xyz, rec.xs, np.zeros(3, np.float32), np.full(3, box, np.float32), SPACING)
         dims, _, _, n_maps = maps.info()
-        texts = [l.to_pdbqt() for l in synth.ligand_set(per_batch * n_batches, seed=100000 + n_rec,
-                                                          heavy=(10, 100), torsions=(0, 30))]
-        P = dict(exhaustiveness=384, max_step=40, seed=42, form=1, use_graph=1, refine_step=args.refine_step)
-        streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+        texts = [l.to_pdbqt() for l in synth.ligand_set(n_lig, seed=100000 + n_rec, heavy=(10, 100),
+                                                        torsions=(0, 30))]
+        # the stream's per-chain shared memory is sized for the largest ligand it takes
+        probe = engine.parse_ligands(texts)
+        max_atoms = max(L.n_atoms for L in probe)
+        max_tors = max(L.n_torsions for L in probe)
+        del probe
         torch.cuda.synchronize()
+        st = engine.Stream(maps, exhaustiveness=384, max_step=40, seed=42, refine_step=args.refine_step,
+                           slot_ligands=slot, max_slots=n_slots, ring=ring, max_atoms=max_atoms,
+                           max_torsions=max_tors, timeout_ms=120000)
         t0 = time.perf_counter()
-        pending = None
-        for k in range(n_batches):
-            st = streams[k % 2].cuda_stream
-            ligs = engine.parse_ligands(texts[k * per_batch:(k + 1) * per_batch])
-            bt = engine.Batch(maps, ligs)
-            bt.search_launch(**P, stream=st)
-            if pending is not None:
-                pending[0].search_collect(stream=pending[1])
-                [pending[0].write(i) for i in range(per_batch)]
-            pending = (bt, st)
-        pending[0].search_collect(stream=pending[1])
-        [pending[0].write(i) for i in range(per_batch)]
-        torch.cuda.synchronize()
+        held = {}
+        written = 0
+        for k in range(n_slots):
+            ligs = engine.parse_ligands(texts[k * slot:(k + 1) * slot])
+            if k >= ring:  # the result area of slot k - ring is reused by slot k
+                st.collect(k - ring)
+                written += sum(len(st.write(k - ring, i)) > 0 for i in range(len(held[k - ring])))
+                del held[k - ring]
+            st.push(ligs)
+            held[k] = ligs
+        st.close()
+        for k in sorted(held):
+            st.collect(k)
+            written += sum(len(st.write(k, i)) > 0 for i in range(len(held[k])))
+        evals = st.finish()
         t = time.perf_counter() - t0
+        del st
         map_bytes = int(dims.prod()) * n_maps * 4
-        out.append({"receptor_atoms": n_rec, "box": box, "grid": [int(d) for d in dims],
-                    "ligands": per_batch * n_batches, "ligands_per_s": round(per_batch * n_batches / t, 2),
-                    "map_mbytes": round(map_bytes / 1e6, 1), "maps_fit_l2_126mb": map_bytes < 126e6})
+        out.append({"receptor_atoms": n_rec, "box": box, "grid": [int(d) for d in dims], "ligands": n_lig,
+                    "ligands_written": int(written), "ligands_per_s": round(n_lig / t, 2),
+                    "evals_per_s": round(evals / t, 1), "seconds": round(t, 1),
+                    "max_atoms": int(max_atoms), "max_torsions": int(max_tors),
+                    "map_mbytes": round(map_bytes / 1e6, 1), "xpair_map_mbytes": round(2 * map_bytes / 1e6, 1),
+                    "maps_fit_l2_126mb": map_bytes < 126e6})
     return {"metric": "sustained ligands/s on 1 B200 (streaming screen)", "unit": "ligands/s", "n_gpus": 1,
             "higher_is_better": True, "dtype": "f32", "data": "synthetic",
             "value": round(min(r["ligands_per_s"] for r in out), 3),
             "config": {"workload": "streaming screen, Vina, search_mode balance (exhaustiveness 384, max_step 40), "
-                                   "ligands U{10..100} heavy / U{0..30} torsions, batches pipelined on two streams, "
-                                   "wall clock", "ligands_per_batch": per_batch, "receptors": out}}
+                                   "ligands U{10..100} heavy / U{0..30} torsions, one persistent kernel per "
+                                   "receptor fed 64-ligand slots from page-locked memory (4 result areas), "
+                                   f"refine_step {args.refine_step}, wall clock from the first push to the "
+                                   "kernel's end", "ligands_per_slot": slot, "receptors": out}}
 
 
 # ------------------------------------------------------------------ reference CPU path
@@ -628,10 +680,58 @@ def run_reference(args, rank, world):
     }
 
 
+def relaunch(args) -> int:
+    """`--gpus N` (N > 1) run directly: start N ranks of this script under
+    torch.distributed.run on this node (rendezvous on 127.0.0.1) and return
+    their exit status."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), str(Path(__file__).resolve())] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def run_dry(args, rank, world):
+    """The multi-rank plumbing without a GPU: each rank's ligand shard of the
+    first step, the timing barrier and the max over ranks (gloo)."""
+    import torch
+    import torch.distributed as dist
+    from unidock_tools.shard import shard
+    from unidock_tools.synth import ligand_set
+    if world > 1:
+        import datetime
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    B = args.batch
+    texts = [l.to_pdbqt() for l in ligand_set(B * world, seed=20261203, heavy=(12, 48), torsions=(0, 10))]
+    mine = shard(len(texts), rank, world, [len(t) for t in texts])
+    t = torch.tensor([float(len(mine))])
+    n = torch.tensor([float(len(mine))])
+    if world > 1:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(n, op=dist.ReduceOp.SUM)
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+    return {"dry_run": True, "metric": METRIC, "n_gpus": world, "ligands_per_step": B * world,
+            "ligands_sharded": int(n.item()), "max_rank_ligands": int(t.item()), "scaling": "weak"}
+
+
 def main():
     args = parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(relaunch(args))
     rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus == 1 else 1)))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world != args.gpus:
+        raise SystemExit(f"bench.py --gpus {args.gpus} launched with WORLD_SIZE={world}: one rank per GPU expected")
+    if args.dry_run:
+        res = run_dry(args, rank, world)
+        if res is not None:
+            print(json.dumps(res), flush=True)
+        return
     if args.profile_case > 0:
         profile_case(args)
         return

@@ -24,6 +24,7 @@ extern "C" {
 #define UD_ERR_CUDA 3     /* CUDA runtime failure (message has the CUDA error) */
 #define UD_ERR_CAPACITY 4 /* ligand exceeds a capacity limit (atoms, torsions) */
 #define UD_ERR_STATE 5    /* call out of order (e.g. results before a search) */
+#define UD_ERR_TIMEOUT 6  /* a device-side wait ran past its time limit (streaming screen) */
 
 #define UD_SF_VINA 0
 #define UD_SF_AD4 1
@@ -32,6 +33,7 @@ extern "C" {
 typedef struct ud_maps_s* ud_maps;
 typedef struct ud_ligand_s* ud_ligand;
 typedef struct ud_batch_s* ud_batch;
+typedef struct ud_stream_s* ud_stream;
 
 /* Library version (major*10000 + minor*100 + patch). */
 int ud_version(void);
@@ -264,7 +266,7 @@ int ud_batch_device_bytes(const ud_ligand* ligs, int n, int sf, const ud_search_
 typedef struct {
     int chains_per_block;      /* warps per CTA */
     int lanes_per_chain;       /* lanes per chain: 32 (a warp) or 16 (half a warp) */
-    int bfgs_cap;              /* BFGS iteration cap, 0 = per-ligand */
+    int bfgs_cap;              /* BFGS iteration cap: always 0 (caps are not tuned) */
     int n_sample;              /* ligands of the batch in the tuning sample */
     int n_tried;               /* configurations timed */
     float ligands_per_s;       /* sample throughput of the picked configuration */
@@ -274,14 +276,15 @@ typedef struct {
 
 /* Autotuner (no counterpart in the reference): times the batched search on a
  * sample of the batch (ligands spread over its size order, enough chains to
- * fill the GPU twice, the caller's exhaustiveness, at most 40 MC steps):
- * first the launch shape, warps per CTA in {4, 2, 1} x lanes per chain in
- * {32, 16}, uncapped; then BFGS caps in {16, 10, 6} on the shape picked.  A
- * configuration replaces the best so far only when it is more than 3% faster
- * and its mean best energy is within 0.1 kcal/mol of the default's (4 warps,
- * 32 lanes, no cap).  Searches of this
- * batch with chains_per_block = 0, lanes_per_chain = 0 and bfgs_cap < 0 then
- * use it.  Synchronous; takes about 10 short searches. */
+ * fill the GPU twice, the caller's exhaustiveness, at most 40 MC steps) at
+ * each launch shape, warps per CTA in {4, 2, 1} x lanes per chain in {32, 16}.
+ * A shape replaces the best so far only when it is more than 3% faster and its
+ * mean best energy is within 0.1 kcal/mol of the default's (4 warps, 32
+ * lanes).  BFGS iteration caps are not tuned (bfgs_cap in the result is 0):
+ * every cap tried moved the search's best-energy distribution away from the
+ * reference's at the fast screen settings.  Searches of this batch with
+ * chains_per_block = 0 and lanes_per_chain = 0 then use the shape picked.
+ * Synchronous; takes about 7 short searches. */
 int ud_autotune(ud_batch batch, const ud_search_params* params, ud_tune_result* out, void* stream);
 
 /* Run the Monte-Carlo + BFGS search of every ligand of the batch.
@@ -310,9 +313,11 @@ int ud_search_chains(ud_batch batch, float* poses, int pose_stride, float* e, in
  * and latency-critical loops where an allocation's implicit device-wide
  * synchronisation is not acceptable.
  *
- * Runs the batched persistent search (form 1; params->form, chains_per_block
- * and use_graph are ignored) on `stream` and returns without waiting.  The
- * caller owns every output, all in device memory of the current device:
+ * Runs the batched persistent search (form 1; params->form and use_graph are
+ * ignored) on `stream` and returns without waiting.  chains_per_block,
+ * lanes_per_chain and bfgs_cap resolve as in ud_search (0 / 0 / <0 = the
+ * batch's autotuned values when it was tuned).  The caller owns every output,
+ * all in device memory of the current device:
  *   d_poses     [n_ligands * exhaustiveness][pose_stride] best pose per chain
  *               (chain-major per ligand, as ud_search_chains), pose_stride >=
  *               7 + the batch's largest torsion count; only the first 7 + T
@@ -321,18 +326,21 @@ int ud_search_chains(ud_batch batch, float* poses, int pose_stride, float* e, in
  *   d_evals     [n_ligands * exhaustiveness] evaluations per chain, or NULL.
  * Results equal those of ud_search_launch + ud_search_chains with the same
  * params.  No clustering or rescoring is done (that host part allocates).
+ * An empty batch is refused (UD_ERR_ARG), as ud_search refuses it.
  *
- * Scratch (work-queue counter, ligand order, per-chain records) lives in one
- * static device array of about 2.1 MB that each GPU using the library holds
- * until the process exits; the call clears what must start at zero.  Limits:
- * at most 8192 ligands and 131072 chains (ligands x exhaustiveness) per call,
- * beyond which it returns UD_ERR_CAPACITY without launching anything.  All
- * calls on one device share that scratch, so calls whose work overlaps on
- * that device (issued on two streams, or from two threads) race: order them
- * on one stream or synchronise between them.  Each device has its own copy,
- * so calls on different devices do not interfere.  The first call on each
- * device looks up the scratch's device address (cudaGetSymbolAddress) with
- * that device current; make that first call before any stream capture. */
+ * Scratch (the work-queue counter and one record per chain) lives in one
+ * static device array of 3,145,984 bytes (about 3.1 MB) that each GPU using
+ * the library holds until the process exits; the call clears what must start
+ * at zero.  The ligand order comes from the batch's own device memory, filled
+ * when the batch was created.  Limit: at most 131072 chains (ligands x
+ * exhaustiveness) per call, beyond which it returns UD_ERR_CAPACITY without
+ * launching anything.  All calls on one device share that scratch, so calls
+ * whose work overlaps on that device (issued on two streams, or from two
+ * threads) race: order them on one stream or synchronise between them.  Each
+ * device has its own copy, so calls on different devices do not interfere.
+ * The first call on each device looks up the scratch's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call before
+ * any stream capture. */
 int ud_search_device_noalloc(ud_batch batch, const ud_search_params* params, float* d_poses, int pose_stride,
                              float* d_energies, int* d_evals, void* stream);
 /* Number of modes kept for ligand `lig` after clustering and rescoring. */
@@ -396,11 +404,76 @@ int ud_refine(ud_batch batch, const int* pose_ligand, float* poses, int n_poses,
  * without --no_refine (vina.cpp:1168-1243). */
 int ud_score_terms_receptor(ud_batch batch, const int* pose_ligand, const float* poses, int n_poses, int pose_stride,
                             float* out, void* stream);
+/* ---------------------------------------------------------------- streaming screen
+ * One persistent search kernel fed slot by slot while it runs.  The reference
+ * CLI has no such mode; it parses and docks one batch after another
+ * (unidock/src/main/main.cpp:975-1070).  The host packs each slot of ligands
+ * into page-locked memory, copies it into a device arena and publishes it;
+ * the kernel, launched by ud_stream_create, takes the published slots' (ligand,
+ * chain) items as they arrive, waiting at most timeout_ms for the next slot;
+ * each finished slot's modes are clustered and refined on SMs the kernel
+ * leaves free and scored on the host.  Every buffer is allocated at creation,
+ * so pushing and collecting never synchronise the device.  Not thread-safe
+ * per stream.  Ligand handles must live until their slot is collected and its
+ * results read. */
+typedef struct {
+    int slot_ligands;   /* ligands per slot (rounded up to a multiple of 16) */
+    int max_slots;      /* slots the stream takes in all (size of the device arena) */
+    int ring;           /* result areas: slot s writes area s % ring, so slot s may be pushed
+                           only after slot s - ring was collected */
+    int max_atoms;      /* largest ligand the stream takes (shared memory per chain is sized by it) */
+    int max_torsions;
+    int timeout_ms;     /* longest wait of the kernel for the next slot (0 = 60000) */
+} ud_stream_config;
+
+/* Create the stream and launch its kernel.  params: exhaustiveness, max_step
+ * (1..11655 required: a chain's step count must not depend on its slot),
+ * num_modes, min_rmsd, energy_range, seed, chains_per_block, bfgs_cap (> 0
+ * caps, else per-ligand), refine_step; one chain per warp.  A ligand of
+ * global id g (slot s, position i: g = s * slot_ligands + i) draws the same
+ * random streams as ligand g of a batch with ud_search, so a stream of full
+ * slots gives the chains of one batch of all its ligands. */
+int ud_stream_create(ud_maps maps, const ud_search_params* params, const ud_stream_config* cfg, ud_stream* out);
+/* Pack, copy and publish the next slot (1..slot_ligands ligands); *slot = its
+ * index.  UD_ERR_STATE while slot (index - ring) is not collected;
+ * UD_ERR_CAPACITY past max_slots, for a ligand beyond max_atoms /
+ * max_torsions, or when the arena is full. */
+int ud_stream_push(ud_stream stream, const ud_ligand* ligs, int n, int* slot);
+/* No further slot: the kernel ends once the published slots are done. */
+int ud_stream_close(ud_stream stream);
+/* Wait until every chain of the slot is done, cluster and refine its modes
+ * and compute the final scores (as ud_search_collect for a batch). */
+int ud_stream_collect(ud_stream stream, int slot);
+/* Results of a collected slot, as ud_result_count / ud_result_mode /
+ * ud_result_write and ud_search_chains for a batch (lig = position in the slot). */
+int ud_stream_result_count(ud_stream stream, int slot, int lig, int* n_modes);
+int ud_stream_result_mode(ud_stream stream, int slot, int lig, int k, float* pose, float energies[8]);
+int ud_stream_result_write(ud_stream stream, int slot, int lig, int format, char* buf, size_t cap, size_t* len);
+int ud_stream_chains(ud_stream stream, int slot, float* poses, int pose_stride, float* e, int* evals);
+/* Wait for the kernel to end (close the stream first, or it ends when a
+ * wait for the next slot runs out: UD_ERR_TIMEOUT); *evals = evaluations of
+ * the collected slots. */
+int ud_stream_finish(ud_stream stream, long long* evals);
+int ud_stream_destroy(ud_stream stream);
+
 /* Measured FP32 FMA throughput of the current device in TFLOP/s (roofline
  * denominator of the search kernels).  No counterpart in the reference. */
 int ud_device_fp32_peak(float* tflops);
-/* Evaluations and device time of the last search. */
+/* Measured L2 read bandwidth of the current device in GB/s: a 32 MB buffer
+ * held in L2 read with L2-only 16-byte loads by every SM (the roofline
+ * denominator of the search kernel, whose grid maps and pair tables stay
+ * L2-resident).  Allocates 32 MB of device memory for the duration of the
+ * call.  No counterpart in the reference. */
+int ud_device_l2_peak(float* gbs);
+/* Evaluations and device time of the last search: the search kernel's own
+ * time (between events recorded around it; in the graph form, event nodes
+ * inside the graph), without the clustering, refinement and copies after it. */
 int ud_search_stats(ud_batch batch, long long* evals, float* kernel_ms);
+/* Host-to-device bytes of the batch's last topology upload (ud_batch_create /
+ * ud_batch_reset): ligand records, atoms, nodes, pair slots and incidence
+ * lists, grid-atom list, work order (and AD4 charges / pair coefficients).
+ * No counterpart in the reference (measurement). */
+int ud_batch_upload_bytes(ud_batch batch, size_t* bytes);
 
 #ifdef __cplusplus
 }

@@ -12,7 +12,8 @@ import numpy as np
 LIB = Path(__file__).resolve().parent / "_ref" / "libudref.so"
 # the reference's source tree (oracle/Makefile's REF points into it); only the
 # checkers read its own test inputs, and only when it is present
-REFERENCE_TREE = Path(os.environ.get("UD_REFERENCE_TREE", "/root/reference"))
+# (UD_REFERENCE_TREE, else a checkout beside this repository)
+REFERENCE_TREE = Path(os.environ.get("UD_REFERENCE_TREE", Path(__file__).resolve().parents[2] / "reference"))
 _lib = None
 
 
@@ -101,6 +102,7 @@ def lib():
         L.udref_refine.argtypes = [vp, vp, fp, fp, fp, C.c_int, fp]
         L.udref_nc_score.argtypes = [vp, vp, fp, fp, fp, C.c_float, fp]
         L.udref_cluster.argtypes = [vp, C.c_int, fp, C.c_int, fp, C.c_float, C.c_int, ip]
+        L.udref_final_scores.argtypes = [vp, vp, C.c_int, fp, C.c_int, fp, C.c_int, fp]
         L.udref_maps_bias.argtypes = [vp, C.c_char_p]
         L.udref_ligand_bias.argtypes = [vp, C.c_char_p]
         L.udref_ad4_maps_read.restype = vp
@@ -306,6 +308,21 @@ class RefLigand:
         out = np.zeros(max(len(e), 1), np.int32)
         n = lib().udref_cluster(self.h, len(e), _f(poses), poses.shape[1], _f(e), min_rmsd, max_modes, _i(out))
         return out[:n]
+
+    def final_scores(self, maps, poses, order_e=None, receptor=True):
+        """The reference's post-search scoring of this ligand's modes
+        (Vina::global_search_gpu after its refinement, vina.h:232-343, score_gpu
+        vina.cpp:1245-1322) from the given mode poses; `order_e` orders them
+        for the choice of the intramolecular energy (Vina / Vinardo).  Rows in
+        the reference's final order: [input index, total, rmsd lb, rmsd ub,
+        inter + intra, inter, intra, conf-independent part, unbound]."""
+        poses = np.ascontiguousarray(poses, np.float32)
+        n = len(poses)
+        oe = None if order_e is None else np.ascontiguousarray(order_e, np.float32)
+        out = np.zeros((max(n, 1), 9), np.float32)
+        k = lib().udref_final_scores(self.h, maps.h, n, _f(poses), poses.shape[1],
+                                     _f(oe) if oe is not None else None, int(bool(receptor)), _f(out))
+        return out[:k]
 
     def mc(self, maps, seed, n_chains, global_steps, local_steps=None, threads=1, hunt_cap=10.0):
         steps = (25 + self.n_atoms) // 3 if local_steps is None else local_steps

@@ -413,6 +413,77 @@ int udref_nc_score(void* lh, void* mh, const float* pos, const float* quat, cons
     return 0;
 }
 
+// Final scores of one ligand's modes as Vina::global_search_gpu computes them
+// after its search (vina.h:232-343 with score_gpu, vina.cpp:1245-1322), from
+// the modes' poses as they stand after any refinement:
+//   Vina / Vinardo: the poses are ordered by `order_e` (the refinement's last
+//     energy, or max when a pose ended outside the box), the intramolecular
+//     energy of the first is taken (model::eval_intramolecular against the
+//     receptor atoms when `receptor`, else the maps), and each pose scores
+//     conf_independent(inter + intra - that energy), inter from non_cache::eval
+//     (slope 1e6) or the maps at cap 1000;
+//   AD4: inter from the maps, total = inter + conf_independent(0), unbound -intra.
+// The poses are then sorted by that total and the RMSD bounds taken against
+// the best.  out (9 floats per mode, in final order): input index, total,
+// rmsd lb, rmsd ub, inter + intra, inter, intra, conf-independent part, unbound.
+int udref_final_scores(void* lh, void* mh, int n, const float* poses, int pose_stride, const float* order_e,
+                       int receptor, float* out) {
+    auto L = (RefLigand*)lh;
+    auto M = (RefMaps*)mh;
+    const bool ad4 = L->sf->get_atom_typing() == atom_type::AD;
+    const vec authentic_v(1000, 1000, 1000);
+    model mm = receptor ? docking_model(M, L) : L->m;
+    const igrid& scorer = receptor ? static_cast<const igrid&>(nc_of(M)) : *M->ig;
+    if (receptor) nc_of(M).slope = 1e6;
+    struct Mode { conf c; fl e; int src; fl inter, intra, conf_indep, unbound, lb, ub; };
+    std::vector<Mode> v;
+    for (int i = 0; i < n; ++i) {
+        const float* p = poses + (size_t)i * pose_stride;
+        v.push_back(Mode{make_conf(mm, p, p + 3, p + 7), order_e ? (fl)order_e[i] : 0, i, 0, 0, 0, 0, 0, 0});
+    }
+    if (v.empty()) return 0;
+    double intramolecular = 0;
+    if (!ad4) {
+        std::stable_sort(v.begin(), v.end(), [](const Mode& a, const Mode& b) { return a.e < b.e; });
+        mm.set(v[0].c);
+        intramolecular = mm.eval_intramolecular(*L->pre, scorer, authentic_v);
+    }
+    for (auto& x : v) {
+        mm.set(x.c);
+        const double grids = scorer.eval(mm, authentic_v[1]);
+        const double lig_intra = mm.evali(*L->pre, authentic_v);
+        x.inter = grids;
+        x.intra = lig_intra;
+        if (ad4) {
+            x.conf_indep = L->sf->conf_independent(mm, 0);
+            x.e = grids + x.conf_indep;
+            x.unbound = -lig_intra;
+        } else {
+            const double total = L->sf->conf_independent(mm, grids + lig_intra - intramolecular);
+            x.e = total;
+            x.conf_indep = total - (grids + lig_intra - intramolecular);
+            x.unbound = intramolecular;
+        }
+    }
+    std::stable_sort(v.begin(), v.end(), [](const Mode& a, const Mode& b) { return a.e < b.e; });
+    mm.set(v[0].c);
+    const model best = mm;
+    for (size_t k = 0; k < v.size(); ++k) {
+        mm.set(v[k].c);
+        float* o = out + 9 * k;
+        o[0] = (float)v[k].src;
+        o[1] = v[k].e;
+        o[2] = mm.rmsd_lower_bound(best);
+        o[3] = mm.rmsd_upper_bound(best);
+        o[4] = v[k].inter + v[k].intra;
+        o[5] = v[k].inter;
+        o[6] = v[k].intra;
+        o[7] = v[k].conf_indep;
+        o[8] = v[k].unbound;
+    }
+    return (int)v.size();
+}
+
 // Clustering of one ligand's chain results as the reference's GPU path does
 // it: each chain's best pose through add_to_output_container (coords.cpp:44-68)
 // with num_saved_mins = max_modes, then Vina::remove_redundant (vina.cpp:

@@ -1,0 +1,207 @@
+"""Accuracy of the adjoint kernel on the differentiation workload's own pose
+set: the bench's adjoint leg, 65,536 fixed poses over 256 ligands of the
+batched screen's size distribution (synth.ligand_set(256, seed=7), 256 poses a
+ligand: centre uniform in the 22.5 A box, uniform random unit quaternion,
+torsions U(-pi, pi)), 3000-atom receptor, 0.375 A spacing (61^3 points).
+
+A seeded subsample of 2,048 poses, 8 of each of the 256 ligands:
+  * reference mode: energy and pose gradient against the reference's own
+    model::eval_deriv (FP32 CPU, oracle/_ref) on all 2,048, within 1e-4
+    relative (the torque mapped to the quaternion gradient 2 (0, tau) (x) q);
+  * exact mode: the pose gradient against FP64 central differences (h = 1e-5,
+    quaternion renormalised; h = 1e-6 where the two disagree, i.e. a
+    trilinear-cell or table-bin kink lies within h) of the FP64 restatement's
+    energy, on one pose of each ligand (256), within 1e-4 relative;
+  * the 6 term-weight gradients against FP64 central differences over the
+    weights (h = 1e-3; maps and tables are linear in the weights, so the
+    perturbed FP64 maps are the base maps plus h times the unweighted term
+    maps) on the same 256 poses, within 1e-4 relative.
+Max and median relative errors are printed for each.
+
+Two conditioning effects are allowed for, and counted and printed:
+  * an atom outside the box adds slope x distance (slope 1e6 kcal/mol/A,
+    vina.cpp:514) to the energy, so an FP32 rounding difference of one unit in
+    the last place of a coordinate (about 1e-6 A at 11 A) moves the energy by
+    about 1 kcal/mol whatever the implementation; such poses are held to 1e-4
+    relative plus 4 ulp x slope per out-of-box atom;
+  * some poses are ill-conditioned in FP32 as such: large opposing atom
+    forces cancel in the total force and torque, and the reference's own FP32
+    model::eval_deriv misses the FP64 difference there by more than 1e-4 too;
+    a pose above 1e-4 is accepted only when the reference's FP32 gradient is
+    at least half as far from the FP64 difference as the engine's.
+"""
+import tempfile
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import ref
+from oracle.oracle import Oracle, VINA_W
+from unidock_tools import engine, synth
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not ref.available(), reason="reference build missing")]
+
+BOX = 22.5
+SPACING = 0.375
+N_LIG = 256
+PER = 256          # poses per ligand in the full set (65,536)
+SUB = 8            # poses per ligand in the subsample (2,048)
+REL = 1e-4
+GLUE = (21, 24, 27, 30)
+FOLD = {19: 0, 22: 0, 25: 0, 28: 0, 20: 1, 23: 1, 26: 1, 29: 1}
+
+
+def quat_grad(tau, q):
+    q0, qv = q[0], q[1:]
+    return np.concatenate([[-2.0 * np.dot(tau, qv)], 2.0 * (q0 * tau + np.cross(tau, qv))])
+
+
+@pytest.fixture(scope="module")
+def workload(receptor):
+    center, size = np.zeros(3, np.float32), np.full(3, BOX, np.float32)
+    ligs_s = synth.ligand_set(N_LIG, seed=7, heavy=(12, 48), torsions=(0, 10))
+    texts = [l.to_pdbqt() for l in ligs_s]
+    ligs = [engine.Ligand(t) for t in texts]
+    exports = [L.export() for L in ligs]
+    types = sorted({FOLD.get(int(t), int(t)) for ex in exports for t in ex["xs"] if t < 36 and t not in GLUE})
+    maps = engine.Maps(receptor.xyz, receptor.xs, center, size, SPACING, types=types)
+    B = engine.Batch(maps, ligs)
+    stride = 7 + B.max_torsions
+    rng = np.random.default_rng(2048)
+    lig_of, poses = [], []
+    for i, L in enumerate(ligs):
+        full = synth.random_poses(PER, L.n_torsions, -BOX / 2, BOX / 2, seed=1000 + i)  # as the bench builds it
+        for k in np.sort(rng.choice(PER, SUB, replace=False)):
+            p = np.zeros(stride, np.float32)
+            p[:7 + L.n_torsions] = full[k]
+            poses.append(p)
+            lig_of.append(i)
+    return dict(center=center, size=size, texts=texts, ligs=ligs, exports=exports, types=types, maps=maps, B=B,
+                lig_of=np.array(lig_of, np.int32), poses=np.array(poses, np.float32), stride=stride)
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(1.0, np.linalg.norm(b)))
+
+
+def test_reference_mode_on_subsample_matches_reference(receptor, workload):
+    w = workload
+    e, g, _ = w["B"].score_adjoint(w["lig_of"], w["poses"], 1000.0, 1000.0, exact=False, weights_grad=False)
+    R = ref.RefMaps(receptor.xyz, receptor.xs, w["center"], w["size"], SPACING, types=w["types"])
+    e_err, g_err, penalty_limited = [], [], []
+    with tempfile.TemporaryDirectory() as d:
+        refs = {}
+        for k, (li, P) in enumerate(zip(w["lig_of"], w["poses"])):
+            if li not in refs:
+                p = Path(d) / f"l{li}.pdbqt"
+                p.write_text(w["texts"][li])
+                refs[li] = ref.RefLigand(p)
+            T = w["ligs"][li].n_torsions
+            er, gr, xyz = refs[li].eval_deriv(R, P[:7 + T], 1000.0, 1000.0)
+            gr = gr.astype(np.float64)
+            want = np.concatenate([gr[:3], quat_grad(gr[3:6], P[3:7].astype(np.float64)), gr[6:]])
+            d = abs(float(e[k]) - er)
+            e_err.append(d / max(1.0, abs(er)))
+            g_err.append(rel(g[k, :7 + T], want))
+            if e_err[-1] > REL:  # conditioning of the out-of-box penalty (see the module docstring)
+                out = np.sum(np.any((xyz < w["center"] - BOX / 2) | (xyz > w["center"] + BOX / 2), axis=1))
+                ulp = float(np.spacing(np.float32(np.abs(xyz).max())))
+                assert out > 0 and d <= REL * max(1.0, abs(er)) + 4 * ulp * 1e6 * out, (k, li, float(e[k]), er, out)
+                penalty_limited.append((k, li, float(e[k]), er, int(out)))
+    print(f"reference mode, {len(e_err)} poses of {N_LIG} ligands: energy max {max(e_err):.3g} median "
+          f"{np.median(e_err):.3g}; pose gradient max {max(g_err):.3g} median {np.median(g_err):.3g} (relative); "
+          f"{len(penalty_limited)} pose(s) above 1e-4 within the out-of-box penalty's conditioning "
+          f"(pose, ligand, engine, reference, atoms out): {penalty_limited}")
+    assert max(g_err) <= REL
+    assert len(penalty_limited) * 100 <= len(e_err)
+
+
+@pytest.fixture(scope="module")
+def fp64(receptor, workload):
+    """FP64 restatement: base maps / tables and the unweighted per-term ones."""
+    w = workload
+    o = Oracle(np.float64)
+    dims, init, fac, _ = w["maps"].info()
+    finv = (np.float32(1.0) / fac).astype(np.float32)   # grid::m_factor_inv, an FP32 reciprocal (grid.cpp:25-38)
+    sm = {t: k for k, t in enumerate(w["types"])}
+    oligs = [o.ligand(ex, sm) for ex in w["exports"]]
+
+    def build(weights):
+        fast, smooth = o.tables(weights=weights)
+        mp = o.maps(receptor.xyz, receptor.xs, dims, init, finv, w["types"], weights=weights)
+        return smooth, mp
+
+    grid = lambda mp: o.grid(mp, dims, init, fac, finv)
+    smooth, mp = build(VINA_W)
+    # maps and tables at w +- h e_t for each term t: linear in the weights, so
+    # the base plus or minus h times the unweighted term's maps and tables
+    h = 1e-3
+    perturbed = []
+    for t in range(6):
+        u = np.zeros_like(VINA_W)
+        u[t] = 1.0
+        u[6] = VINA_W[6]
+        sm_t, mp_t = build(u)
+        perturbed.append([(smooth + s * h * sm_t, grid(mp + s * h * mp_t)) for s in (1.0, -1.0)])
+    return o, oligs, smooth, grid(mp), perturbed, h
+
+
+def test_exact_mode_and_weight_gradients_on_subsample_match_fp64(receptor, workload, fp64):
+    w = workload
+    o, oligs, smooth, G, perturbed, h = fp64
+    sel = np.arange(0, len(w["poses"]), SUB)   # the first subsampled pose of every ligand
+    lig_of, P = w["lig_of"][sel], w["poses"][sel]
+    e, g, dw = w["B"].score_adjoint(lig_of, P, 1000.0, 1000.0, exact=True)
+    g_err, w_err, near_kink, fp32_limited = [], [], 0, []
+    Rm = ref.RefMaps(receptor.xyz, receptor.xs, w["center"], w["size"], SPACING, types=w["types"])
+
+    def energy(li, pose, sm, gr):
+        return o.eval_deriv(oligs[li], gr, sm, pose)[0]
+
+    for k, (li, pose) in enumerate(zip(lig_of, P)):
+        T = w["ligs"][li].n_torsions
+        x = pose[:7 + T].astype(np.float64)
+
+        def fd(h):
+            out = np.zeros(7 + T)
+            for j in range(7 + T):
+                ev = []
+                for s in (1.0, -1.0):
+                    p = x.copy()
+                    p[j] += s * h
+                    p[3:7] /= np.linalg.norm(p[3:7])
+                    ev.append(energy(li, p, smooth, G))
+                out[j] = (ev[0] - ev[1]) / (2 * h)
+            return out
+        f5, f6 = fd(1e-5), fd(1e-6)
+        ref_g = f5
+        if np.linalg.norm(f5 - f6) > 1e-5 * max(1.0, np.linalg.norm(f6)):
+            near_kink += 1
+            ref_g = f6
+        err = rel(g[k, :7 + T], ref_g)
+        if err > REL:
+            # FP32 conditioning of the pose: the reference's own FP32 gradient
+            # against the same FP64 difference (see the module docstring)
+            with tempfile.TemporaryDirectory() as d:
+                p = Path(d) / "l.pdbqt"
+                p.write_text(w["texts"][li])
+                _, gr, _ = ref.RefLigand(p).eval_deriv(Rm, pose[:7 + T], 1000.0, 1000.0)
+            gr = gr.astype(np.float64)
+            ref_err = rel(np.concatenate([gr[:3], quat_grad(gr[3:6], x[3:7]), gr[6:]]), ref_g)
+            assert ref_err >= 0.5 * err, (k, li, err, ref_err)
+            fp32_limited.append((int(k), int(li), round(err, 6), round(ref_err, 6)))
+        g_err.append(err)
+        fw = np.zeros(6)
+        for t, pm in enumerate(perturbed):
+            ev = [energy(li, x, sm, gr) for sm, gr in pm]
+            fw[t] = (ev[0] - ev[1]) / (2 * h)
+        w_err.append(rel(dw[k], fw))
+    print(f"exact mode, {len(g_err)} poses (one per ligand): pose gradient vs FP64 FD max {max(g_err):.3g} median "
+          f"{np.median(g_err):.3g} ({near_kink} within h of a kink, checked at h=1e-6); "
+          f"{len(fp32_limited)} pose(s) above 1e-4 where the reference's FP32 gradient is as far off "
+          f"(pose, ligand, engine error, reference error): {fp32_limited}; weight gradient vs FP64 FD max "
+          f"{max(w_err):.3g} median {np.median(w_err):.3g}")
+    assert max(w_err) <= REL
+    assert all(e <= REL for i, e in enumerate(g_err) if i not in {f[0] for f in fp32_limited})
+    assert len(fp32_limited) * 50 <= len(g_err)

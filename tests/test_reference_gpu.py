@@ -62,22 +62,24 @@ def test_engine_beats_reference_gpu_kernel(receptor, tmp_path, capfd):
     B.search(**P)
     t_ours = time.perf_counter() - t0
     _, kernel_ms = B.stats()
-    our_best = np.array([B.modes(i)[0][1][0] for i in range(N_LIGANDS)], np.float32)
     _, ce, _ = B.chains()
     our_chain_best = ce.reshape(N_LIGANDS, E).min(axis=1)
 
     with capfd.disabled():
-        report(N_LIGANDS, buckets, t_ref, t_ref_kernel, t_ours, kernel_ms, ref_best, our_chain_best, our_best)
+        report(N_LIGANDS, buckets, t_ref, t_ref_kernel, t_ours, kernel_ms, ref_best, our_chain_best)
     assert t_ours < t_ref
     assert kernel_ms / 1e3 < t_ref_kernel
 
 
-def report(n, buckets, t_ref, t_ref_kernel, t_ours, kernel_ms, ref_best, our_chain_best, our_best):
+def report(n, buckets, t_ref, t_ref_kernel, t_ours, kernel_ms, ref_best, our_chain_best):
     print(f"\nreference GPU search: {n / t_ref:.2f} ligands/s ({t_ref:.2f} s with its pair tables; "
           f"buckets {dict(sorted((b, len(i)) for b, i in buckets.items()))}), its kernels alone "
           f"{n / t_ref_kernel:.2f} ligands/s ({t_ref_kernel:.3f} s)")
     print(f"engine: {n / t_ours:.2f} ligands/s ({t_ours:.3f} s for ud_search), its graph alone "
           f"{n / (kernel_ms / 1e3):.2f} ligands/s ({kernel_ms / 1e3:.3f} s); speed-up {t_ref / t_ours:.1f}x "
           f"end to end, {t_ref_kernel / (kernel_ms / 1e3):.1f}x kernels")
-    print(f"median best energy: reference {np.median(ref_best):.3f}, engine search {np.median(our_chain_best):.3f}, "
-          f"engine final {np.median(our_best):.3f} kcal/mol")
+    # like with like: both numbers are the search's own energy (the best over
+    # a ligand's chains of the refined pose energy, inter + intra at curl cap
+    # 1000), before clustering, refinement and the final conf-independent score
+    print(f"median chain-best search energy: reference GPU kernel {np.median(ref_best):.3f}, engine "
+          f"{np.median(our_chain_best):.3f} kcal/mol")

@@ -91,8 +91,8 @@ def test_autotune_picks_valid_configuration(small):
     B = engine.Batch(M, ligs * 8)
     r = B.autotune(exhaustiveness=16, max_step=6, seed=1)
     assert r["chains_per_block"] in (1, 2, 4)
-    assert r["bfgs_cap"] in (0, 16, 10, 6)
-    assert r["lanes_per_chain"] in (16, 32) and r["n_tried"] == 9
+    assert r["bfgs_cap"] == 0  # BFGS caps are not tuned
+    assert r["lanes_per_chain"] in (16, 32) and r["n_tried"] == 6
     assert r["energy_shift"] <= 0.1 and r["ligands_per_s"] >= r["base_ligands_per_s"] > 0
     B.search(exhaustiveness=16, max_step=6, seed=1, form=1, chains_per_block=0, bfgs_cap=-1)
     _, e, ev = B.chains()

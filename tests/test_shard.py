@@ -59,3 +59,36 @@ def test_round_robin_and_argument_checks():
         shard(4, 2, 2)
     with pytest.raises(ValueError):
         shard(3, 0, 2, cost=[1.0])
+
+
+def test_bench_launches_one_rank_per_gpu():
+    """`bench.py --gpus 2` run directly starts two ranks itself (under
+    torch.distributed.run) and reports n_gpus 2; the dry run does no GPU work:
+    each rank shards the first step's ligands and meets the other at the
+    timing barrier and max-reduction over gloo."""
+    import json
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parent.parent
+    r = subprocess.run([sys.executable, str(root / "bench.py"), "--gpus", "2", "--dry-run", "--batch", "64"],
+                       capture_output=True, text=True, timeout=600, cwd=str(root))
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = [l for l in r.stdout.splitlines() if l.startswith("{")][-1]
+    res = json.loads(line)
+    assert res["n_gpus"] == 2
+    assert res["ligands_per_step"] == 128 and res["ligands_sharded"] == 128
+    assert res["max_rank_ligands"] == 64
+
+
+def test_bench_refuses_rank_count_mismatch():
+    """A rank whose WORLD_SIZE differs from --gpus stops before any timing."""
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parent.parent
+    env = dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, str(root / "bench.py"), "--gpus", "2", "--dry-run"], capture_output=True,
+                       text=True, timeout=300, env=env, cwd=str(root))
+    assert r.returncode != 0
+    assert "one rank per GPU" in (r.stdout + r.stderr)

@@ -137,6 +137,7 @@ struct ud_maps_s {
     MapsDesc desc{};
     std::vector<int> slot_types;     // XS type of each map slot
     DevBuf<float> maps;              // [slot][z][y][x]
+    DevBuf<float2> xpairs;           // [slot][z][y][x] = (map at x, map at x + 1): the search's corner loads
     DevBuf<float> smooth;            // [tp][bin][2]
     DevBuf<float> fast;              // [tp][bin]
     int n_bins = 0;
@@ -185,6 +186,7 @@ struct ud_batch_s {
     DevBuf<NodeRec> d_nodes;
     DevBuf<uint32_t> d_pairs;
     DevBuf<uint32_t> d_grid;
+    size_t upload_bytes = 0;  // host-to-device bytes of the last topology fill
     DevBuf<float> d_charge;          // AD4: atom charges
     DevBuf<float> d_pair_coef;       // AD4: (q_a q_b, |q_a| V_b + |q_b| V_a) per pair slot
     int max_atoms = 0, max_tors = 0;
@@ -200,6 +202,9 @@ struct ud_batch_s {
     bool searched = false;
     bool launched = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // around the search kernel alone inside the captured graph (event record
+    // nodes), so that its own device time is known without a separate launch
+    cudaEvent_t evk0 = nullptr, evk1 = nullptr;
     long long evals = 0;
     float kernel_ms = 0;
     std::vector<LigandPost> post;
@@ -252,6 +257,8 @@ struct ud_batch_s {
         if (capture_stream) cudaStreamDestroy(capture_stream);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (evk0) cudaEventDestroy(evk0);
+        if (evk1) cudaEventDestroy(evk1);
     }
     DeviceBatchView view() const {
         return DeviceBatchView{d_desc.p, d_atoms.p, d_nodes.p, d_pairs.p, d_grid.p, max_atoms, max_tors,
@@ -259,7 +266,14 @@ struct ud_batch_s {
     }
 };
 
-static DeviceMapsView maps_view(const ud_maps_s* m) { return DeviceMapsView{m->maps.p, m->desc}; }
+static DeviceMapsView maps_view(const ud_maps_s* m) { return DeviceMapsView{m->maps.p, m->desc, m->xpairs.p}; }
+
+// The x-pair copy of the maps, rebuilt after every change to the maps.
+static void refresh_xpairs(ud_maps_s* m, cudaStream_t s) {
+    const size_t n = (size_t)m->desc.dims[0] * m->desc.dims[1] * m->desc.dims[2] * std::max(1, m->desc.n_maps);
+    m->xpairs.alloc(n);
+    if (m->desc.n_maps > 0) cuda_check(launch_map_xpairs(m->maps.p, m->desc, m->xpairs.p, s), "map x-pairs");
+}
 static DeviceTablesView tables_view(const ud_maps_s* m) {
     return DeviceTablesView{m->smooth.p, m->fast.p, m->n_bins, m->factor, m->cutoff2};
 }
@@ -432,6 +446,7 @@ extern "C" int ud_maps_create(int sf, const float* weights, int n_weights, const
                                    tab.factor, m->cutoff2, d, m->maps.p, s),
                        "maps kernel");
         }
+        refresh_xpairs(m.get(), s);
         cuda_check(cudaStreamSynchronize(s), "maps sync");
         *out = m.release();
     });
@@ -551,6 +566,7 @@ extern "C" int ud_maps_create_ad4(const float* weights, int n_weights, const flo
         cuda_check(launch_maps_ad4(d_rec.p, d_ad.p, (int)m->rec_ad.size(), ad4_params(), ad4_spec(m.get(), -1), d,
                                    m->maps.p, s),
                    "AD4 maps kernel");
+        refresh_xpairs(m.get(), s);
         cuda_check(cudaStreamSynchronize(s), "maps sync");
         *out = m.release();
     });
@@ -699,6 +715,7 @@ extern "C" int ud_maps_load(int sf, const float* weights, int n_weights, const c
         std::vector<float> all(round4(plane * d.n_maps), 0.0f);
         for (int k = 0; k < d.n_maps; ++k) std::copy(data[k].begin(), data[k].end(), all.begin() + plane * k);
         m->maps.upload(all.data(), all.size(), s);
+        refresh_xpairs(m.get(), s);
         cuda_check(cudaStreamSynchronize(s), "maps upload");
         m->loaded = true;
         *out = m.release();
@@ -907,10 +924,6 @@ extern "C" int ud_ligand_destroy(ud_ligand lig) {
 
 // ---------------------------------------------------------------- batches
 
-// Pair records in groups of 32 (one warp-wide step of the pair loop): slots
-// 0-15 and 16-31 are each a matching (no atom twice), so the two half-warps can
-// add their pair forces into shared memory one after the other without
-// atomics.  Unfilled slots hold kPairPad; the list length is a multiple of 32.
 // Index into `pairs` of every slot of the conflict-free 32-slot groups, -1 for
 // padding: each group is kPairPasses lane ranges of kPairPassWidth slots, and
 // no atom occurs twice within a range (the kernel adds one range's forces at a
@@ -941,37 +954,45 @@ static std::vector<int> pair_group_slots(const Ligand& L, const std::vector<Pair
     return out;
 }
 
-// Device topology of `ligs` against `maps` (the body of ud_batch_create; the
-// autotuner builds its sample batches with it too).
-// Topology of `ligs` into the batch's device arrays (grown, never shrunk, so a
-// batch reused for the next ligands allocates nothing once it has seen the
-// largest batch).
-static void fill_batch(ud_batch_s* b, const std::vector<const Ligand*>& ligs, cudaStream_t s) {
+// Host records of the device topology of `ligs` against `maps`: LigDesc,
+// atoms, nodes, pair words, grid-atom list (and AD4 charges / pair
+// coefficients), with every LigDesc offset counted from the given bases (0
+// for a batch of its own; a streaming screen appends slot after slot to one
+// arena), and the work order of the persistent search (most expensive ligands
+// first, BFGS steps x (atoms + pairs) as the cost proxy) as lig_base + index.
+struct TopologyPack {
+    std::vector<LigDesc> desc;
+    std::vector<AtomRec> atoms;
+    std::vector<NodeRec> nodes;
+    std::vector<uint32_t> pairs;
+    std::vector<uint32_t> grid_list;
+    std::vector<float> charges, coef;  // AD4 only
+    std::vector<int> order;
+    int max_atoms = 0, max_tors = 0;
+};
+
+static void pack_topology(const ud_maps_s* maps, const std::vector<const Ligand*>& ligs, int lig_base,
+                          size_t atom_base, size_t node_base, size_t pair_base, size_t grid_base, TopologyPack& tp) {
         const int n = (int)ligs.size();
-        const ud_maps maps = b->maps;
-        b->ligs.clear();
-        b->desc.clear();
-        b->max_atoms = 0;
-        b->max_tors = 0;
-        std::vector<AtomRec> atoms;
-        std::vector<NodeRec> nodes;
-        std::vector<uint32_t> pairs;
-        std::vector<uint32_t> grid_list;
-        std::vector<float> charges, coef;  // AD4 only
+        tp = TopologyPack{};
+        auto& atoms = tp.atoms;
+        auto& nodes = tp.nodes;
+        auto& pairs = tp.pairs;
+        auto& grid_list = tp.grid_list;
+        auto& charges = tp.charges;
+        auto& coef = tp.coef;
         for (int i = 0; i < n; ++i) {
             const Ligand& L = *ligs[i];
             if ((int)L.atoms.size() > kMaxLigAtoms)
                 throw Error(UD_ERR_CAPACITY, "ligand " + std::to_string(i) + " has more than 256 atoms");
             if (L.n_torsions() > kMaxLigTorsions)
                 throw Error(UD_ERR_CAPACITY, "ligand " + std::to_string(i) + " has more than 48 torsions");
-            b->ligs.push_back(&L);
             LigDesc d{};
-            d.atom_off = (int)atoms.size();
+            d.atom_off = (int)(atom_base + atoms.size());
             d.n_atoms = (int)L.atoms.size();
-            d.node_off = (int)nodes.size();
+            d.node_off = (int)(node_base + nodes.size());
             d.n_nodes = (int)L.nodes.size();
-            d.pair_off = (int)pairs.size();
-            d.n_pairs = (int)L.pairs.size();
+            d.pair_off = (int)(pair_base + pairs.size());
             d.n_heavy = L.n_heavy();
             d.local_steps = ligand_local_steps(L);
             std::vector<int> depth(L.nodes.size(), 0);
@@ -995,7 +1016,8 @@ static void fill_batch(ud_batch_s* b, const std::vector<const Ligand*>& ligs, cu
                 r.subtree_end = subtree_end[k];
                 nodes.push_back(r);
             }
-            d.grid_off = (int)grid_list.size();
+            d.grid_off = (int)(grid_base + grid_list.size());
+            const size_t atom0 = atoms.size(), grid0 = grid_list.size(), pair0 = pairs.size();
             const bool ad4 = maps->desc.ad4 != 0;
             for (const Atom& a : L.atoms) {
                 AtomRec r;
@@ -1019,10 +1041,10 @@ static void fill_batch(ud_batch_s* b, const std::vector<const Ligand*>& ligs, cu
                 int heavy = (a.el != EL_H) ? 1 : 0;
                 int xsp = (a.xs < XS_SIZE) ? a.xs + 1 : 0;
                 r.packed = a.node | ((slot + 1) << 8) | (heavy << 16) | (xsp << 24);
-                if (slot >= 0) grid_list.push_back((uint32_t)(atoms.size() - d.atom_off) | ((uint32_t)slot << 8));
+                if (slot >= 0) grid_list.push_back((uint32_t)(atoms.size() - atom0) | ((uint32_t)slot << 8));
                 atoms.push_back(r);
             }
-            d.n_grid = (int)grid_list.size() - d.grid_off;
+            d.n_grid = (int)(grid_list.size() - grid0);
             const std::vector<Pair>& plist = ad4 ? L.pairs_ad : L.pairs;
             for (int k : pair_group_slots(L, plist)) {
                 if (k < 0) {
@@ -1041,32 +1063,49 @@ static void fill_batch(ud_batch_s* b, const std::vector<const Ligand*>& ligs, cu
                     coef.push_back(std::fabs(x.charge) * ad4_volume(y.ad) + std::fabs(y.charge) * ad4_volume(x.ad));
                 }
             }
-            d.n_pairs = (int)pairs.size() - d.pair_off;
-            b->desc.push_back(d);
-            b->max_atoms = std::max(b->max_atoms, d.n_atoms);
-            b->max_tors = std::max(b->max_tors, d.n_nodes - 1);
+            d.n_pairs = (int)(pairs.size() - pair0);
+            tp.desc.push_back(d);
+            tp.max_atoms = std::max(tp.max_atoms, d.n_atoms);
+            tp.max_tors = std::max(tp.max_tors, d.n_nodes - 1);
         }
-        b->d_desc.upload(b->desc.data(), b->desc.size(), s);
-        b->d_atoms.upload(atoms.data(), atoms.size(), s);
-        b->d_nodes.upload(nodes.data(), nodes.size(), s);
-        b->d_pairs.upload(pairs.data(), pairs.size(), s);
-        b->d_grid.upload(grid_list.data(), grid_list.size(), s);
-        if (maps->desc.ad4) {
-            b->d_charge.upload(charges.data(), charges.size(), s);
-            b->d_pair_coef.upload(coef.data(), coef.size(), s);
-        }
-        // work order of the persistent search: most expensive ligands first
-        // (BFGS steps x (atoms + pairs) as the cost proxy).  Uploaded here, with
-        // the topology, so that a search launch does no host-to-device copy
-        // (a copy from pageable memory would wait for the stream's prior work)
         std::vector<int> order(n);
         std::iota(order.begin(), order.end(), 0);
         std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-            long long cx = (long long)b->desc[x].local_steps * (b->desc[x].n_atoms + b->desc[x].n_pairs);
-            long long cy = (long long)b->desc[y].local_steps * (b->desc[y].n_atoms + b->desc[y].n_pairs);
+            long long cx = (long long)tp.desc[x].local_steps * (tp.desc[x].n_atoms + tp.desc[x].n_pairs);
+            long long cy = (long long)tp.desc[y].local_steps * (tp.desc[y].n_atoms + tp.desc[y].n_pairs);
             return cx > cy;
         });
-        b->d_order.upload(order.data(), order.size(), s);
+        for (int& o : order) o += lig_base;
+        tp.order = std::move(order);
+}
+
+// Topology of `ligs` into the batch's device arrays (grown, never shrunk, so a
+// batch reused for the next ligands allocates nothing once it has seen the
+// largest batch).  The work order is uploaded with the topology, so that a
+// search launch does no host-to-device copy (a copy from pageable memory would
+// wait for the stream's prior work).
+static void fill_batch(ud_batch_s* b, const std::vector<const Ligand*>& ligs, cudaStream_t s) {
+        const int n = (int)ligs.size();
+        TopologyPack tp;
+        pack_topology(b->maps, ligs, 0, 0, 0, 0, 0, tp);
+        b->ligs = ligs;
+        b->desc = tp.desc;
+        b->max_atoms = tp.max_atoms;
+        b->max_tors = tp.max_tors;
+        b->d_desc.upload(b->desc.data(), b->desc.size(), s);
+        b->d_atoms.upload(tp.atoms.data(), tp.atoms.size(), s);
+        b->d_nodes.upload(tp.nodes.data(), tp.nodes.size(), s);
+        b->d_pairs.upload(tp.pairs.data(), tp.pairs.size(), s);
+        b->d_grid.upload(tp.grid_list.data(), tp.grid_list.size(), s);
+        b->upload_bytes = b->desc.size() * sizeof(LigDesc) + tp.atoms.size() * sizeof(AtomRec) +
+                          tp.nodes.size() * sizeof(NodeRec) + (tp.pairs.size() + tp.grid_list.size()) * 4 +
+                          (size_t)n * sizeof(int);
+        if (b->maps->desc.ad4) {
+            b->d_charge.upload(tp.charges.data(), tp.charges.size(), s);
+            b->d_pair_coef.upload(tp.coef.data(), tp.coef.size(), s);
+            b->upload_bytes += (tp.charges.size() + tp.coef.size()) * sizeof(float);
+        }
+        b->d_order.upload(tp.order.data(), tp.order.size(), s);
         cuda_check(cudaStreamSynchronize(s), "batch upload");
 }
 
@@ -1259,10 +1298,15 @@ extern "C" int ud_score_terms(ud_batch b, const int* pose_ligand, const float* p
         std::vector<float> p(poses, poses + (size_t)n_poses * pose_stride), sc;
         score_poses_device(b, l, p, pose_stride, 1000.0f, sc, (cudaStream_t)stream);
         const Scoring& sf = b->maps->sf;
+        const bool ad4 = sf.choice == SF_AD42;
         for (int i = 0; i < n_poses; ++i) {
             const Ligand& L = *b->ligs[pose_ligand[i]];
             const float grid = sc[2 * i], intra = sc[2 * i + 1];
-            const float total = sf.conf_independent(grid + intra - intra, L.conf_indep_inputs()[0], (float)L.torsdof);
+            const float num_tors = L.conf_indep_inputs()[0];
+            // AD4 adds the torsional term to the inter energy alone and reports
+            // -intra as the unbound energy (vina.cpp:1207-1237)
+            const float total = ad4 ? grid + sf.conf_independent(0.0f, num_tors, (float)L.torsdof)
+                                    : sf.conf_independent(grid + intra - intra, num_tors, (float)L.torsdof);
             float* o = out + 8 * (size_t)i;
             o[0] = total;
             o[1] = grid;
@@ -1271,7 +1315,7 @@ extern "C" int ud_score_terms(ud_batch b, const int* pose_ligand, const float* p
             o[4] = 0.0f;
             o[5] = intra;
             o[6] = total - grid;
-            o[7] = intra;
+            o[7] = ad4 ? -intra : intra;
         }
     });
 }
@@ -1316,6 +1360,7 @@ extern "C" int ud_maps_add_bias(ud_maps m, const char* text, size_t len, void* s
         DevBuf<BiasMapRec> d;
         d.upload(recs.data(), recs.size(), s);
         cuda_check(launch_bias_maps(d.p, (int)recs.size(), m->desc, m->maps.p, s), "bias maps kernel");
+        refresh_xpairs(m, s);
         cuda_check(cudaStreamSynchronize(s), "bias maps");
         m->bias.insert(m->bias.end(), wells.begin(), wells.end());
         std::vector<BiasRec> all;
@@ -1466,6 +1511,7 @@ extern "C" int ud_maps_set_weights(ud_maps maps, const float* w, int n, void* st
         const size_t fblock = round4(table_rows(maps) * maps->n_bins);
         cuda_check(launch_combine_terms(maps->term_maps.p, (long long)term_map_block(maps), n, w, maps->maps.p, s),
                    "combine maps");
+        refresh_xpairs(maps, s);
         cuda_check(launch_combine_terms(maps->term_rows.p, (long long)rblock, n, w, maps->smooth.p, s), "combine rows");
         cuda_check(launch_combine_terms(maps->term_fast.p, (long long)fblock, n, w, maps->fast.p, s), "combine fast");
         for (int t = 0; t < n; ++t) maps->sf.weights[t] = w[t];
@@ -1721,30 +1767,28 @@ static void alloc_modes(ud_batch b, cudaStream_t s) {
     b->hp_mode_e.alloc(n_slot * 4);
 }
 
-// Final scores of every ligand's modes (vina.h:232-343) from the device
-// clustering (and refinement): without refinement the modes keep their search
-// order and their grid / intramolecular energies at the authentic cap; with
-// it they are ordered by refined energy (max when outside the box), and the
-// inter energies come from the receptor atoms.  The unbound energy is the
-// intramolecular energy of the first mode.
-static void post_process(ud_batch b) {
-    const int n_lig = (int)b->ligs.size();
-    const int E = b->exhaustiveness, cap = b->mode_cap;
-    b->post.assign(n_lig, LigandPost{});
-    const Scoring& sf = b->maps->sf;
-    parallel_for(n_lig, [&](int l) {
-        const Ligand& L = *b->ligs[l];
-        const int nm = b->hp_n_modes.p[l];
+// Final scores of one ligand's modes (vina.h:232-343) from the device
+// clustering (and refinement), in mode slots of `cap` per ligand: without
+// refinement the modes keep their search order and their grid /
+// intramolecular energies at the authentic cap; with it they are ordered by
+// refined energy (max when outside the box), and the inter energies come from
+// the receptor atoms.  Vina / Vinardo: the final score is conf_independent(
+// inter + intra - intra of the first mode) and the unbound energy that first
+// mode's intramolecular energy; AD4: inter plus the torsional term, unbound
+// -intra (score_gpu, vina.cpp:1245-1322).
+static LigandPost post_process_ligand(const Scoring& sf, const Ligand& L, int E, int cap, int pose_stride,
+                                      bool refined, int n_modes, const int* mode_chain, const float* mode_pose,
+                                      const float* mode_e, const ChainResult* results) {
+        LigandPost out;
         std::vector<PoseResult> v;
-        for (int k = 0; k < nm; ++k) {
-            const size_t o = (size_t)l * cap + k;
-            const int ch = b->hp_mode_chain.p[o];
-            const ChainResult& cr = b->h_results[(size_t)l * E + ch];
+        for (int k = 0; k < n_modes; ++k) {
+            const int ch = mode_chain[k];
+            const ChainResult& cr = results[ch];
             PoseResult r;
-            const float* p = b->hp_mode_pose.p + o * b->pose_stride;
+            const float* p = mode_pose + (size_t)k * pose_stride;
             r.pose.assign(p, p + 7 + L.n_torsions());
-            if (b->refined) {
-                const float* me = b->hp_mode_e.p + 4 * o;
+            if (refined) {
+                const float* me = mode_e + 4 * (size_t)k;
                 r.e = me[3] > 0.5f ? me[0] : std::numeric_limits<float>::max();
                 r.inter = me[1];
                 r.intra = me[2];
@@ -1755,20 +1799,28 @@ static void post_process(ud_batch b) {
             }
             v.push_back(r);
         }
-        if (v.empty()) return;
-        if (b->refined)
+        if (v.empty()) return out;
+        if (refined)
             std::stable_sort(v.begin(), v.end(), [](const PoseResult& x, const PoseResult& y) { return x.e < y.e; });
         auto ci = L.conf_indep_inputs();
+        const bool ad4 = sf.choice == SF_AD42;
         const float intramolecular = v[0].intra;
         for (size_t i = 0; i < v.size(); ++i) {
             const float inter = v[i].inter, intra = v[i].intra;
-            float total = sf.conf_independent(inter + intra - intramolecular, ci[0], (float)L.torsdof);
-            v[i].e = total;
+            if (ad4) {  // score_gpu's AD4 branch (vina.cpp:1290-1322): inter + torsional term, unbound -intra
+                const float tors = sf.conf_independent(0.0f, ci[0], (float)L.torsdof);
+                v[i].e = inter + tors;
+                v[i].conf_indep = tors;
+                v[i].unbound = -intra;
+            } else {
+                const float total = sf.conf_independent(inter + intra - intramolecular, ci[0], (float)L.torsdof);
+                v[i].e = total;
+                v[i].conf_indep = total - (inter + intra - intramolecular);
+                v[i].unbound = intramolecular;
+            }
             v[i].inter = inter;
             v[i].intra = intra;
             v[i].total = inter + intra;
-            v[i].conf_indep = total - (inter + intra - intramolecular);
-            v[i].unbound = intramolecular;
         }
         std::stable_sort(v.begin(), v.end(), [](const PoseResult& x, const PoseResult& y) { return x.e < y.e; });
         std::vector<float> best(3 * L.atoms.size()), cur(3 * L.atoms.size());
@@ -1778,7 +1830,22 @@ static void post_process(ud_batch b) {
             r.lb = std::max(rmsd_lb_asym(L, cur, best), rmsd_lb_asym(L, best, cur));
             r.ub = rmsd_ub(heavy_coords(L, cur), heavy_coords(L, best));
         }
-        b->post[l].modes = v;
+        out.modes = std::move(v);
+        return out;
+}
+
+// Final scores of every ligand of the batch (post_process_ligand), on the
+// host's threads.
+static void post_process(ud_batch b) {
+    const int n_lig = (int)b->ligs.size();
+    const int E = b->exhaustiveness, cap = b->mode_cap;
+    b->post.assign(n_lig, LigandPost{});
+    parallel_for(n_lig, [&](int l) {
+        const size_t o = (size_t)l * cap;
+        b->post[l] = post_process_ligand(b->maps->sf, *b->ligs[l], E, cap, b->pose_stride, b->refined,
+                                         b->hp_n_modes.p[l], b->hp_mode_chain.p + o,
+                                         b->hp_mode_pose.p + o * b->pose_stride, b->hp_mode_e.p + 4 * o,
+                                         b->h_results.data() + (size_t)l * E);
     });
 }
 
@@ -1795,7 +1862,7 @@ static void search_graph(ud_batch b, const SearchParams& sp, int n_chain, int bl
     k << n_chain << ' ' << blocks << ' ' << sp.global_steps << ' ' << sp.exhaustiveness << ' ' << sp.seed << ' '
       << sp.chains_per_block << ' ' << sp.lanes_per_chain << ' ' << sp.bfgs_cap << ' ' << (const void*)b->d_poses.p << ' '
       << (const void*)b->d_results.p << ' ' << (const void*)b->d_queue.p << ' ' << (const void*)b->d_order.p << ' '
-      << (const void*)b->hp_poses.p << ' ' << (const void*)b->hp_results.p << ' ' << (const void*)b->maps->maps.p
+      << (const void*)b->hp_poses.p << ' ' << (const void*)b->hp_results.p << ' ' << (const void*)b->maps->maps.p << ' ' << (const void*)b->maps->xpairs.p
       << ' ' << (const void*)b->maps->smooth.p << ' ' << b->mode_cap << ' ' << b->refined << ' '
       << b->params.refine_step << ' ' << b->params.min_rmsd << ' ' << (const void*)b->d_mode_pose.p << ' '
       << (const void*)b->d_mode_e.p << ' ' << (const void*)b->d_cluster_scratch.p << ' '
@@ -1809,7 +1876,8 @@ static void search_graph(ud_batch b, const SearchParams& sp, int n_chain, int bl
     // the per-warp shared-memory layout it sizes
     const DeviceBatchView v = b->view();
     k << ' ' << (const void*)v.ligs << ' ' << (const void*)v.atoms << ' ' << (const void*)v.nodes << ' '
-      << (const void*)v.pairs << ' ' << (const void*)v.grid_list << ' ' << (const void*)v.charges << ' '
+      << (const void*)v.pairs << ' ' << (const void*)v.grid_list << ' '
+      << (const void*)v.charges << ' '
       << (const void*)v.pair_coef << ' ' << v.max_atoms << ' ' << v.max_torsions << ' ' << b->ligs.size() << ' '
       << b->pose_stride;
     if (b->graph_exec && b->graph_key == k.str()) return;
@@ -1819,9 +1887,11 @@ static void search_graph(ud_batch b, const SearchParams& sp, int n_chain, int bl
     cudaStream_t cs = b->capture_stream;
     cuda_check(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");
     cudaError_t e = cudaMemsetAsync(b->d_queue.p, 0, sizeof(unsigned int), cs);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(b->evk0, cs, cudaEventRecordExternal);
     if (e == cudaSuccess)
         e = launch_search(b->view(), maps_view(b->maps), tables_view(b->maps), sp, b->d_order.p, n_chain, 0,
                           b->d_queue.p, b->d_poses.p, b->pose_stride, b->d_results.p, blocks, cs);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(b->evk1, cs, cudaEventRecordExternal);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(b->hp_poses.p, b->d_poses.p, (size_t)n_chain * b->pose_stride * sizeof(float),
                             cudaMemcpyDeviceToHost, cs);
@@ -1887,6 +1957,8 @@ static void search_launch(ud_batch b, const ud_search_params* params, cudaStream
         if (!b->ev0) {
             cuda_check(cudaEventCreate(&b->ev0), "event");
             cuda_check(cudaEventCreate(&b->ev1), "event");
+            cuda_check(cudaEventCreate(&b->evk0), "event");
+            cuda_check(cudaEventCreate(&b->evk1), "event");
         }
         b->graph_results = false;
         if (sp.persistent && P.use_graph && modes) {
@@ -1944,7 +2016,13 @@ static void search_collect(ud_batch b, cudaStream_t s) {
                        "D2H results");
             cuda_check(cudaStreamSynchronize(s), "search sync");
         }
-        cudaEventElapsedTime(&b->kernel_ms, b->ev0, b->ev1);
+        // the search kernel's own device time: between the graph's event
+        // nodes around it, else (no graph) between the events of the launch
+        b->kernel_ms = 0;
+        if (!b->graph_results || cudaEventElapsedTime(&b->kernel_ms, b->evk0, b->evk1) != cudaSuccess) {
+            cudaGetLastError();
+            cudaEventElapsedTime(&b->kernel_ms, b->ev0, b->ev1);
+        }
         b->evals = 0;
         for (auto& r : b->h_results) b->evals += r.evals;
         post_process(b);
@@ -2098,9 +2176,12 @@ extern "C" int ud_autotune(ud_batch b, const ud_search_params* params, ud_tune_r
         tp.use_graph = 0;
         // tuning budget: the caller's MC step cap, or at most 40 steps per chain
         if (tp.max_step <= 0 || tp.max_step > 40) tp.max_step = 40;
+        // BFGS iteration caps are not tuned: every cap tried (16, 10, 6) moved the
+        // median best energy of the fast screen (exhaustiveness 128, max_step 20)
+        // away from the reference's uncapped search by more than 0.1 kcal/mol
+        // beyond sampling noise; searches stay uncapped unless bfgs_cap asks.
         const int cpbs[] = {4, 2, 1};
         const int lanes[] = {32, 16};
-        const int caps[] = {16, 10, 6};
         std::vector<float> base, cur;
         tp.chains_per_block = 4;
         tp.lanes_per_chain = 32;
@@ -2128,13 +2209,10 @@ extern "C" int ud_autotune(ud_batch b, const ud_search_params* params, ud_tune_r
                 best_shift = (float)shift;
             }
         };
-        // launch shape first (warps per CTA x lanes per chain), uncapped; then
-        // the BFGS caps on the shape picked
+        // the launch shape: warps per CTA x lanes per chain
         for (int ln : lanes)
             for (int cpb : cpbs)
                 if (!(cpb == 4 && ln == 32)) trial(cpb, ln, 0);
-        const int shape_cpb = best_cpb, shape_lanes = best_lanes;
-        for (int cap : caps) trial(shape_cpb, shape_lanes, cap);
         b->tuned = true;
         b->tuned_chains_per_block = best_cpb;
         b->tuned_lanes_per_chain = best_lanes;
@@ -2218,20 +2296,24 @@ extern "C" int ud_result_mode(ud_batch b, int lig, int k, float* pose, float ene
 
 // Output text of one ligand: the kept modes within num_modes and energy_range
 // of the best (Vina::get_poses_gpu, vina.cpp:872-923).
-static std::string render_result(const ud_batch_s* b, int lig, int format) {
-    const Ligand& L = *b->ligs[lig];
-    const auto& modes = b->post[lig].modes;
+static std::string render_modes(const Ligand& L, const LigandPost& post, int num_modes, float energy_range, bool ad4,
+                                int format) {
+    const auto& modes = post.modes;
     std::vector<PoseResult> sel;
     if (!modes.empty()) {
         const float best = modes[0].e;
         for (auto& m : modes) {
-            if ((int)sel.size() >= b->params.num_modes) break;
-            if (!(m.e < 0.1f * std::numeric_limits<float>::max()) || m.e > best + b->params.energy_range) break;
+            if ((int)sel.size() >= num_modes) break;
+            if (!(m.e < 0.1f * std::numeric_limits<float>::max()) || m.e > best + energy_range) break;
             sel.push_back(m);
         }
     }
-    const bool ad4 = b->maps->desc.ad4 != 0;
     return format == 1 ? write_sdf_models(L, sel, ad4) : write_pdbqt_models(L, sel, ad4);
+}
+
+static std::string render_result(const ud_batch_s* b, int lig, int format) {
+    return render_modes(*b->ligs[lig], b->post[lig], b->params.num_modes, b->params.energy_range,
+                        b->maps->desc.ad4 != 0, format);
 }
 
 extern "C" int ud_result_write(ud_batch b, int lig, int format, char* buf, size_t cap, size_t* len) {
@@ -2252,6 +2334,13 @@ extern "C" int ud_result_write(ud_batch b, int lig, int format, char* buf, size_
             std::memcpy(buf, s.data(), n);
             buf[n] = 0;
         }
+    });
+}
+
+extern "C" int ud_batch_upload_bytes(ud_batch b, size_t* bytes) {
+    return guarded([&] {
+        if (!b || !bytes) throw Error(UD_ERR_ARG, "null argument");
+        *bytes = b->upload_bytes;
     });
 }
 
@@ -2299,32 +2388,36 @@ extern "C" int ud_device_fp32_peak(float* tflops) {
     });
 }
 
+extern "C" int ud_device_l2_peak(float* gbs) {
+    return guarded([&] {
+        if (!gbs) throw Error(UD_ERR_ARG, "null argument");
+        *gbs = measure_l2_read_gbs();
+        if (!(*gbs > 0)) throw Error(UD_ERR_CUDA, "L2 probe failed");
+    });
+}
+
 // Persistent search with caller-provided device outputs and the library's
-// static device scratch instead of device allocations (see the header).
+// static device scratch instead of device allocations (see the header).  The
+// launch shape and BFGS cap resolve as ud_search resolves them for the
+// batched form, so both give the same per-chain results.
 extern "C" int ud_search_device_noalloc(ud_batch b, const ud_search_params* params, float* d_poses,
                                         int pose_stride, float* d_energies, int* d_evals, void* stream) {
     return guarded([&] {
         if (!b || !params || !d_poses || !d_energies) throw Error(UD_ERR_ARG, "null argument");
         const ud_search_params& P = *params;
         if (P.exhaustiveness < 1) throw Error(UD_ERR_ARG, "exhaustiveness must be >= 1");
+        if (P.chains_per_block < 0 || P.chains_per_block > 4)
+            throw Error(UD_ERR_ARG, "chains_per_block must be 0 (default / autotuned) or 1..4");
+        if (P.lanes_per_chain != 0 && P.lanes_per_chain != 16 && P.lanes_per_chain != 32)
+            throw Error(UD_ERR_ARG, "lanes_per_chain must be 0 (default / autotuned), 16 or 32");
         if (pose_stride < 7 + b->max_tors) throw Error(UD_ERR_ARG, "pose_stride smaller than 7 + max torsions");
         const int n_lig = (int)b->ligs.size();
+        if (n_lig == 0) throw Error(UD_ERR_ARG, "empty batch");
         const long long n_chain = (long long)n_lig * P.exhaustiveness;
-        if (n_lig > kNoAllocMaxLigands)
-            throw Error(UD_ERR_CAPACITY, "ud_search_device_noalloc: batch of " + std::to_string(n_lig) +
-                                             " ligands exceeds the maximum of " + std::to_string(kNoAllocMaxLigands));
         if (n_chain > kNoAllocMaxChains)
             throw Error(UD_ERR_CAPACITY, "ud_search_device_noalloc: " + std::to_string(n_chain) +
                                              " chains (ligands x exhaustiveness) exceed the maximum of " +
                                              std::to_string(kNoAllocMaxChains));
-        if (n_lig == 0) return;
-        std::vector<int> order(n_lig);
-        std::iota(order.begin(), order.end(), 0);
-        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-            long long cx = (long long)b->desc[x].local_steps * (b->desc[x].n_atoms + b->desc[x].n_pairs);
-            long long cy = (long long)b->desc[y].local_steps * (b->desc[y].n_atoms + b->desc[y].n_pairs);
-            return cx > cy;
-        });
         SearchParams sp{};
         sp.global_steps = global_steps_for(b->ligs, P.max_step);
         sp.exhaustiveness = P.exhaustiveness;
@@ -2333,18 +2426,503 @@ extern "C" int ud_search_device_noalloc(ud_batch b, const ud_search_params* para
         sp.authentic_v = 1000.0f;
         sp.temperature = 1.2f;
         sp.mutation_amplitude = 2.0f;
-        sp.lanes_per_chain = 32;
-        sp.chains_per_block = 4;
+        sp.lanes_per_chain = P.lanes_per_chain > 0 ? P.lanes_per_chain : (b->tuned ? b->tuned_lanes_per_chain : 32);
+        sp.chains_per_block = P.chains_per_block > 0 ? P.chains_per_block : (b->tuned ? b->tuned_chains_per_block : 4);
         sp.persistent = 1;
-        sp.bfgs_cap = P.bfgs_cap;
+        sp.bfgs_cap = P.bfgs_cap >= 0 ? P.bfgs_cap : (b->tuned ? b->tuned_bfgs_cap : 0);
+        const int chains_per_cta = sp.chains_per_block * (32 / sp.lanes_per_chain);
         int dev = 0, n_sm = 148;
         cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
         cuda_check(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev), "device attribute");
-        const int per_sm = search_blocks_per_sm(b->view(), sp.chains_per_block);
-        const int needed = (int)((n_chain + sp.chains_per_block - 1) / sp.chains_per_block);
+        const int per_sm = search_blocks_per_sm(b->view(), sp.chains_per_block, sp.lanes_per_chain);
+        const int needed = (int)((n_chain + chains_per_cta - 1) / chains_per_cta);
         const int blocks = std::max(1, std::min(per_sm * n_sm, needed));
-        cuda_check(launch_search_noalloc(b->view(), maps_view(b->maps), tables_view(b->maps), sp, order.data(), n_lig,
+        // the work order (most expensive ligands first) is the batch's own,
+        // uploaded to device memory when the batch was filled
+        cuda_check(launch_search_noalloc(b->view(), maps_view(b->maps), tables_view(b->maps), sp, b->d_order.p, n_lig,
                                          blocks, d_poses, pose_stride, d_energies, d_evals, (cudaStream_t)stream),
                    "allocation-free search");
     });
+}
+
+// ---------------------------------------------------------------- streaming screen
+// One persistent search kernel fed slot by slot from the host (StreamView in
+// ud_engine.h; no counterpart in the reference, whose CLI parses and docks one
+// batch after another, main.cpp:975-1070).  The host packs a slot's ligands
+// into page-locked staging memory, copies them into an append-only device
+// arena and publishes the slot; the kernel, launched once, takes (ligand,
+// chain) items as slots are published and signals each finished slot through
+// host-mapped memory; each slot's modes are then clustered and refined on the
+// SMs the persistent kernel leaves free, and scored on the host.  Every
+// device and page-locked buffer is allocated when the stream is created, so
+// nothing synchronises the device while the kernel runs.
+
+namespace {
+// A slot's block in every arena array starts on this byte boundary, so that
+// no cached line of the read-only data path ever holds a slot that was not
+// yet written when the line was cached.
+constexpr size_t kSlotAlign = 256;
+size_t aligned_elems(size_t n, size_t elem_bytes, size_t unit_elems) {
+    (void)elem_bytes;
+    return (n + unit_elems - 1) / unit_elems * unit_elems;
+}
+// elements per alignment unit of each arena array (unit x element size is a
+// multiple of kSlotAlign for the array and for the arrays that share its index)
+constexpr size_t kAtomUnit = 64;   // AtomRec 16 B (1 KB) and the AD4 charges 4 B (256 B)
+constexpr size_t kNodeUnit = 32;   // NodeRec 40 B (1280 B)
+constexpr size_t kPairUnit = 64;   // pair words 4 B (256 B) and the AD4 coefficients 8 B (512 B)
+constexpr size_t kGridUnit = 64;   // grid-atom words 4 B
+constexpr int kStreamReserveSms = 4;  // SMs left to the per-slot clustering and refinement kernels
+}  // namespace
+
+struct StreamSlot {
+    std::vector<const Ligand*> ligs;
+    int max_atoms = 0, max_tors = 0;
+    bool collected = false;
+    std::vector<LigandPost> post;
+    std::vector<ChainResult> results;
+    std::vector<float> poses;
+};
+
+struct ud_stream_s {
+    ud_maps maps = nullptr;
+    ud_search_params params{};
+    SearchParams sp{};
+    int E = 0, M = 0, max_slots = 0, ring = 0, cap = 0, stride = 0, max_atoms = 0, max_tors = 0;
+    bool refined = false, ad4 = false;
+    size_t atom_cap = 0, node_cap = 0, pair_cap = 0, grid_cap = 0;
+    size_t n_atoms = 0, n_nodes = 0, n_pairs = 0, n_grid = 0;  // arena fill, in elements
+    DevBuf<LigDesc> d_desc;
+    DevBuf<AtomRec> d_atoms;
+    DevBuf<NodeRec> d_nodes;
+    DevBuf<uint32_t> d_pairs, d_grid;
+    DevBuf<float> d_charge, d_coef;
+    DevBuf<unsigned int> d_ctl;  // published, closed, work counter
+    DevBuf<unsigned int> d_slot_left;
+    DevBuf<int> d_slot_nlig, d_order, d_status;
+    unsigned int* h_done = nullptr;  // host-mapped, per slot
+    PinnedBuf<unsigned int> h_counts;  // [k] = k: sources of the published-count copies; [max_slots + 1] = 1
+    PinnedBuf<unsigned char> staging[2];
+    cudaEvent_t staged[2] = {nullptr, nullptr};
+    DevBuf<float> d_poses;
+    DevBuf<ChainResult> d_results;
+    // modes of a slot, one set of buffers per ring area
+    DevBuf<float> d_scratch, d_mode_pose, d_mode_e;
+    DevBuf<int> d_n_modes, d_mode_chain, d_mode_lig;
+    PinnedBuf<int> hp_n_modes, hp_mode_chain;
+    PinnedBuf<float> hp_mode_pose, hp_mode_e, hp_poses;
+    PinnedBuf<ChainResult> hp_results;
+    cudaStream_t ks = nullptr, cs = nullptr, ps = nullptr;  // kernel, copies, post-processing
+    std::vector<StreamSlot> slots;
+    int n_pushed = 0;
+    bool closed = false, running = false, finished = false;
+    int status = 0;
+    long long evals = 0;
+
+    DeviceBatchView view(int slot = -1) const {
+        DeviceBatchView v{d_desc.p, d_atoms.p, d_nodes.p, d_pairs.p, d_grid.p, max_atoms, max_tors,
+                          d_charge.p, d_coef.p, ad4 ? 1 : 0};
+        if (slot >= 0) {  // one slot's ligands as ligands 0..n-1 (offsets stay absolute)
+            v.ligs = d_desc.p + (size_t)slot * M;
+            v.max_atoms = std::max(1, slots[slot].max_atoms);
+            v.max_torsions = slots[slot].max_tors;
+        }
+        return v;
+    }
+    ~ud_stream_s() {
+        if (running) {  // no further slot: the kernel drains and exits
+            if (!closed && cs) {
+                cudaMemcpyAsync(d_ctl.p + 1, h_counts.p + max_slots + 1, sizeof(unsigned int),
+                                cudaMemcpyHostToDevice, cs);
+                cudaStreamSynchronize(cs);
+            }
+            cudaStreamSynchronize(ks);
+        }
+        for (auto& e : staged)
+            if (e) cudaEventDestroy(e);
+        if (h_done) cudaFreeHost(h_done);
+        for (cudaStream_t s : {ks, cs, ps})
+            if (s) cudaStreamDestroy(s);
+    }
+};
+
+extern "C" int ud_stream_create(ud_maps maps, const ud_search_params* params, const ud_stream_config* cfg,
+                                ud_stream* out) {
+    return guarded([&] {
+        if (!maps || !params || !cfg || !out) throw Error(UD_ERR_ARG, "null argument");
+        const ud_search_params& P = *params;
+        if (P.exhaustiveness < 1) throw Error(UD_ERR_ARG, "exhaustiveness must be >= 1");
+        // at or below every ligand's heuristic step count (70*3*(50 + N + 10*DOF)/2 >= 11655),
+        // so a chain's step count does not depend on the ligands that share its slot
+        if (P.max_step < 1 || P.max_step > 11655)
+            throw Error(UD_ERR_ARG, "a streaming screen needs max_step in 1..11655 (--max_step)");
+        if (P.num_modes < 1) throw Error(UD_ERR_ARG, "num_modes must be >= 1");
+        if (P.chains_per_block < 0 || P.chains_per_block > 4)
+            throw Error(UD_ERR_ARG, "chains_per_block must be 0 (default) or 1..4");
+        if (P.lanes_per_chain != 0 && P.lanes_per_chain != 32)
+            throw Error(UD_ERR_ARG, "a streaming screen runs one chain per warp (lanes_per_chain 0 or 32)");
+        if (cfg->slot_ligands < 1 || cfg->max_slots < 1 || cfg->ring < 1 || cfg->max_atoms < 1 ||
+            cfg->max_atoms > kMaxLigAtoms || cfg->max_torsions < 0 || cfg->max_torsions > kMaxLigTorsions ||
+            cfg->timeout_ms < 0)
+            throw Error(UD_ERR_ARG, "invalid stream configuration");
+        auto st = std::make_unique<ud_stream_s>();
+        st->maps = maps;
+        st->params = P;
+        st->E = P.exhaustiveness;
+        st->M = (cfg->slot_ligands + 15) / 16 * 16;  // LigDesc blocks of whole 256-byte units
+        st->max_slots = cfg->max_slots;
+        st->ring = std::min(cfg->ring, cfg->max_slots);
+        st->cap = P.num_modes;
+        st->max_atoms = cfg->max_atoms;
+        st->max_tors = cfg->max_torsions;
+        st->stride = 7 + st->max_tors;
+        st->ad4 = maps->desc.ad4 != 0;
+        st->refined = P.refine_step > 0 && has_receptor(maps);
+        SearchParams& sp = st->sp;
+        sp.global_steps = P.max_step;
+        sp.exhaustiveness = st->E;
+        sp.seed = P.seed;
+        sp.hunt_cap = 10.0f;
+        sp.authentic_v = 1000.0f;
+        sp.temperature = 1.2f;
+        sp.mutation_amplitude = 2.0f;
+        sp.lanes_per_chain = 32;
+        sp.chains_per_block = P.chains_per_block > 0 ? P.chains_per_block : 4;
+        sp.persistent = 1;
+        sp.bfgs_cap = P.bfgs_cap > 0 ? P.bfgs_cap : 0;
+        const size_t S = (size_t)st->max_slots, M = (size_t)st->M, E = (size_t)st->E;
+        const size_t A = (size_t)st->max_atoms;
+        st->atom_cap = S * aligned_elems(M * A, sizeof(AtomRec), kAtomUnit);
+        st->node_cap = S * aligned_elems(M * (st->max_tors + 1), sizeof(NodeRec), kNodeUnit);
+        st->grid_cap = S * aligned_elems(M * A, 4, kGridUnit);
+        st->pair_cap = S * aligned_elems(M * std::max<size_t>(32, A * A / 2), 4, kPairUnit);
+        cudaStream_t s0 = nullptr;
+        for (cudaStream_t* s : {&st->ks, &st->cs, &st->ps})
+            cuda_check(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking), "stream");
+        s0 = st->cs;
+        st->d_desc.alloc(S * M);
+        st->d_atoms.alloc(st->atom_cap);
+        st->d_nodes.alloc(st->node_cap);
+        st->d_pairs.alloc(st->pair_cap);
+        st->d_grid.alloc(st->grid_cap);
+        if (st->ad4) {
+            st->d_charge.alloc(st->atom_cap);
+            st->d_coef.alloc(2 * st->pair_cap);
+        }
+        st->d_ctl.alloc(4);
+        st->d_slot_left.alloc(S);
+        st->d_slot_nlig.alloc(S);
+        st->d_order.alloc(S * M);
+        st->d_status.alloc(1);
+        cuda_check(cudaHostAlloc((void**)&st->h_done, S * sizeof(unsigned int), cudaHostAllocMapped), "mapped memory");
+        std::memset(st->h_done, 0, S * sizeof(unsigned int));
+        st->h_counts.alloc(S + 2);
+        for (size_t k = 0; k <= S; ++k) st->h_counts.p[k] = (unsigned int)k;
+        st->h_counts.p[S + 1] = 1;
+        // staging of one slot: LigDesc, order, counts, atoms, charges, nodes, pairs, coefficients, grid words
+        const size_t stage = M * (sizeof(LigDesc) + 4) + 16 + M * A * (sizeof(AtomRec) + 4) +
+                             M * (st->max_tors + 1) * sizeof(NodeRec) + M * std::max<size_t>(32, A * A / 2) * 12 +
+                             M * A * 4 + 4096;
+        for (int b = 0; b < 2; ++b) {
+            st->staging[b].alloc(stage);
+            cuda_check(cudaEventCreateWithFlags(&st->staged[b], cudaEventDisableTiming), "event");
+            cuda_check(cudaEventRecord(st->staged[b], s0), "event");
+        }
+        const size_t R = (size_t)st->ring;
+        st->d_poses.alloc(R * M * E * st->stride);
+        st->d_results.alloc(R * M * E);
+        const size_t modes = R * M * st->cap;
+        st->d_scratch.alloc(modes * 3 * A);
+        st->d_n_modes.alloc(R * M);
+        st->d_mode_chain.alloc(modes);
+        st->d_mode_lig.alloc(modes);
+        st->d_mode_pose.alloc(modes * st->stride);
+        st->d_mode_e.alloc(modes * 4);
+        st->hp_n_modes.alloc(M);
+        st->hp_mode_chain.alloc(M * st->cap);
+        st->hp_mode_pose.alloc(M * st->cap * st->stride);
+        st->hp_mode_e.alloc(M * st->cap * 4);
+        st->hp_poses.alloc(M * E * st->stride);
+        st->hp_results.alloc(M * E);
+        if (st->refined) ensure_receptor(maps, s0);
+        st->slots.resize(S);
+        cuda_check(cudaMemsetAsync(st->d_ctl.p, 0, 4 * sizeof(unsigned int), s0), "memset");
+        cuda_check(cudaMemsetAsync(st->d_status.p, 0, sizeof(int), s0), "memset");
+        cuda_check(cudaStreamSynchronize(s0), "stream set-up");
+        StreamView sv{};
+        sv.published = st->d_ctl.p;
+        sv.closed = st->d_ctl.p + 1;
+        sv.next_item = st->d_ctl.p + 2;
+        sv.slot_left = st->d_slot_left.p;
+        sv.slot_nlig = st->d_slot_nlig.p;
+        sv.order = st->d_order.p;
+        unsigned int* done_dev = nullptr;
+        cuda_check(cudaHostGetDevicePointer((void**)&done_dev, st->h_done, 0), "mapped pointer");
+        sv.done_host = done_dev;
+        sv.status = st->d_status.p;
+        sv.slot_ligands = st->M;
+        sv.max_slots = st->max_slots;
+        sv.ring = st->ring;
+        sv.timeout_ns = (unsigned long long)(cfg->timeout_ms > 0 ? cfg->timeout_ms : 60000) * 1000000ull;
+        int dev = 0, n_sm = 148;
+        cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+        cuda_check(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev), "device attribute");
+        const int per_sm = stream_blocks_per_sm(st->view(), sp.chains_per_block);
+        const int blocks = per_sm * std::max(1, n_sm - kStreamReserveSms);
+        cuda_check(launch_search_stream(st->view(), maps_view(maps), tables_view(maps), sp, sv, st->d_poses.p,
+                                        st->stride, st->d_results.p, blocks, st->ks),
+                   "stream kernel");
+        st->running = true;
+        *out = st.release();
+    });
+}
+
+extern "C" int ud_stream_push(ud_stream st, const ud_ligand* ligs, int n, int* slot) {
+    return guarded([&] {
+        if (!st || (n > 0 && !ligs)) throw Error(UD_ERR_ARG, "null argument");
+        if (st->closed) throw Error(UD_ERR_STATE, "stream closed");
+        if (n < 1 || n > st->M) throw Error(UD_ERR_ARG, "a slot holds 1.." + std::to_string(st->M) + " ligands");
+        const int k = st->n_pushed;
+        if (k >= st->max_slots) throw Error(UD_ERR_CAPACITY, "all slots of the stream are used");
+        if (k >= st->ring && !st->slots[k - st->ring].collected)
+            throw Error(UD_ERR_STATE, "slot " + std::to_string(k - st->ring) +
+                                          " must be collected before its result area is reused");
+        std::vector<const Ligand*> v;
+        for (int i = 0; i < n; ++i) {
+            if (!ligs[i]) throw Error(UD_ERR_ARG, "null ligand");
+            const Ligand& L = ligs[i]->lig;
+            if ((int)L.atoms.size() > st->max_atoms || L.n_torsions() > st->max_tors)
+                throw Error(UD_ERR_CAPACITY, "ligand " + std::to_string(i) + " exceeds the stream's max_atoms / "
+                                                                         "max_torsions");
+            v.push_back(&L);
+        }
+        const size_t a0 = aligned_elems(st->n_atoms, sizeof(AtomRec), kAtomUnit);
+        const size_t n0 = aligned_elems(st->n_nodes, sizeof(NodeRec), kNodeUnit);
+        const size_t p0 = aligned_elems(st->n_pairs, 4, kPairUnit);
+        const size_t g0 = aligned_elems(st->n_grid, 4, kGridUnit);
+        TopologyPack tp;
+        pack_topology(st->maps, v, k * st->M, a0, n0, p0, g0, tp);
+        if (a0 + tp.atoms.size() > st->atom_cap || n0 + tp.nodes.size() > st->node_cap ||
+            p0 + tp.pairs.size() > st->pair_cap || g0 + tp.grid_list.size() > st->grid_cap)
+            throw Error(UD_ERR_CAPACITY, "the stream's arena is full");
+        // stage the slot in page-locked memory (a buffer whose previous copies are done)
+        PinnedBuf<unsigned char>& stg = st->staging[k & 1];
+        cuda_check(cudaEventSynchronize(st->staged[k & 1]), "staging");
+        size_t off = 0;
+        auto put = [&](const void* src, size_t bytes) {
+            off = (off + 15) & ~(size_t)15;
+            if (off + bytes > stg.n) throw Error(UD_ERR_CAPACITY, "slot larger than the staging buffer");
+            if (bytes) std::memcpy(stg.p + off, src, bytes);
+            const size_t at = off;
+            off += bytes;
+            return stg.p + at;
+        };
+        auto copy = [&](void* dst, const void* src, size_t bytes) {
+            if (bytes) cuda_check(cudaMemcpyAsync(dst, put(src, bytes), bytes, cudaMemcpyHostToDevice, st->cs), "H2D");
+        };
+        const unsigned int chains = (unsigned int)n * (unsigned int)st->E;
+        copy(st->d_desc.p + (size_t)k * st->M, tp.desc.data(), tp.desc.size() * sizeof(LigDesc));
+        copy(st->d_atoms.p + a0, tp.atoms.data(), tp.atoms.size() * sizeof(AtomRec));
+        copy(st->d_nodes.p + n0, tp.nodes.data(), tp.nodes.size() * sizeof(NodeRec));
+        copy(st->d_pairs.p + p0, tp.pairs.data(), tp.pairs.size() * 4);
+        copy(st->d_grid.p + g0, tp.grid_list.data(), tp.grid_list.size() * 4);
+        if (st->ad4) {
+            copy(st->d_charge.p + a0, tp.charges.data(), tp.charges.size() * sizeof(float));
+            copy(st->d_coef.p + 2 * p0, tp.coef.data(), tp.coef.size() * sizeof(float));
+        }
+        copy(st->d_order.p + (size_t)k * st->M, tp.order.data(), tp.order.size() * sizeof(int));
+        copy(st->d_slot_nlig.p + k, &n, sizeof(int));
+        copy(st->d_slot_left.p + k, &chains, sizeof(unsigned int));
+        // then the published count, after every copy of the slot on the same stream
+        cuda_check(cudaMemcpyAsync(st->d_ctl.p, st->h_counts.p + k + 1, sizeof(unsigned int), cudaMemcpyHostToDevice,
+                                   st->cs),
+                   "publish");
+        cuda_check(cudaEventRecord(st->staged[k & 1], st->cs), "event");
+        st->n_atoms = a0 + tp.atoms.size();
+        st->n_nodes = n0 + tp.nodes.size();
+        st->n_pairs = p0 + tp.pairs.size();
+        st->n_grid = g0 + tp.grid_list.size();
+        StreamSlot& sl = st->slots[k];
+        sl.ligs = v;
+        sl.max_atoms = tp.max_atoms;
+        sl.max_tors = tp.max_tors;
+        ++st->n_pushed;
+        if (slot) *slot = k;
+    });
+}
+
+static void stream_close(ud_stream st) {
+    if (st->closed) return;
+    cuda_check(cudaMemcpyAsync(st->d_ctl.p + 1, st->h_counts.p + st->max_slots + 1, sizeof(unsigned int),
+                               cudaMemcpyHostToDevice, st->cs),
+               "close");
+    st->closed = true;
+}
+
+extern "C" int ud_stream_close(ud_stream st) {
+    return guarded([&] {
+        if (!st) throw Error(UD_ERR_ARG, "null stream");
+        stream_close(st);
+    });
+}
+
+// The kernel's end status once it has stopped (it stopped early when a wait
+// ran out or an error ended it).
+static void stream_check_kernel(ud_stream st) {
+    const cudaError_t q = cudaStreamQuery(st->ks);
+    if (q == cudaErrorNotReady) return;
+    st->running = false;
+    st->finished = true;
+    cuda_check(q, "stream kernel");
+    cuda_check(cudaMemcpy(&st->status, st->d_status.p, sizeof(int), cudaMemcpyDeviceToHost), "status");
+}
+
+extern "C" int ud_stream_collect(ud_stream st, int slot) {
+    return guarded([&] {
+        if (!st) throw Error(UD_ERR_ARG, "null stream");
+        if (slot < 0 || slot >= st->n_pushed) throw Error(UD_ERR_ARG, "slot not pushed");
+        StreamSlot& sl = st->slots[slot];
+        if (sl.collected) return;
+        // the slot's chains are done when the kernel has set its flag
+        const volatile unsigned int* done = st->h_done + slot;
+        while (*done == 0) {
+            if (st->running) stream_check_kernel(st);
+            if (!st->running) {
+                if (*done) break;
+                if (st->status == kStreamTimeout)
+                    throw Error(UD_ERR_TIMEOUT, "the stream kernel stopped waiting for a slot to be published");
+                throw Error(UD_ERR_STATE, "the stream kernel ended before slot " + std::to_string(slot) + " was done");
+            }
+            std::this_thread::sleep_for(std::chrono::microseconds(100));
+        }
+        std::atomic_thread_fence(std::memory_order_acquire);
+        const int n = (int)sl.ligs.size(), E = st->E, cap = st->cap, stride = st->stride;
+        const size_t r = (size_t)(slot % st->ring), M = (size_t)st->M;
+        const size_t n_chain = (size_t)n * E, n_mode = (size_t)n * cap;
+        float* poses = st->d_poses.p + r * M * E * stride;
+        ChainResult* results = st->d_results.p + r * M * E;
+        float* scratch = st->d_scratch.p + r * M * cap * 3 * st->max_atoms;
+        int* n_modes = st->d_n_modes.p + r * M;
+        int* mode_chain = st->d_mode_chain.p + r * M * cap;
+        int* mode_lig = st->d_mode_lig.p + r * M * cap;
+        float* mode_pose = st->d_mode_pose.p + r * M * cap * stride;
+        float* mode_e = st->d_mode_e.p + r * M * cap * 4;
+        const DeviceBatchView v = st->view(slot);
+        cudaStream_t ps = st->ps;
+        // launch_cluster indexes the scratch by the view's largest ligand: the slot's,
+        // at most the stream's, so the stream-sized area holds it
+        cuda_check(launch_cluster(v, poses, stride, results, n, E, cap, st->params.min_rmsd, scratch, n_modes,
+                                  mode_chain, mode_lig, mode_pose, ps),
+                   "stream clustering");
+        if (st->refined) {
+            DeviceReceptorView rv = st->maps->rc;
+            rv.lig_bias = nullptr;
+            rv.lig_bias_span = nullptr;
+            cuda_check(launch_receptor(kRecRefine, v, tables_view(st->maps), rv, mode_lig, mode_pose, stride,
+                                       (int)n_mode, st->params.refine_step, 0.0f, 1000.0f, nullptr, nullptr, 0,
+                                       mode_e, ps),
+                       "stream refinement");
+        }
+        auto d2h = [&](void* dst, const void* src, size_t bytes) {
+            cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ps), "D2H");
+        };
+        d2h(st->hp_n_modes.p, n_modes, n * sizeof(int));
+        d2h(st->hp_mode_chain.p, mode_chain, n_mode * sizeof(int));
+        d2h(st->hp_mode_pose.p, mode_pose, n_mode * stride * sizeof(float));
+        if (st->refined) d2h(st->hp_mode_e.p, mode_e, n_mode * 4 * sizeof(float));
+        d2h(st->hp_results.p, results, n_chain * sizeof(ChainResult));
+        d2h(st->hp_poses.p, poses, n_chain * stride * sizeof(float));
+        cuda_check(cudaStreamSynchronize(ps), "stream post-processing");
+        sl.results.assign(st->hp_results.p, st->hp_results.p + n_chain);
+        sl.poses.assign(st->hp_poses.p, st->hp_poses.p + n_chain * stride);
+        for (const ChainResult& c : sl.results) st->evals += c.evals;
+        sl.post.assign(n, LigandPost{});
+        parallel_for(n, [&](int l) {
+            const size_t o = (size_t)l * cap;
+            sl.post[l] = post_process_ligand(st->maps->sf, *sl.ligs[l], E, cap, stride, st->refined,
+                                             st->hp_n_modes.p[l], st->hp_mode_chain.p + o,
+                                             st->hp_mode_pose.p + o * stride, st->hp_mode_e.p + 4 * o,
+                                             sl.results.data() + (size_t)l * E);
+        });
+        sl.collected = true;
+    });
+}
+
+static const StreamSlot& collected_slot(ud_stream st, int slot, int lig) {
+    if (!st) throw Error(UD_ERR_ARG, "null stream");
+    if (slot < 0 || slot >= st->n_pushed || !st->slots[slot].collected) throw Error(UD_ERR_STATE, "slot not collected");
+    const StreamSlot& sl = st->slots[slot];
+    if (lig < 0 || lig >= (int)sl.ligs.size()) throw Error(UD_ERR_ARG, "ligand out of range");
+    return sl;
+}
+
+extern "C" int ud_stream_result_count(ud_stream st, int slot, int lig, int* n_modes) {
+    return guarded([&] {
+        if (!n_modes) throw Error(UD_ERR_ARG, "null argument");
+        *n_modes = (int)collected_slot(st, slot, lig).post[lig].modes.size();
+    });
+}
+
+extern "C" int ud_stream_result_mode(ud_stream st, int slot, int lig, int k, float* pose, float energies[8]) {
+    return guarded([&] {
+        const auto& m = collected_slot(st, slot, lig).post[lig].modes;
+        if (k < 0 || k >= (int)m.size()) throw Error(UD_ERR_ARG, "mode out of range");
+        if (pose) std::copy(m[k].pose.begin(), m[k].pose.end(), pose);
+        if (energies) {
+            const float e[8] = {m[k].e, m[k].lb, m[k].ub, m[k].total, m[k].inter, m[k].intra, m[k].conf_indep,
+                                m[k].unbound};
+            std::copy(e, e + 8, energies);
+        }
+    });
+}
+
+extern "C" int ud_stream_result_write(ud_stream st, int slot, int lig, int format, char* buf, size_t cap,
+                                      size_t* len) {
+    return guarded([&] {
+        const StreamSlot& sl = collected_slot(st, slot, lig);
+        if (format != 0 && format != 1) throw Error(UD_ERR_ARG, "format must be 0 (PDBQT) or 1 (SDF)");
+        const std::string t = render_modes(*sl.ligs[lig], sl.post[lig], st->params.num_modes,
+                                           st->params.energy_range, st->ad4, format);
+        if (len) *len = t.size();
+        if (buf && cap > 0) {
+            const size_t n = std::min(cap - 1, t.size());
+            std::memcpy(buf, t.data(), n);
+            buf[n] = 0;
+        }
+    });
+}
+
+extern "C" int ud_stream_chains(ud_stream st, int slot, float* poses, int pose_stride, float* e, int* evals) {
+    return guarded([&] {
+        const StreamSlot& sl = collected_slot(st, slot, 0);
+        const size_t n_chain = sl.results.size();
+        if (poses) {
+            if (pose_stride < 7 + st->max_tors) throw Error(UD_ERR_ARG, "pose_stride smaller than 7 + max_torsions");
+            for (size_t i = 0; i < n_chain; ++i)
+                std::copy(sl.poses.begin() + i * st->stride, sl.poses.begin() + (i + 1) * st->stride,
+                          poses + i * pose_stride);
+        }
+        for (size_t i = 0; i < n_chain; ++i) {
+            if (e) e[i] = sl.results[i].e;
+            if (evals) evals[i] = sl.results[i].evals;
+        }
+    });
+}
+
+extern "C" int ud_stream_finish(ud_stream st, long long* evals) {
+    return guarded([&] {
+        if (!st) throw Error(UD_ERR_ARG, "null stream");
+        if (st->running) {
+            cuda_check(cudaStreamSynchronize(st->ks), "stream kernel");
+            stream_check_kernel(st);
+        }
+        if (evals) *evals = st->evals;
+        if (st->status == kStreamTimeout)
+            throw Error(UD_ERR_TIMEOUT, "the stream kernel stopped waiting for a slot to be published");
+    });
+}
+
+extern "C" int ud_stream_destroy(ud_stream st) {
+    delete st;
+    return UD_OK;
 }

@@ -24,6 +24,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <mutex>
@@ -190,13 +191,42 @@ struct Batch {
     const float2* pair_coef; // AD4: per pair slot (q_a q_b, |q_a| V_b + |q_b| V_a)
 };
 
-#ifndef UD_PAIR_BATCH
-#define UD_PAIR_BATCH 1
-#endif
 // pair groups whose table rows are in flight together (larger values unroll
 // more code into the hot loop, which costs more in instruction fetch than the
 // extra loads in flight gain)
+#ifndef UD_PAIR_BATCH
+#define UD_PAIR_BATCH 1
+#endif
 constexpr int kPairBatch = UD_PAIR_BATCH;
+
+// Loads of the L2-resident maps and pair tables: read once per use with little
+// reuse in L1, so with UD_NA_LOADS they do not allocate L1 lines
+// (ld.global.nc.L1::no_allocate), leaving L1 to the ligand topology.
+#ifndef UD_NA_LOADS
+#define UD_NA_LOADS 0
+#endif
+#ifndef UD_PAIR_PREFETCH
+#define UD_PAIR_PREFETCH 0
+#endif
+__device__ __forceinline__ float2 ld_stream2(const float2* p) {
+#if UD_NA_LOADS
+    float2 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+    return v;
+#else
+    return __ldg(p);
+#endif
+}
+__device__ __forceinline__ float4 ld_stream4(const float4* p) {
+#if UD_NA_LOADS
+    float4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+    return v;
+#else
+    return __ldg(p);
+#endif
+}
 
 struct Tables {
     const float4* smooth4; // [tp][bin] (e, dE/dr / r) of bin and bin + 1
@@ -212,6 +242,7 @@ constexpr int kAd4RowE = kAd4TableRowElec, kAd4RowG = kAd4TableRowDesolv;
 
 struct Maps {
     const float* data;     // [slot][z][y][x]
+    const float2* xp;      // [slot][z][y][x] = (data at x, data at x + 1): corner pairs in one 8-byte load
     int nx, ny, nz;
     float init[3], factor[3], factor_inv[3], dim_m1[3];
     float slope;
@@ -265,18 +296,25 @@ __host__ inline Layout make_layout(int max_atoms, int max_tors) {
     return L;
 }
 
-// Per-warp context of the ligand being worked on (kept in registers).
+// Per-warp context of the ligand being worked on (kept in registers): the
+// ligand's offsets into the batch arrays, which stay in the kernel parameters
+// (a pointer to them costs no register once inlined), rather than seven
+// 64-bit pointers.
 struct Ctx {
     float* s;              // shared memory of this warp
-    const AtomRec* atoms;
-    const NodeRec* nodes;
-    const uint32_t* pairs;
-    const uint32_t* grid;  // atom | slot << 8 of the atoms with a grid map
-    const float* q;        // AD4: atom charges
-    const float2* coef;    // AD4: per pair slot coefficients
+    const Batch* B;
+    int atom_off, node_off, pair_off, grid_off;
     int n_atoms, R, T, n_pairs, max_depth, local_steps, n_grid;
     int lane;
     int lig;
+    __device__ __forceinline__ const AtomRec* atoms() const { return B->atoms + atom_off; }
+    __device__ __forceinline__ const NodeRec* nodes() const { return B->nodes + node_off; }
+    __device__ __forceinline__ const uint32_t* pairs() const { return B->pairs + pair_off; }
+    // atom | slot << 8 of the atoms with a grid map
+    __device__ __forceinline__ const uint32_t* grid() const { return B->grid_list + grid_off; }
+    // AD4: atom charges and per pair slot coefficients
+    __device__ __forceinline__ const float* q() const { return B->charges + atom_off; }
+    __device__ __forceinline__ const float2* coef() const { return B->pair_coef + pair_off; }
 };
 
 template <int kW = 32>
@@ -284,12 +322,11 @@ __device__ __forceinline__ Ctx make_ctx(const Batch& B, int lig, float* s) {
     Ctx c;
     const LigDesc* d = B.ligs + lig;
     c.s = s;
-    c.atoms = B.atoms + __ldg(&d->atom_off);
-    c.nodes = B.nodes + __ldg(&d->node_off);
-    c.pairs = B.pairs + __ldg(&d->pair_off);
-    c.grid = B.grid_list + __ldg(&d->grid_off);
-    c.q = B.charges + __ldg(&d->atom_off);
-    c.coef = B.pair_coef + __ldg(&d->pair_off);
+    c.B = &B;
+    c.atom_off = __ldg(&d->atom_off);
+    c.node_off = __ldg(&d->node_off);
+    c.pair_off = __ldg(&d->pair_off);
+    c.grid_off = __ldg(&d->grid_off);
     c.n_grid = __ldg(&d->n_grid);
     c.n_atoms = __ldg(&d->n_atoms);
     c.R = __ldg(&d->n_nodes);
@@ -313,11 +350,28 @@ __device__ __forceinline__ Ctx make_ctx(const Batch& B, int lig, float* s) {
 template <int kW = 32>
 __device__ __forceinline__ void kinematics(const Ctx& c, const Layout& L, const float* conf) {
     float* fr = c.s + L.frames;
+    const NodeRec* nodes = c.nodes();
     // frame layout (20 floats): origin[0..2] q[3..6] R[7..15] lab axis[16..18];
-    // [16..19] hold the local torsion quaternion until the node is composed
-    for (int n = 1 + c.lane; n < c.R; n += kW) {
-        const NodeRec* nr = c.nodes + n;
-        float ra[3] = {__ldg(&nr->rel_axis[0]), __ldg(&nr->rel_axis[1]), __ldg(&nr->rel_axis[2])};
+    // [16..19] hold the local torsion quaternion until the node is composed.
+    // A lane's first node (1 + lane) is read from global memory once and kept
+    // in registers for the torsion pass and every tree level; nodes past the
+    // lanes (more than kW - 1 torsions) are read where they are used.
+    const int n0 = 1 + c.lane;
+    float ro0[3] = {0.0f, 0.0f, 0.0f}, ra0[3] = {0.0f, 0.0f, 0.0f};
+    int par0 = 0, dep0 = 0;
+    if (n0 < c.R) {
+        const NodeRec* nr = nodes + n0;
+        ro0[0] = __ldg(&nr->rel_origin[0]); ro0[1] = __ldg(&nr->rel_origin[1]); ro0[2] = __ldg(&nr->rel_origin[2]);
+        ra0[0] = __ldg(&nr->rel_axis[0]); ra0[1] = __ldg(&nr->rel_axis[1]); ra0[2] = __ldg(&nr->rel_axis[2]);
+        par0 = __ldg(&nr->parent);
+        dep0 = __ldg(&nr->depth);
+    }
+    for (int n = n0; n < c.R; n += kW) {
+        float ra[3] = {ra0[0], ra0[1], ra0[2]};
+        if (n != n0) {
+            const NodeRec* nr = nodes + n;
+            ra[0] = __ldg(&nr->rel_axis[0]); ra[1] = __ldg(&nr->rel_axis[1]); ra[2] = __ldg(&nr->rel_axis[2]);
+        }
         axis_angle_q(ra, conf[7 + n - 1], fr + 20 * n + 16);
     }
     if (c.lane == 0) {
@@ -327,14 +381,21 @@ __device__ __forceinline__ void kinematics(const Ctx& c, const Layout& L, const 
     }
     lanes_sync<kW>();
     for (int d = 1; d <= c.max_depth; ++d) {
-        for (int n = 1 + c.lane; n < c.R; n += kW) {
-            const NodeRec* nr = c.nodes + n;
-            if (__ldg(&nr->depth) != d) continue;
-            const float* pf = fr + 20 * __ldg(&nr->parent);
+        for (int n = n0; n < c.R; n += kW) {
+            float ro[3] = {ro0[0], ro0[1], ro0[2]}, ra[3] = {ra0[0], ra0[1], ra0[2]};
+            int parent = par0, depth = dep0;
+            if (n != n0) {
+                const NodeRec* nr = nodes + n;
+                depth = __ldg(&nr->depth);
+                if (depth != d) continue;
+                parent = __ldg(&nr->parent);
+                ro[0] = __ldg(&nr->rel_origin[0]); ro[1] = __ldg(&nr->rel_origin[1]); ro[2] = __ldg(&nr->rel_origin[2]);
+                ra[0] = __ldg(&nr->rel_axis[0]); ra[1] = __ldg(&nr->rel_axis[1]); ra[2] = __ldg(&nr->rel_axis[2]);
+            }
+            if (depth != d) continue;
+            const float* pf = fr + 20 * parent;
             float* f = fr + 20 * n;
             const float* pm = pf + 7;
-            float ro[3] = {__ldg(&nr->rel_origin[0]), __ldg(&nr->rel_origin[1]), __ldg(&nr->rel_origin[2])};
-            float ra[3] = {__ldg(&nr->rel_axis[0]), __ldg(&nr->rel_axis[1]), __ldg(&nr->rel_axis[2])};
             float t[4] = {f[16], f[17], f[18], f[19]};
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
@@ -351,7 +412,7 @@ __device__ __forceinline__ void kinematics(const Ctx& c, const Layout& L, const 
     }
     float4* xyz = reinterpret_cast<float4*>(c.s + L.coords);
     for (int a = c.lane; a < c.n_atoms; a += kW) {
-        AtomRec ar = c.atoms[a];
+        AtomRec ar = c.atoms()[a];
         int n = ar.packed & 0xFF;
         const float* f = fr + 20 * n;
         const float* m = f + 7;
@@ -384,13 +445,14 @@ __device__ __forceinline__ float grid_eval(const Maps& M, int slot, const float4
     }
     const float penalty = M.slope * (miss[0] * M.factor_inv[0] + miss[1] * M.factor_inv[1] +
                                      miss[2] * M.factor_inv[2]);
-    const float* g = M.data + (size_t)slot * M.nx * M.ny * M.nz;
+    // the 8 corners as 4 x-pairs: a[0] <= nx - 2, so x + 1 is always a grid point
+    const float2* g = M.xp + (size_t)slot * M.nx * M.ny * M.nz;
     const int sy = M.nx, sz = M.nx * M.ny;
     const int base = a[0] + sy * a[1] + sz * a[2];
-    const float f000 = __ldg(g + base), f100 = __ldg(g + base + 1);
-    const float f010 = __ldg(g + base + sy), f110 = __ldg(g + base + 1 + sy);
-    const float f001 = __ldg(g + base + sz), f101 = __ldg(g + base + 1 + sz);
-    const float f011 = __ldg(g + base + sy + sz), f111 = __ldg(g + base + 1 + sy + sz);
+    const float2 c00 = ld_stream2(g + base), c10 = ld_stream2(g + base + sy);
+    const float2 c01 = ld_stream2(g + base + sz), c11 = ld_stream2(g + base + sy + sz);
+    const float f000 = c00.x, f100 = c00.y, f010 = c10.x, f110 = c10.y;
+    const float f001 = c01.x, f101 = c01.y, f011 = c11.x, f111 = c11.y;
     const float x = s[0], y = s[1], z = s[2];
     const float mx = 1 - x, my = 1 - y, mz = 1 - z;
     float f = f000 * mx * my * mz + f100 * x * my * mz + f010 * mx * y * mz + f110 * x * y * mz +
@@ -530,8 +592,7 @@ __device__ __forceinline__ float receptor_term(const Receptor& R, const Tables& 
 
 // Energy and gradient (change layout: position, torque, torsions) of `conf`.
 // Pair forces use the table's dE/dr / r column (precalculate.h:48-65) or, with
-// kExactPairs, the slope of the lerped energy itself (the exact derivative of
-// the computed energy, 2 factor (e_bin+1 - e_bin) per unit r^2).
+// kExactPairs, the slope of the lerped energy itself.
 // With kReceptor the receptor term comes from the receptor atoms (`Rc`,
 // out-of-box slope `rslope`) instead of the maps.
 template <bool kExactPairs = false, bool kAD4 = false, bool kReceptor = false, int kW = 32>
@@ -544,6 +605,8 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
     const float4* xyz = reinterpret_cast<const float4*>(c.s + L.coords);
     float4* frc = reinterpret_cast<float4*>(c.s + L.forces);
     float e = 0;
+    // the per-atom force array: the grid (or receptor-atom) force of every
+    // atom, then the pair forces of every pair chunk but the last
     for (int k = c.lane; k < c.n_atoms; k += kW) frc[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     lanes_sync<kW>();
     if constexpr (kReceptor) {
@@ -551,8 +614,8 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
         int n_bias;
         bias_of(*Rc, c.lig, bias, n_bias);
         for (int k = 0; k < c.n_grid; ++k) {  // one atom at a time, lanes over its receptor atoms
-            const int a = __ldg(c.grid + k) & 0xFF;
-            const int t1 = ((__ldg(&c.atoms[a].packed) >> 24) & 0xFF) - 1;
+            const int a = __ldg(c.grid() + k) & 0xFF;
+            const int t1 = ((__ldg(&c.atoms()[a].packed) >> 24) & 0xFF) - 1;
             float gx, gy, gz;
             const float ea = receptor_term<true>(*Rc, Tb, t1, xyz[a], v_inter, rslope, bias, n_bias, gx, gy, gz);
             if (c.lane == 0) {
@@ -561,14 +624,17 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
             }
         }
     } else {
+        // grid energy and gradient (grid.cpp:40-129) over the compacted list of
+        // atoms with a map: one pass of lanes, so that all corner loads of a
+        // ligand of up to kW heavy atoms are in flight together
         for (int k = c.lane; k < c.n_grid; k += kW) {
-            const uint32_t ga = __ldg(c.grid + k);
+            const uint32_t ga = __ldg(c.grid() + k);
             const int a = ga & 0xFF, slot = ga >> 8;
             float gx, gy, gz;
             const float4 pa = xyz[a];
             e += grid_eval(M, slot, pa, v_inter, gx, gy, gz, true);
             if constexpr (kAD4) {  // electrostatic map x q, desolvation map x |q| (ad4cache.cpp:227-269)
-                const float q = __ldg(c.q + a), aq = fabsf(q);
+                const float q = __ldg(c.q() + a), aq = fabsf(q);
                 float hx, hy, hz;
                 e += q * grid_eval(M, M.e_slot, pa, v_inter, hx, hy, hz, true);
                 gx += q * hx; gy += q * hy; gz += q * hz;
@@ -588,6 +654,9 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
     constexpr int kWinShift = kW == 32 ? 5 : 4;
     constexpr int kWinPasses = kW / kPairPassWidth;
     const int n_groups = c.n_pairs >> kWinShift;   // windows; n_pairs is a multiple of 32
+    // with UD_PAIR_PREFETCH the next window's pair word is loaded while this
+    // window is worked on, so its latency is off the window's dependent chain
+    uint32_t pr_next = (UD_PAIR_PREFETCH && n_groups > 0) ? __ldg(c.pairs() + c.lane) : kPairPad;
     for (int g0 = 0; g0 < n_groups; g0 += kPairBatch) {
         float4 tv[kPairBatch];
         float rv[kPairBatch][3];
@@ -597,7 +666,13 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
         for (int u = 0; u < kPairBatch; ++u) {
             prv[u] = kPairPad;
             if (g0 + u < n_groups) {
-                uint32_t pr = __ldg(c.pairs + ((g0 + u) << kWinShift) + c.lane);
+                uint32_t pr;
+                if (UD_PAIR_PREFETCH && kPairBatch == 1) {
+                    pr = pr_next;
+                    pr_next = g0 + 1 < n_groups ? __ldg(c.pairs() + ((g0 + 1) << kWinShift) + c.lane) : kPairPad;
+                } else {
+                    pr = __ldg(c.pairs() + ((g0 + u) << kWinShift) + c.lane);
+                }
                 if (pr != kPairPad) {
                     int a = pr & 0xFF, b = (pr >> 8) & 0xFF, tp = pr >> 16;
                     const float4 pa = xyz[a], pb = xyz[b];
@@ -608,9 +683,9 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
                         int i1 = (int)rf;
                         remv[u] = rf - i1;
                         rv[u][0] = rx; rv[u][1] = ry; rv[u][2] = rz;
-                        tv[u] = __ldg(Tb.smooth4 + (size_t)tp * Tb.n_bins + i1);
+                        tv[u] = ld_stream4(Tb.smooth4 + (size_t)tp * Tb.n_bins + i1);
                         if constexpr (kAD4) {  // + q_a q_b E(r) + (|q_a| V_b + |q_b| V_a) G(r)
-                            const float2 cf = __ldg(c.coef + ((g0 + u) << kWinShift) + c.lane);
+                            const float2 cf = __ldg(c.coef() + ((g0 + u) << kWinShift) + c.lane);
                             const float4 te = __ldg(Tb.smooth4 + (size_t)kAd4RowE * Tb.n_bins + i1);
                             const float4 tg = __ldg(Tb.smooth4 + (size_t)kAd4RowG * Tb.n_bins + i1);
                             tv[u].x += cf.x * te.x + cf.y * tg.x;
@@ -696,7 +771,7 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
     }
     lanes_sync<kW>();
     for (int n = c.lane; n < c.R; n += kW) {
-        const int span = __ldg(&c.nodes[n].atoms);
+        const int span = __ldg(&c.nodes()[n].atoms);
         const int b0 = span & 0xFFFF, b1 = span >> 16;
         const float* hi = pre + 6 * (b1 - 1);
         float sm[6];
@@ -724,7 +799,7 @@ template <bool kAD4 = false, int kW = 32>
 __device__ __forceinline__ float intra_fast(const Ctx& c, const Tables& Tb, const float4* xyz, float v) {
     float ei = 0;
     for (int k = c.lane; k < c.n_pairs; k += kW) {
-        uint32_t pr = __ldg(c.pairs + k);
+        uint32_t pr = __ldg(c.pairs() + k);
         if (pr == kPairPad) continue;
         int a = pr & 0xFF, b = (pr >> 8) & 0xFF, tp = pr >> 16;
         const float4 pa = xyz[a], pb = xyz[b];
@@ -734,7 +809,7 @@ __device__ __forceinline__ float intra_fast(const Ctx& c, const Tables& Tb, cons
             const int bin = (int)(Tb.factor * r2);
             float t = __ldg(Tb.fast + (size_t)tp * Tb.n_bins + bin);
             if constexpr (kAD4) {
-                const float2 cf = __ldg(c.coef + k);
+                const float2 cf = __ldg(c.coef() + k);
                 t += cf.x * __ldg(Tb.fast + (size_t)kAd4RowE * Tb.n_bins + bin) +
                      cf.y * __ldg(Tb.fast + (size_t)kAd4RowG * Tb.n_bins + bin);
             }
@@ -755,12 +830,12 @@ __device__ __forceinline__ void eval_score(const Ctx& c, const Layout& L, const 
     const float4* xyz = reinterpret_cast<const float4*>(c.s + L.coords);
     float eg = 0;
     for (int k = c.lane; k < c.n_grid; k += kW) {
-        const uint32_t ga = __ldg(c.grid + k);
+        const uint32_t ga = __ldg(c.grid() + k);
         float gx, gy, gz;
         const float4 pa = xyz[ga & 0xFF];
         eg += grid_eval(M, ga >> 8, pa, v, gx, gy, gz, false);
         if constexpr (kAD4) {
-            const float q = __ldg(c.q + (ga & 0xFF));
+            const float q = __ldg(c.q() + (ga & 0xFF));
             eg += q * grid_eval(M, M.e_slot, pa, v, gx, gy, gz, false);
             eg += fabsf(q) * grid_eval(M, M.d_slot, pa, v, gx, gy, gz, false);
         }
@@ -913,7 +988,7 @@ __device__ void mutate(const Ctx& c, const Layout& L, Philox& rng, float amplitu
         const float* o = c.s + L.frames;
         float acc = 0, cnt = 0;
         for (int a = c.lane; a < c.n_atoms; a += kW) {
-            int packed = __ldg(&c.atoms[a].packed);
+            int packed = __ldg(&c.atoms()[a].packed);
             if ((packed >> 16) & 1) {
                 const float4 pa = xyz[a];
                 float dx = pa.x - o[0], dy = pa.y - o[1], dz = pa.z - o[2];
@@ -975,13 +1050,59 @@ struct Machine {
 // The MC chain of monte_carlo.cu:237-356 (mutate, BFGS at the hunt cap,
 // Metropolis at temperature T, refine improvements at the authentic cap, keep
 // the best) with the line search and BFGS iterations of bfgs.h:63-146.
-template <bool kSearch, bool kAD4, int kW>
+// Nanoseconds of the GPU's global timer.
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// The next (ligand, chain) item of a streaming screen for lane 0 of a chain
+// (StreamView): the item's global ligand id and chain, or -1 when the stream
+// is closed and drained, the arena is exhausted, or a wait for a publication
+// ran past the time limit (status set to kStreamTimeout).  Stream control
+// words are written by host copies while the kernel runs, so they are read
+// from L2 (ld.global.cg), never from a cached line.
+__device__ __noinline__ int stream_fetch(const StreamView& SV, int E, int* item_out, int* chain_out) {
+    const unsigned per_slot = (unsigned)SV.slot_ligands * (unsigned)E;
+    for (;;) {
+        const unsigned it = atomicAdd(SV.next_item, 1u);
+        const unsigned s = it / per_slot;
+        if (s >= (unsigned)SV.max_slots) return -1;
+        if (__ldcg(SV.published) <= s) {
+            const unsigned long long t0 = global_ns();
+            for (;;) {
+                if (__ldcg(SV.published) > s) break;
+                if (__ldcg(SV.closed)) {
+                    __threadfence();
+                    if (__ldcg(SV.published) > s) break;
+                    return -1;
+                }
+                if (global_ns() - t0 > SV.timeout_ns) {
+                    atomicExch(SV.status, kStreamTimeout);
+                    return -1;
+                }
+                __nanosleep(2000);
+            }
+        }
+        __threadfence();
+        const unsigned within = it - s * per_slot;
+        const int l = (int)(within / (unsigned)E);
+        if (l >= __ldcg(SV.slot_nlig + s)) continue;  // past the slot's ligands
+        *item_out = (int)it;
+        *chain_out = (int)(within % (unsigned)E);
+        return __ldcg(SV.order + (size_t)s * SV.slot_ligands + l);
+    }
+}
+
+template <bool kSearch, bool kAD4, int kW, bool kStream = false>
 __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const Tables& Tb,
                                             const SearchParams& P, const Layout& L, float* sw,
                                             const int* order, int n_items, int first_item,
                                             unsigned int* queue, float* poses, int pose_stride,
                                             ChainResult* results, const int* opt_lig, int opt_steps,
-                                            float opt_v, float* opt_e, int* opt_evals) {
+                                            float opt_v, float* opt_e, int* opt_evals,
+                                            const StreamView* SV = nullptr) {
     const int lane = threadIdx.x & (kW - 1);
     const int slot_in_block = threadIdx.x / kW;    // this chain's index in the CTA
     const int chains_in_block = blockDim.x / kW;
@@ -999,7 +1120,20 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
         while (eval_x == nullptr) {
             if (st == S_FETCH) {
                 int it;
-                if (!kSearch) {
+                if constexpr (kStream) {  // (ligand, chain) of the next published item
+                    int v[3] = {-1, 0, 0};
+                    if (lane == 0) v[0] = stream_fetch(*SV, P.exhaustiveness, &v[1], &v[2]);
+                    const int lig = __shfl_sync(lanes_mask<kW>(), v[0], 0, kW);
+                    if (lig < 0) {
+                        st = S_EXIT;
+                        break;
+                    }
+                    m.item = __shfl_sync(lanes_mask<kW>(), v[1], 0, kW);
+                    m.lig = lig;
+                    m.chain = __shfl_sync(lanes_mask<kW>(), v[2], 0, kW);
+                    first = false;
+                    it = 0;
+                } else if (!kSearch) {
                     it = first ? blockIdx.x * chains_in_block + slot_in_block : n_items;
                 } else if (P.persistent) {
                     unsigned int v = 0;
@@ -1011,15 +1145,17 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                     else it -= first_item;
                 }
                 first = false;
-                if (it < 0 || it >= n_items) {
+                if (!kStream && (it < 0 || it >= n_items)) {
                     st = S_EXIT;
                     break;
                 }
-                m.item = it;
+                if (!kStream) m.item = it;
                 if (kSearch) {
-                    const int gi = P.persistent ? it : it + first_item;
-                    m.lig = order[gi / P.exhaustiveness];
-                    m.chain = gi % P.exhaustiveness;
+                    if (!kStream) {
+                        const int gi = P.persistent ? it : it + first_item;
+                        m.lig = order[gi / P.exhaustiveness];
+                        m.chain = gi % P.exhaustiveness;
+                    }
                     c = make_ctx<kW>(B, m.lig, sw);
                     rng.init(P.seed, (uint32_t)m.lig, (uint32_t)m.chain);
                     m.steps_cap = c.local_steps;
@@ -1169,7 +1305,14 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                 st = S_MC_STEP;
             } else if (st == S_DONE) {
                 if (kSearch) {
-                    const int slot = m.lig * P.exhaustiveness + m.chain;
+                    int slot = m.lig * P.exhaustiveness + m.chain;
+                    unsigned sslot = 0;
+                    if constexpr (kStream) {  // this slot's area of the result ring
+                        sslot = (unsigned)m.item / ((unsigned)SV->slot_ligands * (unsigned)P.exhaustiveness);
+                        const int local = m.lig - (int)sslot * SV->slot_ligands;
+                        slot = ((int)(sslot % (unsigned)SV->ring) * SV->slot_ligands + local) * P.exhaustiveness +
+                               m.chain;
+                    }
                     const float* best = c.s + L.best;
                     for (int i = lane; i < 7 + c.T; i += kW) poses[(size_t)slot * pose_stride + i] = best[i];
                     // scoring-path energies of the best pose for the final rescoring
@@ -1183,6 +1326,16 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                         results[slot].chain = m.chain;
                         results[slot].e_grid = eg;
                         results[slot].e_intra = ei;
+                    }
+                    if constexpr (kStream) {  // the slot's last chain tells the host
+                        lanes_sync<kW>();
+                        if (lane == 0) {
+                            __threadfence();
+                            if (atomicSub(SV->slot_left + sslot, 1u) == 1u) {
+                                __threadfence_system();
+                                *((volatile unsigned int*)(SV->done_host + sslot)) = 1u;
+                            }
+                        }
                     }
                 } else {
                     const float* x = c.s + L.x;
@@ -1225,6 +1378,18 @@ __global__ void __launch_bounds__(128, kAD4 ? UD_SEARCH_MIN_BLOCKS_AD4 : UD_SEAR
     float* sw = smem + (size_t)(threadIdx.x / kW) * L.total;
     run_machine<true, kAD4, kW>(B, M, Tb, P, L, sw, order, n_items, first_item, queue, poses, pose_stride, results,
                             nullptr, 0, 0.f, nullptr, nullptr);
+}
+
+// The persistent search of a streaming screen (StreamView): one warp per chain.
+template <bool kAD4>
+__global__ void __launch_bounds__(128, kAD4 ? UD_SEARCH_MIN_BLOCKS_AD4 : UD_SEARCH_MIN_BLOCKS) stream_kernel(
+    const __grid_constant__ Batch B, const __grid_constant__ Maps M, const __grid_constant__ Tables Tb,
+    const __grid_constant__ SearchParams P, const __grid_constant__ Layout L, const __grid_constant__ StreamView SV,
+    float* poses, int pose_stride, ChainResult* results) {
+    extern __shared__ __align__(16) float smem[];
+    float* sw = smem + (size_t)(threadIdx.x / 32) * L.total;
+    run_machine<true, kAD4, 32, true>(B, M, Tb, P, L, sw, nullptr, 0, 0, nullptr, poses, pose_stride, results,
+                                      nullptr, 0, 0.f, nullptr, nullptr, &SV);
 }
 
 // Local optimisation from given poses (quasi_newton, quasi_newton.cpp:42-53):
@@ -1283,7 +1448,7 @@ __device__ __forceinline__ bool heavy_within(const Ctx& c, const Layout& L, cons
     const float m = 1e-4f;
     bool ok = true;
     for (int a = c.lane; a < c.n_atoms; a += 32) {
-        if (!((__ldg(&c.atoms[a].packed) >> 16) & 1)) continue;
+        if (!((__ldg(&c.atoms()[a].packed) >> 16) & 1)) continue;
         const float4 x = xyz[a];
         if (x.x < R.begin[0] - m || x.x > R.end[0] + m || x.y < R.begin[1] - m || x.y > R.end[1] + m ||
             x.z < R.begin[2] - m || x.z > R.end[2] + m)
@@ -1304,8 +1469,8 @@ __device__ __forceinline__ void eval_score_receptor(const Ctx& c, const Layout& 
     bias_of(R, c.lig, bias, n_bias);
     float ei = 0;
     for (int k = 0; k < c.n_grid; ++k) {
-        const int a = __ldg(c.grid + k) & 0xFF;
-        const int t1 = ((__ldg(&c.atoms[a].packed) >> 24) & 0xFF) - 1;
+        const int a = __ldg(c.grid() + k) & 0xFF;
+        const int t1 = ((__ldg(&c.atoms()[a].packed) >> 24) & 0xFF) - 1;
         float gx, gy, gz;
         ei += receptor_term<false>(R, Tb, t1, xyz[a], v, 1e6f, bias, n_bias, gx, gy, gz);
     }
@@ -1451,7 +1616,7 @@ __device__ __forceinline__ float heavy_rmsd(const Ctx& c, const float4* xyz, con
                                             int n_heavy) {
     float sum = 0;
     for (int i = c.lane; i < c.n_atoms; i += 32) {
-        if (!((__ldg(&c.atoms[i].packed) >> 16) & 1)) continue;
+        if (!((__ldg(&c.atoms()[i].packed) >> 16) & 1)) continue;
         float dx, dy, dz;
         if (a) {
             dx = a[3 * i] - b[3 * i]; dy = a[3 * i + 1] - b[3 * i + 1]; dz = a[3 * i + 2] - b[3 * i + 2];
@@ -1689,7 +1854,7 @@ __global__ void __launch_bounds__(128) adjoint_kernel(
         const float4* xyz = reinterpret_cast<const float4*>(sw + L.coords);  // conformer of the evaluation above
         const size_t plane = (size_t)M.nx * M.ny * M.nz;
         for (int k = c.lane; k < c.n_grid; k += 32) {
-            const uint32_t ga = __ldg(c.grid + k);
+            const uint32_t ga = __ldg(c.grid() + k);
             const int a = ga & 0xFF, slot = ga >> 8;
             int cell;
             float frac[3];
@@ -1699,7 +1864,7 @@ __global__ void __launch_bounds__(128) adjoint_kernel(
             for (int t = 0; t < kMaxTerms; ++t)
                 if (t < TD.n_terms) acc[t] += w * trilinear(M, TD.maps + t * TD.map_block + slot * plane, cell, frac);
             if constexpr (kAD4) {
-                const float q = __ldg(c.q + a), aq = fabsf(q);
+                const float q = __ldg(c.q() + a), aq = fabsf(q);
                 const float we = q * curl_slope(trilinear(M, M.data + M.e_slot * plane, cell, frac), v_inter);
                 const float wd = aq * curl_slope(trilinear(M, M.data + M.d_slot * plane, cell, frac), v_inter);
 #pragma unroll
@@ -1712,7 +1877,7 @@ __global__ void __launch_bounds__(128) adjoint_kernel(
             }
         }
         for (int k = c.lane; k < c.n_pairs; k += 32) {
-            const uint32_t pr = __ldg(c.pairs + k);
+            const uint32_t pr = __ldg(c.pairs() + k);
             if (pr == kPairPad) continue;
             const int a = pr & 0xFF, b = (pr >> 8) & 0xFF, tp = pr >> 16;
             const float4 pa = xyz[a], pb = xyz[b];
@@ -1725,7 +1890,7 @@ __global__ void __launch_bounds__(128) adjoint_kernel(
             float4 row = __ldg(Tb.smooth4 + (size_t)tp * Tb.n_bins + i1);
             float2 cf = make_float2(0.f, 0.f);
             if constexpr (kAD4) {
-                cf = __ldg(c.coef + k);
+                cf = __ldg(c.coef() + k);
                 const float4 te = __ldg(Tb.smooth4 + (size_t)kAd4RowE * Tb.n_bins + i1);
                 const float4 tg = __ldg(Tb.smooth4 + (size_t)kAd4RowG * Tb.n_bins + i1);
                 row.x += cf.x * te.x + cf.y * tg.x;
@@ -1773,6 +1938,16 @@ __global__ void combine_terms_kernel(const float4* __restrict__ in, long long bl
     }
 }
 
+// The x-pair copy of the maps: out[i] = (maps[i], maps[i + 1]) with x + 1
+// clamped to the last point of the row (never read there: trilinear cells
+// start at x <= nx - 2).
+__global__ void map_xpairs_kernel(const float* __restrict__ maps, int nx, size_t n, float2* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % (size_t)nx);
+        out[i] = make_float2(maps[i], maps[x + 1 < nx ? i + 1 : i]);
+    }
+}
+
 // FP32 issue-rate probe: independent FMA chains, used to report the FP32
 // roofline denominator measured on the running GPU.
 __global__ void fp32_peak_kernel(float* out, int iters) {
@@ -1788,6 +1963,29 @@ __global__ void fp32_peak_kernel(float* out, int iters) {
     }
     float r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
     if (r == 123.456f) out[0] = r;
+}
+
+// L2 read-bandwidth probe: every thread streams float4 words of an
+// L2-resident buffer with L2-only loads (ld.global.cg: no L1 allocation, so
+// each word is fetched from L2 every time), `reps` passes over the buffer,
+// each pass starting at another offset so that no thread re-reads its own
+// words back to back.  Used to report the L2 roofline denominator measured on
+// the running GPU.
+__global__ void __launch_bounds__(256) l2_read_kernel(const float4* __restrict__ buf, unsigned n4, int reps,
+                                                      float* out) {
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    const unsigned stride = gridDim.x * blockDim.x;
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int r = 0; r < reps; ++r) {
+        const unsigned shift = (unsigned)r * 7919u * 256u;
+        for (unsigned i = t; i < n4; i += stride) {
+            unsigned j = i + shift;
+            j = j >= n4 ? j % n4 : j;
+            const float4 v = __ldcg(buf + j);
+            acc.x += v.x; acc.y += v.y; acc.z += v.z; acc.w += v.w;
+        }
+    }
+    if (acc.x + acc.y + acc.z + acc.w == 123.456f) out[0] = acc.x;
 }
 
 // Grid maps.  Block = 8x4x4 grid points; receptor atoms within reach of the
@@ -2028,6 +2226,7 @@ __global__ void __launch_bounds__(kMapThreads) maps_ad4_kernel(
 static dev::Maps to_maps(const DeviceMapsView& m) {
     dev::Maps M;
     M.data = m.data;
+    M.xp = m.xpairs;
     M.nx = m.desc.dims[0];
     M.ny = m.desc.dims[1];
     M.nz = m.desc.dims[2];
@@ -2109,6 +2308,17 @@ cudaError_t launch_maps_ad4(const float* rec_xyzq, const int* rec_ad, int n_rec,
     dev::maps_ad4_kernel<<<grid, block, 0, stream>>>(reinterpret_cast<const float4*>(rec_xyzq), rec_ad, n_rec, params,
                                                      spec, d.dims[0], d.dims[1], d.dims[2], d.init[0], d.init[1],
                                                      d.init[2], d.factor_inv[0], d.factor_inv[1], d.factor_inv[2], out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_map_xpairs(const float* maps, const MapsDesc& d, float2* out, cudaStream_t stream) {
+    const size_t n = (size_t)d.dims[0] * d.dims[1] * d.dims[2] * (size_t)d.n_maps;
+    if (n == 0) return cudaSuccess;
+    int dev_id = 0, n_sm = 148;
+    cudaGetDevice(&dev_id);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev_id);
+    const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)n_sm * 8);
+    dev::map_xpairs_kernel<<<blocks, 256, 0, stream>>>(maps, d.dims[0], n, out);
     return cudaGetLastError();
 }
 
@@ -2222,6 +2432,32 @@ cudaError_t launch_search(const DeviceBatchView& b, const DeviceMapsView& m,
     return cudaGetLastError();
 }
 
+cudaError_t launch_search_stream(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
+                                 const SearchParams& P, const StreamView& sv, float* poses, int pose_stride,
+                                 ChainResult* results, int blocks, cudaStream_t stream) {
+    dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
+    if (P.chains_per_block < 1 || P.chains_per_block > 4 || blocks < 1) return cudaErrorInvalidValue;
+    const int warps = P.chains_per_block;
+    size_t smem = (size_t)warps * L.total * sizeof(float);
+    const auto kern = b.ad4 ? dev::stream_kernel<true> : dev::stream_kernel<false>;
+    cudaError_t e = smem_attr((const void*)kern, smem);
+    if (e != cudaSuccess) return e;
+    kern<<<blocks, warps * 32, smem, stream>>>(to_batch(b), to_maps(m), to_tables(t), P, L, sv, poses, pose_stride,
+                                               results);
+    return cudaGetLastError();
+}
+
+// CTAs of the streaming kernel resident per SM at this layout and CTA size.
+int stream_blocks_per_sm(const DeviceBatchView& b, int warps) {
+    dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
+    size_t smem = (size_t)warps * L.total * sizeof(float);
+    const auto kern = b.ad4 ? dev::stream_kernel<true> : dev::stream_kernel<false>;
+    smem_attr((const void*)kern, smem);
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, warps * 32, smem) != cudaSuccess) return 1;
+    return nb > 0 ? nb : 1;
+}
+
 cudaError_t launch_optimize(const DeviceBatchView& b, const DeviceMapsView& m,
                             const DeviceTablesView& t, const int* pose_lig, float* poses,
                             int pose_stride, int n_poses, int max_steps, float v, float* e_out,
@@ -2329,6 +2565,47 @@ float measure_fp32_peak_tflops() {
     return best;
 }
 
+// Measured L2 read bandwidth (GB/s) of the current device: a 32 MB buffer
+// (a quarter of the 126 MB L2) written once, then read 64 times over per
+// launch by 8 CTAs of 256 threads per SM; best of 5 launches timed with CUDA
+// events.
+float measure_l2_read_gbs() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t bytes = 32u << 20;
+    const unsigned n4 = (unsigned)(bytes / sizeof(float4));
+    float4* buf = nullptr;
+    float* out = nullptr;
+    if (cudaMalloc(&buf, bytes) != cudaSuccess) return 0;
+    if (cudaMalloc(&out, sizeof(float)) != cudaSuccess) {
+        cudaFree(buf);
+        return 0;
+    }
+    cudaMemset(buf, 0, bytes);
+    const int blocks = sms * 8, threads = 256, reps = 64;
+    dev::l2_read_kernel<<<blocks, threads>>>(buf, n4, 2, out);
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float best = 0;
+    for (int rep = 0; rep < 5; ++rep) {
+        cudaEventRecord(a);
+        dev::l2_read_kernel<<<blocks, threads>>>(buf, n4, reps, out);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        if (ms > 0) best = std::max(best, (float)((double)bytes * reps / (ms * 1e-3) / 1e9));
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    const bool ok = cudaGetLastError() == cudaSuccess;
+    cudaFree(out);
+    cudaFree(buf);
+    return ok ? best : 0.0f;
+}
+
 int search_blocks_per_sm(const DeviceBatchView& b, int warps, int lanes_per_chain) {
     dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
     const int lanes = lanes_per_chain == 16 ? 16 : 32;
@@ -2345,14 +2622,13 @@ int search_blocks_per_sm(const DeviceBatchView& b, int warps, int lanes_per_chai
 // Scratch of the persistent search for callers that cannot allocate device
 // memory when they search: a file-scope device array that every GPU loading
 // the library holds until the process exits.  Layout: the work-queue counter
-// (256 bytes), the ligand order (kNoAllocMaxLigands ints), then one
-// ChainResult per chain (kNoAllocMaxChains).  Every call shares it: the
-// counter is cleared and the order rewritten on each call, and calls that
-// overlap on the GPU race on it.
-constexpr size_t kNoAllocOrderOff = 256;
-constexpr size_t kNoAllocResultsOff =
-    kNoAllocOrderOff + ((kNoAllocMaxLigands * sizeof(int) + 255) / 256) * 256;
-constexpr size_t kNoAllocBytes = kNoAllocResultsOff + kNoAllocMaxChains * sizeof(ChainResult);
+// (256 bytes), then one ChainResult per chain (kNoAllocMaxChains).  Every
+// call shares it: the counter is cleared on each call, and calls that overlap
+// on the GPU race on it.
+constexpr size_t kNoAllocResultsOff = 256;
+constexpr size_t kNoAllocBytes = kNoAllocResultsOff + (size_t)kNoAllocMaxChains * sizeof(ChainResult);
+// the size the header and the design notes state (3,145,984 bytes, about 3.1 MB)
+static_assert(kNoAllocBytes == 3145984, "documented scratch size");
 static __device__ __align__(256) unsigned char g_search_scratch[kNoAllocBytes];
 
 namespace dev {
@@ -2366,41 +2642,42 @@ __global__ void chain_results_out(const ChainResult* r, int n, float* e, int* ev
 
 // Device address of g_search_scratch on the current device, looked up once per
 // device (host code only holds a stand-in for the array, not its address).
+// Threads racing on a device's first lookup store the same address.
 static cudaError_t noalloc_scratch(unsigned char** out) {
     constexpr int kMaxDevices = 64;
-    static unsigned char* addr[kMaxDevices] = {};
+    static std::atomic<unsigned char*> addr[kMaxDevices];
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    if (!addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_search_scratch);
+    unsigned char* p = addr[dev].load(std::memory_order_acquire);
+    if (!p) {
+        void* q = nullptr;
+        e = cudaGetSymbolAddress(&q, g_search_scratch);
         if (e != cudaSuccess) return e;
-        addr[dev] = static_cast<unsigned char*>(p);
+        p = static_cast<unsigned char*>(q);
+        addr[dev].store(p, std::memory_order_release);
     }
-    *out = addr[dev];
+    *out = p;
     return cudaSuccess;
 }
 
 cudaError_t launch_search_noalloc(const DeviceBatchView& b, const DeviceMapsView& m,
                                   const DeviceTablesView& t, const SearchParams& P,
-                                  const int* h_order, int n_ligands, int grid_blocks, float* poses,
+                                  const int* d_order, int n_ligands, int grid_blocks, float* poses,
                                   int pose_stride, float* e_out, int* evals_out, cudaStream_t stream) {
+    if ((long long)n_ligands * P.exhaustiveness > kNoAllocMaxChains) return cudaErrorInvalidValue;
     unsigned char* base = nullptr;
     cudaError_t e = noalloc_scratch(&base);
     if (e != cudaSuccess) return e;
     unsigned int* queue = reinterpret_cast<unsigned int*>(base);
-    int* order = reinterpret_cast<int*>(base + kNoAllocOrderOff);
     ChainResult* results = reinterpret_cast<ChainResult*>(base + kNoAllocResultsOff);
     const int n_items = n_ligands * P.exhaustiveness;
     e = cudaMemsetAsync(queue, 0, sizeof(unsigned int), stream);
     if (e != cudaSuccess) return e;
-    e = cudaMemcpyAsync(order, h_order, (size_t)n_ligands * sizeof(int), cudaMemcpyHostToDevice, stream);
-    if (e != cudaSuccess) return e;
     SearchParams sp = P;
     sp.persistent = 1;
-    e = launch_search(b, m, t, sp, order, n_items, 0, queue, poses, pose_stride, results, grid_blocks, stream);
+    e = launch_search(b, m, t, sp, d_order, n_items, 0, queue, poses, pose_stride, results, grid_blocks, stream);
     if (e != cudaSuccess) return e;
     dev::chain_results_out<<<(n_items + 255) / 256, 256, 0, stream>>>(results, n_items, e_out, evals_out);
     return cudaGetLastError();

@@ -46,6 +46,7 @@ struct LigDesc {
     int grid_off, n_grid;  // atoms with a grid map: list of atom | slot << 8
     int pad;
 };
+static_assert(sizeof(LigDesc) == 48, "LigDesc layout");
 
 struct NodeRec {            // 40 bytes
     float rel_origin[3];
@@ -61,10 +62,7 @@ struct NodeRec {            // 40 bytes
 constexpr uint32_t kPairPad = 0xFFFF0000u;
 // A 32-slot pair group is kPairPasses lane ranges of 32 / kPairPasses slots,
 // each a matching (no atom twice), whose forces are added one range at a time.
-#ifndef UD_PAIR_PASSES
-#define UD_PAIR_PASSES 4
-#endif
-constexpr int kPairPasses = UD_PAIR_PASSES;
+constexpr int kPairPasses = 4;
 constexpr int kPairPassWidth = 32 / kPairPasses;
 
 // Atom record: local xyz and packed fields (node | (map slot + 1) << 8 |
@@ -88,6 +86,33 @@ struct SearchParams {
     int bfgs_cap;          // 0: per-ligand local_steps; >0: min(local_steps, cap)
 };
 
+// Control of a streaming screen (ud_stream_*): one persistent search over an
+// append-only device arena that the host fills slot by slot.  Slot s holds up
+// to slot_ligands ligands with global ids s * slot_ligands + local index; its
+// chains are the items [s * slot_ligands * E, (s + 1) * slot_ligands * E) of
+// the work counter.  The host copies a slot's topology, order, ligand count
+// and chain count into device memory, then the new published count (the
+// copies are ordered on one stream); a warp whose item lies in an unpublished
+// slot waits, with a time limit, for the count to pass it.  Chain results go
+// to a ring of `ring` result areas (slot s to area s % ring; the host reuses an
+// area only after it has taken the results out), and the warp finishing a
+// slot's last chain sets done_host[s] in host-mapped memory.
+struct StreamView {
+    const unsigned int* published;   // slots whose data is in device memory
+    const unsigned int* closed;      // 1 once the host publishes nothing more
+    unsigned int* next_item;         // work counter
+    unsigned int* slot_left;         // per slot: chains not finished yet
+    const int* slot_nlig;            // per slot: ligands
+    const int* order;                // per slot, slot_ligands entries: global ligand ids, costliest first
+    unsigned int* done_host;         // host-mapped, per slot: 1 when all its chains are finished
+    int* status;                     // 0, or kStreamTimeout when a wait ran out
+    int slot_ligands;
+    int max_slots;
+    int ring;
+    unsigned long long timeout_ns;   // longest wait for a publication
+};
+constexpr int kStreamTimeout = 1;
+
 // AutoDock 4.2 atom-kind parameters indexed by AD type (atom_constants.h
 // ad_type_property) and the set of maps an AD4 map build computes.
 constexpr int kAdTypes = 35;
@@ -101,8 +126,8 @@ struct Ad4MapSpec {
     float w_vdw, w_hb, w_elec, w_dsolv;
 };
 
-// Capacity of the allocation-free search (ud_search_device_noalloc).
-constexpr int kNoAllocMaxLigands = 8192;
+// Capacity of the allocation-free search (ud_search_device_noalloc): chains
+// (ligands x exhaustiveness) per call.
 constexpr int kNoAllocMaxChains = 131072;
 
 // Result record of one chain.
@@ -133,6 +158,7 @@ struct DeviceBatchView {
 struct DeviceMapsView {
     const float* data;
     MapsDesc desc;
+    const float2* xpairs;  // [slot][z][y][x] = (data at x, data at x + 1; x + 1 clamped to the last point)
 };
 
 struct DeviceTablesView {
@@ -222,9 +248,23 @@ int search_blocks_per_sm(const DeviceBatchView& b, int warps, int lanes_per_chai
 cudaError_t launch_optimize(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
                             const int* pose_lig, float* poses, int pose_stride, int n_poses, int max_steps,
                             float v, float* e_out, int* evals_out, cudaStream_t stream);
+// The x-pair copy of the maps (DeviceMapsView::xpairs) from `maps`.
+cudaError_t launch_map_xpairs(const float* maps, const MapsDesc& d, float2* out, cudaStream_t stream);
 float measure_fp32_peak_tflops();
+float measure_l2_read_gbs();
+// The persistent search over the batch's device-resident work order `d_order`
+// with the library's static scratch (queue counter, per-chain records) in
+// place of device allocations; per-chain energies / evaluations written to
+// the caller's device buffers.
+// The persistent search of a streaming screen (StreamView) on `blocks` CTAs:
+// the batch view is the arena (LigDesc offsets absolute), the poses and
+// results are the ring of result areas.
+cudaError_t launch_search_stream(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
+                                 const SearchParams& P, const StreamView& sv, float* poses, int pose_stride,
+                                 ChainResult* results, int blocks, cudaStream_t stream);
+int stream_blocks_per_sm(const DeviceBatchView& b, int warps);
 cudaError_t launch_search_noalloc(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
-                                  const SearchParams& P, const int* h_order, int n_ligands, int grid_blocks,
+                                  const SearchParams& P, const int* d_order, int n_ligands, int grid_blocks,
                                   float* poses, int pose_stride, float* e_out, int* evals_out,
                                   cudaStream_t stream);
 int engine_chain_smem_bytes(int max_atoms, int max_torsions);

@@ -20,7 +20,7 @@ LIB_PATH = Path(os.environ.get("UNIDOCK_B200_LIB", PKG_ROOT / "lib" / "libunidoc
 SF_VINA, SF_AD4, SF_VINARDO = 0, 1, 2
 UD_OK = 0
 UD_ADJOINT_EXACT = 1
-UD_ERR_ARG, UD_ERR_PARSE, UD_ERR_CUDA, UD_ERR_CAPACITY, UD_ERR_STATE = 1, 2, 3, 4, 5
+UD_ERR_ARG, UD_ERR_PARSE, UD_ERR_CUDA, UD_ERR_CAPACITY, UD_ERR_STATE, UD_ERR_TIMEOUT = 1, 2, 3, 4, 5, 6
 
 _lib = None
 
@@ -32,6 +32,11 @@ class TuneResult(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class StreamConfig(C.Structure):
+    _fields_ = [("slot_ligands", C.c_int), ("max_slots", C.c_int), ("ring", C.c_int), ("max_atoms", C.c_int),
+                ("max_torsions", C.c_int), ("timeout_ms", C.c_int)]
 
 
 class UdError(RuntimeError):
@@ -104,12 +109,25 @@ def lib():
         "ud_search_collect": ([vp, vp], C.c_int),
         "ud_search_chains": ([vp, fp, C.c_int, fp, ip], C.c_int),
         "ud_search_device_noalloc": ([vp, C.POINTER(SearchParams), vp, C.c_int, vp, vp, vp], C.c_int),
+        "ud_stream_create": ([vp, C.POINTER(SearchParams), C.POINTER(StreamConfig), C.POINTER(vp)], C.c_int),
+        "ud_stream_push": ([vp, C.POINTER(vp), C.c_int, C.POINTER(C.c_int)], C.c_int),
+        "ud_stream_close": ([vp], C.c_int),
+        "ud_stream_collect": ([vp, C.c_int], C.c_int),
+        "ud_stream_result_count": ([vp, C.c_int, C.c_int, C.POINTER(C.c_int)], C.c_int),
+        "ud_stream_result_mode": ([vp, C.c_int, C.c_int, C.c_int, fp, fp], C.c_int),
+        "ud_stream_result_write": ([vp, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_size_t,
+                                    C.POINTER(C.c_size_t)], C.c_int),
+        "ud_stream_chains": ([vp, C.c_int, fp, C.c_int, fp, ip], C.c_int),
+        "ud_stream_finish": ([vp, C.POINTER(C.c_longlong)], C.c_int),
+        "ud_stream_destroy": ([vp], C.c_int),
         "ud_result_count": ([vp, C.c_int, ip], C.c_int),
         "ud_result_mode": ([vp, C.c_int, C.c_int, fp, fp], C.c_int),
         "ud_result_write": ([vp, C.c_int, C.c_int, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
         "ud_search_stats": ([vp, C.POINTER(C.c_longlong), fp], C.c_int),
+        "ud_batch_upload_bytes": ([vp, C.POINTER(C.c_size_t)], C.c_int),
         "ud_optimize": ([vp, ip, fp, C.c_int, C.c_int, C.c_int, C.c_float, fp, ip, vp], C.c_int),
         "ud_device_fp32_peak": ([fp], C.c_int),
+        "ud_device_l2_peak": ([fp], C.c_int),
         "ud_maps_term_count": ([vp, ip], C.c_int),
         "ud_batch_device_bytes": ([C.POINTER(vp), C.c_int, C.c_int, C.POINTER(SearchParams),
                                    C.POINTER(C.c_size_t)], C.c_int),
@@ -201,6 +219,13 @@ def _i(a):
 def fp32_peak_tflops() -> float:
     v = C.c_float()
     _check(lib().ud_device_fp32_peak(C.byref(v)))
+    return float(v.value)
+
+
+def l2_peak_gbs() -> float:
+    """Measured L2 read bandwidth of the current device in GB/s (ud_device_l2_peak)."""
+    v = C.c_float()
+    _check(lib().ud_device_l2_peak(C.byref(v)))
     return float(v.value)
 
 
@@ -509,13 +534,15 @@ class Batch:
         self.exhaustiveness = exhaustiveness
 
     def search_device_noalloc(self, d_poses, pose_stride, d_energies, d_evals=None, stream=None, exhaustiveness=8,
-                              max_step=0, seed=0, bfgs_cap=0):
+                              max_step=0, seed=0, bfgs_cap=0, chains_per_block=0, lanes_per_chain=0):
         """Batched search into caller-owned device buffers (raw device
         addresses as ints), using the library's static scratch instead of
         device allocations; asynchronous on `stream` (a raw cudaStream_t or
-        None for the legacy default stream).  Returns per-chain results only:
-        no clustering, and the batch's own result state is left untouched."""
-        p = SearchParams(exhaustiveness, max_step, 9, 1.0, 3.0, seed, 1, 0, bfgs_cap, 0)
+        None for the legacy default stream).  Launch shape and BFGS cap as in
+        search().  Returns per-chain results only: no clustering, and the
+        batch's own result state is left untouched."""
+        p = SearchParams(exhaustiveness, max_step, 9, 1.0, 3.0, seed, 1, chains_per_block, bfgs_cap, 0, 0,
+                         lanes_per_chain)
         _check(lib().ud_search_device_noalloc(self.h, C.byref(p), C.c_void_p(d_poses), int(pose_stride),
                                               C.c_void_p(d_energies), C.c_void_p(d_evals) if d_evals else None,
                                               C.c_void_p(stream) if stream else None))
@@ -578,6 +605,12 @@ class Batch:
         _check(lib().ud_result_write(self.h, lig, fmt, buf, ln.value + 1, C.byref(ln)))
         return buf.value.decode()
 
+    def upload_bytes(self):
+        """Host-to-device bytes of the last topology upload (ud_batch_upload_bytes)."""
+        n = C.c_size_t()
+        _check(lib().ud_batch_upload_bytes(self.h, C.byref(n)))
+        return int(n.value)
+
     def stats(self):
         ev = C.c_longlong()
         ms = C.c_float()
@@ -587,4 +620,76 @@ class Batch:
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:
             _lib.ud_batch_destroy(self.h)
+            self.h = None
+
+
+class Stream:
+    """Streaming screen (ud_stream_*): one persistent search kernel, launched
+    at creation, fed slot by slot with push(); collect(slot) waits for a
+    slot's chains and finishes its modes.  Slot s may be pushed once slot
+    s - ring was collected."""
+
+    def __init__(self, maps: Maps, exhaustiveness=8, max_step=20, num_modes=9, min_rmsd=1.0, energy_range=3.0,
+                 seed=0, refine_step=0, bfgs_cap=0, chains_per_block=0, slot_ligands=64, max_slots=64, ring=2,
+                 max_atoms=64, max_torsions=16, timeout_ms=0):
+        self.maps = maps
+        self.exhaustiveness = exhaustiveness
+        self.max_torsions = max_torsions
+        self._p = SearchParams(exhaustiveness, max_step, num_modes, min_rmsd, energy_range, seed, 1,
+                               chains_per_block, bfgs_cap, 0, refine_step, 0)
+        cfg = StreamConfig(slot_ligands, max_slots, ring, max_atoms, max_torsions, timeout_ms)
+        h = C.c_void_p()
+        _check(lib().ud_stream_create(maps.h, C.byref(self._p), C.byref(cfg), C.byref(h)))
+        self.h = h
+        self.slots = {}
+
+    def push(self, ligands):
+        ligands = list(ligands)
+        arr = (C.c_void_p * len(ligands))(*[l.h.value for l in ligands])
+        k = C.c_int()
+        _check(lib().ud_stream_push(self.h, arr, len(ligands), C.byref(k)))
+        self.slots[k.value] = ligands
+        return k.value
+
+    def close(self):
+        _check(lib().ud_stream_close(self.h))
+
+    def collect(self, slot):
+        _check(lib().ud_stream_collect(self.h, int(slot)))
+
+    def chains(self, slot):
+        n = len(self.slots[slot]) * self.exhaustiveness
+        stride = 7 + self.max_torsions
+        poses = np.zeros((n, stride), np.float32)
+        e = np.zeros(n, np.float32)
+        ev = np.zeros(n, np.int32)
+        _check(lib().ud_stream_chains(self.h, int(slot), _f(poses), stride, _f(e), _i(ev)))
+        return poses, e, ev
+
+    def modes(self, slot, lig):
+        n = C.c_int()
+        _check(lib().ud_stream_result_count(self.h, int(slot), int(lig), C.byref(n)))
+        out = []
+        for k in range(n.value):
+            pose = np.zeros(7 + self.slots[slot][lig].n_torsions, np.float32)
+            en = np.zeros(8, np.float32)
+            _check(lib().ud_stream_result_mode(self.h, int(slot), int(lig), k, _f(pose), _f(en)))
+            out.append((pose, en))
+        return out
+
+    def write(self, slot, lig, fmt=0):
+        ln = C.c_size_t()
+        _check(lib().ud_stream_result_write(self.h, int(slot), int(lig), fmt, None, 0, C.byref(ln)))
+        buf = C.create_string_buffer(ln.value + 1)
+        _check(lib().ud_stream_result_write(self.h, int(slot), int(lig), fmt, buf, ln.value + 1, C.byref(ln)))
+        return buf.value.decode()
+
+    def finish(self):
+        ev = C.c_longlong()
+        _check(lib().ud_stream_finish(self.h, C.byref(ev)))
+        return ev.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().ud_stream_destroy(self.h)
             self.h = None
