@@ -628,30 +628,94 @@ def run_stream(args):
 
 # ------------------------------------------------------------------ reference CPU path
 def reference_cpu(sample, step_index, threads=None, seed=7):
-    """Reference CPU Vina search (oracle/_ref, the reference's own sources) on
-    `sample` ligands at the same exhaustiveness / max_step; returns ligands/s."""
+    """The reference's CPU docking at the screen's settings on `sample` ligands
+    of the same generator, all the reference's own code (oracle/_ref, built
+    from its sources): its parallel Monte-Carlo search (parallel_mc over
+    monte_carlo::operator(), the machinery of Vina::global_search,
+    vina.cpp:1495-1540) with the step count capped at max_step as its GPU path
+    caps it, then the refinement of every mode against the receptor atoms and
+    the final scores (vina.h:232-343), on all host threads.  The maps are built
+    once outside the timing, as a screen builds them once per receptor.
+    Returns ligands/s and the threads used."""
     sys.path.insert(0, str(ROOT))
     from oracle import ref
     from unidock_tools import synth
-    if not ref.available():
-        raise RuntimeError("oracle/_ref/libudref.so missing (build it with make -C oracle)")
+    if not ref.gpu_available():
+        raise RuntimeError("oracle/_ref/libudref_gpu.so missing (build it with make -C oracle)")
     threads = threads or os.cpu_count()
     rec = synth.make_receptor(3000, seed=1)
     maps = ref.RefMaps(rec.xyz, rec.xs, np.zeros(3, np.float32), np.full(3, BOX, np.float32), SPACING)
     ligs = synth.ligand_set(sample * (step_index + 1), seed=20261203, heavy=(12, 48), torsions=(0, 10))
     ligs = ligs[sample * step_index:]
+    maxf = float(np.finfo(np.float32).max)
     t_total = 0.0
     with tempfile.TemporaryDirectory() as d:
         for k, L in enumerate(ligs):
             p = Path(d) / f"l{k}.pdbqt"
             p.write_text(L.to_pdbqt())
             R = ref.RefLigand(p)
-            heur = R.n_atoms + 10 * (6 + R.n_torsions)
-            gsteps = min(70 * 3 * (50 + heur) // 2, MAX_STEP)
             t0 = time.perf_counter()
-            R.mc(maps, seed, EXHAUSTIVENESS, gsteps, None, threads)
+            _, poses = ref.parallel_mc(R, maps, EXHAUSTIVENESS, MAX_STEP, seed + k, threads)
+            refined, order_e = [], []
+            for pose in poses:
+                rp, e_last, _, _, within = R.refine(maps, pose, 3)
+                refined.append(rp)
+                order_e.append(e_last if within else maxf)
+            R.final_scores(maps, np.array(refined, np.float32), order_e, receptor=True)
             t_total += time.perf_counter() - t0
     return len(ligs) / t_total, threads
+
+
+CONFIG0 = "plain single docking (configs[0]): Vina, 3000-atom receptor, 22.5 A box at 0.375 A, one ligand of 24 " \
+          "heavy atoms and 6 torsions, exhaustiveness 8, num_modes 9, heuristic step count, refinement 3 steps"
+
+
+def config0_files(d):
+    from unidock_tools import synth
+    rp, lp = Path(d) / "rec.pdbqt", Path(d) / "lig.pdbqt"
+    rp.write_text(synth.make_receptor(3000, seed=1).to_pdbqt())
+    lp.write_text(synth.make_ligand(24, 6, seed=31).to_pdbqt())
+    return rp, lp
+
+
+def config0_reference(threads=None):
+    """configs[0] through the reference's stock CPU docking of one ligand
+    (Vina::set_receptor .. global_search, the reference CLI's --cpu path):
+    wall clock of the whole call and the best mode's energy."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import ref
+    threads = threads or os.cpu_count()
+    with tempfile.TemporaryDirectory() as d:
+        rp, lp = config0_files(d)
+        t0 = time.perf_counter()
+        e = ref.vina_dock(rp, lp, np.zeros(3), np.full(3, BOX), SPACING, 8, 9, 5, threads)
+        t = time.perf_counter() - t0
+    return {"workload": CONFIG0, "path": "reference CPU Vina::global_search (stock CPU path, whole call)",
+            "seconds": round(t, 3), "cores": threads, "best_energy": round(float(e[0]), 3)}
+
+
+def config0_engine():
+    """configs[0] through this engine's C ABI, one ligand: receptor parse, map
+    build, ligand parse, search (exhaustiveness 8, the heuristic step count),
+    clustering, refinement and final scores, output text; wall clock."""
+    import torch
+    from unidock_tools import engine
+    with tempfile.TemporaryDirectory() as d:
+        rp, lp = config0_files(d)
+        for rep in range(2):  # the first call pays module loading and allocation
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            xyz, xs = engine.parse_receptor(rp.read_text())
+            maps = engine.Maps(xyz, xs, np.zeros(3, np.float32), np.full(3, BOX, np.float32), SPACING)
+            L = engine.Ligand(lp.read_text())
+            B = engine.Batch(maps, [L])
+            B.search(exhaustiveness=8, max_step=0, num_modes=9, seed=5, refine_step=3)
+            text = B.write(0)
+            torch.cuda.synchronize()
+            t = time.perf_counter() - t0
+    return {"workload": CONFIG0, "path": "this engine's C ABI: parse, maps, search, clustering, refinement, output",
+            "seconds": round(t, 3), "best_energy": round(float(B.modes(0)[0][1][0]), 3),
+            "output_bytes": len(text)}
 
 
 def run_reference(args, rank, world):
@@ -665,6 +729,10 @@ def run_reference(args, rank, world):
         v, thr = reference_cpu(sample, args.warmup + s)
         vals.append(v)
     value = len(vals) * sample / sum(sample / v for v in vals)
+    try:
+        c0 = config0_reference()
+    except Exception as ex:  # the configs[0] leg never blocks the line
+        c0 = {"workload": CONFIG0, "unavailable": str(ex)}
     return {
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "ligands/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * sample / value, 1),
@@ -674,9 +742,11 @@ def run_reference(args, rank, world):
                                "4096 ligands U{12..48} heavy / U{0..10} torsions, 3000-atom receptor, 22.5 A box",
                    "sample_ligands_per_step": sample},
         "cpu_baseline": {"value": round(value, 4), "unit": "ligands/s", "cores": thr, "kind": "reference",
-                         "sample": f"{sample} ligands per step x {args.steps} steps, 128 chains x 20 MC steps each, "
-                                   "reference CPU Vina search (unidock/src/lib compiled by oracle/Makefile)"},
+                         "sample": f"{sample} ligands per step x {args.steps} steps: the reference's parallel_mc "
+                                   "(128 tasks of monte_carlo::operator(), 20 MC steps each) then refinement and "
+                                   "final scores of every mode, the reference's own sources built by oracle/Makefile"},
         "e2e": {"value": round(value, 4), "unit": "ligands/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "configs0": c0,
     }
 
 
@@ -748,11 +818,17 @@ def main():
             try:
                 v, thr = reference_cpu(args.cpu_sample, 0)
                 res["cpu_baseline"] = {"value": round(v, 4), "unit": "ligands/s", "cores": thr, "kind": "reference",
-                                       "sample": f"{args.cpu_sample} ligands, 128 chains x 20 MC steps, reference "
-                                                 "CPU Vina search on all host threads"}
+                                       "sample": f"{args.cpu_sample} ligands: the reference's parallel_mc (128 "
+                                                 "tasks, 20 MC steps each), refinement and final scores of every "
+                                                 "mode, on all host threads"}
             except Exception as ex:  # the baseline never blocks the GPU line
                 res["cpu_baseline"] = {"value": None, "unit": "ligands/s", "cores": os.cpu_count(),
                                        "kind": "reference", "sample": f"unavailable: {ex}"}
+    if res is not None and args.impl != "reference" and world == 1 and not args.no_cpu_baseline:
+        try:
+            res["configs0"] = {"engine": config0_engine(), "reference": config0_reference()}
+        except Exception as ex:
+            res["configs0"] = {"workload": CONFIG0, "unavailable": str(ex)}
     if res is not None:
         print(json.dumps(res), flush=True)
 

@@ -423,7 +423,7 @@ typedef struct {
                            only after slot s - ring was collected */
     int max_atoms;      /* largest ligand the stream takes (shared memory per chain is sized by it) */
     int max_torsions;
-    int timeout_ms;     /* longest wait of the kernel for the next slot (0 = 60000) */
+    int timeout_ms;     /* longest time the kernel waits with no new slot published (0 = 60000) */
 } ud_stream_config;
 
 /* Create the stream and launch its kernel.  params: exhaustiveness, max_step

@@ -35,8 +35,40 @@ def gpu_lib():
         L.udref_gpu_dock.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int, C.c_ulonglong,
                                      C.POINTER(C.c_float), C.POINTER(C.c_double)]
         L.udref_gpu_last_error.restype = C.c_char_p
+        L.udref_vina_dock.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float,
+                                      C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double), C.c_int]
+        L.udref_parallel_mc.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_uint, C.c_int, C.c_int,
+                                        C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int]
         _gpu_lib = L
     return _gpu_lib
+
+
+def vina_dock(receptor_path, ligand_path, center, size, spacing=0.375, exhaustiveness=8, n_poses=9, seed=0,
+              threads=None):
+    """The reference CLI's CPU docking of one ligand (Vina::set_receptor, set_ligand_from_file,
+    compute_vina_maps, global_search; the reference's own code): energies of the modes."""
+    c = np.ascontiguousarray(center, np.float32)
+    s = np.ascontiguousarray(size, np.float32)
+    e = np.zeros(n_poses, np.float64)
+    n = gpu_lib().udref_vina_dock(str(receptor_path).encode(), str(ligand_path).encode(), _f(c), _f(s), spacing,
+                                  exhaustiveness, n_poses, seed, threads or os.cpu_count(),
+                                  e.ctypes.data_as(C.POINTER(C.c_double)), n_poses)
+    if n < 0:
+        raise RuntimeError("reference CPU docking failed")
+    return e[:n]
+
+
+def parallel_mc(ligand, maps, exhaustiveness, global_steps, seed=0, threads=None, n_saved=9, min_rmsd=1.0):
+    """The reference's own parallel Monte-Carlo search (parallel_mc over monte_carlo::operator()) with the
+    step count set to global_steps: (mode energies, mode poses) of the merged output container."""
+    stride = 7 + ligand.n_torsions
+    e = np.zeros(n_saved, np.float32)
+    p = np.zeros((n_saved, stride), np.float32)
+    n = gpu_lib().udref_parallel_mc(ligand.h, maps.h, exhaustiveness, global_steps, seed, threads or os.cpu_count(),
+                                    n_saved, min_rmsd, _f(e), _f(p), stride)
+    if n < 0:
+        raise RuntimeError("reference parallel_mc failed")
+    return e[:n], p[:n]
 
 
 def gpu_bucket(ligand) -> int:

@@ -1,2 +1,2 @@
 #pragma once
-#include "_shim_common.hpp"
+#include "../_shim_common.hpp"

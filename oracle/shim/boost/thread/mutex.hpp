@@ -2,7 +2,7 @@
 #include "../_shim_common.hpp"
 #include <condition_variable>
 namespace boost {
-struct mutex : std::mutex { using scoped_lock = std::lock_guard<std::mutex>; };
+struct mutex : std::mutex { using scoped_lock = std::unique_lock<std::mutex>; };
 using condition = std::condition_variable_any;
 struct thread : std::thread {
     using std::thread::thread;

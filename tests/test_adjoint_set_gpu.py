@@ -101,13 +101,13 @@ def test_reference_mode_on_subsample_matches_reference(receptor, workload):
             er, gr, xyz = refs[li].eval_deriv(R, P[:7 + T], 1000.0, 1000.0)
             gr = gr.astype(np.float64)
             want = np.concatenate([gr[:3], quat_grad(gr[3:6], P[3:7].astype(np.float64)), gr[6:]])
-            d = abs(float(e[k]) - er)
-            e_err.append(d / max(1.0, abs(er)))
+            diff = abs(float(e[k]) - er)
+            e_err.append(diff / max(1.0, abs(er)))
             g_err.append(rel(g[k, :7 + T], want))
             if e_err[-1] > REL:  # conditioning of the out-of-box penalty (see the module docstring)
                 out = np.sum(np.any((xyz < w["center"] - BOX / 2) | (xyz > w["center"] + BOX / 2), axis=1))
                 ulp = float(np.spacing(np.float32(np.abs(xyz).max())))
-                assert out > 0 and d <= REL * max(1.0, abs(er)) + 4 * ulp * 1e6 * out, (k, li, float(e[k]), er, out)
+                assert out > 0 and diff <= REL * max(1.0, abs(er)) + 4 * ulp * 1e6 * out, (k, li, float(e[k]), er, out)
                 penalty_limited.append((k, li, float(e[k]), er, int(out)))
     print(f"reference mode, {len(e_err)} poses of {N_LIG} ligands: energy max {max(e_err):.3g} median "
           f"{np.median(e_err):.3g}; pose gradient max {max(g_err):.3g} median {np.median(g_err):.3g} (relative); "

@@ -2667,8 +2667,12 @@ extern "C" int ud_stream_create(ud_maps maps, const ud_search_params* params, co
         int dev = 0, n_sm = 148;
         cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
         cuda_check(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev), "device attribute");
+        // one full wave of blocks; those on every reserve_every-th SM return at
+        // once and leave their SM to the per-slot post-processing kernels
+        cuda_check(prepare_stream_post(st->view(), st->cap, st->refined), "stream post-processing kernels");
         const int per_sm = stream_blocks_per_sm(st->view(), sp.chains_per_block);
-        const int blocks = per_sm * std::max(1, n_sm - kStreamReserveSms);
+        const int blocks = per_sm * n_sm;
+        sv.reserve_every = n_sm >= 2 * kStreamReserveSms ? n_sm / kStreamReserveSms : 0;
         cuda_check(launch_search_stream(st->view(), maps_view(maps), tables_view(maps), sp, sv, st->d_poses.p,
                                         st->stride, st->d_results.p, blocks, st->ks),
                    "stream kernel");

@@ -203,10 +203,10 @@ constexpr int kPairBatch = UD_PAIR_BATCH;
 // reuse in L1, so with UD_NA_LOADS they do not allocate L1 lines
 // (ld.global.nc.L1::no_allocate), leaving L1 to the ligand topology.
 #ifndef UD_NA_LOADS
-#define UD_NA_LOADS 0
+#define UD_NA_LOADS 1
 #endif
 #ifndef UD_PAIR_PREFETCH
-#define UD_PAIR_PREFETCH 0
+#define UD_PAIR_PREFETCH 1
 #endif
 __device__ __forceinline__ float2 ld_stream2(const float2* p) {
 #if UD_NA_LOADS
@@ -1057,25 +1057,46 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
+// Loads of stream control words, which host copies write while the kernel
+// runs: volatile asm (never merged with an earlier load or hoisted out of a
+// wait loop) at GPU scope (read where the copies land, not from a line cached
+// in L1).  The acquire load of the published count orders the reads of the
+// slot's data after it.
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ int ld_relaxed_s32(const int* p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
 // The next (ligand, chain) item of a streaming screen for lane 0 of a chain
 // (StreamView): the item's global ligand id and chain, or -1 when the stream
 // is closed and drained, the arena is exhausted, or a wait for a publication
-// ran past the time limit (status set to kStreamTimeout).  Stream control
-// words are written by host copies while the kernel runs, so they are read
-// from L2 (ld.global.cg), never from a cached line.
+// ran past the time limit (status set to kStreamTimeout).
 __device__ __noinline__ int stream_fetch(const StreamView& SV, int E, int* item_out, int* chain_out) {
     const unsigned per_slot = (unsigned)SV.slot_ligands * (unsigned)E;
     for (;;) {
         const unsigned it = atomicAdd(SV.next_item, 1u);
         const unsigned s = it / per_slot;
         if (s >= (unsigned)SV.max_slots) return -1;
-        if (__ldcg(SV.published) <= s) {
-            const unsigned long long t0 = global_ns();
+        unsigned pub = ld_acquire_u32(SV.published);
+        if (pub <= s) {
+            // the limit runs from the last publication seen: a slot far ahead
+            // waits as long as the host keeps publishing earlier ones
+            unsigned long long t0 = global_ns();
             for (;;) {
-                if (__ldcg(SV.published) > s) break;
-                if (__ldcg(SV.closed)) {
-                    __threadfence();
-                    if (__ldcg(SV.published) > s) break;
+                const unsigned now = ld_acquire_u32(SV.published);
+                if (now > s) break;
+                if (now != pub) {
+                    pub = now;
+                    t0 = global_ns();
+                }
+                if (ld_acquire_u32(SV.closed)) {
+                    if (ld_acquire_u32(SV.published) > s) break;
                     return -1;
                 }
                 if (global_ns() - t0 > SV.timeout_ns) {
@@ -1085,13 +1106,12 @@ __device__ __noinline__ int stream_fetch(const StreamView& SV, int E, int* item_
                 __nanosleep(2000);
             }
         }
-        __threadfence();
         const unsigned within = it - s * per_slot;
         const int l = (int)(within / (unsigned)E);
-        if (l >= __ldcg(SV.slot_nlig + s)) continue;  // past the slot's ligands
+        if (l >= ld_relaxed_s32(SV.slot_nlig + s)) continue;  // past the slot's ligands
         *item_out = (int)it;
         *chain_out = (int)(within % (unsigned)E);
-        return __ldcg(SV.order + (size_t)s * SV.slot_ligands + l);
+        return ld_relaxed_s32(SV.order + (size_t)s * SV.slot_ligands + l);
     }
 }
 
@@ -1386,6 +1406,14 @@ __global__ void __launch_bounds__(128, kAD4 ? UD_SEARCH_MIN_BLOCKS_AD4 : UD_SEAR
     const __grid_constant__ Batch B, const __grid_constant__ Maps M, const __grid_constant__ Tables Tb,
     const __grid_constant__ SearchParams P, const __grid_constant__ Layout L, const __grid_constant__ StreamView SV,
     float* poses, int pose_stride, ChainResult* results) {
+    // The grid is one full wave (blocks per SM x SMs), so every SM starts
+    // with its share of blocks; those on the SMs left to the per-slot
+    // clustering and refinement kernels return at once.  (Fewer blocks would
+    // not do: the block scheduler spreads them over all SMs, and the leftover
+    // room on each may be too small for a post-processing CTA.)
+    unsigned smid;
+    asm("mov.u32 %0, %%smid;" : "=r"(smid));
+    if (SV.reserve_every > 0 && smid % (unsigned)SV.reserve_every == 0) return;
     extern __shared__ __align__(16) float smem[];
     float* sw = smem + (size_t)(threadIdx.x / 32) * L.total;
     run_machine<true, kAD4, 32, true>(B, M, Tb, P, L, sw, nullptr, 0, 0, nullptr, poses, pose_stride, results,
@@ -2505,6 +2533,19 @@ cudaError_t launch_cluster(const DeviceBatchView& b, const float* poses, int pos
     return cudaGetLastError();
 }
 
+cudaError_t prepare_stream_post(const DeviceBatchView& b, int cap, bool refine) {
+    const dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
+    const int warps = 4;
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, (const void*)dev::cluster_kernel);
+    if (e == cudaSuccess)
+        e = smem_attr((const void*)dev::cluster_kernel, (size_t)warps * (L.total + 4 * dev::pad4(cap)) * sizeof(float));
+    if (e != cudaSuccess || !refine) return e;
+    const void* fn = (const void*)dev::receptor_kernel<kRecRefine>;
+    e = cudaFuncGetAttributes(&fa, fn);
+    if (e == cudaSuccess) e = smem_attr(fn, (size_t)warps * L.total * sizeof(float));
+    return e;
+}
 cudaError_t launch_receptor(int mode, const DeviceBatchView& b, const DeviceTablesView& t,
                             const DeviceReceptorView& r, const int* pose_lig, float* poses, int pose_stride,
                             int n_poses, int refine_step, float slope, float v, float* e_out, float* g_out,

@@ -109,6 +109,7 @@ struct StreamView {
     int slot_ligands;
     int max_slots;
     int ring;
+    int reserve_every;               // blocks on SMs whose id is a multiple of this return at once (0: none)
     unsigned long long timeout_ns;   // longest wait for a publication
 };
 constexpr int kStreamTimeout = 1;
@@ -252,10 +253,6 @@ cudaError_t launch_optimize(const DeviceBatchView& b, const DeviceMapsView& m, c
 cudaError_t launch_map_xpairs(const float* maps, const MapsDesc& d, float2* out, cudaStream_t stream);
 float measure_fp32_peak_tflops();
 float measure_l2_read_gbs();
-// The persistent search over the batch's device-resident work order `d_order`
-// with the library's static scratch (queue counter, per-chain records) in
-// place of device allocations; per-chain energies / evaluations written to
-// the caller's device buffers.
 // The persistent search of a streaming screen (StreamView) on `blocks` CTAs:
 // the batch view is the arena (LigDesc offsets absolute), the poses and
 // results are the ring of result areas.
@@ -263,6 +260,16 @@ cudaError_t launch_search_stream(const DeviceBatchView& b, const DeviceMapsView&
                                  const SearchParams& P, const StreamView& sv, float* poses, int pose_stride,
                                  ChainResult* results, int blocks, cudaStream_t stream);
 int stream_blocks_per_sm(const DeviceBatchView& b, int warps);
+// Loads the per-slot clustering kernel (and the refinement kernel when
+// `refine`) into the context and raises their shared-memory limits to the
+// stream's largest layout (`b`), so that launching them while the persistent
+// stream kernel runs needs no module load (a lazy load waits for the kernels
+// running in the context, the persistent one included) and no attribute change.
+cudaError_t prepare_stream_post(const DeviceBatchView& b, int cap, bool refine);
+// The persistent search over the batch's device-resident work order `d_order`
+// with the library's static scratch (queue counter, per-chain records) in
+// place of device allocations; per-chain energies / evaluations written to
+// the caller's device buffers.
 cudaError_t launch_search_noalloc(const DeviceBatchView& b, const DeviceMapsView& m, const DeviceTablesView& t,
                                   const SearchParams& P, const int* d_order, int n_ligands, int grid_blocks,
                                   float* poses, int pose_stride, float* e_out, int* evals_out,
