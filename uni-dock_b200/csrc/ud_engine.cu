@@ -208,6 +208,11 @@ constexpr int kPairBatch = UD_PAIR_BATCH;
 #ifndef UD_PAIR_PREFETCH
 #define UD_PAIR_PREFETCH 1
 #endif
+// UD_FORCE_SPLIT: the pair forces of odd lane ranges go to a second force
+// array, so that two ranges add their forces at once (half the passes)
+#ifndef UD_FORCE_SPLIT
+#define UD_FORCE_SPLIT 1
+#endif
 __device__ __forceinline__ float2 ld_stream2(const float2* p) {
 #if UD_NA_LOADS
     float2 v;
@@ -271,6 +276,9 @@ struct Layout {
     int coords, forces;
     int frames;
     int prefix;            // per-atom prefix sums of force and moment (6 floats)
+    int forces2;           // second pair-force array (float4 per atom) inside the prefix area
+    int atomrec;           // the ligand's AtomRec records (4 words per atom), staged at chain start
+    int gridl;             // the ligand's grid-atom words (atom | slot << 8), staged at chain start
     int misc;
     int total;
 };
@@ -291,6 +299,15 @@ __host__ inline Layout make_layout(int max_atoms, int max_tors) {
     L.forces = take(4 * max_atoms);
     L.frames = take(20 * R);
     L.prefix = take(6 * max_atoms);
+    // floats [pad4(2A), pad4(2A) + 4A) of the prefix area (A = max_atoms): an
+    // iteration of the prefix scan over atoms [base, base + W) reads the
+    // second forces of its atoms before its shuffles and writes prefix entries
+    // after them, and the entries written so far end at float 6 (base + W),
+    // at or below 2A + 4 (base + W) where the next iteration's reads begin
+    // (base + W <= A whenever a next iteration exists)
+    L.forces2 = L.prefix + pad4(2 * max_atoms);
+    L.atomrec = take(4 * max_atoms);
+    L.gridl = take(max_atoms);
     L.misc = take(32);
     L.total = o;
     return L;
@@ -308,6 +325,20 @@ struct Ctx {
     int lane;
     int lig;
     __device__ __forceinline__ const AtomRec* atoms() const { return B->atoms + atom_off; }
+    // the staged copies (make_ctx) in this warp's shared memory
+    __device__ __forceinline__ AtomRec atom(const Layout& L, int a) const {
+        const float4 v = reinterpret_cast<const float4*>(s + L.atomrec)[a];
+        AtomRec r;
+        r.x = v.x; r.y = v.y; r.z = v.z;
+        r.packed = __float_as_int(v.w);
+        return r;
+    }
+    __device__ __forceinline__ int atom_packed(const Layout& L, int a) const {
+        return __float_as_int(s[L.atomrec + 4 * a + 3]);
+    }
+    __device__ __forceinline__ uint32_t grid_word(const Layout& L, int k) const {
+        return __float_as_uint(s[L.gridl + k]);
+    }
     __device__ __forceinline__ const NodeRec* nodes() const { return B->nodes + node_off; }
     __device__ __forceinline__ const uint32_t* pairs() const { return B->pairs + pair_off; }
     // atom | slot << 8 of the atoms with a grid map
@@ -317,8 +348,10 @@ struct Ctx {
     __device__ __forceinline__ const float2* coef() const { return B->pair_coef + pair_off; }
 };
 
+// The ligand's context, with its atom records and grid-atom words copied into
+// the warp's shared memory (read there by every evaluation).
 template <int kW = 32>
-__device__ __forceinline__ Ctx make_ctx(const Batch& B, int lig, float* s) {
+__device__ __forceinline__ Ctx make_ctx(const Batch& B, int lig, float* s, const Layout& L) {
     Ctx c;
     const LigDesc* d = B.ligs + lig;
     c.s = s;
@@ -336,6 +369,12 @@ __device__ __forceinline__ Ctx make_ctx(const Batch& B, int lig, float* s) {
     c.local_steps = __ldg(&d->local_steps);
     c.lane = threadIdx.x & (kW - 1);
     c.lig = lig;
+    const float4* ar = reinterpret_cast<const float4*>(B.atoms + c.atom_off);
+    float4* sa = reinterpret_cast<float4*>(s + L.atomrec);
+    for (int a = c.lane; a < c.n_atoms; a += kW) sa[a] = __ldg(ar + a);
+    uint32_t* sg = reinterpret_cast<uint32_t*>(s + L.gridl);
+    for (int k = c.lane; k < c.n_grid; k += kW) sg[k] = __ldg(B.grid_list + c.grid_off + k);
+    lanes_sync<kW>();
     return c;
 }
 
@@ -412,7 +451,7 @@ __device__ __forceinline__ void kinematics(const Ctx& c, const Layout& L, const 
     }
     float4* xyz = reinterpret_cast<float4*>(c.s + L.coords);
     for (int a = c.lane; a < c.n_atoms; a += kW) {
-        AtomRec ar = c.atoms()[a];
+        const AtomRec ar = c.atom(L, a);
         int n = ar.packed & 0xFF;
         const float* f = fr + 20 * n;
         const float* m = f + 7;
@@ -604,18 +643,24 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
     kinematics<kW>(c, L, conf);
     const float4* xyz = reinterpret_cast<const float4*>(c.s + L.coords);
     float4* frc = reinterpret_cast<float4*>(c.s + L.forces);
+    // pair forces of the odd lane ranges (UD_FORCE_SPLIT), summed into the
+    // per-atom forces by the prefix scan
+    float4* frc2 = reinterpret_cast<float4*>(c.s + L.forces2);
     float e = 0;
     // the per-atom force array: the grid (or receptor-atom) force of every
-    // atom, then the pair forces of every pair chunk but the last
-    for (int k = c.lane; k < c.n_atoms; k += kW) frc[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    // atom, then the pair forces
+    for (int k = c.lane; k < c.n_atoms; k += kW) {
+        frc[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (UD_FORCE_SPLIT) frc2[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
     lanes_sync<kW>();
     if constexpr (kReceptor) {
         const BiasRec* bias;
         int n_bias;
         bias_of(*Rc, c.lig, bias, n_bias);
         for (int k = 0; k < c.n_grid; ++k) {  // one atom at a time, lanes over its receptor atoms
-            const int a = __ldg(c.grid() + k) & 0xFF;
-            const int t1 = ((__ldg(&c.atoms()[a].packed) >> 24) & 0xFF) - 1;
+            const int a = c.grid_word(L, k) & 0xFF;
+            const int t1 = ((c.atom_packed(L, a) >> 24) & 0xFF) - 1;
             float gx, gy, gz;
             const float ea = receptor_term<true>(*Rc, Tb, t1, xyz[a], v_inter, rslope, bias, n_bias, gx, gy, gz);
             if (c.lane == 0) {
@@ -628,7 +673,7 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
         // atoms with a map: one pass of lanes, so that all corner loads of a
         // ligand of up to kW heavy atoms are in flight together
         for (int k = c.lane; k < c.n_grid; k += kW) {
-            const uint32_t ga = __ldg(c.grid() + k);
+            const uint32_t ga = c.grid_word(L, k);
             const int a = ga & 0xFF, slot = ga >> 8;
             float gx, gy, gz;
             const float4 pa = xyz[a];
@@ -717,14 +762,19 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
                 e += ep;
             }
             const int a = prv[u] & 0xFF, b = (prv[u] >> 8) & 0xFF;
+            // ranges 2p and 2p + 1 add in pass p, one to each force array
+            // (a range is a matching, so no atom is written twice in a pass)
+            constexpr int kSplit = UD_FORCE_SPLIT ? 2 : 1;
+            const int range = c.lane / kPairPassWidth;
+            float4* fd = (kSplit == 2 && (range & 1)) ? frc2 : frc;
 #pragma unroll
-            for (int pass = 0; pass < kWinPasses; ++pass) {
-                if (live && c.lane / kPairPassWidth == pass) {
-                    float4 fa = frc[a], fb = frc[b];
+            for (int pass = 0; pass < kWinPasses / kSplit; ++pass) {
+                if (live && range / kSplit == pass) {
+                    float4 fa = fd[a], fb = fd[b];
                     fa.x -= fx; fa.y -= fy; fa.z -= fz;
                     fb.x += fx; fb.y += fy; fb.z += fz;
-                    frc[a] = fa;
-                    frc[b] = fb;
+                    fd[a] = fa;
+                    fd[b] = fb;
                 }
                 lanes_sync<kW>();
             }
@@ -744,7 +794,12 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
         const int a = base + c.lane;
         float v[6] = {0, 0, 0, 0, 0, 0};
         if (a < c.n_atoms) {
-            const float4 fa = frc[a], xa = xyz[a];
+            float4 fa = frc[a];
+            if (UD_FORCE_SPLIT) {
+                const float4 fb = frc2[a];
+                fa.x += fb.x; fa.y += fb.y; fa.z += fb.z;
+            }
+            const float4 xa = xyz[a];
             const float f0 = fa.x, f1 = fa.y, f2 = fa.z;
             const float r0 = xa.x - fr[0], r1 = xa.y - fr[1], r2 = xa.z - fr[2];
             v[0] = f0; v[1] = f1; v[2] = f2;
@@ -830,7 +885,7 @@ __device__ __forceinline__ void eval_score(const Ctx& c, const Layout& L, const 
     const float4* xyz = reinterpret_cast<const float4*>(c.s + L.coords);
     float eg = 0;
     for (int k = c.lane; k < c.n_grid; k += kW) {
-        const uint32_t ga = __ldg(c.grid() + k);
+        const uint32_t ga = c.grid_word(L, k);
         float gx, gy, gz;
         const float4 pa = xyz[ga & 0xFF];
         eg += grid_eval(M, ga >> 8, pa, v, gx, gy, gz, false);
@@ -988,7 +1043,7 @@ __device__ void mutate(const Ctx& c, const Layout& L, Philox& rng, float amplitu
         const float* o = c.s + L.frames;
         float acc = 0, cnt = 0;
         for (int a = c.lane; a < c.n_atoms; a += kW) {
-            int packed = __ldg(&c.atoms()[a].packed);
+            int packed = c.atom_packed(L, a);
             if ((packed >> 16) & 1) {
                 const float4 pa = xyz[a];
                 float dx = pa.x - o[0], dy = pa.y - o[1], dz = pa.z - o[2];
@@ -1176,7 +1231,7 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                         m.lig = order[gi / P.exhaustiveness];
                         m.chain = gi % P.exhaustiveness;
                     }
-                    c = make_ctx<kW>(B, m.lig, sw);
+                    c = make_ctx<kW>(B, m.lig, sw, L);
                     rng.init(P.seed, (uint32_t)m.lig, (uint32_t)m.chain);
                     m.steps_cap = c.local_steps;
                     if (P.bfgs_cap > 0 && P.bfgs_cap < m.steps_cap) m.steps_cap = P.bfgs_cap;
@@ -1195,7 +1250,7 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                     st = S_MC_STEP;
                 } else {
                     m.lig = opt_lig[it];
-                    c = make_ctx<kW>(B, m.lig, sw);
+                    c = make_ctx<kW>(B, m.lig, sw, L);
                     float* x = c.s + L.x;
                     for (int i = lane; i < 7 + c.T; i += kW) x[i] = poses[(size_t)it * pose_stride + i];
                     lanes_sync<kW>();
@@ -1444,7 +1499,7 @@ __global__ void __launch_bounds__(128) score_kernel(
     const int pose = blockIdx.x * (blockDim.x >> 5) + warp;
     if (pose >= n_poses) return;
     float* sw = smem + (size_t)warp * L.total;
-    const Ctx c = make_ctx(B, pose_lig[pose], sw);
+    const Ctx c = make_ctx(B, pose_lig[pose], sw, L);
     float* x = sw + L.x;
     const int cs = 7 + c.T;
     for (int i = c.lane; i < cs; i += 32) x[i] = poses[(size_t)pose * pose_stride + i];
@@ -1476,7 +1531,7 @@ __device__ __forceinline__ bool heavy_within(const Ctx& c, const Layout& L, cons
     const float m = 1e-4f;
     bool ok = true;
     for (int a = c.lane; a < c.n_atoms; a += 32) {
-        if (!((__ldg(&c.atoms()[a].packed) >> 16) & 1)) continue;
+        if (!((c.atom_packed(L, a) >> 16) & 1)) continue;
         const float4 x = xyz[a];
         if (x.x < R.begin[0] - m || x.x > R.end[0] + m || x.y < R.begin[1] - m || x.y > R.end[1] + m ||
             x.z < R.begin[2] - m || x.z > R.end[2] + m)
@@ -1497,8 +1552,8 @@ __device__ __forceinline__ void eval_score_receptor(const Ctx& c, const Layout& 
     bias_of(R, c.lig, bias, n_bias);
     float ei = 0;
     for (int k = 0; k < c.n_grid; ++k) {
-        const int a = __ldg(c.grid() + k) & 0xFF;
-        const int t1 = ((__ldg(&c.atoms()[a].packed) >> 24) & 0xFF) - 1;
+        const int a = c.grid_word(L, k) & 0xFF;
+        const int t1 = ((c.atom_packed(L, a) >> 24) & 0xFF) - 1;
         float gx, gy, gz;
         ei += receptor_term<false>(R, Tb, t1, xyz[a], v, 1e6f, bias, n_bias, gx, gy, gz);
     }
@@ -1579,7 +1634,7 @@ __global__ void __launch_bounds__(128) receptor_kernel(
     const int lig = pose_lig[pose];
     if (lig < 0) return;
     float* sw = smem + (size_t)warp * L.total;
-    const Ctx c = make_ctx(B, lig, sw);
+    const Ctx c = make_ctx(B, lig, sw, L);
     float* x = sw + L.x;
     const int cs = 7 + c.T;
     for (int i = c.lane; i < cs; i += 32) x[i] = poses[(size_t)pose * pose_stride + i];
@@ -1690,7 +1745,7 @@ __global__ void __launch_bounds__(128) cluster_kernel(
     float* ent_e = sw + L.total + cap4;
     int* ent_chain = reinterpret_cast<int*>(sw + L.total + 2 * cap4);
     int* keep = reinterpret_cast<int*>(sw + L.total + 3 * cap4);
-    const Ctx c = make_ctx(B, lig, sw);
+    const Ctx c = make_ctx(B, lig, sw, L);
     const int n_heavy = __ldg(&B.ligs[lig].n_heavy);
     const float4* xyz = reinterpret_cast<const float4*>(c.s + L.coords);
     float* S = scratch + (size_t)lig * cap * 3 * max_atoms;
@@ -1853,7 +1908,7 @@ __global__ void __launch_bounds__(128) adjoint_kernel(
         return;
     }
     float* sw = smem + (size_t)warp * L.total;
-    const Ctx c = make_ctx(B, lig, sw);
+    const Ctx c = make_ctx(B, lig, sw, L);
     float* x = sw + L.x;
     const int cs = 7 + c.T;
     for (int i = c.lane; i < cs; i += 32) x[i] = poses[(size_t)pose * pose_stride + i];
@@ -1882,7 +1937,7 @@ __global__ void __launch_bounds__(128) adjoint_kernel(
         const float4* xyz = reinterpret_cast<const float4*>(sw + L.coords);  // conformer of the evaluation above
         const size_t plane = (size_t)M.nx * M.ny * M.nz;
         for (int k = c.lane; k < c.n_grid; k += 32) {
-            const uint32_t ga = __ldg(c.grid() + k);
+            const uint32_t ga = c.grid_word(L, k);
             const int a = ga & 0xFF, slot = ga >> 8;
             int cell;
             float frac[3];
