@@ -35,9 +35,13 @@ BOX = 22.5
 SPACING = 0.375
 ADJOINT_POSES = 65536
 # DRAM bytes (read + write) of one search launch of this workload at 1024
-# ligands per step, measured with ncu (dram__bytes_read.sum 13.36 MB +
-# dram__bytes_write.sum 3.98 MB, one-pass capture of a timed launch)
-SEARCH_LAUNCH_DRAM_BYTES = 13.36e6 + 3.98e6
+# ligands per step, measured with ncu (dram__bytes_read.sum 17.83 GB +
+# dram__bytes_write.sum 0.067 GB, one-pass capture of the first timed launch):
+# about 1.3 % of the launch's algorithmic L2 bytes miss L2
+SEARCH_LAUNCH_DRAM_BYTES = 17.832e9 + 0.0667e9
+# the same for one adjoint launch of the differentiation workload
+# (dram__bytes_read.sum 657.0 MB + dram__bytes_write.sum 22.9 MB, ncu --set full)
+ADJOINT_LAUNCH_DRAM_BYTES = 657.0e6 + 22.9e6
 
 
 def parse_args():
@@ -69,6 +73,9 @@ def parse_args():
                          "multi-rank launch on a machine without GPUs")
     ap.add_argument("--profile-case", type=int, default=0,
                     help="profiling aid: search N ligands of the workload twice and exit (no JSON)")
+    ap.add_argument("--profile-adjoint", action="store_true",
+                    help="profiling aid: the adjoint leg alone (3 warm-up launches and 1 timed, 65,536 poses) "
+                         "and exit; the second adjoint launch is the one to capture")
     ap.add_argument("--profile-receptor", type=int, default=3000, choices=[3000, 6000, 12000],
                     help="receptor of the profiling case: 3000 atoms in a 22.5 A box (61^3 maps), "
                          "6000 in 30 A (81^3) or 12000 in 36 A (97^3), as the streaming screen")
@@ -364,8 +371,8 @@ def run_ours(args, rank, world):
             "batched_over_plain": None if plain is None else round(value / plain, 2),
             "evals_per_s": round(evals_total / t_total, 1),
             # the search reads L2-resident maps and pair tables: its memory
-            # ceiling is L2 read bandwidth (measured here), not HBM; DRAM
-            # traffic per launch stays at the maps' first load
+            # ceiling is L2 read bandwidth (measured here), not HBM; about
+            # 1.3 % of its L2 reads go on to DRAM
             "roofline": {"bound": "l2", "achieved": round(achieved_gbs, 2), "peak": round(l2_peak, 1),
                          "unit": "GB/s", "frac": round(achieved_gbs / l2_peak, 4),
                          "traffic": SEARCH_LAUNCH_DRAM_BYTES if B == 1024 else None,
@@ -455,6 +462,8 @@ def adjoint_leg(maps, l2_peak, n_ligands=256, reps=5):
             "roofline": {"bound": "l2", "kernel": "ud::dev::adjoint_kernel", "achieved": round(gbs, 1),
                          "peak": round(l2_peak, 1), "unit": "GB/s", "frac": round(gbs / l2_peak, 4),
                          "algorithmic_bytes_per_launch": round(bytes_launch),
+                         "traffic": ADJOINT_LAUNCH_DRAM_BYTES if n == ADJOINT_POSES and n_ligands == 256 else None,
+                         "traffic_note": "DRAM bytes (read + write) per launch from one ncu capture of this workload",
                          "note": "the 7 map sets (weighted + 6 term maps, 153 MB at 61^3) exceed the 126 MB L2, "
                                  "so part of the reads come from HBM"}}
 
@@ -804,6 +813,12 @@ def main():
         return
     if args.profile_case > 0:
         profile_case(args)
+        return
+    if args.profile_adjoint:
+        from unidock_tools import engine, synth
+        rec = synth.make_receptor(3000, seed=1)
+        maps = engine.Maps(rec.xyz, rec.xs, np.zeros(3, np.float32), np.full(3, BOX, np.float32), SPACING)
+        print(json.dumps(adjoint_leg(maps, engine.l2_peak_gbs(), reps=1)), flush=True)
         return
     if args.workload != "screen-fast" and args.impl != "reference":
         res = (run_stream(args) if args.workload == "stream" else

@@ -237,7 +237,9 @@ typedef struct {
     float energy_range;     /* output energy window (--energy_range) */
     unsigned long long seed;/* --seed */
     int form;               /* 0 = plain (one launch per ligand), 1 = batched persistent */
-    int chains_per_block;   /* warps per CTA, 1..4; 0 = the batch's autotuned value, else 4 */
+    int chains_per_block;   /* warps per CTA, 1..4; 0 = the batch's autotuned value, else the CTA size of
+                               4, 2 or 1 warps that keeps the most chains resident per SM at the
+                               batch's layout (the plain form: 4) */
     int bfgs_cap;           /* 0 = per-ligand (25 + atoms)/3 BFGS steps; >0 caps it;
                                <0 = the batch's autotuned cap (per-ligand when not tuned) */
     int use_graph;          /* batched form: the per-batch sequence (queue reset, search

@@ -1913,6 +1913,22 @@ static void search_graph(ud_batch b, const SearchParams& sp, int n_chain, int bl
 // Launch the search kernels of the batch asynchronously on `s`, followed by the
 // clustering (and refinement) of the modes unless `modes` is false.
 // `launch` false: only the set-up (buffers, ligand order, graph capture).
+// CTA size (warps) of a persistent search whose caller and autotuner gave
+// none: of 4, 2 and 1 warps, the one that keeps the most chains resident per
+// SM at the batch's layout, ties to the larger CTA.  A large layout, whose
+// per-chain shared memory lets few 4-warp CTAs onto an SM, gets smaller CTAs.
+static int default_chains_per_block(const DeviceBatchView& v, int lanes, bool stream) {
+    int best = 4, best_resident = 0;
+    for (int w : {4, 2, 1}) {
+        const int per_sm = stream ? stream_blocks_per_sm(v, w) : search_blocks_per_sm(v, w, lanes);
+        if (per_sm * w > best_resident) {
+            best = w;
+            best_resident = per_sm * w;
+        }
+    }
+    return best;
+}
+
 static void search_launch(ud_batch b, const ud_search_params* params, cudaStream_t s, bool launch = true,
                           bool modes = true) {
         if (!b || !params) throw Error(UD_ERR_ARG, "null argument");
@@ -1947,7 +1963,10 @@ static void search_launch(ud_batch b, const ud_search_params* params, cudaStream
         // the plain form keeps one chain per warp (the fixed tiling it stands for)
         sp.lanes_per_chain = P.form != 1 ? 32
                              : P.lanes_per_chain > 0 ? P.lanes_per_chain : (b->tuned ? b->tuned_lanes_per_chain : 32);
-        sp.chains_per_block = P.chains_per_block > 0 ? P.chains_per_block : (b->tuned ? b->tuned_chains_per_block : 4);
+        sp.chains_per_block = P.chains_per_block > 0 ? P.chains_per_block
+                              : b->tuned                 ? b->tuned_chains_per_block
+                              : P.form == 1              ? default_chains_per_block(b->view(), sp.lanes_per_chain, false)
+                                                         : 4;
         const int chains_per_cta = sp.chains_per_block * (32 / sp.lanes_per_chain);
         sp.persistent = P.form == 1 ? 1 : 0;
         sp.bfgs_cap = P.bfgs_cap >= 0 ? P.bfgs_cap : (b->tuned ? b->tuned_bfgs_cap : 0);
@@ -2427,7 +2446,9 @@ extern "C" int ud_search_device_noalloc(ud_batch b, const ud_search_params* para
         sp.temperature = 1.2f;
         sp.mutation_amplitude = 2.0f;
         sp.lanes_per_chain = P.lanes_per_chain > 0 ? P.lanes_per_chain : (b->tuned ? b->tuned_lanes_per_chain : 32);
-        sp.chains_per_block = P.chains_per_block > 0 ? P.chains_per_block : (b->tuned ? b->tuned_chains_per_block : 4);
+        sp.chains_per_block = P.chains_per_block > 0 ? P.chains_per_block
+                              : b->tuned ? b->tuned_chains_per_block
+                                         : default_chains_per_block(b->view(), sp.lanes_per_chain, false);
         sp.persistent = 1;
         sp.bfgs_cap = P.bfgs_cap >= 0 ? P.bfgs_cap : (b->tuned ? b->tuned_bfgs_cap : 0);
         const int chains_per_cta = sp.chains_per_block * (32 / sp.lanes_per_chain);
@@ -2587,7 +2608,7 @@ extern "C" int ud_stream_create(ud_maps maps, const ud_search_params* params, co
         sp.temperature = 1.2f;
         sp.mutation_amplitude = 2.0f;
         sp.lanes_per_chain = 32;
-        sp.chains_per_block = P.chains_per_block > 0 ? P.chains_per_block : 4;
+        sp.chains_per_block = P.chains_per_block;  // 0: set from the layout below
         sp.persistent = 1;
         sp.bfgs_cap = P.bfgs_cap > 0 ? P.bfgs_cap : 0;
         const size_t S = (size_t)st->max_slots, M = (size_t)st->M, E = (size_t)st->E;
@@ -2670,6 +2691,7 @@ extern "C" int ud_stream_create(ud_maps maps, const ud_search_params* params, co
         // one full wave of blocks; those on every reserve_every-th SM return at
         // once and leave their SM to the per-slot post-processing kernels
         cuda_check(prepare_stream_post(st->view(), st->cap, st->refined), "stream post-processing kernels");
+        if (sp.chains_per_block == 0) sp.chains_per_block = default_chains_per_block(st->view(), 32, true);
         const int per_sm = stream_blocks_per_sm(st->view(), sp.chains_per_block);
         const int blocks = per_sm * n_sm;
         sv.reserve_every = n_sm >= 2 * kStreamReserveSms ? n_sm / kStreamReserveSms : 0;

@@ -208,10 +208,18 @@ constexpr int kPairBatch = UD_PAIR_BATCH;
 #ifndef UD_PAIR_PREFETCH
 #define UD_PAIR_PREFETCH 1
 #endif
-// UD_FORCE_SPLIT: the pair forces of odd lane ranges go to a second force
-// array, so that two ranges add their forces at once (half the passes)
+// UD_FORCE_SPLIT (1 or 2): the number of per-atom pair-force arrays; lane
+// range r of a pair window adds into array r % UD_FORCE_SPLIT, so that two
+// ranges add their forces at once (half the read-modify-write passes)
 #ifndef UD_FORCE_SPLIT
-#define UD_FORCE_SPLIT 1
+#define UD_FORCE_SPLIT 2
+#endif
+static_assert(UD_FORCE_SPLIT == 1 || UD_FORCE_SPLIT == 2, "1 or 2 force arrays");
+// UD_STAGE_ATOMS: each chain copies its ligand's atom records and grid-atom
+// words into shared memory at chain start instead of reading them through
+// the read-only cache every evaluation
+#ifndef UD_STAGE_ATOMS
+#define UD_STAGE_ATOMS 1
 #endif
 __device__ __forceinline__ float2 ld_stream2(const float2* p) {
 #if UD_NA_LOADS
@@ -306,8 +314,8 @@ __host__ inline Layout make_layout(int max_atoms, int max_tors) {
     // at or below 2A + 4 (base + W) where the next iteration's reads begin
     // (base + W <= A whenever a next iteration exists)
     L.forces2 = L.prefix + pad4(2 * max_atoms);
-    L.atomrec = take(4 * max_atoms);
-    L.gridl = take(max_atoms);
+    L.atomrec = take(UD_STAGE_ATOMS ? 4 * max_atoms : 0);
+    L.gridl = take(UD_STAGE_ATOMS ? max_atoms : 0);
     L.misc = take(32);
     L.total = o;
     return L;
@@ -327,17 +335,29 @@ struct Ctx {
     __device__ __forceinline__ const AtomRec* atoms() const { return B->atoms + atom_off; }
     // the staged copies (make_ctx) in this warp's shared memory
     __device__ __forceinline__ AtomRec atom(const Layout& L, int a) const {
+#if UD_STAGE_ATOMS
         const float4 v = reinterpret_cast<const float4*>(s + L.atomrec)[a];
+#else
+        const float4 v = __ldg(reinterpret_cast<const float4*>(B->atoms + atom_off) + a);
+#endif
         AtomRec r;
         r.x = v.x; r.y = v.y; r.z = v.z;
         r.packed = __float_as_int(v.w);
         return r;
     }
     __device__ __forceinline__ int atom_packed(const Layout& L, int a) const {
+#if UD_STAGE_ATOMS
         return __float_as_int(s[L.atomrec + 4 * a + 3]);
+#else
+        return __ldg(&B->atoms[atom_off + a].packed);
+#endif
     }
     __device__ __forceinline__ uint32_t grid_word(const Layout& L, int k) const {
+#if UD_STAGE_ATOMS
         return __float_as_uint(s[L.gridl + k]);
+#else
+        return __ldg(B->grid_list + grid_off + k);
+#endif
     }
     __device__ __forceinline__ const NodeRec* nodes() const { return B->nodes + node_off; }
     __device__ __forceinline__ const uint32_t* pairs() const { return B->pairs + pair_off; }
@@ -369,12 +389,14 @@ __device__ __forceinline__ Ctx make_ctx(const Batch& B, int lig, float* s, const
     c.local_steps = __ldg(&d->local_steps);
     c.lane = threadIdx.x & (kW - 1);
     c.lig = lig;
+#if UD_STAGE_ATOMS
     const float4* ar = reinterpret_cast<const float4*>(B.atoms + c.atom_off);
     float4* sa = reinterpret_cast<float4*>(s + L.atomrec);
     for (int a = c.lane; a < c.n_atoms; a += kW) sa[a] = __ldg(ar + a);
     uint32_t* sg = reinterpret_cast<uint32_t*>(s + L.gridl);
     for (int k = c.lane; k < c.n_grid; k += kW) sg[k] = __ldg(B.grid_list + c.grid_off + k);
     lanes_sync<kW>();
+#endif
     return c;
 }
 
@@ -651,7 +673,7 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
     // atom, then the pair forces
     for (int k = c.lane; k < c.n_atoms; k += kW) {
         frc[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (UD_FORCE_SPLIT) frc2[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (UD_FORCE_SPLIT == 2) frc2[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
     lanes_sync<kW>();
     if constexpr (kReceptor) {
@@ -762,9 +784,9 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
                 e += ep;
             }
             const int a = prv[u] & 0xFF, b = (prv[u] >> 8) & 0xFF;
-            // ranges 2p and 2p + 1 add in pass p, one to each force array
+            // ranges 2p and 2p + 1 add in pass p, one into each force array
             // (a range is a matching, so no atom is written twice in a pass)
-            constexpr int kSplit = UD_FORCE_SPLIT ? 2 : 1;
+            constexpr int kSplit = UD_FORCE_SPLIT;
             const int range = c.lane / kPairPassWidth;
             float4* fd = (kSplit == 2 && (range & 1)) ? frc2 : frc;
 #pragma unroll
@@ -795,7 +817,7 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
         float v[6] = {0, 0, 0, 0, 0, 0};
         if (a < c.n_atoms) {
             float4 fa = frc[a];
-            if (UD_FORCE_SPLIT) {
+            if (UD_FORCE_SPLIT == 2) {
                 const float4 fb = frc2[a];
                 fa.x += fb.x; fa.y += fb.y; fa.z += fb.z;
             }
@@ -1102,9 +1124,6 @@ struct Machine {
     float alpha, f0, f_orig, pg, last_e;
 };
 
-// The MC chain of monte_carlo.cu:237-356 (mutate, BFGS at the hunt cap,
-// Metropolis at temperature T, refine improvements at the authentic cap, keep
-// the best) with the line search and BFGS iterations of bfgs.h:63-146.
 // Nanoseconds of the GPU's global timer.
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -1170,6 +1189,9 @@ __device__ __noinline__ int stream_fetch(const StreamView& SV, int E, int* item_
     }
 }
 
+// The MC chain of monte_carlo.cu:237-356 (mutate, BFGS at the hunt cap,
+// Metropolis at temperature T, refine improvements at the authentic cap, keep
+// the best) with the line search and BFGS iterations of bfgs.h:63-146.
 template <bool kSearch, bool kAD4, int kW, bool kStream = false>
 __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const Tables& Tb,
                                             const SearchParams& P, const Layout& L, float* sw,
