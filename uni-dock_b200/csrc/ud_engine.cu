@@ -221,15 +221,10 @@ static_assert(UD_FORCE_SPLIT == 1 || UD_FORCE_SPLIT == 2, "1 or 2 force arrays")
 #ifndef UD_STAGE_ATOMS
 #define UD_STAGE_ATOMS 1
 #endif
-// UD_MACHINE_SMEM: a chain's control state (Machine, Philox counter) is parked
-// in shared memory across each evaluation, so that its registers are free
-// inside the evaluation
-#ifndef UD_MACHINE_SMEM
-#define UD_MACHINE_SMEM 0
-#endif
 // UD_PAIR_PIPE: pair windows software-pipelined one table row ahead
+// (Vina / Vinardo)
 #ifndef UD_PAIR_PIPE
-#define UD_PAIR_PIPE 0
+#define UD_PAIR_PIPE 1
 #endif
 __device__ __forceinline__ float2 ld_stream2(const float2* p) {
 #if UD_NA_LOADS
@@ -297,7 +292,6 @@ struct Layout {
     int forces2;           // second pair-force array (float4 per atom) inside the prefix area
     int atomrec;           // the ligand's AtomRec records (4 words per atom), staged at chain start
     int gridl;             // the ligand's grid-atom words (atom | slot << 8), staged at chain start
-    int mach;              // the control state parked across an evaluation (UD_MACHINE_SMEM)
     int misc;
     int total;
 };
@@ -327,7 +321,6 @@ __host__ inline Layout make_layout(int max_atoms, int max_tors) {
     L.forces2 = L.prefix + pad4(2 * max_atoms);
     L.atomrec = take(UD_STAGE_ATOMS ? 4 * max_atoms : 0);
     L.gridl = take(UD_STAGE_ATOMS ? max_atoms : 0);
-    L.mach = take(UD_MACHINE_SMEM ? 32 : 0);
     L.misc = take(32);
     L.total = o;
     return L;
@@ -738,47 +731,53 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
     uint32_t pr_next = (UD_PAIR_PREFETCH && n_groups > 0) ? __ldg(c.pairs() + c.lane) : kPairPad;
 #if UD_PAIR_PIPE
     // Software-pipelined windows (Vina / Vinardo): the table row of window
-    // g + 1 is requested before window g's forces are added, and the pair
-    // word two windows ahead, so each window's L2 round trip overlaps the
-    // previous window's work.
+    // g + UD_PAIR_PIPE is requested before window g's forces are added (and
+    // its pair word one window earlier), so each window's L2 round trip
+    // overlaps the work of the windows before it.
     if constexpr (!kAD4) {
+        constexpr int kPipe = UD_PAIR_PIPE;
         constexpr int kSplit = UD_FORCE_SPLIT;
         const int range = c.lane / kPairPassWidth;
         float4* fd = (kSplit == 2 && (range & 1)) ? frc2 : frc;
         const uint32_t* pw = c.pairs() + c.lane;
-        auto request = [&](uint32_t w, uint32_t& pr, float4& t, float& rem, float& rx, float& ry, float& rz) {
-            pr = kPairPad;
+        struct Stage {
+            uint32_t pr;   // pair word, kPairPad when the slot adds nothing
+            float4 t;      // table row (e_i, dor_i, e_i+1, dor_i+1)
+            float rem, rx, ry, rz;
+        };
+        auto request = [&](uint32_t w, Stage& q) {
+            q.pr = kPairPad;
+            q.t = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            q.rem = q.rx = q.ry = q.rz = 0.0f;
             if (w != kPairPad) {
                 const float4 pa = xyz[w & 0xFF], pb = xyz[(w >> 8) & 0xFF];
-                rx = pb.x - pa.x; ry = pb.y - pa.y; rz = pb.z - pa.z;
-                const float r2 = rx * rx + ry * ry + rz * rz;
+                q.rx = pb.x - pa.x; q.ry = pb.y - pa.y; q.rz = pb.z - pa.z;
+                const float r2 = q.rx * q.rx + q.ry * q.ry + q.rz * q.rz;
                 if (r2 < Tb.cutoff2) {
                     const float rf = Tb.factor * r2;
                     const int i1 = (int)rf;
-                    rem = rf - i1;
-                    t = ld_stream4(Tb.smooth4 + (size_t)(w >> 16) * Tb.n_bins + i1);
-                    pr = w;
+                    q.rem = rf - i1;
+                    q.t = ld_stream4(Tb.smooth4 + (size_t)(w >> 16) * Tb.n_bins + i1);
+                    q.pr = w;
                 }
             }
         };
-        uint32_t w_next = n_groups > 1 ? __ldg(pw + (1 << kWinShift)) : kPairPad;
-        uint32_t pr_c = kPairPad;
-        float4 t_c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        float rem_c = 0.0f, rx_c = 0.0f, ry_c = 0.0f, rz_c = 0.0f;
-        if (n_groups > 0) request(__ldg(pw), pr_c, t_c, rem_c, rx_c, ry_c, rz_c);
+        auto word = [&](int g) { return g < n_groups ? __ldg(pw + (g << kWinShift)) : kPairPad; };
+        Stage q[kPipe + 1];
+#pragma unroll
+        for (int k = 0; k < kPipe; ++k) request(word(k), q[k]);
+        uint32_t w_next = word(kPipe);
         for (int g = 0; g < n_groups; ++g) {
-            uint32_t pr_n = kPairPad;
-            float4 t_n = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            float rem_n = 0.0f, rx_n = 0.0f, ry_n = 0.0f, rz_n = 0.0f;
             const uint32_t w1 = w_next;
-            w_next = g + 2 < n_groups ? __ldg(pw + ((g + 2) << kWinShift)) : kPairPad;
-            request(w1, pr_n, t_n, rem_n, rx_n, ry_n, rz_n);
+            w_next = word(g + kPipe + 1);
+            request(w1, q[kPipe]);
+            const Stage& h = q[0];
             float fx = 0, fy = 0, fz = 0;
-            const bool live = pr_c != kPairPad;
+            const bool live = h.pr != kPairPad;
             if (live) {
-                float ep = t_c.x + rem_c * (t_c.z - t_c.x);
-                float dor = kExactPairs ? 2.0f * Tb.factor * (t_c.z - t_c.x) : t_c.y + rem_c * (t_c.w - t_c.y);
-                fx = dor * rx_c; fy = dor * ry_c; fz = dor * rz_c;
+                float ep = h.t.x + h.rem * (h.t.z - h.t.x);
+                float dor = kExactPairs ? 2.0f * Tb.factor * (h.t.z - h.t.x) : h.t.y + h.rem * (h.t.w - h.t.y);
+                fx = dor * h.rx; fy = dor * h.ry; fz = dor * h.rz;
                 if (ep > 0 && v_intra < 0.1f * kMaxFl) {
                     float tmp = (v_intra < kEps) ? 0 : __fdividef(v_intra, v_intra + ep);
                     ep *= tmp;
@@ -787,7 +786,7 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
                 }
                 e += ep;
             }
-            const int a = pr_c & 0xFF, b = (pr_c >> 8) & 0xFF;
+            const int a = h.pr & 0xFF, b = (h.pr >> 8) & 0xFF;
 #pragma unroll
             for (int pass = 0; pass < kWinPasses / kSplit; ++pass) {
                 if (live && range / kSplit == pass) {
@@ -799,7 +798,8 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
                 }
                 lanes_sync<kW>();
             }
-            pr_c = pr_n; t_c = t_n; rem_c = rem_n; rx_c = rx_n; ry_c = ry_n; rz_c = rz_n;
+#pragma unroll
+            for (int k = 0; k < kPipe; ++k) q[k] = q[k + 1];
         }
     } else
 #endif
@@ -1529,26 +1529,7 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
         }
         if (st == S_EXIT) return;
         // ---- the single evaluation site
-#if UD_MACHINE_SMEM
-        {
-            static_assert(sizeof(Machine) + sizeof(Philox) <= 32 * sizeof(float), "parked state fits");
-            Machine* pm = reinterpret_cast<Machine*>(sw + L.mach);
-            Philox* pr = reinterpret_cast<Philox*>(pm + 1);
-            // every lane stores the same values and reads them back after
-            // the evaluation; the barrier keeps the next store behind every
-            // lane's read
-            *pm = m;
-            *pr = rng;
-            const float v = m.v;
-            const float e = eval_deriv<false, kAD4, false, kW>(c, L, M, Tb, eval_x, eval_g, v, v);
-            m = *pm;
-            rng = *pr;
-            m.last_e = e;
-            lanes_sync<kW>();
-        }
-#else
         m.last_e = eval_deriv<false, kAD4, false, kW>(c, L, M, Tb, eval_x, eval_g, m.v, m.v);
-#endif
         ++m.evals;
     }
 }
