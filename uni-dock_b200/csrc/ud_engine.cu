@@ -177,6 +177,30 @@ __device__ __forceinline__ float lanes_sum(float v) {
     return v;
 }
 
+// Two or three sums at once: the same shuffle tree per value, interleaved so
+// that one reduction's latency covers all of them.
+template <int kW>
+__device__ __forceinline__ void lanes_sum2(float& a, float& b) {
+    const unsigned m = lanes_mask<kW>();
+#pragma unroll
+    for (int o = kW / 2; o > 0; o >>= 1) {
+        const float ta = __shfl_xor_sync(m, a, o), tb = __shfl_xor_sync(m, b, o);
+        a += ta;
+        b += tb;
+    }
+}
+template <int kW>
+__device__ __forceinline__ void lanes_sum3(float& a, float& b, float& c) {
+    const unsigned m = lanes_mask<kW>();
+#pragma unroll
+    for (int o = kW / 2; o > 0; o >>= 1) {
+        const float ta = __shfl_xor_sync(m, a, o), tb = __shfl_xor_sync(m, b, o), tc = __shfl_xor_sync(m, c, o);
+        a += ta;
+        b += tb;
+        c += tc;
+    }
+}
+
 template <int kW>
 __device__ __forceinline__ void lanes_sync() { __syncwarp(lanes_mask<kW>()); }
 
@@ -438,7 +462,9 @@ __device__ __forceinline__ void kinematics(const Ctx& c, const Layout& L, const 
             const NodeRec* nr = nodes + n;
             ra[0] = __ldg(&nr->rel_axis[0]); ra[1] = __ldg(&nr->rel_axis[1]); ra[2] = __ldg(&nr->rel_axis[2]);
         }
-        axis_angle_q(ra, conf[7 + n - 1], fr + 20 * n + 16);
+        float tq[4];
+        axis_angle_q(ra, conf[7 + n - 1], tq);
+        reinterpret_cast<float4*>(fr + 20 * n)[4] = make_float4(tq[0], tq[1], tq[2], tq[3]);
     }
     if (c.lane == 0) {
         fr[0] = conf[0]; fr[1] = conf[1]; fr[2] = conf[2];
@@ -459,32 +485,41 @@ __device__ __forceinline__ void kinematics(const Ctx& c, const Layout& L, const 
                 ra[0] = __ldg(&nr->rel_axis[0]); ra[1] = __ldg(&nr->rel_axis[1]); ra[2] = __ldg(&nr->rel_axis[2]);
             }
             if (depth != d) continue;
-            const float* pf = fr + 20 * parent;
-            float* f = fr + 20 * n;
-            const float* pm = pf + 7;
-            float t[4] = {f[16], f[17], f[18], f[19]};
+            // frames as five float4: (o, q0) (q1..3, R0) (R1..4) (R5..8) (axis, -)
+            const float4* pf = reinterpret_cast<const float4*>(fr + 20 * parent);
+            float4* f = reinterpret_cast<float4*>(fr + 20 * n);
+            const float4 p0 = pf[0], p1 = pf[1], p2 = pf[2], p3 = pf[3], tq = f[4];
+            const float pm[9] = {p1.w, p2.x, p2.y, p2.z, p2.w, p3.x, p3.y, p3.z, p3.w};
+            const float po[3] = {p0.x, p0.y, p0.z}, pq[4] = {p0.w, p1.x, p1.y, p1.z};
+            const float t[4] = {tq.x, tq.y, tq.z, tq.w};
+            float o[3], ax[3];
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
-                f[i] = pf[i] + (pm[3 * i] * ro[0] + pm[3 * i + 1] * ro[1] + pm[3 * i + 2] * ro[2]);
-                f[16 + i] = pm[3 * i] * ra[0] + pm[3 * i + 1] * ra[1] + pm[3 * i + 2] * ra[2];
+                o[i] = po[i] + (pm[3 * i] * ro[0] + pm[3 * i + 1] * ro[1] + pm[3 * i + 2] * ro[2]);
+                ax[i] = pm[3 * i] * ra[0] + pm[3 * i + 1] * ra[1] + pm[3 * i + 2] * ra[2];
             }
-            float q[4];
-            qmul(pf + 3, t, q);
+            float q[4], m[9];
+            qmul(pq, t, q);
             qnormalize_approx(q);
-            f[3] = q[0]; f[4] = q[1]; f[5] = q[2]; f[6] = q[3];
-            q_to_r3(q, f + 7);
+            q_to_r3(q, m);
+            f[0] = make_float4(o[0], o[1], o[2], q[0]);
+            f[1] = make_float4(q[1], q[2], q[3], m[0]);
+            f[2] = make_float4(m[1], m[2], m[3], m[4]);
+            f[3] = make_float4(m[5], m[6], m[7], m[8]);
+            f[4] = make_float4(ax[0], ax[1], ax[2], 0.0f);
         }
         lanes_sync<kW>();
     }
     float4* xyz = reinterpret_cast<float4*>(c.s + L.coords);
     for (int a = c.lane; a < c.n_atoms; a += kW) {
         const AtomRec ar = c.atom(L, a);
-        int n = ar.packed & 0xFF;
-        const float* f = fr + 20 * n;
-        const float* m = f + 7;
+        const float4* f = reinterpret_cast<const float4*>(fr + 20 * (ar.packed & 0xFF));
+        const float4 f0 = f[0], f1 = f[1], f2 = f[2], f3 = f[3];
+        const float fo[3] = {f0.x, f0.y, f0.z};
+        const float m[9] = {f1.w, f2.x, f2.y, f2.z, f2.w, f3.x, f3.y, f3.z, f3.w};
         float o[3];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) o[i] = f[i] + (m[3 * i] * ar.x + m[3 * i + 1] * ar.y + m[3 * i + 2] * ar.z);
+        for (int i = 0; i < 3; ++i) o[i] = fo[i] + (m[3 * i] * ar.x + m[3 * i + 1] * ar.y + m[3 * i + 2] * ar.z);
         xyz[a] = make_float4(o[0], o[1], o[2], 0.0f);
     }
     lanes_sync<kW>();
@@ -921,18 +956,25 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
             v[q] += carry[q];
             carry[q] = __shfl_sync(lanes, v[q], kW - 1, kW);
         }
-        if (a < c.n_atoms)
-#pragma unroll
-            for (int q = 0; q < 6; ++q) pre[6 * a + q] = v[q];
+        if (a < c.n_atoms) {  // 6 floats an atom: three 8-byte stores
+            float2* pa = reinterpret_cast<float2*>(pre + 6 * a);
+            pa[0] = make_float2(v[0], v[1]);
+            pa[1] = make_float2(v[2], v[3]);
+            pa[2] = make_float2(v[4], v[5]);
+        }
     }
     lanes_sync<kW>();
     for (int n = c.lane; n < c.R; n += kW) {
         const int span = __ldg(&c.nodes()[n].atoms);
         const int b0 = span & 0xFFFF, b1 = span >> 16;
-        const float* hi = pre + 6 * (b1 - 1);
-        float sm[6];
-#pragma unroll
-        for (int q = 0; q < 6; ++q) sm[q] = hi[q] - (b0 > 0 ? pre[6 * (b0 - 1) + q] : 0.0f);
+        const float2* hi = reinterpret_cast<const float2*>(pre + 6 * (b1 - 1));
+        const float2 h0 = hi[0], h1 = hi[1], h2 = hi[2];
+        float2 l0 = make_float2(0.0f, 0.0f), l1 = l0, l2 = l0;
+        if (b0 > 0) {
+            const float2* lo = reinterpret_cast<const float2*>(pre + 6 * (b0 - 1));
+            l0 = lo[0]; l1 = lo[1]; l2 = lo[2];
+        }
+        const float sm[6] = {h0.x - l0.x, h0.y - l0.y, h1.x - l1.x, h1.y - l1.y, h2.x - l2.x, h2.y - l2.y};
         const float* on = fr + 20 * n;
         const float d0 = on[0] - fr[0], d1 = on[1] - fr[1], d2 = on[2] - fr[2];
         const float T0 = sm[3] - (d1 * sm[2] - d2 * sm[1]);
@@ -1048,6 +1090,22 @@ __device__ __forceinline__ void minus_hv(const Ctx& c, const float* H, const flo
     lanes_sync<kW>();
 }
 
+// out = -H v as minus_hv, returning the dot product out . w, summed as dotw
+// does (the lane's terms in order of i, then the shuffle tree).
+template <int kW = 32>
+__device__ __forceinline__ float minus_hv_dot(const Ctx& c, const float* H, const float* v, float* out,
+                                              const float* w, int n) {
+    float d = 0;
+    for (int i = c.lane; i < n; i += kW) {
+        float sum = 0;
+        for (int j = 0; j < n; ++j) sum += H[j * n + i] * v[j];
+        out[i] = -sum;
+        d += -sum * w[i];
+    }
+    lanes_sync<kW>();
+    return lanes_sum<kW>(d);
+}
+
 template <int kW = 32>
 __device__ __forceinline__ void h_identity(const Ctx& c, float* H, int n) {
     for (int k = c.lane; k < n * n; k += kW) H[k] = 0;
@@ -1059,11 +1117,9 @@ __device__ __forceinline__ void h_identity(const Ctx& c, float* H, int n) {
 // BFGS update of the inverse Hessian (bfgs.h:40-58), applied to both triangles
 template <int kW = 32>
 __device__ __forceinline__ void h_update(const Ctx& c, float* H, const float* p, const float* y,
-                                         float* mhy, float alpha, int n) {
-    const float yp = dotw<kW>(c, y, p, n);
+                                         float* mhy, float alpha, int n, float yp) {
     if (alpha * yp < kEps) return;
-    minus_hv<kW>(c, H, y, mhy, n);
-    const float yhy = -dotw<kW>(c, y, mhy, n);
+    const float yhy = -minus_hv_dot<kW>(c, H, y, mhy, y, n);
     const float r = __frcp_rn(alpha * yp);
     const float a1 = alpha * r, a2 = alpha * alpha * (r * r * yhy + r);
     for (int i = c.lane; i < n; i += kW) {
@@ -1393,8 +1449,7 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                 }
                 const int n = 6 + c.T;
                 float* p = c.s + L.p;
-                minus_hv<kW>(c, c.s + L.h, c.s + L.g, p, n);
-                m.pg = dotw<kW>(c, p, c.s + L.g, n);
+                m.pg = minus_hv_dot<kW>(c, c.s + L.h, c.s + L.g, p, c.s + L.g, n);
                 m.alpha = 1.0f;
                 m.trial = 0;
                 conf_increment<kW>(c, c.s + m.bx_off, p, m.alpha, c.s + L.xnew);
@@ -1413,33 +1468,39 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                         continue;
                     }
                 }
-                // line search done (bfgs.h:120-141)
+                // line search done (bfgs.h:120-141): y = g_new - g, x = x_new,
+                // and the sums g.g, y.p (and y.y at the first iteration) in one
+                // pass and one reduction (each the same per-lane terms and
+                // shuffle tree as a separate dot product)
                 const int n = 6 + c.T;
                 float* g = c.s + L.g;
                 float* gnew = c.s + L.gnew;
                 float* y = c.s + L.y;
-                for (int i = lane; i < n; i += kW) y[i] = gnew[i] - g[i];
-                lanes_sync<kW>();
+                float* H = c.s + L.h;
+                float* p = c.s + L.p;
+                float gg = 0.0f, yp = 0.0f, yy = 0.0f;
+                for (int i = lane; i < n; i += kW) {
+                    const float gi = g[i], yi = gnew[i] - gi;
+                    y[i] = yi;
+                    gg += gi * gi;
+                    yp += yi * p[i];
+                    yy += yi * yi;
+                }
                 m.f0 = f1;
                 copyw<kW>(c, c.s + m.bx_off, c.s + L.xnew, 7 + c.T);
-                const float gg = dotw<kW>(c, g, g, n);
+                if (m.iter == 0) lanes_sum3<kW>(gg, yp, yy);
+                else lanes_sum2<kW>(gg, yp);
                 if (!(sqrtf(gg) >= 1e-5f)) {
                     st = S_BFGS_END;
                     continue;
                 }
                 copyw<kW>(c, g, gnew, n);
-                float* H = c.s + L.h;
-                float* p = c.s + L.p;
-                if (m.iter == 0) {
-                    float yy = dotw<kW>(c, y, y, n);
-                    if (fabsf(yy) > kEps) {
-                        float yp = dotw<kW>(c, y, p, n);
-                        const float d = __fdividef(m.alpha * yp, yy);
-                        for (int i = lane; i < n; i += kW) H[i * n + i] = d;
-                        lanes_sync<kW>();
-                    }
+                if (m.iter == 0 && fabsf(yy) > kEps) {
+                    const float d = __fdividef(m.alpha * yp, yy);
+                    for (int i = lane; i < n; i += kW) H[i * n + i] = d;
+                    lanes_sync<kW>();
                 }
-                h_update<kW>(c, H, p, y, c.s + L.mhy, m.alpha, n);
+                h_update<kW>(c, H, p, y, c.s + L.mhy, m.alpha, n, yp);
                 ++m.iter;
                 st = S_BFGS_ITER;
             } else if (st == S_BFGS_END) {
@@ -1709,7 +1770,7 @@ __device__ float bfgs_receptor(const Ctx& c, const Layout& L, const Tables& Tb, 
                 __syncwarp();
             }
         }
-        h_update(c, H, p, y, c.s + L.mhy, alpha, n);
+        h_update(c, H, p, y, c.s + L.mhy, alpha, n, dotw(c, y, p, n));
     }
     if (!(f0 <= f_orig)) {
         f0 = f_orig;
