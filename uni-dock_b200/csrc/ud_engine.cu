@@ -1348,9 +1348,72 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
     for (;;) {
         const float* eval_x = nullptr;
         float* eval_g = nullptr;
-        // ---- warp-uniform control until the next evaluation is needed
+        // ---- warp-uniform control until the next evaluation is needed; the
+        // states are tested in order of frequency (a line-search result after
+        // nearly every evaluation, then the next BFGS iteration)
         while (eval_x == nullptr) {
-            if (st == S_FETCH) {
+            if (st == S_LS_DONE) {
+                const float f1 = m.last_e;
+                bool accept = (f1 - m.f0 < 0.0001f * m.alpha * m.pg);
+                if (!accept) {
+                    m.alpha *= 0.5f;
+                    if (++m.trial < 10) {
+                        conf_increment<kW>(c, c.s + m.bx_off, c.s + L.p, m.alpha, c.s + L.xnew);
+                        eval_x = c.s + L.xnew;
+                        eval_g = c.s + L.gnew;
+                        continue;
+                    }
+                }
+                // line search done (bfgs.h:120-141): y = g_new - g, x = x_new,
+                // and the sums g.g, y.p (and y.y at the first iteration) in one
+                // pass and one reduction (each the same per-lane terms and
+                // shuffle tree as a separate dot product)
+                const int n = 6 + c.T;
+                float* g = c.s + L.g;
+                float* gnew = c.s + L.gnew;
+                float* y = c.s + L.y;
+                float* H = c.s + L.h;
+                float* p = c.s + L.p;
+                float gg = 0.0f, yp = 0.0f, yy = 0.0f;
+                for (int i = lane; i < n; i += kW) {
+                    const float gi = g[i], yi = gnew[i] - gi;
+                    y[i] = yi;
+                    gg += gi * gi;
+                    yp += yi * p[i];
+                    yy += yi * yi;
+                }
+                m.f0 = f1;
+                copyw<kW>(c, c.s + m.bx_off, c.s + L.xnew, 7 + c.T);
+                if (m.iter == 0) lanes_sum3<kW>(gg, yp, yy);
+                else lanes_sum2<kW>(gg, yp);
+                if (!(sqrtf(gg) >= 1e-5f)) {
+                    st = S_BFGS_END;
+                    continue;
+                }
+                copyw<kW>(c, g, gnew, n);
+                if (m.iter == 0 && fabsf(yy) > kEps) {
+                    const float d = __fdividef(m.alpha * yp, yy);
+                    for (int i = lane; i < n; i += kW) H[i * n + i] = d;
+                    lanes_sync<kW>();
+                }
+                h_update<kW>(c, H, p, y, c.s + L.mhy, m.alpha, n, yp);
+                ++m.iter;
+                st = S_BFGS_ITER;
+            } else if (st == S_BFGS_ITER) {
+                if (m.iter >= m.steps_cap) {
+                    st = S_BFGS_END;
+                    continue;
+                }
+                const int n = 6 + c.T;
+                float* p = c.s + L.p;
+                m.pg = minus_hv_dot<kW>(c, c.s + L.h, c.s + L.g, p, c.s + L.g, n);
+                m.alpha = 1.0f;
+                m.trial = 0;
+                conf_increment<kW>(c, c.s + m.bx_off, p, m.alpha, c.s + L.xnew);
+                eval_x = c.s + L.xnew;
+                eval_g = c.s + L.gnew;
+                st = S_LS_DONE;
+            } else if (st == S_FETCH) {
                 int it;
                 if constexpr (kStream) {  // (ligand, chain) of the next published item
                     int v[3] = {-1, 0, 0};
@@ -1441,67 +1504,6 @@ __device__ __forceinline__ void run_machine(const Batch& B, const Maps& M, const
                 copyw<kW>(c, c.s + L.gorig, c.s + L.g, 6 + c.T);
                 copyw<kW>(c, c.s + L.xorig, c.s + m.bx_off, 7 + c.T);
                 m.iter = 0;
-                st = S_BFGS_ITER;
-            } else if (st == S_BFGS_ITER) {
-                if (m.iter >= m.steps_cap) {
-                    st = S_BFGS_END;
-                    continue;
-                }
-                const int n = 6 + c.T;
-                float* p = c.s + L.p;
-                m.pg = minus_hv_dot<kW>(c, c.s + L.h, c.s + L.g, p, c.s + L.g, n);
-                m.alpha = 1.0f;
-                m.trial = 0;
-                conf_increment<kW>(c, c.s + m.bx_off, p, m.alpha, c.s + L.xnew);
-                eval_x = c.s + L.xnew;
-                eval_g = c.s + L.gnew;
-                st = S_LS_DONE;
-            } else if (st == S_LS_DONE) {
-                const float f1 = m.last_e;
-                bool accept = (f1 - m.f0 < 0.0001f * m.alpha * m.pg);
-                if (!accept) {
-                    m.alpha *= 0.5f;
-                    if (++m.trial < 10) {
-                        conf_increment<kW>(c, c.s + m.bx_off, c.s + L.p, m.alpha, c.s + L.xnew);
-                        eval_x = c.s + L.xnew;
-                        eval_g = c.s + L.gnew;
-                        continue;
-                    }
-                }
-                // line search done (bfgs.h:120-141): y = g_new - g, x = x_new,
-                // and the sums g.g, y.p (and y.y at the first iteration) in one
-                // pass and one reduction (each the same per-lane terms and
-                // shuffle tree as a separate dot product)
-                const int n = 6 + c.T;
-                float* g = c.s + L.g;
-                float* gnew = c.s + L.gnew;
-                float* y = c.s + L.y;
-                float* H = c.s + L.h;
-                float* p = c.s + L.p;
-                float gg = 0.0f, yp = 0.0f, yy = 0.0f;
-                for (int i = lane; i < n; i += kW) {
-                    const float gi = g[i], yi = gnew[i] - gi;
-                    y[i] = yi;
-                    gg += gi * gi;
-                    yp += yi * p[i];
-                    yy += yi * yi;
-                }
-                m.f0 = f1;
-                copyw<kW>(c, c.s + m.bx_off, c.s + L.xnew, 7 + c.T);
-                if (m.iter == 0) lanes_sum3<kW>(gg, yp, yy);
-                else lanes_sum2<kW>(gg, yp);
-                if (!(sqrtf(gg) >= 1e-5f)) {
-                    st = S_BFGS_END;
-                    continue;
-                }
-                copyw<kW>(c, g, gnew, n);
-                if (m.iter == 0 && fabsf(yy) > kEps) {
-                    const float d = __fdividef(m.alpha * yp, yy);
-                    for (int i = lane; i < n; i += kW) H[i * n + i] = d;
-                    lanes_sync<kW>();
-                }
-                h_update<kW>(c, H, p, y, c.s + L.mhy, m.alpha, n, yp);
-                ++m.iter;
                 st = S_BFGS_ITER;
             } else if (st == S_BFGS_END) {
                 if (!(m.f0 <= m.f_orig)) {
