@@ -35,10 +35,10 @@ BOX = 22.5
 SPACING = 0.375
 ADJOINT_POSES = 65536
 # DRAM bytes (read + write) of one search launch of this workload at 1024
-# ligands per step, measured with ncu (dram__bytes_read.sum 17.83 GB +
+# ligands per step, measured with ncu (dram__bytes_read.sum 18.64 GB +
 # dram__bytes_write.sum 0.067 GB, one-pass capture of the first timed launch):
 # about 1.3 % of the launch's algorithmic L2 bytes miss L2
-SEARCH_LAUNCH_DRAM_BYTES = 17.832e9 + 0.0667e9
+SEARCH_LAUNCH_DRAM_BYTES = 18.639e9 + 0.0665e9
 # the same for one adjoint launch of the differentiation workload
 # (dram__bytes_read.sum 657.0 MB + dram__bytes_write.sum 22.9 MB, ncu --set full)
 ADJOINT_LAUNCH_DRAM_BYTES = 657.0e6 + 22.9e6

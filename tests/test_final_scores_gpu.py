@@ -15,7 +15,14 @@ torsional term, unbound -intra), the final order, and the RMSD bounds to the
 best mode.
 
 Bar: 1e-4 relative on the energies, 1e-3 A on lb / ub, and the same order.
-One exception is counted and printed, not hidden: the scoring-path energies
+Two exceptions are counted and printed, not hidden.  A mode with an atom on
+a box wall (within 1e-4 A of it or outside): the receptor-atom energy adds
+1e6 kcal/mol per A of distance outside the box (non_cache.cpp:35-110), so
+coordinates that agree to FP32 rounding (about 1e-6 A) give inter energies
+that differ by up to about a kcal/mol; refinement against a penalised box
+leaves such poses, resting on the wall.  For those modes only the intra
+energy is compared (and the order and RMSD bounds when the orders agree).
+Second, the scoring-path energies
 read the nearest-bin table (model::evali, non_cache::eval with eval_fast), so
 a pair whose r^2 lies within FP32 rounding of a bin edge can fall into either
 bin; the two implementations' coordinates agree to about 1e-7 relative, and
@@ -54,6 +61,15 @@ def within_box(L, pose):
 
 BIN_STEP = 1e-2
 FLIPS = []
+WALL = []
+
+
+def on_wall(L, pose):
+    """An atom (any, as non_cache scores every movable atom) within 1e-4 A of
+    a box wall or outside it."""
+    xyz = L.coords(pose)
+    lo, hi = BOX_CENTER - HALF, BOX_CENTER + HALF
+    return bool(np.any(xyz < lo + 1e-4) or np.any(xyz > hi - 1e-4))
 
 
 def compare(case, L, RL, RM, modes, order_e, receptor):
@@ -63,12 +79,20 @@ def compare(case, L, RL, RM, modes, order_e, receptor):
     assert len(rows) == len(modes)
     src = rows[:, 0].astype(int)
     tie = any(close(rows[k, 1], rows[k + 1, 1]) for k in range(len(rows) - 1))
-    if not tie:
-        assert list(src) == list(range(len(modes))), (case, src, ours[:, 0], rows[:, 1])
+    wall = [on_wall(L, p) for p, _ in modes]
+    same_order = list(src) == list(range(len(modes)))
+    if not tie and not any(wall):
+        assert same_order, (case, src, ours[:, 0], rows[:, 1])
     worst = 0.0
     for k, s in enumerate(src):
         o, r = ours[s], rows[k]
         # ours: affinity, lb, ub, inter+intra, inter, intra, conf-indep, unbound
+        if wall[s]:
+            assert close(o[5], r[6]), (case, k, o, r)
+            WALL.append((case, k, float(o[4]), float(r[5])))
+            if not tie and same_order:
+                assert abs(o[1] - r[2]) <= 1e-3 and abs(o[2] - r[3]) <= 1e-3, (case, k, o, r)
+            continue
         flipped = False
         for a, b in ((o[0], r[1]), (o[3], r[4]), (o[4], r[5]), (o[5], r[6]), (o[6], r[7]), (o[7], r[8])):
             if not close(a, b):
@@ -78,7 +102,7 @@ def compare(case, L, RL, RM, modes, order_e, receptor):
             worst = max(worst, abs(float(a) - float(b)) / max(1.0, abs(float(b))))
         if flipped:
             FLIPS.append((case, k, o.tolist(), r.tolist()))
-        if not tie:
+        if not tie and same_order:
             assert abs(o[1] - r[2]) <= 1e-3 and abs(o[2] - r[3]) <= 1e-3, (case, k, o, r)
     return worst
 
@@ -115,8 +139,10 @@ def test_final_scores_match_reference(receptor, setup, sf, refine):
         worst = max(worst, compare(f"sf {sf} refine {refine} ligand {i}", L, RL, RM, modes, order_e, refine > 0))
         n += len(modes)
     flips = [f for f in FLIPS if f[0].startswith(f"sf {sf} refine {refine} ")]
+    wall = [w for w in WALL if w[0].startswith(f"sf {sf} refine {refine} ")]
     print(f"sf {sf}, refine_step {refine}: {n} modes of {len(ligs)} ligands, worst relative energy difference "
-          f"{worst:.2e}; {len(flips)} mode(s) with a nearest-bin flip: {flips}")
+          f"{worst:.2e}; {len(flips)} mode(s) with a nearest-bin flip: {flips}; {len(wall)} mode(s) on a box wall "
+          f"(case, rank, inter ours, inter reference): {wall}")
     assert len(flips) * 20 <= n
 
 

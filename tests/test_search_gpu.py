@@ -105,7 +105,10 @@ def test_half_warp_chains(small, warps):
     captured graph replays the direct launch exactly, chain energies are their
     poses' energies, and every chain's random stream is its own, so the
     results track the one-chain-per-warp search (same streams, a different
-    FP32 summation order)."""
+    FP32 summation order, so the trajectories part after a few steps): over
+    64 chains per ligand the median chain energies of the two widths differ
+    by at most 0.3 kcal/mol beyond twice the bootstrap standard error of the
+    difference."""
     M, ligs = small
     B = engine.Batch(M, ligs)
     P = dict(exhaustiveness=8, max_step=8, seed=13, form=1, chains_per_block=warps, lanes_per_chain=16)
@@ -117,9 +120,18 @@ def test_half_warp_chains(small, warps):
     np.testing.assert_array_equal(ev1, ev0)
     e2, _ = B.score_grad(np.repeat(np.arange(len(ligs)), 8), p0, 1000.0, 1000.0)
     np.testing.assert_allclose(e2, e0, rtol=1e-4, atol=1e-4)
-    B.search(use_graph=0, **dict(P, lanes_per_chain=32))
+    Pt = dict(P, exhaustiveness=64, use_graph=0)
+    B.search(**Pt)
+    _, e16, _ = B.chains()
+    B.search(**dict(Pt, lanes_per_chain=32))
     _, e32, _ = B.chains()
-    assert abs(np.median(e0) - np.median(e32)) < 0.5
+    rng = np.random.default_rng(5)
+    d = float(np.median(e16) - np.median(e32))
+    se = float(np.std([np.median(rng.choice(e16, len(e16))) - np.median(rng.choice(e32, len(e32)))
+                       for _ in range(1000)]))
+    print(f"{warps} warps per CTA: median chain energy 16 lanes {np.median(e16):.3f}, 32 lanes {np.median(e32):.3f} "
+          f"(diff {d:+.3f}, se {se:.3f})")
+    assert abs(d) <= 0.3 + 2 * se
     with pytest.raises(engine.UdError):
         B.search(**dict(P, lanes_per_chain=8))
 
