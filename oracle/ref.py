@@ -137,6 +137,8 @@ def lib():
         L.udref_final_scores.argtypes = [vp, vp, C.c_int, fp, C.c_int, fp, C.c_int, fp]
         L.udref_maps_bias.argtypes = [vp, C.c_char_p]
         L.udref_ligand_bias.argtypes = [vp, C.c_char_p]
+        L.udref_ad4_bias.argtypes = [vp, C.c_char_p]
+        L.udref_ad4_map_get.argtypes = [vp, C.c_int, fp]
         L.udref_ad4_maps_read.restype = vp
         L.udref_ad4_maps_read.argtypes = [C.c_char_p, fp, C.c_int]
         L.udref_ad4_pair.argtypes = [C.c_int, C.c_float, C.c_int, C.c_float, C.c_float, fp, C.c_int]
@@ -191,6 +193,16 @@ class RefAd4Maps:
         self.h = lib().udref_ad4_maps_read(str(prefix).encode(), _f(w), len(w))
         if not self.h:
             raise RuntimeError("reference could not read AD4 maps " + str(prefix))
+
+    def add_bias(self, bpf: str):
+        """Bias wells added to the AD4 maps (ad4cache::set_bias)."""
+        return lib().udref_ad4_bias(self.h, bpf.encode())
+
+    def get(self, t, n):
+        """The n values of map t (AD type; 35 / 36 for the electrostatic /
+        desolvation map), x fastest, or None when the map is absent."""
+        out = np.zeros(int(n), np.float32)
+        return out if lib().udref_ad4_map_get(self.h, int(t), _f(out)) == n else None
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -336,6 +336,27 @@ int udref_maps_bias(void* mh, const char* text) {
     return (int)M->bias.size();
 }
 
+// --bias on AutoDock 4.2 maps read from files: ad4cache::set_bias
+// (ad4cache.cpp:54-88), as Vina::load_maps applies it (vina.cpp:577-586).
+int udref_ad4_bias(void* mh, const char* text) {
+    auto M = (RefMaps*)mh;
+    const std::vector<bias_element> wells = parse_bpf(text);
+    M->ad4.set_bias(wells);
+    return (int)wells.size();
+}
+
+// Values of AD4 map t (an AD type, or AD_TYPE_SIZE / AD_TYPE_SIZE + 1 for the
+// electrostatic / desolvation map), x fastest; -1 when the map is absent.
+int udref_ad4_map_get(void* mh, int t, float* out) {
+    auto M = (RefMaps*)mh;
+    if (t < 0 || t >= (int)M->ad4.m_grids.size()) return -1;
+    const grid& g = M->ad4.m_grids[t];
+    if (!g.initialized()) return -1;
+    const auto& v = g.m_data.m_data;
+    for (size_t i = 0; i < v.size(); ++i) out[i] = (float)v[i];
+    return (int)v.size();
+}
+
 // --multi_bias: the ligand's own wells.
 int udref_ligand_bias(void* lh, const char* text) {
     auto L = (RefLigand*)lh;

@@ -3,7 +3,8 @@ reference's own code: the wells added to the maps (cache::compute_bias) within
 1e-5 of the map's scale, and energies and gradients against the receptor
 atoms with the maps' wells or a ligand's own wells (non_cache with bias,
 model::bias_list): energies within 1e-4, gradients within 2e-4 (summation
-order over the receptor atoms; see the test)."""
+order over the receptor atoms; see the test).  AutoDock 4.2 maps: the wells
+of ad4cache::set_bias within 1e-5 of each map's scale."""
 import numpy as np
 import pytest
 
@@ -100,3 +101,63 @@ def test_bias_changes_the_maps_and_blocks_term_weights(setup, receptor):
     assert np.abs(M.read(8) - plain.read(8)).max() > 0.01  # O_A: acceptor and OA map wells
     with pytest.raises(engine.UdError):
         M.set_weights(M.weights())
+
+
+# AutoDock 4.2 maps: donor wells go to HD, acceptor wells to OA and NA,
+# aromatic wells to A, map wells to the AD types named or, with none named,
+# to every map including the electrostatic and desolvation maps
+AD4_BPF = """x y z Vset r type
+ 1.0  2.0 -1.5 -2.0 1.2 don
+-3.0  0.5  2.0 -1.5 1.0 acc
+ 2.5 -2.0  1.0 -1.0 1.5 aro
+ 0.0  0.0  0.0 -0.8 2.0 map C OA
+-1.0  3.0 -2.0 -0.6 1.1 map
+ 0.0  0.0  4.0 -1.0 2.0 what
+"""
+
+
+def test_ad4_bias_maps_match_reference(tmp_path):
+    """--bias with --scoring ad4: the engine's AD4 maps are written as AutoGrid
+    files and read by the reference's ad4cache; both then add the same wells
+    (ad4cache::set_bias, ad4cache.cpp:54-88, against ud_maps_add_bias), and
+    every map, the electrostatic and desolvation maps included, agrees within
+    1e-5 of its scale, and every map changed (the untyped map well reaches
+    them all).  A search on the biased maps then runs."""
+    rec = synth.make_receptor(3000, seed=1, with_charges=True)
+    xyz, _, ad, q = engine.parse_receptor_ex(rec.to_pdbqt())
+    M = engine.Maps(xyz, ad, BOX_CENTER, BOX_SIZE, 0.375, sf=engine.SF_AD4, charges=q)
+    prefix = str(tmp_path / "rec")
+    M.write(prefix)
+    R = ref.RefAd4Maps(prefix)
+    dims = M.info()[0]
+    n = int(dims.prod())
+    before = {}
+    for t in range(37):
+        try:
+            before[t] = M.read(t).ravel().copy()
+        except engine.UdError:
+            pass
+    assert R.add_bias(AD4_BPF) == 6
+    M.add_bias(AD4_BPF)
+    changed, compared = set(), 0
+    for t, b in before.items():
+        got = M.read(t).ravel()
+        want = R.get(t, n)
+        assert want is not None, t
+        scale = max(1.0, float(np.abs(want).max()))
+        np.testing.assert_allclose(got, want, rtol=0, atol=1e-5 * scale, err_msg=f"AD4 map {t}")
+        compared += 1
+        if np.any(got != b):
+            changed.add(t)
+    AD_A, AD_C, AD_NA, AD_OA, AD_HD = 1, 0, 9, 10, 12
+    # the all-maps well reaches every map; the typed wells add to their own
+    assert changed == set(before), (sorted(changed), sorted(before))
+    for t in (AD_A, AD_C, AD_NA, AD_OA, AD_HD, 35, 36):
+        if t in before:
+            assert t in changed
+    print(f"AD4 bias: {compared} maps compared with the reference, {len(changed)} changed")
+    # a search on the biased maps runs
+    lig = engine.Ligand(synth.ligand_set(1, seed=4242, dist="lognormal", with_charges=True)[0].to_pdbqt())
+    B = engine.Batch(M, [lig])
+    B.search(exhaustiveness=8, max_step=5, seed=3)
+    assert B.modes(0)

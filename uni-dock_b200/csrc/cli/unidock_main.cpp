@@ -966,8 +966,8 @@ int run(int argc, char** argv) {
     S.spacing = (float)o.num("spacing", 0.375);
     S.autotune = o.has("autotune");
     S.multi_bias = o.has("multi_bias");
-    if ((o.has("bias") || S.multi_bias) && S.sf == UD_SF_AD4)
-        throw std::runtime_error("bias wells with --scoring ad4 are not supported by this build");
+    if (S.multi_bias && S.sf == UD_SF_AD4)
+        throw std::runtime_error("--multi_bias with --scoring ad4 is not supported by this build");
     // search parameters and search_mode presets (main.cpp:644-661)
     const bool batch_mode = o.has("gpu_batch") || o.has("batch") || o.has("ligand_index");
     int exhaustiveness = (int)o.num("exhaustiveness", 8);
@@ -1109,6 +1109,10 @@ int run(int argc, char** argv) {
     if (o.has("maps")) {
         check(ud_maps_load(S.sf, S.weights.data(), (int)S.weights.size(), o.str("maps").c_str(), nullptr, &maps),
               "maps");
+        if (o.has("bias") && S.sf == UD_SF_AD4) {  // AD4.2 maps read, then ad4cache::set_bias (vina.cpp:577-586)
+            const std::string bpf = read_file(o.str("bias"));
+            check(ud_maps_add_bias(maps, bpf.data(), bpf.size(), nullptr), "bias");
+        }
     } else {
         maps = build_maps(S, o.str("receptor"));
         S.receptor_scoring = !no_refine && S.sf != UD_SF_AD4;

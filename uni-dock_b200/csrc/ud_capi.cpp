@@ -1336,11 +1336,42 @@ static BiasRec bias_rec(const BiasElement& e) {
 extern "C" int ud_maps_add_bias(ud_maps m, const char* text, size_t len, void* stream) {
     return guarded([&] {
         if (!m || !text) throw Error(UD_ERR_ARG, "null argument");
-        if (m->desc.ad4) throw Error(UD_ERR_STATE, "bias wells on AutoDock 4.2 maps are not supported by this build");
         if (m->terms_built)
             throw Error(UD_ERR_STATE, "add bias wells before the maps' term decomposition is first used");
         cudaStream_t s = (cudaStream_t)stream;
         const std::vector<BiasElement> wells = parse_bias(std::string(text, len));
+        if (m->desc.ad4) {
+            // AutoDock 4.2: the wells go into the maps only (ad4cache::set_bias);
+            // receptor-atom scoring is for Vina / Vinardo maps
+            std::vector<BiasMapRec> recs;
+            for (const BiasElement& e : wells) {
+                BiasMapRec r{};
+                r.x = e.xyz[0];
+                r.y = e.xyz[1];
+                r.z = e.xyz[2];
+                r.vset = e.vset;
+                r.r = e.r;
+                const uint64_t types = bias_ad4_map_types(e);
+                auto set = [&](int k) {
+                    if (k < 32) r.slots_lo |= 1u << k;
+                    else r.slots_hi |= 1u << (k - 32);
+                };
+                for (size_t k = 0; k < m->slot_types.size(); ++k)
+                    if ((types >> m->slot_types[k]) & 1u) set((int)k);
+                if (types == ~(uint64_t)0) {  // every map: the electrostatic and desolvation maps too
+                    set(m->desc.e_slot);
+                    set(m->desc.d_slot);
+                }
+                recs.push_back(r);
+            }
+            DevBuf<BiasMapRec> d;
+            d.upload(recs.data(), recs.size(), s);
+            cuda_check(launch_bias_maps(d.p, (int)recs.size(), m->desc, m->maps.p, s), "bias maps kernel");
+            refresh_xpairs(m, s);
+            cuda_check(cudaStreamSynchronize(s), "bias maps");
+            m->bias.insert(m->bias.end(), wells.begin(), wells.end());
+            return;
+        }
         std::vector<BiasMapRec> recs;
         for (const BiasElement& e : wells) {
             BiasMapRec r{};

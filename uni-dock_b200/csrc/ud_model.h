@@ -115,6 +115,11 @@ struct BiasElement {
 };
 // The entries of a bias file (its first line is a header; blank lines skipped).
 std::vector<BiasElement> parse_bias(const std::string& text);
+// AD types whose AutoDock 4.2 maps get the well (ad4cache::set_bias,
+// ad4cache.cpp:54-88): don HD; acc OA and NA; aro A; map the AD types named,
+// or with none named every map, the electrostatic and desolvation maps
+// included (all bits set).
+uint64_t bias_ad4_map_types(const BiasElement& b);
 // XS types whose maps get the well (cache::compute_bias, cache.cpp:789-957):
 // acceptor wells the acceptor maps, map wells every map or the types of the
 // named AD types' elements; donor and aromatic wells none.

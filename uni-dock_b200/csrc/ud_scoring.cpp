@@ -443,6 +443,22 @@ std::vector<BiasElement> parse_bias(const std::string& text) {
     return out;
 }
 
+uint64_t bias_ad4_map_types(const BiasElement& b) {
+    auto bit = [](int t) { return (uint64_t)1 << t; };
+    switch (b.type) {
+        case BIAS_DON: return bit(AD_HD);
+        case BIAS_ACC: return bit(AD_OA) | bit(AD_NA);
+        case BIAS_ARO: return bit(AD_A);
+        case BIAS_MAP: {
+            if (b.ad_list.empty()) return ~(uint64_t)0;
+            uint64_t m = 0;
+            for (int ad : b.ad_list) m |= bit(ad);
+            return m;
+        }
+        default: return 0;
+    }
+}
+
 uint64_t bias_map_types(const BiasElement& b) {
     auto bit = [](int t) { return (uint64_t)1 << t; };
     uint64_t m = 0;
