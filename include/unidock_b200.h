@@ -369,9 +369,12 @@ int ud_optimize(ud_batch batch, const int* pose_ligand, float* poses, int n_pose
  * (Vina::set_bias + cache::compute_bias, vina.cpp:1472-1480, cache.cpp:789-957):
  * every map point gets Vset exp(-d^2/r^2) on the maps the well reaches when it
  * is below -0.01; the wells also enter the scoring against the receptor atoms
- * (refinement, ud_score_terms_receptor).  Wells accumulate over calls.  The
- * maps then have no term decomposition (ud_maps_set_weights, weight
- * gradients: UD_ERR_STATE). */
+ * (refinement, ud_score_terms_receptor).  On AutoDock 4.2 maps the wells go
+ * into the maps only, as ad4cache::set_bias (ad4cache.cpp:54-88) places them:
+ * don -> HD, acc -> OA and NA, aro -> A, map -> the AD types named, or every
+ * map with the electrostatic and desolvation maps when none is named.  Wells
+ * accumulate over calls.  The maps then have no term decomposition
+ * (ud_maps_set_weights, weight gradients: UD_ERR_STATE). */
 int ud_maps_add_bias(ud_maps maps, const char* bpf, size_t len, void* stream);
 /* Ligand `lig`'s own wells (--multi_bias, Vina::set_batch_bias,
  * vina.cpp:1482-1493), used instead of the maps' when it is scored against
