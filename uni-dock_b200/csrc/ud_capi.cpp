@@ -2724,6 +2724,8 @@ extern "C" int ud_stream_create(ud_maps maps, const ud_search_params* params, co
         cuda_check(prepare_stream_post(st->view(), st->cap, st->refined), "stream post-processing kernels");
         if (sp.chains_per_block == 0) sp.chains_per_block = default_chains_per_block(st->view(), 32, true);
         const int per_sm = stream_blocks_per_sm(st->view(), sp.chains_per_block);
+        if (per_sm < 1)
+            throw Error(UD_ERR_CAPACITY, "a CTA of the stream's largest ligand layout does not fit an SM");
         const int blocks = per_sm * n_sm;
         sv.reserve_every = n_sm >= 2 * kStreamReserveSms ? n_sm / kStreamReserveSms : 0;
         cuda_check(launch_search_stream(st->view(), maps_view(maps), tables_view(maps), sp, sv, st->d_poses.p,

@@ -2699,10 +2699,13 @@ int stream_blocks_per_sm(const DeviceBatchView& b, int warps) {
     dev::Layout L = dev::make_layout(b.max_atoms, b.max_torsions);
     size_t smem = (size_t)warps * L.total * sizeof(float);
     const auto kern = b.ad4 ? dev::stream_kernel<true> : dev::stream_kernel<false>;
-    smem_attr((const void*)kern, smem);
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, warps * 32, smem) != cudaSuccess) return 1;
-    return nb > 0 ? nb : 1;
+    if (smem_attr((const void*)kern, smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, warps * 32, smem) != cudaSuccess) {
+        cudaGetLastError();  // a CTA this size does not fit: no error left behind for the next launch
+        return 0;
+    }
+    return nb;
 }
 
 cudaError_t launch_optimize(const DeviceBatchView& b, const DeviceMapsView& m,
@@ -2871,11 +2874,13 @@ int search_blocks_per_sm(const DeviceBatchView& b, int warps, int lanes_per_chai
     const int lanes = lanes_per_chain == 16 ? 16 : 32;
     size_t smem = (size_t)warps * (32 / lanes) * L.total * sizeof(float);
     const auto kern = search_kernel_for(b.ad4 != 0, lanes);
-    smem_attr((const void*)kern, smem);
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, warps * 32, smem) != cudaSuccess)
-        return 1;
-    return nb > 0 ? nb : 1;
+    if (smem_attr((const void*)kern, smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, warps * 32, smem) != cudaSuccess) {
+        cudaGetLastError();  // a CTA this size does not fit: no error left behind for the next launch
+        return 0;
+    }
+    return nb;
 }
 
 // ---------------------------------------------------------------- allocation-free search
