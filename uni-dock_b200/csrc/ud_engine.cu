@@ -754,9 +754,10 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
     lanes_sync<kW>();
     // Pairs in 32-slot groups made of kPairPasses lane ranges that are each a
     // matching (no atom twice within a range), taken kW slots (a window of
-    // whole ranges) at a time: table rows of kPairBatch windows are loaded
-    // before any is consumed, then each range adds its forces in turn (no
-    // atomics, a fixed summation order).
+    // whole ranges) at a time; the ranges add their forces in a fixed order
+    // of passes (no atomics, a fixed summation order).  Vina / Vinardo run
+    // the software-pipelined loop (UD_PAIR_PIPE); AD4 the loop after it,
+    // which loads the table rows of kPairBatch windows before consuming any.
     static_assert(kW % kPairPassWidth == 0, "a window holds whole lane ranges");
     constexpr int kWinShift = kW == 32 ? 5 : 4;
     constexpr int kWinPasses = kW / kPairPassWidth;
