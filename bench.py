@@ -12,6 +12,7 @@ whole C-ABI path from PDBQT text to written poses with host buffers.
 from __future__ import annotations
 
 import argparse
+import contextlib
 import json
 import os
 import statistics
@@ -636,7 +637,27 @@ def run_stream(args):
 
 
 # ------------------------------------------------------------------ reference CPU path
+@contextlib.contextmanager
+def c_stdout_to_stderr():
+    """The reference's own code prints diagnostics with printf; while it runs,
+    file descriptor 1 points at stderr so that stdout carries the JSON line
+    alone."""
+    sys.stdout.flush()
+    saved = os.dup(1)
+    os.dup2(2, 1)
+    try:
+        yield
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+
+
 def reference_cpu(sample, step_index, threads=None, seed=7):
+    with c_stdout_to_stderr():
+        return _reference_cpu(sample, step_index, threads, seed)
+
+
+def _reference_cpu(sample, step_index, threads=None, seed=7):
     """The reference's CPU docking at the screen's settings on `sample` ligands
     of the same generator, all the reference's own code (oracle/_ref, built
     from its sources): its parallel Monte-Carlo search (parallel_mc over
@@ -688,6 +709,11 @@ def config0_files(d):
 
 
 def config0_reference(threads=None):
+    with c_stdout_to_stderr():
+        return _config0_reference(threads)
+
+
+def _config0_reference(threads=None):
     """configs[0] through the reference's stock CPU docking of one ligand
     (Vina::set_receptor .. global_search, the reference CLI's --cpu path):
     wall clock of the whole call and the best mode's energy."""
