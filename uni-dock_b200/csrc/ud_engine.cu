@@ -246,9 +246,12 @@ static_assert(UD_FORCE_SPLIT == 1 || UD_FORCE_SPLIT == 2, "1 or 2 force arrays")
 #define UD_STAGE_ATOMS 1
 #endif
 // UD_PAIR_PIPE: pair windows software-pipelined one table row ahead
-// (Vina / Vinardo)
+// (UD_PAIR_PIPE_AD4: the AD4 instantiation too, with its E and G rows)
 #ifndef UD_PAIR_PIPE
 #define UD_PAIR_PIPE 1
+#endif
+#ifndef UD_PAIR_PIPE_AD4
+#define UD_PAIR_PIPE_AD4 1
 #endif
 __device__ __forceinline__ float2 ld_stream2(const float2* p) {
 #if UD_NA_LOADS
@@ -755,9 +758,9 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
     // Pairs in 32-slot groups made of kPairPasses lane ranges that are each a
     // matching (no atom twice within a range), taken kW slots (a window of
     // whole ranges) at a time; the ranges add their forces in a fixed order
-    // of passes (no atomics, a fixed summation order).  Vina / Vinardo run
-    // the software-pipelined loop (UD_PAIR_PIPE); AD4 the loop after it,
-    // which loads the table rows of kPairBatch windows before consuming any.
+    // of passes (no atomics, a fixed summation order).  The software-pipelined
+    // loop (UD_PAIR_PIPE) runs by default; the loop after it loads the table
+    // rows of kPairBatch windows before consuming any.
     static_assert(kW % kPairPassWidth == 0, "a window holds whole lane ranges");
     constexpr int kWinShift = kW == 32 ? 5 : 4;
     constexpr int kWinPasses = kW / kPairPassWidth;
@@ -766,11 +769,11 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
     // window is worked on, so its latency is off the window's dependent chain
     uint32_t pr_next = (UD_PAIR_PREFETCH && n_groups > 0) ? __ldg(c.pairs() + c.lane) : kPairPad;
 #if UD_PAIR_PIPE
-    // Software-pipelined windows (Vina / Vinardo): the table row of window
+    // Software-pipelined windows: the table row (AD4: and the E and G rows) of window
     // g + UD_PAIR_PIPE is requested before window g's forces are added (and
     // its pair word one window earlier), so each window's L2 round trip
     // overlaps the work of the windows before it.
-    if constexpr (!kAD4) {
+    if constexpr (!kAD4 || UD_PAIR_PIPE_AD4) {
         constexpr int kPipe = UD_PAIR_PIPE;
         constexpr int kSplit = UD_FORCE_SPLIT;
         const int range = c.lane / kPairPassWidth;
@@ -780,11 +783,17 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
             uint32_t pr;   // pair word, kPairPad when the slot adds nothing
             float4 t;      // table row (e_i, dor_i, e_i+1, dor_i+1)
             float rem, rx, ry, rz;
+            float4 te, tg; // AD4: the shared E and G rows and the pair's scales of them
+            float2 cf;
         };
-        auto request = [&](uint32_t w, Stage& q) {
+        auto request = [&](int g, uint32_t w, Stage& q) {
             q.pr = kPairPad;
             q.t = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             q.rem = q.rx = q.ry = q.rz = 0.0f;
+            if constexpr (kAD4) {
+                q.te = q.tg = q.t;
+                q.cf = make_float2(0.0f, 0.0f);
+            }
             if (w != kPairPad) {
                 const float4 pa = xyz[w & 0xFF], pb = xyz[(w >> 8) & 0xFF];
                 q.rx = pb.x - pa.x; q.ry = pb.y - pa.y; q.rz = pb.z - pa.z;
@@ -794,6 +803,11 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
                     const int i1 = (int)rf;
                     q.rem = rf - i1;
                     q.t = ld_stream4(Tb.smooth4 + (size_t)(w >> 16) * Tb.n_bins + i1);
+                    if constexpr (kAD4) {  // + q_a q_b E(r) + (|q_a| V_b + |q_b| V_a) G(r)
+                        q.cf = __ldg(c.coef() + (g << kWinShift) + c.lane);
+                        q.te = __ldg(Tb.smooth4 + (size_t)kAd4RowE * Tb.n_bins + i1);
+                        q.tg = __ldg(Tb.smooth4 + (size_t)kAd4RowG * Tb.n_bins + i1);
+                    }
                     q.pr = w;
                 }
             }
@@ -801,18 +815,25 @@ __device__ __forceinline__ float eval_deriv(const Ctx& c, const Layout& L, const
         auto word = [&](int g) { return g < n_groups ? __ldg(pw + (g << kWinShift)) : kPairPad; };
         Stage q[kPipe + 1];
 #pragma unroll
-        for (int k = 0; k < kPipe; ++k) request(word(k), q[k]);
+        for (int k = 0; k < kPipe; ++k) request(k, word(k), q[k]);
         uint32_t w_next = word(kPipe);
         for (int g = 0; g < n_groups; ++g) {
             const uint32_t w1 = w_next;
             w_next = word(g + kPipe + 1);
-            request(w1, q[kPipe]);
+            request(g + kPipe, w1, q[kPipe]);
             const Stage& h = q[0];
             float fx = 0, fy = 0, fz = 0;
             const bool live = h.pr != kPairPad;
             if (live) {
-                float ep = h.t.x + h.rem * (h.t.z - h.t.x);
-                float dor = kExactPairs ? 2.0f * Tb.factor * (h.t.z - h.t.x) : h.t.y + h.rem * (h.t.w - h.t.y);
+                float4 t = h.t;
+                if constexpr (kAD4) {
+                    t.x += h.cf.x * h.te.x + h.cf.y * h.tg.x;
+                    t.y += h.cf.x * h.te.y + h.cf.y * h.tg.y;
+                    t.z += h.cf.x * h.te.z + h.cf.y * h.tg.z;
+                    t.w += h.cf.x * h.te.w + h.cf.y * h.tg.w;
+                }
+                float ep = t.x + h.rem * (t.z - t.x);
+                float dor = kExactPairs ? 2.0f * Tb.factor * (t.z - t.x) : t.y + h.rem * (t.w - t.y);
                 fx = dor * h.rx; fy = dor * h.ry; fz = dor * h.rz;
                 if (ep > 0 && v_intra < 0.1f * kMaxFl) {
                     float tmp = (v_intra < kEps) ? 0 : __fdividef(v_intra, v_intra + ep);
