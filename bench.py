@@ -696,11 +696,11 @@ def _reference_cpu(sample, step_index, threads=None, seed=7):
     return len(ligs) / t_total, threads
 
 
-CONFIG0 = "plain single docking (configs[0]): Vina, 3000-atom receptor, 22.5 A box at 0.375 A, one ligand of 24 " \
-          "heavy atoms and 6 torsions, exhaustiveness 8, num_modes 9, heuristic step count, refinement 3 steps"
+SINGLE_DOCKING = "plain single docking: Vina, 3000-atom receptor, 22.5 A box at 0.375 A, one ligand of 24 " \
+    "heavy atoms and 6 torsions, exhaustiveness 8, num_modes 9, heuristic step count, refinement 3 steps"
 
 
-def config0_files(d):
+def single_docking_files(d):
     from unidock_tools import synth
     rp, lp = Path(d) / "rec.pdbqt", Path(d) / "lig.pdbqt"
     rp.write_text(synth.make_receptor(3000, seed=1).to_pdbqt())
@@ -708,35 +708,35 @@ def config0_files(d):
     return rp, lp
 
 
-def config0_reference(threads=None):
+def single_docking_reference(threads=None):
     with c_stdout_to_stderr():
-        return _config0_reference(threads)
+        return _single_docking_reference(threads)
 
 
-def _config0_reference(threads=None):
-    """configs[0] through the reference's stock CPU docking of one ligand
+def _single_docking_reference(threads=None):
+    """The plain single docking through the reference's stock CPU docking of one ligand
     (Vina::set_receptor .. global_search, the reference CLI's --cpu path):
     wall clock of the whole call and the best mode's energy."""
     sys.path.insert(0, str(ROOT))
     from oracle import ref
     threads = threads or os.cpu_count()
     with tempfile.TemporaryDirectory() as d:
-        rp, lp = config0_files(d)
+        rp, lp = single_docking_files(d)
         t0 = time.perf_counter()
         e = ref.vina_dock(rp, lp, np.zeros(3), np.full(3, BOX), SPACING, 8, 9, 5, threads)
         t = time.perf_counter() - t0
-    return {"workload": CONFIG0, "path": "reference CPU Vina::global_search (stock CPU path, whole call)",
+    return {"workload": SINGLE_DOCKING, "path": "reference CPU Vina::global_search (stock CPU path, whole call)",
             "seconds": round(t, 3), "cores": threads, "best_energy": round(float(e[0]), 3)}
 
 
-def config0_engine():
-    """configs[0] through this engine's C ABI, one ligand: receptor parse, map
+def single_docking_engine():
+    """The plain single docking through this engine's C ABI, one ligand: receptor parse, map
     build, ligand parse, search (exhaustiveness 8, the heuristic step count),
     clustering, refinement and final scores, output text; wall clock."""
     import torch
     from unidock_tools import engine
     with tempfile.TemporaryDirectory() as d:
-        rp, lp = config0_files(d)
+        rp, lp = single_docking_files(d)
         for rep in range(2):  # the first call pays module loading and allocation
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -748,7 +748,7 @@ def config0_engine():
             text = B.write(0)
             torch.cuda.synchronize()
             t = time.perf_counter() - t0
-    return {"workload": CONFIG0, "path": "this engine's C ABI: parse, maps, search, clustering, refinement, output",
+    return {"workload": SINGLE_DOCKING, "path": "this engine's C ABI: parse, maps, search, clustering, refinement, output",
             "seconds": round(t, 3), "best_energy": round(float(B.modes(0)[0][1][0]), 3),
             "output_bytes": len(text)}
 
@@ -765,9 +765,9 @@ def run_reference(args, rank, world):
         vals.append(v)
     value = len(vals) * sample / sum(sample / v for v in vals)
     try:
-        c0 = config0_reference()
-    except Exception as ex:  # the configs[0] leg never blocks the line
-        c0 = {"workload": CONFIG0, "unavailable": str(ex)}
+        c0 = single_docking_reference()
+    except Exception as ex:  # the single-docking leg never blocks the line
+        c0 = {"workload": SINGLE_DOCKING, "unavailable": str(ex)}
     return {
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "ligands/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * sample / value, 1),
@@ -781,7 +781,7 @@ def run_reference(args, rank, world):
                                    "(128 tasks of monte_carlo::operator(), 20 MC steps each) then refinement and "
                                    "final scores of every mode, the reference's own sources built by oracle/Makefile"},
         "e2e": {"value": round(value, 4), "unit": "ligands/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "configs0": c0,
+        "single_docking": c0,
     }
 
 
@@ -867,9 +867,9 @@ def main():
                                        "kind": "reference", "sample": f"unavailable: {ex}"}
     if res is not None and args.impl != "reference" and world == 1 and not args.no_cpu_baseline:
         try:
-            res["configs0"] = {"engine": config0_engine(), "reference": config0_reference()}
+            res["single_docking"] = {"engine": single_docking_engine(), "reference": single_docking_reference()}
         except Exception as ex:
-            res["configs0"] = {"workload": CONFIG0, "unavailable": str(ex)}
+            res["single_docking"] = {"workload": SINGLE_DOCKING, "unavailable": str(ex)}
     if res is not None:
         print(json.dumps(res), flush=True)
 
