@@ -42,7 +42,7 @@ def test_help_lists_every_reference_option():
     (["--receptor", "r.pdbqt", "--gpu_batch", "a.pdbqt"], "Need to specify an output directory for batch mode."),
     (["--receptor", "r.pdbqt", "--gpu_batch", "a.pdbqt", "--dir", "/nonexistent_dir_x"], "does not exist"),
     (["--receptor", "r.pdbqt", "--ligand", "a.pdbqt", "--scoring", "xyz"], "Scoring function xyz unknown."),
-    (["--receptor", "r.pdbqt", "--ligand", "a.pdbqt", "--flex", "f.pdbqt"], "--flex is not supported by this build"),
+    (["--receptor", "r.pdbqt", "--ligand", "a.pdbqt", "--flex", "f.pdbqt"], "--flex is not supported by this engine"),
     (["--ligand", "a.pdbqt"], "The receptor or affinity maps must be specified."),
     (["--bogus", "1"], "unrecognised option '--bogus'"),
     (["--receptor", "r.pdbqt", "--ligand", "a.pdbqt", "--gpu_batch", "b.pdbqt", "--dir", "."],

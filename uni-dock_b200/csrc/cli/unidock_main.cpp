@@ -44,7 +44,7 @@ struct OptSpec {
 
 const OptSpec kOptions[] = {
     {"receptor", 0, "rigid part of the receptor (PDBQT)", "Input"},
-    {"flex", 0, "flexible side chains (not supported by this build)", "Input"},
+    {"flex", 0, "flexible side chains (not supported by this engine)", "Input"},
     {"ligand", 2, "ligand (PDBQT or SDF)", "Input"},
     {"ligand_index", 0, "file containing paths to ligands (PDBQT or SDF)", "Input"},
     {"paired_batch_size", 0, "If > 0, uses batching for one-ligand-one-protein docking, with json config in "
@@ -74,7 +74,7 @@ const OptSpec kOptions[] = {
                      "--score_only", "Advanced"},
     {"force_even_voxels", 1, "calculated grid maps will have an even number of voxels in each dimension",
      "Advanced"},
-    {"randomize_only", 1, "randomize input (not supported by this build)", "Advanced"},
+    {"randomize_only", 1, "randomize input (not supported by this engine)", "Advanced"},
     {"weight_gauss1", 0, "gauss_1 weight", "Advanced"},
     {"weight_gauss2", 0, "gauss_2 weight", "Advanced"},
     {"weight_repulsion", 0, "repulsion weight", "Advanced"},
@@ -805,7 +805,7 @@ bool read_ligand_config(const std::string& path, const float* box, PairedComplex
 // refine_step and seed.
 int run_paired(const Setup& S0, const std::string& config, const std::string& dir, int batch_size, const float* box,
                bool local_only) {
-    if (local_only) throw std::runtime_error("--local_only with --paired_batch_size is not supported by this build");
+    if (local_only) throw std::runtime_error("--local_only with --paired_batch_size is not supported by this engine");
     Setup S = S0;
     S.sf = UD_SF_VINA;
     S.weights = {-0.035579f, -0.005156f, 0.840245f, -0.035069f, -0.587439f, 50.0f, 0.05846f};
@@ -936,7 +936,7 @@ int run(int argc, char** argv) {
     }
     for (const char* unsupported : {"flex", "randomize_only"})
         if (o.has(unsupported))
-            throw std::runtime_error(std::string("--") + unsupported + " is not supported by this build");
+            throw std::runtime_error(std::string("--") + unsupported + " is not supported by this engine");
     Setup S;
     const std::string sf_name = o.str("scoring", "vina");
     if (sf_name == "vina") {
@@ -967,7 +967,7 @@ int run(int argc, char** argv) {
     S.autotune = o.has("autotune");
     S.multi_bias = o.has("multi_bias");
     if (S.multi_bias && S.sf == UD_SF_AD4)
-        throw std::runtime_error("--multi_bias with --scoring ad4 is not supported by this build");
+        throw std::runtime_error("--multi_bias with --scoring ad4 is not supported by this engine");
     // search parameters and search_mode presets (main.cpp:644-661)
     const bool batch_mode = o.has("gpu_batch") || o.has("batch") || o.has("ligand_index");
     int exhaustiveness = (int)o.num("exhaustiveness", 8);
@@ -1042,7 +1042,7 @@ int run(int argc, char** argv) {
     if (batch_mode && !o.has("dir")) throw std::runtime_error("Need to specify an output directory for batch mode.");
     if (o.has("dir") && !is_directory(dir)) throw std::runtime_error("Directory " + dir + " does not exist.");
     if (ligand_names.size() > 1) throw std::runtime_error("docking several --ligand files together is not supported "
-                                                          "by this build; use --gpu_batch");
+                                                          "by this engine; use --gpu_batch");
     // box
     const bool autobox = o.has("autobox");
     for (int i = 0; i < 3; ++i) {

@@ -1407,7 +1407,7 @@ extern "C" int ud_batch_set_bias(ud_batch b, int lig, const char* text, size_t l
     return guarded([&] {
         if (!b || (len > 0 && !text)) throw Error(UD_ERR_ARG, "null argument");
         if (lig < 0 || lig >= (int)b->ligs.size()) throw Error(UD_ERR_ARG, "ligand out of range");
-        if (b->maps->desc.ad4) throw Error(UD_ERR_STATE, "bias wells with AutoDock 4.2 maps are not supported by this build");
+        if (b->maps->desc.ad4) throw Error(UD_ERR_STATE, "bias wells with AutoDock 4.2 maps are not supported by this engine");
         b->lig_bias.resize(b->ligs.size());
         b->lig_bias[lig].clear();
         for (const BiasElement& e : parse_bias(std::string(text ? text : "", len))) b->lig_bias[lig].push_back(bias_rec(e));
